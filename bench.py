@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 gap-affine WFA engine (one JSON line on rank 0).
+
+A step is one pass of the path over one batch: pack -> align (scores and
+WFA2-style CIGARs) -> CIGAR compaction, for the whole batch.
+
+  value  GCUPS (reference formula sum(m*n)/t/1e9, wfa_gpu.cu:130-133) with the
+         batch resident in HBM, time from CUDA events on the engine's stream
+  e2e    the same through tsu_align_batch with pinned HOST buffers: H2D of
+         the sequences, the device work and D2H of scores + CIGARs per step
+
+Default workload: 1,000,000 pairs of 1,000 bp, 5% edits (equal sub/ins/del),
+penalties 4/6/2, seeded synthetic data.  `--impl reference` times the CPU
+path (the oracle's WFA, the stand-in for the reference's WFA2-lib check,
+wfa_gpu.cu:150-166) on all host cores over a bounded sample of the same
+workload.  Under torchrun each rank aligns its own batch (weak scaling, no
+collective on the data path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 0x5453554E414D49
+METRIC = "GCUPS & pairs/s on 1 B200 vs plain launch; serving p50/p99 latency; bit-exact"
+WORKLOADS = {
+    # name: (pairs, length, edit rate, seed index)
+    "c1": (10_000, 150, 0.02, 0),
+    "c2": (1_000_000, 1_000, 0.05, 1),
+    "c3": (20_000, 10_000, 0.15, 2),
+}
+PEN = (4, 6, 2)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_batch(workload: str, rank: int):
+    import tsunami_pact_b200 as T
+
+    n, L, rate, si = WORKLOADS[workload]
+    lengths = np.full(n, L, np.int32)
+    rates = np.full(n, rate)
+    # each rank gets its own pairs: indices [rank*n, (rank+1)*n)
+    return T.gen_batch(SEED + si, lengths, rates, first=rank * n)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/*.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen, target_s=10.0):
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    n = len(plen)
+    probe = min(n, max(256, cores * 64))
+    t0 = time.perf_counter()
+    O.align_batch_arrays(pbuf, poff[:probe], plen[:probe], tbuf, toff[:probe], tlen[:probe], *PEN, cigar=True,
+                         threads=cores)
+    dt = time.perf_counter() - t0
+    rate = probe / max(dt, 1e-6)
+    sample = int(min(n, max(probe, rate * target_s)))
+    t0 = time.perf_counter()
+    O.align_batch_arrays(pbuf, poff[:sample], plen[:sample], tbuf, toff[:sample], tlen[:sample], *PEN, cigar=True,
+                         threads=cores)
+    dt = time.perf_counter() - t0
+    cells = float(np.sum(plen[:sample].astype(np.float64) * tlen[:sample]))
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": "port",
+            "pairs_per_s": sample / dt,
+            "sample": f"first {sample} pairs of the workload, scores + CIGARs, {cores} threads, {dt:.1f} s"}
+
+
+def run_reference(args, workload):
+    """CPU path on the host cores, rank 0 only (other ranks exit 0)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    n_all, L, rate, si = WORKLOADS[workload]
+    cores = os.cpu_count() or 1
+    import tsunami_pact_b200 as T
+
+    # a bounded sample of the same workload: sized so each step is ~5-10 s
+    probe = max(256, cores * 64)
+    lengths = np.full(probe, L, np.int32)
+    pb, po, pl, tb, to, tl = T.gen_batch(SEED + si, lengths, np.full(probe, rate))
+    t0 = time.perf_counter()
+    O.align_batch_arrays(pb, po, pl, tb, to, tl, *PEN, cigar=True, threads=cores)
+    r = probe / max(time.perf_counter() - t0, 1e-6)
+    sample = int(min(n_all, max(probe, r * 6.0)))
+    pb, po, pl, tb, to, tl = T.gen_batch(SEED + si, np.full(sample, L, np.int32), np.full(sample, rate))
+    cells = float(np.sum(pl.astype(np.float64) * tl))
+    for _ in range(args.warmup):
+        O.align_batch_arrays(pb, po[: min(sample, probe)], pl[: min(sample, probe)], tb, to[: min(sample, probe)],
+                             tl[: min(sample, probe)], *PEN, cigar=True, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.align_batch_arrays(pb, po, pl, tb, to, tl, *PEN, cigar=True, threads=cores)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    gcups = cells / t / 1e9
+    out = {
+        "metric": METRIC, "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
+        "impl": "reference",
+        "config": {"workload": f"{workload}: {n_all} pairs x {L} bp, {rate:.0%} edits, penalties 4/6/2",
+                   "sample_pairs": sample},
+        "pairs_per_s": sample / t,
+        "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": cores, "kind": "port",
+                         "sample": f"first {sample} pairs of the workload per step, scores + CIGARs, "
+                                   f"{cores} threads (WFA2-lib absent: the oracle's CPU WFA)"},
+        "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tsunami", choices=["tsunami", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--score-only", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    workload = args.workload
+    if args.impl == "reference":
+        run_reference(args, workload)
+        return
+
+    import torch
+
+    import tsunami_pact_b200 as T
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n_pairs, L, rate, si = WORKLOADS[workload]
+    pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank)
+    cells = float(np.sum(plen.astype(np.float64) * tlen))
+    want_cigar = not args.score_only
+    al = T.Aligner(*PEN, device=local)
+
+    # ---- value: batch resident in HBM ----------------------------------
+    dev = torch.device("cuda", local)
+    d_p = torch.from_numpy(pbuf).to(dev)
+    d_t = torch.from_numpy(tbuf).to(dev)
+    d_po, d_pl, d_to, d_tl = (torch.from_numpy(x).to(dev) for x in (poff, plen, toff, tlen))
+    d_sc = torch.zeros(n_pairs, dtype=torch.int32, device=dev)
+    d_off = torch.zeros(n_pairs + 1, dtype=torch.int64, device=dev)
+    cap = n_pairs * 64 + 1024
+    d_runs = torch.zeros(cap, dtype=torch.int32, device=dev) if want_cigar else None
+
+    def dev_step():
+        nonlocal d_runs, cap
+        try:
+            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off if want_cigar else None)
+        except T.AlignError as e:
+            if e.code != 5:
+                raise
+            cap = int(cap * 2)
+            d_runs = torch.zeros(cap, dtype=torch.int32, device=dev)
+            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off)
+
+    for _ in range(max(args.warmup, 1)):
+        nruns = dev_step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, align_ms, launches, work_cells = [], [], 0, 0
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        nruns = dev_step()
+        tm = al.timing()
+        step_ms.append(tm["total_ms"])
+        align_ms.append(tm["align_ms"])
+        launches += int(tm["kernel_launches"])
+        work_cells = tm["cells"]
+    barrier()
+    wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
+    clk = clocks.stop()
+    ms = max_over_ranks(float(np.mean(step_ms)))
+    value = cells * world / (ms / 1e3) / 1e9
+    pairs_s = n_pairs * world / (ms / 1e3)
+
+    # ---- e2e: host buffers (pinned) through tsu_align_batch ---------------
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.empty(a.shape, dtype={np.uint8: torch.uint8, np.int64: torch.int64,
+                                            np.int32: torch.int32}[a.dtype.type], pin_memory=True)
+            t.numpy()[...] = a
+            return t
+
+        hp = [pinned(x) for x in (pbuf, poff, plen, tbuf, toff, tlen)]
+        h_sc = torch.empty(n_pairs, dtype=torch.int32, pin_memory=True)
+        h_off = torch.empty(n_pairs + 1, dtype=torch.int64, pin_memory=True)
+        h_runs = torch.empty(max(nruns, 1) + 4096, dtype=torch.int32, pin_memory=True)
+        outs = (h_sc.numpy(), h_off.numpy(), h_runs.numpy().view(np.uint32)) if want_cigar else None
+
+        def e2e_step():
+            return al.align_arrays(*(t.numpy() for t in hp), cigar=want_cigar, out=outs)
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_step()
+        barrier()
+        e_ms, hb, db = [], 0, 0
+        for _ in range(args.steps):
+            e2e_step()
+            tm = al.timing()
+            e_ms.append(tm["total_ms"])
+            hb, db = tm["h2d_bytes"], tm["d2h_bytes"]
+            launches_e2e = int(tm["kernel_launches"])
+        barrier()
+        ems = max_over_ranks(float(np.mean(e_ms)))
+        e2e = {"value": cells * world / (ems / 1e3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": int(hb),
+               "d2h_bytes_per_step": int(db), "ms_per_step": ems, "pairs_per_s": n_pairs * world / (ems / 1e3)}
+        # correctness of the e2e output against the device leg
+        if want_cigar and not np.array_equal(outs[0], d_sc.cpu().numpy()):
+            raise SystemExit("e2e scores differ from the device-resident leg")
+
+    # ---- roofline of the align kernel ------------------------------------
+    peak, peak_kind = measured_peaks()
+    a_ms = float(np.mean(align_ms))
+    words = 2 * ((L + 31) // 32 + 1)
+    per_pair_in = words * 8
+    per_pair_out = 4 + (4 * nruns / n_pairs if want_cigar else 0)
+    hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
+    algo = n_pairs * (per_pair_in + per_pair_out) + hist_bytes
+    achieved = algo / (a_ms / 1e3) / 1e9
+    traffic = load_traffic(f"align_{workload}")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
+            "align_kernel<score>", "kernel_ms": a_ms,
+            "algorithmic_bytes_per_launch": algo,
+            "cells_per_s": work_cells / (a_ms / 1e3)}
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen)
+        out = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
+            "config": {"workload": f"{workload}: {n_pairs} pairs x {L} bp per GPU, {rate:.0%} edits, penalties 4/6/2",
+                       "output": "scores + CIGARs" if want_cigar else "scores only",
+                       "l2": f"inputs larger than L2 ({(pbuf.nbytes + tbuf.nbytes) / 1e9:.1f} GB ASCII per GPU)",
+                       "parallelism": f"data-parallel over pairs, {world} GPU(s)"},
+            "pairs_per_s": pairs_s,
+            "wall_ms_per_step": wall_ms,
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    al.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+/*
+ * tsunami_b200.h -- C ABI of the B200-native gap-affine WaveFront Alignment
+ * (WFA) engine.  Plain pointers and sizes only; every call returns a status
+ * code (TSU_OK == 0) and never exits the process.
+ *
+ * The reference (giuliagerometta/TSUNAMI_PACT) exposes this path as
+ *   - the command line `wfa_gpu mismatch gap_opening gap_extension
+ *     input_file wf_length check` (wfa_gpu.cu:43-188), and
+ *   - its kernel ABI `wfa_dispatcher(char* pattern_d, char* text_d,
+ *     short* score_d, ...)` over fixed-stride equal-length pairs
+ *     (wfa_gpu.cu:36-39, launched at wfa_gpu.cu:118-120),
+ * with the CPU check through WFA2-lib's `wavefront_align`
+ * (wfa_gpu.cu:154-166).  The entry points below replace those; each one
+ * names the reference interface it stands in for.
+ *
+ * Conventions: the pattern is the vertical sequence, the text the horizontal
+ * one (wfa_gpu.cu:164 passes pattern first).  Penalties: match 0, mismatch x,
+ * a gap of length L costs gap_opening + gap_extension * L.  Scores are the
+ * positive penalty sums (the reference prints -(cigar->score),
+ * wfa_gpu.cu:165).  CIGARs are WFA2-style operation sequences (M match,
+ * X mismatch, I insertion = text character, D deletion = pattern character)
+ * delivered run-length encoded, one uint32 per run: (length << 4) | code,
+ * code M=0, I=1, D=2, X=8.
+ */
+#ifndef TSUNAMI_B200_H
+#define TSUNAMI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define TSU_OK 0
+#define TSU_EINVAL 1    /* bad argument (penalties, lengths, null pointer)  */
+#define TSU_ENOMEM 2    /* device memory budget exceeded / allocation failed */
+#define TSU_EDEVICE 3   /* CUDA error (launch, copy, device lost)            */
+#define TSU_ETIMEOUT 4  /* a wait ran out of time                            */
+#define TSU_EOVERFLOW 5 /* caller's output buffer too small (see *_needed)   */
+#define TSU_EBUSY 6     /* serving queue full / admission refused            */
+#define TSU_ENOTFOUND 7 /* unknown request id                                */
+#define TSU_EINTERNAL 8 /* an internal consistency check failed              */
+#define TSU_EIO 9       /* file could not be opened / parsed                 */
+
+/* Per-pair status values written by the engine. */
+#define TSU_PAIR_OK 0
+#define TSU_PAIR_SCRATCH 1 /* wavefront scratch exhausted at this config     */
+#define TSU_PAIR_ARENA 2   /* CIGAR arena exhausted                          */
+#define TSU_PAIR_INTERNAL 3
+
+/* Flags for the align calls. */
+#define TSU_SCORE_ONLY 0x1u  /* skip the CIGAR (the reference kernel's work) */
+
+typedef struct tsu_ctx tsu_ctx;
+
+typedef struct {
+  int32_t mismatch;      /* > 0  (wfa_gpu.cu:59)  */
+  int32_t gap_opening;   /* >= 0 (wfa_gpu.cu:60)  */
+  int32_t gap_extension; /* > 0  (wfa_gpu.cu:61)  */
+} tsu_penalties;
+
+typedef struct {
+  int32_t device;        /* CUDA device ordinal                                */
+  int32_t reserved0;
+  size_t mem_budget;     /* bytes of device memory the context may hold;
+                            0 = 80% of the device's free memory at create    */
+  double max_error_hint; /* expected worst per-pair edit rate used to size
+                            wavefront scratch (0 = 0.20).  Pairs that exceed
+                            it are retried with larger scratch, never dropped */
+} tsu_config;
+
+/* Host-side batch: sequences are byte strings at pattern + pattern_off[i]
+ * (pattern_len[i] bytes) and text + text_off[i].  Any byte values are
+ * accepted; A/C/G/T-only pairs take the 2-bit packed path. */
+typedef struct {
+  int64_t num_pairs;
+  const char* pattern;
+  const int64_t* pattern_off;
+  const int32_t* pattern_len;
+  const char* text;
+  const int64_t* text_off;
+  const int32_t* text_len;
+} tsu_batch;
+
+/* Results.  score[num_pairs] is required.  For CIGARs, cigar_offset has
+ * num_pairs + 1 entries and pair i's runs are
+ * cigar[cigar_offset[i] .. cigar_offset[i+1]).  If cigar_capacity (in runs)
+ * is too small the call returns TSU_EOVERFLOW with scores filled and
+ * cigar_needed set. */
+typedef struct {
+  int32_t* score;
+  uint32_t* cigar;
+  int64_t cigar_capacity;
+  int64_t* cigar_offset;
+  int64_t cigar_needed; /* out */
+  int32_t* pair_status; /* optional [num_pairs], TSU_PAIR_* */
+} tsu_result;
+
+/* Timing of the last align call, measured with CUDA events on the context's
+ * stream (milliseconds). */
+typedef struct {
+  double h2d_ms, pack_ms, align_ms, compact_ms, d2h_ms, total_ms;
+  int64_t kernel_launches; /* kernels of this library launched by the call */
+  int64_t retried_pairs;   /* pairs re-run with larger scratch            */
+  int64_t h2d_bytes, d2h_bytes;
+  int64_t cells; /* wavefront (score, diagonal) cells computed, all passes */
+  int64_t steps; /* non-null score steps computed, all passes              */
+} tsu_timing;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the reference's per-run setup: cudaDeviceReset + 12 cudaMalloc
+ * (wfa_gpu.cu:96-108).  One context = one device, one stream, one memory
+ * budget.  A context is used by one host thread at a time. */
+int tsu_create(const tsu_penalties* pen, const tsu_config* cfg /* nullable */, tsu_ctx** out);
+int tsu_destroy(tsu_ctx* ctx);
+const char* tsu_status_str(int status);
+const char* tsu_last_error(const tsu_ctx* ctx);
+int tsu_get_timing(const tsu_ctx* ctx, tsu_timing* out);
+
+/* ---- batch alignment, host buffers -------------------------------------
+ * Replaces H2D + wfa_dispatcher launch + D2H of the reference
+ * (wfa_gpu.cu:110-128) for arbitrary-length pairs, plus the CIGARs the
+ * reference's WFA2-lib check computes (wfa_gpu.cu:164). */
+int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* batch, tsu_result* res, uint32_t flags);
+
+/* Fixed-stride, equal-length layout of the reference host buffers
+ * (wfa_gpu.cu:75-81): pair i is pattern + i*pattern_len and
+ * text + i*text_len.  Scores only (the reference kernel's output,
+ * short* score_d, wfa_gpu.cu:99,128 -- int32 here). */
+int tsu_align_fixed(tsu_ctx* ctx, const char* pattern, const char* text, int64_t num_couples,
+                    int32_t pattern_len, int32_t text_len, int32_t* score, uint32_t flags);
+
+/* ---- batch alignment, device-resident buffers ---------------------------
+ * Same as tsu_align_batch, but every pointer in batch and res is device
+ * memory (res->cigar_offset must hold num_pairs + 1 entries; pair_status is
+ * optional).  Work is queued on the context's stream and the call returns
+ * when it is complete.  This is the entry a caller with resident data (or
+ * the benchmark's kernel-time leg) uses; no host copies of sequence data. */
+int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* dev_batch, tsu_result* dev_res, uint32_t flags);
+
+/* ---- render ------------------------------------------------------------
+ * Expand run-length CIGAR runs into WFA2's one-char-per-operation string
+ * (cigar->operations), or into the compact text form ("12M1X3I...").
+ * Return the number of chars written (no terminator), or -1 if cap is too
+ * small. */
+int64_t tsu_cigar_to_ops(const uint32_t* runs, int64_t nruns, char* out, int64_t cap);
+int64_t tsu_cigar_to_string(const uint32_t* runs, int64_t nruns, char* out, int64_t cap);
+
+/* ---- input format (generate_dataset.cpp:39-41,68-69; read as in
+ * wfa_gpu.cu:71-81) --------------------------------------------------------
+ * sequences.txt: "N\nL\nerr\n" then N x (pattern line, text line).  Lines may
+ * have any length up to the header L... or longer: each line is read at its
+ * own length.  tsu_file_* hold the parsed batch in host memory. */
+typedef struct tsu_file tsu_file;
+int tsu_file_read(const char* path, tsu_file** out);
+int tsu_file_batch(const tsu_file* f, tsu_batch* out); /* views into f */
+int tsu_file_header(const tsu_file* f, int64_t* num, int32_t* seq_len, int32_t* error_rate);
+void tsu_file_free(tsu_file* f);
+
+/* Seeded synthetic pairs (replaces generate_dataset.cpp:11-75).  Pattern:
+ * i.i.d. uniform ACGT of length L; text: pattern with E = round(L*rate)
+ * edits, floor(E/3) insertions, floor(E/3) deletions and the rest
+ * substitutions at distinct uniform positions.  xoshiro256** seeded by
+ * splitmix64(seed ^ pair index): each pair is reproducible on its own.
+ * Writes into caller buffers: pattern/text bytes at pattern_off/text_off
+ * (the caller sizes them from len_fn below). */
+int tsu_gen_pair(uint64_t seed, int64_t pair_index, int32_t length, double error_rate, char* pattern_out,
+                 int32_t* pattern_len, char* text_out, int32_t* text_len);
+
+/* Many pairs at once on `threads` host threads (<= 0: all cores): pair i is
+ * tsu_gen_pair(seed, first + i, lengths[i], rates[i], ...).  The text of a
+ * pair has the pattern's length (equal insertion and deletion counts), so
+ * each output slot needs lengths[i] bytes. */
+int tsu_gen_batch(uint64_t seed, int64_t first, int64_t count, const int32_t* lengths, const double* rates,
+                  char* pattern, const int64_t* pattern_off, int32_t* pattern_len, char* text,
+                  const int64_t* text_off, int32_t* text_len, int threads);
+
+/* Write a batch in the sequences.txt format (generate_dataset.cpp:39-41,
+ * 68-69): header num / seq_len / error_rate, then pattern and text lines. */
+int tsu_file_write(const char* path, int64_t num, int32_t seq_len, int32_t error_rate, const tsu_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

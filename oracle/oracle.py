@@ -1,0 +1,150 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+as the checker and by ``bench.py``'s CPU-baseline / reference leg.  The
+product (``tsunami_pact_b200``) never imports this module.
+
+The oracle restates the gap-affine end-to-end WFA of the reference kernel
+(wfa_gpu.cu:191-722) and of the WFA2-lib call it checks against
+(wfa_gpu.cu:150-166); see ``wfa_oracle.h`` for the parity status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+class OraStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64),
+        ("cells", ctypes.c_int64),
+        ("ext_chars", ctypes.c_int64),
+        ("ext_calls", ctypes.c_int64),
+        ("final_score", ctypes.c_int64),
+    ]
+
+
+def build() -> str:
+    """Compile liboracle.so with the Makefile beside this file."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        c_char_p = ctypes.c_char_p
+        i32, i64 = ctypes.c_int32, ctypes.c_int64
+        P = ctypes.POINTER
+        L.ora_align.restype = ctypes.c_int
+        L.ora_align.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(OraStats)]
+        L.ora_gotoh_score.restype = ctypes.c_int
+        L.ora_gotoh_score.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int]
+        L.ora_cigar_cost.restype = i64
+        L.ora_cigar_cost.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, c_char_p, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.ora_align_batch.restype = ctypes.c_int
+        L.ora_align_batch.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, P(OraStats)]
+        L.ora_ops_to_rle.restype = ctypes.c_int
+        L.ora_ops_to_rle.argtypes = [c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        L.ora_max_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _b(s) -> bytes:
+    return s if isinstance(s, (bytes, bytearray)) else s.encode()
+
+
+def align(pattern, text, x=4, o=6, e=2, cigar=True) -> Tuple[int, Optional[str]]:
+    """Align one pair; returns (score, WFA2-style operation string or None)."""
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap) if cigar else None
+    n_ops = ctypes.c_int(0)
+    r = lib().ora_align(p, len(p), t, len(t), x, o, e, buf, cap, ctypes.byref(n_ops), None)
+    if r < 0:
+        raise RuntimeError(f"oracle error {r}")
+    return r, (buf.raw[: n_ops.value].decode() if cigar else None)
+
+
+def gotoh(pattern, text, x=4, o=6, e=2) -> int:
+    p, t = _b(pattern), _b(text)
+    return lib().ora_gotoh_score(p, len(p), t, len(t), x, o, e)
+
+
+def cigar_cost(ops: str, pattern, text, x=4, o=6, e=2) -> int:
+    p, t, c = _b(pattern), _b(text), _b(ops)
+    return lib().ora_cigar_cost(c, len(c), p, len(p), t, len(t), x, o, e)
+
+
+def ops_to_rle(ops: str) -> np.ndarray:
+    c = _b(ops)
+    out = np.zeros(max(1, len(c)), dtype=np.uint32)
+    n = lib().ora_ops_to_rle(c, len(c), out.ctypes.data, out.size)
+    return out[:n]
+
+
+def align_batch(patterns: Sequence, texts: Sequence, x=4, o=6, e=2, cigar=True, threads=0,
+                stats: bool = False):
+    """OpenMP batch alignment.  Returns (scores int32[N], list of op strings or None[, OraStats])."""
+    pats = [_b(p) for p in patterns]
+    txts = [_b(t) for t in texts]
+    n = len(pats)
+    plen = np.array([len(p) for p in pats], dtype=np.int32)
+    tlen = np.array([len(t) for t in txts], dtype=np.int32)
+    poff = np.zeros(n + 1, dtype=np.int64)
+    toff = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(plen, out=poff[1:])
+    np.cumsum(tlen, out=toff[1:])
+    pbuf = np.frombuffer(b"".join(pats) + b"\0", dtype=np.uint8)
+    tbuf = np.frombuffer(b"".join(txts) + b"\0", dtype=np.uint8)
+    return align_batch_arrays(pbuf, poff, plen, tbuf, toff, tlen, x, o, e, cigar, threads, stats)
+
+
+def align_batch_arrays(pbuf, poff, plen, tbuf, toff, tlen, x=4, o=6, e=2, cigar=True, threads=0,
+                       stats: bool = False):
+    n = len(plen)
+    scores = np.zeros(n, dtype=np.int32)
+    ops = ops_off = ops_len = None
+    if cigar:
+        caps = plen.astype(np.int64) + tlen.astype(np.int64) + 1
+        ops_off = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(caps, out=ops_off[1:])
+        ops = np.zeros(int(ops_off[-1]) + 1, dtype=np.uint8)
+        ops_len = np.zeros(n, dtype=np.int32)
+    st = OraStats()
+    r = lib().ora_align_batch(
+        n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+        tlen.ctypes.data, x, o, e, scores.ctypes.data,
+        ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
+        ops_len.ctypes.data if cigar else None, threads, ctypes.byref(st))
+    if r < 0:
+        raise RuntimeError(f"oracle batch error {r}")
+    cig: Optional[List[str]] = None
+    if cigar:
+        raw = ops.tobytes()
+        cig = [raw[ops_off[i]: ops_off[i] + ops_len[i]].decode() for i in range(n)]
+    if stats:
+        return scores, cig, st
+    return scores, cig
+
+
+def max_threads() -> int:
+    return lib().ora_max_threads()

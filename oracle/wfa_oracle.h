@@ -1,0 +1,100 @@
+/*
+ * wfa_oracle.h -- CPU oracle for gap-affine end-to-end WaveFront Alignment.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the tsunami_pact_b200
+ * library, its CLI, its Python binding) links, loads or calls this code.  It
+ * is used by tests/ as the parity checker, by __graft_entry__.smoke() as the
+ * checker, and by bench.py's cpu_baseline / --impl reference leg as the
+ * stand-in for the reference's CPU path (WFA2-lib, whose source is absent:
+ * the reference's WFA2-lib/ submodule directory is empty, .gitmodules:1-3).
+ *
+ * What it restates:
+ *   - the score semantics of the reference kernel wfa_dispatcher
+ *     (wfa_gpu.cu:191-722): offsets are text positions h on diagonal
+ *     k = h - v, the I/D/M recurrences of wfa_gpu.cu:616-626, the
+ *     out-of-bounds nullification of wfa_gpu.cu:628-629, the end test of
+ *     wfa_gpu.cu:289-300 and the end trimming of wfa_gpu.cu:636-719 --
+ *     computed with int32 offsets and without the reference's indexing
+ *     defects;
+ *   - the published WFA2-lib gap-affine algorithm that the reference calls
+ *     for its check (wfa_gpu.cu:150-166, default attributes: end-to-end,
+ *     exact, high-memory, full CIGAR): wavefront limits from the sources'
+ *     envelopes, nullification of only the M component, trimming of the ends
+ *     of M, I and D, and the wavefront backtrace that resolves ties by the
+ *     piggyback order whose numeric codes the reference copies in
+ *     common.h:67-77 (bt_M=9 > D_ext=6 > D_open=5 > I_ext=2 > I_open=1).
+ *
+ * Parity status: scores are pinned by an independent O(mn) Gotoh DP in this
+ * same file (ora_gotoh_score) -- the optimal end-to-end gap-affine score is
+ * unique.  CIGAR byte-identity with WFA2-lib is UNPINNED: WFA2-lib's source
+ * and tests are not available, so the tie-breaking restated here follows the
+ * published algorithm and the reference's bt_type_t codes only.
+ */
+#ifndef TSU_WFA_ORACLE_H
+#define TSU_WFA_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int64_t steps;        /* non-null score steps computed                    */
+  int64_t cells;        /* sum over steps of (hi - lo + 1), compute range    */
+  int64_t ext_chars;    /* characters matched by the extend step            */
+  int64_t ext_calls;    /* extend calls on non-null M offsets               */
+  int64_t final_score;  /* score of the last aligned pair                   */
+} ora_stats_t;
+
+/* Error codes (negative returns). */
+#define ORA_EINVAL  (-1)
+#define ORA_ENOMEM  (-2)
+#define ORA_ECIGCAP (-3)  /* ops buffer too small */
+
+/* Align one pair end-to-end.  Returns the score (>= 0) or a negative error.
+ * When ops != NULL the WFA2-style operation string ('M','X','I','D', one char
+ * per operation, pattern = vertical, text = horizontal) is written to ops
+ * (no terminator) and its length to *ops_len.  ops_cap >= m + n suffices. */
+int ora_align(const char* pattern, int m, const char* text, int n,
+              int x, int o, int e,
+              char* ops, int ops_cap, int* ops_len, ora_stats_t* st);
+
+/* Independent Gotoh DP (O(n) memory, O(mn) time).  Returns the score. */
+int ora_gotoh_score(const char* pattern, int m, const char* text, int n,
+                    int x, int o, int e);
+
+/* Cost of an operation string, or -1 if it does not transform pattern into
+ * text (length mismatch or an 'M' on unequal characters / 'X' on equal). */
+int64_t ora_cigar_cost(const char* ops, int len,
+                       const char* pattern, int m, const char* text, int n,
+                       int x, int o, int e);
+
+/* Batch over concatenated sequences, OpenMP over pairs with nthreads threads
+ * (<= 0: all available).  ops may be NULL (scores only); otherwise pair i's
+ * operations go to ops + ops_off[i] (capacity ops_off[i+1] - ops_off[i])
+ * and their count to ops_len[i].  Returns 0 or a negative error (first
+ * failing pair's error). */
+int ora_align_batch(int npairs,
+                    const char* pat, const int64_t* poff, const int32_t* plen,
+                    const char* txt, const int64_t* toff, const int32_t* tlen,
+                    int x, int o, int e,
+                    int32_t* scores, char* ops, const int64_t* ops_off,
+                    int32_t* ops_len, int nthreads, ora_stats_t* st);
+
+/* Run-length form of an operation string, BAM-style: (len << 4) | code with
+ * M=0, I=1, D=2, X=8.  Returns the number of runs written, or -1 when cap is
+ * too small. */
+int ora_ops_to_rle(const char* ops, int len, uint32_t* runs, int cap);
+
+int ora_max_threads(void);
+
+/* CPU-check plugin for the wfa_gpu command line (TSU_CHECK_LIB). */
+int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                           const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,
+                           int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

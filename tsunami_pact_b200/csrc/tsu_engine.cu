@@ -1,0 +1,725 @@
+// tsu_engine.cu -- host runtime of the B200 gap-affine WFA engine and the
+// C ABI declared in include/tsunami_b200.h.
+//
+// Replaces the reference host driver's device part (wfa_gpu.cu:83-135):
+// instead of 12 cudaMalloc per run, a fixed 32-thread block per pair and
+// `wf_length`-sized int16 wavefront slots, a context owns a grow-only device
+// workspace inside a memory budget and each call runs
+//   H2D -> word-count scan -> pack -> align pass(es) -> CIGAR compaction -> D2H
+// on one stream.  Pairs whose wavefronts outgrow the scratch of a pass are
+// re-run in a further pass with larger, global-memory scratch; nothing is
+// dropped and nothing runs on the CPU.
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tsunami_b200.h"
+#include "tsu_kernels.cuh"
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Pass {
+  int smem_ring = 1;
+  int ring_w = 0;
+  int64_t warps = 0;
+  int blocks = 0;
+  int wpb = 4;  // warps per block
+  int64_t hist_cap = 0;
+  int table_cap = 0;
+  size_t smem_bytes = 0;
+};
+
+}  // namespace
+
+struct tsu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  tsu_penalties pen{};
+  int x = 0, go = 0, ge = 0, g = 1, rm = 0, re = 0;
+  size_t budget = 0;
+  double err_hint = 0.2;
+  int sms = 0;
+  int smem_optin = 0;
+  std::string err;
+  tsu_timing timing{};
+  // workspace buffers (grow-only)
+  DevBuf b_pat, b_txt, b_poff, b_toff, b_plen, b_tlen;   // H2D staging of inputs
+  DevBuf b_words_cnt, b_woff, b_words, b_nonacgt;         // packing
+  DevBuf b_score, b_status, b_cpos, b_clen, b_clen64, b_coff, b_out;  // outputs
+  DevBuf b_order, b_retry, b_counters;                    // queue, retry list, counters
+  DevBuf b_ring, b_hist, b_table, b_arena, b_scan_tmp;    // scratch
+  size_t held() const {
+    const DevBuf* all[] = {&b_pat, &b_txt, &b_poff, &b_toff, &b_plen, &b_tlen, &b_words_cnt, &b_woff,
+                           &b_words, &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,
+                           &b_out, &b_order, &b_retry, &b_counters, &b_ring, &b_hist, &b_table, &b_arena,
+                           &b_scan_tmp};
+    size_t s = 0;
+    for (auto* b : all) s += b->cap;
+    return s;
+  }
+};
+
+namespace {
+
+int set_err(tsu_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                                     \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return set_err(ctx, TSU_EDEVICE, "%s at %s:%d: %s", #call, __FILE__, __LINE__, cudaGetErrorString(e_)); \
+  } while (0)
+
+int gcd(int a, int b) {
+  while (b) {
+    int t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Grow a buffer to at least `bytes` within the context budget.
+int grow(tsu_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return TSU_OK;
+  size_t nb = std::max(bytes, b.cap + b.cap / 2);
+  nb = (nb + 255) & ~(size_t)255;
+  if (ctx->held() - b.cap + nb > ctx->budget) {
+    nb = bytes;
+    if (ctx->held() - b.cap + nb > ctx->budget)
+      return set_err(ctx, TSU_ENOMEM, "device budget %zu B exceeded (need %zu more)", ctx->budget, bytes);
+  }
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  cudaError_t e = cudaMalloc(&b.p, nb);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, TSU_ENOMEM, "cudaMalloc(%zu) failed: %s", nb, cudaGetErrorString(e));
+  }
+  b.cap = nb;
+  return TSU_OK;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+template <class T>
+T* P(DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Reduced-unit score expected at the error hint for a pair of length L.
+int64_t hint_score(const tsu_ctx* ctx, int64_t L, double hint) {
+  const double per_edit = std::max(ctx->x, ctx->go);
+  return (int64_t)(hint * (double)L * per_edit) + 16;
+}
+
+struct BatchInfo {
+  int64_t n = 0;
+  int32_t max_m = 0, max_n = 0;
+  int64_t total_words = 0;
+};
+
+// Configure a pass.  first: shared-memory ring sized for occupancy;
+// otherwise global-memory ring wide enough for any pair of the batch.
+int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, double hint, bool want_cigar,
+              size_t reserve_bytes, Pass* out) {
+  Pass p;
+  const int ns = tsu::ring_slots(ctx->rm, ctx->re);
+  const int wpb = 4;
+  const int64_t maxlen = std::max(bi.max_m, bi.max_n);
+  int64_t s_hint = hint_score(ctx, maxlen, hint);
+  const int64_t full_w = (int64_t)bi.max_m + bi.max_n + 3;
+  int64_t width_hint = std::min<int64_t>(full_w, 2 * s_hint / ctx->ge + 3);
+  if (first) {
+    // Ring width: enough for ~12 warps per SM, capped by the widest possible
+    // wavefront of this batch.
+    int w = (int)std::min<int64_t>(full_w, 384);
+    w = (w + 31) & ~31;
+    p.smem_ring = 1;
+    p.ring_w = std::max(w, 32);
+  } else {
+    p.smem_ring = 0;
+    p.ring_w = (int)full_w;
+  }
+  p.smem_bytes = (size_t)wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, p.smem_ring) * 4;
+  if (p.smem_bytes > (size_t)ctx->smem_optin) {
+    p.smem_ring = 0;
+    p.ring_w = (int)full_w;
+    p.smem_bytes = (size_t)wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, 0) * 4;
+  }
+  int occ = 0;
+  cudaError_t e;
+  if (want_cigar) {
+    cudaFuncSetAttribute(tsu::align_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tsu::align_kernel<true>, wpb * 32, p.smem_bytes);
+  } else {
+    cudaFuncSetAttribute(tsu::align_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tsu::align_kernel<false>, wpb * 32, p.smem_bytes);
+  }
+  if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
+  int64_t warps = (int64_t)ctx->sms * occ * wpb;
+  // scratch per warp
+  // Backtrace words up to score s: sum_j (2j/ge + 1) ~= s^2/ge + 2s.
+  const int64_t table_cap = want_cigar ? std::min<int64_t>(s_hint + 1, INT32_MAX / 2) : 0;
+  int64_t hist_cap = 0;
+  if (want_cigar) {
+    const int64_t sq = s_hint * s_hint / ctx->ge + 2 * s_hint + 64;
+    hist_cap = std::min<int64_t>(std::min<int64_t>(sq, (s_hint + 1) * width_hint), INT32_MAX - 64);
+  }
+  const int64_t ring_ints = p.smem_ring ? 0 : (int64_t)ns * p.ring_w;
+  // scratch buffers are regrown for this pass: their current size is free
+  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
+  const size_t avail = ctx->budget > fixed + reserve_bytes ? ctx->budget - fixed - reserve_bytes : 0;
+  auto per_warp = [&](int64_t hc) { return (size_t)(ring_ints * 4 + hc * 4 + table_cap * 8 + 64); };
+  // fewer warps when the pass has fewer pairs or the budget is tight
+  warps = std::min<int64_t>(warps, std::max<int64_t>(n_pairs, 1));
+  if ((size_t)warps * per_warp(hist_cap) > avail) {
+    int64_t w2 = (int64_t)(avail / per_warp(hist_cap));
+    if (w2 < 1) return set_err(ctx, TSU_ENOMEM, "scratch for one pair (%zu B) exceeds the budget", per_warp(hist_cap));
+    warps = w2;
+  }
+  if (warps >= wpb) {
+    warps = warps / wpb * wpb;
+    p.wpb = wpb;
+  } else {
+    p.wpb = (int)warps;  // a single block of fewer warps
+  }
+  p.warps = warps;
+  p.blocks = (int)(warps / p.wpb);
+  p.smem_bytes = (size_t)p.wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, p.smem_ring) * 4;
+  p.hist_cap = hist_cap;
+  p.table_cap = (int)table_cap;
+  *out = p;
+  return TSU_OK;
+}
+
+// Core: inputs resident on the device (sv).  Writes score/status (device)
+// and, for CIGARs, compacts runs into out_runs with offsets out_off
+// (device, n+1 entries).  *runs_needed receives the total.
+// When d_out_runs is null the runs go to the context's own b_out buffer
+// (grown to fit) and *out_used receives its address.
+int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d_score, int32_t* d_status,
+               uint32_t* d_out_runs, int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, BatchInfo bi,
+               uint32_t** out_used = nullptr) {
+  const int64_t n = sv.n;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if (n == 0) {
+    if (runs_needed) *runs_needed = 0;
+    if (want_cigar && d_out_off) CU(cudaMemsetAsync(d_out_off, 0, sizeof(int64_t), st));
+    return TSU_OK;
+  }
+  // ---- word counts + scan -> packed offsets
+  if ((rc = grow(ctx, ctx->b_words_cnt, sizeof(int64_t) * 2 * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_woff, sizeof(int64_t) * 2 * n))) return rc;
+  tsu::word_count_kernel<<<std::min<int64_t>((2 * n + 255) / 256, 4096), 256, 0, st>>>(n, sv.pat_len, sv.txt_len,
+                                                                                        P<int64_t>(ctx->b_words_cnt));
+  ctx->timing.kernel_launches++;
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff), (int)(2 * n), st);
+  if ((rc = grow(ctx, ctx->b_scan_tmp, tmp_bytes))) return rc;
+  CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tmp_bytes, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff),
+                                   (int)(2 * n), st));
+  ctx->timing.kernel_launches++;
+  if ((rc = grow(ctx, ctx->b_words, sizeof(uint64_t) * (size_t)bi.total_words))) return rc;
+  if ((rc = grow(ctx, ctx->b_nonacgt, (size_t)(2 * n)))) return rc;
+  tsu::PackView pk{P<uint64_t>(ctx->b_words), P<int64_t>(ctx->b_woff), P<uint8_t>(ctx->b_nonacgt)};
+  CU(cudaEventRecord(ctx->ev[2], st));
+  {
+    const int64_t blocks = std::min<int64_t>((2 * n + 7) / 8, (int64_t)ctx->sms * 16);
+    tsu::pack_kernel<<<(int)blocks, 256, 0, st>>>(sv, pk);
+    ctx->timing.kernel_launches++;
+  }
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(ctx->ev[3], st));
+
+  // ---- outputs/queues
+  if ((rc = grow(ctx, ctx->b_cpos, sizeof(int64_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_clen, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_retry, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_order, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
+  const int min_pen = std::min(ctx->x, ctx->go);
+  int64_t arena_cap = 0;
+  if (want_cigar) {
+    const int64_t maxlen = std::max(bi.max_m, bi.max_n);
+    const int64_t per_pair = 2 * hint_score(ctx, maxlen, ctx->err_hint) / min_pen + 1;
+    arena_cap = std::max<int64_t>(n * std::min<int64_t>(per_pair, (int64_t)bi.max_m + bi.max_n + 1), 1024);
+    size_t room = ctx->budget > ctx->held() ? ctx->budget - ctx->held() : 0;
+    arena_cap = std::min<int64_t>(arena_cap, (int64_t)(room / 8));  // leave half for scratch
+    if ((rc = grow(ctx, ctx->b_arena, sizeof(uint32_t) * (size_t)std::max<int64_t>(arena_cap, 1024)))) return rc;
+    arena_cap = (int64_t)(ctx->b_arena.cap / sizeof(uint32_t));
+  }
+  unsigned int* d_queue = P<unsigned int>(ctx->b_counters);
+  unsigned int* d_retry_cnt = d_queue + 1;
+  unsigned long long* d_cursor = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 16);
+  CU(cudaMemsetAsync(ctx->b_counters.p, 0, 64, st));
+
+  // ---- passes
+  double hint = ctx->err_hint;
+  bool first = true;
+  int64_t n_order = n;
+  const int32_t* order = nullptr;
+  int passes = 0;
+  CU(cudaEventRecord(ctx->ev[4], st));
+  for (;;) {
+    Pass ps;
+    if ((rc = plan_pass(ctx, bi, n_order, first, hint, want_cigar, 0, &ps))) return rc;
+    if (!ps.smem_ring) {
+      if ((rc = grow(ctx, ctx->b_ring, sizeof(int32_t) * (size_t)ps.warps * tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w)))
+        return rc;
+    }
+    if (want_cigar) {
+      if ((rc = grow(ctx, ctx->b_hist, sizeof(uint32_t) * (size_t)ps.warps * ps.hist_cap))) return rc;
+      if ((rc = grow(ctx, ctx->b_table, sizeof(int2) * (size_t)ps.warps * ps.table_cap))) return rc;
+    }
+    tsu::AlignArgs a{};
+    a.seq = sv;
+    a.pk = pk;
+    a.order = order;
+    a.n_order = n_order;
+    a.x = ctx->x;
+    a.go = ctx->go;
+    a.ge = ctx->ge;
+    a.g = ctx->g;
+    a.rm = ctx->rm;
+    a.re = ctx->re;
+    a.ring_w = ps.ring_w;
+    a.smem_ring = ps.smem_ring;
+    a.ring_global = ps.smem_ring ? nullptr : P<int32_t>(ctx->b_ring);
+    a.ring_stride = (int64_t)tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w;
+    a.hist = want_cigar ? P<uint32_t>(ctx->b_hist) : nullptr;
+    a.hist_cap = ps.hist_cap;
+    a.table = want_cigar ? P<int2>(ctx->b_table) : nullptr;
+    a.table_cap = ps.table_cap;
+    a.want_cigar = want_cigar;
+    a.score = d_score;
+    a.status = d_status;
+    a.arena = want_cigar ? P<uint32_t>(ctx->b_arena) : nullptr;
+    a.arena_cursor = d_cursor;
+    a.arena_cap = arena_cap;
+    a.cig_pos = P<int64_t>(ctx->b_cpos);
+    a.cig_len = P<int32_t>(ctx->b_clen);
+    a.queue = d_queue;
+    a.retry = P<int32_t>(ctx->b_retry);
+    a.retry_count = d_retry_cnt;
+    a.work = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 24);
+    if (want_cigar)
+      tsu::align_kernel<true><<<ps.blocks, 32 * ps.wpb, ps.smem_bytes, st>>>(a);
+    else
+      tsu::align_kernel<false><<<ps.blocks, 32 * ps.wpb, ps.smem_bytes, st>>>(a);
+    ctx->timing.kernel_launches++;
+    CU(cudaGetLastError());
+    ++passes;
+    unsigned int nretry = 0;
+    CU(cudaMemcpyAsync(&nretry, d_retry_cnt, sizeof nretry, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (nretry == 0) break;
+    ctx->timing.retried_pairs += nretry;
+    if (passes > 12) return set_err(ctx, TSU_ENOMEM, "pairs still exceed scratch after %d passes", passes);
+    // the retry list becomes the next pass's order; arena overflow grows it
+    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry,
+                       cudaMemcpyDeviceToDevice, st));
+    order = P<int32_t>(ctx->b_order);
+    n_order = nretry;
+    if (!first) hint *= 2.0;
+    first = false;
+    if (want_cigar) {
+      unsigned long long used = 0;
+      CU(cudaMemcpyAsync(&used, d_cursor, sizeof used, cudaMemcpyDeviceToHost, st));
+      CU(cudaStreamSynchronize(st));
+      const int64_t maxlen = std::max(bi.max_m, bi.max_n);
+      const int64_t need = (int64_t)used + (int64_t)nretry * (2 * hint_score(ctx, maxlen, hint) / min_pen + 1);
+      if (need > arena_cap) {
+        // keep the runs written so far: grow by copy
+        DevBuf nb;
+        size_t bytes = sizeof(uint32_t) * (size_t)need;
+        if (ctx->held() + bytes > ctx->budget) return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
+        CU(cudaMalloc(&nb.p, bytes));
+        nb.cap = bytes;
+        const int64_t keep = std::min<int64_t>((int64_t)used, arena_cap);
+        CU(cudaMemcpyAsync(nb.p, ctx->b_arena.p, sizeof(uint32_t) * (size_t)keep, cudaMemcpyDeviceToDevice, st));
+        CU(cudaStreamSynchronize(st));
+        release(ctx->b_arena);
+        ctx->b_arena = nb;
+        arena_cap = need;
+      }
+    }
+    CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
+  }
+  CU(cudaEventRecord(ctx->ev[5], st));
+  {
+    unsigned long long work[2] = {0, 0};
+    CU(cudaMemcpyAsync(work, P<char>(ctx->b_counters) + 24, sizeof work, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    ctx->timing.cells = (int64_t)work[0];
+    ctx->timing.steps = (int64_t)work[1];
+  }
+
+  // ---- CIGAR compaction
+  if (want_cigar) {
+    if ((rc = grow(ctx, ctx->b_clen64, sizeof(int64_t) * (n + 1)))) return rc;
+    tsu::cig_len64_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+        n, P<int32_t>(ctx->b_clen), d_status, P<int64_t>(ctx->b_clen64));
+    CU(cudaMemsetAsync(P<int64_t>(ctx->b_clen64) + n, 0, sizeof(int64_t), st));
+    ctx->timing.kernel_launches++;
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, P<int64_t>(ctx->b_clen64), d_out_off, (int)(n + 1), st);
+    if ((rc = grow(ctx, ctx->b_scan_tmp, tb))) return rc;
+    CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tb, P<int64_t>(ctx->b_clen64), d_out_off, (int)(n + 1), st));
+    ctx->timing.kernel_launches++;
+    int64_t total = 0;
+    CU(cudaMemcpyAsync(&total, d_out_off + n, sizeof total, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (runs_needed) *runs_needed = total;
+    if (!d_out_runs) {
+      if ((rc = grow(ctx, ctx->b_out, sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)))) return rc;
+      d_out_runs = P<uint32_t>(ctx->b_out);
+      out_cap = total;
+      if (out_used) *out_used = d_out_runs;
+    }
+    if (total > out_cap) return TSU_EOVERFLOW;
+    const int64_t blocks = std::min<int64_t>((n + 7) / 8, (int64_t)ctx->sms * 16);
+    tsu::compact_kernel<<<(int)blocks, 256, 0, st>>>(n, P<uint32_t>(ctx->b_arena), P<int64_t>(ctx->b_cpos),
+                                                    P<int32_t>(ctx->b_clen), d_out_off, d_out_runs);
+    ctx->timing.kernel_launches++;
+    CU(cudaGetLastError());
+  }
+  CU(cudaEventRecord(ctx->ev[6], st));
+  return TSU_OK;
+}
+
+int check_batch_host(tsu_ctx* ctx, const tsu_batch* b, BatchInfo* bi, int64_t* pat_bytes, int64_t* txt_bytes) {
+  if (!b || b->num_pairs < 0) return set_err(ctx, TSU_EINVAL, "null batch or negative num_pairs");
+  if (b->num_pairs > INT32_MAX) return set_err(ctx, TSU_EINVAL, "num_pairs > INT32_MAX");
+  if (b->num_pairs && (!b->pattern || !b->pattern_off || !b->pattern_len || !b->text || !b->text_off || !b->text_len))
+    return set_err(ctx, TSU_EINVAL, "null sequence pointer");
+  int64_t pe = 0, te = 0, words = 0;
+  int32_t mm = 0, mn = 0;
+  for (int64_t i = 0; i < b->num_pairs; ++i) {
+    const int32_t m = b->pattern_len[i], n = b->text_len[i];
+    if (m < 0 || n < 0 || m > (1 << 26) || n > (1 << 26) || b->pattern_off[i] < 0 || b->text_off[i] < 0)
+      return set_err(ctx, TSU_EINVAL, "pair %lld: bad length/offset", (long long)i);
+    pe = std::max(pe, b->pattern_off[i] + m);
+    te = std::max(te, b->text_off[i] + n);
+    mm = std::max(mm, m);
+    mn = std::max(mn, n);
+    words += (m + 31) / 32 + 1 + (n + 31) / 32 + 1;
+  }
+  bi->n = b->num_pairs;
+  bi->max_m = mm;
+  bi->max_n = mn;
+  bi->total_words = words;
+  *pat_bytes = pe;
+  *txt_bytes = te;
+  return TSU_OK;
+}
+
+// Per-pair statuses -> call status.
+int collect_status(tsu_ctx* ctx, const int32_t* hs, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (hs[i] != tsu::kPairOk)
+      return set_err(ctx, hs[i] == tsu::kPairInternal ? TSU_EINTERNAL : TSU_ENOMEM, "pair %lld status %d",
+                     (long long)i, hs[i]);
+  return TSU_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* tsu_status_str(int s) {
+  switch (s) {
+    case TSU_OK: return "ok";
+    case TSU_EINVAL: return "invalid argument";
+    case TSU_ENOMEM: return "device memory budget exceeded";
+    case TSU_EDEVICE: return "CUDA device error";
+    case TSU_ETIMEOUT: return "timed out";
+    case TSU_EOVERFLOW: return "output buffer too small";
+    case TSU_EBUSY: return "busy / admission refused";
+    case TSU_ENOTFOUND: return "not found";
+    case TSU_EINTERNAL: return "internal error";
+    case TSU_EIO: return "i/o error";
+    default: return "unknown status";
+  }
+}
+
+const char* tsu_last_error(const tsu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
+  tsu_ctx* ctx = nullptr;
+  if (!pen || !out) return TSU_EINVAL;
+  *out = nullptr;
+  if (pen->mismatch <= 0 || pen->gap_opening < 0 || pen->gap_extension <= 0 || pen->mismatch > 1 << 20 ||
+      pen->gap_opening > 1 << 20 || pen->gap_extension > 1 << 20)
+    return TSU_EINVAL;
+  ctx = new tsu_ctx();
+  ctx->pen = *pen;
+  ctx->g = gcd(gcd(pen->mismatch, pen->gap_opening), pen->gap_extension);
+  ctx->x = pen->mismatch / ctx->g;
+  ctx->go = (pen->gap_opening + pen->gap_extension) / ctx->g;
+  ctx->ge = pen->gap_extension / ctx->g;
+  ctx->rm = std::max(ctx->x, ctx->go) + 1;
+  ctx->re = ctx->ge + 1;
+  if (tsu::ring_slots(ctx->rm, ctx->re) > 4096) {
+    delete ctx;
+    return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
+  }
+  ctx->device = cfg ? cfg->device : 0;
+  ctx->err_hint = (cfg && cfg->max_error_hint > 0) ? cfg->max_error_hint : 0.2;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  ctx->sms = prop.multiProcessorCount;
+  ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  ctx->budget = (cfg && cfg->mem_budget) ? cfg->mem_budget : (size_t)(0.8 * (double)fr);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  *out = ctx;
+  return TSU_OK;
+}
+
+int tsu_destroy(tsu_ctx* ctx) {
+  if (!ctx) return TSU_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  DevBuf* all[] = {&ctx->b_pat, &ctx->b_txt, &ctx->b_poff, &ctx->b_toff, &ctx->b_plen, &ctx->b_tlen,
+                   &ctx->b_words_cnt, &ctx->b_woff, &ctx->b_words, &ctx->b_nonacgt, &ctx->b_score,
+                   &ctx->b_status, &ctx->b_cpos, &ctx->b_clen, &ctx->b_clen64, &ctx->b_coff, &ctx->b_out,
+                   &ctx->b_order, &ctx->b_retry, &ctx->b_counters, &ctx->b_ring, &ctx->b_hist, &ctx->b_table,
+                   &ctx->b_arena, &ctx->b_scan_tmp};
+  for (auto* b : all) release(*b);
+  for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TSU_OK;
+}
+
+int tsu_get_timing(const tsu_ctx* ctx, tsu_timing* out) {
+  if (!ctx || !out) return TSU_EINVAL;
+  *out = ctx->timing;
+  return TSU_OK;
+}
+
+int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t flags) {
+  if (!ctx || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null result") : TSU_EINVAL;
+  const bool want_cigar = !(flags & TSU_SCORE_ONLY);
+  if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
+  BatchInfo bi;
+  int64_t pb = 0, tb = 0;
+  int rc = check_batch_host(ctx, b, &bi, &pb, &tb);
+  if (rc) return rc;
+  CU(cudaSetDevice(ctx->device));
+  ctx->timing = tsu_timing{};
+  const int64_t n = bi.n;
+  cudaStream_t st = ctx->stream;
+  if ((rc = grow(ctx, ctx->b_pat, (size_t)pb))) return rc;
+  if ((rc = grow(ctx, ctx->b_txt, (size_t)tb))) return rc;
+  if ((rc = grow(ctx, ctx->b_poff, sizeof(int64_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_toff, sizeof(int64_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_plen, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_tlen, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_score, sizeof(int32_t) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_status, sizeof(int32_t) * n))) return rc;
+  if (want_cigar && (rc = grow(ctx, ctx->b_coff, sizeof(int64_t) * (n + 1)))) return rc;
+  CU(cudaEventRecord(ctx->ev[0], st));
+  if (n) {
+    if (pb) CU(cudaMemcpyAsync(ctx->b_pat.p, b->pattern, (size_t)pb, cudaMemcpyHostToDevice, st));
+    if (tb) CU(cudaMemcpyAsync(ctx->b_txt.p, b->text, (size_t)tb, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->b_poff.p, b->pattern_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->b_toff.p, b->text_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->b_plen.p, b->pattern_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->b_tlen.p, b->text_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  }
+  ctx->timing.h2d_bytes = pb + tb + n * 24;
+  CU(cudaEventRecord(ctx->ev[1], st));
+  tsu::SeqView sv{n, P<uint8_t>(ctx->b_pat), P<int64_t>(ctx->b_poff), P<int32_t>(ctx->b_plen),
+                  P<uint8_t>(ctx->b_txt), P<int64_t>(ctx->b_toff), P<int32_t>(ctx->b_tlen)};
+  int64_t needed = 0;
+  uint32_t* d_runs = nullptr;  // compacted runs in the context's b_out
+  rc = run_device(ctx, sv, want_cigar, P<int32_t>(ctx->b_score), P<int32_t>(ctx->b_status), nullptr, 0,
+                  want_cigar ? P<int64_t>(ctx->b_coff) : nullptr, &needed, bi, &d_runs);
+  if (rc) return rc;
+  CU(cudaEventRecord(ctx->ev[7], st));
+  CU(cudaMemcpyAsync(res->score, ctx->b_score.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+  std::vector<int32_t> hs((size_t)n);
+  CU(cudaMemcpyAsync(hs.data(), ctx->b_status.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+  int64_t d2h = n * 8;
+  if (want_cigar) {
+    res->cigar_needed = needed;
+    CU(cudaMemcpyAsync(res->cigar_offset, ctx->b_coff.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    d2h += (n + 1) * 8;
+    if (needed <= res->cigar_capacity && res->cigar) {
+      if (needed) CU(cudaMemcpyAsync(res->cigar, d_runs, sizeof(uint32_t) * needed, cudaMemcpyDeviceToHost, st));
+      d2h += needed * 4;
+    }
+  }
+  CU(cudaStreamSynchronize(st));
+  ctx->timing.d2h_bytes = d2h;
+  // timings
+  ctx->timing.h2d_ms = ev_ms(ctx->ev[0], ctx->ev[1]);
+  ctx->timing.pack_ms = n ? ev_ms(ctx->ev[2], ctx->ev[3]) : 0;
+  ctx->timing.align_ms = n ? ev_ms(ctx->ev[4], ctx->ev[5]) : 0;
+  ctx->timing.compact_ms = (n && want_cigar) ? ev_ms(ctx->ev[5], ctx->ev[6]) : 0;
+  {
+    cudaEvent_t e_end;
+    cudaEventCreate(&e_end);
+    cudaEventRecord(e_end, st);
+    cudaEventSynchronize(e_end);
+    ctx->timing.d2h_ms = ev_ms(ctx->ev[7], e_end);
+    ctx->timing.total_ms = ev_ms(ctx->ev[0], e_end);
+    cudaEventDestroy(e_end);
+  }
+  if (res->pair_status) memcpy(res->pair_status, hs.data(), sizeof(int32_t) * n);
+  if ((rc = collect_status(ctx, hs.data(), n))) return rc;
+  if (want_cigar && (needed > res->cigar_capacity || !res->cigar)) return TSU_EOVERFLOW;
+  return TSU_OK;
+}
+
+int tsu_align_fixed(tsu_ctx* ctx, const char* pattern, const char* text, int64_t num, int32_t plen, int32_t tlen,
+                    int32_t* score, uint32_t flags) {
+  if (!ctx) return TSU_EINVAL;
+  if (num < 0 || plen < 0 || tlen < 0 || (num && (!pattern || !text || !score)))
+    return set_err(ctx, TSU_EINVAL, "bad fixed-stride arguments");
+  std::vector<int64_t> po((size_t)num), to((size_t)num);
+  std::vector<int32_t> pl((size_t)num, plen), tl((size_t)num, tlen);
+  for (int64_t i = 0; i < num; ++i) {
+    po[(size_t)i] = i * (int64_t)plen;
+    to[(size_t)i] = i * (int64_t)tlen;
+  }
+  tsu_batch b{num, pattern, po.data(), pl.data(), text, to.data(), tl.data()};
+  tsu_result r{};
+  r.score = score;
+  return tsu_align_batch(ctx, &b, &r, flags | TSU_SCORE_ONLY);
+}
+
+int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t flags) {
+  if (!ctx || !b || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null argument") : TSU_EINVAL;
+  const bool want_cigar = !(flags & TSU_SCORE_ONLY);
+  if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
+  CU(cudaSetDevice(ctx->device));
+  ctx->timing = tsu_timing{};
+  const int64_t n = b->num_pairs;
+  if (n < 0 || n > INT32_MAX) return set_err(ctx, TSU_EINVAL, "bad num_pairs");
+  cudaStream_t st = ctx->stream;
+  // batch info: lengths are on the device; bring them over once.
+  BatchInfo bi;
+  bi.n = n;
+  {
+    std::vector<int32_t> pl((size_t)n), tl((size_t)n);
+    if (n) {
+      CU(cudaMemcpyAsync(pl.data(), b->pattern_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+      CU(cudaMemcpyAsync(tl.data(), b->text_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+      CU(cudaStreamSynchronize(st));
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      if (pl[(size_t)i] < 0 || tl[(size_t)i] < 0 || pl[(size_t)i] > (1 << 26) || tl[(size_t)i] > (1 << 26))
+        return set_err(ctx, TSU_EINVAL, "pair %lld: bad length", (long long)i);
+      bi.max_m = std::max(bi.max_m, pl[(size_t)i]);
+      bi.max_n = std::max(bi.max_n, tl[(size_t)i]);
+      bi.total_words += (pl[(size_t)i] + 31) / 32 + 1 + (tl[(size_t)i] + 31) / 32 + 1;
+    }
+  }
+  CU(cudaEventRecord(ctx->ev[0], st));
+  CU(cudaEventRecord(ctx->ev[1], st));
+  tsu::SeqView sv{n, (const uint8_t*)b->pattern, b->pattern_off, b->pattern_len, (const uint8_t*)b->text, b->text_off,
+                  b->text_len};
+  int32_t* d_status = res->pair_status;
+  if (!d_status) {
+    int rc = grow(ctx, ctx->b_status, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    if (rc) return rc;
+    d_status = P<int32_t>(ctx->b_status);
+  }
+  int64_t needed = 0;
+  int rc = run_device(ctx, sv, want_cigar, res->score, d_status, res->cigar, res->cigar_capacity, res->cigar_offset,
+                      &needed, bi);
+  res->cigar_needed = needed;
+  if (rc) return rc;
+  CU(cudaEventRecord(ctx->ev[7], st));
+  CU(cudaStreamSynchronize(st));
+  ctx->timing.pack_ms = n ? ev_ms(ctx->ev[2], ctx->ev[3]) : 0;
+  ctx->timing.align_ms = n ? ev_ms(ctx->ev[4], ctx->ev[5]) : 0;
+  ctx->timing.compact_ms = (n && want_cigar) ? ev_ms(ctx->ev[5], ctx->ev[6]) : 0;
+  ctx->timing.total_ms = ev_ms(ctx->ev[0], ctx->ev[7]);
+  // statuses
+  std::vector<int32_t> hs((size_t)n);
+  if (n) {
+    CU(cudaMemcpy(hs.data(), d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+  }
+  return collect_status(ctx, hs.data(), n);
+}
+
+int64_t tsu_cigar_to_ops(const uint32_t* runs, int64_t nruns, char* out, int64_t cap) {
+  static const char code2c[16] = {'M', 'I', 'D', 'N', 'S', 'H', 'P', '=', 'X', '?', '?', '?', '?', '?', '?', '?'};
+  int64_t w = 0;
+  for (int64_t i = 0; i < nruns; ++i) {
+    const int64_t len = runs[i] >> 4;
+    const char c = code2c[runs[i] & 15];
+    if (w + len > cap) return -1;
+    memset(out + w, c, (size_t)len);
+    w += len;
+  }
+  return w;
+}
+
+int64_t tsu_cigar_to_string(const uint32_t* runs, int64_t nruns, char* out, int64_t cap) {
+  static const char code2c[16] = {'M', 'I', 'D', 'N', 'S', 'H', 'P', '=', 'X', '?', '?', '?', '?', '?', '?', '?'};
+  int64_t w = 0;
+  char tmp[24];
+  for (int64_t i = 0; i < nruns; ++i) {
+    int k = snprintf(tmp, sizeof tmp, "%u%c", runs[i] >> 4, code2c[runs[i] & 15]);
+    if (w + k > cap) return -1;
+    memcpy(out + w, tmp, (size_t)k);
+    w += k;
+  }
+  return w;
+}
+
+}  // extern "C"
