@@ -213,7 +213,12 @@ def main():
     ap.add_argument("--score-only", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--pairs", type=int, default=0, help="override the pair count (small profiling cases)")
+    ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
     args = ap.parse_args()
+    if args.pairs:
+        n, L, r, si = WORKLOADS[args.workload]
+        WORKLOADS[args.workload] = (args.pairs, L, r, si)
     workload = args.workload
     if args.impl == "reference":
         run_reference(args, workload)
@@ -249,7 +254,7 @@ def main():
     pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
-    al = T.Aligner(*PEN, device=local)
+    al = T.Aligner(*PEN, device=local, max_error_hint=args.hint)
 
     # ---- value: batch resident in HBM ----------------------------------
     dev = torch.device("cuda", local)

@@ -100,6 +100,7 @@ int main(int argc, char const* argv[]) {
   long double gcups = cells / 1e9L / (long double)gpu_s;  // wfa_gpu.cu:130-133
   printf("GPU Time: %lf\n", gpu_s);
   printf("Estimated GCUPS GPU: : %Lf\n", gcups);
+  fflush(stdout);
 
   if (cig_out) {
     FILE* fo = fopen(cig_out, "w");
@@ -142,7 +143,8 @@ int main(int argc, char const* argv[]) {
       else
         printf("\n\n |ERROR|\n");
     }
-    if (h) dlclose(h);
+    // The plugin stays loaded until exit: unloading a library whose thread
+    // pool (e.g. OpenMP workers) is still alive crashes the process.
   }
   tsu_destroy(ctx);
   tsu_file_free(f);
