@@ -1,0 +1,313 @@
+// tsu_align.cuh -- the persistent gap-affine WFA kernel.
+//
+// Re-design of the reference kernel wfa_dispatcher (wfa_gpu.cu:191-722):
+//   * persistent grid; each warp pulls pairs from a device work queue
+//     (the reference launched one 32-thread block per pair, wfa_gpu.cu:113);
+//   * score steps s = 0, 1, ... in units of g = gcd(x, o, e);
+//   * one fused pass per step: every lane owns diagonals k = lo + lane + 32j
+//     and computes I, D and M of score s from the ring slots of scores
+//     s - x, s - o - e and s - e (wfa_gpu.cu:610-631), nullifies an
+//     out-of-bounds M (wfa_gpu.cu:628-629), extends M along its diagonal
+//     (wfa_gpu.cu:257-287), checks the end point (wfa_gpu.cu:288-338) and,
+//     with kCigar, streams one backtrace word per (score, diagonal) to HBM;
+//     the ends of M, I and D are trimmed with warp min/max reductions
+//     (wfa_gpu.cu:636-719);
+//   * kModeShared: the ring of the last max(x, o+e)+1 scores is int16 in
+//     shared memory (offsets clamped to [null, n+1], which changes no valid
+//     cell: validity depends only on the value and the diagonal, so a clamped
+//     out-of-bounds candidate still loses every max to -- or stays invalid
+//     against -- any valid one) and the pair's packed sequences are staged
+//     in shared memory.  Pairs wider than the ring or longer than the staging
+//     area are handed back for a kModeGlobal pass (int32 ring in global
+//     memory, sequences read through the read-only cache).
+// Lane 0 walks the backtrace once the end is reached (tsu_backtrace.cuh).
+#pragma once
+
+#include <type_traits>
+
+#include "tsu_backtrace.cuh"
+#include "tsu_common.cuh"
+#include "tsu_extend.cuh"
+
+namespace tsu {
+
+template <bool kCigar, int kMode>
+__global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_kernel(AlignArgs a) {
+  using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
+  using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int64_t gwarp = (int64_t)blockIdx.x * wpb + wib;
+  const int ns = ring_slots(a.rm, a.re);
+  const int W = a.ring_w;
+  unsigned char* wsm = smem_raw + (size_t)wib * warp_smem_bytes(a.rm, a.re, W, kMode, a.seq_cap);
+  int* s_lo = reinterpret_cast<int*>(wsm);
+  int* s_hi = s_lo + ns;
+  int* s_alo = s_hi + ns;
+  RT* ring;
+  uint32_t* sseq = nullptr;
+  if constexpr (kMode == kModeShared) {
+    ring = reinterpret_cast<RT*>(wsm + 3 * ns * 4);
+    sseq = reinterpret_cast<uint32_t*>(wsm + 3 * ns * 4 + ((ns * W * 2 + 15) & ~15));
+  } else {
+    ring = reinterpret_cast<RT*>(a.ring_global + gwarp * a.ring_stride);
+  }
+  uint32_t* const hist = kCigar ? a.hist + gwarp * a.hist_cap : nullptr;
+  int2* const table = kCigar ? a.table + gwarp * (int64_t)a.table_cap : nullptr;
+
+  for (;;) {
+    unsigned qi = 0;
+    if (lane == 0) qi = atomicAdd(a.queue, 1u);
+    qi = __shfl_sync(FULL, qi, 0);
+    if ((int64_t)qi >= a.n_order) break;
+    const int64_t pair = a.order ? a.order[qi] : (int64_t)qi;
+    const int m = a.seq.pat_len[pair];
+    const int n = a.seq.txt_len[pair];
+    const bool bytemode = a.pk.nonacgt[pair] | a.pk.nonacgt[a.seq.n + pair];
+    const uint32_t* gpw = reinterpret_cast<const uint32_t*>(a.pk.words + a.pk.woff[pair]);
+    const uint32_t* gtw = reinterpret_cast<const uint32_t*>(a.pk.words + a.pk.woff[a.seq.n + pair]);
+    const uint8_t* pb = a.seq.pat + a.seq.pat_off[pair];
+    const uint8_t* tb = a.seq.txt + a.seq.txt_off[pair];
+    const int k_end = n - m;
+    const int64_t s_max = score_bound(m, n, a.x, a.go, a.ge);
+    const int pwn = 2 * ((m + 31) / 32 + 1);
+    const int twn = 2 * ((n + 31) / 32 + 1);
+
+    int32_t st = kPairOk;
+    if constexpr (kMode == kModeShared) {
+      // bytes outside ACGT, lengths beyond int16 or sequences beyond the
+      // staging area: handled by the global variant
+      if (bytemode || m > 32000 || n > 32000 || pwn + twn > a.seq_cap) st = kPairScratch;
+    }
+    int s_end = -1;
+    int64_t hbase = 0;
+    unsigned long long n_cells = 0, n_steps = 0;
+
+    if (st == kPairOk) {
+      const uint32_t* pws;
+      const uint32_t* tws;
+      if constexpr (kMode == kModeShared) {
+        for (int i = lane; i < pwn; i += 32) sseq[i] = __ldg(gpw + i);
+        for (int i = lane; i < twn; i += 32) sseq[pwn + i] = __ldg(gtw + i);
+        pws = sseq;
+        tws = sseq + pwn;
+      } else {
+        pws = gpw;
+        tws = gtw;
+      }
+      const S P{pws}, T{tws};
+      for (int i = lane; i < ns; i += 32) {
+        s_lo[i] = 1;
+        s_hi[i] = 0;
+        s_alo[i] = 0;
+      }
+      __syncwarp();
+      auto store = [&](int idx, int32_t v) {
+        if constexpr (kMode == kModeShared)
+          ring[idx] = (RT)(v < 0 ? (int32_t)kNull16 : (v > n + 1 ? n + 1 : v));
+        else
+          ring[idx] = v;
+      };
+      // ---- score 0: M[0] = {k = 0: offset 0}, extended (wfa_gpu.cu:239-242)
+      {
+        int32_t o0 = 0;
+        if (lane == 0) {
+          const int rem = m < n ? m : n;
+          o0 = (kMode == kModeGlobal && bytemode) ? lcp8(pb, m, 0, tb, n, 0, rem) : lcp16(P, 0, T, 0, rem);
+          store(0, o0);
+          s_lo[0] = 0;
+          s_hi[0] = 0;
+          s_alo[0] = 0;
+          if (kCigar) {
+            table[0] = make_int2(0, 0);
+            hist[0] = 0u;
+          }
+        }
+        o0 = __shfl_sync(FULL, o0, 0);
+        hbase = 1;
+        n_cells = n_steps = 1;
+        if (k_end == 0 && o0 >= n) s_end = 0;
+        __syncwarp();
+      }
+
+      int s = 0;
+      int slm = 0, sli = 0;  // s mod rm, s mod re
+      while (s_end < 0) {
+        ++s;
+        if (++slm == a.rm) slm = 0;
+        if (++sli == a.re) sli = 0;
+        if (s > s_max) {  // the end is reachable by s_max: inconsistency
+          st = kPairInternal;
+          break;
+        }
+        int q;
+        q = slm - a.x;
+        if (q < 0) q += a.rm;
+        const int slot_mm = q;
+        q = slm - a.go;
+        if (q < 0) q += a.rm;
+        const int slot_mo = q;
+        q = sli - a.ge;
+        if (q < 0) q += a.re;
+        const int slot_ie = a.rm + q;
+        const int slot_de = a.rm + a.re + q;
+        // sources: first diagonal, cell count (0 = null), ring index of lo
+        int lo_mm = 0, c_mm = 0, b_mm = 0, lo_mo = 0, c_mo = 0, b_mo = 0;
+        int lo_ie = 0, c_ie = 0, b_ie = 0, lo_de = 0, c_de = 0, b_de = 0;
+        if (s - a.x >= 0) {
+          lo_mm = s_lo[slot_mm];
+          c_mm = max(s_hi[slot_mm] - lo_mm + 1, 0);
+          b_mm = slot_mm * W + lo_mm - s_alo[slot_mm];
+        }
+        if (s - a.go >= 0) {
+          lo_mo = s_lo[slot_mo];
+          c_mo = max(s_hi[slot_mo] - lo_mo + 1, 0);
+          b_mo = slot_mo * W + lo_mo - s_alo[slot_mo];
+        }
+        if (s - a.ge >= 0) {
+          lo_ie = s_lo[slot_ie];
+          c_ie = max(s_hi[slot_ie] - lo_ie + 1, 0);
+          b_ie = slot_ie * W + lo_ie - s_alo[slot_ie];
+          lo_de = s_lo[slot_de];
+          c_de = max(s_hi[slot_de] - lo_de + 1, 0);
+          b_de = slot_de * W + lo_de - s_alo[slot_de];
+        }
+        const int out_m = slm, out_i = a.rm + sli, out_d = a.rm + a.re + sli;
+        if ((c_mm | c_mo | c_ie | c_de) == 0) {  // null step (wfa_gpu.cu:417-422)
+          __syncwarp();
+          if (lane == 0) {
+            s_lo[out_m] = 1; s_hi[out_m] = 0;
+            s_lo[out_i] = 1; s_hi[out_i] = 0;
+            s_lo[out_d] = 1; s_hi[out_d] = 0;
+          }
+          __syncwarp();
+          continue;
+        }
+        int lo = INT_MAX, hi = INT_MIN;  // envelope of the sources (wfa_gpu.cu:429-439)
+        if (c_mm) { lo = lo_mm; hi = lo_mm + c_mm - 1; }
+        if (c_mo) { lo = min(lo, lo_mo - 1); hi = max(hi, lo_mo + c_mo); }
+        if (c_ie) { lo = min(lo, lo_ie + 1); hi = max(hi, lo_ie + c_ie); }
+        if (c_de) { lo = min(lo, lo_de - 1); hi = max(hi, lo_de + c_de - 2); }
+        const int width = hi - lo + 1;
+        const bool i_present = c_mo || c_ie;
+        const bool d_present = c_mo || c_de;
+        if (width > W || (kCigar && (s >= a.table_cap || hbase + width > a.hist_cap))) {
+          st = kPairScratch;
+          break;
+        }
+        const int w_m = out_m * W - lo, w_i = out_i * W - lo, w_d = out_d * W - lo;
+        uint32_t* hrow = kCigar ? hist + hbase - lo : nullptr;
+        int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
+        bool found = false;
+        for (int k = lo + lane; k <= hi; k += 32) {
+          int j;
+          j = k - 1 - lo_mo;
+          const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+          j = k - 1 - lo_ie;
+          const int32_t ins_e = ((unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
+          j = k + 1 - lo_mo;
+          const int32_t del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+          j = k + 1 - lo_de;
+          const int32_t del_e = ((unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
+          j = k - lo_mm;
+          const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
+          const int32_t ins = max(ins_o, ins_e) + 1;
+          const int32_t del = max(del_o, del_e);
+          // M = max(D, mismatch, I); ties: mismatch > D > I (piggyback order)
+          int32_t p = ins;
+          uint32_t bits = kSrcIns;
+          if (del >= p) { p = del; bits = kSrcDel; }
+          if (mis >= p) { p = mis; bits = kSrcMis; }
+          if (ins_e >= ins_o) bits |= kIExt;
+          if (del_e >= del_o) bits |= kDExt;
+          int32_t om = kNull;
+          if (in_bounds(p, k, m, n)) {
+            const int vv = p - k;
+            const int rem = min(m - vv, n - p);
+            om = p + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem));
+            fm = min(fm, k);
+            lm = k;
+            found |= (k == k_end) & (om >= n);
+          }
+          store(w_m + k, om);
+          if (i_present) {
+            store(w_i + k, ins);
+            if (in_bounds(ins, k, m, n)) { fi = min(fi, k); li = k; }
+          }
+          if (d_present) {
+            store(w_d + k, del);
+            if (in_bounds(del, k, m, n)) { fd = min(fd, k); ld = k; }
+          }
+          if (kCigar) hrow[k] = ((uint32_t)p << 4) | bits;
+        }
+        fm = __reduce_min_sync(FULL, fm);
+        lm = __reduce_max_sync(FULL, lm);
+        fi = __reduce_min_sync(FULL, fi);
+        li = __reduce_max_sync(FULL, li);
+        fd = __reduce_min_sync(FULL, fd);
+        ld = __reduce_max_sync(FULL, ld);
+        const bool any_found = __any_sync(FULL, found);
+        if (lane == 0) {
+          // trimmed limits (wfa_gpu.cu:636-719); empty => null
+          s_lo[out_m] = fm; s_hi[out_m] = lm; s_alo[out_m] = lo;
+          if (i_present) { s_lo[out_i] = fi; s_hi[out_i] = li; } else { s_lo[out_i] = 1; s_hi[out_i] = 0; }
+          s_alo[out_i] = lo;
+          if (d_present) { s_lo[out_d] = fd; s_hi[out_d] = ld; } else { s_lo[out_d] = 1; s_hi[out_d] = 0; }
+          s_alo[out_d] = lo;
+          if (kCigar) table[s] = make_int2(lo, (int)hbase);
+        }
+        hbase += width;
+        n_cells += (unsigned long long)width;
+        ++n_steps;
+        __syncwarp();
+        if (any_found) s_end = s;
+      }
+    }
+
+    if (st == kPairOk) {
+      if (lane == 0) a.score[pair] = s_end * a.g;
+      if (kCigar) {
+        // reserve the run bound 2*s/min_pen + 1 in the arena, then walk
+        const int min_pen = min(a.x, a.go);
+        const int64_t bound = 2 * (int64_t)s_end / min_pen + 1;
+        if (lane == 0) {
+          int32_t len = 0;
+          int64_t pos = 0;
+          const unsigned long long at = atomicAdd(a.arena_cursor, (unsigned long long)bound);
+          if ((int64_t)(at + bound) > a.arena_cap) {
+            st = kPairArena;
+          } else {
+            const int r =
+                backtrace_walk(hist, hbase, table, s_end, m, n, a.x, a.go, a.ge, a.arena + at + bound, (int)bound);
+            if (r < 0) {
+              st = kPairInternal;
+            } else {
+              len = r;
+              pos = (int64_t)(at + bound) - r;
+            }
+          }
+          a.cig_pos[pair] = pos;
+          a.cig_len[pair] = len;
+        }
+        st = __shfl_sync(FULL, st, 0);
+      }
+    }
+    if (lane == 0) {
+      a.status[pair] = st;
+      if (st == kPairScratch || st == kPairArena) {
+        const unsigned r = atomicAdd(a.retry_count, 1u);
+        a.retry[r] = (int32_t)pair;
+      }
+      if (a.work) {
+        atomicAdd(a.work, n_cells);
+        atomicAdd(a.work + 1, n_steps);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace tsu

@@ -1,0 +1,126 @@
+// tsu_backtrace.cuh -- CIGAR backtrace from the per-(score, diagonal) words.
+//
+// The reference computes no CIGAR (its backtrace types are declared but
+// unused, common.h:17-31,48-49,67-77); its check takes CIGARs from WFA2-lib
+// (wfa_gpu.cu:164).  This walk restates the WFA2 wavefront backtrace: in M,
+// first the matches down to the pre-extension offset, then one operation
+// chosen by the source bits stored at compute time, whose tie order is the
+// piggyback order of the reference's bt_type_t codes (mismatch 9 > D_ext 6 >
+// D_open 5 > I_ext 2 > I_open 1).  Runs are written backwards, one uint32 per
+// run ((len << 4) | op), ending at out_end.
+#pragma once
+
+#include "tsu_common.cuh"
+
+namespace tsu {
+
+struct RunWriter {
+  uint32_t* end;
+  int cnt, cap;
+  uint32_t op;
+  int64_t len;
+  __device__ __forceinline__ void put(uint32_t o, int64_t l) {
+    if (l <= 0) return;
+    if (o == op) {
+      len += l;
+      return;
+    }
+    flush();
+    op = o;
+    len = l;
+  }
+  __device__ __forceinline__ void flush() {
+    if (len > 0) {
+      if (cnt < cap) end[-1 - cnt] = ((uint32_t)len << 4) | op;
+      ++cnt;
+    }
+    len = 0;
+  }
+};
+
+// Returns the number of runs, or -1 on an inconsistency (a word outside the
+// history, a predecessor beyond the current offset, more runs than cap).
+__device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
+                              int s_end, int m, int n, int x, int go, int ge, uint32_t* out_end, int cap) {
+  RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
+  enum { M = 0, I = 1, D = 2 };
+  int state = M, s = s_end, k = n - m;
+  int32_t off = n;
+  int v = off - k, h = off;
+  int guard = 4 * (m + n) + 8;
+  while (v > 0 && h > 0 && s > 0) {
+    if (--guard < 0) return -1;
+    const int2 te = table[s];
+    const int64_t hidx = (int64_t)te.y + (k - te.x);
+    if (k < te.x || hidx >= hist_used) return -1;  // never on a valid path
+    const uint32_t word = hist[hidx];
+    if (state == M) {
+      const int32_t p = (int32_t)(word >> 4);
+      if (p > off) return -1;
+      w.put(kOpM, off - p);
+      off = p;
+      v = off - k;
+      h = off;
+      if (v <= 0 || h <= 0) break;
+      const uint32_t src = word & 3u;
+      if (src == kSrcMis) {
+        w.put(kOpX, 1);
+        s -= x;
+        --off;
+      } else if (src == kSrcIns) {
+        w.put(kOpI, 1);
+        if (word & kIExt) {
+          s -= ge;
+          state = I;
+        } else {
+          s -= go;
+        }
+        --k;
+        --off;
+      } else {
+        w.put(kOpD, 1);
+        if (word & kDExt) {
+          s -= ge;
+          state = D;
+        } else {
+          s -= go;
+        }
+        ++k;
+      }
+    } else if (state == I) {
+      w.put(kOpI, 1);
+      if (word & kIExt) {
+        s -= ge;
+      } else {
+        s -= go;
+        state = M;
+      }
+      --k;
+      --off;
+    } else {
+      w.put(kOpD, 1);
+      if (word & kDExt) {
+        s -= ge;
+      } else {
+        s -= go;
+        state = M;
+      }
+      ++k;
+    }
+    v = off - k;
+    h = off;
+    if (s < 0) return -1;
+  }
+  if (v > 0 && h > 0) {
+    const int nm = v < h ? v : h;
+    w.put(kOpM, nm);
+    v -= nm;
+    h -= nm;
+  }
+  w.put(kOpD, v);
+  w.put(kOpI, h);
+  w.flush();
+  return w.cnt <= cap ? w.cnt : -1;
+}
+
+}  // namespace tsu

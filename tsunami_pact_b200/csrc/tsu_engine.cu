@@ -30,8 +30,9 @@ struct DevBuf {
 };
 
 struct Pass {
-  int smem_ring = 1;
+  int mode = 0;  // tsu::kModeShared / kModeGlobal
   int ring_w = 0;
+  int seq_cap = 0;
   int64_t warps = 0;
   int blocks = 0;
   int wpb = 4;  // warps per block
@@ -151,6 +152,38 @@ struct BatchInfo {
   int64_t total_words = 0;
 };
 
+// The four align_kernel instantiations: CIGAR or score only, shared or
+// global wavefront ring.
+template <bool kCigar, int kMode>
+cudaError_t occ_one(int threads, size_t smem, int* occ) {
+  cudaError_t e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode>, threads, smem);
+}
+
+cudaError_t align_occupancy(bool cigar, int mode, int threads, size_t smem, int* occ) {
+  if (cigar) return mode == tsu::kModeShared ? occ_one<true, tsu::kModeShared>(threads, smem, occ)
+                                             : occ_one<true, tsu::kModeGlobal>(threads, smem, occ);
+  return mode == tsu::kModeShared ? occ_one<false, tsu::kModeShared>(threads, smem, occ)
+                                  : occ_one<false, tsu::kModeGlobal>(threads, smem, occ);
+}
+
+void launch_align(bool cigar, int mode, int blocks, int threads, size_t smem, cudaStream_t st,
+                  const tsu::AlignArgs& a) {
+  if (cigar) {
+    if (mode == tsu::kModeShared)
+      tsu::align_kernel<true, tsu::kModeShared><<<blocks, threads, smem, st>>>(a);
+    else
+      tsu::align_kernel<true, tsu::kModeGlobal><<<blocks, threads, smem, st>>>(a);
+  } else {
+    if (mode == tsu::kModeShared)
+      tsu::align_kernel<false, tsu::kModeShared><<<blocks, threads, smem, st>>>(a);
+    else
+      tsu::align_kernel<false, tsu::kModeGlobal><<<blocks, threads, smem, st>>>(a);
+  }
+}
+
 // Configure a pass.  first: shared-memory ring sized for occupancy;
 // otherwise global-memory ring wide enough for any pair of the batch.
 int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, double hint, bool want_cigar,
@@ -162,32 +195,29 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
   int64_t s_hint = hint_score(ctx, maxlen, hint);
   const int64_t full_w = (int64_t)bi.max_m + bi.max_n + 3;
   int64_t width_hint = std::min<int64_t>(full_w, 2 * s_hint / ctx->ge + 3);
-  if (first) {
-    // Ring width: enough for ~12 warps per SM, capped by the widest possible
-    // wavefront of this batch.
-    int w = (int)std::min<int64_t>(full_w, 384);
-    w = (w + 31) & ~31;
-    p.smem_ring = 1;
-    p.ring_w = std::max(w, 32);
+  // Shared mode for the first pass: int16 ring of kSharedW diagonals per
+  // slot and the pair's packed sequences staged per warp (up to
+  // kSharedSeqWords); pairs beyond either come back for a global pass.
+  constexpr int kSharedW = 384, kSharedSeqWords = 544;
+  if (first && maxlen <= 32000) {
+    p.mode = tsu::kModeShared;
+    p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, kSharedW) + 15) & ~15);
+    const int64_t seqw = 2 * ((bi.max_m + 31) / 32 + 1) + 2 * ((bi.max_n + 31) / 32 + 1);
+    p.seq_cap = (int)std::min<int64_t>(seqw, kSharedSeqWords);
   } else {
-    p.smem_ring = 0;
+    p.mode = tsu::kModeGlobal;
     p.ring_w = (int)full_w;
+    p.seq_cap = 0;
   }
-  p.smem_bytes = (size_t)wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, p.smem_ring) * 4;
+  p.smem_bytes = (size_t)wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, p.seq_cap);
   if (p.smem_bytes > (size_t)ctx->smem_optin) {
-    p.smem_ring = 0;
+    p.mode = tsu::kModeGlobal;
     p.ring_w = (int)full_w;
-    p.smem_bytes = (size_t)wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, 0) * 4;
+    p.seq_cap = 0;
+    p.smem_bytes = (size_t)wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, 0);
   }
   int occ = 0;
-  cudaError_t e;
-  if (want_cigar) {
-    cudaFuncSetAttribute(tsu::align_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tsu::align_kernel<true>, wpb * 32, p.smem_bytes);
-  } else {
-    cudaFuncSetAttribute(tsu::align_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tsu::align_kernel<false>, wpb * 32, p.smem_bytes);
-  }
+  cudaError_t e = align_occupancy(want_cigar, p.mode, wpb * 32, p.smem_bytes, &occ);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
   int64_t warps = (int64_t)ctx->sms * occ * wpb;
   // scratch per warp
@@ -198,7 +228,7 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
     const int64_t sq = s_hint * s_hint / ctx->ge + 2 * s_hint + 64;
     hist_cap = std::min<int64_t>(std::min<int64_t>(sq, (s_hint + 1) * width_hint), INT32_MAX - 64);
   }
-  const int64_t ring_ints = p.smem_ring ? 0 : (int64_t)ns * p.ring_w;
+  const int64_t ring_ints = p.mode == tsu::kModeShared ? 0 : (int64_t)ns * p.ring_w;
   // scratch buffers are regrown for this pass: their current size is free
   const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
   const size_t avail = ctx->budget > fixed + reserve_bytes ? ctx->budget - fixed - reserve_bytes : 0;
@@ -218,7 +248,7 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
   }
   p.warps = warps;
   p.blocks = (int)(warps / p.wpb);
-  p.smem_bytes = (size_t)p.wpb * tsu::warp_smem_ints(ctx->rm, ctx->re, p.ring_w, p.smem_ring) * 4;
+  p.smem_bytes = (size_t)p.wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, p.seq_cap);
   p.hist_cap = hist_cap;
   p.table_cap = (int)table_cap;
   *out = p;
@@ -297,7 +327,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   for (;;) {
     Pass ps;
     if ((rc = plan_pass(ctx, bi, n_order, first, hint, want_cigar, 0, &ps))) return rc;
-    if (!ps.smem_ring) {
+    if (ps.mode == tsu::kModeGlobal) {
       if ((rc = grow(ctx, ctx->b_ring, sizeof(int32_t) * (size_t)ps.warps * tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w)))
         return rc;
     }
@@ -317,14 +347,13 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.rm = ctx->rm;
     a.re = ctx->re;
     a.ring_w = ps.ring_w;
-    a.smem_ring = ps.smem_ring;
-    a.ring_global = ps.smem_ring ? nullptr : P<int32_t>(ctx->b_ring);
+    a.seq_cap = ps.seq_cap;
+    a.ring_global = ps.mode == tsu::kModeShared ? nullptr : P<int32_t>(ctx->b_ring);
     a.ring_stride = (int64_t)tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w;
     a.hist = want_cigar ? P<uint32_t>(ctx->b_hist) : nullptr;
     a.hist_cap = ps.hist_cap;
     a.table = want_cigar ? P<int2>(ctx->b_table) : nullptr;
     a.table_cap = ps.table_cap;
-    a.want_cigar = want_cigar;
     a.score = d_score;
     a.status = d_status;
     a.arena = want_cigar ? P<uint32_t>(ctx->b_arena) : nullptr;
@@ -336,10 +365,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.retry = P<int32_t>(ctx->b_retry);
     a.retry_count = d_retry_cnt;
     a.work = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 24);
-    if (want_cigar)
-      tsu::align_kernel<true><<<ps.blocks, 32 * ps.wpb, ps.smem_bytes, st>>>(a);
-    else
-      tsu::align_kernel<false><<<ps.blocks, 32 * ps.wpb, ps.smem_bytes, st>>>(a);
+    launch_align(want_cigar, ps.mode, ps.blocks, 32 * ps.wpb, ps.smem_bytes, st, a);
     ctx->timing.kernel_launches++;
     CU(cudaGetLastError());
     ++passes;
@@ -412,8 +438,8 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     }
     if (total > out_cap) return TSU_EOVERFLOW;
     const int64_t blocks = std::min<int64_t>((n + 7) / 8, (int64_t)ctx->sms * 16);
-    tsu::compact_kernel<<<(int)blocks, 256, 0, st>>>(n, P<uint32_t>(ctx->b_arena), P<int64_t>(ctx->b_cpos),
-                                                    P<int32_t>(ctx->b_clen), d_out_off, d_out_runs);
+    tsu::compact_kernel<<<(int)blocks, 256, 0, st>>>(n, P<uint32_t>(ctx->b_arena), P<int64_t>(ctx->b_cpos), d_out_off,
+                                                    d_out_runs);
     ctx->timing.kernel_launches++;
     CU(cudaGetLastError());
   }
