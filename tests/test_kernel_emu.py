@@ -1,0 +1,134 @@
+"""The CUDA kernels' own source, run on the CPU through the warp emulator
+(tests/emu/warp_emu.h) under AddressSanitizer/UBSan, against the oracle.
+
+This checks the kernels' index arithmetic and outputs without a GPU: any
+shared- or global-memory access outside its buffer aborts the run, and every
+score and operation string must equal the oracle's."""
+import os
+import random
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EMU_DIR = os.path.join(ROOT, "tests", "emu")
+EXE = os.path.join(EMU_DIR, "_build", "emu_driver")
+SRCS = [os.path.join(EMU_DIR, "emu_driver.cpp"), os.path.join(EMU_DIR, "warp_emu.h")] + [
+    os.path.join(ROOT, "tsunami_pact_b200", "csrc", f)
+    for f in os.listdir(os.path.join(ROOT, "tsunami_pact_b200", "csrc"))
+    if f.endswith((".cuh", ".h"))
+]
+
+
+@pytest.fixture(scope="module")
+def emu():
+    os.makedirs(os.path.dirname(EXE), exist_ok=True)
+    newest = max(os.path.getmtime(s) for s in SRCS)
+    if not os.path.exists(EXE) or os.path.getmtime(EXE) < newest:
+        subprocess.run(["g++", "-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+                        "-fno-sanitize-recover=undefined", "-o", EXE, os.path.join(EMU_DIR, "emu_driver.cpp"),
+                        "-lpthread"], check=True)
+    return EXE
+
+
+def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, wpb=2):
+    hdr = f"{pen[0]} {pen[1]} {pen[2]} {int(cigar)} {hint} {int(shared_first)} {wpb} {len(pairs)}\n"
+    body = b"".join(f"{len(p)} {len(t)}\n".encode() + p + b"\n" + t + b"\n" for p, t in pairs)
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1")
+    r = subprocess.run([exe], input=hdr.encode() + body, capture_output=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr.decode()[-3000:]
+    lines = r.stdout.decode().split("\n")
+    out = []
+    for ln in lines[: len(pairs)]:
+        s, ops = ln.split("\t")
+        out.append((int(s), ops))
+    tail = lines[len(pairs)].split()
+    return out, int(tail[1]), int(tail[3])
+
+
+def _b(s):
+    return s if isinstance(s, bytes) else s.encode()
+
+
+def check(exe, oracle, pairs, pen=(4, 6, 2), **kw):
+    pairs = [(_b(p), _b(t)) for p, t in pairs]
+    got, passes, retried = run_emu(exe, pairs, pen, **kw)
+    for (p, t), (s, ops) in zip(pairs, got):
+        es, eops = oracle.align(p, t, *pen)
+        assert (s, ops) == (es, eops), (p, t, pen, s, es, ops, eops)
+    return passes, retried
+
+
+def test_kat_each_alone(emu, oracle, kat_cases):
+    """One pair per batch: single-pair launches, tiny rings."""
+    for c in kat_cases:
+        check(emu, oracle, [(c["p"], c["t"])], tuple(c["pen"]))
+
+
+def test_kat_as_batch(emu, oracle, kat_cases):
+    by = {}
+    for c in kat_cases:
+        by.setdefault(tuple(c["pen"]), []).append((c["p"], c["t"]))
+    for pen, pairs in by.items():
+        check(emu, oracle, pairs, pen)
+
+
+def test_regression_fixture(emu, oracle, regress_cases):
+    by = {}
+    for c in regress_cases:
+        by.setdefault(tuple(c["pen"]), []).append((c["p"], c["t"]))
+    for pen, pairs in by.items():
+        check(emu, oracle, pairs, pen)
+
+
+@pytest.mark.parametrize("pen", [(4, 6, 2), (20, 1, 1), (3, 5, 1), (5, 11, 3)])
+def test_random_mixed(emu, oracle, pen):
+    rng = random.Random(sum(pen))
+    pairs = []
+    for i in range(60):
+        alpha = "ACGT" if i % 5 else "ACGTN"
+        p = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 120)))
+        t = list(p)
+        for _ in range(rng.randint(0, 12)):
+            pos = rng.randint(0, max(0, len(t) - 1))
+            r = rng.random()
+            if r < 0.33 and t:
+                t[pos] = rng.choice(alpha)
+            elif r < 0.66:
+                t.insert(pos, rng.choice(alpha))
+            elif t:
+                del t[pos]
+        pairs.append((p, "".join(t)))
+    check(emu, oracle, pairs, pen)
+
+
+def test_global_mode_and_retries(emu, oracle):
+    """A tiny hint forces scratch overflow and several global-mode passes."""
+    rng = random.Random(3)
+    pairs = []
+    for _ in range(12):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(50, 400)))
+        t = "".join(rng.choice("ACGT") for _ in range(rng.randint(50, 400)))
+        pairs.append((p, t))
+    passes, retried = check(emu, oracle, pairs, hint=0.0001)
+    assert passes > 1 and retried > 0
+    check(emu, oracle, pairs, shared_first=False)
+
+
+def test_wide_pairs_leave_shared_ring(emu, oracle):
+    """Wavefronts wider than the shared ring (384 diagonals) are re-run in
+    global mode; a batch mixing both kinds."""
+    rng = random.Random(9)
+    pairs = [("".join(rng.choice("ACGT") for _ in range(300)), "".join(rng.choice("ACGT") for _ in range(300)))]
+    pairs += [("ACGT" * 10, "ACGA" * 10), ("", "A" * 500), ("C" * 450, "")]
+    passes, retried = check(emu, oracle, pairs)
+    assert retried >= 1
+
+
+def test_score_only(emu, oracle):
+    rng = random.Random(4)
+    pairs = [("".join(rng.choice("ACGT") for _ in range(rng.randint(0, 90))),
+              "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 90)))) for _ in range(30)]
+    got, _, _ = run_emu(emu, [(_b(p), _b(t)) for p, t in pairs], cigar=False)
+    for (p, t), (s, ops) in zip(pairs, got):
+        assert s == oracle.align(p, t)[0] and ops == ""

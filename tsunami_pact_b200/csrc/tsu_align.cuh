@@ -35,7 +35,11 @@ template <bool kCigar, int kMode>
 __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_kernel(AlignArgs a) {
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
+#ifdef TSU_WARP_EMU
+  unsigned char* smem_raw = emu::dyn_smem();  // CPU warp emulation of the tests
+#else
   extern __shared__ __align__(16) unsigned char smem_raw[];
+#endif
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -154,26 +158,24 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         if (q < 0) q += a.re;
         const int slot_ie = a.rm + q;
         const int slot_de = a.rm + a.re + q;
-        // sources: first diagonal, cell count (0 = null), ring index of lo
+        // sources: first diagonal, cell count (0 = null), ring index of lo.
+        // Slot limits are either a trimmed range inside the slot's compute
+        // range or the empty range (1, 0); the count is taken by comparison.
         int lo_mm = 0, c_mm = 0, b_mm = 0, lo_mo = 0, c_mo = 0, b_mo = 0;
         int lo_ie = 0, c_ie = 0, b_ie = 0, lo_de = 0, c_de = 0, b_de = 0;
-        if (s - a.x >= 0) {
-          lo_mm = s_lo[slot_mm];
-          c_mm = max(s_hi[slot_mm] - lo_mm + 1, 0);
-          b_mm = slot_mm * W + lo_mm - s_alo[slot_mm];
-        }
-        if (s - a.go >= 0) {
-          lo_mo = s_lo[slot_mo];
-          c_mo = max(s_hi[slot_mo] - lo_mo + 1, 0);
-          b_mo = slot_mo * W + lo_mo - s_alo[slot_mo];
-        }
+        auto src = [&](int slot, int& lo_x, int& c_x, int& b_x) {
+          const int l = s_lo[slot], h = s_hi[slot];
+          if (h >= l) {
+            lo_x = l;
+            c_x = h - l + 1;
+            b_x = slot * W + l - s_alo[slot];
+          }
+        };
+        if (s - a.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
+        if (s - a.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
         if (s - a.ge >= 0) {
-          lo_ie = s_lo[slot_ie];
-          c_ie = max(s_hi[slot_ie] - lo_ie + 1, 0);
-          b_ie = slot_ie * W + lo_ie - s_alo[slot_ie];
-          lo_de = s_lo[slot_de];
-          c_de = max(s_hi[slot_de] - lo_de + 1, 0);
-          b_de = slot_de * W + lo_de - s_alo[slot_de];
+          src(slot_ie, lo_ie, c_ie, b_ie);
+          src(slot_de, lo_de, c_de, b_de);
         }
         const int out_m = slm, out_i = a.rm + sli, out_d = a.rm + a.re + sli;
         if ((c_mm | c_mo | c_ie | c_de) == 0) {  // null step (wfa_gpu.cu:417-422)
@@ -251,12 +253,12 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         ld = __reduce_max_sync(FULL, ld);
         const bool any_found = __any_sync(FULL, found);
         if (lane == 0) {
-          // trimmed limits (wfa_gpu.cu:636-719); empty => null
-          s_lo[out_m] = fm; s_hi[out_m] = lm; s_alo[out_m] = lo;
-          if (i_present) { s_lo[out_i] = fi; s_hi[out_i] = li; } else { s_lo[out_i] = 1; s_hi[out_i] = 0; }
-          s_alo[out_i] = lo;
-          if (d_present) { s_lo[out_d] = fd; s_hi[out_d] = ld; } else { s_lo[out_d] = 1; s_hi[out_d] = 0; }
-          s_alo[out_d] = lo;
+          // trimmed limits (wfa_gpu.cu:636-719); no in-bounds cell (first
+          // > last, e.g. INT_MAX > INT_MIN) stores the empty range (1, 0)
+          const bool em = fm > lm, ei = !i_present || fi > li, ed = !d_present || fd > ld;
+          s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
+          s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
+          s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
           if (kCigar) table[s] = make_int2(lo, (int)hbase);
         }
         hbase += width;

@@ -21,6 +21,7 @@
 
 #include "../../include/tsunami_b200.h"
 #include "tsu_kernels.cuh"
+#include "tsu_plan.h"
 
 namespace {
 
@@ -140,11 +141,6 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-// Reduced-unit score expected at the error hint for a pair of length L.
-int64_t hint_score(const tsu_ctx* ctx, int64_t L, double hint) {
-  const double per_edit = std::max(ctx->x, ctx->go);
-  return (int64_t)(hint * (double)L * per_edit) + 16;
-}
 
 struct BatchInfo {
   int64_t n = 0;
@@ -189,46 +185,20 @@ void launch_align(bool cigar, int mode, int blocks, int threads, size_t smem, cu
 int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, double hint, bool want_cigar,
               size_t reserve_bytes, Pass* out) {
   Pass p;
-  const int ns = tsu::ring_slots(ctx->rm, ctx->re);
   const int wpb = 4;
-  const int64_t maxlen = std::max(bi.max_m, bi.max_n);
-  int64_t s_hint = hint_score(ctx, maxlen, hint);
-  const int64_t full_w = (int64_t)bi.max_m + bi.max_n + 3;
-  int64_t width_hint = std::min<int64_t>(full_w, 2 * s_hint / ctx->ge + 3);
-  // Shared mode for the first pass: int16 ring of kSharedW diagonals per
-  // slot and the pair's packed sequences staged per warp (up to
-  // kSharedSeqWords); pairs beyond either come back for a global pass.
-  constexpr int kSharedW = 384, kSharedSeqWords = 544;
-  if (first && maxlen <= 32000) {
-    p.mode = tsu::kModeShared;
-    p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, kSharedW) + 15) & ~15);
-    const int64_t seqw = 2 * ((bi.max_m + 31) / 32 + 1) + 2 * ((bi.max_n + 31) / 32 + 1);
-    p.seq_cap = (int)std::min<int64_t>(seqw, kSharedSeqWords);
-  } else {
-    p.mode = tsu::kModeGlobal;
-    p.ring_w = (int)full_w;
-    p.seq_cap = 0;
-  }
-  p.smem_bytes = (size_t)wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, p.seq_cap);
-  if (p.smem_bytes > (size_t)ctx->smem_optin) {
-    p.mode = tsu::kModeGlobal;
-    p.ring_w = (int)full_w;
-    p.seq_cap = 0;
-    p.smem_bytes = (size_t)wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, 0);
-  }
+  const tsu::PassGeom g = tsu::plan_geometry(ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, bi.max_m, bi.max_n, first,
+                                             hint, want_cigar, ctx->smem_optin, wpb);
+  p.mode = g.mode;
+  p.ring_w = g.ring_w;
+  p.seq_cap = g.seq_cap;
+  p.smem_bytes = (size_t)wpb * g.warp_smem;
   int occ = 0;
   cudaError_t e = align_occupancy(want_cigar, p.mode, wpb * 32, p.smem_bytes, &occ);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
   int64_t warps = (int64_t)ctx->sms * occ * wpb;
-  // scratch per warp
-  // Backtrace words up to score s: sum_j (2j/ge + 1) ~= s^2/ge + 2s.
-  const int64_t table_cap = want_cigar ? std::min<int64_t>(s_hint + 1, INT32_MAX / 2) : 0;
-  int64_t hist_cap = 0;
-  if (want_cigar) {
-    const int64_t sq = s_hint * s_hint / ctx->ge + 2 * s_hint + 64;
-    hist_cap = std::min<int64_t>(std::min<int64_t>(sq, (s_hint + 1) * width_hint), INT32_MAX - 64);
-  }
-  const int64_t ring_ints = p.mode == tsu::kModeShared ? 0 : (int64_t)ns * p.ring_w;
+  const int64_t table_cap = g.table_cap;
+  const int64_t hist_cap = g.hist_cap;
+  const int64_t ring_ints = g.ring_ints;
   // scratch buffers are regrown for this pass: their current size is free
   const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
   const size_t avail = ctx->budget > fixed + reserve_bytes ? ctx->budget - fixed - reserve_bytes : 0;
@@ -248,7 +218,7 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
   }
   p.warps = warps;
   p.blocks = (int)(warps / p.wpb);
-  p.smem_bytes = (size_t)p.wpb * tsu::warp_smem_bytes(ctx->rm, ctx->re, p.ring_w, p.mode, p.seq_cap);
+  p.smem_bytes = (size_t)p.wpb * g.warp_smem;
   p.hist_cap = hist_cap;
   p.table_cap = (int)table_cap;
   *out = p;
@@ -304,9 +274,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   const int min_pen = std::min(ctx->x, ctx->go);
   int64_t arena_cap = 0;
   if (want_cigar) {
-    const int64_t maxlen = std::max(bi.max_m, bi.max_n);
-    const int64_t per_pair = 2 * hint_score(ctx, maxlen, ctx->err_hint) / min_pen + 1;
-    arena_cap = std::max<int64_t>(n * std::min<int64_t>(per_pair, (int64_t)bi.max_m + bi.max_n + 1), 1024);
+    arena_cap = tsu::arena_runs(ctx->x, ctx->go, n, bi.max_m, bi.max_n, ctx->err_hint);
     size_t room = ctx->budget > ctx->held() ? ctx->budget - ctx->held() : 0;
     arena_cap = std::min<int64_t>(arena_cap, (int64_t)(room / 8));  // leave half for scratch
     if ((rc = grow(ctx, ctx->b_arena, sizeof(uint32_t) * (size_t)std::max<int64_t>(arena_cap, 1024)))) return rc;
@@ -374,20 +342,22 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     CU(cudaStreamSynchronize(st));
     if (nretry == 0) break;
     ctx->timing.retried_pairs += nretry;
-    if (passes > 12) return set_err(ctx, TSU_ENOMEM, "pairs still exceed scratch after %d passes", passes);
+    if (passes > 16) return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes", passes);
     // the retry list becomes the next pass's order; arena overflow grows it
     CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry,
                        cudaMemcpyDeviceToDevice, st));
     order = P<int32_t>(ctx->b_order);
     n_order = nretry;
-    if (!first) hint *= 2.0;
+    if (!first && hint >= tsu::kHintCeiling)
+      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one warp can hold within the budget", nretry);
+    hint = tsu::next_hint(hint, first);
     first = false;
     if (want_cigar) {
       unsigned long long used = 0;
       CU(cudaMemcpyAsync(&used, d_cursor, sizeof used, cudaMemcpyDeviceToHost, st));
       CU(cudaStreamSynchronize(st));
       const int64_t maxlen = std::max(bi.max_m, bi.max_n);
-      const int64_t need = (int64_t)used + (int64_t)nretry * (2 * hint_score(ctx, maxlen, hint) / min_pen + 1);
+      const int64_t need = (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
       if (need > arena_cap) {
         // keep the runs written so far: grow by copy
         DevBuf nb;
