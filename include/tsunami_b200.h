@@ -140,6 +140,24 @@ int tsu_align_fixed(tsu_ctx* ctx, const char* pattern, const char* text, int64_t
  * the benchmark's kernel-time leg) uses; no host copies of sequence data. */
 int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* dev_batch, tsu_result* dev_res, uint32_t flags);
 
+/* ---- scores without allocating -----------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code recording a CUDA graph (allocation is illegal during capture),
+ * plug-ins whose host framework owns every device allocation, services that
+ * must not block on or fail in the driver's allocator mid-request.
+ * Same inputs as tsu_align_batch_device (device pointers), scores only, work
+ * queued on `stream` (a cudaStream_t; NULL = default stream) and finished
+ * before the call returns.  It allocates no device memory: its scratch is a
+ * fixed 32 MiB array compiled into this library, held by every GPU that
+ * loads the library until the process exits.  The first call on a device
+ * looks up that array's device address (driver work: make it before any
+ * stream capture).  All calls share the one array: calls whose GPU work
+ * overlaps race on it, so serialize them per device.  Batches needing more
+ * than the array holds (about 55,000 pairs of 1 kbp, fewer for longer
+ * pairs) return TSU_EOVERFLOW without touching the outputs; bad lengths or
+ * penalties return TSU_EINVAL. */
+int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batch* dev_batch, int32_t* dev_score, void* stream);
+
 /* ---- render ------------------------------------------------------------
  * Expand run-length CIGAR runs into WFA2's one-char-per-operation string
  * (cigar->operations), or into the compact text form ("12M1X3I...").

@@ -40,7 +40,7 @@ struct RunWriter {
 
 // Returns the number of runs, or -1 on an inconsistency (a word outside the
 // history, a predecessor beyond the current offset, more runs than cap).
-__device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
+static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
                               int s_end, int m, int n, int x, int go, int ge, uint32_t* out_end, int cap) {
   RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
   enum { M = 0, I = 1, D = 2 };

@@ -21,7 +21,7 @@ __device__ __forceinline__ uint64_t spread32(uint32_t v) {
 // load instruction of the warp touches 32 consecutive bytes.  The 2-bit code
 // of a base is (c >> 1) & 3 (A=0, C=1, T=2, G=3), a bijection on "ACGT"; any
 // other byte marks the sequence for the byte-compare path.
-__global__ void pack_kernel(SeqView sv, PackView pk) {
+static __global__ void pack_kernel(SeqView sv, PackView pk) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t nseq = 2 * sv.n;
@@ -52,7 +52,7 @@ __global__ void pack_kernel(SeqView sv, PackView pk) {
 }
 
 // words per sequence: ceil(len/32) data words + 1 padding word
-__global__ void word_count_kernel(int64_t n, const int32_t* __restrict__ pat_len, const int32_t* __restrict__ txt_len,
+static __global__ void word_count_kernel(int64_t n, const int32_t* __restrict__ pat_len, const int32_t* __restrict__ txt_len,
                                   int64_t* __restrict__ words) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += (int64_t)gridDim.x * blockDim.x) {
     const int len = j < n ? pat_len[j] : txt_len[j - n];
