@@ -273,7 +273,7 @@ def main():
         except T.AlignError as e:
             if e.code != 5:
                 raise
-            cap = int(cap * 2)
+            cap = int(e.needed) + 1024
             d_runs = torch.zeros(cap, dtype=torch.int32, device=dev)
             return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off)
 

@@ -179,6 +179,37 @@ def test_device_api(aligner_factory, oracle):
         assert T.runs_to_ops(r[c[i]:c[i + 1]]) == oops[i]
 
 
+def test_chunked_host_pipeline(aligner_factory, oracle):
+    """A batch large enough for the multi-chunk host pipeline (several chunks
+    uploaded, aligned and downloaded on three streams) gives the same scores
+    and CIGARs as the single-launch device path, and the oracle's on a sample."""
+    torch = pytest.importorskip("torch")
+    import tsunami_pact_b200 as T
+
+    n = 300_000
+    rng = np.random.default_rng(8)
+    lengths = rng.integers(60, 160, n).astype(np.int32)
+    rates = rng.uniform(0.0, 0.06, n)
+    pbuf, poff, plen, tbuf, toff, tlen = T.gen_batch(555, lengths, rates)
+    al = aligner_factory()
+    scores, coff, runs = al.align_arrays(pbuf, poff, plen, tbuf, toff, tlen)
+    dev = "cuda:0"
+    d = [torch.from_numpy(x).to(dev) for x in (pbuf, poff, plen, tbuf, toff, tlen)]
+    dsc = torch.zeros(n, dtype=torch.int32, device=dev)
+    druns = torch.zeros(int(coff[-1]) + 16, dtype=torch.int32, device=dev)
+    doff = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    nr = al.align_device(d[0], d[1], d[2], d[3], d[4], d[5], dsc, druns, doff)
+    assert np.array_equal(scores, dsc.cpu().numpy())
+    assert nr == int(coff[-1]) and np.array_equal(coff, doff.cpu().numpy())
+    assert np.array_equal(runs, druns[:nr].cpu().numpy().view(np.uint32))
+    idx = rng.choice(n, 2000, replace=False)
+    pats = [bytes(pbuf[poff[i]:poff[i] + plen[i]]) for i in idx]
+    txts = [bytes(tbuf[toff[i]:toff[i] + tlen[i]]) for i in idx]
+    osc, oops = oracle.align_batch(pats, txts)
+    for j, i in enumerate(idx):
+        assert scores[i] == osc[j] and T.runs_to_ops(runs[coff[i]:coff[i + 1]]) == oops[j]
+
+
 def test_empty_batch(aligner_factory):
     al = aligner_factory()
     s, ops = al.align([], [])

@@ -47,9 +47,10 @@ class Timing(ctypes.Structure):
 
 
 class AlignError(RuntimeError):
-    def __init__(self, code: int, msg: str):
+    def __init__(self, code: int, msg: str, needed: int = 0):
         super().__init__(f"tsunami_b200 error {code}: {msg}")
         self.code = code
+        self.needed = needed  # CIGAR runs needed, for TSU_EOVERFLOW
 
 
 def lib_path() -> str:
@@ -247,7 +248,7 @@ class Aligner:
                    pair_status.data_ptr() if pair_status is not None else None)
         rc = lib().tsu_align_batch_device(self._h, ctypes.byref(b), ctypes.byref(r), flags)
         if rc == TSU_EOVERFLOW:
-            raise AlignError(rc, f"cigar buffer too small: need {r.cigar_needed} runs")
+            raise AlignError(rc, f"cigar buffer too small: need {r.cigar_needed} runs", int(r.cigar_needed))
         self._check(rc)
         return int(r.cigar_needed)
 

@@ -62,11 +62,13 @@ struct tsu_ctx {
   DevBuf b_score, b_status, b_cpos, b_clen, b_clen64, b_coff, b_out;  // outputs
   DevBuf b_order, b_retry, b_counters;                    // queue, retry list, counters
   DevBuf b_ring, b_hist, b_table, b_arena, b_scan_tmp;    // scratch
+  DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
+  cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;  // chunk pipeline copy streams
   size_t held() const {
     const DevBuf* all[] = {&b_pat, &b_txt, &b_poff, &b_toff, &b_plen, &b_tlen, &b_words_cnt, &b_woff,
                            &b_words, &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,
                            &b_out, &b_order, &b_retry, &b_counters, &b_ring, &b_hist, &b_table, &b_arena,
-                           &b_scan_tmp};
+                           &b_scan_tmp, &b_out2};
     size_t s = 0;
     for (auto* b : all) s += b->cap;
     return s;
@@ -228,11 +230,11 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
 // Core: inputs resident on the device (sv).  Writes score/status (device)
 // and, for CIGARs, compacts runs into out_runs with offsets out_off
 // (device, n+1 entries).  *runs_needed receives the total.
-// When d_out_runs is null the runs go to the context's own b_out buffer
-// (grown to fit) and *out_used receives its address.
+// When d_out_runs is null the runs go to the context buffer *out_buf (b_out
+// unless given; grown to fit) and *out_used receives its address.
 int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d_score, int32_t* d_status,
                uint32_t* d_out_runs, int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, BatchInfo bi,
-               uint32_t** out_used = nullptr) {
+               uint32_t** out_used = nullptr, DevBuf* out_buf = nullptr) {
   const int64_t n = sv.n;
   cudaStream_t st = ctx->stream;
   int rc;
@@ -401,8 +403,9 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     CU(cudaStreamSynchronize(st));
     if (runs_needed) *runs_needed = total;
     if (!d_out_runs) {
-      if ((rc = grow(ctx, ctx->b_out, sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)))) return rc;
-      d_out_runs = P<uint32_t>(ctx->b_out);
+      DevBuf& ob = out_buf ? *out_buf : ctx->b_out;
+      if ((rc = grow(ctx, ob, sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)))) return rc;
+      d_out_runs = P<uint32_t>(ob);
       out_cap = total;
       if (out_used) *out_used = d_out_runs;
     }
@@ -518,6 +521,8 @@ int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
     return TSU_EDEVICE;
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
   *out = ctx;
   return TSU_OK;
 }
@@ -530,10 +535,12 @@ int tsu_destroy(tsu_ctx* ctx) {
                    &ctx->b_words_cnt, &ctx->b_woff, &ctx->b_words, &ctx->b_nonacgt, &ctx->b_score,
                    &ctx->b_status, &ctx->b_cpos, &ctx->b_clen, &ctx->b_clen64, &ctx->b_coff, &ctx->b_out,
                    &ctx->b_order, &ctx->b_retry, &ctx->b_counters, &ctx->b_ring, &ctx->b_hist, &ctx->b_table,
-                   &ctx->b_arena, &ctx->b_scan_tmp};
+                   &ctx->b_arena, &ctx->b_scan_tmp, &ctx->b_out2};
   for (auto* b : all) release(*b);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
   cudaStreamDestroy(ctx->stream);
+  if (ctx->h2d_stream) cudaStreamDestroy(ctx->h2d_stream);
+  if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
   delete ctx;
   return TSU_OK;
 }
@@ -556,6 +563,14 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   ctx->timing = tsu_timing{};
   const int64_t n = bi.n;
   cudaStream_t st = ctx->stream;
+  // Pipeline of K chunks of consecutive pairs on three streams: chunk c's
+  // sequence bytes go up on h2d_stream while chunk c-1 aligns on the compute
+  // stream and chunk c-2's results come down on d2h_stream.  A chunk's bytes
+  // are copied to the same offsets in the device buffers, so the offsets the
+  // caller gave stay valid; chunks of non-monotonic offsets just copy a wider
+  // (overlapping, identical) byte range.
+  const int64_t kChunkPairs = 131072;
+  const int K = (int)std::min<int64_t>(8, std::max<int64_t>(1, n / kChunkPairs));
   if ((rc = grow(ctx, ctx->b_pat, (size_t)pb))) return rc;
   if ((rc = grow(ctx, ctx->b_txt, (size_t)tb))) return rc;
   if ((rc = grow(ctx, ctx->b_poff, sizeof(int64_t) * n))) return rc;
@@ -564,54 +579,141 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   if ((rc = grow(ctx, ctx->b_tlen, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_score, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_status, sizeof(int32_t) * n))) return rc;
-  if (want_cigar && (rc = grow(ctx, ctx->b_coff, sizeof(int64_t) * (n + 1)))) return rc;
-  CU(cudaEventRecord(ctx->ev[0], st));
-  if (n) {
-    if (pb) CU(cudaMemcpyAsync(ctx->b_pat.p, b->pattern, (size_t)pb, cudaMemcpyHostToDevice, st));
-    if (tb) CU(cudaMemcpyAsync(ctx->b_txt.p, b->text, (size_t)tb, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ctx->b_poff.p, b->pattern_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ctx->b_toff.p, b->text_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ctx->b_plen.p, b->pattern_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ctx->b_tlen.p, b->text_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  if (want_cigar && (rc = grow(ctx, ctx->b_coff, sizeof(int64_t) * (n + K + 1)))) return rc;
+  std::vector<int64_t> cs((size_t)K + 1);  // chunk boundaries (pairs)
+  for (int c = 0; c <= K; ++c) cs[(size_t)c] = n * c / K;
+  std::vector<cudaEvent_t> ev_up((size_t)K), ev_done((size_t)K), ev_down((size_t)K);
+  for (int c = 0; c < K; ++c) {
+    CU(cudaEventCreateWithFlags(&ev_up[(size_t)c], cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_done[(size_t)c], cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_down[(size_t)c], cudaEventDisableTiming));
   }
-  ctx->timing.h2d_bytes = pb + tb + n * 24;
-  CU(cudaEventRecord(ctx->ev[1], st));
-  tsu::SeqView sv{n, P<uint8_t>(ctx->b_pat), P<int64_t>(ctx->b_poff), P<int32_t>(ctx->b_plen),
-                  P<uint8_t>(ctx->b_txt), P<int64_t>(ctx->b_toff), P<int32_t>(ctx->b_tlen)};
-  int64_t needed = 0;
-  uint32_t* d_runs = nullptr;  // compacted runs in the context's b_out
-  rc = run_device(ctx, sv, want_cigar, P<int32_t>(ctx->b_score), P<int32_t>(ctx->b_status), nullptr, 0,
-                  want_cigar ? P<int64_t>(ctx->b_coff) : nullptr, &needed, bi, &d_runs);
-  if (rc) return rc;
-  CU(cudaEventRecord(ctx->ev[7], st));
-  CU(cudaMemcpyAsync(res->score, ctx->b_score.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
-  std::vector<int32_t> hs((size_t)n);
-  CU(cudaMemcpyAsync(hs.data(), ctx->b_status.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
-  int64_t d2h = n * 8;
-  if (want_cigar) {
-    res->cigar_needed = needed;
-    CU(cudaMemcpyAsync(res->cigar_offset, ctx->b_coff.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st));
-    d2h += (n + 1) * 8;
-    if (needed <= res->cigar_capacity && res->cigar) {
-      if (needed) CU(cudaMemcpyAsync(res->cigar, d_runs, sizeof(uint32_t) * needed, cudaMemcpyDeviceToHost, st));
-      d2h += needed * 4;
+  struct EvGuard {
+    std::vector<cudaEvent_t>* v[3];
+    ~EvGuard() {
+      for (auto* e : v)
+        for (auto x : *e) cudaEventDestroy(x);
     }
+  } guard{{&ev_up, &ev_done, &ev_down}};
+  cudaEvent_t t_begin, t_end;
+  CU(cudaEventCreate(&t_begin));
+  CU(cudaEventCreate(&t_end));
+  struct TGuard {
+    cudaEvent_t a, b;
+    ~TGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } tguard{t_begin, t_end};
+  CU(cudaEventRecord(t_begin, ctx->h2d_stream));
+  int64_t h2d = 0;
+  if (n) {
+    CU(cudaMemcpyAsync(ctx->b_poff.p, b->pattern_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->h2d_stream));
+    CU(cudaMemcpyAsync(ctx->b_toff.p, b->text_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->h2d_stream));
+    CU(cudaMemcpyAsync(ctx->b_plen.p, b->pattern_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->h2d_stream));
+    CU(cudaMemcpyAsync(ctx->b_tlen.p, b->text_len, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->h2d_stream));
+    h2d += n * 24;
   }
-  CU(cudaStreamSynchronize(st));
+  std::vector<BatchInfo> cbi((size_t)K);
+  for (int c = 0; c < K; ++c) {
+    int64_t p0 = INT64_MAX, p1 = 0, t0 = INT64_MAX, t1 = 0;
+    BatchInfo& ci = cbi[(size_t)c];
+    ci.n = cs[(size_t)c + 1] - cs[(size_t)c];
+    for (int64_t i = cs[(size_t)c]; i < cs[(size_t)c + 1]; ++i) {
+      const int32_t m = b->pattern_len[i], t = b->text_len[i];
+      p0 = std::min(p0, b->pattern_off[i]);
+      p1 = std::max(p1, b->pattern_off[i] + m);
+      t0 = std::min(t0, b->text_off[i]);
+      t1 = std::max(t1, b->text_off[i] + t);
+      ci.max_m = std::max(ci.max_m, m);
+      ci.max_n = std::max(ci.max_n, t);
+      ci.total_words += (m + 31) / 32 + 1 + (t + 31) / 32 + 1;
+    }
+    if (p1 > p0) {
+      CU(cudaMemcpyAsync(P<char>(ctx->b_pat) + p0, b->pattern + p0, (size_t)(p1 - p0), cudaMemcpyHostToDevice,
+                         ctx->h2d_stream));
+      h2d += p1 - p0;
+    }
+    if (t1 > t0) {
+      CU(cudaMemcpyAsync(P<char>(ctx->b_txt) + t0, b->text + t0, (size_t)(t1 - t0), cudaMemcpyHostToDevice,
+                         ctx->h2d_stream));
+      h2d += t1 - t0;
+    }
+    CU(cudaEventRecord(ev_up[(size_t)c], ctx->h2d_stream));
+  }
+  ctx->timing.h2d_bytes = h2d;
+  int64_t needed = 0, d2h = 0;
+  double pack_ms = 0, align_ms = 0, compact_ms = 0;
+  int64_t launches = 0, retried = 0, cells = 0, steps = 0;
+  std::vector<int32_t> hs((size_t)n);
+  std::vector<int64_t> run_base((size_t)K + 1, 0);
+  for (int c = 0; c < K; ++c) {
+    const int64_t c0 = cs[(size_t)c], nc = cbi[(size_t)c].n;
+    DevBuf& ob = (c & 1) ? ctx->b_out2 : ctx->b_out;
+    // the output buffer is reused two chunks later: its download must be done
+    if (c >= 2) CU(cudaEventSynchronize(ev_down[(size_t)c - 2]));
+    CU(cudaStreamWaitEvent(st, ev_up[(size_t)c], 0));
+    tsu::SeqView sv{nc, P<uint8_t>(ctx->b_pat), P<int64_t>(ctx->b_poff) + c0, P<int32_t>(ctx->b_plen) + c0,
+                    P<uint8_t>(ctx->b_txt), P<int64_t>(ctx->b_toff) + c0, P<int32_t>(ctx->b_tlen) + c0};
+    int64_t* d_coff = want_cigar ? P<int64_t>(ctx->b_coff) + c0 + c : nullptr;  // nc + 1 chunk-local offsets
+    int64_t cneed = 0;
+    uint32_t* d_runs = nullptr;
+    ctx->timing.kernel_launches = 0;
+    ctx->timing.retried_pairs = 0;
+    rc = run_device(ctx, sv, want_cigar, P<int32_t>(ctx->b_score) + c0, P<int32_t>(ctx->b_status) + c0, nullptr, 0,
+                    d_coff, &cneed, cbi[(size_t)c], &d_runs, &ob);
+    if (rc) return rc;
+    if (nc) {
+      pack_ms += ev_ms(ctx->ev[2], ctx->ev[3]);
+      align_ms += ev_ms(ctx->ev[4], ctx->ev[5]);
+      if (want_cigar) compact_ms += ev_ms(ctx->ev[5], ctx->ev[6]);
+    }
+    launches += ctx->timing.kernel_launches;
+    retried += ctx->timing.retried_pairs;
+    cells += ctx->timing.cells;
+    steps += ctx->timing.steps;
+    CU(cudaEventRecord(ev_done[(size_t)c], st));
+    CU(cudaStreamWaitEvent(ctx->d2h_stream, ev_done[(size_t)c], 0));
+    if (nc) {
+      CU(cudaMemcpyAsync(res->score + c0, P<int32_t>(ctx->b_score) + c0, sizeof(int32_t) * nc,
+                         cudaMemcpyDeviceToHost, ctx->d2h_stream));
+      CU(cudaMemcpyAsync(hs.data() + c0, P<int32_t>(ctx->b_status) + c0, sizeof(int32_t) * nc,
+                         cudaMemcpyDeviceToHost, ctx->d2h_stream));
+      d2h += nc * 8;
+    }
+    if (want_cigar) {
+      // chunk-local offsets land at cigar_offset[c0 ..]; made global below
+      CU(cudaMemcpyAsync(res->cigar_offset + c0, d_coff, sizeof(int64_t) * nc, cudaMemcpyDeviceToHost,
+                         ctx->d2h_stream));
+      d2h += nc * 8;
+      run_base[(size_t)c + 1] = run_base[(size_t)c] + cneed;
+      if (res->cigar && run_base[(size_t)c + 1] <= res->cigar_capacity && cneed) {
+        CU(cudaMemcpyAsync(res->cigar + run_base[(size_t)c], d_runs, sizeof(uint32_t) * cneed,
+                           cudaMemcpyDeviceToHost, ctx->d2h_stream));
+        d2h += cneed * 4;
+      }
+      needed += cneed;
+    }
+    CU(cudaEventRecord(ev_down[(size_t)c], ctx->d2h_stream));
+  }
+  CU(cudaEventRecord(t_end, ctx->d2h_stream));
+  CU(cudaEventSynchronize(t_end));
   ctx->timing.d2h_bytes = d2h;
-  // timings
-  ctx->timing.h2d_ms = ev_ms(ctx->ev[0], ctx->ev[1]);
-  ctx->timing.pack_ms = n ? ev_ms(ctx->ev[2], ctx->ev[3]) : 0;
-  ctx->timing.align_ms = n ? ev_ms(ctx->ev[4], ctx->ev[5]) : 0;
-  ctx->timing.compact_ms = (n && want_cigar) ? ev_ms(ctx->ev[5], ctx->ev[6]) : 0;
-  {
-    cudaEvent_t e_end;
-    cudaEventCreate(&e_end);
-    cudaEventRecord(e_end, st);
-    cudaEventSynchronize(e_end);
-    ctx->timing.d2h_ms = ev_ms(ctx->ev[7], e_end);
-    ctx->timing.total_ms = ev_ms(ctx->ev[0], e_end);
-    cudaEventDestroy(e_end);
+  ctx->timing.pack_ms = pack_ms;
+  ctx->timing.align_ms = align_ms;
+  ctx->timing.compact_ms = compact_ms;
+  ctx->timing.kernel_launches = launches;
+  ctx->timing.retried_pairs = retried;
+  ctx->timing.cells = cells;
+  ctx->timing.steps = steps;
+  ctx->timing.total_ms = ev_ms(t_begin, t_end);
+  ctx->timing.h2d_ms = 0;  // overlapped with the alignment
+  ctx->timing.d2h_ms = 0;
+  if (want_cigar) {
+    for (int c = 0; c < K; ++c)
+      for (int64_t i = cs[(size_t)c]; i < cs[(size_t)c + 1]; ++i) res->cigar_offset[i] += run_base[(size_t)c];
+    res->cigar_offset[n] = needed;
+    res->cigar_needed = needed;
   }
   if (res->pair_status) memcpy(res->pair_status, hs.data(), sizeof(int32_t) * n);
   if ((rc = collect_status(ctx, hs.data(), n))) return rc;
