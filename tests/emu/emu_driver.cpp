@@ -3,10 +3,13 @@
 // emulator.  Test infrastructure: compiled by tests/test_kernel_emu.py with
 // AddressSanitizer, it checks the kernels' indexing and outputs on the CPU.
 //
-// Input (stdin):  x o e cigar hint first_mode warps_per_block N
+// Input (stdin):  x o e cigar hint first_mode first_gw N
 //                 then N records "m n\n<pattern>\n<text>\n"
+//   first_mode 1 = shared ring, 0 = global ring; first_gw = warps per pair
+//   of the first pass (1, 2, 4, 8, 16).  Retry passes follow the engine's
+//   ladder (tsu_plan.h next_pass).
 // Output (stdout): per pair "score<TAB>ops" (ops = WFA2 operation string),
-//                 then a line "passes <k> retried <r>".
+//                 then a line "passes <k> retried <r> gws <g1,g2,...>".
 #include "warp_emu.h"
 // clang-format off
 #include "../../tsunami_pact_b200/csrc/tsu_kernels.cuh"
@@ -43,11 +46,23 @@ static int gcd(int a, int b) {
   return a;
 }
 
+template <bool kCigar, int kMode>
+static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
+  switch (gw) {
+    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1>(a); }); break;
+    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2>(a); }); break;
+    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4>(a); }); break;
+    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8>(a); }); break;
+    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16>(a); }); break;
+    default: std::abort();
+  }
+}
+
 int main() {
-  int X, O, E, cigar, first_mode, wpb;
+  int X, O, E, cigar, first_mode, first_gw;
   double hint;
   int64_t N;
-  if (!(std::cin >> X >> O >> E >> cigar >> hint >> first_mode >> wpb >> N)) return 2;
+  if (!(std::cin >> X >> O >> E >> cigar >> hint >> first_mode >> first_gw >> N)) return 2;
   std::vector<std::string> pats(N), txts(N);
   for (int64_t i = 0; i < N; ++i) {
     int m, n;
@@ -63,6 +78,7 @@ int main() {
   const int g = gcd(gcd(X, O), E);
   const int x = X / g, go = (O + E) / g, ge = E / g;
   const int rm = std::max(x, go) + 1, re = ge + 1;
+  const int smem_optin = 232448;
   // sequences: exact-size buffers (pattern i, text i concatenated)
   int64_t ptot = 0, ttot = 0;
   for (auto& s : pats) ptot += (int64_t)s.size();
@@ -107,7 +123,6 @@ int main() {
   int64_t arena_cap = tsu::arena_runs(x, go, N, max_m, max_n, hint);
   Buf<uint32_t> arena(arena_cap);
   const bool want_cigar = cigar != 0;
-  bool first = first_mode != 0;
   int64_t n_order = N;
   const int32_t* ord = nullptr;
   int passes = 0;
@@ -116,12 +131,15 @@ int main() {
   unsigned* queue = reinterpret_cast<unsigned*>(counters.p);
   unsigned* retry_cnt = queue + 1;
   unsigned long long* cursor = counters.p + 2;
+  tsu::PassChoice pc{first_mode ? tsu::kModeShared : tsu::kModeGlobal, first_gw};
+  int32_t pm = max_m, pn = max_n;
+  std::string gws;
   for (;;) {
-    const tsu::PassGeom geo = tsu::plan_geometry(x, go, ge, rm, re, max_m, max_n, first, h, want_cigar, 232448, wpb);
-    const int warps = wpb;  // one block
-    Buf<int32_t> ring(geo.mode == tsu::kModeGlobal ? (size_t)warps * geo.ring_ints : 0);
-    Buf<uint32_t> hist(want_cigar ? (size_t)warps * geo.hist_cap : 0);
-    Buf<int2> table(want_cigar ? (size_t)warps * geo.table_cap : 0);
+    const tsu::PassGeom geo = tsu::plan_geometry(x, go, ge, rm, re, pm, pn, pc.mode, pc.gw, h, want_cigar, smem_optin);
+    const int groups = geo.groups_per_cta;  // one block
+    Buf<int32_t> ring(geo.mode == tsu::kModeGlobal ? (size_t)groups * geo.ring_ints : 0);
+    Buf<uint32_t> hist(want_cigar ? (size_t)groups * geo.hist_cap : 0);
+    Buf<int2> table(want_cigar ? (size_t)groups * geo.table_cap : 0);
     tsu::AlignArgs a{};
     a.seq = sv;
     a.pk = pk;
@@ -152,17 +170,19 @@ int main() {
     a.retry = retry.p;
     a.retry_count = retry_cnt;
     a.work = counters.p + 3;
-    const size_t smem = (size_t)wpb * geo.warp_smem;
+    const size_t smem = (size_t)groups * geo.group_smem;
+    const int threads = geo.cta_threads;
+    gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);
     if (want_cigar) {
       if (geo.mode == tsu::kModeShared)
-        emu::launch(1, 32 * wpb, smem, [&] { tsu::align_kernel<true, tsu::kModeShared>(a); });
+        run_gw<true, tsu::kModeShared>(geo.gw, threads, smem, a);
       else
-        emu::launch(1, 32 * wpb, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal>(a); });
+        run_gw<true, tsu::kModeGlobal>(geo.gw, threads, smem, a);
     } else {
       if (geo.mode == tsu::kModeShared)
-        emu::launch(1, 32 * wpb, smem, [&] { tsu::align_kernel<false, tsu::kModeShared>(a); });
+        run_gw<false, tsu::kModeShared>(geo.gw, threads, smem, a);
       else
-        emu::launch(1, 32 * wpb, smem, [&] { tsu::align_kernel<false, tsu::kModeGlobal>(a); });
+        run_gw<false, tsu::kModeGlobal>(geo.gw, threads, smem, a);
     }
     ++passes;
     const unsigned nretry = *retry_cnt;
@@ -172,18 +192,25 @@ int main() {
       std::fprintf(stderr, "pairs still fail after %d passes\n", passes);
       return 3;
     }
-    std::memcpy(order.p, retry.p, sizeof(int32_t) * nretry);
-    ord = order.p;
-    n_order = nretry;
-    if (!first && h >= tsu::kHintCeiling) {
+    if (geo.mode == tsu::kModeGlobal && h >= tsu::kHintCeiling) {
       std::fprintf(stderr, "pairs exceed the scratch ceiling\n");
       return 3;
     }
-    h = tsu::next_hint(h, first);
-    first = false;
+    std::vector<int32_t> rl(retry.p, retry.p + nretry);
+    pm = pn = 0;
+    for (int32_t i : rl) {
+      pm = std::max(pm, pl.p[i]);
+      pn = std::max(pn, tl.p[i]);
+    }
+    std::sort(rl.begin(), rl.end(), [&](int32_t u, int32_t v) { return pl.p[u] + tl.p[u] > pl.p[v] + tl.p[v]; });
+    std::memcpy(order.p, rl.data(), sizeof(int32_t) * nretry);
+    ord = order.p;
+    n_order = nretry;
+    h = tsu::next_hint(h, geo.mode == tsu::kModeGlobal);
+    pc = tsu::next_pass(pc, rm, re, pm, pn, smem_optin);
     if (want_cigar) {
       const unsigned long long used = *cursor;
-      const int64_t maxlen = std::max(max_m, max_n);
+      const int64_t maxlen = std::max(pm, pn);
       const int64_t need =
           (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(x, go, maxlen, h) / std::min(x, go) + 1);
       if (need > arena_cap) {
@@ -224,6 +251,6 @@ int main() {
     line += '\n';
     std::fwrite(line.data(), 1, line.size(), stdout);
   }
-  std::printf("passes %d retried %lld\n", passes, (long long)retried);
+  std::printf("passes %d retried %lld gws %s\n", passes, (long long)retried, gws.c_str());
   return 0;
 }

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -86,6 +87,25 @@ inline unsigned ballot(bool p) {
 }
 inline unsigned char* dyn_smem() { return smem_block; }
 
+// Named barriers of the block (bar.sync id, nthreads): one std::barrier per
+// (id, group of threads) -- the kernels use id = 1 + group index and the
+// group's thread count, so the key is the id alone.
+struct Named {
+  std::unique_ptr<std::barrier<>> bar[16];
+};
+inline std::unique_ptr<Named> named;
+inline void named_bar(int id, int nthreads) {
+  static std::mutex mu;
+  std::barrier<>* b;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto& slot = named->bar[id & 15];
+    if (!slot) slot.reset(new std::barrier<>(nthreads));
+    b = slot.get();
+  }
+  b->arrive_and_wait();
+}
+
 // Launch body() on blocks x threads lanes, block after block.
 template <class F>
 void launch(int blocks, int threads, size_t smem_bytes, F body) {
@@ -97,6 +117,7 @@ void launch(int blocks, int threads, size_t smem_bytes, F body) {
     smem_block = sm;
     warps.clear();
     for (int w = 0; w < threads / 32; ++w) warps.emplace_back(new Warp());
+    named.reset(new Named());
     std::vector<std::thread> th;
     for (int t = 0; t < threads; ++t)
       th.emplace_back([=] {

@@ -31,8 +31,8 @@ def emu():
     return EXE
 
 
-def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, wpb=2):
-    hdr = f"{pen[0]} {pen[1]} {pen[2]} {int(cigar)} {hint} {int(shared_first)} {wpb} {len(pairs)}\n"
+def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1):
+    hdr = f"{pen[0]} {pen[1]} {pen[2]} {int(cigar)} {hint} {int(shared_first)} {gw} {len(pairs)}\n"
     body = b"".join(f"{len(p)} {len(t)}\n".encode() + p + b"\n" + t + b"\n" for p, t in pairs)
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1")
     r = subprocess.run([exe], input=hdr.encode() + body, capture_output=True, env=env, timeout=600)
@@ -43,20 +43,36 @@ def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, 
         s, ops = ln.split("\t")
         out.append((int(s), ops))
     tail = lines[len(pairs)].split()
-    return out, int(tail[1]), int(tail[3])
+    return out, int(tail[1]), int(tail[3]), tail[5]
 
 
 def _b(s):
     return s if isinstance(s, bytes) else s.encode()
 
 
+def _edited(rng, L, rate):
+    """A random pattern and a text with about L*rate substitutions/indels."""
+    p = "".join(rng.choice("ACGT") for _ in range(L))
+    t = list(p)
+    for _ in range(int(L * rate)):
+        pos = rng.randint(0, max(0, len(t) - 1))
+        r = rng.random()
+        if r < 0.33 and t:
+            t[pos] = rng.choice("ACGT")
+        elif r < 0.66:
+            t.insert(pos, rng.choice("ACGT"))
+        elif t:
+            del t[pos]
+    return p, "".join(t)
+
+
 def check(exe, oracle, pairs, pen=(4, 6, 2), **kw):
     pairs = [(_b(p), _b(t)) for p, t in pairs]
-    got, passes, retried = run_emu(exe, pairs, pen, **kw)
+    got, passes, retried, gws = run_emu(exe, pairs, pen, **kw)
     for (p, t), (s, ops) in zip(pairs, got):
         es, eops = oracle.align(p, t, *pen)
         assert (s, ops) == (es, eops), (p, t, pen, s, es, ops, eops)
-    return passes, retried
+    return passes, retried, gws
 
 
 def test_kat_each_alone(emu, oracle, kat_cases):
@@ -74,9 +90,11 @@ def test_kat_as_batch(emu, oracle, kat_cases):
 
 
 def test_regression_fixture(emu, oracle, regress_cases):
+    """The regression set up to 1 kbp (the 3 kbp pairs run in the GPU suite)."""
     by = {}
     for c in regress_cases:
-        by.setdefault(tuple(c["pen"]), []).append((c["p"], c["t"]))
+        if len(c["p"]) <= 1000:
+            by.setdefault(tuple(c["pen"]), []).append((c["p"], c["t"]))
     for pen, pairs in by.items():
         check(emu, oracle, pairs, pen)
 
@@ -106,11 +124,11 @@ def test_global_mode_and_retries(emu, oracle):
     """A tiny hint forces scratch overflow and several global-mode passes."""
     rng = random.Random(3)
     pairs = []
-    for _ in range(12):
-        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(50, 400)))
-        t = "".join(rng.choice("ACGT") for _ in range(rng.randint(50, 400)))
+    for _ in range(5):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 160)))
+        t = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 160)))
         pairs.append((p, t))
-    passes, retried = check(emu, oracle, pairs, hint=0.0001)
+    passes, retried, gws = check(emu, oracle, pairs, hint=0.0001)
     assert passes > 1 and retried > 0
     check(emu, oracle, pairs, shared_first=False)
 
@@ -119,16 +137,52 @@ def test_wide_pairs_leave_shared_ring(emu, oracle):
     """Wavefronts wider than the shared ring (384 diagonals) are re-run in
     global mode; a batch mixing both kinds."""
     rng = random.Random(9)
-    pairs = [("".join(rng.choice("ACGT") for _ in range(300)), "".join(rng.choice("ACGT") for _ in range(300)))]
-    pairs += [("ACGT" * 10, "ACGA" * 10), ("", "A" * 500), ("C" * 450, "")]
-    passes, retried = check(emu, oracle, pairs)
-    assert retried >= 1
+    pairs = [_edited(rng, 330, 0.25)]
+    pairs += [("ACGT" * 10, "ACGA" * 10), ("", "A" * 400)]
+    passes, retried, gws = check(emu, oracle, pairs)
+    assert retried >= 1 and gws.split(",")[1] != "s1", gws
 
 
 def test_score_only(emu, oracle):
     rng = random.Random(4)
     pairs = [("".join(rng.choice("ACGT") for _ in range(rng.randint(0, 90))),
               "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 90)))) for _ in range(30)]
-    got, _, _ = run_emu(emu, [(_b(p), _b(t)) for p, t in pairs], cigar=False)
+    got, _, _, _ = run_emu(emu, [(_b(p), _b(t)) for p, t in pairs], cigar=False)
     for (p, t), (s, ops) in zip(pairs, got):
         assert s == oracle.align(p, t)[0] and ops == ""
+
+
+@pytest.mark.parametrize("gw,shared", [(2, True), (4, True), (8, True), (16, True), (2, False), (8, False)])
+def test_warp_groups(emu, oracle, gw, shared):
+    """Several warps per pair (named barriers, partial reductions combined
+    across warps), in both ring modes, with CIGARs."""
+    rng = random.Random(gw * 7 + shared)
+    pairs = []
+    for i in range(6):
+        L = rng.randint(100, 700)
+        p = "".join(rng.choice("ACGT") for _ in range(L))
+        t = list(p)
+        for _ in range(rng.randint(0, L // 8)):
+            pos = rng.randint(0, max(0, len(t) - 1))
+            r = rng.random()
+            if r < 0.33 and t:
+                t[pos] = rng.choice("ACGT")
+            elif r < 0.66:
+                t.insert(pos, rng.choice("ACGT"))
+            elif t:
+                del t[pos]
+        pairs.append((p, "".join(t)))
+    pairs += [("", "ACGTACGTAC"), ("ACGTNNACGT", "ACGTACGT"), ("A" * 64, "A" * 64)]
+    passes, retried, gws = check(emu, oracle, pairs, shared_first=shared, gw=gw)
+    assert gws.split(",")[0] == ("s" if shared else "g") + str(gw) or not shared
+
+
+def test_ladder_to_groups(emu, oracle):
+    """Pairs whose wavefronts outgrow one warp's shared ring (384 diagonals)
+    climb the ladder to a group with a wider shared ring."""
+    rng = random.Random(21)
+    pairs = [_edited(rng, 420, 0.22) for _ in range(2)]
+    pairs += [("ACGT" * 30, "ACGA" * 30)]
+    passes, retried, gws = check(emu, oracle, pairs)
+    steps = gws.split(",")
+    assert steps[0] == "s1" and steps[1].startswith("s") and int(steps[1][1:]) > 1, gws

@@ -1,17 +1,19 @@
 // tsu_align.cuh -- the persistent gap-affine WFA kernel.
 //
 // Re-design of the reference kernel wfa_dispatcher (wfa_gpu.cu:191-722):
-//   * persistent grid; each warp pulls pairs from a device work queue
-//     (the reference launched one 32-thread block per pair, wfa_gpu.cu:113);
+//   * persistent grid; each group of GW warps pulls pairs from a device work
+//     queue (the reference launched one 32-thread block per pair,
+//     wfa_gpu.cu:113).  GW = 1 for short pairs (four independent warps per
+//     block); GW = 2..16 lets one long pair use several warps;
 //   * score steps s = 0, 1, ... in units of g = gcd(x, o, e);
-//   * one fused pass per step: every lane owns diagonals k = lo + lane + 32j
-//     and computes I, D and M of score s from the ring slots of scores
-//     s - x, s - o - e and s - e (wfa_gpu.cu:610-631), nullifies an
-//     out-of-bounds M (wfa_gpu.cu:628-629), extends M along its diagonal
-//     (wfa_gpu.cu:257-287), checks the end point (wfa_gpu.cu:288-338) and,
-//     with kCigar, streams one backtrace word per (score, diagonal) to HBM;
-//     the ends of M, I and D are trimmed with warp min/max reductions
-//     (wfa_gpu.cu:636-719);
+//   * one fused pass per step: thread t of the group owns diagonals
+//     k = lo + t + 32*GW*j and computes I, D and M of score s from the ring
+//     slots of scores s - x, s - o - e and s - e (wfa_gpu.cu:610-631),
+//     nullifies an out-of-bounds M (wfa_gpu.cu:628-629), extends M along its
+//     diagonal (wfa_gpu.cu:257-287), checks the end point (wfa_gpu.cu:288-338)
+//     and, with kCigar, streams one backtrace word per (score, diagonal) to
+//     HBM; the ends of M, I and D are trimmed with warp min/max reductions
+//     combined across the group's warps (wfa_gpu.cu:636-719);
 //   * kModeShared: the ring of the last max(x, o+e)+1 scores is int16 in
 //     shared memory (offsets clamped to [null, n+1], which changes no valid
 //     cell: validity depends only on the value and the diagonal, so a clamped
@@ -20,7 +22,13 @@
 //     in shared memory.  Pairs wider than the ring or longer than the staging
 //     area are handed back for a kModeGlobal pass (int32 ring in global
 //     memory, sequences read through the read-only cache).
-// Lane 0 walks the backtrace once the end is reached (tsu_backtrace.cuh).
+// Synchronisation of a group (GW > 1): one named barrier per step, after the
+// cell loop; warp partial reductions are double-buffered by step parity and
+// every thread writes the (identical) slot limits itself, so the next step
+// reads them without a second barrier.  Null steps, which read slot limits
+// and then overwrite one, take a barrier in between.
+// Thread 0 of the group walks the backtrace once the end is reached
+// (tsu_backtrace.cuh).
 #pragma once
 
 #include <type_traits>
@@ -31,8 +39,30 @@
 
 namespace tsu {
 
-template <bool kCigar, int kMode>
-__global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_kernel(AlignArgs a) {
+template <int GW>
+__device__ __forceinline__ void group_sync(int gid) {
+  if constexpr (GW == 1) {
+    __syncwarp();
+  } else {
+#ifdef TSU_WARP_EMU
+    emu::named_bar(1 + gid, 32 * GW);
+#else
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + gid), "r"(32 * GW) : "memory");
+#endif
+  }
+}
+
+template <int GW>
+constexpr int cta_threads() {
+  return GW <= 4 ? 128 : 32 * GW;
+}
+template <int kMode, int GW>
+constexpr int cta_min_blocks() {
+  return kMode == kModeShared ? (GW <= 4 ? 6 : (GW == 8 ? 3 : 1)) : (GW <= 4 ? 4 : (GW == 8 ? 2 : 1));
+}
+
+template <bool kCigar, int kMode, int GW>
+__global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>())) align_kernel(AlignArgs a) {
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
 #ifdef TSU_WARP_EMU
@@ -41,31 +71,45 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
   extern __shared__ __align__(16) unsigned char smem_raw[];
 #endif
   constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int wpb = blockDim.x >> 5;
-  const int64_t gwarp = (int64_t)blockIdx.x * wpb + wib;
+  constexpr int GT = 32 * GW;  // threads per group
+  const int tid = threadIdx.x;
+  const int gid = tid / GT;  // group within the block
+  const int gt = tid - gid * GT;
+  const int lane = tid & 31;
+  const int wig = gt >> 5;  // warp within the group
+  const int gpb = blockDim.x / GT;
+  const int64_t ggroup = (int64_t)blockIdx.x * gpb + gid;
   const int ns = ring_slots(a.rm, a.re);
   const int W = a.ring_w;
-  unsigned char* wsm = smem_raw + (size_t)wib * warp_smem_bytes(a.rm, a.re, W, kMode, a.seq_cap);
-  int* s_lo = reinterpret_cast<int*>(wsm);
+  unsigned char* gsm = smem_raw + (size_t)gid * group_smem_bytes(a.rm, a.re, W, kMode, a.seq_cap, GW);
+  int* s_lo = reinterpret_cast<int*>(gsm);
   int* s_hi = s_lo + ns;
   int* s_alo = s_hi + ns;
+  int* part = s_alo + ns;                  // [2][GW][8] warp partials (GW > 1)
+  int* bc = part + (GW > 1 ? 16 * GW : 0);  // broadcast words
+  unsigned char* tail = reinterpret_cast<unsigned char*>(bc + 4);
   RT* ring;
   uint32_t* sseq = nullptr;
   if constexpr (kMode == kModeShared) {
-    ring = reinterpret_cast<RT*>(wsm + 3 * ns * 4);
-    sseq = reinterpret_cast<uint32_t*>(wsm + 3 * ns * 4 + ((ns * W * 2 + 15) & ~15));
+    ring = reinterpret_cast<RT*>(tail);
+    sseq = reinterpret_cast<uint32_t*>(tail + ((ns * W * 2 + 15) & ~15));
   } else {
-    ring = reinterpret_cast<RT*>(a.ring_global + gwarp * a.ring_stride);
+    ring = reinterpret_cast<RT*>(a.ring_global + ggroup * a.ring_stride);
   }
-  uint32_t* const hist = kCigar ? a.hist + gwarp * a.hist_cap : nullptr;
-  int2* const table = kCigar ? a.table + gwarp * (int64_t)a.table_cap : nullptr;
+  uint32_t* const hist = kCigar ? a.hist + ggroup * a.hist_cap : nullptr;
+  int2* const table = kCigar ? a.table + ggroup * (int64_t)a.table_cap : nullptr;
 
   for (;;) {
-    unsigned qi = 0;
-    if (lane == 0) qi = atomicAdd(a.queue, 1u);
-    qi = __shfl_sync(FULL, qi, 0);
+    unsigned qi;
+    if constexpr (GW == 1) {
+      unsigned q = 0;
+      if (lane == 0) q = atomicAdd(a.queue, 1u);
+      qi = __shfl_sync(FULL, q, 0);
+    } else {
+      if (gt == 0) bc[0] = (int)atomicAdd(a.queue, 1u);
+      group_sync<GW>(gid);
+      qi = (unsigned)bc[0];
+    }
     if ((int64_t)qi >= a.n_order) break;
     const int64_t pair = a.order ? a.order[qi] : (int64_t)qi;
     const int m = a.seq.pat_len[pair];
@@ -94,8 +138,8 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
       const uint32_t* pws;
       const uint32_t* tws;
       if constexpr (kMode == kModeShared) {
-        for (int i = lane; i < pwn; i += 32) sseq[i] = __ldg(gpw + i);
-        for (int i = lane; i < twn; i += 32) sseq[pwn + i] = __ldg(gtw + i);
+        for (int i = gt; i < pwn; i += GT) sseq[i] = __ldg(gpw + i);
+        for (int i = gt; i < twn; i += GT) sseq[pwn + i] = __ldg(gtw + i);
         pws = sseq;
         tws = sseq + pwn;
       } else {
@@ -103,12 +147,12 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         tws = gtw;
       }
       const S P{pws}, T{tws};
-      for (int i = lane; i < ns; i += 32) {
+      for (int i = gt; i < ns; i += GT) {
         s_lo[i] = 1;
         s_hi[i] = 0;
         s_alo[i] = 0;
       }
-      __syncwarp();
+      group_sync<GW>(gid);
       auto store = [&](int idx, int32_t v) {
         if constexpr (kMode == kModeShared)
           ring[idx] = (RT)(v < 0 ? (int32_t)kNull16 : (v > n + 1 ? n + 1 : v));
@@ -117,24 +161,25 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
       };
       // ---- score 0: M[0] = {k = 0: offset 0}, extended (wfa_gpu.cu:239-242)
       {
-        int32_t o0 = 0;
-        if (lane == 0) {
+        if (gt == 0) {
           const int rem = m < n ? m : n;
-          o0 = (kMode == kModeGlobal && bytemode) ? lcp8(pb, m, 0, tb, n, 0, rem) : lcp16(P, 0, T, 0, rem);
+          const int32_t o0 =
+              (kMode == kModeGlobal && bytemode) ? lcp8(pb, m, 0, tb, n, 0, rem) : lcp16(P, 0, T, 0, rem);
           store(0, o0);
           s_lo[0] = 0;
           s_hi[0] = 0;
           s_alo[0] = 0;
+          bc[1] = o0;
           if (kCigar) {
             table[0] = make_int2(0, 0);
             hist[0] = 0u;
           }
         }
-        o0 = __shfl_sync(FULL, o0, 0);
+        group_sync<GW>(gid);
+        const int32_t o0 = bc[1];
         hbase = 1;
         n_cells = n_steps = 1;
         if (k_end == 0 && o0 >= n) s_end = 0;
-        __syncwarp();
       }
 
       int s = 0;
@@ -179,13 +224,11 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         }
         const int out_m = slm, out_i = a.rm + sli, out_d = a.rm + a.re + sli;
         if ((c_mm | c_mo | c_ie | c_de) == 0) {  // null step (wfa_gpu.cu:417-422)
-          __syncwarp();
-          if (lane == 0) {
-            s_lo[out_m] = 1; s_hi[out_m] = 0;
-            s_lo[out_i] = 1; s_hi[out_i] = 0;
-            s_lo[out_d] = 1; s_hi[out_d] = 0;
-          }
-          __syncwarp();
+          group_sync<GW>(gid);  // everyone has read the slot limits
+          s_lo[out_m] = 1; s_hi[out_m] = 0;
+          s_lo[out_i] = 1; s_hi[out_i] = 0;
+          s_lo[out_d] = 1; s_hi[out_d] = 0;
+          if constexpr (GW == 1) __syncwarp();
           continue;
         }
         int lo = INT_MAX, hi = INT_MIN;  // envelope of the sources (wfa_gpu.cu:429-439)
@@ -204,7 +247,7 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         uint32_t* hrow = kCigar ? hist + hbase - lo : nullptr;
         int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
         bool found = false;
-        for (int k = lo + lane; k <= hi; k += 32) {
+        for (int k = lo + gt; k <= hi; k += GT) {
           int j;
           j = k - 1 - lo_mo;
           const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
@@ -251,31 +294,48 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         li = __reduce_max_sync(FULL, li);
         fd = __reduce_min_sync(FULL, fd);
         ld = __reduce_max_sync(FULL, ld);
-        const bool any_found = __any_sync(FULL, found);
-        if (lane == 0) {
-          // trimmed limits (wfa_gpu.cu:636-719); no in-bounds cell (first
-          // > last, e.g. INT_MAX > INT_MIN) stores the empty range (1, 0)
+        bool any_found = __any_sync(FULL, found);
+        if constexpr (GW > 1) {
+          int* pp = part + ((s & 1) * GW + wig) * 8;
+          if (lane == 0) {
+            pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = any_found;
+          }
+          group_sync<GW>(gid);  // the step's ring writes and partials are complete
+          const int* q0 = part + (s & 1) * GW * 8;
+          any_found = false;
+          for (int w = 0; w < GW; ++w) {
+            const int* qw = q0 + w * 8;
+            fm = min(fm, qw[0]); lm = max(lm, qw[1]);
+            fi = min(fi, qw[2]); li = max(li, qw[3]);
+            fd = min(fd, qw[4]); ld = max(ld, qw[5]);
+            any_found |= qw[6] != 0;
+          }
+        }
+        {
+          // trimmed limits (wfa_gpu.cu:636-719), written by every thread
+          // (identical values); no in-bounds cell (first > last) stores the
+          // empty range (1, 0)
           const bool em = fm > lm, ei = !i_present || fi > li, ed = !d_present || fd > ld;
           s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
           s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
           s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
-          if (kCigar) table[s] = make_int2(lo, (int)hbase);
+          if (kCigar && gt == 0) table[s] = make_int2(lo, (int)hbase);
         }
         hbase += width;
         n_cells += (unsigned long long)width;
         ++n_steps;
-        __syncwarp();
+        if constexpr (GW == 1) __syncwarp();
         if (any_found) s_end = s;
       }
     }
 
     if (st == kPairOk) {
-      if (lane == 0) a.score[pair] = s_end * a.g;
+      if (gt == 0) a.score[pair] = s_end * a.g;
       if (kCigar) {
         // reserve the run bound 2*s/min_pen + 1 in the arena, then walk
         const int min_pen = min(a.x, a.go);
         const int64_t bound = 2 * (int64_t)s_end / min_pen + 1;
-        if (lane == 0) {
+        if (gt == 0) {
           int32_t len = 0;
           int64_t pos = 0;
           const unsigned long long at = atomicAdd(a.arena_cursor, (unsigned long long)bound);
@@ -294,10 +354,9 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
           a.cig_pos[pair] = pos;
           a.cig_len[pair] = len;
         }
-        st = __shfl_sync(FULL, st, 0);
       }
     }
-    if (lane == 0) {
+    if (gt == 0) {
       a.status[pair] = st;
       if (st == kPairScratch || st == kPairArena) {
         const unsigned r = atomicAdd(a.retry_count, 1u);
@@ -308,7 +367,7 @@ __global__ void __launch_bounds__(128, (kMode == kModeShared) ? 6 : 4) align_ker
         atomicAdd(a.work + 1, n_steps);
       }
     }
-    __syncwarp();
+    group_sync<GW>(gid);  // the group's shared memory is free for the next pair
   }
 }
 

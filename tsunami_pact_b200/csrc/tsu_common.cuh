@@ -68,12 +68,13 @@ struct AlignArgs {
 
 __host__ __device__ inline int ring_slots(int rm, int re) { return rm + 2 * re; }
 
-// Shared memory per warp in bytes: slot metadata (lo, hi, alo per slot),
-// then in shared mode an int16 ring of ring_slots * ring_w and seq_cap
-// sequence words.
-__host__ __device__ inline int warp_smem_bytes(int rm, int re, int ring_w, int mode, int seq_cap) {
+// Shared memory per group of gw warps, in bytes: slot limits (lo, hi, alo
+// per slot), warp partials [2][gw][8] (gw > 1), 4 broadcast words, then in
+// shared mode an int16 ring of ring_slots * ring_w and seq_cap sequence
+// words.
+__host__ __device__ inline int group_smem_bytes(int rm, int re, int ring_w, int mode, int seq_cap, int gw) {
   const int ns = ring_slots(rm, re);
-  int b = 3 * ns * 4;
+  int b = 3 * ns * 4 + (gw > 1 ? 16 * gw * 4 : 0) + 16;
   if (mode == kModeShared) {
     b += ((ns * ring_w * 2 + 15) & ~15) + seq_cap * 4;
   }

@@ -31,14 +31,10 @@ struct DevBuf {
 };
 
 struct Pass {
-  int mode = 0;  // tsu::kModeShared / kModeGlobal
-  int ring_w = 0;
-  int seq_cap = 0;
-  int64_t warps = 0;
+  tsu::PassGeom g;
+  int64_t groups = 0;  // pairs in flight (groups of g.gw warps)
   int blocks = 0;
-  int wpb = 4;  // warps per block
-  int64_t hist_cap = 0;
-  int table_cap = 0;
+  int threads = 0;     // per block
   size_t smem_bytes = 0;
 };
 
@@ -150,54 +146,75 @@ struct BatchInfo {
   int64_t total_words = 0;
 };
 
-// The four align_kernel instantiations: CIGAR or score only, shared or
-// global wavefront ring.
-template <bool kCigar, int kMode>
+// The align_kernel instantiations: CIGAR or score only, shared or global
+// wavefront ring, 1/2/4/8/16 warps per pair.
+template <bool kCigar, int kMode, int GW>
 cudaError_t occ_one(int threads, size_t smem, int* occ) {
-  cudaError_t e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode, GW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode>, threads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode, GW>, threads, smem);
 }
 
-cudaError_t align_occupancy(bool cigar, int mode, int threads, size_t smem, int* occ) {
-  if (cigar) return mode == tsu::kModeShared ? occ_one<true, tsu::kModeShared>(threads, smem, occ)
-                                             : occ_one<true, tsu::kModeGlobal>(threads, smem, occ);
-  return mode == tsu::kModeShared ? occ_one<false, tsu::kModeShared>(threads, smem, occ)
-                                  : occ_one<false, tsu::kModeGlobal>(threads, smem, occ);
-}
-
-void launch_align(bool cigar, int mode, int blocks, int threads, size_t smem, cudaStream_t st,
-                  const tsu::AlignArgs& a) {
-  if (cigar) {
-    if (mode == tsu::kModeShared)
-      tsu::align_kernel<true, tsu::kModeShared><<<blocks, threads, smem, st>>>(a);
-    else
-      tsu::align_kernel<true, tsu::kModeGlobal><<<blocks, threads, smem, st>>>(a);
-  } else {
-    if (mode == tsu::kModeShared)
-      tsu::align_kernel<false, tsu::kModeShared><<<blocks, threads, smem, st>>>(a);
-    else
-      tsu::align_kernel<false, tsu::kModeGlobal><<<blocks, threads, smem, st>>>(a);
+template <bool kCigar, int kMode>
+cudaError_t occ_gw(int gw, int threads, size_t smem, int* occ) {
+  switch (gw) {
+    case 1: return occ_one<kCigar, kMode, 1>(threads, smem, occ);
+    case 2: return occ_one<kCigar, kMode, 2>(threads, smem, occ);
+    case 4: return occ_one<kCigar, kMode, 4>(threads, smem, occ);
+    case 8: return occ_one<kCigar, kMode, 8>(threads, smem, occ);
+    case 16: return occ_one<kCigar, kMode, 16>(threads, smem, occ);
+    default: return cudaErrorInvalidValue;
   }
 }
 
-// Configure a pass.  first: shared-memory ring sized for occupancy;
-// otherwise global-memory ring wide enough for any pair of the batch.
-int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, double hint, bool want_cigar,
+cudaError_t align_occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int* occ) {
+  if (cigar) return mode == tsu::kModeShared ? occ_gw<true, tsu::kModeShared>(gw, threads, smem, occ)
+                                             : occ_gw<true, tsu::kModeGlobal>(gw, threads, smem, occ);
+  return mode == tsu::kModeShared ? occ_gw<false, tsu::kModeShared>(gw, threads, smem, occ)
+                                  : occ_gw<false, tsu::kModeGlobal>(gw, threads, smem, occ);
+}
+
+template <bool kCigar, int kMode>
+void launch_gw(int gw, int blocks, int threads, size_t smem, cudaStream_t st, const tsu::AlignArgs& a) {
+  switch (gw) {
+    case 1: tsu::align_kernel<kCigar, kMode, 1><<<blocks, threads, smem, st>>>(a); break;
+    case 2: tsu::align_kernel<kCigar, kMode, 2><<<blocks, threads, smem, st>>>(a); break;
+    case 4: tsu::align_kernel<kCigar, kMode, 4><<<blocks, threads, smem, st>>>(a); break;
+    case 8: tsu::align_kernel<kCigar, kMode, 8><<<blocks, threads, smem, st>>>(a); break;
+    case 16: tsu::align_kernel<kCigar, kMode, 16><<<blocks, threads, smem, st>>>(a); break;
+    default: break;
+  }
+}
+
+void launch_align(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
+                  const tsu::AlignArgs& a) {
+  if (cigar) {
+    if (mode == tsu::kModeShared)
+      launch_gw<true, tsu::kModeShared>(gw, blocks, threads, smem, st, a);
+    else
+      launch_gw<true, tsu::kModeGlobal>(gw, blocks, threads, smem, st, a);
+  } else {
+    if (mode == tsu::kModeShared)
+      launch_gw<false, tsu::kModeShared>(gw, blocks, threads, smem, st, a);
+    else
+      launch_gw<false, tsu::kModeGlobal>(gw, blocks, threads, smem, st, a);
+  }
+}
+
+// Configure a pass of configuration pc over pairs of at most bi's lengths:
+// geometry, then as many groups as fit the SMs, the pairs and the budget.
+int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint, bool want_cigar,
               size_t reserve_bytes, Pass* out) {
   Pass p;
-  const int wpb = 4;
-  const tsu::PassGeom g = tsu::plan_geometry(ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, bi.max_m, bi.max_n, first,
-                                             hint, want_cigar, ctx->smem_optin, wpb);
-  p.mode = g.mode;
-  p.ring_w = g.ring_w;
-  p.seq_cap = g.seq_cap;
-  p.smem_bytes = (size_t)wpb * g.warp_smem;
+  const tsu::PassGeom g = tsu::plan_geometry(ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, bi.max_m, bi.max_n, pc.mode,
+                                             pc.gw, hint, want_cigar, ctx->smem_optin);
+  p.g = g;
+  const int gpc = g.groups_per_cta;
   int occ = 0;
-  cudaError_t e = align_occupancy(want_cigar, p.mode, wpb * 32, p.smem_bytes, &occ);
+  cudaError_t e = align_occupancy(want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, &occ);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
-  int64_t warps = (int64_t)ctx->sms * occ * wpb;
+  int64_t warps = (int64_t)ctx->sms * occ * gpc;  // groups
   const int64_t table_cap = g.table_cap;
   const int64_t hist_cap = g.hist_cap;
   const int64_t ring_ints = g.ring_ints;
@@ -212,17 +229,18 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
     if (w2 < 1) return set_err(ctx, TSU_ENOMEM, "scratch for one pair (%zu B) exceeds the budget", per_warp(hist_cap));
     warps = w2;
   }
-  if (warps >= wpb) {
-    warps = warps / wpb * wpb;
-    p.wpb = wpb;
+  int gpb = gpc;  // groups per block
+  if (warps >= gpc) {
+    warps = warps / gpc * gpc;
   } else {
-    p.wpb = (int)warps;  // a single block of fewer warps
+    gpb = (int)warps;  // a single block of fewer groups
   }
-  p.warps = warps;
-  p.blocks = (int)(warps / p.wpb);
-  p.smem_bytes = (size_t)p.wpb * g.warp_smem;
-  p.hist_cap = hist_cap;
-  p.table_cap = (int)table_cap;
+  p.groups = warps;
+  p.blocks = (int)(warps / gpb);
+  p.threads = 32 * g.gw * gpb;
+  p.smem_bytes = (size_t)gpb * g.group_smem;
+  (void)hist_cap;
+  (void)table_cap;
   *out = p;
   return TSU_OK;
 }
@@ -232,9 +250,11 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, bool first, do
 // (device, n+1 entries).  *runs_needed receives the total.
 // When d_out_runs is null the runs go to the context buffer *out_buf (b_out
 // unless given; grown to fit) and *out_used receives its address.
+// h_plen/h_tlen: the same lengths in host memory (used to plan retry passes).
 int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d_score, int32_t* d_status,
                uint32_t* d_out_runs, int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, BatchInfo bi,
-               uint32_t** out_used = nullptr, DevBuf* out_buf = nullptr) {
+               const int32_t* h_plen, const int32_t* h_tlen, uint32_t** out_used = nullptr,
+               DevBuf* out_buf = nullptr) {
   const int64_t n = sv.n;
   cudaStream_t st = ctx->stream;
   int rc;
@@ -289,21 +309,23 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
 
   // ---- passes
   double hint = ctx->err_hint;
-  bool first = true;
   int64_t n_order = n;
   const int32_t* order = nullptr;
   int passes = 0;
   CU(cudaEventRecord(ctx->ev[4], st));
+  tsu::PassChoice pc{tsu::kModeShared, 1};
+  BatchInfo pbi = bi;  // lengths of the pairs of the current pass
+  std::vector<int32_t> rlist;
   for (;;) {
     Pass ps;
-    if ((rc = plan_pass(ctx, bi, n_order, first, hint, want_cigar, 0, &ps))) return rc;
-    if (ps.mode == tsu::kModeGlobal) {
-      if ((rc = grow(ctx, ctx->b_ring, sizeof(int32_t) * (size_t)ps.warps * tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w)))
-        return rc;
+    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, 0, &ps))) return rc;
+    const tsu::PassGeom& g = ps.g;
+    if (g.mode == tsu::kModeGlobal) {
+      if ((rc = grow(ctx, ctx->b_ring, sizeof(int32_t) * (size_t)ps.groups * g.ring_ints))) return rc;
     }
     if (want_cigar) {
-      if ((rc = grow(ctx, ctx->b_hist, sizeof(uint32_t) * (size_t)ps.warps * ps.hist_cap))) return rc;
-      if ((rc = grow(ctx, ctx->b_table, sizeof(int2) * (size_t)ps.warps * ps.table_cap))) return rc;
+      if ((rc = grow(ctx, ctx->b_hist, sizeof(uint32_t) * (size_t)ps.groups * g.hist_cap))) return rc;
+      if ((rc = grow(ctx, ctx->b_table, sizeof(int2) * (size_t)ps.groups * g.table_cap))) return rc;
     }
     tsu::AlignArgs a{};
     a.seq = sv;
@@ -316,14 +338,14 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.g = ctx->g;
     a.rm = ctx->rm;
     a.re = ctx->re;
-    a.ring_w = ps.ring_w;
-    a.seq_cap = ps.seq_cap;
-    a.ring_global = ps.mode == tsu::kModeShared ? nullptr : P<int32_t>(ctx->b_ring);
-    a.ring_stride = (int64_t)tsu::ring_slots(ctx->rm, ctx->re) * ps.ring_w;
+    a.ring_w = g.ring_w;
+    a.seq_cap = g.seq_cap;
+    a.ring_global = g.mode == tsu::kModeShared ? nullptr : P<int32_t>(ctx->b_ring);
+    a.ring_stride = g.ring_ints;
     a.hist = want_cigar ? P<uint32_t>(ctx->b_hist) : nullptr;
-    a.hist_cap = ps.hist_cap;
+    a.hist_cap = g.hist_cap;
     a.table = want_cigar ? P<int2>(ctx->b_table) : nullptr;
-    a.table_cap = ps.table_cap;
+    a.table_cap = g.table_cap;
     a.score = d_score;
     a.status = d_status;
     a.arena = want_cigar ? P<uint32_t>(ctx->b_arena) : nullptr;
@@ -335,7 +357,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.retry = P<int32_t>(ctx->b_retry);
     a.retry_count = d_retry_cnt;
     a.work = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 24);
-    launch_align(want_cigar, ps.mode, ps.blocks, 32 * ps.wpb, ps.smem_bytes, st, a);
+    launch_align(want_cigar, g.mode, g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
     ctx->timing.kernel_launches++;
     CU(cudaGetLastError());
     ++passes;
@@ -345,20 +367,31 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     if (nretry == 0) break;
     ctx->timing.retried_pairs += nretry;
     if (passes > 16) return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes", passes);
-    // the retry list becomes the next pass's order; arena overflow grows it
-    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry,
-                       cudaMemcpyDeviceToDevice, st));
+    if (g.mode == tsu::kModeGlobal && hint >= tsu::kHintCeiling)
+      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget", nretry);
+    // The retry list, longest pairs first, becomes the next pass's order; its
+    // lengths pick the next rung of the ladder.  Global passes grow the hint.
+    rlist.resize(nretry);
+    CU(cudaMemcpyAsync(rlist.data(), P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    pbi = BatchInfo{};
+    pbi.n = nretry;
+    for (int32_t i : rlist) {
+      pbi.max_m = std::max(pbi.max_m, h_plen[i]);
+      pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
+    }
+    std::sort(rlist.begin(), rlist.end(),
+              [&](int32_t u, int32_t v) { return (int64_t)h_plen[u] + h_tlen[u] > (int64_t)h_plen[v] + h_tlen[v]; });
+    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), rlist.data(), sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
     order = P<int32_t>(ctx->b_order);
     n_order = nretry;
-    if (!first && hint >= tsu::kHintCeiling)
-      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one warp can hold within the budget", nretry);
-    hint = tsu::next_hint(hint, first);
-    first = false;
+    hint = tsu::next_hint(hint, g.mode == tsu::kModeGlobal);
+    pc = tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
     if (want_cigar) {
       unsigned long long used = 0;
       CU(cudaMemcpyAsync(&used, d_cursor, sizeof used, cudaMemcpyDeviceToHost, st));
       CU(cudaStreamSynchronize(st));
-      const int64_t maxlen = std::max(bi.max_m, bi.max_n);
+      const int64_t maxlen = std::max(pbi.max_m, pbi.max_n);
       const int64_t need = (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
       if (need > arena_cap) {
         // keep the runs written so far: grow by copy
@@ -661,7 +694,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
     ctx->timing.kernel_launches = 0;
     ctx->timing.retried_pairs = 0;
     rc = run_device(ctx, sv, want_cigar, P<int32_t>(ctx->b_score) + c0, P<int32_t>(ctx->b_status) + c0, nullptr, 0,
-                    d_coff, &cneed, cbi[(size_t)c], &d_runs, &ob);
+                    d_coff, &cneed, cbi[(size_t)c], b->pattern_len + c0, b->text_len + c0, &d_runs, &ob);
     if (rc) return rc;
     if (nc) {
       pack_ms += ev_ms(ctx->ev[2], ctx->ev[3]);
@@ -750,8 +783,8 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
   // batch info: lengths are on the device; bring them over once.
   BatchInfo bi;
   bi.n = n;
+  std::vector<int32_t> pl((size_t)n), tl((size_t)n);
   {
-    std::vector<int32_t> pl((size_t)n), tl((size_t)n);
     if (n) {
       CU(cudaMemcpyAsync(pl.data(), b->pattern_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
       CU(cudaMemcpyAsync(tl.data(), b->text_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
@@ -777,7 +810,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
   }
   int64_t needed = 0;
   int rc = run_device(ctx, sv, want_cigar, res->score, d_status, res->cigar, res->cigar_capacity, res->cigar_offset,
-                      &needed, bi);
+                      &needed, bi, pl.data(), tl.data());
   res->cigar_needed = needed;
   if (rc) return rc;
   CU(cudaEventRecord(ctx->ev[7], st));

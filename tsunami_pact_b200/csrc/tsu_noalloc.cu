@@ -110,9 +110,9 @@ int gcd(int a, int b) {
 template <int kMode>
 cudaError_t occupancy(int threads, size_t smem, int* occ) {
   cudaError_t e =
-      cudaFuncSetAttribute(tsu::align_kernel<false, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(tsu::align_kernel<false, kMode, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<false, kMode>, threads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<false, kMode, 1>, threads, smem);
 }
 
 }  // namespace
@@ -204,11 +204,12 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
   int64_t n_order = n;
   for (int pass = 0; pass < 2; ++pass) {
     const int wpb = 4;
-    const tsu::PassGeom geo =
-        tsu::plan_geometry(x, go, ge, rm, re, max_m, max_n, pass == 0, 0.2, false, smem_optin, wpb);
+    const tsu::PassGeom geo = tsu::plan_geometry(x, go, ge, rm, re, max_m, max_n,
+                                                 pass == 0 ? tsu::kModeShared : tsu::kModeGlobal, 1, 0.2, false,
+                                                 smem_optin);
     int occ = 0;
-    NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.warp_smem, &occ)
-                                       : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.warp_smem, &occ));
+    NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.group_smem, &occ)
+                                       : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.group_smem, &occ));
     if (occ < 1) return TSU_EDEVICE;
     int64_t warps = std::min<int64_t>((int64_t)sms * occ * wpb, n_order);
     if (geo.mode == tsu::kModeGlobal)
@@ -237,11 +238,11 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
     a.retry = retry;
     a.retry_count = queue + 1;
     NA_CU(cudaMemsetAsync(queue, 0, 2 * sizeof(unsigned int), st));
-    const size_t smem = (size_t)bw * geo.warp_smem;
+    const size_t smem = (size_t)bw * geo.group_smem;
     if (geo.mode == tsu::kModeShared)
-      tsu::align_kernel<false, tsu::kModeShared><<<(int)(warps / bw), 32 * bw, smem, st>>>(a);
+      tsu::align_kernel<false, tsu::kModeShared, 1><<<(int)(warps / bw), 32 * bw, smem, st>>>(a);
     else
-      tsu::align_kernel<false, tsu::kModeGlobal><<<(int)(warps / bw), 32 * bw, smem, st>>>(a);
+      tsu::align_kernel<false, tsu::kModeGlobal, 1><<<(int)(warps / bw), 32 * bw, smem, st>>>(a);
     NA_CU(cudaGetLastError());
     unsigned int nretry = 0;
     NA_CU(cudaMemcpyAsync(&nretry, queue + 1, sizeof nretry, cudaMemcpyDeviceToHost, st));

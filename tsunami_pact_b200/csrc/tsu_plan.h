@@ -1,8 +1,9 @@
 // tsu_plan.h -- pass geometry of the align kernel (host only, no CUDA).
 //
-// Shared by the engine (tsu_engine.cu) and the CPU warp emulation used by the
-// tests, so both run the kernel with the same ring width, staging size and
-// scratch capacities.
+// Shared by the engine (tsu_engine.cu), the no-allocation entry point
+// (tsu_noalloc.cu) and the CPU warp emulation used by the tests, so all run
+// the kernel with the same group size, ring width, staging size and scratch
+// capacities.
 #pragma once
 
 #include <algorithm>
@@ -14,50 +15,74 @@ namespace tsu {
 
 struct PassGeom {
   int mode = kModeShared;
+  int gw = 1;              // warps per pair
+  int cta_threads = 128;   // threads per block
+  int groups_per_cta = 4;  // pairs in flight per block
+  int min_blocks = 6;      // blocks per SM the kernel is compiled for
   int ring_w = 0;          // diagonals per ring slot
-  int seq_cap = 0;         // staged sequence words per warp (shared mode)
-  int64_t hist_cap = 0;    // backtrace words per warp
-  int table_cap = 0;       // step-table entries per warp
-  int warp_smem = 0;       // dynamic shared memory per warp (bytes)
-  int64_t ring_ints = 0;   // global ring int32 per warp (global mode)
+  int seq_cap = 0;         // staged sequence words per group (shared mode)
+  int64_t hist_cap = 0;    // backtrace words per group
+  int table_cap = 0;       // step-table entries per group
+  int group_smem = 0;      // dynamic shared memory per group (bytes)
+  int64_t ring_ints = 0;   // global ring int32 per group (global mode)
 };
 
-constexpr int kSharedW = 384;          // shared-mode ring width (diagonals)
-constexpr int kSharedSeqWords = 544;   // shared-mode staging area (uint32 words)
+constexpr int kSharedW1 = 384;         // shared-mode ring width for one warp per pair (diagonals)
+constexpr int kSharedSeqWords1 = 544;  // staging area for one warp per pair (uint32 words)
+constexpr int kSharedSeqWordsN = 4096; // staging area for a group of warps
 constexpr int kSharedMaxLen = 32000;   // int16 ring limit
+constexpr int kSmemPerSM = 228 * 1024; // B200 shared memory per SM (bytes)
 
 // Reduced-unit score expected at edit rate `hint` for a pair of length L.
 inline int64_t hint_score(int x, int go, int64_t L, double hint) {
   return (int64_t)(hint * (double)L * (double)std::max(x, go)) + 16;
 }
 
-// first: shared-mode pass (int16 ring + staged sequences) when the batch
-// allows it; otherwise a global-mode pass wide enough for any pair.
-inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max_m, int32_t max_n, bool first,
-                              double hint, bool want_cigar, int smem_optin, int warps_per_block) {
+inline int cta_threads_for(int gw) { return gw <= 4 ? 128 : 32 * gw; }
+inline int min_blocks_for(int mode, int gw) {
+  return mode == kModeShared ? (gw <= 4 ? 6 : (gw == 8 ? 3 : 1)) : (gw <= 4 ? 4 : (gw == 8 ? 2 : 1));
+}
+
+// Ring width a shared-mode group of gw warps can hold with seq_cap staged
+// words, at the block count the kernel is compiled for.
+inline int shared_ring_width(int rm, int re, int gw, int seq_cap, int smem_optin) {
+  const int ns = ring_slots(rm, re);
+  const int blocks = min_blocks_for(kModeShared, gw);
+  const int per_cta = std::min(smem_optin, kSmemPerSM / blocks - 1024);
+  const int gpc = cta_threads_for(gw) / (32 * gw);
+  const int per_group = per_cta / gpc;
+  const int fixed = group_smem_bytes(rm, re, 0, kModeShared, seq_cap, gw) + 16;
+  const int w = (per_group - fixed) / (2 * ns);
+  return std::max(0, w & ~15);
+}
+
+// mode/gw: the configuration of this pass.  Shared mode needs lengths within
+// the int16 ring; otherwise the pass falls back to the global ring.
+inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max_m, int32_t max_n, int mode, int gw,
+                              double hint, bool want_cigar, int smem_optin) {
   PassGeom p;
   const int ns = ring_slots(rm, re);
   const int64_t maxlen = std::max(max_m, max_n);
   const int64_t s_hint = hint_score(x, go, maxlen, hint);
   const int64_t full_w = (int64_t)max_m + max_n + 3;
   const int64_t width_hint = std::min<int64_t>(full_w, 2 * s_hint / ge + 3);
-  if (first && maxlen <= kSharedMaxLen) {
-    p.mode = kModeShared;
-    p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, kSharedW) + 15) & ~15);
+  p.gw = gw;
+  p.cta_threads = cta_threads_for(gw);
+  p.groups_per_cta = p.cta_threads / (32 * gw);
+  p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen) ? kModeShared : kModeGlobal;
+  if (p.mode == kModeShared) {
     const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
-    p.seq_cap = (int)std::min<int64_t>(seqw, kSharedSeqWords);
-  } else {
-    p.mode = kModeGlobal;
+    p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
+    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(rm, re, gw, p.seq_cap, smem_optin);
+    p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, cap) + 15) & ~15);
+    if (cap < 64) p.mode = kModeGlobal;
+  }
+  if (p.mode == kModeGlobal) {
     p.ring_w = (int)full_w;
     p.seq_cap = 0;
   }
-  p.warp_smem = warp_smem_bytes(rm, re, p.ring_w, p.mode, p.seq_cap);
-  if ((int64_t)p.warp_smem * warps_per_block > smem_optin) {
-    p.mode = kModeGlobal;
-    p.ring_w = (int)full_w;
-    p.seq_cap = 0;
-    p.warp_smem = warp_smem_bytes(rm, re, p.ring_w, p.mode, 0);
-  }
+  p.min_blocks = min_blocks_for(p.mode, gw);
+  p.group_smem = group_smem_bytes(rm, re, p.ring_w, p.mode, p.seq_cap, gw);
   // Backtrace words up to score s: sum_j (2j/ge + 1) ~= s^2/ge + 2s.
   p.table_cap = want_cigar ? (int)std::min<int64_t>(s_hint + 1, INT32_MAX / 2) : 0;
   if (want_cigar) {
@@ -68,16 +93,36 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
   return p;
 }
 
-// Edit-rate hint of the next retry pass.  The first retry keeps the hint
-// (the first pass may have failed on ring width or staging alone); later
-// ones grow it 4x up to kHintCeiling, at which the step table and the
-// history cover the score bound of every pair (s_max <= max(x, o+e) *
-// maxlen + o+e < s_hint), so a pass there can fail only on memory.
-constexpr double kHintCeiling = 2.0;
-inline double next_hint(double hint, bool first_retry) {
-  if (first_retry) return hint;
-  return std::min(hint * 4.0, kHintCeiling);
+// Retry ladder: the configuration of the pass after `prev` for pairs of at
+// most max_m x max_n that outgrew it.  The smallest group whose shared ring
+// holds the widest possible wavefront (m + n + 3 diagonals, so it cannot
+// overflow), else the largest shared group, then the global ring with 8
+// warps per pair.
+struct PassChoice {
+  int mode, gw;
+};
+inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int32_t max_n, int smem_optin) {
+  const int64_t need_w = (int64_t)max_m + max_n + 3;
+  if (prev.mode == kModeShared && std::max(max_m, max_n) <= kSharedMaxLen) {
+    const int64_t seqw =
+        std::min<int64_t>(2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1), kSharedSeqWordsN);
+    static const int kGW[] = {2, 4, 8, 16};
+    for (int gw : kGW) {
+      if (gw <= prev.gw) continue;
+      if (shared_ring_width(rm, re, gw, (int)seqw, smem_optin) >= need_w) return {kModeShared, gw};
+    }
+    if (prev.gw < 16) return {kModeShared, 16};
+  }
+  return {kModeGlobal, 8};
 }
+
+// Edit-rate hint of the next retry pass.  Shared-ring passes keep the hint
+// (they fail on ring width, staging or history); from the second global pass
+// on it grows 4x up to kHintCeiling, at which the step table and the history
+// cover the score bound of every pair (s_max <= max(x, o+e) * maxlen + o+e <
+// s_hint), so a pass there can fail only on memory.
+constexpr double kHintCeiling = 2.0;
+inline double next_hint(double hint, bool grow) { return grow ? std::min(hint * 4.0, kHintCeiling) : hint; }
 
 // CIGAR arena runs for a batch: 2*s/min(x, go) + 1 per pair at the hint.
 inline int64_t arena_runs(int x, int go, int64_t n, int32_t max_m, int32_t max_n, double hint) {
