@@ -34,10 +34,11 @@ sys.path.insert(0, ROOT)
 SEED = 0x5453554E414D49
 METRIC = "GCUPS & pairs/s on 1 B200 vs plain launch; serving p50/p99 latency; bit-exact"
 WORKLOADS = {
-    # name: (pairs, length, edit rate, seed index)
-    "c1": (10_000, 150, 0.02, 0),
-    "c2": (1_000_000, 1_000, 0.05, 1),
-    "c3": (20_000, 10_000, 0.15, 2),
+    # name: [pairs per GPU, description]  (shapes: tsunami_pact_b200/datasets.py)
+    "c1": [10_000, "150 bp, 2% edits"],
+    "c2": [1_000_000, "1,000 bp, 5% edits"],
+    "c3": [20_000, "10,000 bp, 15% edits"],
+    "c4": [200_000, "lengths log-uniform 100-20,000 bp, edits uniform 1-15% per pair"],
 }
 PEN = (4, 6, 2)
 
@@ -50,13 +51,11 @@ def dist_env():
 
 
 def make_batch(workload: str, rank: int):
-    import tsunami_pact_b200 as T
+    from tsunami_pact_b200 import datasets
 
-    n, L, rate, si = WORKLOADS[workload]
-    lengths = np.full(n, L, np.int32)
-    rates = np.full(n, rate)
+    n = WORKLOADS[workload][0]
     # each rank gets its own pairs: indices [rank*n, (rank+1)*n)
-    return T.gen_batch(SEED + si, lengths, rates, first=rank * n)
+    return datasets.generate(workload, n, first=rank * n)
 
 
 class ClockSampler:
@@ -163,19 +162,18 @@ def run_reference(args, workload):
         return
     from oracle import oracle as O
 
-    n_all, L, rate, si = WORKLOADS[workload]
-    cores = os.cpu_count() or 1
-    import tsunami_pact_b200 as T
+    from tsunami_pact_b200 import datasets
 
+    n_all, desc = WORKLOADS[workload]
+    cores = os.cpu_count() or 1
     # a bounded sample of the same workload: sized so each step is ~5-10 s
     probe = max(256, cores * 64)
-    lengths = np.full(probe, L, np.int32)
-    pb, po, pl, tb, to, tl = T.gen_batch(SEED + si, lengths, np.full(probe, rate))
+    pb, po, pl, tb, to, tl = datasets.generate(workload, probe)
     t0 = time.perf_counter()
     O.align_batch_arrays(pb, po, pl, tb, to, tl, *PEN, cigar=True, threads=cores)
     r = probe / max(time.perf_counter() - t0, 1e-6)
     sample = int(min(n_all, max(probe, r * 6.0)))
-    pb, po, pl, tb, to, tl = T.gen_batch(SEED + si, np.full(sample, L, np.int32), np.full(sample, rate))
+    pb, po, pl, tb, to, tl = datasets.generate(workload, sample)
     cells = float(np.sum(pl.astype(np.float64) * tl))
     for _ in range(args.warmup):
         O.align_batch_arrays(pb, po[: min(sample, probe)], pl[: min(sample, probe)], tb, to[: min(sample, probe)],
@@ -192,8 +190,7 @@ def run_reference(args, workload):
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
         "impl": "reference",
-        "config": {"workload": f"{workload}: {n_all} pairs x {L} bp, {rate:.0%} edits, penalties 4/6/2",
-                   "sample_pairs": sample},
+        "config": {"workload": f"{workload}: {n_all} pairs, {desc}, penalties 4/6/2", "sample_pairs": sample},
         "pairs_per_s": sample / t,
         "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": cores, "kind": "port",
                          "sample": f"first {sample} pairs of the workload per step, scores + CIGARs, "
@@ -215,10 +212,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--pairs", type=int, default=0, help="override the pair count (small profiling cases)")
     ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
+    ap.add_argument("--plain", action="store_true", help="also time the plain one-warp-per-pair bucketed form")
     args = ap.parse_args()
     if args.pairs:
-        n, L, r, si = WORKLOADS[args.workload]
-        WORKLOADS[args.workload] = (args.pairs, L, r, si)
+        WORKLOADS[args.workload][0] = args.pairs
     workload = args.workload
     if args.impl == "reference":
         run_reference(args, workload)
@@ -250,7 +247,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    n_pairs, L, rate, si = WORKLOADS[workload]
+    n_pairs, desc = WORKLOADS[workload]
     pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
@@ -298,6 +295,47 @@ def main():
     value = cells * world / (ms / 1e3) / 1e9
     pairs_s = n_pairs * world / (ms / 1e3)
 
+    # ---- plain form (c4): one call per log2-length bucket, one warp per pair
+    plain = None
+    if workload == "c4" or args.plain:
+        from tsunami_pact_b200 import datasets
+
+        buckets = datasets.length_buckets(plen)
+        ref_scores = d_sc.cpu().numpy()
+        sub = []
+        for b in np.unique(buckets):
+            idx = np.nonzero(buckets == b)[0]
+            sub.append((int(b), len(idx), [torch.from_numpy(x[idx]).to(dev) for x in (poff, plen, toff, tlen)]))
+        p_ms, p_launch = [], 0
+        for rep in range(max(args.steps, 1) + 1):  # the first repetition warms up
+            tot = 0.0
+            for b, nb, (bo, bl, to_, tl_) in sub:
+                sc = torch.zeros(nb, dtype=torch.int32, device=dev)
+                off = torch.zeros(nb + 1, dtype=torch.int64, device=dev)
+                runs = torch.zeros(max(int(nb * 64), 1024), dtype=torch.int32, device=dev) if want_cigar else None
+                try:
+                    al.align_device(d_p, bo, bl, d_t, to_, tl_, sc, runs, off if want_cigar else None, one_warp=True)
+                except T.AlignError as e:
+                    if e.code != 5:
+                        raise
+                    runs = torch.zeros(int(e.needed) + 1024, dtype=torch.int32, device=dev)
+                    al.align_device(d_p, bo, bl, d_t, to_, tl_, sc, runs, off, one_warp=True)
+                tm = al.timing()
+                tot += tm["total_ms"]
+                if rep:
+                    p_launch += int(tm["kernel_launches"])
+                if rep == 0:  # same scores as the batched form
+                    idx = np.nonzero(buckets == b)[0]
+                    if not np.array_equal(sc.cpu().numpy(), ref_scores[idx]):
+                        raise SystemExit(f"plain form differs from the batched form in bucket {b}")
+            if rep:
+                p_ms.append(tot)
+        pm = max_over_ranks(float(np.mean(p_ms)))
+        plain = {"form": "one call per floor(log2 L) bucket, one warp per pair (TSU_ONE_WARP), in turn",
+                 "buckets": len(sub), "ms_per_step": pm, "value": cells * world / (pm / 1e3) / 1e9,
+                 "unit": "GCUPS", "pairs_per_s": n_pairs * world / (pm / 1e3),
+                 "batched_over_plain_pairs_per_s": pm / ms, "gpu_launches": p_launch}
+
     # ---- e2e: host buffers (pinned) through tsu_align_batch ---------------
     e2e = None
     if not args.no_e2e:
@@ -337,11 +375,11 @@ def main():
     # ---- roofline of the align kernel ------------------------------------
     peak, peak_kind = measured_peaks()
     a_ms = float(np.mean(align_ms))
-    words = 2 * ((L + 31) // 32 + 1)
-    per_pair_in = words * 8
-    per_pair_out = 4 + (4 * nruns / n_pairs if want_cigar else 0)
+    words = float(np.sum((plen.astype(np.int64) + 31) // 32 + 1) + np.sum((tlen.astype(np.int64) + 31) // 32 + 1))
+    packed_in = words * 8
+    out_bytes = n_pairs * 4 + (4 * nruns if want_cigar else 0)
     hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
-    algo = n_pairs * (per_pair_in + per_pair_out) + hist_bytes
+    algo = packed_in + out_bytes + hist_bytes
     achieved = algo / (a_ms / 1e3) / 1e9
     traffic = load_traffic(f"align_{workload}")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -359,13 +397,14 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
-            "config": {"workload": f"{workload}: {n_pairs} pairs x {L} bp per GPU, {rate:.0%} edits, penalties 4/6/2",
+            "config": {"workload": f"{workload}: {n_pairs} pairs per GPU, {desc}, penalties 4/6/2",
                        "output": "scores + CIGARs" if want_cigar else "scores only",
                        "l2": f"inputs larger than L2 ({(pbuf.nbytes + tbuf.nbytes) / 1e9:.1f} GB ASCII per GPU)",
                        "parallelism": f"data-parallel over pairs, {world} GPU(s)"},
             "pairs_per_s": pairs_s,
             "wall_ms_per_step": wall_ms,
             "gpu_launches": launches,
+            "plain": plain,
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,

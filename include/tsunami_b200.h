@@ -52,6 +52,10 @@ extern "C" {
 
 /* Flags for the align calls. */
 #define TSU_SCORE_ONLY 0x1u  /* skip the CIGAR (the reference kernel's work) */
+#define TSU_ONE_WARP 0x2u    /* one warp per pair in every pass, no warp groups and
+                                no longest-first order: the reference's scheduling
+                                (one 32-thread block per pair, wfa_gpu.cu:113-114),
+                                kept as the "plain" baseline of the benchmarks */
 
 typedef struct tsu_ctx tsu_ctx;
 

@@ -210,6 +210,30 @@ def test_chunked_host_pipeline(aligner_factory, oracle):
         assert scores[i] == osc[j] and T.runs_to_ops(runs[coff[i]:coff[i + 1]]) == oops[j]
 
 
+def test_one_warp_flag_same_results(aligner_factory):
+    """TSU_ONE_WARP (the plain baseline: one warp per pair in every pass, no
+    warp groups, no longest-first order) gives the same scores and CIGARs as
+    the default scheduling on a mixed batch with long pairs."""
+    torch = pytest.importorskip("torch")
+    import tsunami_pact_b200 as T
+
+    lengths = np.array([150] * 300 + [1000] * 100 + [3000] * 8 + [6000] * 2, np.int32)
+    rates = np.array([0.02] * 300 + [0.08] * 100 + [0.15] * 8 + [0.12] * 2)
+    pbuf, poff, plen, tbuf, toff, tlen = T.gen_batch(31, lengths, rates)
+    dev = "cuda:0"
+    d = [torch.from_numpy(x).to(dev) for x in (pbuf, poff, plen, tbuf, toff, tlen)]
+    al = aligner_factory()
+    outs = []
+    for one in (False, True):
+        sc = torch.zeros(len(plen), dtype=torch.int32, device=dev)
+        runs = torch.zeros(2_000_000, dtype=torch.int32, device=dev)
+        off = torch.zeros(len(plen) + 1, dtype=torch.int64, device=dev)
+        nr = al.align_device(d[0], d[1], d[2], d[3], d[4], d[5], sc, runs, off, one_warp=one)
+        outs.append((sc.cpu().numpy(), off.cpu().numpy(), runs[:nr].cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1]) and np.array_equal(outs[0][2], outs[1][2])
+
+
 def test_empty_batch(aligner_factory):
     al = aligner_factory()
     s, ops = al.align([], [])

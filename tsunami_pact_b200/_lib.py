@@ -15,6 +15,7 @@ _lib = None
 TSU_OK = 0
 TSU_EOVERFLOW = 5
 TSU_SCORE_ONLY = 0x1
+TSU_ONE_WARP = 0x2
 
 P = ctypes.POINTER
 c_i32, c_i64, c_u32, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p
@@ -235,13 +236,13 @@ class Aligner:
 
     # -- device buffers (torch CUDA tensors) --------------------------------
     def align_device(self, pat, poff, plen, txt, toff, tlen, scores, cigar_runs=None, cigar_off=None,
-                     pair_status=None) -> int:
+                     pair_status=None, one_warp: bool = False) -> int:
         """All arguments are CUDA tensors (uint8 / int64 / int32).  Returns the
         number of CIGAR runs written (0 with cigar_runs=None)."""
         n = int(plen.numel())
         b = Batch(n, pat.data_ptr(), poff.data_ptr(), plen.data_ptr(), txt.data_ptr(), toff.data_ptr(),
                   tlen.data_ptr())
-        flags = 0 if cigar_runs is not None else TSU_SCORE_ONLY
+        flags = (0 if cigar_runs is not None else TSU_SCORE_ONLY) | (TSU_ONE_WARP if one_warp else 0)
         r = Result(scores.data_ptr(), cigar_runs.data_ptr() if cigar_runs is not None else None,
                    int(cigar_runs.numel()) if cigar_runs is not None else 0,
                    cigar_off.data_ptr() if cigar_off is not None else None, 0,

@@ -59,6 +59,7 @@ struct tsu_ctx {
   DevBuf b_order, b_retry, b_counters;                    // queue, retry list, counters
   DevBuf b_ring, b_hist, b_table, b_arena, b_scan_tmp;    // scratch
   DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
+  bool one_warp = false;  // TSU_ONE_WARP of the current call
   cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;  // chunk pipeline copy streams
   size_t held() const {
     const DevBuf* all[] = {&b_pat, &b_txt, &b_poff, &b_toff, &b_plen, &b_tlen, &b_words_cnt, &b_woff,
@@ -312,6 +313,36 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   int64_t n_order = n;
   const int32_t* order = nullptr;
   int passes = 0;
+  // Longest pairs first (a counting sort by floor(log2(m + n)), stable
+  // inside a class) when lengths vary, so the pairs that take longest start
+  // first and the pass ends without a long tail; not in TSU_ONE_WARP mode.
+  std::vector<int32_t> lpt;
+  if (!ctx->one_warp && h_plen && bi.max_m + bi.max_n > 0) {
+    int64_t cnt[34] = {0};
+    auto cls = [&](int64_t i) {
+      const uint32_t l = (uint32_t)h_plen[i] + (uint32_t)h_tlen[i];
+      return l ? 32 - __builtin_clz(l) : 0;
+    };
+    int cmin = 33, cmax = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      const int c = cls(i);
+      ++cnt[c];
+      cmin = std::min(cmin, c);
+      cmax = std::max(cmax, c);
+    }
+    if (cmax > cmin) {
+      int64_t start[34];
+      int64_t acc = 0;
+      for (int c = 33; c >= 0; --c) {
+        start[c] = acc;
+        acc += cnt[c];
+      }
+      lpt.resize((size_t)n);
+      for (int64_t i = 0; i < n; ++i) lpt[(size_t)start[cls(i)]++] = (int32_t)i;
+      CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), lpt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+      order = P<int32_t>(ctx->b_order);
+    }
+  }
   CU(cudaEventRecord(ctx->ev[4], st));
   tsu::PassChoice pc{tsu::kModeShared, 1};
   BatchInfo pbi = bi;  // lengths of the pairs of the current pass
@@ -386,7 +417,8 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     order = P<int32_t>(ctx->b_order);
     n_order = nretry;
     hint = tsu::next_hint(hint, g.mode == tsu::kModeGlobal);
-    pc = tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
+    pc = ctx->one_warp ? tsu::PassChoice{tsu::kModeGlobal, 1}
+                       : tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
     if (want_cigar) {
       unsigned long long used = 0;
       CU(cudaMemcpyAsync(&used, d_cursor, sizeof used, cudaMemcpyDeviceToHost, st));
@@ -587,6 +619,7 @@ int tsu_get_timing(const tsu_ctx* ctx, tsu_timing* out) {
 int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t flags) {
   if (!ctx || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null result") : TSU_EINVAL;
   const bool want_cigar = !(flags & TSU_SCORE_ONLY);
+  ctx->one_warp = (flags & TSU_ONE_WARP) != 0;
   if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
   BatchInfo bi;
   int64_t pb = 0, tb = 0;
@@ -774,6 +807,7 @@ int tsu_align_fixed(tsu_ctx* ctx, const char* pattern, const char* text, int64_t
 int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t flags) {
   if (!ctx || !b || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null argument") : TSU_EINVAL;
   const bool want_cigar = !(flags & TSU_SCORE_ONLY);
+  ctx->one_warp = (flags & TSU_ONE_WARP) != 0;
   if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
   CU(cudaSetDevice(ctx->device));
   ctx->timing = tsu_timing{};
