@@ -345,18 +345,30 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   }
   CU(cudaEventRecord(ctx->ev[4], st));
   tsu::PassChoice pc{tsu::kModeShared, 1};
+  std::string passlog;  // mode, warps per pair x groups : pairs, per pass (for error messages)
   BatchInfo pbi = bi;  // lengths of the pairs of the current pass
   std::vector<int32_t> rlist;
   for (;;) {
     Pass ps;
     if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, 0, &ps))) return rc;
     const tsu::PassGeom& g = ps.g;
-    if (g.mode == tsu::kModeGlobal) {
-      if ((rc = grow(ctx, ctx->b_ring, sizeof(int32_t) * (size_t)ps.groups * g.ring_ints))) return rc;
-    }
-    if (want_cigar) {
-      if ((rc = grow(ctx, ctx->b_hist, sizeof(uint32_t) * (size_t)ps.groups * g.hist_cap))) return rc;
-      if ((rc = grow(ctx, ctx->b_table, sizeof(int2) * (size_t)ps.groups * g.table_cap))) return rc;
+    {
+      // plan_pass counted the scratch buffers as free: if any of them must
+      // grow, release all three first so the budget holds during regrowth
+      const size_t need_ring = g.mode == tsu::kModeGlobal ? sizeof(int32_t) * (size_t)ps.groups * g.ring_ints : 0;
+      const size_t need_hist = want_cigar ? sizeof(uint32_t) * (size_t)ps.groups * g.hist_cap : 0;
+      const size_t need_table = want_cigar ? sizeof(int2) * (size_t)ps.groups * g.table_cap : 0;
+      if (need_ring > ctx->b_ring.cap || need_hist > ctx->b_hist.cap || need_table > ctx->b_table.cap) {
+        CU(cudaStreamSynchronize(st));
+        release(ctx->b_ring);
+        release(ctx->b_hist);
+        release(ctx->b_table);
+      }
+      passlog += (passlog.empty() ? "" : " ") + std::string(g.mode == tsu::kModeShared ? "s" : "g") +
+                 std::to_string(g.gw) + "x" + std::to_string(ps.groups) + ":" + std::to_string(n_order);
+      if (need_ring && (rc = grow(ctx, ctx->b_ring, need_ring))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
+      if (need_hist && (rc = grow(ctx, ctx->b_hist, need_hist))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
+      if (need_table && (rc = grow(ctx, ctx->b_table, need_table))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
     }
     tsu::AlignArgs a{};
     a.seq = sv;
@@ -397,9 +409,11 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     CU(cudaStreamSynchronize(st));
     if (nretry == 0) break;
     ctx->timing.retried_pairs += nretry;
-    if (passes > 16) return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes", passes);
+    if (passes > 16)
+      return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes [passes %s]", passes, passlog.c_str());
     if (g.mode == tsu::kModeGlobal && hint >= tsu::kHintCeiling)
-      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget", nretry);
+      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget [passes %s]",
+                     nretry, passlog.c_str());
     // The retry list, longest pairs first, becomes the next pass's order; its
     // lengths pick the next rung of the ladder.  Global passes grow the hint.
     rlist.resize(nretry);
