@@ -213,6 +213,7 @@ def main():
     ap.add_argument("--pairs", type=int, default=0, help="override the pair count (small profiling cases)")
     ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
     ap.add_argument("--plain", action="store_true", help="also time the plain one-warp-per-pair bucketed form")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain form (c4)")
     args = ap.parse_args()
     if args.pairs:
         WORKLOADS[args.workload][0] = args.pairs
@@ -288,6 +289,7 @@ def main():
         align_ms.append(tm["align_ms"])
         launches += int(tm["kernel_launches"])
         work_cells = tm["cells"]
+        pass_log = al.pass_log()
     barrier()
     wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
     clk = clocks.stop()
@@ -297,7 +299,7 @@ def main():
 
     # ---- plain form (c4): one call per log2-length bucket, one warp per pair
     plain = None
-    if workload == "c4" or args.plain:
+    if (workload == "c4" or args.plain) and not args.no_plain:
         from tsunami_pact_b200 import datasets
 
         buckets = datasets.length_buckets(plen)
@@ -386,7 +388,7 @@ def main():
             "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
             "align_kernel<score>", "kernel_ms": a_ms,
             "algorithmic_bytes_per_launch": algo,
-            "cells_per_s": work_cells / (a_ms / 1e3)}
+            "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log}
 
     if rank == 0:
         cpu = None

@@ -122,6 +122,11 @@ int tsu_destroy(tsu_ctx* ctx);
 const char* tsu_status_str(int status);
 const char* tsu_last_error(const tsu_ctx* ctx);
 int tsu_get_timing(const tsu_ctx* ctx, tsu_timing* out);
+/* The align passes of the last call (of its last chunk), e.g.
+ * "s1x2368:200000@812.3ms s16x148:3120@4410.0ms": ring mode (s shared,
+ * g global), warps per pair x pairs in flight : pairs, device time.  No
+ * counterpart in the reference (one fixed launch, wfa_gpu.cu:118). */
+const char* tsu_pass_log(const tsu_ctx* ctx);
 
 /* ---- batch alignment, host buffers -------------------------------------
  * Replaces H2D + wfa_dispatcher launch + D2H of the reference

@@ -172,6 +172,13 @@ class Aligner:
         lib().tsu_get_timing(self._h, ctypes.byref(t))
         return {f: getattr(t, f) for f, _ in Timing._fields_}
 
+    def pass_log(self) -> str:
+        """Align passes of the last call: mode+warps per pair x groups : pairs @ time."""
+        L = lib()
+        L.tsu_pass_log.restype = ctypes.c_char_p
+        L.tsu_pass_log.argtypes = [c_vp]
+        return L.tsu_pass_log(self._h).decode()
+
     # -- host buffers ------------------------------------------------------
     def align_arrays(self, pbuf: np.ndarray, poff: np.ndarray, plen: np.ndarray, tbuf: np.ndarray,
                      toff: np.ndarray, tlen: np.ndarray, cigar: bool = True, status: bool = False,

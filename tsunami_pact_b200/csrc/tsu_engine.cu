@@ -60,6 +60,8 @@ struct tsu_ctx {
   DevBuf b_ring, b_hist, b_table, b_arena, b_scan_tmp;    // scratch
   DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
   bool one_warp = false;  // TSU_ONE_WARP of the current call
+  cudaEvent_t pev[2] = {};  // per-pass timing
+  std::string passlog;      // passes of the last align call (tsu_pass_log)
   cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;  // chunk pipeline copy streams
   size_t held() const {
     const DevBuf* all[] = {&b_pat, &b_txt, &b_poff, &b_toff, &b_plen, &b_tlen, &b_words_cnt, &b_woff,
@@ -309,45 +311,73 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   CU(cudaMemsetAsync(ctx->b_counters.p, 0, 64, st));
 
   // ---- passes
-  double hint = ctx->err_hint;
-  int64_t n_order = n;
-  const int32_t* order = nullptr;
+  // Pairs are split into length bands (tsu::length_band of max(m, n)); each
+  // band runs its own ladder of passes from the band's starting rung
+  // (tsu::band_start), with scratch sized for that band's longest pair, so
+  // short pairs run many to an SM and long ones get warp groups.  Bands run
+  // longest first; inside a band pairs are ordered longest first (a counting
+  // sort by floor(log2(m + n))).  TSU_ONE_WARP keeps one band in input order
+  // starting at one warp per pair.
   int passes = 0;
-  // Longest pairs first (a counting sort by floor(log2(m + n)), stable
-  // inside a class) when lengths vary, so the pairs that take longest start
-  // first and the pass ends without a long tail; not in TSU_ONE_WARP mode.
-  std::vector<int32_t> lpt;
-  if (!ctx->one_warp && h_plen && bi.max_m + bi.max_n > 0) {
+  std::vector<std::vector<int32_t>> bands(tsu::kBands);
+  bool uniform = true;  // every pair in one length class: one band, input order
+  int uniform_band = 0;
+  if (!ctx->one_warp && h_plen) {
     int64_t cnt[34] = {0};
     auto cls = [&](int64_t i) {
       const uint32_t l = (uint32_t)h_plen[i] + (uint32_t)h_tlen[i];
       return l ? 32 - __builtin_clz(l) : 0;
     };
-    int cmin = 33, cmax = 0;
+    int cmin = 33, cmax = 0, bmin = tsu::kBands, bmax = -1;
     for (int64_t i = 0; i < n; ++i) {
       const int c = cls(i);
       ++cnt[c];
       cmin = std::min(cmin, c);
       cmax = std::max(cmax, c);
+      const int b = tsu::length_band(std::max(h_plen[i], h_tlen[i]));
+      bmin = std::min(bmin, b);
+      bmax = std::max(bmax, b);
     }
-    if (cmax > cmin) {
+    uniform = cmin == cmax && bmin == bmax;
+    uniform_band = bmax < 0 ? 0 : bmax;
+    if (!uniform) {
+      std::vector<int32_t> by_len((size_t)n);
       int64_t start[34];
       int64_t acc = 0;
       for (int c = 33; c >= 0; --c) {
         start[c] = acc;
         acc += cnt[c];
       }
-      lpt.resize((size_t)n);
-      for (int64_t i = 0; i < n; ++i) lpt[(size_t)start[cls(i)]++] = (int32_t)i;
-      CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), lpt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-      order = P<int32_t>(ctx->b_order);
+      for (int64_t i = 0; i < n; ++i) by_len[(size_t)start[cls(i)]++] = (int32_t)i;
+      for (int32_t i : by_len) bands[(size_t)tsu::length_band(std::max(h_plen[i], h_tlen[i]))].push_back(i);
     }
   }
   CU(cudaEventRecord(ctx->ev[4], st));
-  tsu::PassChoice pc{tsu::kModeShared, 1};
   std::string passlog;  // mode, warps per pair x groups : pairs, per pass (for error messages)
-  BatchInfo pbi = bi;  // lengths of the pairs of the current pass
   std::vector<int32_t> rlist;
+  for (int band = tsu::kBands - 1; band >= 0; --band) {
+  const bool all_pairs = ctx->one_warp || !h_plen || uniform;  // a single band of every pair, input order
+  if (all_pairs && band != 0) continue;
+  if (!all_pairs && bands[(size_t)band].empty()) continue;
+  double hint = ctx->err_hint;
+  int64_t n_order = all_pairs ? n : (int64_t)bands[(size_t)band].size();
+  const int32_t* order = nullptr;
+  BatchInfo pbi = bi;  // lengths of the pairs of the current pass
+  tsu::PassChoice pc{tsu::kModeShared, 1};
+  if (all_pairs && !ctx->one_warp && h_plen) pc = tsu::band_start(uniform_band, std::max(bi.max_m, bi.max_n));
+  if (!all_pairs) {
+    const std::vector<int32_t>& bp = bands[(size_t)band];
+    pbi = BatchInfo{};
+    pbi.n = n_order;
+    for (int32_t i : bp) {
+      pbi.max_m = std::max(pbi.max_m, h_plen[i]);
+      pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
+    }
+    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), bp.data(), sizeof(int32_t) * n_order, cudaMemcpyHostToDevice, st));
+    order = P<int32_t>(ctx->b_order);
+    pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
+  }
+  CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
   for (;;) {
     Pass ps;
     if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, 0, &ps))) return rc;
@@ -400,13 +430,21 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.retry = P<int32_t>(ctx->b_retry);
     a.retry_count = d_retry_cnt;
     a.work = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 24);
+    CU(cudaEventRecord(ctx->pev[0], st));
     launch_align(want_cigar, g.mode, g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
     ctx->timing.kernel_launches++;
     CU(cudaGetLastError());
+    CU(cudaEventRecord(ctx->pev[1], st));
     ++passes;
     unsigned int nretry = 0;
     CU(cudaMemcpyAsync(&nretry, d_retry_cnt, sizeof nretry, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
+    {
+      char t[48];
+      snprintf(t, sizeof t, "@%.1fms", ev_ms(ctx->pev[0], ctx->pev[1]));
+      passlog += t;
+      ctx->passlog = passlog;
+    }
     if (nretry == 0) break;
     ctx->timing.retried_pairs += nretry;
     if (passes > 16)
@@ -456,6 +494,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     }
     CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
   }
+  }  // bands
   CU(cudaEventRecord(ctx->ev[5], st));
   {
     unsigned long long work[2] = {0, 0};
@@ -559,6 +598,8 @@ const char* tsu_status_str(int s) {
 
 const char* tsu_last_error(const tsu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+const char* tsu_pass_log(const tsu_ctx* ctx) { return ctx ? ctx->passlog.c_str() : ""; }
+
 int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
   tsu_ctx* ctx = nullptr;
   if (!pen || !out) return TSU_EINVAL;
@@ -600,6 +641,7 @@ int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
     return TSU_EDEVICE;
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  for (auto& ev : ctx->pev) cudaEventCreate(&ev);
   cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
   *out = ctx;
@@ -617,6 +659,7 @@ int tsu_destroy(tsu_ctx* ctx) {
                    &ctx->b_arena, &ctx->b_scan_tmp, &ctx->b_out2};
   for (auto* b : all) release(*b);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->pev) cudaEventDestroy(ev);
   cudaStreamDestroy(ctx->stream);
   if (ctx->h2d_stream) cudaStreamDestroy(ctx->h2d_stream);
   if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);

@@ -10,8 +10,14 @@
 #include <cstdint>
 
 #include "tsu_common.cuh"
+#include "tsu_tuning.h"
 
 namespace tsu {
+
+// A rung of the pass ladder: ring mode and warps per pair.
+struct PassChoice {
+  int mode, gw;
+};
 
 struct PassGeom {
   int mode = kModeShared;
@@ -98,9 +104,6 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
 // holds the widest possible wavefront (m + n + 3 diagonals, so it cannot
 // overflow), else the largest shared group, then the global ring with 8
 // warps per pair.
-struct PassChoice {
-  int mode, gw;
-};
 inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int32_t max_n, int smem_optin) {
   const int64_t need_w = (int64_t)max_m + max_n + 3;
   if (prev.mode == kModeShared && std::max(max_m, max_n) <= kSharedMaxLen) {
@@ -114,6 +117,25 @@ inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int3
     if (prev.gw < 16) return {kModeShared, 16};
   }
   return {kModeGlobal, 8};
+}
+
+// Length bands of the batched scheduler: max(m, n) < 1024, < 2048, < 4096,
+// < 8192, < 16384, >= 16384.  Each band starts its ladder at the rung the
+// autotuner measured fastest for it (tsu_tuning.h).
+constexpr int kBands = 6;
+inline int length_band(int32_t L) {
+  if (L < 1024) return 0;
+  if (L < 2048) return 1;
+  if (L < 4096) return 2;
+  if (L < 8192) return 3;
+  if (L < 16384) return 4;
+  return 5;
+}
+inline PassChoice band_start(int band, int32_t maxlen) {
+  static const PassChoice kStart[kBands] = TSU_BAND_START;
+  PassChoice r = kStart[band < 0 ? 0 : (band >= kBands ? kBands - 1 : band)];
+  if (r.mode == kModeShared && maxlen > kSharedMaxLen) r = {kModeGlobal, r.gw >= 8 ? r.gw : 8};
+  return r;
 }
 
 // Edit-rate hint of the next retry pass.  Shared-ring passes keep the hint
