@@ -378,6 +378,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
   }
   CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
+  const int band_first_pass = passes;
   for (;;) {
     Pass ps;
     if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, 0, &ps))) return rc;
@@ -447,7 +448,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     }
     if (nretry == 0) break;
     ctx->timing.retried_pairs += nretry;
-    if (passes > 16)
+    if (passes - band_first_pass > 24)
       return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes [passes %s]", passes, passlog.c_str());
     if (g.mode == tsu::kModeGlobal && hint >= tsu::kHintCeiling)
       return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget [passes %s]",
