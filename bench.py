@@ -155,6 +155,92 @@ def cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen, target_s=10.0):
             "sample": f"first {sample} pairs of the workload, scores + CIGARs, {cores} threads, {dt:.1f} s"}
 
 
+def run_serving(args):
+    """c5: the request server under Poisson arrivals.  For each offered rate,
+    `--requests` requests of uniform 1..256 pairs from the serving mixture
+    (70 % 150 bp @ 1-3 %, 25 % 1-5 kbp @ 5-10 %, 5 % 10-50 kbp @ 10-20 %) are
+    submitted from host buffers at their arrival times by one
+    client thread while another waits for the results; one JSON line per
+    rate: pairs/s completed, GCUPS, latency percentiles (submit -> result
+    visible, measured by the server), requests merged per job."""
+    import queue
+
+    import tsunami_pact_b200 as T
+    from tsunami_pact_b200 import datasets as D
+
+    rates = [float(x) for x in args.rates.split(",") if x]
+    budget = int(args.budget_gb * (1 << 30))
+    srv = T.Server(*PEN, workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2)
+
+    def stream(index, n_req, rate):
+        arrivals, sizes = D.c5_stream(n_req, rate, index=index)
+        lengths, rates_, seed = D.shape("c5", int(sizes.sum()) + 1000 * index)
+        first = 1000 * index
+        lengths, rates_ = lengths[first:], rates_[first:]
+        pbuf, poff, plen, tbuf, toff, tlen = T.gen_batch(seed, lengths, rates_, first=first)
+        reqs, k = [], 0
+        for sz in sizes:
+            sl = slice(k, k + int(sz))
+            reqs.append((pbuf, poff[sl].copy(), plen[sl].copy(), tbuf, toff[sl].copy(), tlen[sl].copy()))
+            k += int(sz)
+        cells = float(np.sum(plen.astype(np.float64) * tlen))
+        return arrivals, sizes, reqs, cells
+
+    # warm-up: a few requests through every worker
+    _, _, wreqs, _ = stream(99, 4 * max(args.workers, 1), 1000.0)
+    for rid in [srv.submit_arrays(*r) for r in wreqs]:
+        srv.wait(rid)
+    for k, rate in enumerate(rates):
+        arrivals, sizes, reqs, cells = stream(k, args.requests, rate)
+        srv.reset_stats()
+        ids: "queue.Queue" = queue.Queue()
+        errors = []
+
+        def submitter():
+            t0 = time.perf_counter()
+            for a, r in zip(arrivals, reqs):
+                dt = t0 + a - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                try:
+                    ids.put(srv.submit_arrays(*r))
+                except T.AlignError as e:
+                    errors.append(str(e))
+                    ids.put(None)
+
+        clocks = ClockSampler(0)
+        clocks.start()
+        t0 = time.perf_counter()
+        th = threading.Thread(target=submitter)
+        th.start()
+        for _ in reqs:
+            rid = ids.get()
+            if rid is not None:
+                srv.wait(rid)
+        t1 = time.perf_counter()
+        th.join()
+        clk = clocks.stop()
+        st = srv.stats()
+        wall = t1 - t0
+        out = {
+            "metric": "pairs/s (serving)", "value": st["pairs_completed"] / wall, "unit": "pairs/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "c5 serving: Poisson arrivals, requests of U{1..256} pairs, mixture 70% 150 bp "
+                                   "@1-3%, 25% 1-5 kbp @5-10%, 5% 10-50 kbp @10-20%, penalties 4/6/2",
+                       "offered_rate_rps": rate, "requests": len(reqs), "pairs": int(sizes.sum()),
+                       "workers": args.workers, "budget_gb": st["budget_bytes"] / 2**30},
+            "offered_pairs_s": float(sizes.sum()) / max(float(arrivals[-1]), 1e-9),
+            "gcups": cells / wall / 1e9,
+            "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "p999": st["p999_ms"], "mean": st["mean_ms"],
+                           "max": st["max_ms"]},
+            "completed": st["completed"], "failed": st["failed"], "rejected": st["rejected"] + len(errors),
+            "jobs": st["jobs"], "mean_requests_per_job": st["mean_requests_per_job"],
+            "peak_granted_gb": st["peak_granted_bytes"] / 2**30, "wall_s": wall, "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    srv.close()
+
+
 def run_reference(args, workload):
     """CPU path on the host cores, rank 0 only (other ranks exit 0)."""
     rank, world, _ = dist_env()
@@ -206,7 +292,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tsunami", choices=["tsunami", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c5"])
     ap.add_argument("--score-only", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -214,7 +300,17 @@ def main():
     ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
     ap.add_argument("--plain", action="store_true", help="also time the plain one-warp-per-pair bucketed form")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain form (c4)")
+    ap.add_argument("--rates", default="25,50,100,200", help="c5: offered request rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
+    ap.add_argument("--workers", type=int, default=4, help="c5: server workers")
+    ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
     args = ap.parse_args()
+    if args.workload == "c5":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "no serving path in the reference"}))
+        else:
+            run_serving(args)
+        return
     if args.pairs:
         WORKLOADS[args.workload][0] = args.pairs
     workload = args.workload

@@ -43,6 +43,7 @@ extern "C" {
 #define TSU_ENOTFOUND 7 /* unknown request id                                */
 #define TSU_EINTERNAL 8 /* an internal consistency check failed              */
 #define TSU_EIO 9       /* file could not be opened / parsed                 */
+#define TSU_EPENDING 10 /* request not finished yet (tsu_poll)               */
 
 /* Per-pair status values written by the engine. */
 #define TSU_PAIR_OK 0
@@ -207,6 +208,88 @@ int tsu_gen_batch(uint64_t seed, int64_t first, int64_t count, const int32_t* le
 /* Write a batch in the sequences.txt format (generate_dataset.cpp:39-41,
  * 68-69): header num / seq_len / error_rate, then pattern and text lines. */
 int tsu_file_write(const char* path, int64_t num, int32_t seq_len, int32_t error_rate, const tsu_batch* batch);
+
+/* ---- request server -------------------------------------------------------
+ * No counterpart in the reference (one file per process, wfa_gpu.cu:43-188).
+ * Continuous batching on one device: tsu_submit copies a request (a batch of
+ * any size) into the server and returns at once; a pool of workers -- engine
+ * contexts with their own streams and buffers -- runs jobs, each the oldest
+ * queued request plus the ones queued behind it (same flags), through the
+ * same path as tsu_align_batch, and jobs overlap on the device.  A job starts
+ * when a worker is free and its predicted device memory (inputs, CIGAR
+ * arena, wavefront scratch sized by max_error_hint and bounded by the
+ * penalty-derived score bound of each pair) fits in mem_budget beside the
+ * memory the other workers hold.  Requests start in submission order.
+ * Scores and CIGARs of a request are the same alone and in any mix.
+ * submit / poll / wait / cancel / stats may be called from any threads. */
+typedef struct tsu_server tsu_server;
+
+typedef struct {
+  int32_t device;
+  int32_t workers;          /* jobs in flight (engine contexts); 0 = 4          */
+  size_t mem_budget;        /* device bytes of all workers; 0 = 80% of free      */
+  double max_error_hint;    /* edit rate sizing predicted wavefront memory (0 = 0.20);
+                               pairs beyond it are retried, never dropped       */
+  int64_t max_queue;        /* queued requests before submit says TSU_EBUSY (0 = 65536) */
+  int64_t max_job_pairs;    /* pairs merged into one job (0 = 16384)             */
+  int32_t max_job_requests; /* requests merged into one job (0 = 64; 1 = none)   */
+  int32_t reserved0;
+  double watchdog_ms;       /* a job running longer completes its requests with
+                               TSU_ETIMEOUT (0 = off)                             */
+  size_t resident_bytes;    /* device bytes an idle worker keeps for the next job
+                               (0 = mem_budget / (2 * workers))                   */
+} tsu_server_config;
+
+/* Per-request timing, from tsu_poll / tsu_wait. */
+typedef struct {
+  int64_t num_pairs;
+  double queue_ms;       /* submit -> its job started                      */
+  double latency_ms;     /* submit -> result visible to poll / wait        */
+  int32_t job_requests;  /* requests merged into the job that ran it       */
+  int32_t attempts;      /* jobs it took (> 1 after a retry)               */
+  int64_t job_seq;       /* number of the job that ran it; jobs are numbered
+                            in the order they start                        */
+} tsu_request_info;
+
+/* Counters since create or the last tsu_server_reset_stats; latencies are
+ * those of completed requests (submit -> result visible). */
+typedef struct {
+  int64_t submitted, completed, failed, rejected, cancelled, timed_out;
+  int64_t queued, running; /* requests now */
+  int64_t jobs, pairs_completed;
+  double mean_requests_per_job;
+  double p50_ms, p99_ms, p999_ms, mean_ms, max_ms;
+  double elapsed_s;
+  uint64_t budget_bytes, granted_bytes, peak_granted_bytes;
+  int32_t workers, reserved0;
+} tsu_server_stats;
+
+int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg /* nullable */, tsu_server** out);
+/* Queued requests are dropped; running jobs finish first. */
+int tsu_server_destroy(tsu_server* srv);
+/* flags: TSU_SCORE_ONLY or 0.  TSU_EINVAL for bad pairs, TSU_ENOMEM when the
+ * request cannot fit the budget even alone, TSU_EBUSY when the queue is
+ * full.  The caller's buffers may be reused when it returns. */
+int tsu_submit(tsu_server* srv, const tsu_batch* request, uint32_t flags, uint64_t* id);
+/* TSU_EPENDING until the request is done; then its results are copied into
+ * res (as tsu_align_batch fills it; cigar_offset has num_pairs + 1 entries),
+ * the request is forgotten and its status returned.  TSU_EOVERFLOW keeps the
+ * request and sets res->cigar_needed.  info is optional. */
+int tsu_poll(tsu_server* srv, uint64_t id, tsu_result* res, tsu_request_info* info);
+/* tsu_poll after waiting up to timeout_ms (< 0: no limit); TSU_ETIMEOUT if
+ * the request is still not done. */
+int tsu_wait(tsu_server* srv, uint64_t id, double timeout_ms, tsu_result* res, tsu_request_info* info);
+/* Drop a request: queued ones never run, running ones' results are
+ * discarded.  TSU_ENOTFOUND for unknown ids. */
+int tsu_cancel(tsu_server* srv, uint64_t id);
+int tsu_server_get_stats(tsu_server* srv, tsu_server_stats* out);
+int tsu_server_reset_stats(tsu_server* srv);
+const char* tsu_server_last_error(tsu_server* srv);
+
+/* Device bytes tsu_align_batch(ctx, batch, flags) holds at its peak, with
+ * every pair of a length band in flight (*full) or one (*min); the server
+ * admits requests by this prediction. */
+int tsu_predict_bytes(tsu_ctx* ctx, const tsu_batch* batch, uint32_t flags, size_t* full, size_t* min);
 
 #ifdef __cplusplus
 }

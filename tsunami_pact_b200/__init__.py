@@ -13,6 +13,7 @@ the library is missing or CUDA is unavailable the calls raise.
 from ._lib import (  # noqa: F401
     Aligner,
     AlignError,
+    Server,
     TSU_SCORE_ONLY,
     build,
     gen_batch,
@@ -27,6 +28,7 @@ from ._lib import (  # noqa: F401
 __all__ = [
     "Aligner",
     "AlignError",
+    "Server",
     "TSU_SCORE_ONLY",
     "build",
     "gen_batch",

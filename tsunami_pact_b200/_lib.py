@@ -13,7 +13,12 @@ _LIB = os.path.join(_HERE, "libtsunami_b200.so")
 _lib = None
 
 TSU_OK = 0
+TSU_ENOMEM = 2
+TSU_ETIMEOUT = 4
 TSU_EOVERFLOW = 5
+TSU_EBUSY = 6
+TSU_ENOTFOUND = 7
+TSU_EPENDING = 10
 TSU_SCORE_ONLY = 0x1
 TSU_ONE_WARP = 0x2
 
@@ -45,6 +50,28 @@ class Timing(ctypes.Structure):
                 ("compact_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("kernel_launches", c_i64), ("retried_pairs", c_i64), ("h2d_bytes", c_i64),
                 ("d2h_bytes", c_i64), ("cells", c_i64), ("steps", c_i64)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", c_i32), ("workers", c_i32), ("mem_budget", ctypes.c_size_t),
+                ("max_error_hint", ctypes.c_double), ("max_queue", c_i64), ("max_job_pairs", c_i64),
+                ("max_job_requests", c_i32), ("reserved0", c_i32), ("watchdog_ms", ctypes.c_double),
+                ("resident_bytes", ctypes.c_size_t)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("num_pairs", c_i64), ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("job_requests", c_i32), ("attempts", c_i32), ("job_seq", c_i64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", c_i64), ("completed", c_i64), ("failed", c_i64), ("rejected", c_i64),
+                ("cancelled", c_i64), ("timed_out", c_i64), ("queued", c_i64), ("running", c_i64),
+                ("jobs", c_i64), ("pairs_completed", c_i64), ("mean_requests_per_job", ctypes.c_double),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("elapsed_s", ctypes.c_double),
+                ("budget_bytes", ctypes.c_uint64), ("granted_bytes", ctypes.c_uint64),
+                ("peak_granted_bytes", ctypes.c_uint64), ("workers", c_i32), ("reserved0", c_i32)]
 
 
 class AlignError(RuntimeError):
@@ -94,6 +121,17 @@ def lib():
     L.tsu_gen_pair.argtypes = [ctypes.c_uint64, c_i64, c_i32, ctypes.c_double, c_vp, P(c_i32), c_vp, P(c_i32)]
     L.tsu_gen_batch.argtypes = [ctypes.c_uint64, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                 ctypes.c_int]
+    L.tsu_predict_bytes.argtypes = [c_vp, P(Batch), c_u32, P(ctypes.c_size_t), P(ctypes.c_size_t)]
+    L.tsu_server_create.argtypes = [P(Penalties), P(ServerConfig), P(c_vp)]
+    L.tsu_server_destroy.argtypes = [c_vp]
+    L.tsu_submit.argtypes = [c_vp, P(Batch), c_u32, P(ctypes.c_uint64)]
+    L.tsu_poll.argtypes = [c_vp, ctypes.c_uint64, P(Result), P(RequestInfo)]
+    L.tsu_wait.argtypes = [c_vp, ctypes.c_uint64, ctypes.c_double, P(Result), P(RequestInfo)]
+    L.tsu_cancel.argtypes = [c_vp, ctypes.c_uint64]
+    L.tsu_server_get_stats.argtypes = [c_vp, P(ServerStats)]
+    L.tsu_server_reset_stats.argtypes = [c_vp]
+    L.tsu_server_last_error.restype = ctypes.c_char_p
+    L.tsu_server_last_error.argtypes = [c_vp]
     _lib = L
     return L
 
@@ -259,6 +297,113 @@ class Aligner:
             raise AlignError(rc, f"cigar buffer too small: need {r.cigar_needed} runs", int(r.cigar_needed))
         self._check(rc)
         return int(r.cigar_needed)
+
+
+class Server:
+    """Request server (tsu_server_*): continuous batching of alignment
+    requests on one device with memory admission.  ``submit`` returns a
+    request id at once; ``wait``/``poll`` return its results."""
+
+    def __init__(self, mismatch: int = 4, gap_opening: int = 6, gap_extension: int = 2, device: int = 0,
+                 workers: int = 0, mem_budget: int = 0, max_error_hint: float = 0.0, max_queue: int = 0,
+                 max_job_pairs: int = 0, max_job_requests: int = 0, watchdog_ms: float = 0.0,
+                 resident_bytes: int = 0):
+        L = lib()
+        pen = Penalties(mismatch, gap_opening, gap_extension)
+        cfg = ServerConfig(device, workers, mem_budget, max_error_hint, max_queue, max_job_pairs,
+                           max_job_requests, 0, watchdog_ms, resident_bytes)
+        h = c_vp()
+        rc = L.tsu_server_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
+        if rc != TSU_OK:
+            raise AlignError(rc, L.tsu_status_str(rc).decode())
+        self._h = h
+        self._cigar = {}  # id -> (wants CIGAR, pairs, run capacity)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tsu_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _err(self, rc: int) -> AlignError:
+        L = lib()
+        return AlignError(rc, f"{L.tsu_status_str(rc).decode()}: {L.tsu_server_last_error(self._h).decode()}")
+
+    def submit_arrays(self, pbuf, poff, plen, tbuf, toff, tlen, cigar: bool = True) -> int:
+        n = len(plen)
+        poff = np.ascontiguousarray(poff, dtype=np.int64)
+        toff = np.ascontiguousarray(toff, dtype=np.int64)
+        plen = np.ascontiguousarray(plen, dtype=np.int32)
+        tlen = np.ascontiguousarray(tlen, dtype=np.int32)
+        b = Batch(n, _ptr(pbuf), _ptr(poff), _ptr(plen), _ptr(tbuf), _ptr(toff), _ptr(tlen))
+        rid = ctypes.c_uint64()
+        rc = lib().tsu_submit(self._h, ctypes.byref(b), 0 if cigar else TSU_SCORE_ONLY, ctypes.byref(rid))
+        if rc != TSU_OK:
+            raise self._err(rc)
+        cap = int(plen.astype(np.int64).sum() + tlen.astype(np.int64).sum()) + 1
+        self._cigar[rid.value] = (cigar, n, cap)
+        return rid.value
+
+    def submit(self, patterns: Sequence, texts: Sequence, cigar: bool = True) -> int:
+        if len(patterns) != len(texts):
+            raise ValueError("patterns and texts differ in length")
+        pb, po, pl = _concat(patterns)
+        tb, to, tl = _concat(texts)
+        return self.submit_arrays(pb, po, pl, tb, to, tl, cigar=cigar)
+
+    def _take(self, rid: int, timeout_ms: Optional[float]):
+        cig, n, cap = self._cigar[rid]
+        scores = np.zeros(max(n, 1), dtype=np.int32)
+        st = np.zeros(max(n, 1), dtype=np.int32)
+        coff = np.zeros(n + 1, dtype=np.int64) if cig else None
+        runs = np.zeros(cap, dtype=np.uint32) if cig else None
+        r = Result(_ptr(scores), _ptr(runs), cap if cig else 0, _ptr(coff), 0, _ptr(st))
+        info = RequestInfo()
+        L = lib()
+        if timeout_ms is None:
+            rc = L.tsu_poll(self._h, rid, ctypes.byref(r), ctypes.byref(info))
+        else:
+            rc = L.tsu_wait(self._h, rid, timeout_ms, ctypes.byref(r), ctypes.byref(info))
+        if rc in (TSU_EPENDING, TSU_ETIMEOUT):
+            return None
+        self._cigar.pop(rid, None)
+        if rc != TSU_OK:
+            raise self._err(rc)
+        inf = {f: getattr(info, f) for f, _ in RequestInfo._fields_}
+        if not cig:
+            return scores[:n], None, None, inf
+        return scores[:n], coff, runs[: int(coff[-1])], inf
+
+    def poll(self, rid: int):
+        """(scores, cigar_offsets, runs, info) if done, else None."""
+        return self._take(rid, None)
+
+    def wait(self, rid: int, timeout_ms: float = -1.0):
+        """Block until done (timeout_ms < 0: no limit); None on timeout."""
+        return self._take(rid, timeout_ms)
+
+    def cancel(self, rid: int) -> int:
+        self._cigar.pop(rid, None)
+        return lib().tsu_cancel(self._h, rid)
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        lib().tsu_server_get_stats(self._h, ctypes.byref(s))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        lib().tsu_server_reset_stats(self._h)
 
 
 def read_sequences(path: str):

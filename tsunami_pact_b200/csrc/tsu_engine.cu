@@ -16,10 +16,13 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/tsunami_b200.h"
+#include "tsu_engine_internal.h"
 #include "tsu_kernels.cuh"
 #include "tsu_plan.h"
 
@@ -63,13 +66,18 @@ struct tsu_ctx {
   cudaEvent_t pev[2] = {};  // per-pass timing
   std::string passlog;      // passes of the last align call (tsu_pass_log)
   cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;  // chunk pipeline copy streams
+  cudaEvent_t fence_ev[2] = {};  // orders frees after the copy streams' queued work
+  cudaMemPool_t pool = nullptr;  // the device's buffer pool
+  bool exact_grow = false;       // grow buffers to the asked size only
+  size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
+  std::vector<DevBuf*> bufs() {
+    return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
+            &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
+            &b_retry, &b_counters, &b_ring,  &b_hist, &b_table, &b_arena, &b_scan_tmp,  &b_out2};
+  }
   size_t held() const {
-    const DevBuf* all[] = {&b_pat, &b_txt, &b_poff, &b_toff, &b_plen, &b_tlen, &b_words_cnt, &b_woff,
-                           &b_words, &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,
-                           &b_out, &b_order, &b_retry, &b_counters, &b_ring, &b_hist, &b_table, &b_arena,
-                           &b_scan_tmp, &b_out2};
     size_t s = 0;
-    for (auto* b : all) s += b->cap;
+    for (const DevBuf* b : const_cast<tsu_ctx*>(this)->bufs()) s += b->cap;
     return s;
   }
 };
@@ -102,33 +110,88 @@ int gcd(int a, int b) {
   return a;
 }
 
-// Grow a buffer to at least `bytes` within the context budget.
+// Device memory of every context comes from one stream-ordered pool per
+// device: a buffer is regrown with cudaFreeAsync + cudaMallocFromPoolAsync on
+// the context's stream, which never synchronises the device (cudaFree does),
+// so contexts driven from several host threads -- the request server's
+// workers -- do not stall each other.  Freed blocks stay in the pool
+// (release threshold unlimited) for the next allocation of any context.
+cudaMemPool_t device_pool(int dev) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t p = nullptr;
+  if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = p;
+  return p;
+}
+
+// Free a buffer in stream order after everything queued so far on the
+// context's three streams (copy streams read and write some buffers).
+void release(tsu_ctx* ctx, DevBuf& b) {
+  if (!b.p) return;
+  cudaEventRecord(ctx->fence_ev[0], ctx->h2d_stream);
+  cudaEventRecord(ctx->fence_ev[1], ctx->d2h_stream);
+  cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[0], 0);
+  cudaStreamWaitEvent(ctx->stream, ctx->fence_ev[1], 0);
+  cudaFreeAsync(b.p, ctx->stream);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+// Grow a buffer to at least `bytes` within the context budget.  The new
+// buffer is ordered on the context's stream; work on the copy streams that
+// uses it must wait for that stream (alloc_fence).
 int grow(tsu_ctx* ctx, DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.cap >= bytes) return TSU_OK;
-  size_t nb = std::max(bytes, b.cap + b.cap / 2);
+  size_t nb = ctx->exact_grow ? bytes : std::max(bytes, b.cap + b.cap / 2);
   nb = (nb + 255) & ~(size_t)255;
   if (ctx->held() - b.cap + nb > ctx->budget) {
-    nb = bytes;
-    if (ctx->held() - b.cap + nb > ctx->budget)
+    nb = (bytes + 255) & ~(size_t)255;
+    if (ctx->held() - b.cap + nb > ctx->budget) {
+      ctx->need_bytes = ctx->held() - b.cap + nb;
       return set_err(ctx, TSU_ENOMEM, "device budget %zu B exceeded (need %zu more)", ctx->budget, bytes);
+    }
   }
-  if (b.p) cudaFree(b.p);
-  b.p = nullptr;
-  b.cap = 0;
-  cudaError_t e = cudaMalloc(&b.p, nb);
+  release(ctx, b);
+  cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(&b.p, nb, ctx->pool, ctx->stream) : cudaErrorInvalidValue;
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return set_err(ctx, TSU_ENOMEM, "cudaMalloc(%zu) failed: %s", nb, cudaGetErrorString(e));
+    b.p = nullptr;
+    ctx->need_bytes = ctx->held() + nb;
+    return set_err(ctx, TSU_ENOMEM, "device allocation of %zu B failed: %s", nb, cudaGetErrorString(e));
   }
   b.cap = nb;
   return TSU_OK;
 }
 
-void release(DevBuf& b) {
-  if (b.p) cudaFree(b.p);
-  b.p = nullptr;
-  b.cap = 0;
+// Make the copy streams wait for the allocations queued on the context's
+// stream so far.
+void alloc_fence(tsu_ctx* ctx) {
+  cudaEventRecord(ctx->fence_ev[0], ctx->stream);
+  cudaStreamWaitEvent(ctx->h2d_stream, ctx->fence_ev[0], 0);
+  cudaStreamWaitEvent(ctx->d2h_stream, ctx->fence_ev[0], 0);
+}
+
+// Every buffer back to the pool, once the context's streams are idle.
+int release_all(tsu_ctx* ctx) {
+  cudaStreamSynchronize(ctx->h2d_stream);
+  cudaStreamSynchronize(ctx->d2h_stream);
+  cudaStreamSynchronize(ctx->stream);
+  for (DevBuf* b : ctx->bufs()) release(ctx, *b);
+  return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? TSU_OK : TSU_EDEVICE;
 }
 
 template <class T>
@@ -150,32 +213,35 @@ struct BatchInfo {
 };
 
 // The align_kernel instantiations: CIGAR or score only, shared or global
-// wavefront ring, 1/2/4/8/16 warps per pair.
+// wavefront ring, 1/2/4/8/16 warps per pair.  Each kernel's dynamic shared
+// memory limit is set to the device maximum (the same value on every call),
+// so contexts planning on several host threads cannot lower it under
+// another's launch.
 template <bool kCigar, int kMode, int GW>
-cudaError_t occ_one(int threads, size_t smem, int* occ) {
+cudaError_t occ_one(int threads, size_t smem, int optin, int* occ) {
   cudaError_t e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode, GW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode, GW>, threads, smem);
 }
 
 template <bool kCigar, int kMode>
-cudaError_t occ_gw(int gw, int threads, size_t smem, int* occ) {
+cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
   switch (gw) {
-    case 1: return occ_one<kCigar, kMode, 1>(threads, smem, occ);
-    case 2: return occ_one<kCigar, kMode, 2>(threads, smem, occ);
-    case 4: return occ_one<kCigar, kMode, 4>(threads, smem, occ);
-    case 8: return occ_one<kCigar, kMode, 8>(threads, smem, occ);
-    case 16: return occ_one<kCigar, kMode, 16>(threads, smem, occ);
+    case 1: return occ_one<kCigar, kMode, 1>(threads, smem, optin, occ);
+    case 2: return occ_one<kCigar, kMode, 2>(threads, smem, optin, occ);
+    case 4: return occ_one<kCigar, kMode, 4>(threads, smem, optin, occ);
+    case 8: return occ_one<kCigar, kMode, 8>(threads, smem, optin, occ);
+    case 16: return occ_one<kCigar, kMode, 16>(threads, smem, optin, occ);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t align_occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int* occ) {
-  if (cigar) return mode == tsu::kModeShared ? occ_gw<true, tsu::kModeShared>(gw, threads, smem, occ)
-                                             : occ_gw<true, tsu::kModeGlobal>(gw, threads, smem, occ);
-  return mode == tsu::kModeShared ? occ_gw<false, tsu::kModeShared>(gw, threads, smem, occ)
-                                  : occ_gw<false, tsu::kModeGlobal>(gw, threads, smem, occ);
+cudaError_t align_occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ) {
+  if (cigar) return mode == tsu::kModeShared ? occ_gw<true, tsu::kModeShared>(gw, threads, smem, optin, occ)
+                                             : occ_gw<true, tsu::kModeGlobal>(gw, threads, smem, optin, occ);
+  return mode == tsu::kModeShared ? occ_gw<false, tsu::kModeShared>(gw, threads, smem, optin, occ)
+                                  : occ_gw<false, tsu::kModeGlobal>(gw, threads, smem, optin, occ);
 }
 
 template <bool kCigar, int kMode>
@@ -205,31 +271,35 @@ void launch_align(bool cigar, int mode, int gw, int blocks, int threads, size_t 
   }
 }
 
+// Scratch bytes of one group of a pass (ring, history, step table).
+size_t group_scratch_bytes(const tsu::PassGeom& g) {
+  return (size_t)(g.ring_ints * 4 + g.hist_cap * 4 + (int64_t)g.table_cap * 8 + 64);
+}
+
 // Configure a pass of configuration pc over pairs of at most bi's lengths:
-// geometry, then as many groups as fit the SMs, the pairs and the budget.
-int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint, bool want_cigar,
-              size_t reserve_bytes, Pass* out) {
+// geometry, then as many groups as fit the SMs, the pairs and `avail` bytes
+// of scratch.
+int plan_pass_within(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint,
+                     bool want_cigar, size_t avail, Pass* out) {
   Pass p;
   const tsu::PassGeom g = tsu::plan_geometry(ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, bi.max_m, bi.max_n, pc.mode,
                                              pc.gw, hint, want_cigar, ctx->smem_optin);
   p.g = g;
   const int gpc = g.groups_per_cta;
   int occ = 0;
-  cudaError_t e = align_occupancy(want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, &occ);
+  cudaError_t e =
+      align_occupancy(want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, ctx->smem_optin, &occ);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
   int64_t warps = (int64_t)ctx->sms * occ * gpc;  // groups
-  const int64_t table_cap = g.table_cap;
-  const int64_t hist_cap = g.hist_cap;
-  const int64_t ring_ints = g.ring_ints;
-  // scratch buffers are regrown for this pass: their current size is free
-  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
-  const size_t avail = ctx->budget > fixed + reserve_bytes ? ctx->budget - fixed - reserve_bytes : 0;
-  auto per_warp = [&](int64_t hc) { return (size_t)(ring_ints * 4 + hc * 4 + table_cap * 8 + 64); };
+  const size_t per_warp = group_scratch_bytes(g);
   // fewer warps when the pass has fewer pairs or the budget is tight
   warps = std::min<int64_t>(warps, std::max<int64_t>(n_pairs, 1));
-  if ((size_t)warps * per_warp(hist_cap) > avail) {
-    int64_t w2 = (int64_t)(avail / per_warp(hist_cap));
-    if (w2 < 1) return set_err(ctx, TSU_ENOMEM, "scratch for one pair (%zu B) exceeds the budget", per_warp(hist_cap));
+  if ((size_t)warps * per_warp > avail) {
+    int64_t w2 = (int64_t)(avail / per_warp);
+    if (w2 < 1) {
+      ctx->need_bytes = ctx->budget - avail + per_warp;
+      return set_err(ctx, TSU_ENOMEM, "scratch for one pair (%zu B) exceeds the budget", per_warp);
+    }
     warps = w2;
   }
   int gpb = gpc;  // groups per block
@@ -242,10 +312,57 @@ int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoic
   p.blocks = (int)(warps / gpb);
   p.threads = 32 * g.gw * gpb;
   p.smem_bytes = (size_t)gpb * g.group_smem;
-  (void)hist_cap;
-  (void)table_cap;
   *out = p;
   return TSU_OK;
+}
+
+// plan_pass_within with the budget left beside the context's other buffers
+// (the scratch buffers are regrown for the pass: their current size is free).
+int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint, bool want_cigar,
+              Pass* out) {
+  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
+  const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+  return plan_pass_within(ctx, bi, n_pairs, pc, hint, want_cigar, avail, out);
+}
+
+// Pairs of a run by length band (tsu::length_band of max(m, n)), each band
+// ordered longest first (a counting sort by floor(log2(m + n))).  `uniform`:
+// every pair in one length class and band -- run as one band in input order
+// (bands stay empty).
+struct BandSplit {
+  std::vector<std::vector<int32_t>> bands = std::vector<std::vector<int32_t>>(tsu::kBands);
+  bool uniform = true;
+  int uniform_band = 0;
+};
+
+void split_bands(int64_t n, const int32_t* h_plen, const int32_t* h_tlen, BandSplit* out) {
+  int64_t cnt[34] = {0};
+  auto cls = [&](int64_t i) {
+    const uint32_t l = (uint32_t)h_plen[i] + (uint32_t)h_tlen[i];
+    return l ? 32 - __builtin_clz(l) : 0;
+  };
+  int cmin = 33, cmax = 0, bmin = tsu::kBands, bmax = -1;
+  for (int64_t i = 0; i < n; ++i) {
+    const int c = cls(i);
+    ++cnt[c];
+    cmin = std::min(cmin, c);
+    cmax = std::max(cmax, c);
+    const int b = tsu::length_band(std::max(h_plen[i], h_tlen[i]));
+    bmin = std::min(bmin, b);
+    bmax = std::max(bmax, b);
+  }
+  out->uniform = cmin == cmax && bmin == bmax;
+  out->uniform_band = bmax < 0 ? 0 : bmax;
+  if (out->uniform) return;
+  std::vector<int32_t> by_len((size_t)n);
+  int64_t start[34];
+  int64_t acc = 0;
+  for (int c = 33; c >= 0; --c) {
+    start[c] = acc;
+    acc += cnt[c];
+  }
+  for (int64_t i = 0; i < n; ++i) by_len[(size_t)start[cls(i)]++] = (int32_t)i;
+  for (int32_t i : by_len) out->bands[(size_t)tsu::length_band(std::max(h_plen[i], h_tlen[i]))].push_back(i);
 }
 
 // Core: inputs resident on the device (sv).  Writes score/status (device)
@@ -319,39 +436,11 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   // sort by floor(log2(m + n))).  TSU_ONE_WARP keeps one band in input order
   // starting at one warp per pair.
   int passes = 0;
-  std::vector<std::vector<int32_t>> bands(tsu::kBands);
-  bool uniform = true;  // every pair in one length class: one band, input order
-  int uniform_band = 0;
-  if (!ctx->one_warp && h_plen) {
-    int64_t cnt[34] = {0};
-    auto cls = [&](int64_t i) {
-      const uint32_t l = (uint32_t)h_plen[i] + (uint32_t)h_tlen[i];
-      return l ? 32 - __builtin_clz(l) : 0;
-    };
-    int cmin = 33, cmax = 0, bmin = tsu::kBands, bmax = -1;
-    for (int64_t i = 0; i < n; ++i) {
-      const int c = cls(i);
-      ++cnt[c];
-      cmin = std::min(cmin, c);
-      cmax = std::max(cmax, c);
-      const int b = tsu::length_band(std::max(h_plen[i], h_tlen[i]));
-      bmin = std::min(bmin, b);
-      bmax = std::max(bmax, b);
-    }
-    uniform = cmin == cmax && bmin == bmax;
-    uniform_band = bmax < 0 ? 0 : bmax;
-    if (!uniform) {
-      std::vector<int32_t> by_len((size_t)n);
-      int64_t start[34];
-      int64_t acc = 0;
-      for (int c = 33; c >= 0; --c) {
-        start[c] = acc;
-        acc += cnt[c];
-      }
-      for (int64_t i = 0; i < n; ++i) by_len[(size_t)start[cls(i)]++] = (int32_t)i;
-      for (int32_t i : by_len) bands[(size_t)tsu::length_band(std::max(h_plen[i], h_tlen[i]))].push_back(i);
-    }
-  }
+  BandSplit split;
+  if (!ctx->one_warp && h_plen) split_bands(n, h_plen, h_tlen, &split);
+  const std::vector<std::vector<int32_t>>& bands = split.bands;
+  const bool uniform = split.uniform;
+  const int uniform_band = split.uniform_band;
   CU(cudaEventRecord(ctx->ev[4], st));
   std::string passlog;  // mode, warps per pair x groups : pairs, per pass (for error messages)
   std::vector<int32_t> rlist;
@@ -381,7 +470,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   const int band_first_pass = passes;
   for (;;) {
     Pass ps;
-    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, 0, &ps))) return rc;
+    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, &ps))) return rc;
     const tsu::PassGeom& g = ps.g;
     {
       // plan_pass counted the scratch buffers as free: if any of them must
@@ -391,9 +480,9 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       const size_t need_table = want_cigar ? sizeof(int2) * (size_t)ps.groups * g.table_cap : 0;
       if (need_ring > ctx->b_ring.cap || need_hist > ctx->b_hist.cap || need_table > ctx->b_table.cap) {
         CU(cudaStreamSynchronize(st));
-        release(ctx->b_ring);
-        release(ctx->b_hist);
-        release(ctx->b_table);
+        release(ctx, ctx->b_ring);
+        release(ctx, ctx->b_hist);
+        release(ctx, ctx->b_table);
       }
       passlog += (passlog.empty() ? "" : " ") + std::string(g.mode == tsu::kModeShared ? "s" : "g") +
                  std::to_string(g.gw) + "x" + std::to_string(ps.groups) + ":" + std::to_string(n_order);
@@ -481,14 +570,16 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       if (need > arena_cap) {
         // keep the runs written so far: grow by copy
         DevBuf nb;
-        size_t bytes = sizeof(uint32_t) * (size_t)need;
-        if (ctx->held() + bytes > ctx->budget) return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
-        CU(cudaMalloc(&nb.p, bytes));
+        const size_t bytes = (sizeof(uint32_t) * (size_t)need + 255) & ~(size_t)255;
+        if (ctx->held() + bytes > ctx->budget) {
+          ctx->need_bytes = ctx->held() + bytes;
+          return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
+        }
+        CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
         nb.cap = bytes;
         const int64_t keep = std::min<int64_t>((int64_t)used, arena_cap);
         CU(cudaMemcpyAsync(nb.p, ctx->b_arena.p, sizeof(uint32_t) * (size_t)keep, cudaMemcpyDeviceToDevice, st));
-        CU(cudaStreamSynchronize(st));
-        release(ctx->b_arena);
+        release(ctx, ctx->b_arena);
         ctx->b_arena = nb;
         arena_cap = need;
       }
@@ -539,6 +630,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   return TSU_OK;
 }
 
+// Chunks of the host-buffer pipeline (tsu_align_batch): 131072 pairs or
+// more each, at most 8.
+int chunk_count(int64_t n) { return (int)std::min<int64_t>(8, std::max<int64_t>(1, n / 131072)); }
+
 int check_batch_host(tsu_ctx* ctx, const tsu_batch* b, BatchInfo* bi, int64_t* pat_bytes, int64_t* txt_bytes) {
   if (!b || b->num_pairs < 0) return set_err(ctx, TSU_EINVAL, "null batch or negative num_pairs");
   if (b->num_pairs > INT32_MAX) return set_err(ctx, TSU_EINVAL, "num_pairs > INT32_MAX");
@@ -577,6 +672,112 @@ int collect_status(tsu_ctx* ctx, const int32_t* hs, int64_t n) {
 }  // namespace
 
 // ===========================================================================
+// Engine calls of the request server (tsu_engine_internal.h)
+// ===========================================================================
+namespace tsu {
+namespace engine {
+
+int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, size_t* full, size_t* min) {
+  if (!ctx || sh.n < 0 || (sh.n && (!sh.plen || !sh.tlen)) || !full || !min) return TSU_EINVAL;
+  const bool want_cigar = !(flags & TSU_SCORE_ONLY);
+  const bool one_warp = (flags & TSU_ONE_WARP) != 0;
+  const int64_t n = sh.n;
+  auto r = [](size_t b) { return (std::max<size_t>(b, 16) + 255) & ~(size_t)255; };
+  auto scan_tmp = [](int64_t items) {
+    size_t t = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t, (const int64_t*)nullptr, (int64_t*)nullptr, (int)std::max<int64_t>(items, 1));
+    return t;
+  };
+  const int K = chunk_count(n);
+  // buffers of the whole call (tsu_align_batch)
+  size_t call = r((size_t)sh.pattern_bytes) + r((size_t)sh.text_bytes) + 2 * r(8 * (size_t)n) +
+                4 * r(4 * (size_t)n) + (want_cigar ? r(8 * (size_t)(n + K + 1)) : 0);
+  // buffers of a chunk (run_device): reused chunk after chunk, so the largest
+  // chunk sets them; scratch: the largest first pass of any band
+  size_t chunk_max = 0, scratch_full = 0, scratch_min = 0;
+  for (int c = 0; c < K; ++c) {
+    const int64_t c0 = n * c / K, nc = n * (c + 1) / K - c0;
+    if (nc == 0) continue;
+    const int32_t* pl = sh.plen + c0;
+    const int32_t* tl = sh.tlen + c0;
+    BatchInfo ci;
+    ci.n = nc;
+    int64_t len_sum = 0;
+    for (int64_t i = 0; i < nc; ++i) {
+      ci.max_m = std::max(ci.max_m, pl[i]);
+      ci.max_n = std::max(ci.max_n, tl[i]);
+      ci.total_words += (pl[i] + 31) / 32 + 1 + (tl[i] + 31) / 32 + 1;
+      len_sum += (int64_t)pl[i] + tl[i];
+    }
+    size_t f = 2 * r(16 * (size_t)nc) + r(8 * (size_t)ci.total_words) + r(2 * (size_t)nc) + r(8 * (size_t)nc) +
+               3 * r(4 * (size_t)nc) + r(64);
+    size_t tmp = scan_tmp(2 * nc);
+    if (want_cigar) {
+      const int64_t arena = std::max<int64_t>(tsu::arena_runs(ctx->x, ctx->go, nc, ci.max_m, ci.max_n, ctx->err_hint), 1024);
+      const int64_t out_runs = std::min<int64_t>(arena, len_sum + 1);
+      f += r(4 * (size_t)arena) + r(8 * (size_t)(nc + 1)) + (K > 1 ? 2 : 1) * r(4 * (size_t)out_runs);
+      tmp = std::max(tmp, scan_tmp(nc + 1));
+    }
+    chunk_max = std::max(chunk_max, f + r(tmp));
+    BandSplit split;
+    if (!one_warp) split_bands(nc, pl, tl, &split);
+    const bool all_pairs = one_warp || split.uniform;
+    for (int band = 0; band < tsu::kBands; ++band) {
+      if (all_pairs && band != 0) break;
+      if (!all_pairs && split.bands[(size_t)band].empty()) continue;
+      BatchInfo pbi = ci;
+      int64_t np = nc;
+      tsu::PassChoice pc{tsu::kModeShared, 1};
+      if (all_pairs) {
+        if (!one_warp) pc = tsu::band_start(split.uniform_band, std::max(ci.max_m, ci.max_n));
+      } else {
+        const std::vector<int32_t>& bp = split.bands[(size_t)band];
+        pbi = BatchInfo{};
+        np = pbi.n = (int64_t)bp.size();
+        for (int32_t i : bp) {
+          pbi.max_m = std::max(pbi.max_m, pl[i]);
+          pbi.max_n = std::max(pbi.max_n, tl[i]);
+        }
+        pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
+      }
+      Pass ps;
+      const int rc = plan_pass_within(ctx, pbi, np, pc, ctx->err_hint, want_cigar, SIZE_MAX / 4, &ps);
+      if (rc) return rc;
+      const size_t per = group_scratch_bytes(ps.g);
+      scratch_full = std::max(scratch_full, (size_t)ps.groups * per);
+      scratch_min = std::max(scratch_min, per);
+    }
+  }
+  const size_t slack = 64 << 10;  // 256-byte rounding of the buffers
+  *full = call + chunk_max + scratch_full + slack;
+  *min = call + chunk_max + scratch_min + slack;
+  return TSU_OK;
+}
+
+size_t held_bytes(const tsu_ctx* ctx) { return ctx ? ctx->held() : 0; }
+
+void set_budget(tsu_ctx* ctx, size_t bytes) {
+  if (ctx) ctx->budget = bytes;
+}
+
+size_t budget_bytes(const tsu_ctx* ctx) { return ctx ? ctx->budget : 0; }
+
+void set_exact_growth(tsu_ctx* ctx, bool exact) {
+  if (ctx) ctx->exact_grow = exact;
+}
+
+int trim(tsu_ctx* ctx) {
+  if (!ctx) return TSU_EINVAL;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return TSU_EDEVICE;
+  return release_all(ctx);
+}
+
+size_t needed_bytes(const tsu_ctx* ctx) { return ctx ? ctx->need_bytes : 0; }
+
+}  // namespace engine
+}  // namespace tsu
+
+// ===========================================================================
 // C ABI
 // ===========================================================================
 extern "C" {
@@ -593,6 +794,7 @@ const char* tsu_status_str(int s) {
     case TSU_ENOTFOUND: return "not found";
     case TSU_EINTERNAL: return "internal error";
     case TSU_EIO: return "i/o error";
+    case TSU_EPENDING: return "request not finished";
     default: return "unknown status";
   }
 }
@@ -643,8 +845,14 @@ int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
   for (auto& ev : ctx->pev) cudaEventCreate(&ev);
+  for (auto& ev : ctx->fence_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
+  ctx->pool = device_pool(ctx->device);
+  if (!ctx->pool) {
+    tsu_destroy(ctx);
+    return TSU_EDEVICE;
+  }
   *out = ctx;
   return TSU_OK;
 }
@@ -652,15 +860,10 @@ int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
 int tsu_destroy(tsu_ctx* ctx) {
   if (!ctx) return TSU_EINVAL;
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  DevBuf* all[] = {&ctx->b_pat, &ctx->b_txt, &ctx->b_poff, &ctx->b_toff, &ctx->b_plen, &ctx->b_tlen,
-                   &ctx->b_words_cnt, &ctx->b_woff, &ctx->b_words, &ctx->b_nonacgt, &ctx->b_score,
-                   &ctx->b_status, &ctx->b_cpos, &ctx->b_clen, &ctx->b_clen64, &ctx->b_coff, &ctx->b_out,
-                   &ctx->b_order, &ctx->b_retry, &ctx->b_counters, &ctx->b_ring, &ctx->b_hist, &ctx->b_table,
-                   &ctx->b_arena, &ctx->b_scan_tmp, &ctx->b_out2};
-  for (auto* b : all) release(*b);
+  release_all(ctx);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->pev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->fence_ev) cudaEventDestroy(ev);
   cudaStreamDestroy(ctx->stream);
   if (ctx->h2d_stream) cudaStreamDestroy(ctx->h2d_stream);
   if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
@@ -693,8 +896,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   // are copied to the same offsets in the device buffers, so the offsets the
   // caller gave stay valid; chunks of non-monotonic offsets just copy a wider
   // (overlapping, identical) byte range.
-  const int64_t kChunkPairs = 131072;
-  const int K = (int)std::min<int64_t>(8, std::max<int64_t>(1, n / kChunkPairs));
+  const int K = chunk_count(n);
   if ((rc = grow(ctx, ctx->b_pat, (size_t)pb))) return rc;
   if ((rc = grow(ctx, ctx->b_txt, (size_t)tb))) return rc;
   if ((rc = grow(ctx, ctx->b_poff, sizeof(int64_t) * n))) return rc;
@@ -704,6 +906,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   if ((rc = grow(ctx, ctx->b_score, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_status, sizeof(int32_t) * n))) return rc;
   if (want_cigar && (rc = grow(ctx, ctx->b_coff, sizeof(int64_t) * (n + K + 1)))) return rc;
+  alloc_fence(ctx);  // the copy streams write the buffers just grown
   std::vector<int64_t> cs((size_t)K + 1);  // chunk boundaries (pairs)
   for (int c = 0; c <= K; ++c) cs[(size_t)c] = n * c / K;
   std::vector<cudaEvent_t> ev_up((size_t)K), ev_done((size_t)K), ev_down((size_t)K);
@@ -917,6 +1120,22 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
     CU(cudaMemcpy(hs.data(), d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
   }
   return collect_status(ctx, hs.data(), n);
+}
+
+int tsu_predict_bytes(tsu_ctx* ctx, const tsu_batch* b, uint32_t flags, size_t* full, size_t* min) {
+  if (!ctx || !full || !min) return TSU_EINVAL;
+  BatchInfo bi;
+  int64_t pb = 0, tb = 0;
+  int rc = check_batch_host(ctx, b, &bi, &pb, &tb);
+  if (rc) return rc;
+  CU(cudaSetDevice(ctx->device));
+  tsu::engine::BatchShape sh;
+  sh.n = bi.n;
+  sh.plen = b->pattern_len;
+  sh.tlen = b->text_len;
+  sh.pattern_bytes = pb;
+  sh.text_bytes = tb;
+  return tsu::engine::predict_bytes(ctx, sh, flags, full, min);
 }
 
 int64_t tsu_cigar_to_ops(const uint32_t* runs, int64_t nruns, char* out, int64_t cap) {

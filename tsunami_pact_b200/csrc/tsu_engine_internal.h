@@ -1,0 +1,45 @@
+// tsu_engine_internal.h -- engine calls used by the request server
+// (tsu_server.cpp).  Not part of the C ABI: C++ linkage, library-internal.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/tsunami_b200.h"
+
+namespace tsu {
+namespace engine {
+
+// Lengths of the pairs of a planned batch (host memory).
+struct BatchShape {
+  int64_t n = 0;
+  const int32_t* plen = nullptr;
+  const int32_t* tlen = nullptr;
+  int64_t pattern_bytes = 0;  // bytes tsu_align_batch copies up (max offset + length)
+  int64_t text_bytes = 0;
+};
+
+// Device bytes tsu_align_batch(ctx, batch, flags) will hold at its peak:
+// inputs, packed words, outputs, CIGAR arena and the largest length band's
+// wavefront scratch at the context's edit-rate hint.  *full: every pair of a
+// band in flight at once (up to what the SMs hold); *min: one pair in flight
+// per band (the engine plans fewer pairs in flight when its budget is
+// smaller than *full, and fails only below *min).
+int predict_bytes(tsu_ctx* ctx, const BatchShape& shape, uint32_t flags, size_t* full, size_t* min);
+
+// Device bytes the context holds now.
+size_t held_bytes(const tsu_ctx* ctx);
+// Budget of the next calls (bytes), and its current value.
+void set_budget(tsu_ctx* ctx, size_t bytes);
+size_t budget_bytes(const tsu_ctx* ctx);
+// Grow buffers to exactly the size asked for (no 1.5x headroom), so a
+// context holds no more than its predicted peak.
+void set_exact_growth(tsu_ctx* ctx, bool exact);
+// Return every device buffer of the context to the pool (waits for the
+// context's streams first).
+int trim(tsu_ctx* ctx);
+// After TSU_ENOMEM: the budget the failed step needed (0 if unknown).
+size_t needed_bytes(const tsu_ctx* ctx);
+
+}  // namespace engine
+}  // namespace tsu

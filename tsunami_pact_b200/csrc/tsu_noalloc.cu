@@ -107,10 +107,13 @@ int gcd(int a, int b) {
   return a;
 }
 
+// The kernel's dynamic shared memory limit is set to the device maximum, the
+// value the engine's contexts set too, so concurrent callers never lower it
+// under each other's launches.
 template <int kMode>
-cudaError_t occupancy(int threads, size_t smem, int* occ) {
+cudaError_t occupancy(int threads, size_t smem, int optin, int* occ) {
   cudaError_t e =
-      cudaFuncSetAttribute(tsu::align_kernel<false, kMode, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(tsu::align_kernel<false, kMode, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<false, kMode, 1>, threads, smem);
 }
@@ -208,8 +211,8 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
                                                  pass == 0 ? tsu::kModeShared : tsu::kModeGlobal, 1, 0.2, false,
                                                  smem_optin);
     int occ = 0;
-    NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.group_smem, &occ)
-                                       : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.group_smem, &occ));
+    NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ)
+                                       : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ));
     if (occ < 1) return TSU_EDEVICE;
     int64_t warps = std::min<int64_t>((int64_t)sms * occ * wpb, n_order);
     if (geo.mode == tsu::kModeGlobal)

@@ -1,0 +1,173 @@
+// tsu_server.cpp -- C ABI of the request server (include/tsunami_b200.h):
+// the scheduler of tsu_serve.h over engine contexts.
+//
+// Each worker is one tsu_ctx (its own streams and device buffers, growing to
+// exactly the size asked, from the device's stream-ordered pool) driven by
+// its own host thread through tsu_align_batch -- the batch path, so a served
+// request gets the kernels, the length bands and the retry ladder of a batch
+// call.  A further context (no buffers) predicts the device memory of
+// requests and jobs.
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/tsunami_b200.h"
+#include "tsu_engine_internal.h"
+#include "tsu_serve.h"
+
+namespace {
+
+using tsu::serve::Output;
+using tsu::serve::Pairs;
+
+class EngineExecutor final : public tsu::serve::Executor {
+ public:
+  explicit EngineExecutor(tsu_ctx* ctx) : ctx_(ctx) { tsu::engine::set_exact_growth(ctx_, true); }
+  ~EngineExecutor() override { tsu_destroy(ctx_); }
+
+  int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t flags,
+              size_t* full, size_t* min) override {
+    tsu::engine::BatchShape sh;
+    sh.n = n;
+    sh.plen = plen;
+    sh.tlen = tlen;
+    sh.pattern_bytes = pb;
+    sh.text_bytes = tb;
+    return tsu::engine::predict_bytes(ctx_, sh, flags, full, min);
+  }
+  size_t held() override { return tsu::engine::held_bytes(ctx_); }
+  void set_budget(size_t bytes) override { tsu::engine::set_budget(ctx_, bytes); }
+  int trim() override { return tsu::engine::trim(ctx_); }
+  size_t needed() override { return tsu::engine::needed_bytes(ctx_); }
+  std::string error() override { return tsu_last_error(ctx_); }
+
+  int run(const Pairs& in, uint32_t flags, Output* out) override {
+    const int64_t n = in.n();
+    const bool cig = !(flags & TSU_SCORE_ONLY);
+    out->score.assign((size_t)n, 0);
+    out->pair_status.assign((size_t)n, -1);
+    int64_t cap = 1;  // a pair has at most m + n runs
+    for (int64_t i = 0; i < n; ++i) cap += (int64_t)in.plen[(size_t)i] + in.tlen[(size_t)i];
+    if (cig) {
+      out->coff.assign((size_t)n + 1, 0);
+      out->cigar.resize((size_t)cap);
+    }
+    tsu_batch b = in.view();
+    tsu_result r{};
+    r.score = out->score.data();
+    r.pair_status = out->pair_status.data();
+    if (cig) {
+      r.cigar = out->cigar.data();
+      r.cigar_capacity = cap;
+      r.cigar_offset = out->coff.data();
+    }
+    const int rc = tsu_align_batch(ctx_, &b, &r, flags & TSU_SCORE_ONLY);
+    if (rc == TSU_OK && cig) out->cigar.resize((size_t)r.cigar_needed);
+    return rc;
+  }
+
+ private:
+  tsu_ctx* ctx_;
+};
+
+int make_ctx(const tsu_penalties* pen, int device, double hint, size_t budget, tsu_ctx** out) {
+  tsu_config c{};
+  c.device = device;
+  c.mem_budget = budget;
+  c.max_error_hint = hint;
+  return tsu_create(pen, &c, out);
+}
+
+}  // namespace
+
+struct tsu_server {
+  std::unique_ptr<tsu::serve::Server> s;
+  std::string err;
+};
+
+extern "C" {
+
+int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, tsu_server** out) {
+  if (!pen || !out) return TSU_EINVAL;
+  *out = nullptr;
+  tsu_server_config c{};
+  if (cfg) c = *cfg;
+  if (c.workers < 0 || c.workers > 256 || c.max_queue < 0 || c.max_job_pairs < 0 || c.max_job_requests < 0 ||
+      c.watchdog_ms < 0 || c.max_error_hint < 0)
+    return TSU_EINVAL;
+  tsu::serve::Config sc;
+  sc.workers = c.workers ? c.workers : 4;
+  sc.max_queue = c.max_queue ? c.max_queue : (1 << 16);
+  sc.max_job_pairs = c.max_job_pairs ? c.max_job_pairs : 16384;
+  sc.max_job_requests = c.max_job_requests ? c.max_job_requests : 64;
+  sc.watchdog_ms = c.watchdog_ms;
+  sc.resident_cap = c.resident_bytes;
+  // the planner context: no buffers; its create resolves the default budget
+  tsu_ctx* planner = nullptr;
+  int rc = make_ctx(pen, c.device, c.max_error_hint, c.mem_budget, &planner);
+  if (rc) return rc;
+  std::unique_ptr<tsu::serve::Executor> plan(new EngineExecutor(planner));
+  sc.budget = tsu::engine::budget_bytes(planner);  // mem_budget, or 80% of the free memory when 0
+  std::vector<std::unique_ptr<tsu::serve::Executor>> ws;
+  for (int i = 0; i < sc.workers; ++i) {
+    tsu_ctx* ctx = nullptr;
+    rc = make_ctx(pen, c.device, c.max_error_hint, sc.budget, &ctx);
+    if (rc) return rc;  // unique_ptrs destroy the contexts made so far
+    ws.emplace_back(new EngineExecutor(ctx));
+  }
+  auto* srv = new tsu_server();
+  srv->s = std::make_unique<tsu::serve::Server>(sc, std::move(ws), std::move(plan));
+  *out = srv;
+  return TSU_OK;
+}
+
+int tsu_server_destroy(tsu_server* srv) {
+  if (!srv) return TSU_EINVAL;
+  srv->s->shutdown();
+  srv->s.reset();
+  delete srv;
+  return TSU_OK;
+}
+
+int tsu_submit(tsu_server* srv, const tsu_batch* request, uint32_t flags, uint64_t* id) {
+  if (!srv) return TSU_EINVAL;
+  return srv->s->submit(request, flags, id);
+}
+
+int tsu_poll(tsu_server* srv, uint64_t id, tsu_result* res, tsu_request_info* info) {
+  if (!srv) return TSU_EINVAL;
+  return srv->s->poll(id, res, info);
+}
+
+int tsu_wait(tsu_server* srv, uint64_t id, double timeout_ms, tsu_result* res, tsu_request_info* info) {
+  if (!srv) return TSU_EINVAL;
+  return srv->s->wait(id, timeout_ms, res, info);
+}
+
+int tsu_cancel(tsu_server* srv, uint64_t id) {
+  if (!srv) return TSU_EINVAL;
+  return srv->s->cancel(id);
+}
+
+int tsu_server_get_stats(tsu_server* srv, tsu_server_stats* out) {
+  if (!srv || !out) return TSU_EINVAL;
+  srv->s->stats(out);
+  return TSU_OK;
+}
+
+int tsu_server_reset_stats(tsu_server* srv) {
+  if (!srv) return TSU_EINVAL;
+  srv->s->reset_stats();
+  return TSU_OK;
+}
+
+const char* tsu_server_last_error(tsu_server* srv) {
+  if (!srv) return "null server";
+  static thread_local std::string msg;
+  msg = srv->s->error();
+  return msg.c_str();
+}
+
+}  // extern "C"

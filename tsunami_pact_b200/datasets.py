@@ -69,3 +69,15 @@ def length_buckets(lengths: np.ndarray) -> np.ndarray:
     """floor(log2(L)) per pair: the buckets of the one-launch-per-uniform-batch
     (plain) form."""
     return np.floor(np.log2(np.maximum(lengths, 1))).astype(np.int32)
+
+
+def c5_stream(n_requests: int, rate_per_s: float, index: int = 0, max_pairs: int = 256):
+    """A serving stream: arrival times in seconds (Poisson process of
+    rate_per_s, the first at 0) and request sizes (uniform 1..max_pairs
+    pairs) of n_requests requests.  Pairs are drawn from the c5 mixture in
+    order (request k takes the next sizes[k] pairs)."""
+    r = _rng(5 + index)
+    gaps = r.exponential(1.0 / rate_per_s, n_requests)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    sizes = r.integers(1, max_pairs + 1, n_requests).astype(np.int64)
+    return arrivals, sizes
