@@ -170,7 +170,8 @@ def run_serving(args):
 
     rates = [float(x) for x in args.rates.split(",") if x]
     budget = int(args.budget_gb * (1 << 30))
-    srv = T.Server(*PEN, workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2)
+    srv = T.Server(*PEN, workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2,
+                   estimate_hint=not args.no_estimate)
 
     def stream(index, n_req, rate):
         arrivals, sizes = D.c5_stream(n_req, rate, index=index)
@@ -228,7 +229,8 @@ def run_serving(args):
             "config": {"workload": "c5 serving: Poisson arrivals, requests of U{1..256} pairs, mixture 70% 150 bp "
                                    "@1-3%, 25% 1-5 kbp @5-10%, 5% 10-50 kbp @10-20%, penalties 4/6/2",
                        "offered_rate_rps": rate, "requests": len(reqs), "pairs": int(sizes.sum()),
-                       "workers": args.workers, "budget_gb": st["budget_bytes"] / 2**30},
+                       "workers": args.workers, "budget_gb": st["budget_bytes"] / 2**30,
+                       "long_pair_memory": "max_error_hint" if args.no_estimate else "k-mer estimate"},
             "offered_pairs_s": float(sizes.sum()) / max(float(arrivals[-1]), 1e-9),
             "gcups": cells / wall / 1e9,
             "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "p999": st["p999_ms"], "mean": st["mean_ms"],
@@ -302,7 +304,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain form (c4)")
     ap.add_argument("--rates", default="25,50,100,200", help="c5: offered request rates (requests/s)")
     ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
-    ap.add_argument("--workers", type=int, default=4, help="c5: server workers")
+    ap.add_argument("--workers", type=int, default=48, help="c5: server workers")
+    ap.add_argument("--no-estimate", action="store_true", help="c5: size long pairs by --hint, not by estimate")
     ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
     args = ap.parse_args()
     if args.workload == "c5":

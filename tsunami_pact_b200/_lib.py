@@ -55,8 +55,8 @@ class Timing(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", c_i32), ("workers", c_i32), ("mem_budget", ctypes.c_size_t),
                 ("max_error_hint", ctypes.c_double), ("max_queue", c_i64), ("max_job_pairs", c_i64),
-                ("max_job_requests", c_i32), ("reserved0", c_i32), ("watchdog_ms", ctypes.c_double),
-                ("resident_bytes", ctypes.c_size_t)]
+                ("max_job_requests", c_i32), ("heavy_len", c_i32), ("heavy_workers", c_i32), ("estimate_hint", c_i32),
+                ("watchdog_ms", ctypes.c_double), ("resident_bytes", ctypes.c_size_t)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -306,12 +306,13 @@ class Server:
 
     def __init__(self, mismatch: int = 4, gap_opening: int = 6, gap_extension: int = 2, device: int = 0,
                  workers: int = 0, mem_budget: int = 0, max_error_hint: float = 0.0, max_queue: int = 0,
-                 max_job_pairs: int = 0, max_job_requests: int = 0, watchdog_ms: float = 0.0,
-                 resident_bytes: int = 0):
+                 max_job_pairs: int = 0, max_job_requests: int = 0, heavy_len: int = 0, heavy_workers: int = 0,
+                 estimate_hint: bool = True, watchdog_ms: float = 0.0, resident_bytes: int = 0):
         L = lib()
         pen = Penalties(mismatch, gap_opening, gap_extension)
         cfg = ServerConfig(device, workers, mem_budget, max_error_hint, max_queue, max_job_pairs,
-                           max_job_requests, 0, watchdog_ms, resident_bytes)
+                           max_job_requests, heavy_len, heavy_workers, 0 if estimate_hint else -1, watchdog_ms,
+                           resident_bytes)
         h = c_vp()
         rc = L.tsu_server_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
         if rc != TSU_OK:

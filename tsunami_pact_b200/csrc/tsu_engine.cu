@@ -69,6 +69,7 @@ struct tsu_ctx {
   cudaEvent_t fence_ev[2] = {};  // orders frees after the copy streams' queued work
   cudaMemPool_t pool = nullptr;  // the device's buffer pool
   bool exact_grow = false;       // grow buffers to the asked size only
+  bool fit_start = false;        // start rungs by the hint's predicted width (tsu::fit_start)
   size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
@@ -317,10 +318,11 @@ int plan_pass_within(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::Pa
 }
 
 // plan_pass_within with the budget left beside the context's other buffers
-// (the scratch buffers are regrown for the pass: their current size is free).
+// (the scratch buffers are regrown for the pass: their current size is free)
+// and `reserve` bytes that later steps of the call still need.
 int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint, bool want_cigar,
-              Pass* out) {
-  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap;
+              size_t reserve, Pass* out) {
+  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap + reserve;
   const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
   return plan_pass_within(ctx, bi, n_pairs, pc, hint, want_cigar, avail, out);
 }
@@ -421,7 +423,20 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     arena_cap = std::min<int64_t>(arena_cap, (int64_t)(room / 8));  // leave half for scratch
     if ((rc = grow(ctx, ctx->b_arena, sizeof(uint32_t) * (size_t)std::max<int64_t>(arena_cap, 1024)))) return rc;
     arena_cap = (int64_t)(ctx->b_arena.cap / sizeof(uint32_t));
+    // run lengths of the compaction, allocated before the passes' scratch
+    if ((rc = grow(ctx, ctx->b_clen64, sizeof(int64_t) * (n + 1)))) return rc;
   }
+  // The compacted runs (at most the arena's, at most m + n per pair) are
+  // allocated after the passes: each pass's scratch leaves room for them.
+  int64_t len_sum = 0;
+  for (int64_t i = 0; h_plen && i < n; ++i) len_sum += (int64_t)h_plen[i] + h_tlen[i];
+  if (!h_plen) len_sum = n * ((int64_t)bi.max_m + bi.max_n);
+  auto out_reserve = [&]() -> size_t {
+    if (!want_cigar || d_out_runs) return 0;
+    const DevBuf& ob = out_buf ? *out_buf : ctx->b_out;
+    const size_t need = (sizeof(uint32_t) * (size_t)std::min<int64_t>(arena_cap, len_sum + 1) + 255) & ~(size_t)255;
+    return need > ob.cap ? need - ob.cap : 0;
+  };
   unsigned int* d_queue = P<unsigned int>(ctx->b_counters);
   unsigned int* d_retry_cnt = d_queue + 1;
   unsigned long long* d_cursor = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 16);
@@ -466,11 +481,13 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     order = P<int32_t>(ctx->b_order);
     pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
   }
+  if (ctx->fit_start && !ctx->one_warp)
+    pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
   CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
   const int band_first_pass = passes;
   for (;;) {
     Pass ps;
-    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, &ps))) return rc;
+    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, out_reserve(), &ps))) return rc;
     const tsu::PassGeom& g = ps.g;
     {
       // plan_pass counted the scratch buffers as free: if any of them must
@@ -677,8 +694,9 @@ int collect_status(tsu_ctx* ctx, const int32_t* hs, int64_t n) {
 namespace tsu {
 namespace engine {
 
-int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, size_t* full, size_t* min) {
+int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hint, size_t* full, size_t* min) {
   if (!ctx || sh.n < 0 || (sh.n && (!sh.plen || !sh.tlen)) || !full || !min) return TSU_EINVAL;
+  if (hint <= 0) hint = ctx->err_hint;
   const bool want_cigar = !(flags & TSU_SCORE_ONLY);
   const bool one_warp = (flags & TSU_ONE_WARP) != 0;
   const int64_t n = sh.n;
@@ -713,7 +731,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, size_t* fu
                3 * r(4 * (size_t)nc) + r(64);
     size_t tmp = scan_tmp(2 * nc);
     if (want_cigar) {
-      const int64_t arena = std::max<int64_t>(tsu::arena_runs(ctx->x, ctx->go, nc, ci.max_m, ci.max_n, ctx->err_hint), 1024);
+      const int64_t arena = std::max<int64_t>(tsu::arena_runs(ctx->x, ctx->go, nc, ci.max_m, ci.max_n, hint), 1024);
       const int64_t out_runs = std::min<int64_t>(arena, len_sum + 1);
       f += r(4 * (size_t)arena) + r(8 * (size_t)(nc + 1)) + (K > 1 ? 2 : 1) * r(4 * (size_t)out_runs);
       tmp = std::max(tmp, scan_tmp(nc + 1));
@@ -740,8 +758,10 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, size_t* fu
         }
         pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
       }
+      if (ctx->fit_start && !one_warp)
+        pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
       Pass ps;
-      const int rc = plan_pass_within(ctx, pbi, np, pc, ctx->err_hint, want_cigar, SIZE_MAX / 4, &ps);
+      const int rc = plan_pass_within(ctx, pbi, np, pc, hint, want_cigar, SIZE_MAX / 4, &ps);
       if (rc) return rc;
       const size_t per = group_scratch_bytes(ps.g);
       scratch_full = std::max(scratch_full, (size_t)ps.groups * per);
@@ -761,6 +781,16 @@ void set_budget(tsu_ctx* ctx, size_t bytes) {
 }
 
 size_t budget_bytes(const tsu_ctx* ctx) { return ctx ? ctx->budget : 0; }
+
+void set_hint(tsu_ctx* ctx, double h) {
+  if (ctx && h > 0) ctx->err_hint = h;
+}
+
+double hint(const tsu_ctx* ctx) { return ctx ? ctx->err_hint : 0.0; }
+
+void set_fit_start(tsu_ctx* ctx, bool on) {
+  if (ctx) ctx->fit_start = on;
+}
 
 void set_exact_growth(tsu_ctx* ctx, bool exact) {
   if (ctx) ctx->exact_grow = exact;
@@ -1135,7 +1165,7 @@ int tsu_predict_bytes(tsu_ctx* ctx, const tsu_batch* b, uint32_t flags, size_t* 
   sh.tlen = b->text_len;
   sh.pattern_bytes = pb;
   sh.text_bytes = tb;
-  return tsu::engine::predict_bytes(ctx, sh, flags, full, min);
+  return tsu::engine::predict_bytes(ctx, sh, flags, 0.0, full, min);
 }
 
 int64_t tsu_cigar_to_ops(const uint32_t* runs, int64_t nruns, char* out, int64_t cap) {

@@ -21,17 +21,23 @@ struct BatchShape {
 
 // Device bytes tsu_align_batch(ctx, batch, flags) will hold at its peak:
 // inputs, packed words, outputs, CIGAR arena and the largest length band's
-// wavefront scratch at the context's edit-rate hint.  *full: every pair of a
-// band in flight at once (up to what the SMs hold); *min: one pair in flight
-// per band (the engine plans fewer pairs in flight when its budget is
-// smaller than *full, and fails only below *min).
-int predict_bytes(tsu_ctx* ctx, const BatchShape& shape, uint32_t flags, size_t* full, size_t* min);
+// wavefront scratch at edit-rate hint `hint` (0: the context's).  *full:
+// every pair of a band in flight at once (up to what the SMs hold); *min:
+// one pair in flight per band (the engine plans fewer pairs in flight when
+// its budget is smaller than *full, and fails only below *min).
+int predict_bytes(tsu_ctx* ctx, const BatchShape& shape, uint32_t flags, double hint, size_t* full, size_t* min);
 
 // Device bytes the context holds now.
 size_t held_bytes(const tsu_ctx* ctx);
 // Budget of the next calls (bytes), and its current value.
 void set_budget(tsu_ctx* ctx, size_t bytes);
 size_t budget_bytes(const tsu_ctx* ctx);
+// Edit-rate hint of the next calls (> 0), and its current value.
+void set_hint(tsu_ctx* ctx, double hint);
+double hint(const tsu_ctx* ctx);
+// Choose each band's first rung by the wavefront width the hint predicts
+// (tsu::fit_start) -- for hints estimated per pair.
+void set_fit_start(tsu_ctx* ctx, bool on);
 // Grow buffers to exactly the size asked for (no 1.5x headroom), so a
 // context holds no more than its predicted peak.
 void set_exact_growth(tsu_ctx* ctx, bool exact);

@@ -4,32 +4,41 @@
 //
 // No counterpart in the reference, which aligns one file per process
 // (wfa_gpu.cu:43-188).  Design:
-//   * submit copies a request's pairs into the server and queues it (FIFO);
+//   * submit copies a request's pairs into the server and splits them into
+//     parts: one part with its light pairs (max(m, n) < heavy_len) and one
+//     part per heavy pair.  Each part carries its predicted device memory
+//     (Executor::predict: inputs, packed words, outputs, CIGAR arena and
+//     wavefront scratch at its edit-rate hint, bounded by the
+//     penalty-derived score bound of each pair);
+//   * light parts wait in one FIFO queue, heavy parts in another;
 //   * a pool of workers, each an Executor with its own CUDA streams and
-//     device buffers, runs jobs; a job is the head request of the queue plus
-//     the requests behind it (same flags, up to max_job_pairs pairs and
-//     max_job_requests requests), aligned in one engine call -- continuous
-//     batching: requests that arrive while others run join the next job and
-//     their kernels overlap the running jobs' kernels on the device;
-//   * admission: a job starts when a worker is idle and the job's predicted
-//     device bytes (Executor::predict: inputs, packed words, outputs, CIGAR
-//     arena and wavefront scratch at the edit-rate hint, capped by the
-//     penalty-derived score bound) fit in the budget beside what the other
-//     workers were granted or still hold.  Idle workers keep their buffers
-//     (resident state) until the memory is needed elsewhere, then are
-//     trimmed.  A job that does not fit is shrunk to its head request; a
-//     head request that cannot fit even alone in an idle device is refused
-//     with TSU_ENOMEM; otherwise the head waits (strict FIFO, so large
-//     requests are not starved by small ones);
-//   * results are split per request and made visible to poll/wait; latency
-//     is measured from submit to that moment;
-//   * a job of several requests that fails is re-queued at the head as
-//     single-request jobs, so a failure stays with the request that caused
-//     it; a single request that ran out of memory is re-queued with the
-//     reservation the engine asked for (up to 3 attempts);
-//   * watchdog: a job running longer than watchdog_ms completes its
-//     requests with TSU_ETIMEOUT; the worker's late results are discarded
-//     and it takes no new job until it returns.
+//     device buffers, runs jobs.  A light job is the oldest light part plus
+//     the light parts queued behind it (same flags, up to max_job_pairs
+//     pairs and max_job_requests parts), aligned in one engine call -- so
+//     requests that arrive while others run are batched into the next job;
+//     a heavy job is one heavy pair, so its memory is sized by that pair and
+//     returned when that pair is done.  At most heavy_workers heavy jobs run
+//     at once, so light jobs always find a worker.  Jobs of different
+//     workers overlap on the device;
+//   * admission: a job starts when a worker is idle and its predicted bytes
+//     fit in the budget beside what the other workers were granted or still
+//     hold.  Idle workers keep their buffers (resident state) up to
+//     resident_cap and until the memory is needed elsewhere.  A job of
+//     several parts that does not fit is halved down to one part; a part
+//     that fits only with fewer pairs in flight runs when nothing else does;
+//     a part that cannot fit even then fails with TSU_ENOMEM.  Each queue
+//     starts its parts in order (no overtaking within a queue);
+//   * a request is done when all its parts are: its results are assembled
+//     in its own pair order and made visible to poll/wait; latency is
+//     measured from submit to that moment;
+//   * a job of several parts that fails is re-queued at the head as
+//     single-part jobs, so a failure stays with the request that caused it;
+//     a single part that ran out of memory is re-queued with the reservation
+//     the engine asked for (up to 3 attempts); a failed part fails its
+//     request and drops the request's other parts;
+//   * watchdog: a job running longer than watchdog_ms fails its requests
+//     with TSU_ETIMEOUT; the worker's late results are discarded and it
+//     takes no new job until it returns.
 // Alignment of a pair does not depend on the other pairs of its job, so a
 // request's results are the same alone and in any mix.
 #pragma once
@@ -48,9 +57,14 @@
 #include <vector>
 
 #include "../../include/tsunami_b200.h"
+#include "tsu_estimate.h"
 
 namespace tsu {
 namespace serve {
+
+// Executor flag beside TSU_SCORE_ONLY: the hint is a per-pair estimate, so
+// choose the first rung by the width it predicts (tsu::fit_start).
+constexpr uint32_t kFitStart = 0x100;
 
 using Clock = std::chrono::steady_clock;
 
@@ -91,14 +105,17 @@ struct Pairs {
     }
   }
 
-  void append(const Pairs& o) {
-    const int64_t pb = (int64_t)pat.size(), tb = (int64_t)txt.size();
-    pat.insert(pat.end(), o.pat.begin(), o.pat.end());
-    txt.insert(txt.end(), o.txt.begin(), o.txt.end());
-    for (int64_t v : o.poff) poff.push_back(v + pb);
-    for (int64_t v : o.toff) toff.push_back(v + tb);
-    plen.insert(plen.end(), o.plen.begin(), o.plen.end());
-    tlen.insert(tlen.end(), o.tlen.begin(), o.tlen.end());
+  // Append pairs idx of o.
+  void append(const Pairs& o, const std::vector<int32_t>& idx) {
+    for (int32_t i : idx) {
+      poff.push_back((int64_t)pat.size());
+      toff.push_back((int64_t)txt.size());
+      const int32_t m = o.plen[(size_t)i], n = o.tlen[(size_t)i];
+      pat.insert(pat.end(), o.pat.begin() + o.poff[(size_t)i], o.pat.begin() + o.poff[(size_t)i] + m);
+      txt.insert(txt.end(), o.txt.begin() + o.toff[(size_t)i], o.txt.begin() + o.toff[(size_t)i] + n);
+      plen.push_back(m);
+      tlen.push_back(n);
+    }
   }
 
   tsu_batch view() const {
@@ -118,54 +135,78 @@ struct Output {
 };
 
 // One worker's device side (or a fake of it).  Calls on one executor come
-// from one thread at a time.
+// from one thread at a time.  hint: the edit rate sizing wavefront scratch
+// (0: the executor's default).
 class Executor {
  public:
   virtual ~Executor() = default;
   // Predicted device bytes to align `plen`/`tlen` (n pairs, pb/tb sequence
   // bytes) in one call: every pair of a band in flight (*full) or one (*min).
   virtual int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t flags,
-                      size_t* full, size_t* min) = 0;
-  virtual size_t held() = 0;                 // device bytes held now
+                      double hint, size_t* full, size_t* min) = 0;
+  virtual size_t held() = 0;                  // device bytes held now
   virtual void set_budget(size_t bytes) = 0;  // for the next run
-  virtual int trim() = 0;                    // release every buffer
+  virtual int trim() = 0;                     // release every buffer
   // Align every pair; fills out->score and out->pair_status (and CIGARs).
-  virtual int run(const Pairs& in, uint32_t flags, Output* out) = 0;
+  virtual int run(const Pairs& in, uint32_t flags, double hint, Output* out) = 0;
   virtual size_t needed() = 0;  // after TSU_ENOMEM: the bytes the run needed (0: unknown)
   virtual std::string error() = 0;
 };
 
 struct Config {
   int workers = 4;
-  size_t budget = 0;               // device bytes for all workers
-  int64_t max_queue = 1 << 16;     // queued requests before submit says TSU_EBUSY
-  int64_t max_job_pairs = 16384;   // pairs merged into one job
-  int max_job_requests = 64;       // requests merged into one job
-  double watchdog_ms = 0;          // 0: off
-  size_t resident_cap = 0;         // bytes an idle worker may keep (0: budget / (2 * workers))
+  size_t budget = 0;              // device bytes for all workers
+  int64_t max_queue = 1 << 16;    // queued requests before submit says TSU_EBUSY
+  int64_t max_job_pairs = 16384;  // pairs merged into one light job
+  int max_job_requests = 64;      // parts merged into one light job
+  double watchdog_ms = 0;         // 0: off
+  size_t resident_cap = 0;        // bytes an idle worker may keep (0: budget / (2 * workers))
+  int32_t heavy_len = 16384;      // max(m, n) from which a pair is a part of its own (0: never)
+  int heavy_workers = 0;          // heavy jobs at once (0: workers - 1, at least 1)
+  double hint = 0;                // edit-rate hint of light parts (0: the executor's default)
+  bool estimate = true;           // heavy pairs: hint from their shared k-mers (tsu_estimate.h)
 };
+
+struct Request;
+using ReqPtr = std::shared_ptr<Request>;
+
+// A request's pairs idx, run as (part of) a job.
+struct Part {
+  ReqPtr req;
+  std::vector<int32_t> idx;
+  bool heavy = false;
+  bool alone = false;  // run as a job of its own (after a job-level failure)
+  int attempts = 0;
+  double hint = 0;
+  uint32_t flags = 0;        // executor flags: the request's, plus kFitStart
+  size_t full = 0, min = 0;  // predicted bytes alone
+  int64_t pairs() const { return (int64_t)idx.size(); }
+};
+using PartPtr = std::shared_ptr<Part>;
 
 struct Request {
   uint64_t id = 0;
   Pairs in;
   uint32_t flags = 0;
-  size_t full = 0, min = 0;  // predicted bytes alone
   enum State { kQueued, kRunning, kDone } state = kQueued;
   bool cancelled = false;
-  bool alone = false;  // run as a job of its own (after a job-level failure)
-  int attempts = 0;
-  int job_requests = 0;
-  int64_t job_seq = 0;
+  int parts_left = 0;
+  int attempts = 0;      // most attempts of any part
+  int job_requests = 0;  // most parts in a job that delivered one of its parts
+  int64_t job_seq = 0;   // job that started its first part
   Clock::time_point t_submit, t_start, t_done;
+  bool started = false;
+  std::vector<std::pair<PartPtr, Output>> done_parts;
   Output out;
 };
-using ReqPtr = std::shared_ptr<Request>;
 
 class Server {
  public:
   Server(const Config& cfg, std::vector<std::unique_ptr<Executor>> workers, std::unique_ptr<Executor> planner)
       : cfg_(cfg), planner_(std::move(planner)) {
-    if (cfg_.resident_cap == 0) cfg_.resident_cap = cfg_.budget / (2 * std::max<size_t>(1, workers.size()));
+    const size_t nw = std::max<size_t>(1, workers.size());
+    if (cfg_.resident_cap == 0) cfg_.resident_cap = cfg_.budget / (2 * nw);
+    if (cfg_.heavy_workers <= 0 || cfg_.heavy_workers > (int)nw - 1) cfg_.heavy_workers = std::max(1, (int)nw - 1);
     t_reset_ = Clock::now();
     for (size_t i = 0; i < workers.size(); ++i) {
       auto w = std::make_unique<Worker>();
@@ -180,18 +221,15 @@ class Server {
 
   ~Server() { shutdown(); }
 
-  // Cancel queued requests, let running jobs finish, stop the threads.
+  // Drop queued requests, let running jobs finish, stop the threads.
   void shutdown() {
     {
       std::lock_guard<std::mutex> lk(mu_);
       if (stopped_) return;
       stopping_ = true;
-      for (auto& r : queue_) {
-        r->state = Request::kDone;
-        r->out.status = TSU_EBUSY;
-        r->t_done = Clock::now();
-      }
-      queue_.clear();
+      std::vector<PartPtr> queued(light_.begin(), light_.end());
+      queued.insert(queued.end(), heavy_.begin(), heavy_.end());
+      for (auto& p : queued) fail_request(*p->req, TSU_EBUSY, Clock::now());  // empties the queues
     }
     cv_sched_.notify_all();
     cv_work_.notify_all();
@@ -217,20 +255,52 @@ class Server {
     r->t_submit = Clock::now();
     r->flags = flags & TSU_SCORE_ONLY;
     r->in.assign(*b);
-    if (r->in.n()) {
-      std::lock_guard<std::mutex> pl(plan_mu_);
-      const int rc = planner_->predict(r->in.n(), r->in.plen.data(), r->in.tlen.data(), (int64_t)r->in.pat.size(),
-                                       (int64_t)r->in.txt.size(), r->flags, &r->full, &r->min);
+    // parts: each heavy pair alone (longest first), then the light pairs
+    std::vector<PartPtr> parts;
+    auto light = std::make_shared<Part>();
+    for (int32_t i = 0; i < (int32_t)r->in.n(); ++i) {
+      const int32_t L = std::max(r->in.plen[(size_t)i], r->in.tlen[(size_t)i]);
+      if (cfg_.heavy_len > 0 && L >= cfg_.heavy_len) {
+        auto h = std::make_shared<Part>();
+        h->heavy = true;
+        h->idx.push_back(i);
+        parts.push_back(h);
+      } else {
+        light->idx.push_back(i);
+      }
+    }
+    std::stable_sort(parts.begin(), parts.end(), [&](const PartPtr& a, const PartPtr& c) {
+      const int32_t i = a->idx[0], j = c->idx[0];
+      return (int64_t)r->in.plen[(size_t)i] + r->in.tlen[(size_t)i] >
+             (int64_t)r->in.plen[(size_t)j] + r->in.tlen[(size_t)j];
+    });
+    if (!light->idx.empty()) parts.push_back(light);
+    for (auto& p : parts) {
+      p->req = r;
+      p->hint = cfg_.hint;
+      p->flags = r->flags;
+      if (p->heavy && cfg_.estimate) {
+        const int32_t i = p->idx[0];
+        const double e = estimate_edit_rate(r->in.pat.data() + r->in.poff[(size_t)i], r->in.plen[(size_t)i],
+                                            r->in.txt.data() + r->in.toff[(size_t)i], r->in.tlen[(size_t)i]);
+        if (e >= 0) {
+          p->hint = std::min(1.0, std::max(0.02, 1.3 * e + 0.01));
+          p->flags |= kFitStart;
+        }
+      }
+      const int rc = predict_parts({p}, p->flags, p->hint, &p->full, &p->min);
       if (rc) return rc;
     }
     std::lock_guard<std::mutex> lk(mu_);
     if (stopping_) return TSU_EBUSY;
-    if (r->min > cfg_.budget) {
-      ++st_rejected_;
-      err_ = "request needs " + std::to_string(r->min) + " B of device memory, budget " + std::to_string(cfg_.budget);
-      return TSU_ENOMEM;
-    }
-    if ((int64_t)queue_.size() >= cfg_.max_queue) {
+    for (auto& p : parts)
+      if (p->min > cfg_.budget) {
+        ++st_rejected_;
+        err_ = "request needs " + std::to_string(p->min) + " B of device memory for " + std::to_string(p->pairs()) +
+               " pair(s), budget " + std::to_string(cfg_.budget);
+        return TSU_ENOMEM;
+      }
+    if (waiting_ >= cfg_.max_queue) {
       ++st_rejected_;
       err_ = "queue full";
       return TSU_EBUSY;
@@ -239,14 +309,17 @@ class Server {
     *id = r->id;
     ++st_submitted_;
     reqs_[r->id] = r;
-    if (r->in.n() == 0) {  // nothing to align
+    if (parts.empty()) {  // nothing to align
       r->state = Request::kDone;
       r->t_start = r->t_done = r->t_submit;
       record_done(*r);
       cv_done_.notify_all();
       return TSU_OK;
     }
-    queue_.push_back(r);
+    r->parts_left = (int)parts.size();
+    ++open_;
+    ++waiting_;
+    for (auto& p : parts) (p->heavy ? heavy_ : light_).push_back(p);
     cv_sched_.notify_one();
     return TSU_OK;
   }
@@ -275,20 +348,15 @@ class Server {
     return take(id, res, info);
   }
 
-  // Queued: removed.  Running: its results are dropped when the job ends.
-  // Done: forgotten.
+  // Queued: never runs.  Running: its results are dropped.  Done: forgotten.
   int cancel(uint64_t id) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = reqs_.find(id);
     if (it == reqs_.end()) return TSU_ENOTFOUND;
     ReqPtr r = it->second;
     reqs_.erase(it);
-    if (r->state == Request::kQueued) {
-      queue_.erase(std::remove(queue_.begin(), queue_.end(), r), queue_.end());
-      r->state = Request::kDone;
-      r->out.status = TSU_EBUSY;
-    }
     r->cancelled = true;
+    fail_request(*r, TSU_EBUSY, Clock::now());
     ++st_cancelled_;
     cv_sched_.notify_one();
     return TSU_OK;
@@ -303,11 +371,13 @@ class Server {
     s->rejected = st_rejected_;
     s->cancelled = st_cancelled_;
     s->timed_out = st_timed_out_;
-    s->queued = (int64_t)queue_.size();
-    for (auto& w : workers_) s->running += w->busy ? (int64_t)w->job.size() : 0;
+    int64_t running = 0;
+    for (auto& kv : reqs_) running += kv.second->state == Request::kRunning;
+    s->running = running;
+    s->queued = waiting_;
     s->jobs = st_jobs_;
     s->pairs_completed = st_pairs_;
-    s->mean_requests_per_job = st_jobs_ ? (double)st_job_reqs_ / (double)st_jobs_ : 0.0;
+    s->mean_requests_per_job = st_jobs_ ? (double)st_job_parts_ / (double)st_jobs_ : 0.0;
     std::vector<double> v = lat_;
     if (!v.empty()) {
       auto pct = [&](double q) {
@@ -336,7 +406,7 @@ class Server {
   void reset_stats() {
     std::lock_guard<std::mutex> lk(mu_);
     st_submitted_ = st_completed_ = st_failed_ = st_rejected_ = st_cancelled_ = st_timed_out_ = 0;
-    st_jobs_ = st_job_reqs_ = st_pairs_ = 0;
+    st_jobs_ = st_job_parts_ = st_pairs_ = 0;
     lat_.clear();
     peak_granted_ = granted();
     t_reset_ = Clock::now();
@@ -353,9 +423,11 @@ class Server {
     std::unique_ptr<Executor> ex;
     std::thread th;
     bool busy = false;   // a job is assigned
-    bool stuck = false;  // the watchdog completed its requests
+    bool heavy = false;  // the job is a heavy one
+    bool stuck = false;  // the watchdog failed its requests
     size_t grant = 0;    // bytes granted to the running job, or held while idle
-    std::vector<ReqPtr> job;
+    double hint = 0;
+    std::vector<PartPtr> job;
     Clock::time_point started;
   };
 
@@ -363,6 +435,21 @@ class Server {
     size_t g = 0;
     for (auto& w : workers_) g += w->grant;
     return g;
+  }
+
+  int predict_parts(const std::vector<PartPtr>& parts, uint32_t flags, double hint, size_t* full, size_t* min) {
+    std::vector<int32_t> pl, tl;
+    int64_t pb = 0, tb = 0;
+    for (auto& p : parts)
+      for (int32_t i : p->idx) {
+        const Pairs& in = p->req->in;
+        pl.push_back(in.plen[(size_t)i]);
+        tl.push_back(in.tlen[(size_t)i]);
+        pb += in.plen[(size_t)i];
+        tb += in.tlen[(size_t)i];
+      }
+    std::lock_guard<std::mutex> lk(plan_mu_);
+    return planner_->predict((int64_t)pl.size(), pl.data(), tl.data(), pb, tb, flags, hint, full, min);
   }
 
   void record_done(Request& r) {
@@ -375,6 +462,61 @@ class Server {
     } else {
       ++st_failed_;
     }
+  }
+
+  void drop_queued_parts(const Request& r) {
+    for (auto* q : {&light_, &heavy_})
+      q->erase(std::remove_if(q->begin(), q->end(), [&](const PartPtr& p) { return p->req.get() == &r; }), q->end());
+  }
+
+  // A request fails (mu_ held): its queued parts are dropped, running ones
+  // are ignored when they return.
+  void fail_request(Request& r, int status, Clock::time_point now) {
+    if (r.state == Request::kDone) return;
+    drop_queued_parts(r);
+    --open_;
+    if (!r.started) --waiting_;
+    r.state = Request::kDone;
+    r.out = Output{};
+    r.out.status = status;
+    r.done_parts.clear();
+    r.t_done = now;
+    if (!r.started) r.t_start = now;
+    if (!r.cancelled) record_done(r);
+  }
+
+  // All parts done (mu_ held): scatter the parts' results into the
+  // request's pair order.
+  void assemble(Request& r) {
+    const int64_t n = r.in.n();
+    const bool cig = !(r.flags & TSU_SCORE_ONLY);
+    r.out = Output{};
+    r.out.score.assign((size_t)n, 0);
+    r.out.pair_status.assign((size_t)n, -1);
+    std::vector<const uint32_t*> run_ptr(cig ? (size_t)n : 0, nullptr);
+    std::vector<int64_t> run_len(cig ? (size_t)n : 0, 0);
+    for (auto& po : r.done_parts) {
+      const Part& p = *po.first;
+      const Output& o = po.second;
+      for (size_t k = 0; k < p.idx.size(); ++k) {
+        const size_t i = (size_t)p.idx[k];
+        r.out.score[i] = o.score[k];
+        r.out.pair_status[i] = o.pair_status[k];
+        if (cig) {
+          run_ptr[i] = o.cigar.data() + o.coff[k];
+          run_len[i] = o.coff[k + 1] - o.coff[k];
+        }
+      }
+    }
+    if (cig) {
+      r.out.coff.assign((size_t)n + 1, 0);
+      for (int64_t i = 0; i < n; ++i) r.out.coff[(size_t)i + 1] = r.out.coff[(size_t)i] + run_len[(size_t)i];
+      r.out.cigar.resize((size_t)r.out.coff[(size_t)n]);
+      for (int64_t i = 0; i < n; ++i)
+        if (run_len[(size_t)i])
+          memcpy(r.out.cigar.data() + r.out.coff[(size_t)i], run_ptr[(size_t)i], sizeof(uint32_t) * (size_t)run_len[(size_t)i]);
+    }
+    r.done_parts.clear();
   }
 
   int take(uint64_t id, tsu_result* res, tsu_request_info* info) {
@@ -417,7 +559,11 @@ class Server {
   void sched_loop() {
     std::unique_lock<std::mutex> lk(mu_);
     for (;;) {
-      while (!stopping_ && admit_one()) {
+      for (;;) {
+        if (stopping_) break;
+        const bool a = admit(light_);
+        const bool b = admit(heavy_);
+        if (!a && !b) break;
       }
       if (stopping_) break;
       watchdog();
@@ -433,13 +579,9 @@ class Server {
     for (auto& w : workers_) {
       if (!w->busy || w->stuck || ms_between(w->started, now) <= cfg_.watchdog_ms) continue;
       w->stuck = true;
-      for (auto& r : w->job) {
-        if (r->state == Request::kDone) continue;
-        r->state = Request::kDone;
-        r->out = Output{};
-        r->out.status = TSU_ETIMEOUT;
-        r->t_done = now;
-        record_done(*r);
+      for (auto& p : w->job) {
+        if (p->req->state == Request::kDone) continue;
+        fail_request(*p->req, TSU_ETIMEOUT, now);
         any = true;
       }
       err_ = "watchdog: job on worker " + std::to_string(w->idx) + " exceeded " + std::to_string(cfg_.watchdog_ms) + " ms";
@@ -447,38 +589,59 @@ class Server {
     if (any) cv_done_.notify_all();
   }
 
-  // Start one job if possible (mu_ held).  Returns whether anything changed.
-  bool admit_one() {
-    while (!queue_.empty() && queue_.front()->cancelled) queue_.pop_front();
-    if (queue_.empty()) return false;
+  size_t avail_for(const Worker* x) const {
+    size_t others = 0;
+    for (auto& v : workers_)
+      if (v.get() != x) others += v->grant;
+    return cfg_.budget > others ? cfg_.budget - others : 0;
+  }
+
+  void trim_worker(Worker* w) {
+    if (w->busy) return;
+    w->ex->trim();
+    w->grant = w->ex->held();
+  }
+
+  // Start the head job of queue q if possible (mu_ held).  Returns whether
+  // anything changed.
+  bool admit(std::deque<PartPtr>& q) {
+    while (!q.empty() && q.front()->req->state == Request::kDone) q.pop_front();  // failed or cancelled
+    if (q.empty()) {
+      if (drain_for_ == &q) drain_for_ = nullptr;
+      return false;
+    }
+    if (drain_for_ && drain_for_ != &q) return false;
+    const bool heavy = &q == &heavy_;
+    if (heavy) {
+      int running = 0;
+      for (auto& v : workers_) running += v->busy && v->heavy;
+      if (running >= cfg_.heavy_workers) return false;
+    }
     Worker* w = nullptr;
     for (auto& v : workers_)
       if (!v->busy && (!w || v->grant > w->grant)) w = v.get();  // reuse the most resident memory
     if (!w) return false;
-    ReqPtr head = queue_.front();
-    // candidate job: the head and the requests behind it
+    PartPtr head = q.front();
+    const uint32_t flags = head->flags;
     size_t take = 1;
-    if (!head->alone) {
-      int64_t pairs = head->in.n();
-      while (take < queue_.size() && (int)take < cfg_.max_job_requests) {
-        const ReqPtr& r = queue_[take];
-        if (r->alone || r->cancelled || r->flags != head->flags || pairs + r->in.n() > cfg_.max_job_pairs) break;
-        pairs += r->in.n();
+    if (!heavy && !head->alone) {
+      int64_t pairs = head->pairs();
+      while (take < q.size() && (int)take < cfg_.max_job_requests) {
+        const PartPtr& p = q[take];
+        if (p->alone || p->req->state == Request::kDone || p->flags != flags ||
+            pairs + p->pairs() > cfg_.max_job_pairs)
+          break;
+        pairs += p->pairs();
         ++take;
       }
     }
-    auto avail_for = [&](Worker* x) {
-      size_t others = 0;
-      for (auto& v : workers_)
-        if (v.get() != x) others += v->grant;
-      return cfg_.budget > others ? cfg_.budget - others : 0;
-    };
     size_t full = 0, min = 0;
     for (;;) {
       if (take == 1) {
         full = head->full;
         min = head->min;
-      } else if (!predict_job(take, &full, &min)) {
+      } else if (predict_parts(std::vector<PartPtr>(q.begin(), q.begin() + (long)take), flags, head->hint, &full,
+                               &min) != TSU_OK) {
         take = 1;
         continue;
       }
@@ -506,72 +669,56 @@ class Server {
         take = std::max<size_t>(1, take / 2);
         continue;
       }
-      // the head alone does not fit at full concurrency
+      // one part that does not fit at full concurrency
       bool others_busy = false;
       for (auto& v : workers_) others_busy |= v->busy;
-      if (!others_busy) {
-        trim_worker(w);
-        avail = avail_for(w);
-        if (min <= avail) {
-          full = avail;  // run with fewer pairs in flight
-          break;
-        }
-        // cannot fit even in an idle device
-        queue_.pop_front();
-        head->state = Request::kDone;
-        head->out = Output{};
-        head->out.status = TSU_ENOMEM;
-        head->t_start = head->t_done = Clock::now();
-        record_done(*head);
-        err_ = "request " + std::to_string(head->id) + " needs " + std::to_string(min) + " B, budget " +
-               std::to_string(cfg_.budget);
-        cv_done_.notify_all();
-        return true;
+      if (others_busy) {
+        drain_for_ = &q;  // let the device drain, then run it alone
+        return false;
       }
-      return false;  // wait for running jobs to finish
+      drain_for_ = nullptr;
+      trim_worker(w);
+      avail = avail_for(w);
+      if (min <= avail) {
+        full = avail;  // run with fewer pairs in flight
+        break;
+      }
+      q.pop_front();  // cannot fit even in an idle device
+      err_ = "request " + std::to_string(head->req->id) + " needs " + std::to_string(min) + " B, budget " +
+             std::to_string(cfg_.budget);
+      fail_request(*head->req, TSU_ENOMEM, Clock::now());
+      cv_done_.notify_all();
+      return true;
     }
     // assign
+    if (drain_for_ == &q) drain_for_ = nullptr;
     const auto now = Clock::now();
     w->busy = true;
+    w->heavy = heavy;
     w->stuck = false;
     w->grant = w->grant + full;
+    w->hint = head->hint;
     w->started = now;
-    w->job.assign(queue_.begin(), queue_.begin() + (long)take);
-    queue_.erase(queue_.begin(), queue_.begin() + (long)take);
+    w->job.assign(q.begin(), q.begin() + (long)take);
+    q.erase(q.begin(), q.begin() + (long)take);
     ++job_seq_;
-    for (auto& r : w->job) {
-      r->state = Request::kRunning;
-      r->t_start = now;
-      r->job_requests = (int)take;
-      r->job_seq = job_seq_;
-      ++r->attempts;
+    for (auto& p : w->job) {
+      Request& r = *p->req;
+      ++p->attempts;
+      if (!r.started) {
+        r.started = true;
+        --waiting_;
+        r.t_start = now;
+        r.job_seq = job_seq_;
+        r.state = Request::kRunning;
+      }
+      r.attempts = std::max(r.attempts, p->attempts);
     }
     ++st_jobs_;
-    st_job_reqs_ += (int64_t)take;
+    st_job_parts_ += (int64_t)take;
     peak_granted_ = std::max(peak_granted_, granted());
     cv_work_.notify_all();
     return true;
-  }
-
-  bool predict_job(size_t take, size_t* full, size_t* min) {
-    std::vector<int32_t> pl, tl;
-    int64_t pb = 0, tb = 0;
-    for (size_t i = 0; i < take; ++i) {
-      const Pairs& p = queue_[i]->in;
-      pl.insert(pl.end(), p.plen.begin(), p.plen.end());
-      tl.insert(tl.end(), p.tlen.begin(), p.tlen.end());
-      pb += (int64_t)p.pat.size();
-      tb += (int64_t)p.txt.size();
-    }
-    std::lock_guard<std::mutex> pl_lk(plan_mu_);
-    return planner_->predict((int64_t)pl.size(), pl.data(), tl.data(), pb, tb, queue_.front()->flags, full, min) ==
-           TSU_OK;
-  }
-
-  void trim_worker(Worker* w) {
-    if (w->busy) return;
-    w->ex->trim();
-    w->grant = w->ex->held();
   }
 
   // ---- worker threads
@@ -583,18 +730,16 @@ class Server {
         if (stopping_) break;
         continue;
       }
-      std::vector<ReqPtr> job = w->job;
+      std::vector<PartPtr> job = w->job;
       const size_t grant = w->grant;
+      const double hint = w->hint;
+      const uint32_t flags = job[0]->flags;
       lk.unlock();
-      Pairs merged;
-      const Pairs* in = &job[0]->in;
-      if (job.size() > 1) {
-        for (auto& r : job) merged.append(r->in);
-        in = &merged;
-      }
+      Pairs in;  // the requests' pairs are immutable once queued
+      for (auto& p : job) in.append(p->req->in, p->idx);
       w->ex->set_budget(grant);
       Output out;
-      const int rc = w->ex->run(*in, job[0]->flags, &out);
+      const int rc = w->ex->run(in, flags, hint, &out);
       const size_t needed = rc == TSU_ENOMEM ? w->ex->needed() : 0;
       const std::string why = rc ? w->ex->error() : std::string();
       if (w->ex->held() > cfg_.resident_cap) w->ex->trim();
@@ -602,6 +747,7 @@ class Server {
       lk.lock();
       finish(w, job, rc, out, needed, why);
       w->busy = false;
+      w->heavy = false;
       w->stuck = false;
       w->job.clear();
       w->grant = held;
@@ -610,55 +756,66 @@ class Server {
     }
   }
 
-  // Split a job's output per request (mu_ held).
-  void finish(Worker* w, std::vector<ReqPtr>& job, int rc, Output& out, size_t needed, const std::string& why) {
+  // Hand a job's output to its parts' requests (mu_ held).
+  void finish(Worker* w, std::vector<PartPtr>& job, int rc, Output& out, size_t needed, const std::string& why) {
     const auto now = Clock::now();
-    const bool cig = !(job[0]->flags & TSU_SCORE_ONLY);
+    const bool cig = !(job[0]->req->flags & TSU_SCORE_ONLY);
     if (rc) err_ = why;
     if (rc != TSU_OK && !stopping_ && (job.size() > 1 || rc == TSU_ENOMEM)) {
-      // re-queue at the head, each request alone, so a failure stays with
-      // the request that caused it; a single request that ran out of memory
-      // gets the reservation the engine asked for
-      std::vector<ReqPtr> again;
-      for (auto& r : job) {
-        if (r->cancelled || r->state == Request::kDone) continue;
-        const bool retry = job.size() > 1 || (needed > w->grant && needed <= cfg_.budget && r->attempts < 3);
+      // re-queue at the head: each part alone; a single part that ran out of
+      // memory gets the reservation the engine asked for
+      std::vector<PartPtr> again;
+      for (auto& p : job) {
+        if (p->req->state == Request::kDone) continue;
+        const bool retry = job.size() > 1 || (needed > w->grant && needed <= cfg_.budget && p->attempts < 3);
         if (!retry) continue;
-        if (job.size() == 1) r->full = r->min = std::max(r->full, needed);
-        r->alone = true;
-        r->state = Request::kQueued;
-        again.push_back(r);
+        if (job.size() == 1) p->full = p->min = std::max(p->full, needed);
+        p->alone = true;
+        again.push_back(p);
       }
-      for (auto it = again.rbegin(); it != again.rend(); ++it) queue_.push_front(*it);
+      for (auto it = again.rbegin(); it != again.rend(); ++it) (job[0]->heavy ? heavy_ : light_).push_front(*it);
+      if (!again.empty()) {
+        job.erase(std::remove_if(job.begin(), job.end(),
+                                 [&](const PartPtr& p) { return std::find(again.begin(), again.end(), p) != again.end(); }),
+                  job.end());
+        if (job.empty()) return;
+      }
     }
-    int64_t p0 = 0;
-    for (auto& rp : job) {
-      Request& r = *rp;
-      const int64_t n = r.in.n();
-      const int64_t p1 = p0 + n;
-      if (r.state == Request::kQueued || r.cancelled || r.state == Request::kDone) {
-        p0 = p1;
-        continue;  // re-queued, cancelled, or completed by the watchdog
+    int64_t k0 = 0;
+    int64_t base = 0;  // offset of this part's pairs in the job
+    for (auto& p : job) {
+      Request& r = *p->req;
+      const int64_t n = p->pairs();
+      (void)k0;
+      if (r.state == Request::kDone) {  // failed, cancelled or timed out meanwhile
+        base += n;
+        continue;
       }
-      r.out = Output{};
-      if (rc == TSU_OK) {
-        r.out.score.assign(out.score.begin() + p0, out.score.begin() + p1);
-        r.out.pair_status.assign(out.pair_status.begin() + p0, out.pair_status.begin() + p1);
-        if (cig) {
-          const int64_t c0 = out.coff[(size_t)p0], c1 = out.coff[(size_t)p1];
-          r.out.coff.resize((size_t)n + 1);
-          for (int64_t i = 0; i <= n; ++i) r.out.coff[(size_t)i] = out.coff[(size_t)(p0 + i)] - c0;
-          r.out.cigar.assign(out.cigar.begin() + c0, out.cigar.begin() + c1);
-        }
-      } else {
-        r.out.status = rc;
+      if (rc != TSU_OK) {
+        fail_request(r, rc, now);
+        base += n;
+        continue;
       }
-      r.state = Request::kDone;
-      r.t_done = now;
-      record_done(r);
-      p0 = p1;
+      Output po;
+      po.score.assign(out.score.begin() + base, out.score.begin() + base + n);
+      po.pair_status.assign(out.pair_status.begin() + base, out.pair_status.begin() + base + n);
+      if (cig) {
+        const int64_t c0 = out.coff[(size_t)base], c1 = out.coff[(size_t)(base + n)];
+        po.coff.resize((size_t)n + 1);
+        for (int64_t i = 0; i <= n; ++i) po.coff[(size_t)i] = out.coff[(size_t)(base + i)] - c0;
+        po.cigar.assign(out.cigar.begin() + c0, out.cigar.begin() + c1);
+      }
+      r.done_parts.emplace_back(p, std::move(po));
+      r.job_requests = std::max(r.job_requests, (int)job.size());
+      base += n;
+      if (--r.parts_left == 0) {
+        assemble(r);
+        r.state = Request::kDone;
+        r.t_done = now;
+        --open_;
+        record_done(r);
+      }
     }
-    (void)w;
   }
 
   Config cfg_;
@@ -668,15 +825,20 @@ class Server {
   std::thread sched_;
   std::mutex mu_;
   std::condition_variable cv_sched_, cv_work_, cv_done_;
-  std::deque<ReqPtr> queue_;
+  std::deque<PartPtr> light_, heavy_;
   std::map<uint64_t, ReqPtr> reqs_;
+  int64_t open_ = 0;     // requests not done
+  int64_t waiting_ = 0;  // requests none of whose parts has started
+  // a head part that needs the whole device: the other queue starts nothing
+  // until it has started
+  const std::deque<PartPtr>* drain_for_ = nullptr;
   uint64_t next_id_ = 0;
   int64_t job_seq_ = 0;
   bool stopping_ = false, stopped_ = false;
   std::string err_;
   // statistics since the last reset
   int64_t st_submitted_ = 0, st_completed_ = 0, st_failed_ = 0, st_rejected_ = 0, st_cancelled_ = 0,
-          st_timed_out_ = 0, st_jobs_ = 0, st_job_reqs_ = 0, st_pairs_ = 0;
+          st_timed_out_ = 0, st_jobs_ = 0, st_job_parts_ = 0, st_pairs_ = 0;
   std::vector<double> lat_;
   size_t peak_granted_ = 0;
   Clock::time_point t_reset_;

@@ -7,6 +7,7 @@
 // request gets the kernels, the length bands and the retry ladder of a batch
 // call.  A further context (no buffers) predicts the device memory of
 // requests and jobs.
+#include <algorithm>
 #include <cstdio>
 #include <memory>
 #include <string>
@@ -24,18 +25,21 @@ using tsu::serve::Pairs;
 
 class EngineExecutor final : public tsu::serve::Executor {
  public:
-  explicit EngineExecutor(tsu_ctx* ctx) : ctx_(ctx) { tsu::engine::set_exact_growth(ctx_, true); }
+  explicit EngineExecutor(tsu_ctx* ctx) : ctx_(ctx), default_hint_(tsu::engine::hint(ctx)) {
+    tsu::engine::set_exact_growth(ctx_, true);
+  }
   ~EngineExecutor() override { tsu_destroy(ctx_); }
 
   int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t flags,
-              size_t* full, size_t* min) override {
+              double hint, size_t* full, size_t* min) override {
     tsu::engine::BatchShape sh;
     sh.n = n;
     sh.plen = plen;
     sh.tlen = tlen;
     sh.pattern_bytes = pb;
     sh.text_bytes = tb;
-    return tsu::engine::predict_bytes(ctx_, sh, flags, full, min);
+    tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
+    return tsu::engine::predict_bytes(ctx_, sh, flags & TSU_SCORE_ONLY, hint, full, min);
   }
   size_t held() override { return tsu::engine::held_bytes(ctx_); }
   void set_budget(size_t bytes) override { tsu::engine::set_budget(ctx_, bytes); }
@@ -43,7 +47,9 @@ class EngineExecutor final : public tsu::serve::Executor {
   size_t needed() override { return tsu::engine::needed_bytes(ctx_); }
   std::string error() override { return tsu_last_error(ctx_); }
 
-  int run(const Pairs& in, uint32_t flags, Output* out) override {
+  int run(const Pairs& in, uint32_t flags, double hint, Output* out) override {
+    tsu::engine::set_hint(ctx_, hint > 0 ? hint : default_hint_);
+    tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
     const int64_t n = in.n();
     const bool cig = !(flags & TSU_SCORE_ONLY);
     out->score.assign((size_t)n, 0);
@@ -70,6 +76,7 @@ class EngineExecutor final : public tsu::serve::Executor {
 
  private:
   tsu_ctx* ctx_;
+  double default_hint_;
 };
 
 int make_ctx(const tsu_penalties* pen, int device, double hint, size_t budget, tsu_ctx** out) {
@@ -98,12 +105,15 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
       c.watchdog_ms < 0 || c.max_error_hint < 0)
     return TSU_EINVAL;
   tsu::serve::Config sc;
-  sc.workers = c.workers ? c.workers : 4;
+  sc.workers = c.workers ? c.workers : 16;
   sc.max_queue = c.max_queue ? c.max_queue : (1 << 16);
   sc.max_job_pairs = c.max_job_pairs ? c.max_job_pairs : 16384;
   sc.max_job_requests = c.max_job_requests ? c.max_job_requests : 64;
   sc.watchdog_ms = c.watchdog_ms;
   sc.resident_cap = c.resident_bytes;
+  sc.heavy_len = c.heavy_len == 0 ? 16384 : (c.heavy_len < 0 ? 0 : c.heavy_len);
+  sc.heavy_workers = c.heavy_workers > 0 ? c.heavy_workers : std::max(1, sc.workers - 2);
+  sc.estimate = c.estimate_hint >= 0;
   // the planner context: no buffers; its create resolves the default budget
   tsu_ctx* planner = nullptr;
   int rc = make_ctx(pen, c.device, c.max_error_hint, c.mem_budget, &planner);
