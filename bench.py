@@ -174,7 +174,9 @@ def run_serving(args):
                    estimate_hint=not args.no_estimate)
 
     def stream(index, n_req, rate):
-        arrivals, sizes = D.c5_stream(n_req, rate, index=index)
+        arrivals, sizes = D.c5_stream(n_req, rate if rate > 0 else 1.0, index=index)
+        if rate <= 0:  # all at once: the server's capacity
+            arrivals = np.zeros_like(arrivals)
         lengths, rates_, seed = D.shape("c5", int(sizes.sum()) + 1000 * index)
         first = 1000 * index
         lengths, rates_ = lengths[first:], rates_[first:]
@@ -231,13 +233,16 @@ def run_serving(args):
                        "offered_rate_rps": rate, "requests": len(reqs), "pairs": int(sizes.sum()),
                        "workers": args.workers, "budget_gb": st["budget_bytes"] / 2**30,
                        "long_pair_memory": "max_error_hint" if args.no_estimate else "k-mer estimate"},
-            "offered_pairs_s": float(sizes.sum()) / max(float(arrivals[-1]), 1e-9),
+            "offered_pairs_s": float(sizes.sum()) / float(arrivals[-1]) if arrivals[-1] > 0 else None,
             "gcups": cells / wall / 1e9,
             "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "p999": st["p999_ms"], "mean": st["mean_ms"],
                            "max": st["max_ms"]},
             "completed": st["completed"], "failed": st["failed"], "rejected": st["rejected"] + len(errors),
             "jobs": st["jobs"], "mean_requests_per_job": st["mean_requests_per_job"],
             "peak_granted_gb": st["peak_granted_bytes"] / 2**30, "wall_s": wall, "clocks": clk,
+            "heavy_jobs": st["heavy_jobs"], "mean_jobs_running": st["busy_s"] / wall,
+            "mean_heavy_job_ms": 1e3 * st["heavy_busy_s"] / max(st["heavy_jobs"], 1),
+            "mean_light_job_ms": 1e3 * (st["busy_s"] - st["heavy_busy_s"]) / max(st["jobs"] - st["heavy_jobs"], 1),
         }
         print(json.dumps(out), flush=True)
     srv.close()
@@ -302,9 +307,9 @@ def main():
     ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
     ap.add_argument("--plain", action="store_true", help="also time the plain one-warp-per-pair bucketed form")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain form (c4)")
-    ap.add_argument("--rates", default="25,50,100,200", help="c5: offered request rates (requests/s)")
+    ap.add_argument("--rates", default="5,10,20,0", help="c5: offered request rates (requests/s; 0: all at once)")
     ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
-    ap.add_argument("--workers", type=int, default=48, help="c5: server workers")
+    ap.add_argument("--workers", type=int, default=32, help="c5: server workers")
     ap.add_argument("--no-estimate", action="store_true", help="c5: size long pairs by --hint, not by estimate")
     ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
     args = ap.parse_args()

@@ -228,7 +228,12 @@ typedef struct tsu_server tsu_server;
 
 typedef struct {
   int32_t device;
-  int32_t workers;          /* jobs in flight (engine contexts); 0 = 16         */
+  int32_t workers;          /* jobs in flight (engine contexts, one stream
+                               each); 0 = 32.  Jobs overlap on the device only
+                               as far as CUDA_DEVICE_MAX_CONNECTIONS hardware
+                               queues allow: tsu_server_create sets it to 32
+                               when unset, which takes effect if no CUDA work
+                               ran in the process before                         */
   size_t mem_budget;        /* device bytes of all workers; 0 = 80% of free      */
   double max_error_hint;    /* edit rate sizing predicted wavefront memory (0 = 0.20);
                                pairs beyond it are retried, never dropped       */
@@ -272,6 +277,9 @@ typedef struct {
   double elapsed_s;
   uint64_t budget_bytes, granted_bytes, peak_granted_bytes;
   int32_t workers, reserved0;
+  int64_t heavy_jobs;        /* jobs of one long pair                            */
+  double busy_s;             /* worker time spent in jobs (all workers)          */
+  double heavy_busy_s;       /* of which in jobs of one long pair                */
 } tsu_server_stats;
 
 int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg /* nullable */, tsu_server** out);

@@ -71,7 +71,8 @@ class ServerStats(ctypes.Structure):
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("elapsed_s", ctypes.c_double),
                 ("budget_bytes", ctypes.c_uint64), ("granted_bytes", ctypes.c_uint64),
-                ("peak_granted_bytes", ctypes.c_uint64), ("workers", c_i32), ("reserved0", c_i32)]
+                ("peak_granted_bytes", ctypes.c_uint64), ("workers", c_i32), ("reserved0", c_i32),
+                ("heavy_jobs", c_i64), ("busy_s", ctypes.c_double), ("heavy_busy_s", ctypes.c_double)]
 
 
 class AlignError(RuntimeError):

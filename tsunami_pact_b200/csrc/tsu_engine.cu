@@ -13,6 +13,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -29,6 +30,12 @@
 namespace {
 
 struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+// Page-locked host memory.
+struct HostBuf {
   void* p = nullptr;
   size_t cap = 0;
 };
@@ -70,6 +77,20 @@ struct tsu_ctx {
   cudaMemPool_t pool = nullptr;  // the device's buffer pool
   bool exact_grow = false;       // grow buffers to the asked size only
   bool fit_start = false;        // start rungs by the hint's predicted width (tsu::fit_start)
+  // The engine's own host transfers (counters, pass orders, retry lists,
+  // statuses) go through page-locked buffers: a copy to or from pageable
+  // memory blocks the calling thread inside the driver until its stream
+  // reaches it, and several host threads' contexts then run one at a time.
+  HostBuf h_scalars;  // 64 bytes: retry count, arena cursor, work counters, run total
+  HostBuf h_list;     // int32 pass order / retry list
+  HostBuf h_status;   // int32 pair statuses (tsu_align_batch)
+  // events of the host-buffer pipeline (tsu_align_batch): 8 chunks at most
+  cudaEvent_t cev_up[8] = {}, cev_done[8] = {}, cev_down[8] = {}, cev_t[2] = {};
+  // Waits for the GPU sleep on an event instead of spinning (set by the
+  // request server, whose many worker threads would otherwise spin on all
+  // the host's cores); batch callers keep the driver's default.
+  bool blocking_sync = false;
+  cudaEvent_t wait_ev = nullptr;  // blocking-sync event of those waits
   size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
@@ -178,6 +199,37 @@ int grow(tsu_ctx* ctx, DevBuf& b, size_t bytes) {
   return TSU_OK;
 }
 
+// Wait until everything queued so far on stream s is done: a spin in the
+// driver, or a sleep on a blocking-sync event (ctx->blocking_sync).
+cudaError_t wait_stream(tsu_ctx* ctx, cudaStream_t s) {
+  if (!ctx->blocking_sync) return cudaStreamSynchronize(s);
+  cudaError_t e = cudaEventRecord(ctx->wait_ev, s);
+  if (e != cudaSuccess) return e;
+  return cudaEventSynchronize(ctx->wait_ev);
+}
+
+// Grow a page-locked buffer to at least `bytes` (doubling).  The old one is
+// freed once the context's streams are idle.
+int host_grow(tsu_ctx* ctx, HostBuf& b, size_t bytes) {
+  if (b.cap >= bytes) return TSU_OK;
+  const size_t nb = std::max<size_t>(std::max(bytes, 2 * b.cap), 4096);
+  if (b.p) {
+    wait_stream(ctx, ctx->h2d_stream);
+    wait_stream(ctx, ctx->d2h_stream);
+    wait_stream(ctx, ctx->stream);
+    cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  if (cudaHostAlloc(&b.p, nb, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return set_err(ctx, TSU_EDEVICE, "page-locked host allocation of %zu B failed", nb);
+  }
+  b.cap = nb;
+  return TSU_OK;
+}
+
 // Make the copy streams wait for the allocations queued on the context's
 // stream so far.
 void alloc_fence(tsu_ctx* ctx) {
@@ -188,11 +240,11 @@ void alloc_fence(tsu_ctx* ctx) {
 
 // Every buffer back to the pool, once the context's streams are idle.
 int release_all(tsu_ctx* ctx) {
-  cudaStreamSynchronize(ctx->h2d_stream);
-  cudaStreamSynchronize(ctx->d2h_stream);
-  cudaStreamSynchronize(ctx->stream);
+  wait_stream(ctx, ctx->h2d_stream);
+  wait_stream(ctx, ctx->d2h_stream);
+  wait_stream(ctx, ctx->stream);
   for (DevBuf* b : ctx->bufs()) release(ctx, *b);
-  return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? TSU_OK : TSU_EDEVICE;
+  return wait_stream(ctx, ctx->stream) == cudaSuccess ? TSU_OK : TSU_EDEVICE;
 }
 
 template <class T>
@@ -215,14 +267,21 @@ struct BatchInfo {
 
 // The align_kernel instantiations: CIGAR or score only, shared or global
 // wavefront ring, 1/2/4/8/16 warps per pair.  Each kernel's dynamic shared
-// memory limit is set to the device maximum (the same value on every call),
-// so contexts planning on several host threads cannot lower it under
-// another's launch.
+// memory limit is set to the device maximum once per device (always the same
+// value, so contexts planning on several host threads cannot lower it under
+// another's launch).
 template <bool kCigar, int kMode, int GW>
 cudaError_t occ_one(int threads, size_t smem, int optin, int* occ) {
-  cudaError_t e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode, GW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  static std::atomic<uint64_t> limit_set{0};  // bit d: set on device d
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (1ull << dev) : 0;
+  if (!bit || !(limit_set.load() & bit)) {
+    e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode, GW>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    limit_set.fetch_or(bit);
+  }
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode, GW>, threads, smem);
 }
 
@@ -477,7 +536,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       pbi.max_m = std::max(pbi.max_m, h_plen[i]);
       pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
     }
-    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), bp.data(), sizeof(int32_t) * n_order, cudaMemcpyHostToDevice, st));
+    if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * (size_t)n_order))) return rc;
+    memcpy(ctx->h_list.p, bp.data(), sizeof(int32_t) * (size_t)n_order);  // the previous list's copy is done
+    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * n_order, cudaMemcpyHostToDevice,
+                       st));
     order = P<int32_t>(ctx->b_order);
     pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
   }
@@ -496,7 +558,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       const size_t need_hist = want_cigar ? sizeof(uint32_t) * (size_t)ps.groups * g.hist_cap : 0;
       const size_t need_table = want_cigar ? sizeof(int2) * (size_t)ps.groups * g.table_cap : 0;
       if (need_ring > ctx->b_ring.cap || need_hist > ctx->b_hist.cap || need_table > ctx->b_table.cap) {
-        CU(cudaStreamSynchronize(st));
+        CU(wait_stream(ctx, st));
         release(ctx, ctx->b_ring);
         release(ctx, ctx->b_hist);
         release(ctx, ctx->b_table);
@@ -543,9 +605,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     CU(cudaGetLastError());
     CU(cudaEventRecord(ctx->pev[1], st));
     ++passes;
-    unsigned int nretry = 0;
-    CU(cudaMemcpyAsync(&nretry, d_retry_cnt, sizeof nretry, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    unsigned int* h_nretry = static_cast<unsigned int*>(ctx->h_scalars.p);
+    CU(cudaMemcpyAsync(h_nretry, d_retry_cnt, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    const unsigned int nretry = *h_nretry;
     {
       char t[48];
       snprintf(t, sizeof t, "@%.1fms", ev_ms(ctx->pev[0], ctx->pev[1]));
@@ -562,8 +625,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     // The retry list, longest pairs first, becomes the next pass's order; its
     // lengths pick the next rung of the ladder.  Global passes grow the hint.
     rlist.resize(nretry);
-    CU(cudaMemcpyAsync(rlist.data(), P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * nretry))) return rc;
+    CU(cudaMemcpyAsync(ctx->h_list.p, P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry, cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    memcpy(rlist.data(), ctx->h_list.p, sizeof(int32_t) * nretry);
     pbi = BatchInfo{};
     pbi.n = nretry;
     for (int32_t i : rlist) {
@@ -572,16 +637,18 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     }
     std::sort(rlist.begin(), rlist.end(),
               [&](int32_t u, int32_t v) { return (int64_t)h_plen[u] + h_tlen[u] > (int64_t)h_plen[v] + h_tlen[v]; });
-    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), rlist.data(), sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
+    memcpy(ctx->h_list.p, rlist.data(), sizeof(int32_t) * nretry);
+    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
     order = P<int32_t>(ctx->b_order);
     n_order = nretry;
     hint = tsu::next_hint(hint, g.mode == tsu::kModeGlobal);
     pc = ctx->one_warp ? tsu::PassChoice{tsu::kModeGlobal, 1}
                        : tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
     if (want_cigar) {
-      unsigned long long used = 0;
-      CU(cudaMemcpyAsync(&used, d_cursor, sizeof used, cudaMemcpyDeviceToHost, st));
-      CU(cudaStreamSynchronize(st));
+      unsigned long long* h_used = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 8);
+      CU(cudaMemcpyAsync(h_used, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      CU(wait_stream(ctx, st));
+      const unsigned long long used = *h_used;
       const int64_t maxlen = std::max(pbi.max_m, pbi.max_n);
       const int64_t need = (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
       if (need > arena_cap) {
@@ -606,9 +673,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   }  // bands
   CU(cudaEventRecord(ctx->ev[5], st));
   {
-    unsigned long long work[2] = {0, 0};
-    CU(cudaMemcpyAsync(work, P<char>(ctx->b_counters) + 24, sizeof work, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    unsigned long long* work = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 16);
+    CU(cudaMemcpyAsync(work, P<char>(ctx->b_counters) + 24, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       st));
+    CU(wait_stream(ctx, st));
     ctx->timing.cells = (int64_t)work[0];
     ctx->timing.steps = (int64_t)work[1];
   }
@@ -625,9 +693,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     if ((rc = grow(ctx, ctx->b_scan_tmp, tb))) return rc;
     CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tb, P<int64_t>(ctx->b_clen64), d_out_off, (int)(n + 1), st));
     ctx->timing.kernel_launches++;
-    int64_t total = 0;
-    CU(cudaMemcpyAsync(&total, d_out_off + n, sizeof total, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    int64_t* h_total = reinterpret_cast<int64_t*>(static_cast<char*>(ctx->h_scalars.p) + 32);
+    CU(cudaMemcpyAsync(h_total, d_out_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    const int64_t total = *h_total;
     if (runs_needed) *runs_needed = total;
     if (!d_out_runs) {
       DevBuf& ob = out_buf ? *out_buf : ctx->b_out;
@@ -774,6 +843,71 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
   return TSU_OK;
 }
 
+int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out) {
+  tsu_ctx* ctx = nullptr;
+  if (!pen || !out) return TSU_EINVAL;
+  *out = nullptr;
+  if (pen->mismatch <= 0 || pen->gap_opening < 0 || pen->gap_extension <= 0 || pen->mismatch > 1 << 20 ||
+      pen->gap_opening > 1 << 20 || pen->gap_extension > 1 << 20)
+    return TSU_EINVAL;
+  ctx = new tsu_ctx();
+  ctx->pen = *pen;
+  ctx->g = gcd(gcd(pen->mismatch, pen->gap_opening), pen->gap_extension);
+  ctx->x = pen->mismatch / ctx->g;
+  ctx->go = (pen->gap_opening + pen->gap_extension) / ctx->g;
+  ctx->ge = pen->gap_extension / ctx->g;
+  ctx->rm = std::max(ctx->x, ctx->go) + 1;
+  ctx->re = ctx->ge + 1;
+  if (tsu::ring_slots(ctx->rm, ctx->re) > 4096) {
+    delete ctx;
+    return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
+  }
+  ctx->device = cfg ? cfg->device : 0;
+  ctx->err_hint = (cfg && cfg->max_error_hint > 0) ? cfg->max_error_hint : 0.2;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  ctx->sms = prop.multiProcessorCount;
+  ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  ctx->budget = (cfg && cfg->mem_budget) ? cfg->mem_budget : (size_t)(0.8 * (double)fr);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return TSU_EDEVICE;
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  for (auto& ev : ctx->pev) cudaEventCreate(&ev);
+  for (auto& ev : ctx->fence_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  for (int c = 0; c < 8; ++c) {
+    cudaEventCreateWithFlags(&ctx->cev_up[c], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ctx->cev_done[c], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ctx->cev_down[c], cudaEventDisableTiming);
+  }
+  for (auto& ev : ctx->cev_t) cudaEventCreate(&ev);
+  cudaEventCreateWithFlags(&ctx->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming);
+  if (single_stream) {
+    ctx->h2d_stream = ctx->d2h_stream = ctx->stream;
+  } else {
+    cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
+  }
+  ctx->pool = device_pool(ctx->device);
+  if (!ctx->pool || host_grow(ctx, ctx->h_scalars, 64) != TSU_OK) {
+    tsu_destroy(ctx);
+    return TSU_EDEVICE;
+  }
+  *out = ctx;
+  return TSU_OK;
+}
+
 size_t held_bytes(const tsu_ctx* ctx) { return ctx ? ctx->held() : 0; }
 
 void set_budget(tsu_ctx* ctx, size_t bytes) {
@@ -790,6 +924,10 @@ double hint(const tsu_ctx* ctx) { return ctx ? ctx->err_hint : 0.0; }
 
 void set_fit_start(tsu_ctx* ctx, bool on) {
   if (ctx) ctx->fit_start = on;
+}
+
+void set_blocking_sync(tsu_ctx* ctx, bool on) {
+  if (ctx) ctx->blocking_sync = on;
 }
 
 void set_exact_growth(tsu_ctx* ctx, bool exact) {
@@ -834,57 +972,7 @@ const char* tsu_last_error(const tsu_ctx* ctx) { return ctx ? ctx->err.c_str() :
 const char* tsu_pass_log(const tsu_ctx* ctx) { return ctx ? ctx->passlog.c_str() : ""; }
 
 int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
-  tsu_ctx* ctx = nullptr;
-  if (!pen || !out) return TSU_EINVAL;
-  *out = nullptr;
-  if (pen->mismatch <= 0 || pen->gap_opening < 0 || pen->gap_extension <= 0 || pen->mismatch > 1 << 20 ||
-      pen->gap_opening > 1 << 20 || pen->gap_extension > 1 << 20)
-    return TSU_EINVAL;
-  ctx = new tsu_ctx();
-  ctx->pen = *pen;
-  ctx->g = gcd(gcd(pen->mismatch, pen->gap_opening), pen->gap_extension);
-  ctx->x = pen->mismatch / ctx->g;
-  ctx->go = (pen->gap_opening + pen->gap_extension) / ctx->g;
-  ctx->ge = pen->gap_extension / ctx->g;
-  ctx->rm = std::max(ctx->x, ctx->go) + 1;
-  ctx->re = ctx->ge + 1;
-  if (tsu::ring_slots(ctx->rm, ctx->re) > 4096) {
-    delete ctx;
-    return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
-  }
-  ctx->device = cfg ? cfg->device : 0;
-  ctx->err_hint = (cfg && cfg->max_error_hint > 0) ? cfg->max_error_hint : 0.2;
-  cudaError_t e = cudaSetDevice(ctx->device);
-  if (e != cudaSuccess) {
-    delete ctx;
-    return TSU_EDEVICE;
-  }
-  cudaDeviceProp prop{};
-  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) {
-    delete ctx;
-    return TSU_EDEVICE;
-  }
-  ctx->sms = prop.multiProcessorCount;
-  ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
-  size_t fr = 0, tot = 0;
-  cudaMemGetInfo(&fr, &tot);
-  ctx->budget = (cfg && cfg->mem_budget) ? cfg->mem_budget : (size_t)(0.8 * (double)fr);
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete ctx;
-    return TSU_EDEVICE;
-  }
-  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
-  for (auto& ev : ctx->pev) cudaEventCreate(&ev);
-  for (auto& ev : ctx->fence_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-  cudaStreamCreateWithFlags(&ctx->h2d_stream, cudaStreamNonBlocking);
-  cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
-  ctx->pool = device_pool(ctx->device);
-  if (!ctx->pool) {
-    tsu_destroy(ctx);
-    return TSU_EDEVICE;
-  }
-  *out = ctx;
-  return TSU_OK;
+  return tsu::engine::create(pen, cfg, false, out);
 }
 
 int tsu_destroy(tsu_ctx* ctx) {
@@ -894,9 +982,18 @@ int tsu_destroy(tsu_ctx* ctx) {
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->pev) cudaEventDestroy(ev);
   for (auto& ev : ctx->fence_ev) cudaEventDestroy(ev);
+  for (int c = 0; c < 8; ++c) {
+    cudaEventDestroy(ctx->cev_up[c]);
+    cudaEventDestroy(ctx->cev_done[c]);
+    cudaEventDestroy(ctx->cev_down[c]);
+  }
+  for (auto& ev : ctx->cev_t) cudaEventDestroy(ev);
+  if (ctx->wait_ev) cudaEventDestroy(ctx->wait_ev);
+  for (HostBuf* hb : {&ctx->h_scalars, &ctx->h_list, &ctx->h_status})
+    if (hb->p) cudaFreeHost(hb->p);
+  if (ctx->h2d_stream && ctx->h2d_stream != ctx->stream) cudaStreamDestroy(ctx->h2d_stream);
+  if (ctx->d2h_stream && ctx->d2h_stream != ctx->stream) cudaStreamDestroy(ctx->d2h_stream);
   cudaStreamDestroy(ctx->stream);
-  if (ctx->h2d_stream) cudaStreamDestroy(ctx->h2d_stream);
-  if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
   delete ctx;
   return TSU_OK;
 }
@@ -939,29 +1036,12 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   alloc_fence(ctx);  // the copy streams write the buffers just grown
   std::vector<int64_t> cs((size_t)K + 1);  // chunk boundaries (pairs)
   for (int c = 0; c <= K; ++c) cs[(size_t)c] = n * c / K;
-  std::vector<cudaEvent_t> ev_up((size_t)K), ev_done((size_t)K), ev_down((size_t)K);
-  for (int c = 0; c < K; ++c) {
-    CU(cudaEventCreateWithFlags(&ev_up[(size_t)c], cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&ev_done[(size_t)c], cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&ev_down[(size_t)c], cudaEventDisableTiming));
-  }
-  struct EvGuard {
-    std::vector<cudaEvent_t>* v[3];
-    ~EvGuard() {
-      for (auto* e : v)
-        for (auto x : *e) cudaEventDestroy(x);
-    }
-  } guard{{&ev_up, &ev_done, &ev_down}};
-  cudaEvent_t t_begin, t_end;
-  CU(cudaEventCreate(&t_begin));
-  CU(cudaEventCreate(&t_end));
-  struct TGuard {
-    cudaEvent_t a, b;
-    ~TGuard() {
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
-    }
-  } tguard{t_begin, t_end};
+  cudaEvent_t* ev_up = ctx->cev_up;  // K <= 8 (chunk_count)
+  cudaEvent_t* ev_done = ctx->cev_done;
+  cudaEvent_t* ev_down = ctx->cev_down;
+  cudaEvent_t t_begin = ctx->cev_t[0], t_end = ctx->cev_t[1];
+  if ((rc = host_grow(ctx, ctx->h_status, sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)))) return rc;
+  int32_t* hs = static_cast<int32_t*>(ctx->h_status.p);
   CU(cudaEventRecord(t_begin, ctx->h2d_stream));
   int64_t h2d = 0;
   if (n) {
@@ -1002,13 +1082,18 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   int64_t needed = 0, d2h = 0;
   double pack_ms = 0, align_ms = 0, compact_ms = 0;
   int64_t launches = 0, retried = 0, cells = 0, steps = 0;
-  std::vector<int32_t> hs((size_t)n);
   std::vector<int64_t> run_base((size_t)K + 1, 0);
   for (int c = 0; c < K; ++c) {
     const int64_t c0 = cs[(size_t)c], nc = cbi[(size_t)c].n;
     DevBuf& ob = (c & 1) ? ctx->b_out2 : ctx->b_out;
     // the output buffer is reused two chunks later: its download must be done
-    if (c >= 2) CU(cudaEventSynchronize(ev_down[(size_t)c - 2]));
+    if (c >= 2) {
+      if (ctx->blocking_sync) {
+        CU(wait_stream(ctx, ctx->d2h_stream));  // sleeps until that download (and any later one) is done
+      } else {
+        CU(cudaEventSynchronize(ev_down[(size_t)c - 2]));
+      }
+    }
     CU(cudaStreamWaitEvent(st, ev_up[(size_t)c], 0));
     tsu::SeqView sv{nc, P<uint8_t>(ctx->b_pat), P<int64_t>(ctx->b_poff) + c0, P<int32_t>(ctx->b_plen) + c0,
                     P<uint8_t>(ctx->b_txt), P<int64_t>(ctx->b_toff) + c0, P<int32_t>(ctx->b_tlen) + c0};
@@ -1034,7 +1119,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
     if (nc) {
       CU(cudaMemcpyAsync(res->score + c0, P<int32_t>(ctx->b_score) + c0, sizeof(int32_t) * nc,
                          cudaMemcpyDeviceToHost, ctx->d2h_stream));
-      CU(cudaMemcpyAsync(hs.data() + c0, P<int32_t>(ctx->b_status) + c0, sizeof(int32_t) * nc,
+      CU(cudaMemcpyAsync(hs + c0, P<int32_t>(ctx->b_status) + c0, sizeof(int32_t) * nc,
                          cudaMemcpyDeviceToHost, ctx->d2h_stream));
       d2h += nc * 8;
     }
@@ -1054,7 +1139,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
     CU(cudaEventRecord(ev_down[(size_t)c], ctx->d2h_stream));
   }
   CU(cudaEventRecord(t_end, ctx->d2h_stream));
-  CU(cudaEventSynchronize(t_end));
+  CU(ctx->blocking_sync ? wait_stream(ctx, ctx->d2h_stream) : cudaEventSynchronize(t_end));
   ctx->timing.d2h_bytes = d2h;
   ctx->timing.pack_ms = pack_ms;
   ctx->timing.align_ms = align_ms;
@@ -1072,8 +1157,8 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
     res->cigar_offset[n] = needed;
     res->cigar_needed = needed;
   }
-  if (res->pair_status) memcpy(res->pair_status, hs.data(), sizeof(int32_t) * n);
-  if ((rc = collect_status(ctx, hs.data(), n))) return rc;
+  if (res->pair_status) memcpy(res->pair_status, hs, sizeof(int32_t) * n);
+  if ((rc = collect_status(ctx, hs, n))) return rc;
   if (want_cigar && (needed > res->cigar_capacity || !res->cigar)) return TSU_EOVERFLOW;
   return TSU_OK;
 }
@@ -1113,7 +1198,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
     if (n) {
       CU(cudaMemcpyAsync(pl.data(), b->pattern_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
       CU(cudaMemcpyAsync(tl.data(), b->text_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
-      CU(cudaStreamSynchronize(st));
+      CU(wait_stream(ctx, st));
     }
     for (int64_t i = 0; i < n; ++i) {
       if (pl[(size_t)i] < 0 || tl[(size_t)i] < 0 || pl[(size_t)i] > (1 << 26) || tl[(size_t)i] > (1 << 26))
@@ -1139,7 +1224,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
   res->cigar_needed = needed;
   if (rc) return rc;
   CU(cudaEventRecord(ctx->ev[7], st));
-  CU(cudaStreamSynchronize(st));
+  CU(wait_stream(ctx, st));
   ctx->timing.pack_ms = n ? ev_ms(ctx->ev[2], ctx->ev[3]) : 0;
   ctx->timing.align_ms = n ? ev_ms(ctx->ev[4], ctx->ev[5]) : 0;
   ctx->timing.compact_ms = (n && want_cigar) ? ev_ms(ctx->ev[5], ctx->ev[6]) : 0;

@@ -10,6 +10,13 @@
 namespace tsu {
 namespace engine {
 
+// tsu_create, optionally with one stream for all work: the host-buffer
+// pipeline's copy streams are then the compute stream.  The device runs a
+// limited number of hardware queues (CUDA_DEVICE_MAX_CONNECTIONS) that
+// streams share in turn; work queued behind a long kernel on a shared queue
+// waits for it, so contexts of many host threads use one stream each.
+int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out);
+
 // Lengths of the pairs of a planned batch (host memory).
 struct BatchShape {
   int64_t n = 0;
@@ -38,6 +45,9 @@ double hint(const tsu_ctx* ctx);
 // Choose each band's first rung by the wavefront width the hint predicts
 // (tsu::fit_start) -- for hints estimated per pair.
 void set_fit_start(tsu_ctx* ctx, bool on);
+// Wait for the GPU by sleeping on blocking-sync events instead of spinning
+// (for many contexts driven from many host threads).
+void set_blocking_sync(tsu_ctx* ctx, bool on);
 // Grow buffers to exactly the size asked for (no 1.5x headroom), so a
 // context holds no more than its predicted peak.
 void set_exact_growth(tsu_ctx* ctx, bool exact);

@@ -401,12 +401,16 @@ class Server {
     s->granted_bytes = granted();
     s->peak_granted_bytes = peak_granted_;
     s->workers = (int32_t)workers_.size();
+    s->heavy_jobs = st_heavy_jobs_;
+    s->busy_s = st_busy_ms_ / 1000.0;
+    s->heavy_busy_s = st_heavy_busy_ms_ / 1000.0;
   }
 
   void reset_stats() {
     std::lock_guard<std::mutex> lk(mu_);
     st_submitted_ = st_completed_ = st_failed_ = st_rejected_ = st_cancelled_ = st_timed_out_ = 0;
-    st_jobs_ = st_job_parts_ = st_pairs_ = 0;
+    st_jobs_ = st_job_parts_ = st_pairs_ = st_heavy_jobs_ = 0;
+    st_busy_ms_ = st_heavy_busy_ms_ = 0;
     lat_.clear();
     peak_granted_ = granted();
     t_reset_ = Clock::now();
@@ -744,7 +748,13 @@ class Server {
       const std::string why = rc ? w->ex->error() : std::string();
       if (w->ex->held() > cfg_.resident_cap) w->ex->trim();
       const size_t held = w->ex->held();
+      const double ran_ms = ms_between(w->started, Clock::now());
       lk.lock();
+      st_busy_ms_ += ran_ms;
+      if (w->heavy) {
+        st_heavy_busy_ms_ += ran_ms;
+        ++st_heavy_jobs_;
+      }
       finish(w, job, rc, out, needed, why);
       w->busy = false;
       w->heavy = false;
@@ -838,7 +848,8 @@ class Server {
   std::string err_;
   // statistics since the last reset
   int64_t st_submitted_ = 0, st_completed_ = 0, st_failed_ = 0, st_rejected_ = 0, st_cancelled_ = 0,
-          st_timed_out_ = 0, st_jobs_ = 0, st_job_parts_ = 0, st_pairs_ = 0;
+          st_timed_out_ = 0, st_jobs_ = 0, st_job_parts_ = 0, st_pairs_ = 0, st_heavy_jobs_ = 0;
+  double st_busy_ms_ = 0, st_heavy_busy_ms_ = 0;
   std::vector<double> lat_;
   size_t peak_granted_ = 0;
   Clock::time_point t_reset_;

@@ -6,9 +6,16 @@
 // its own host thread through tsu_align_batch -- the batch path, so a served
 // request gets the kernels, the length bands and the retry ladder of a batch
 // call.  A further context (no buffers) predicts the device memory of
-// requests and jobs.
+// requests and jobs.  Jobs go through page-locked staging buffers of the
+// worker: copies from or to pageable memory block the worker's thread inside
+// the driver while its stream is busy, and with many workers that
+// serializes jobs that would otherwise overlap on the device.
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <memory>
 #include <string>
 #include <thread>
@@ -23,10 +30,41 @@ namespace {
 using tsu::serve::Output;
 using tsu::serve::Pairs;
 
+// A growing page-locked host buffer.
+class HostStage {
+ public:
+  ~HostStage() {
+    if (p_) cudaFreeHost(p_);
+  }
+  // At least `bytes`, doubling; nullptr if the allocation fails.
+  char* get(size_t bytes) {
+    if (bytes > cap_) {
+      const size_t nb = std::max<size_t>(std::max(bytes, 2 * cap_), 1 << 20);
+      if (p_) cudaFreeHost(p_);
+      p_ = nullptr;
+      cap_ = 0;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&p_), nb, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        p_ = nullptr;
+        return nullptr;
+      }
+      cap_ = nb;
+    }
+    return p_;
+  }
+
+ private:
+  char* p_ = nullptr;
+  size_t cap_ = 0;
+};
+
+size_t up16(size_t b) { return (b + 15) & ~(size_t)15; }
+
 class EngineExecutor final : public tsu::serve::Executor {
  public:
   explicit EngineExecutor(tsu_ctx* ctx) : ctx_(ctx), default_hint_(tsu::engine::hint(ctx)) {
     tsu::engine::set_exact_growth(ctx_, true);
+    tsu::engine::set_blocking_sync(ctx_, true);
   }
   ~EngineExecutor() override { tsu_destroy(ctx_); }
 
@@ -50,33 +88,56 @@ class EngineExecutor final : public tsu::serve::Executor {
   int run(const Pairs& in, uint32_t flags, double hint, Output* out) override {
     tsu::engine::set_hint(ctx_, hint > 0 ? hint : default_hint_);
     tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
-    const int64_t n = in.n();
+    const size_t n = (size_t)in.n();
     const bool cig = !(flags & TSU_SCORE_ONLY);
-    out->score.assign((size_t)n, 0);
-    out->pair_status.assign((size_t)n, -1);
     int64_t cap = 1;  // a pair has at most m + n runs
-    for (int64_t i = 0; i < n; ++i) cap += (int64_t)in.plen[(size_t)i] + in.tlen[(size_t)i];
-    if (cig) {
-      out->coff.assign((size_t)n + 1, 0);
-      out->cigar.resize((size_t)cap);
-    }
-    tsu_batch b = in.view();
+    for (size_t i = 0; i < n; ++i) cap += (int64_t)in.plen[i] + in.tlen[i];
+    // inputs: pattern bytes | text bytes | offsets | lengths
+    const size_t a_pat = 0, a_txt = up16(in.pat.size() + 1), a_poff = a_txt + up16(in.txt.size() + 1);
+    const size_t a_toff = a_poff + up16(8 * n), a_plen = a_toff + up16(8 * n), a_tlen = a_plen + up16(4 * n);
+    char* hi = in_.get(a_tlen + up16(4 * n));
+    // outputs: scores | statuses | CIGAR offsets | runs
+    const size_t o_st = up16(4 * n), o_coff = o_st + up16(4 * n), o_runs = o_coff + up16(8 * (n + 1));
+    char* ho = out_.get(o_runs + (cig ? 4 * (size_t)cap : 0));
+    if (!hi || !ho) return TSU_ENOMEM;
+    if (!in.pat.empty()) memcpy(hi + a_pat, in.pat.data(), in.pat.size());
+    if (!in.txt.empty()) memcpy(hi + a_txt, in.txt.data(), in.txt.size());
+    memcpy(hi + a_poff, in.poff.data(), 8 * n);
+    memcpy(hi + a_toff, in.toff.data(), 8 * n);
+    memcpy(hi + a_plen, in.plen.data(), 4 * n);
+    memcpy(hi + a_tlen, in.tlen.data(), 4 * n);
+    tsu_batch b{(int64_t)n,
+                hi + a_pat,
+                reinterpret_cast<const int64_t*>(hi + a_poff),
+                reinterpret_cast<const int32_t*>(hi + a_plen),
+                hi + a_txt,
+                reinterpret_cast<const int64_t*>(hi + a_toff),
+                reinterpret_cast<const int32_t*>(hi + a_tlen)};
+    int32_t* h_score = reinterpret_cast<int32_t*>(ho);
+    int32_t* h_status = reinterpret_cast<int32_t*>(ho + o_st);
+    for (size_t i = 0; i < n; ++i) h_status[i] = -1;
     tsu_result r{};
-    r.score = out->score.data();
-    r.pair_status = out->pair_status.data();
+    r.score = h_score;
+    r.pair_status = h_status;
     if (cig) {
-      r.cigar = out->cigar.data();
+      r.cigar = reinterpret_cast<uint32_t*>(ho + o_runs);
       r.cigar_capacity = cap;
-      r.cigar_offset = out->coff.data();
+      r.cigar_offset = reinterpret_cast<int64_t*>(ho + o_coff);
     }
     const int rc = tsu_align_batch(ctx_, &b, &r, flags & TSU_SCORE_ONLY);
-    if (rc == TSU_OK && cig) out->cigar.resize((size_t)r.cigar_needed);
+    out->score.assign(h_score, h_score + n);
+    out->pair_status.assign(h_status, h_status + n);
+    if (rc == TSU_OK && cig) {
+      out->coff.assign(r.cigar_offset, r.cigar_offset + n + 1);
+      out->cigar.assign(r.cigar, r.cigar + r.cigar_needed);
+    }
     return rc;
   }
 
  private:
   tsu_ctx* ctx_;
   double default_hint_;
+  HostStage in_, out_;
 };
 
 int make_ctx(const tsu_penalties* pen, int device, double hint, size_t budget, tsu_ctx** out) {
@@ -84,7 +145,7 @@ int make_ctx(const tsu_penalties* pen, int device, double hint, size_t budget, t
   c.device = device;
   c.mem_budget = budget;
   c.max_error_hint = hint;
-  return tsu_create(pen, &c, out);
+  return tsu::engine::create(pen, &c, true, out);
 }
 
 }  // namespace
@@ -105,7 +166,7 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
       c.watchdog_ms < 0 || c.max_error_hint < 0)
     return TSU_EINVAL;
   tsu::serve::Config sc;
-  sc.workers = c.workers ? c.workers : 16;
+  sc.workers = c.workers ? c.workers : 32;
   sc.max_queue = c.max_queue ? c.max_queue : (1 << 16);
   sc.max_job_pairs = c.max_job_pairs ? c.max_job_pairs : 16384;
   sc.max_job_requests = c.max_job_requests ? c.max_job_requests : 64;
@@ -114,6 +175,10 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
   sc.heavy_len = c.heavy_len == 0 ? 16384 : (c.heavy_len < 0 ? 0 : c.heavy_len);
   sc.heavy_workers = c.heavy_workers > 0 ? c.heavy_workers : std::max(1, sc.workers - 2);
   sc.estimate = c.estimate_hint >= 0;
+  // Jobs of different workers overlap only on different hardware queues: ask
+  // for the most (32) unless the process chose otherwise.  It takes effect
+  // if this is the process's first CUDA work on the device.
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
   // the planner context: no buffers; its create resolves the default budget
   tsu_ctx* planner = nullptr;
   int rc = make_ctx(pen, c.device, c.max_error_hint, c.mem_budget, &planner);
