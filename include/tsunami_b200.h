@@ -129,6 +129,18 @@ int tsu_get_timing(const tsu_ctx* ctx, tsu_timing* out);
  * counterpart in the reference (one fixed launch, wfa_gpu.cu:118). */
 const char* tsu_pass_log(const tsu_ctx* ctx);
 
+/* ---- pass plan ------------------------------------------------------------
+ * Pairs are aligned by length band (max(m, n) < 1024, < 2048, < 4096, < 8192,
+ * < 16384, >= 16384 for bands 0..5); each band starts at a rung: the wavefront
+ * ring in shared memory (mode 0) or in device memory (mode 1), with 1, 2, 4,
+ * 8 or 16 warps per pair.  A context starts from the table compiled in
+ * (tsu_tuning.h, written by the autotuner tsunami_pact_b200/tune.py); these
+ * calls read and change the context's copy.  Pairs that outgrow a rung are
+ * retried at the next one, so a rung never changes a result.  No
+ * counterpart in the reference (one fixed launch shape, wfa_gpu.cu:113-114). */
+int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair);
+int tsu_get_band_start(const tsu_ctx* ctx, int band, int* mode, int* warps_per_pair);
+
 /* ---- batch alignment, host buffers -------------------------------------
  * Replaces H2D + wfa_dispatcher launch + D2H of the reference
  * (wfa_gpu.cu:110-128) for arbitrary-length pairs, plus the CIGARs the

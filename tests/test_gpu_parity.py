@@ -255,3 +255,30 @@ def test_cli_check(tmp_path):
     assert "|ALIGNEMENT FINISHED CORRECTLY|" in r.stdout, r.stdout
     rows = (tmp_path / "cig.tsv").read_text().strip().split("\n")
     assert len(rows) == 3000
+
+
+def test_every_starting_rung_same_results(aligner_factory, oracle):
+    """tsu_set_band_start: whatever rung a band starts at (shared ring with
+    1-16 warps per pair, global ring with 8 or 16), pairs that outgrow it are
+    retried and the results are the oracle's."""
+    import ctypes
+
+    import tsunami_pact_b200 as T
+
+    rng = np.random.default_rng(21)
+    n = 120
+    lengths = np.exp(rng.uniform(np.log(100), np.log(6000), n)).astype(np.int32)
+    rates = rng.uniform(0.01, 0.15, n)
+    pats, txts = _gen(0x5453554E414D49 + 9, lengths, rates)
+    osc, oops = oracle.align_batch(pats, txts, 4, 6, 2)
+    L = T.lib()
+    L.tsu_set_band_start.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    with T.Aligner(4, 6, 2) as al:
+        assert L.tsu_set_band_start(al._h, 6, 0, 1) != 0  # no band 6
+        assert L.tsu_set_band_start(al._h, 0, 0, 3) != 0  # no 3-warp groups
+        for mode, gw in [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (1, 1), (1, 8), (1, 16)]:
+            for band in range(6):
+                assert L.tsu_set_band_start(al._h, band, mode, gw) == 0
+            scores, ops = al.align(pats, txts)
+            assert list(scores) == list(osc), (mode, gw)
+            assert ops == oops, (mode, gw)

@@ -77,6 +77,7 @@ struct tsu_ctx {
   cudaMemPool_t pool = nullptr;  // the device's buffer pool
   bool exact_grow = false;       // grow buffers to the asked size only
   bool fit_start = false;        // start rungs by the hint's predicted width (tsu::fit_start)
+  tsu::PassChoice band_start[tsu::kBands] = {};  // starting rung per length band (tsu_set_band_start)
   // The engine's own host transfers (counters, pass orders, retry lists,
   // statuses) go through page-locked buffers: a copy to or from pageable
   // memory blocks the calling thread inside the driver until its stream
@@ -527,7 +528,8 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   const int32_t* order = nullptr;
   BatchInfo pbi = bi;  // lengths of the pairs of the current pass
   tsu::PassChoice pc{tsu::kModeShared, 1};
-  if (all_pairs && !ctx->one_warp && h_plen) pc = tsu::band_start(uniform_band, std::max(bi.max_m, bi.max_n));
+  if (all_pairs && !ctx->one_warp && h_plen)
+    pc = tsu::band_start_in(ctx->band_start, uniform_band, std::max(bi.max_m, bi.max_n));
   if (!all_pairs) {
     const std::vector<int32_t>& bp = bands[(size_t)band];
     pbi = BatchInfo{};
@@ -541,7 +543,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * n_order, cudaMemcpyHostToDevice,
                        st));
     order = P<int32_t>(ctx->b_order);
-    pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
+    pc = tsu::band_start_in(ctx->band_start, band, std::max(pbi.max_m, pbi.max_n));
   }
   if (ctx->fit_start && !ctx->one_warp)
     pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
@@ -816,7 +818,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
       int64_t np = nc;
       tsu::PassChoice pc{tsu::kModeShared, 1};
       if (all_pairs) {
-        if (!one_warp) pc = tsu::band_start(split.uniform_band, std::max(ci.max_m, ci.max_n));
+        if (!one_warp) pc = tsu::band_start_in(ctx->band_start, split.uniform_band, std::max(ci.max_m, ci.max_n));
       } else {
         const std::vector<int32_t>& bp = split.bands[(size_t)band];
         pbi = BatchInfo{};
@@ -825,7 +827,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
           pbi.max_m = std::max(pbi.max_m, pl[i]);
           pbi.max_n = std::max(pbi.max_n, tl[i]);
         }
-        pc = tsu::band_start(band, std::max(pbi.max_m, pbi.max_n));
+        pc = tsu::band_start_in(ctx->band_start, band, std::max(pbi.max_m, pbi.max_n));
       }
       if (ctx->fit_start && !one_warp)
         pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
@@ -863,6 +865,7 @@ int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, 
     return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
   }
   ctx->device = cfg ? cfg->device : 0;
+  for (int b = 0; b < tsu::kBands; ++b) ctx->band_start[b] = tsu::band_start_table()[b];
   ctx->err_hint = (cfg && cfg->max_error_hint > 0) ? cfg->max_error_hint : 0.2;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) {
@@ -1235,6 +1238,23 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
     CU(cudaMemcpy(hs.data(), d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
   }
   return collect_status(ctx, hs.data(), n);
+}
+
+int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair) {
+  if (!ctx) return TSU_EINVAL;
+  const int gw = warps_per_pair;
+  if (band < 0 || band >= tsu::kBands || (mode != tsu::kModeShared && mode != tsu::kModeGlobal) ||
+      (gw != 1 && gw != 2 && gw != 4 && gw != 8 && gw != 16))
+    return set_err(ctx, TSU_EINVAL, "band %d, mode %d, %d warps per pair: not a rung", band, mode, gw);
+  ctx->band_start[band] = tsu::PassChoice{mode, gw};
+  return TSU_OK;
+}
+
+int tsu_get_band_start(const tsu_ctx* ctx, int band, int* mode, int* warps_per_pair) {
+  if (!ctx || band < 0 || band >= tsu::kBands || !mode || !warps_per_pair) return TSU_EINVAL;
+  *mode = ctx->band_start[band].mode;
+  *warps_per_pair = ctx->band_start[band].gw;
+  return TSU_OK;
 }
 
 int tsu_predict_bytes(tsu_ctx* ctx, const tsu_batch* b, uint32_t flags, size_t* full, size_t* min) {

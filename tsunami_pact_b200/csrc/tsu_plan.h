@@ -154,12 +154,18 @@ inline int length_band(int32_t L) {
   if (L < 16384) return 4;
   return 5;
 }
-inline PassChoice band_start(int band, int32_t maxlen) {
-  static const PassChoice kStart[kBands] = TSU_BAND_START;
-  PassChoice r = kStart[band < 0 ? 0 : (band >= kBands ? kBands - 1 : band)];
+// The starting rung of each band in a table (a context's copy of the
+// compiled one), adjusted for lengths beyond the int16 shared ring.
+inline PassChoice band_start_in(const PassChoice* table, int band, int32_t maxlen) {
+  PassChoice r = table[band < 0 ? 0 : (band >= kBands ? kBands - 1 : band)];
   if (r.mode == kModeShared && maxlen > kSharedMaxLen) r = {kModeGlobal, r.gw >= 8 ? r.gw : 8};
   return r;
 }
+inline const PassChoice* band_start_table() {
+  static const PassChoice kStart[kBands] = TSU_BAND_START;
+  return kStart;
+}
+inline PassChoice band_start(int band, int32_t maxlen) { return band_start_in(band_start_table(), band, maxlen); }
 
 // Edit-rate hint of the next retry pass.  Shared-ring passes keep the hint
 // (they fail on ring width, staging or history); from the second global pass
