@@ -207,7 +207,10 @@ int main() {
     ord = order.p;
     n_order = nretry;
     h = tsu::next_hint(h, geo.mode == tsu::kModeGlobal);
-    pc = tsu::next_pass(pc, rm, re, pm, pn, smem_optin);
+    // the ladder's global step at 8 warps: emulating 16-warp groups (one
+    // host thread per lane) is slow; the 16-warp global kernel has its own
+    // test (test_warp_groups)
+    pc = tsu::next_pass(pc, rm, re, pm, pn, smem_optin, 8);
     if (want_cigar) {
       const unsigned long long used = *cursor;
       const int64_t maxlen = std::max(pm, pn);

@@ -90,10 +90,10 @@ def test_kat_as_batch(emu, oracle, kat_cases):
 
 
 def test_regression_fixture(emu, oracle, regress_cases):
-    """The regression set up to 1 kbp (the 3 kbp pairs run in the GPU suite)."""
+    """The regression set up to 600 bp (the longer pairs run in the GPU suite)."""
     by = {}
     for c in regress_cases:
-        if len(c["p"]) <= 1000:
+        if max(len(c["p"]), len(c["t"])) <= 600:
             by.setdefault(tuple(c["pen"]), []).append((c["p"], c["t"]))
     for pen, pairs in by.items():
         check(emu, oracle, pairs, pen)
@@ -152,7 +152,8 @@ def test_score_only(emu, oracle):
         assert s == oracle.align(p, t)[0] and ops == ""
 
 
-@pytest.mark.parametrize("gw,shared", [(2, True), (4, True), (8, True), (16, True), (2, False), (8, False)])
+@pytest.mark.parametrize("gw,shared", [(2, True), (4, True), (8, True), (16, True), (2, False), (8, False),
+                                       (16, False)])
 def test_warp_groups(emu, oracle, gw, shared):
     """Several warps per pair (named barriers, partial reductions combined
     across warps), in both ring modes, with CIGARs."""

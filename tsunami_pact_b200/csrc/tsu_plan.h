@@ -99,12 +99,15 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
   return p;
 }
 
-// Retry ladder: the configuration of the pass after `prev` for pairs of at
-// most max_m x max_n that outgrew it.  The smallest group whose shared ring
-// holds the widest possible wavefront (m + n + 3 diagonals, so it cannot
-// overflow), else the largest shared group, then the global ring with 8
-// warps per pair.
-inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int32_t max_n, int smem_optin) {
+// Retry ladder: the configuration of the pass after `prev` for n_pairs pairs
+// of at most max_m x max_n that outgrew it.  The smallest group whose shared
+// ring holds the widest possible wavefront (m + n + 3 diagonals, so it cannot
+// overflow), else the largest shared group, then the global ring with
+// global_gw (16) warps per pair (the pairs that reach it are the longest and
+// most divergent ones; their count in flight is bounded by memory, not by
+// warps).
+inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int32_t max_n, int smem_optin,
+                            int global_gw = 16) {
   const int64_t need_w = (int64_t)max_m + max_n + 3;
   if (prev.mode == kModeShared && std::max(max_m, max_n) <= kSharedMaxLen) {
     const int64_t seqw =
@@ -116,7 +119,7 @@ inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int3
     }
     if (prev.gw < 16) return {kModeShared, 16};
   }
-  return {kModeGlobal, 8};
+  return {kModeGlobal, global_gw};
 }
 
 // The first rung at or above pc whose ring holds the wavefront width the

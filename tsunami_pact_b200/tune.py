@@ -1,18 +1,25 @@
 """Autotuner of the pass plan: the starting rung of each length band.
 
-For each length band (max(m, n) < 1 k, 2 k, 4 k, 8 k, 16 k, >= 16 k) it aligns
-a seeded workload of that band -- lengths log-uniform over the band, edit
-rates uniform 1-15 %, penalties 4/6/2, the uneven batched configuration --
-from every candidate rung (wavefront ring in shared memory with 1, 2, 4, 8 or
-16 warps per pair, or in device memory with 8 or 16), checks that every rung
-gives the same scores and CIGARs, and keeps the rung with the shortest device
-time of the align passes (the minimum over --reps runs after one warm-up).
+The batch engine splits a batch into length bands (max(m, n) < 1 k, 2 k,
+4 k, 8 k, 16 k, >= 16 k) and starts each band at the rung of a table.  The
+tuner takes the pairs of each band out of the workloads it is given (by
+default the uneven batched configuration, c4: lengths log-uniform 100-20,000,
+edit rates 1-15 %, and the long-read one, c3: 10 kbp at 15 %; seeded, see
+datasets.py; penalties 4/6/2), aligns them from every candidate rung
+(wavefront ring in shared memory with 1, 2, 4, 8 or 16 warps per pair, or in
+device memory with 8 or 16), checks that every rung gives the same scores and
+CIGARs, and keeps the rung with the shortest device time of the align passes
+summed over the workloads (each the minimum over --reps runs after one
+warm-up).  Bands are measured at the sizes they have in the workloads,
+because a rung's cost includes the retry passes of the pairs that outgrow
+it, whose weight depends on how many pairs share the band.
 
 It writes the table as a C header (tsunami_pact_b200/csrc/tsu_tuning.h by
 default; rebuild the library afterwards) and every measurement as JSON.
 
 usage: python -m tsunami_pact_b200.tune [--out-header PATH] [--out-json PATH]
-                                         [--reps N] [--scale F] [--device D]
+                                         [--workloads c4:100000,c3:5000]
+                                         [--reps N] [--device D]
 """
 from __future__ import annotations
 
@@ -27,27 +34,38 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BAND_NAMES = ["< 1024", "< 2048", "< 4096", "< 8192", "< 16384", ">= 16384"]
-# (shortest, longest + 1, pairs) per band
-BANDS = [(100, 1024, 40000), (1024, 2048, 16000), (2048, 4096, 6000), (4096, 8192, 2400), (8192, 16384, 800),
-         (16384, 32001, 300)]
+BAND_LIMITS = [1024, 2048, 4096, 8192, 16384]  # tsu::length_band
+N_BANDS = 6
 CANDIDATES = [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (1, 8), (1, 16)]
-SEED = 0x54554E45
+SHARED_MAX_LEN = 32000  # the int16 shared ring's limit
+DEFAULT_WORKLOADS = "c4:100000,c3:5000"
 
 
 def rung_name(r) -> str:
     return ("s" if r[0] == 0 else "g") + str(r[1])
 
 
-def band_workload(band: int, scale: float = 1.0):
-    """Seeded pairs of one band: (pbuf, poff, plen, tbuf, toff, tlen)."""
-    from . import gen_batch
+def length_band(L: np.ndarray) -> np.ndarray:
+    """The engine's length band of max(m, n) (tsu::length_band)."""
+    return np.searchsorted(np.asarray(BAND_LIMITS), L, side="right")
 
-    lo, hi, n = BANDS[band]
-    n = max(16, int(n * scale))
-    rng = np.random.Generator(np.random.PCG64(SEED + band))
-    lengths = np.exp(rng.uniform(np.log(lo), np.log(hi - 1), n)).astype(np.int32)
-    rates = rng.uniform(0.01, 0.15, n)
-    return gen_batch(SEED + band, lengths, rates)
+
+def band_batches(workloads: str):
+    """{band: [(workload, batch)]}: each workload's pairs split by band, as
+    (pbuf, poff, plen, tbuf, toff, tlen) views into the workload's buffers."""
+    from . import datasets
+
+    out = {b: [] for b in range(N_BANDS)}
+    for item in workloads.split(","):
+        name, _, n = item.partition(":")
+        pbuf, poff, plen, tbuf, toff, tlen = datasets.generate(name, int(n) if n else 0)
+        bands = length_band(np.maximum(plen, tlen))
+        for b in range(N_BANDS):
+            sel = np.nonzero(bands == b)[0]
+            if sel.size:
+                out[b].append((name, (pbuf, poff[sel].copy(), plen[sel].copy(), tbuf, toff[sel].copy(),
+                                      tlen[sel].copy())))
+    return out
 
 
 def render_header(table, source: str, times=None) -> str:
@@ -93,42 +111,57 @@ def gpu_name(device: int) -> str:
         return "unknown GPU"
 
 
-def tune(reps: int = 2, scale: float = 1.0, device: int = 0, log=print):
+def tune(workloads: str = DEFAULT_WORKLOADS, reps: int = 2, device: int = 0, log=print):
+    """Returns (table, times per band {rung: ms}, one record per measurement)."""
     import ctypes
 
     from . import Aligner, lib
 
     L = lib()
     L.tsu_set_band_start.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.tsu_get_band_start.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]
+    per_band = band_batches(workloads)
     table, times, record = [], [], []
     with Aligner(4, 6, 2, device=device) as al:
-        for band in range(len(BANDS)):
-            data = band_workload(band, scale)
-            cap = int(data[2].astype(np.int64).sum() + data[5].astype(np.int64).sum()) + 1
-            row, ref, best = {}, None, None
+        for band in range(N_BANDS):
+            if not per_band[band]:  # no pairs of this band: keep the compiled rung
+                m, w = ctypes.c_int(), ctypes.c_int()
+                L.tsu_get_band_start(al._h, band, ctypes.byref(m), ctypes.byref(w))
+                table.append((m.value, w.value))
+                times.append({})
+                continue
+            longest = max(int(np.maximum(d[2], d[5]).max()) for _, d in per_band[band])
+            row, refs, best = {}, {}, None
             for r in CANDIDATES:
-                if r[0] == 0 and BANDS[band][1] - 1 > 32000:
+                if r[0] == 0 and longest > SHARED_MAX_LEN:
                     continue
                 rc = L.tsu_set_band_start(al._h, band, r[0], r[1])
                 if rc != 0:
                     raise RuntimeError(f"tsu_set_band_start({band}, {r}) = {rc}")
-                ms = []
-                for k in range(reps + 1):
-                    s, co, runs = al.align_arrays(*data, cigar_capacity=cap)
-                    t = al.timing()
-                    if k:
-                        ms.append(t["align_ms"])
-                got = (s.copy(), co.copy(), runs.copy())
-                if ref is None:
-                    ref = got
-                elif not all(np.array_equal(a, b) for a, b in zip(ref, got)):
-                    raise RuntimeError(f"band {band}: rung {rung_name(r)} changed the results")
-                row[rung_name(r)] = min(ms)
-                record.append({"band": band, "rung": rung_name(r), "align_ms": ms, "pairs": int(len(data[2])),
-                               "passes": al.pass_log()})
-                log("band %d %-6s %8.2f ms  %s" % (band, rung_name(r), min(ms), al.pass_log()))
-                if best is None or min(ms) < row[rung_name(best)]:
-                    best = r
+                total = 0.0
+                for name, data in per_band[band]:
+                    cap = int(data[2].astype(np.int64).sum() + data[5].astype(np.int64).sum()) + 1
+                    ms = []
+                    for k in range(reps + 1):
+                        s, co, runs = al.align_arrays(*data, cigar_capacity=cap)
+                        if k:
+                            ms.append(al.timing()["align_ms"])
+                    got = (s.copy(), co.copy(), runs.copy())
+                    if name not in refs:
+                        refs[name] = got
+                    elif not all(np.array_equal(a, b) for a, b in zip(refs[name], got)):
+                        raise RuntimeError(f"band {band}: rung {rung_name(r)} changed the results of {name}")
+                    total += min(ms)
+                    record.append({"band": band, "workload": name, "pairs": int(len(data[2])), "rung": rung_name(r),
+                                   "align_ms": ms, "passes": al.pass_log()})
+                    log("band %d %-3s %-6s %6d pairs %9.2f ms  %s" % (band, name, rung_name(r), len(data[2]), min(ms),
+                                                                   al.pass_log()))
+                row[rung_name(r)] = total
+            # the fastest rung; of rungs within 1.5 % of it, the last (widest)
+            # one, whose first pass does the work the narrower ones hand on
+            fastest = min(row.values())
+            best = [r for r in CANDIDATES if rung_name(r) in row and row[rung_name(r)] <= 1.015 * fastest][-1]
             table.append(best)
             times.append(row)
             L.tsu_set_band_start(al._h, band, best[0], best[1])
@@ -139,20 +172,19 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out-header", default=os.path.join(HERE, "csrc", "tsu_tuning.h"))
     ap.add_argument("--out-json", default="")
+    ap.add_argument("--workloads", default=DEFAULT_WORKLOADS, help="name:pairs,... (tsunami_pact_b200/datasets.py)")
     ap.add_argument("--reps", type=int, default=2)
-    ap.add_argument("--scale", type=float, default=1.0, help="pairs per band x this")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
-    table, times, record = tune(args.reps, args.scale, args.device)
+    table, times, record = tune(args.workloads, args.reps, args.device)
     stamp = datetime.datetime.now(datetime.timezone.utc).strftime("%Y-%m-%d")
-    source = "tune.py on %s, %s" % (gpu_name(args.device), stamp)
+    source = "tune.py on %s, %s, workloads %s" % (gpu_name(args.device), stamp, args.workloads)
     with open(args.out_header, "w") as f:
         f.write(render_header(table, source, times))
     if args.out_json:
         with open(args.out_json, "w") as f:
-            json.dump({"source": source, "table": table, "times_ms": times, "runs": record,
-                       "bands": [{"lengths": [lo, hi - 1], "pairs": n, "rates": [0.01, 0.15]} for lo, hi, n in BANDS]},
-                      f, indent=1)
+            json.dump({"source": source, "workloads": args.workloads, "table": table, "times_ms": times,
+                       "runs": record}, f, indent=1)
     print("table:", " ".join(rung_name(r) for r in table), file=sys.stderr)
 
 
