@@ -114,8 +114,10 @@ class ClockSampler:
 
 
 def load_traffic(kernel_key: str):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/*.json), or None."""
+    """ncu figures of the dominant kernel from the committed summary
+    (profiles/traffic.json): DRAM bytes of one captured launch and the pairs
+    it processed (traffic grows in proportion to pairs), issue and ALU pipe
+    utilisation; or None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
@@ -487,12 +489,18 @@ def main():
     hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
     algo = packed_in + out_bytes + hist_bytes
     achieved = algo / (a_ms / 1e3) / 1e9
-    traffic = load_traffic(f"align_{workload}")
+    prof = load_traffic(f"align_{workload}") if want_cigar else None
+    traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
             "align_kernel<score>", "kernel_ms": a_ms,
             "algorithmic_bytes_per_launch": algo,
             "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log}
+    if prof:
+        # the binding resource of this integer kernel is instruction issue, not DRAM
+        roof["issue_active_frac"] = prof.get("issue_active_frac")
+        roof["alu_pipe_frac"] = prof.get("alu_pipe_frac")
+        roof["traffic_source"] = prof.get("source")
 
     if rank == 0:
         cpu = None

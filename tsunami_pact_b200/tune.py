@@ -3,9 +3,10 @@
 The batch engine splits a batch into length bands (max(m, n) < 1 k, 2 k,
 4 k, 8 k, 16 k, >= 16 k) and starts each band at the rung of a table.  The
 tuner takes the pairs of each band out of the workloads it is given (by
-default the uneven batched configuration, c4: lengths log-uniform 100-20,000,
-edit rates 1-15 %, and the long-read one, c3: 10 kbp at 15 %; seeded, see
-datasets.py; penalties 4/6/2), aligns them from every candidate rung
+default the uniform 1 kbp configuration, c2: 1 kbp at 5 %, the uneven
+batched one, c4: lengths log-uniform 100-20,000, edit rates 1-15 %, and the
+long-read one, c3: 10 kbp at 15 %; seeded, see datasets.py; penalties
+4/6/2), aligns them from every candidate rung
 (wavefront ring in shared memory with 1, 2, 4, 8 or 16 warps per pair, or in
 device memory with 8 or 16), checks that every rung gives the same scores and
 CIGARs, and keeps the rung with the shortest device time of the align passes
@@ -18,7 +19,7 @@ It writes the table as a C header (tsunami_pact_b200/csrc/tsu_tuning.h by
 default; rebuild the library afterwards) and every measurement as JSON.
 
 usage: python -m tsunami_pact_b200.tune [--out-header PATH] [--out-json PATH]
-                                         [--workloads c4:100000,c3:5000]
+                                         [--workloads c2:200000,c4:100000,c3:5000]
                                          [--reps N] [--device D]
 """
 from __future__ import annotations
@@ -38,7 +39,7 @@ BAND_LIMITS = [1024, 2048, 4096, 8192, 16384]  # tsu::length_band
 N_BANDS = 6
 CANDIDATES = [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (1, 8), (1, 16)]
 SHARED_MAX_LEN = 32000  # the int16 shared ring's limit
-DEFAULT_WORKLOADS = "c4:100000,c3:5000"
+DEFAULT_WORKLOADS = "c2:200000,c4:100000,c3:5000"
 
 
 def rung_name(r) -> str:
