@@ -104,7 +104,10 @@ typedef struct {
 } tsu_result;
 
 /* Timing of the last align call, measured with CUDA events on the context's
- * stream (milliseconds). */
+ * stream (milliseconds).  A call's fixed launch sequence (packing, the first
+ * pass of every length band, counter read-back) runs as one CUDA graph kept
+ * by the context and updated in place from call to call; set TSU_GRAPH=0 in
+ * the environment before tsu_create to queue the same launches directly. */
 typedef struct {
   double h2d_ms, pack_ms, align_ms, compact_ms, d2h_ms, total_ms;
   int64_t kernel_launches; /* kernels of this library launched by the call */

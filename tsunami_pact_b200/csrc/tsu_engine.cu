@@ -16,6 +16,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -67,7 +68,7 @@ struct tsu_ctx {
   DevBuf b_words_cnt, b_woff, b_words, b_nonacgt;         // packing
   DevBuf b_score, b_status, b_cpos, b_clen, b_clen64, b_coff, b_out;  // outputs
   DevBuf b_order, b_retry, b_counters;                    // queue, retry list, counters
-  DevBuf b_ring, b_hist, b_table, b_arena, b_scan_tmp;    // scratch
+  DevBuf b_scratch, b_arena, b_scan_tmp;                  // wavefront scratch of a pass (carve_scratch), CIGAR arena
   DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
   bool one_warp = false;  // TSU_ONE_WARP of the current call
   cudaEvent_t pev[2] = {};  // per-pass timing
@@ -91,12 +92,20 @@ struct tsu_ctx {
   // request server, whose many worker threads would otherwise spin on all
   // the host's cores); batch callers keep the driver's default.
   bool blocking_sync = false;
+  // The call's fixed launch sequence runs as a CUDA graph, captured anew on
+  // each call and updated into this executable graph (re-instantiated when
+  // its shape changes).
+  bool use_graph = true;
+  bool capturing = false;
+  cudaGraphExec_t gexec = nullptr;
+  int64_t graph_launches = 0;
+  cudaEvent_t bev[2 * tsu::kBands] = {};  // first pass of each band: start, end
   cudaEvent_t wait_ev = nullptr;  // blocking-sync event of those waits
   size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
             &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
-            &b_retry, &b_counters, &b_ring,  &b_hist, &b_table, &b_arena, &b_scan_tmp,  &b_out2};
+            &b_retry, &b_counters, &b_scratch, &b_arena, &b_scan_tmp, &b_out2};
   }
   size_t held() const {
     size_t s = 0;
@@ -382,7 +391,7 @@ int plan_pass_within(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::Pa
 // and `reserve` bytes that later steps of the call still need.
 int plan_pass(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint, bool want_cigar,
               size_t reserve, Pass* out) {
-  const size_t fixed = ctx->held() - ctx->b_hist.cap - ctx->b_table.cap - ctx->b_ring.cap + reserve;
+  const size_t fixed = ctx->held() - ctx->b_scratch.cap + reserve;
   const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
   return plan_pass_within(ctx, bi, n_pairs, pc, hint, want_cigar, avail, out);
 }
@@ -427,12 +436,100 @@ void split_bands(int64_t n, const int32_t* h_plen, const int32_t* h_tlen, BandSp
   for (int32_t i : by_len) out->bands[(size_t)tsu::length_band(std::max(h_plen[i], h_tlen[i]))].push_back(i);
 }
 
+// Record an event on the stream; inside a stream capture as an event node
+// that the graph records when it runs.
+cudaError_t record(tsu_ctx* ctx, cudaEvent_t ev, cudaStream_t st) {
+  return ctx->capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
+}
+
+// Queue the work of enqueue() on st: captured as a CUDA graph, updated into
+// the context's executable graph (instantiated anew when the update is
+// refused: another shape) and launched; or, with ctx->use_graph off, queued
+// directly.  enqueue() only queues stream work (no allocation, no
+// synchronisation).
+template <class F>
+int run_graph(tsu_ctx* ctx, cudaStream_t st, F&& enqueue) {
+  if (!ctx->use_graph) return enqueue();
+  CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  ctx->capturing = true;
+  const int rc = enqueue();
+  ctx->capturing = false;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc;
+  }
+  if (e != cudaSuccess) return set_err(ctx, TSU_EDEVICE, "stream capture failed: %s", cudaGetErrorString(e));
+  bool updated = false;
+  if (ctx->gexec) {
+    cudaGraphExecUpdateResultInfo info{};
+    updated = cudaGraphExecUpdate(ctx->gexec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ctx->gexec);
+      ctx->gexec = nullptr;
+    }
+  }
+  if (!updated) {
+    const cudaError_t ei = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    if (ei != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      ctx->gexec = nullptr;
+      return set_err(ctx, TSU_EDEVICE, "graph instantiation failed: %s", cudaGetErrorString(ei));
+    }
+  }
+  cudaGraphDestroy(graph);
+  CU(cudaGraphLaunch(ctx->gexec, st));
+  ++ctx->graph_launches;
+  return TSU_OK;
+}
+
+// Scratch of a pass, carved from one buffer: backtrace words, step table,
+// global ring, each 256-byte aligned.
+size_t scratch_bytes(const Pass& ps, bool cigar) {
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t groups = (size_t)ps.groups;
+  size_t b = 0;
+  if (cigar) b += up(4 * groups * (size_t)ps.g.hist_cap) + up(8 * groups * (size_t)ps.g.table_cap);
+  if (ps.g.mode == tsu::kModeGlobal) b += up(4 * groups * (size_t)ps.g.ring_ints);
+  return std::max<size_t>(b, 256);
+}
+
+void carve_scratch(tsu_ctx* ctx, const Pass& ps, bool cigar, tsu::AlignArgs* a) {
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  char* p = P<char>(ctx->b_scratch);
+  const size_t groups = (size_t)ps.groups;
+  a->hist = nullptr;
+  a->table = nullptr;
+  a->ring_global = nullptr;
+  if (cigar) {
+    a->hist = reinterpret_cast<uint32_t*>(p);
+    p += up(4 * groups * (size_t)ps.g.hist_cap);
+    a->table = reinterpret_cast<int2*>(p);
+    p += up(8 * groups * (size_t)ps.g.table_cap);
+  }
+  if (ps.g.mode == tsu::kModeGlobal) a->ring_global = reinterpret_cast<int32_t*>(p);
+}
+
 // Core: inputs resident on the device (sv).  Writes score/status (device)
 // and, for CIGARs, compacts runs into out_runs with offsets out_off
 // (device, n+1 entries).  *runs_needed receives the total.
 // When d_out_runs is null the runs go to the context buffer *out_buf (b_out
 // unless given; grown to fit) and *out_used receives its address.
-// h_plen/h_tlen: the same lengths in host memory (used to plan retry passes).
+// h_plen/h_tlen: the same lengths in host memory (used to plan the passes).
+//
+// Pairs are split into length bands (tsu::length_band of max(m, n)), each
+// band ordered longest first (a counting sort by floor(log2(m + n))) and
+// started at its rung (the context's band table, tsu_set_band_start), with
+// scratch sized for its longest pair, so short pairs run many to an SM and
+// long ones get warp groups.  The call's fixed launch sequence -- word
+// counts, scan, packing, pass orders up, counters cleared, the first pass of
+// every band (longest band first), counters down -- is one CUDA graph; pairs
+// that outgrew their band's first rung then climb the retry ladder, band by
+// band, in passes the host plans from their lengths.  TSU_ONE_WARP keeps one
+// band in input order starting at one warp per pair.
 int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d_score, int32_t* d_status,
                uint32_t* d_out_runs, int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, BatchInfo bi,
                const int32_t* h_plen, const int32_t* h_tlen, uint32_t** out_used = nullptr,
@@ -445,36 +542,23 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     if (want_cigar && d_out_off) CU(cudaMemsetAsync(d_out_off, 0, sizeof(int64_t), st));
     return TSU_OK;
   }
-  // ---- word counts + scan -> packed offsets
+  // ---- buffers (all grown before the launch sequence is captured)
   if ((rc = grow(ctx, ctx->b_words_cnt, sizeof(int64_t) * 2 * n))) return rc;
   if ((rc = grow(ctx, ctx->b_woff, sizeof(int64_t) * 2 * n))) return rc;
-  tsu::word_count_kernel<<<std::min<int64_t>((2 * n + 255) / 256, 4096), 256, 0, st>>>(n, sv.pat_len, sv.txt_len,
-                                                                                        P<int64_t>(ctx->b_words_cnt));
-  ctx->timing.kernel_launches++;
   size_t tmp_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff), (int)(2 * n), st);
   if ((rc = grow(ctx, ctx->b_scan_tmp, tmp_bytes))) return rc;
-  CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tmp_bytes, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff),
-                                   (int)(2 * n), st));
-  ctx->timing.kernel_launches++;
   if ((rc = grow(ctx, ctx->b_words, sizeof(uint64_t) * (size_t)bi.total_words))) return rc;
   if ((rc = grow(ctx, ctx->b_nonacgt, (size_t)(2 * n)))) return rc;
-  tsu::PackView pk{P<uint64_t>(ctx->b_words), P<int64_t>(ctx->b_woff), P<uint8_t>(ctx->b_nonacgt)};
-  CU(cudaEventRecord(ctx->ev[2], st));
-  {
-    const int64_t blocks = std::min<int64_t>((2 * n + 7) / 8, (int64_t)ctx->sms * 16);
-    tsu::pack_kernel<<<(int)blocks, 256, 0, st>>>(sv, pk);
-    ctx->timing.kernel_launches++;
-  }
-  CU(cudaGetLastError());
-  CU(cudaEventRecord(ctx->ev[3], st));
-
-  // ---- outputs/queues
+  const tsu::PackView pk{P<uint64_t>(ctx->b_words), P<int64_t>(ctx->b_woff), P<uint8_t>(ctx->b_nonacgt)};
   if ((rc = grow(ctx, ctx->b_cpos, sizeof(int64_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_clen, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_retry, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_order, sizeof(int32_t) * n))) return rc;
-  if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
+  // counters: +16 arena cursor, +24 work (cells, steps), +64 + 8b queue head
+  // and retry count of band slot b
+  constexpr size_t kCounterBytes = 64 + 8 * tsu::kBands;
+  if ((rc = grow(ctx, ctx->b_counters, kCounterBytes))) return rc;
   const int min_pen = std::min(ctx->x, ctx->go);
   int64_t arena_cap = 0;
   if (want_cigar) {
@@ -495,82 +579,78 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     if (!want_cigar || d_out_runs) return 0;
     const DevBuf& ob = out_buf ? *out_buf : ctx->b_out;
     const size_t need = (sizeof(uint32_t) * (size_t)std::min<int64_t>(arena_cap, len_sum + 1) + 255) & ~(size_t)255;
-    return need > ob.cap ? need - ob.cap : 0;
+    return (need > ob.cap ? need - ob.cap : 0) + 1024;  // + the scratch carving's alignment
   };
-  unsigned int* d_queue = P<unsigned int>(ctx->b_counters);
-  unsigned int* d_retry_cnt = d_queue + 1;
-  unsigned long long* d_cursor = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 16);
-  CU(cudaMemsetAsync(ctx->b_counters.p, 0, 64, st));
+  char* const d_cnt = P<char>(ctx->b_counters);
+  unsigned long long* const d_cursor = reinterpret_cast<unsigned long long*>(d_cnt + 16);
+  unsigned long long* const d_work = reinterpret_cast<unsigned long long*>(d_cnt + 24);
+  char* const h_cnt = static_cast<char*>(ctx->h_scalars.p);  // page-locked copy of the counters
 
-  // ---- passes
-  // Pairs are split into length bands (tsu::length_band of max(m, n)); each
-  // band runs its own ladder of passes from the band's starting rung
-  // (tsu::band_start), with scratch sized for that band's longest pair, so
-  // short pairs run many to an SM and long ones get warp groups.  Bands run
-  // longest first; inside a band pairs are ordered longest first (a counting
-  // sort by floor(log2(m + n))).  TSU_ONE_WARP keeps one band in input order
-  // starting at one warp per pair.
-  int passes = 0;
+  // ---- bands: pairs, first rung and first pass plan, longest band first
+  struct BandRun {
+    int band = 0, slot = 0;
+    int64_t off = 0, n = 0;  // slice of the pass order / retry list
+    BatchInfo bi;
+    tsu::PassChoice pc;
+    double hint = 0;
+    Pass ps;
+  };
   BandSplit split;
   if (!ctx->one_warp && h_plen) split_bands(n, h_plen, h_tlen, &split);
-  const std::vector<std::vector<int32_t>>& bands = split.bands;
-  const bool uniform = split.uniform;
-  const int uniform_band = split.uniform_band;
-  CU(cudaEventRecord(ctx->ev[4], st));
-  std::string passlog;  // mode, warps per pair x groups : pairs, per pass (for error messages)
-  std::vector<int32_t> rlist;
-  for (int band = tsu::kBands - 1; band >= 0; --band) {
-  const bool all_pairs = ctx->one_warp || !h_plen || uniform;  // a single band of every pair, input order
-  if (all_pairs && band != 0) continue;
-  if (!all_pairs && bands[(size_t)band].empty()) continue;
-  double hint = ctx->err_hint;
-  int64_t n_order = all_pairs ? n : (int64_t)bands[(size_t)band].size();
-  const int32_t* order = nullptr;
-  BatchInfo pbi = bi;  // lengths of the pairs of the current pass
-  tsu::PassChoice pc{tsu::kModeShared, 1};
-  if (all_pairs && !ctx->one_warp && h_plen)
-    pc = tsu::band_start_in(ctx->band_start, uniform_band, std::max(bi.max_m, bi.max_n));
-  if (!all_pairs) {
-    const std::vector<int32_t>& bp = bands[(size_t)band];
-    pbi = BatchInfo{};
-    pbi.n = n_order;
-    for (int32_t i : bp) {
-      pbi.max_m = std::max(pbi.max_m, h_plen[i]);
-      pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
-    }
-    if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * (size_t)n_order))) return rc;
-    memcpy(ctx->h_list.p, bp.data(), sizeof(int32_t) * (size_t)n_order);  // the previous list's copy is done
-    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * n_order, cudaMemcpyHostToDevice,
-                       st));
-    order = P<int32_t>(ctx->b_order);
-    pc = tsu::band_start_in(ctx->band_start, band, std::max(pbi.max_m, pbi.max_n));
-  }
-  if (ctx->fit_start && !ctx->one_warp)
-    pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
-  CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
-  const int band_first_pass = passes;
-  for (;;) {
-    Pass ps;
-    if ((rc = plan_pass(ctx, pbi, n_order, pc, hint, want_cigar, out_reserve(), &ps))) return rc;
-    const tsu::PassGeom& g = ps.g;
-    {
-      // plan_pass counted the scratch buffers as free: if any of them must
-      // grow, release all three first so the budget holds during regrowth
-      const size_t need_ring = g.mode == tsu::kModeGlobal ? sizeof(int32_t) * (size_t)ps.groups * g.ring_ints : 0;
-      const size_t need_hist = want_cigar ? sizeof(uint32_t) * (size_t)ps.groups * g.hist_cap : 0;
-      const size_t need_table = want_cigar ? sizeof(int2) * (size_t)ps.groups * g.table_cap : 0;
-      if (need_ring > ctx->b_ring.cap || need_hist > ctx->b_hist.cap || need_table > ctx->b_table.cap) {
-        CU(wait_stream(ctx, st));
-        release(ctx, ctx->b_ring);
-        release(ctx, ctx->b_hist);
-        release(ctx, ctx->b_table);
+  const bool all_pairs = ctx->one_warp || !h_plen || split.uniform;  // one band of every pair, input order
+  std::vector<BandRun> runs;
+  std::vector<int32_t> order_all;
+  if (all_pairs) {
+    BandRun r;
+    r.n = n;
+    r.bi = bi;
+    r.pc = tsu::PassChoice{tsu::kModeShared, 1};
+    if (!ctx->one_warp && h_plen) r.pc = tsu::band_start_in(ctx->band_start, split.uniform_band, std::max(bi.max_m, bi.max_n));
+    runs.push_back(r);
+  } else {
+    for (int band = tsu::kBands - 1; band >= 0; --band) {
+      const std::vector<int32_t>& bp = split.bands[(size_t)band];
+      if (bp.empty()) continue;
+      BandRun r;
+      r.band = band;
+      r.off = (int64_t)order_all.size();
+      r.n = (int64_t)bp.size();
+      r.bi.n = r.n;
+      for (int32_t i : bp) {
+        r.bi.max_m = std::max(r.bi.max_m, h_plen[i]);
+        r.bi.max_n = std::max(r.bi.max_n, h_tlen[i]);
       }
-      passlog += (passlog.empty() ? "" : " ") + std::string(g.mode == tsu::kModeShared ? "s" : "g") +
-                 std::to_string(g.gw) + "x" + std::to_string(ps.groups) + ":" + std::to_string(n_order);
-      if (need_ring && (rc = grow(ctx, ctx->b_ring, need_ring))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
-      if (need_hist && (rc = grow(ctx, ctx->b_hist, need_hist))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
-      if (need_table && (rc = grow(ctx, ctx->b_table, need_table))) return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
+      r.pc = tsu::band_start_in(ctx->band_start, band, std::max(r.bi.max_m, r.bi.max_n));
+      order_all.insert(order_all.end(), bp.begin(), bp.end());
+      runs.push_back(r);
     }
+  }
+  {
+    // first passes run one after the other in one scratch buffer sized for
+    // the largest; each is planned within what the other buffers leave
+    const size_t fixed = ctx->held() - ctx->b_scratch.cap + out_reserve();
+    const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+    size_t need = 0;
+    for (size_t k = 0; k < runs.size(); ++k) {
+      BandRun& r = runs[k];
+      r.slot = (int)k;
+      r.hint = ctx->err_hint;
+      if (ctx->fit_start && !ctx->one_warp)
+        r.pc = tsu::fit_start(r.pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, r.bi.max_m, r.bi.max_n, r.hint,
+                              ctx->smem_optin);
+      if ((rc = plan_pass_within(ctx, r.bi, r.n, r.pc, r.hint, want_cigar, avail, &r.ps))) return rc;
+      need = std::max(need, scratch_bytes(r.ps, want_cigar));
+    }
+    if (need > ctx->b_scratch.cap) {
+      release(ctx, ctx->b_scratch);
+      if ((rc = grow(ctx, ctx->b_scratch, need))) return rc;
+    }
+  }
+  if (!order_all.empty()) {
+    if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * order_all.size()))) return rc;
+    memcpy(ctx->h_list.p, order_all.data(), sizeof(int32_t) * order_all.size());
+  }
+  auto align_args = [&](const Pass& ps, const int32_t* order, int64_t n_order, int slot, int32_t* retry) {
     tsu::AlignArgs a{};
     a.seq = sv;
     a.pk = pk;
@@ -582,14 +662,12 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.g = ctx->g;
     a.rm = ctx->rm;
     a.re = ctx->re;
-    a.ring_w = g.ring_w;
-    a.seq_cap = g.seq_cap;
-    a.ring_global = g.mode == tsu::kModeShared ? nullptr : P<int32_t>(ctx->b_ring);
-    a.ring_stride = g.ring_ints;
-    a.hist = want_cigar ? P<uint32_t>(ctx->b_hist) : nullptr;
-    a.hist_cap = g.hist_cap;
-    a.table = want_cigar ? P<int2>(ctx->b_table) : nullptr;
-    a.table_cap = g.table_cap;
+    a.ring_w = ps.g.ring_w;
+    a.seq_cap = ps.g.seq_cap;
+    carve_scratch(ctx, ps, want_cigar, &a);
+    a.ring_stride = ps.g.ring_ints;
+    a.hist_cap = ps.g.hist_cap;
+    a.table_cap = ps.g.table_cap;
     a.score = d_score;
     a.status = d_status;
     a.arena = want_cigar ? P<uint32_t>(ctx->b_arena) : nullptr;
@@ -597,91 +675,162 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.arena_cap = arena_cap;
     a.cig_pos = P<int64_t>(ctx->b_cpos);
     a.cig_len = P<int32_t>(ctx->b_clen);
-    a.queue = d_queue;
-    a.retry = P<int32_t>(ctx->b_retry);
-    a.retry_count = d_retry_cnt;
-    a.work = reinterpret_cast<unsigned long long*>(P<char>(ctx->b_counters) + 24);
-    CU(cudaEventRecord(ctx->pev[0], st));
-    launch_align(want_cigar, g.mode, g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
-    ctx->timing.kernel_launches++;
+    a.queue = reinterpret_cast<unsigned int*>(d_cnt + 64 + 8 * slot);
+    a.retry = retry;
+    a.retry_count = a.queue + 1;
+    a.work = d_work;
+    return a;
+  };
+  std::string passlog;  // mode, warps per pair x groups : pairs @ time, per pass (for error messages)
+  auto log_pass = [&](const Pass& ps, int64_t pairs) {
+    passlog += (passlog.empty() ? "" : " ") + std::string(ps.g.mode == tsu::kModeShared ? "s" : "g") +
+               std::to_string(ps.g.gw) + "x" + std::to_string(ps.groups) + ":" + std::to_string(pairs);
+  };
+
+  // ---- the fixed launch sequence of the call (one CUDA graph)
+  rc = run_graph(ctx, st, [&]() -> int {
+    CU(record(ctx, ctx->ev[2], st));
+    tsu::word_count_kernel<<<std::min<int64_t>((2 * n + 255) / 256, 4096), 256, 0, st>>>(
+        n, sv.pat_len, sv.txt_len, P<int64_t>(ctx->b_words_cnt));
+    size_t tb = tmp_bytes;
+    CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tb, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff),
+                                     (int)(2 * n), st));
+    const int64_t blocks = std::min<int64_t>((2 * n + 7) / 8, (int64_t)ctx->sms * 16);
+    tsu::pack_kernel<<<(int)blocks, 256, 0, st>>>(sv, pk);
     CU(cudaGetLastError());
-    CU(cudaEventRecord(ctx->pev[1], st));
-    ++passes;
-    unsigned int* h_nretry = static_cast<unsigned int*>(ctx->h_scalars.p);
-    CU(cudaMemcpyAsync(h_nretry, d_retry_cnt, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-    CU(wait_stream(ctx, st));
-    const unsigned int nretry = *h_nretry;
-    {
+    CU(record(ctx, ctx->ev[3], st));
+    if (!order_all.empty())
+      CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * order_all.size(),
+                         cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(d_cnt, 0, kCounterBytes, st));
+    CU(record(ctx, ctx->ev[4], st));
+    for (const BandRun& r : runs) {
+      const tsu::AlignArgs a = align_args(r.ps, all_pairs ? nullptr : P<int32_t>(ctx->b_order) + r.off, r.n, r.slot,
+                                          P<int32_t>(ctx->b_retry) + r.off);
+      CU(record(ctx, ctx->bev[2 * r.slot], st));
+      launch_align(want_cigar, r.ps.g.mode, r.ps.g.gw, r.ps.blocks, r.ps.threads, r.ps.smem_bytes, st, a);
+      CU(cudaGetLastError());
+      CU(record(ctx, ctx->bev[2 * r.slot + 1], st));
+    }
+    CU(cudaMemcpyAsync(h_cnt, d_cnt, kCounterBytes, cudaMemcpyDeviceToHost, st));
+    return TSU_OK;
+  });
+  if (rc) return rc;
+  ctx->timing.kernel_launches += 3 + (int64_t)runs.size();
+  CU(wait_stream(ctx, st));
+  std::vector<unsigned int> first_retry(runs.size());
+  for (const BandRun& r : runs) {
+    first_retry[(size_t)r.slot] = *reinterpret_cast<const unsigned int*>(h_cnt + 64 + 8 * r.slot + 4);
+    log_pass(r.ps, r.n);
+    char t[48];
+    snprintf(t, sizeof t, "@%.1fms", ev_ms(ctx->bev[2 * r.slot], ctx->bev[2 * r.slot + 1]));
+    passlog += t;
+  }
+  ctx->passlog = passlog;
+  int passes = (int)runs.size();
+
+  // ---- retry ladders: per band, the pairs that outgrew its last rung
+  bool laddered = false;
+  std::vector<int32_t> rlist;
+  for (const BandRun& r : runs) {
+    unsigned int nretry = first_retry[(size_t)r.slot];
+    if (nretry == 0) continue;
+    laddered = true;
+    tsu::PassChoice pc = r.pc;
+    double hint = r.hint;
+    int last_mode = r.ps.g.mode;
+    int32_t* const d_order = P<int32_t>(ctx->b_order) + r.off;  // this band's slices
+    int32_t* const d_retry = P<int32_t>(ctx->b_retry) + r.off;
+    unsigned int* const d_slot = reinterpret_cast<unsigned int*>(d_cnt + 64 + 8 * r.slot);
+    const int band_first_pass = passes - 1;
+    for (;;) {
+      ctx->timing.retried_pairs += nretry;
+      if (passes - band_first_pass > 24)
+        return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes [passes %s]", passes, passlog.c_str());
+      if (last_mode == tsu::kModeGlobal && hint >= tsu::kHintCeiling)
+        return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget [passes %s]",
+                       nretry, passlog.c_str());
+      // The retry list, longest pairs first, becomes the next pass's order;
+      // its lengths pick the next rung.  Global passes grow the hint.
+      rlist.resize(nretry);
+      if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * nretry))) return rc;
+      CU(cudaMemcpyAsync(ctx->h_list.p, d_retry, sizeof(int32_t) * nretry, cudaMemcpyDeviceToHost, st));
+      CU(wait_stream(ctx, st));
+      memcpy(rlist.data(), ctx->h_list.p, sizeof(int32_t) * nretry);
+      BatchInfo pbi;
+      pbi.n = nretry;
+      for (int32_t i : rlist) {
+        pbi.max_m = std::max(pbi.max_m, h_plen[i]);
+        pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
+      }
+      std::sort(rlist.begin(), rlist.end(),
+                [&](int32_t u, int32_t v) { return (int64_t)h_plen[u] + h_tlen[u] > (int64_t)h_plen[v] + h_tlen[v]; });
+      memcpy(ctx->h_list.p, rlist.data(), sizeof(int32_t) * nretry);
+      CU(cudaMemcpyAsync(d_order, ctx->h_list.p, sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
+      hint = tsu::next_hint(hint, last_mode == tsu::kModeGlobal);
+      pc = ctx->one_warp ? tsu::PassChoice{tsu::kModeGlobal, 1}
+                         : tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
+      if (want_cigar) {
+        unsigned long long* h_used = reinterpret_cast<unsigned long long*>(h_cnt + 16);
+        CU(cudaMemcpyAsync(h_used, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        CU(wait_stream(ctx, st));
+        const unsigned long long used = *h_used;
+        const int64_t maxlen = std::max(pbi.max_m, pbi.max_n);
+        const int64_t need =
+            (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
+        if (need > arena_cap) {
+          // keep the runs written so far: grow by copy
+          DevBuf nb;
+          const size_t bytes = (sizeof(uint32_t) * (size_t)need + 255) & ~(size_t)255;
+          if (ctx->held() + bytes > ctx->budget) {
+            ctx->need_bytes = ctx->held() + bytes;
+            return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
+          }
+          CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
+          nb.cap = bytes;
+          const int64_t keep = std::min<int64_t>((int64_t)used, arena_cap);
+          CU(cudaMemcpyAsync(nb.p, ctx->b_arena.p, sizeof(uint32_t) * (size_t)keep, cudaMemcpyDeviceToDevice, st));
+          release(ctx, ctx->b_arena);
+          ctx->b_arena = nb;
+          arena_cap = need;
+        }
+      }
+      Pass ps;
+      if ((rc = plan_pass(ctx, pbi, nretry, pc, hint, want_cigar, out_reserve(), &ps))) return rc;
+      log_pass(ps, nretry);
+      const size_t need = scratch_bytes(ps, want_cigar);
+      if (need > ctx->b_scratch.cap) {
+        release(ctx, ctx->b_scratch);  // plan_pass counted the scratch as free
+        if ((rc = grow(ctx, ctx->b_scratch, need)))
+          return set_err(ctx, rc, "%s [passes %s]", ctx->err.c_str(), passlog.c_str());
+      }
+      CU(cudaMemsetAsync(d_slot, 0, 8, st));  // queue head + retry count
+      const tsu::AlignArgs a = align_args(ps, d_order, nretry, r.slot, d_retry);
+      CU(cudaEventRecord(ctx->pev[0], st));
+      launch_align(want_cigar, ps.g.mode, ps.g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
+      ctx->timing.kernel_launches++;
+      CU(cudaGetLastError());
+      CU(cudaEventRecord(ctx->pev[1], st));
+      ++passes;
+      last_mode = ps.g.mode;
+      unsigned int* h_nretry = reinterpret_cast<unsigned int*>(h_cnt + 64 + 8 * r.slot + 4);
+      CU(cudaMemcpyAsync(h_nretry, d_slot + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+      CU(wait_stream(ctx, st));
+      nretry = *h_nretry;
       char t[48];
       snprintf(t, sizeof t, "@%.1fms", ev_ms(ctx->pev[0], ctx->pev[1]));
       passlog += t;
       ctx->passlog = passlog;
+      if (nretry == 0) break;
     }
-    if (nretry == 0) break;
-    ctx->timing.retried_pairs += nretry;
-    if (passes - band_first_pass > 24)
-      return set_err(ctx, TSU_EINTERNAL, "pairs still fail after %d passes [passes %s]", passes, passlog.c_str());
-    if (g.mode == tsu::kModeGlobal && hint >= tsu::kHintCeiling)
-      return set_err(ctx, TSU_ENOMEM, "%u pairs exceed the scratch one group can hold within the budget [passes %s]",
-                     nretry, passlog.c_str());
-    // The retry list, longest pairs first, becomes the next pass's order; its
-    // lengths pick the next rung of the ladder.  Global passes grow the hint.
-    rlist.resize(nretry);
-    if ((rc = host_grow(ctx, ctx->h_list, sizeof(int32_t) * nretry))) return rc;
-    CU(cudaMemcpyAsync(ctx->h_list.p, P<int32_t>(ctx->b_retry), sizeof(int32_t) * nretry, cudaMemcpyDeviceToHost, st));
-    CU(wait_stream(ctx, st));
-    memcpy(rlist.data(), ctx->h_list.p, sizeof(int32_t) * nretry);
-    pbi = BatchInfo{};
-    pbi.n = nretry;
-    for (int32_t i : rlist) {
-      pbi.max_m = std::max(pbi.max_m, h_plen[i]);
-      pbi.max_n = std::max(pbi.max_n, h_tlen[i]);
-    }
-    std::sort(rlist.begin(), rlist.end(),
-              [&](int32_t u, int32_t v) { return (int64_t)h_plen[u] + h_tlen[u] > (int64_t)h_plen[v] + h_tlen[v]; });
-    memcpy(ctx->h_list.p, rlist.data(), sizeof(int32_t) * nretry);
-    CU(cudaMemcpyAsync(P<int32_t>(ctx->b_order), ctx->h_list.p, sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
-    order = P<int32_t>(ctx->b_order);
-    n_order = nretry;
-    hint = tsu::next_hint(hint, g.mode == tsu::kModeGlobal);
-    pc = ctx->one_warp ? tsu::PassChoice{tsu::kModeGlobal, 1}
-                       : tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
-    if (want_cigar) {
-      unsigned long long* h_used = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 8);
-      CU(cudaMemcpyAsync(h_used, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-      CU(wait_stream(ctx, st));
-      const unsigned long long used = *h_used;
-      const int64_t maxlen = std::max(pbi.max_m, pbi.max_n);
-      const int64_t need = (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
-      if (need > arena_cap) {
-        // keep the runs written so far: grow by copy
-        DevBuf nb;
-        const size_t bytes = (sizeof(uint32_t) * (size_t)need + 255) & ~(size_t)255;
-        if (ctx->held() + bytes > ctx->budget) {
-          ctx->need_bytes = ctx->held() + bytes;
-          return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
-        }
-        CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
-        nb.cap = bytes;
-        const int64_t keep = std::min<int64_t>((int64_t)used, arena_cap);
-        CU(cudaMemcpyAsync(nb.p, ctx->b_arena.p, sizeof(uint32_t) * (size_t)keep, cudaMemcpyDeviceToDevice, st));
-        release(ctx, ctx->b_arena);
-        ctx->b_arena = nb;
-        arena_cap = need;
-      }
-    }
-    CU(cudaMemsetAsync(d_queue, 0, 8, st));  // queue head + retry count
   }
-  }  // bands
   CU(cudaEventRecord(ctx->ev[5], st));
-  {
-    unsigned long long* work = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 16);
-    CU(cudaMemcpyAsync(work, P<char>(ctx->b_counters) + 24, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                       st));
+  if (laddered) {
+    CU(cudaMemcpyAsync(h_cnt + 24, d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CU(wait_stream(ctx, st));
-    ctx->timing.cells = (int64_t)work[0];
-    ctx->timing.steps = (int64_t)work[1];
   }
+  ctx->timing.cells = (int64_t)reinterpret_cast<const unsigned long long*>(h_cnt + 24)[0];
+  ctx->timing.steps = (int64_t)reinterpret_cast<const unsigned long long*>(h_cnt + 24)[1];
 
   // ---- CIGAR compaction
   if (want_cigar) {
@@ -903,7 +1052,13 @@ int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, 
     cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking);
   }
   ctx->pool = device_pool(ctx->device);
-  if (!ctx->pool || host_grow(ctx, ctx->h_scalars, 64) != TSU_OK) {
+  for (auto& ev : ctx->bev) cudaEventCreate(&ev);
+  {
+    // TSU_GRAPH=0 queues the launch sequence directly instead of as a graph
+    const char* gv = getenv("TSU_GRAPH");
+    ctx->use_graph = !(gv && gv[0] == '0');
+  }
+  if (!ctx->pool || host_grow(ctx, ctx->h_scalars, 256) != TSU_OK) {
     tsu_destroy(ctx);
     return TSU_EDEVICE;
   }
@@ -992,6 +1147,8 @@ int tsu_destroy(tsu_ctx* ctx) {
   }
   for (auto& ev : ctx->cev_t) cudaEventDestroy(ev);
   if (ctx->wait_ev) cudaEventDestroy(ctx->wait_ev);
+  for (auto& ev : ctx->bev) cudaEventDestroy(ev);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   for (HostBuf* hb : {&ctx->h_scalars, &ctx->h_list, &ctx->h_status})
     if (hb->p) cudaFreeHost(hb->p);
   if (ctx->h2d_stream && ctx->h2d_stream != ctx->stream) cudaStreamDestroy(ctx->h2d_stream);
