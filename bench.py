@@ -50,12 +50,12 @@ def dist_env():
     return rank, world, local
 
 
-def make_batch(workload: str, rank: int):
+def make_batch(workload: str, rank: int, world: int):
     from tsunami_pact_b200 import datasets
+    from tsunami_pact_b200.shard import shard
 
-    n = WORKLOADS[workload][0]
-    # each rank gets its own pairs: indices [rank*n, (rank+1)*n)
-    return datasets.generate(workload, n, first=rank * n)
+    first, n = shard(rank, world, WORKLOADS[workload][0])  # this rank's own pairs
+    return datasets.generate(workload, n, first=first)
 
 
 class ClockSampler:
@@ -135,7 +135,7 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen, target_s=10.0):
+def cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen, target_s=15.0):
     from oracle import oracle as O
 
     cores = os.cpu_count() or 1
@@ -342,20 +342,17 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    from tsunami_pact_b200.shard import barrier as shard_barrier
+    from tsunami_pact_b200.shard import combine, throughput
+
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        shard_barrier(dist, f"cuda:{local}")
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return combine([x], ["max"], dist, f"cuda:{local}")[0]
 
     n_pairs, desc = WORKLOADS[workload]
-    pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank)
+    pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank, world)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
     al = T.Aligner(*PEN, device=local, max_error_hint=args.hint)
@@ -399,9 +396,11 @@ def main():
     barrier()
     wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
     clk = clocks.stop()
-    ms = max_over_ranks(float(np.mean(step_ms)))
-    value = cells * world / (ms / 1e3) / 1e9
-    pairs_s = n_pairs * world / (ms / 1e3)
+    # slowest rank's step time; work summed over ranks
+    ms, cells_all, pairs_all = combine([float(np.mean(step_ms)), cells, float(n_pairs)], ["max", "sum", "sum"], dist,
+                                       f"cuda:{local}")
+    value = throughput(cells_all, ms) / 1e9
+    pairs_s = throughput(pairs_all, ms)
 
     # ---- plain form (c4): one call per log2-length bucket, one warp per pair
     plain = None
@@ -440,8 +439,8 @@ def main():
                 p_ms.append(tot)
         pm = max_over_ranks(float(np.mean(p_ms)))
         plain = {"form": "one call per floor(log2 L) bucket, one warp per pair (TSU_ONE_WARP), in turn",
-                 "buckets": len(sub), "ms_per_step": pm, "value": cells * world / (pm / 1e3) / 1e9,
-                 "unit": "GCUPS", "pairs_per_s": n_pairs * world / (pm / 1e3),
+                 "buckets": len(sub), "ms_per_step": pm, "value": throughput(cells_all, pm) / 1e9,
+                 "unit": "GCUPS", "pairs_per_s": throughput(pairs_all, pm),
                  "batched_over_plain_pairs_per_s": pm / ms, "gpu_launches": p_launch}
 
     # ---- e2e: host buffers (pinned) through tsu_align_batch ---------------
@@ -474,8 +473,8 @@ def main():
             launches_e2e = int(tm["kernel_launches"])
         barrier()
         ems = max_over_ranks(float(np.mean(e_ms)))
-        e2e = {"value": cells * world / (ems / 1e3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": int(hb),
-               "d2h_bytes_per_step": int(db), "ms_per_step": ems, "pairs_per_s": n_pairs * world / (ems / 1e3)}
+        e2e = {"value": throughput(cells_all, ems) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": int(hb),
+               "d2h_bytes_per_step": int(db), "ms_per_step": ems, "pairs_per_s": throughput(pairs_all, ems)}
         # correctness of the e2e output against the device leg
         if want_cigar and not np.array_equal(outs[0], d_sc.cpu().numpy()):
             raise SystemExit("e2e scores differ from the device-resident leg")
