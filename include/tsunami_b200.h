@@ -257,7 +257,7 @@ typedef struct {
   int64_t max_job_pairs;    /* light pairs merged into one job (0 = 16384)       */
   int32_t max_job_requests; /* requests merged into one job (0 = 64; 1 = none)   */
   int32_t heavy_len;        /* pairs with max(m, n) >= heavy_len run as jobs of
-                               their own (0 = 16384; < 0 = never)                 */
+                               their own (0 = 8192; < 0 = never)                  */
   int32_t heavy_workers;    /* such jobs at once (0 = workers - 2, at least 1)   */
   int32_t estimate_hint;    /* 0: size each long pair's memory by its edit rate
                                estimated from shared k-mers (x 1.3 + 0.01);

@@ -161,7 +161,7 @@ struct Config {
   int max_job_requests = 64;      // parts merged into one light job
   double watchdog_ms = 0;         // 0: off
   size_t resident_cap = 0;        // bytes an idle worker may keep (0: budget / (2 * workers))
-  int32_t heavy_len = 16384;      // max(m, n) from which a pair is a part of its own (0: never)
+  int32_t heavy_len = 8192;       // max(m, n) from which a pair is a part of its own (0: never)
   int heavy_workers = 0;          // heavy jobs at once (0: workers - 1, at least 1)
   double hint = 0;                // edit-rate hint of light parts (0: the executor's default)
   bool estimate = true;           // heavy pairs: hint from their shared k-mers (tsu_estimate.h)

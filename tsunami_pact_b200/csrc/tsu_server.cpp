@@ -172,7 +172,7 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
   sc.max_job_requests = c.max_job_requests ? c.max_job_requests : 64;
   sc.watchdog_ms = c.watchdog_ms;
   sc.resident_cap = c.resident_bytes;
-  sc.heavy_len = c.heavy_len == 0 ? 16384 : (c.heavy_len < 0 ? 0 : c.heavy_len);
+  sc.heavy_len = c.heavy_len == 0 ? 8192 : (c.heavy_len < 0 ? 0 : c.heavy_len);
   sc.heavy_workers = c.heavy_workers > 0 ? c.heavy_workers : std::max(1, sc.workers - 2);
   sc.estimate = c.estimate_hint >= 0;
   // Jobs of different workers overlap only on different hardware queues: ask
