@@ -63,6 +63,7 @@ constexpr int cta_min_blocks() {
 
 template <bool kCigar, int kMode, int GW>
 __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>())) align_kernel(AlignArgs a) {
+  static_assert(GW == 1 || GW == 2 || GW == 4 || GW == 8 || GW == 16 || GW == 32, "warps per pair");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
 #ifdef TSU_WARP_EMU
@@ -301,15 +302,20 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = any_found;
           }
           group_sync<GW>(gid);  // the step's ring writes and partials are complete
-          const int* q0 = part + (s & 1) * GW * 8;
-          any_found = false;
-          for (int w = 0; w < GW; ++w) {
-            const int* qw = q0 + w * 8;
-            fm = min(fm, qw[0]); lm = max(lm, qw[1]);
-            fi = min(fi, qw[2]); li = max(li, qw[3]);
-            fd = min(fd, qw[4]); ld = max(ld, qw[5]);
-            any_found |= qw[6] != 0;
+          // lane w takes warp w's partials; warp reductions combine them
+          // (7 loads and 7 reductions per thread instead of 7 * GW)
+          int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = 0;
+          if (lane < GW) {
+            const int* qw = part + ((s & 1) * GW + lane) * 8;
+            p0 = qw[0]; p1 = qw[1]; p2 = qw[2]; p3 = qw[3]; p4 = qw[4]; p5 = qw[5]; p6 = qw[6];
           }
+          fm = __reduce_min_sync(FULL, p0);
+          lm = __reduce_max_sync(FULL, p1);
+          fi = __reduce_min_sync(FULL, p2);
+          li = __reduce_max_sync(FULL, p3);
+          fd = __reduce_min_sync(FULL, p4);
+          ld = __reduce_max_sync(FULL, p5);
+          any_found = __any_sync(FULL, p6 != 0);
         }
         {
           // trimmed limits (wfa_gpu.cu:636-719), written by every thread

@@ -276,7 +276,7 @@ struct BatchInfo {
 };
 
 // The align_kernel instantiations: CIGAR or score only, shared or global
-// wavefront ring, 1/2/4/8/16 warps per pair.  Each kernel's dynamic shared
+// wavefront ring, 1/2/4/8/16 warps per pair (and 32 with the global ring).  Each kernel's dynamic shared
 // memory limit is set to the device maximum once per device (always the same
 // value, so contexts planning on several host threads cannot lower it under
 // another's launch).
@@ -303,6 +303,9 @@ cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
     case 4: return occ_one<kCigar, kMode, 4>(threads, smem, optin, occ);
     case 8: return occ_one<kCigar, kMode, 8>(threads, smem, optin, occ);
     case 16: return occ_one<kCigar, kMode, 16>(threads, smem, optin, occ);
+    case 32:
+      if constexpr (kMode == tsu::kModeGlobal) return occ_one<kCigar, kMode, 32>(threads, smem, optin, occ);
+      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }
@@ -322,6 +325,9 @@ void launch_gw(int gw, int blocks, int threads, size_t smem, cudaStream_t st, co
     case 4: tsu::align_kernel<kCigar, kMode, 4><<<blocks, threads, smem, st>>>(a); break;
     case 8: tsu::align_kernel<kCigar, kMode, 8><<<blocks, threads, smem, st>>>(a); break;
     case 16: tsu::align_kernel<kCigar, kMode, 16><<<blocks, threads, smem, st>>>(a); break;
+    case 32:
+      if constexpr (kMode == tsu::kModeGlobal) tsu::align_kernel<kCigar, kMode, 32><<<blocks, threads, smem, st>>>(a);
+      break;
     default: break;
   }
 }
@@ -563,6 +569,9 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   int64_t arena_cap = 0;
   if (want_cigar) {
     arena_cap = tsu::arena_runs(ctx->x, ctx->go, n, bi.max_m, bi.max_n, ctx->err_hint);
+    // the wavefront scratch of an earlier call is regrown for this call's
+    // passes anyway: drop it rather than let it shrink the arena
+    if (ctx->held() + sizeof(uint32_t) * (size_t)arena_cap > ctx->budget) release(ctx, ctx->b_scratch);
     size_t room = ctx->budget > ctx->held() ? ctx->budget - ctx->held() : 0;
     arena_cap = std::min<int64_t>(arena_cap, (int64_t)(room / 8));  // leave half for scratch
     if ((rc = grow(ctx, ctx->b_arena, sizeof(uint32_t) * (size_t)std::max<int64_t>(arena_cap, 1024)))) return rc;
@@ -782,6 +791,8 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
           // keep the runs written so far: grow by copy
           DevBuf nb;
           const size_t bytes = (sizeof(uint32_t) * (size_t)need + 255) & ~(size_t)255;
+          // the last pass's scratch is regrown for the next one: free it first
+          if (ctx->held() + bytes > ctx->budget) release(ctx, ctx->b_scratch);
           if (ctx->held() + bytes > ctx->budget) {
             ctx->need_bytes = ctx->held() + bytes;
             return set_err(ctx, TSU_ENOMEM, "CIGAR arena exceeds budget");
@@ -1401,7 +1412,7 @@ int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair) {
   if (!ctx) return TSU_EINVAL;
   const int gw = warps_per_pair;
   if (band < 0 || band >= tsu::kBands || (mode != tsu::kModeShared && mode != tsu::kModeGlobal) ||
-      (gw != 1 && gw != 2 && gw != 4 && gw != 8 && gw != 16))
+      (gw != 1 && gw != 2 && gw != 4 && gw != 8 && gw != 16 && !(gw == 32 && mode == tsu::kModeGlobal)))
     return set_err(ctx, TSU_EINVAL, "band %d, mode %d, %d warps per pair: not a rung", band, mode, gw);
   ctx->band_start[band] = tsu::PassChoice{mode, gw};
   return TSU_OK;

@@ -127,13 +127,13 @@ inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int3
 // diagonals, at most m + n + 3): pc itself, a larger shared group, or the
 // global ring with 8 or more warps.  Used when the hint is a per-pair
 // estimate, so a pair that is bound to outgrow the shared ring does not
-// start there.
+// start there; a wavefront wider than 16,384 diagonals gets 32 warps.
 inline PassChoice fit_start(PassChoice pc, int x, int go, int ge, int rm, int re, int32_t max_m, int32_t max_n,
                             double hint, int smem_optin) {
-  if (pc.mode != kModeShared) return pc;
   const int64_t maxlen = std::max(max_m, max_n);
-  if (maxlen > kSharedMaxLen) return {kModeGlobal, std::max(8, pc.gw)};
   const int64_t w = std::min<int64_t>((int64_t)max_m + max_n + 3, 2 * hint_score(x, go, maxlen, hint) / ge + 3);
+  if (pc.mode != kModeShared) return {kModeGlobal, w > 16384 ? 32 : pc.gw};
+  if (maxlen > kSharedMaxLen) return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
   const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
   static const int kGW[] = {1, 2, 4, 8, 16};
   for (int gw : kGW) {
@@ -142,7 +142,8 @@ inline PassChoice fit_start(PassChoice pc, int x, int go, int ge, int rm, int re
     const int cap = gw == 1 ? kSharedW1 : shared_ring_width(rm, re, gw, (int)seqw, smem_optin);
     if (cap >= w) return {kModeShared, gw};
   }
-  return {kModeGlobal, std::max(8, pc.gw)};
+  // wavefronts wider than 16,384 diagonals: 32 warps (one 1024-thread block)
+  return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
 }
 
 // Length bands of the batched scheduler: max(m, n) < 1024, < 2048, < 4096,
