@@ -136,7 +136,7 @@ const char* tsu_pass_log(const tsu_ctx* ctx);
  * Pairs are aligned by length band (max(m, n) < 1024, < 2048, < 4096, < 8192,
  * < 16384, >= 16384 for bands 0..5); each band starts at a rung: the wavefront
  * ring in shared memory (mode 0) or in device memory (mode 1), with 1, 2, 4,
- * 8 or 16 warps per pair (mode 1 also 32).  A context starts from the table compiled in
+ * 8, 16 or 32 warps per pair.  A context starts from the table compiled in
  * (tsu_tuning.h, written by the autotuner tsunami_pact_b200/tune.py); these
  * calls read and change the context's copy.  Pairs that outgrow a rung are
  * retried at the next one, so a rung never changes a result.  No

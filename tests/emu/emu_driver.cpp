@@ -54,12 +54,7 @@ static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
     case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4>(a); }); break;
     case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8>(a); }); break;
     case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16>(a); }); break;
-    case 32:
-      if constexpr (kMode == tsu::kModeGlobal) {
-        emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32>(a); });
-        break;
-      }
-      std::abort();
+    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32>(a); }); break;
     default: std::abort();
   }
 }

@@ -259,7 +259,7 @@ def test_cli_check(tmp_path):
 
 def test_every_starting_rung_same_results(aligner_factory, oracle):
     """tsu_set_band_start: whatever rung a band starts at (shared ring with
-    1-16 warps per pair, global ring with 1-32), pairs that outgrow it are
+    1-32 warps per pair, global ring with 1-32), pairs that outgrow it are
     retried and the results are the oracle's."""
     import ctypes
 
@@ -276,8 +276,8 @@ def test_every_starting_rung_same_results(aligner_factory, oracle):
     with T.Aligner(4, 6, 2) as al:
         assert L.tsu_set_band_start(al._h, 6, 0, 1) != 0  # no band 6
         assert L.tsu_set_band_start(al._h, 0, 0, 3) != 0  # no 3-warp groups
-        assert L.tsu_set_band_start(al._h, 0, 0, 32) != 0  # 32 warps: global ring only
-        for mode, gw in [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (1, 1), (1, 8), (1, 16), (1, 32)]:
+        assert L.tsu_set_band_start(al._h, 0, 0, 64) != 0  # no 64-warp groups
+        for mode, gw in [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (0, 32), (1, 1), (1, 8), (1, 16), (1, 32)]:
             for band in range(6):
                 assert L.tsu_set_band_start(al._h, band, mode, gw) == 0
             scores, ops = al.align(pats, txts)

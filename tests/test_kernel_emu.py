@@ -153,7 +153,7 @@ def test_score_only(emu, oracle):
 
 
 @pytest.mark.parametrize("gw,shared", [(2, True), (4, True), (8, True), (16, True), (2, False), (8, False),
-                                       (16, False), (32, False)])
+                                       (16, False), (32, True), (32, False)])
 def test_warp_groups(emu, oracle, gw, shared):
     """Several warps per pair (named barriers, partial reductions combined
     across warps), in both ring modes, with CIGARs."""

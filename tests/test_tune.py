@@ -16,7 +16,7 @@ def test_committed_table_is_valid():
     table = tune.parse_header(text)
     assert len(table) == tune.N_BANDS == 6
     for mode, warps in table:
-        assert mode in (0, 1) and warps in ((1, 2, 4, 8, 16) if mode == 0 else (1, 2, 4, 8, 16, 32))
+        assert mode in (0, 1) and warps in (1, 2, 4, 8, 16, 32)
     assert "TSU_TUNING_SOURCE" in text
 
 

@@ -86,6 +86,7 @@ struct tsu_ctx {
   HostBuf h_scalars;  // 64 bytes: retry count, arena cursor, work counters, run total
   HostBuf h_list;     // int32 pass order / retry list
   HostBuf h_status;   // int32 pair statuses (tsu_align_batch)
+  std::vector<void*> h_retired;  // outgrown page-locked buffers, freed at destroy
   // events of the host-buffer pipeline (tsu_align_batch): 8 chunks at most
   cudaEvent_t cev_up[8] = {}, cev_done[8] = {}, cev_down[8] = {}, cev_t[2] = {};
   // Waits for the GPU sleep on an event instead of spinning (set by the
@@ -218,24 +219,19 @@ cudaError_t wait_stream(tsu_ctx* ctx, cudaStream_t s) {
   return cudaEventSynchronize(ctx->wait_ev);
 }
 
-// Grow a page-locked buffer to at least `bytes` (doubling).  The old one is
-// freed once the context's streams are idle.
+// Grow a page-locked buffer to at least `bytes` (doubling).  The outgrown
+// one is kept until the context is destroyed: cudaFreeHost can synchronize
+// the whole device, stalling other contexts' work.
 int host_grow(tsu_ctx* ctx, HostBuf& b, size_t bytes) {
   if (b.cap >= bytes) return TSU_OK;
   const size_t nb = std::max<size_t>(std::max(bytes, 2 * b.cap), 4096);
-  if (b.p) {
-    wait_stream(ctx, ctx->h2d_stream);
-    wait_stream(ctx, ctx->d2h_stream);
-    wait_stream(ctx, ctx->stream);
-    cudaFreeHost(b.p);
-    b.p = nullptr;
-    b.cap = 0;
-  }
-  if (cudaHostAlloc(&b.p, nb, cudaHostAllocDefault) != cudaSuccess) {
+  void* np = nullptr;
+  if (cudaHostAlloc(&np, nb, cudaHostAllocDefault) != cudaSuccess) {
     cudaGetLastError();
-    b.p = nullptr;
     return set_err(ctx, TSU_EDEVICE, "page-locked host allocation of %zu B failed", nb);
   }
+  if (b.p) ctx->h_retired.push_back(b.p);
+  b.p = np;
   b.cap = nb;
   return TSU_OK;
 }
@@ -276,7 +272,7 @@ struct BatchInfo {
 };
 
 // The align_kernel instantiations: CIGAR or score only, shared or global
-// wavefront ring, 1/2/4/8/16 warps per pair (and 32 with the global ring).  Each kernel's dynamic shared
+// wavefront ring, 1/2/4/8/16/32 warps per pair.  Each kernel's dynamic shared
 // memory limit is set to the device maximum once per device (always the same
 // value, so contexts planning on several host threads cannot lower it under
 // another's launch).
@@ -303,9 +299,7 @@ cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
     case 4: return occ_one<kCigar, kMode, 4>(threads, smem, optin, occ);
     case 8: return occ_one<kCigar, kMode, 8>(threads, smem, optin, occ);
     case 16: return occ_one<kCigar, kMode, 16>(threads, smem, optin, occ);
-    case 32:
-      if constexpr (kMode == tsu::kModeGlobal) return occ_one<kCigar, kMode, 32>(threads, smem, optin, occ);
-      return cudaErrorInvalidValue;
+    case 32: return occ_one<kCigar, kMode, 32>(threads, smem, optin, occ);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -325,9 +319,7 @@ void launch_gw(int gw, int blocks, int threads, size_t smem, cudaStream_t st, co
     case 4: tsu::align_kernel<kCigar, kMode, 4><<<blocks, threads, smem, st>>>(a); break;
     case 8: tsu::align_kernel<kCigar, kMode, 8><<<blocks, threads, smem, st>>>(a); break;
     case 16: tsu::align_kernel<kCigar, kMode, 16><<<blocks, threads, smem, st>>>(a); break;
-    case 32:
-      if constexpr (kMode == tsu::kModeGlobal) tsu::align_kernel<kCigar, kMode, 32><<<blocks, threads, smem, st>>>(a);
-      break;
+    case 32: tsu::align_kernel<kCigar, kMode, 32><<<blocks, threads, smem, st>>>(a); break;
     default: break;
   }
 }
@@ -1111,6 +1103,17 @@ int trim(tsu_ctx* ctx) {
 
 size_t needed_bytes(const tsu_ctx* ctx) { return ctx ? ctx->need_bytes : 0; }
 
+void prime_pool(tsu_ctx* ctx, size_t bytes) {
+  if (!ctx || !bytes || cudaSetDevice(ctx->device) != cudaSuccess) return;
+  void* p = nullptr;
+  if (cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaFreeAsync(p, ctx->stream);
+  wait_stream(ctx, ctx->stream);
+}
+
 }  // namespace engine
 }  // namespace tsu
 
@@ -1162,6 +1165,7 @@ int tsu_destroy(tsu_ctx* ctx) {
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   for (HostBuf* hb : {&ctx->h_scalars, &ctx->h_list, &ctx->h_status})
     if (hb->p) cudaFreeHost(hb->p);
+  for (void* p : ctx->h_retired) cudaFreeHost(p);
   if (ctx->h2d_stream && ctx->h2d_stream != ctx->stream) cudaStreamDestroy(ctx->h2d_stream);
   if (ctx->d2h_stream && ctx->d2h_stream != ctx->stream) cudaStreamDestroy(ctx->d2h_stream);
   cudaStreamDestroy(ctx->stream);
@@ -1412,7 +1416,7 @@ int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair) {
   if (!ctx) return TSU_EINVAL;
   const int gw = warps_per_pair;
   if (band < 0 || band >= tsu::kBands || (mode != tsu::kModeShared && mode != tsu::kModeGlobal) ||
-      (gw != 1 && gw != 2 && gw != 4 && gw != 8 && gw != 16 && !(gw == 32 && mode == tsu::kModeGlobal)))
+      (gw != 1 && gw != 2 && gw != 4 && gw != 8 && gw != 16 && gw != 32))
     return set_err(ctx, TSU_EINVAL, "band %d, mode %d, %d warps per pair: not a rung", band, mode, gw);
   ctx->band_start[band] = tsu::PassChoice{mode, gw};
   return TSU_OK;

@@ -54,6 +54,10 @@ void set_exact_growth(tsu_ctx* ctx, bool exact);
 // Return every device buffer of the context to the pool (waits for the
 // context's streams first).
 int trim(tsu_ctx* ctx);
+// Reserve `bytes` in the device's buffer pool (one allocation, freed at
+// once: the pool keeps the memory), so later allocations of any context are
+// carved from it instead of growing the pool under load.  Best effort.
+void prime_pool(tsu_ctx* ctx, size_t bytes);
 // After TSU_ENOMEM: the budget the failed step needed (0 if unknown).
 size_t needed_bytes(const tsu_ctx* ctx);
 

@@ -30,24 +30,26 @@ namespace {
 using tsu::serve::Output;
 using tsu::serve::Pairs;
 
-// A growing page-locked host buffer.
+// A growing page-locked host buffer.  Outgrown buffers are kept until the
+// worker ends: cudaFreeHost can synchronize the whole device, which would
+// stall every other worker's jobs.
 class HostStage {
  public:
   ~HostStage() {
+    for (char* p : retired_) cudaFreeHost(p);
     if (p_) cudaFreeHost(p_);
   }
   // At least `bytes`, doubling; nullptr if the allocation fails.
   char* get(size_t bytes) {
     if (bytes > cap_) {
-      const size_t nb = std::max<size_t>(std::max(bytes, 2 * cap_), 1 << 20);
-      if (p_) cudaFreeHost(p_);
-      p_ = nullptr;
-      cap_ = 0;
-      if (cudaHostAlloc(reinterpret_cast<void**>(&p_), nb, cudaHostAllocPortable) != cudaSuccess) {
+      const size_t nb = std::max<size_t>(std::max(bytes, 2 * cap_), 4 << 20);
+      char* np = nullptr;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&np), nb, cudaHostAllocPortable) != cudaSuccess) {
         cudaGetLastError();
-        p_ = nullptr;
         return nullptr;
       }
+      if (p_) retired_.push_back(p_);
+      p_ = np;
       cap_ = nb;
     }
     return p_;
@@ -56,6 +58,7 @@ class HostStage {
  private:
   char* p_ = nullptr;
   size_t cap_ = 0;
+  std::vector<char*> retired_;
 };
 
 size_t up16(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -65,6 +68,8 @@ class EngineExecutor final : public tsu::serve::Executor {
   explicit EngineExecutor(tsu_ctx* ctx) : ctx_(ctx), default_hint_(tsu::engine::hint(ctx)) {
     tsu::engine::set_exact_growth(ctx_, true);
     tsu::engine::set_blocking_sync(ctx_, true);
+    in_.get(16 << 20);  // page-locked staging allocated now, not under load
+    out_.get(16 << 20);
   }
   ~EngineExecutor() override { tsu_destroy(ctx_); }
 
@@ -192,6 +197,8 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
     if (rc) return rc;  // unique_ptrs destroy the contexts made so far
     ws.emplace_back(new EngineExecutor(ctx));
   }
+  // the device pool holds the whole budget from the start
+  tsu::engine::prime_pool(planner, sc.budget);
   auto* srv = new tsu_server();
   srv->s = std::make_unique<tsu::serve::Server>(sc, std::move(ws), std::move(plan));
   *out = srv;

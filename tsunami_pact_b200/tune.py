@@ -7,8 +7,8 @@ default the uniform 1 kbp configuration, c2: 1 kbp at 5 %, the uneven
 batched one, c4: lengths log-uniform 100-20,000, edit rates 1-15 %, and the
 long-read one, c3: 10 kbp at 15 %; seeded, see datasets.py; penalties
 4/6/2), aligns them from every candidate rung
-(wavefront ring in shared memory with 1, 2, 4, 8 or 16 warps per pair, or in
-device memory with 8, 16 or 32), checks that every rung gives the same scores and
+(wavefront ring in shared memory with 1, 2, 4, 8, 16 or 32 warps per pair,
+or in device memory with 8, 16 or 32), checks that every rung gives the same scores and
 CIGARs, and keeps the rung with the shortest device time of the align passes
 summed over the workloads (each the minimum over --reps runs after one
 warm-up).  Bands are measured at the sizes they have in the workloads,
@@ -37,7 +37,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BAND_NAMES = ["< 1024", "< 2048", "< 4096", "< 8192", "< 16384", ">= 16384"]
 BAND_LIMITS = [1024, 2048, 4096, 8192, 16384]  # tsu::length_band
 N_BANDS = 6
-CANDIDATES = [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (1, 8), (1, 16), (1, 32)]
+CANDIDATES = [(0, 1), (0, 2), (0, 4), (0, 8), (0, 16), (0, 32), (1, 8), (1, 16), (1, 32)]
 SHARED_MAX_LEN = 32000  # the int16 shared ring's limit
 DEFAULT_WORKLOADS = "c2:200000,c4:100000,c3:5000"
 
