@@ -195,9 +195,19 @@ int64_t tsu_cigar_to_string(const uint32_t* runs, int64_t nruns, char* out, int6
  * wfa_gpu.cu:71-81) --------------------------------------------------------
  * sequences.txt: "N\nL\nerr\n" then N x (pattern line, text line).  Lines may
  * have any length up to the header L... or longer: each line is read at its
- * own length.  tsu_file_* hold the parsed batch in host memory. */
+ * own length.  tsu_file_* hold the parsed batch in host memory -- page-locked
+ * when a CUDA device is present, so tsu_align_batch copies it to the GPU at
+ * full link speed; the file is read with parallel preads and tokenized in
+ * parallel (the reference's reader is a single-threaded fscanf). */
 typedef struct tsu_file tsu_file;
 int tsu_file_read(const char* path, tsu_file** out);
+/* Pairs from two FASTA or FASTQ files (either format, detected per file;
+ * multi-line FASTA sequences are joined): record i of pattern_path is the
+ * pattern of pair i, record i of text_path its text; the files must hold
+ * the same number of records.  No counterpart in the reference (its only
+ * input is sequences.txt).  tsu_file_header then gives the longest
+ * sequence as seq_len and 0 as error_rate. */
+int tsu_file_read_pairs(const char* pattern_path, const char* text_path, tsu_file** out);
 int tsu_file_batch(const tsu_file* f, tsu_batch* out); /* views into f */
 int tsu_file_header(const tsu_file* f, int64_t* num, int32_t* seq_len, int32_t* error_rate);
 void tsu_file_free(tsu_file* f);

@@ -19,6 +19,7 @@ from ._lib import (  # noqa: F401
     gen_batch,
     lib,
     lib_path,
+    read_pairs,
     read_sequences,
     runs_to_ops,
     runs_to_string,
@@ -34,6 +35,7 @@ __all__ = [
     "gen_batch",
     "lib",
     "lib_path",
+    "read_pairs",
     "read_sequences",
     "runs_to_ops",
     "runs_to_string",

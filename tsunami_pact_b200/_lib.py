@@ -114,6 +114,7 @@ def lib():
     L.tsu_cigar_to_string.restype = c_i64
     L.tsu_cigar_to_string.argtypes = [c_vp, c_i64, c_vp, c_i64]
     L.tsu_file_read.argtypes = [ctypes.c_char_p, P(c_vp)]
+    L.tsu_file_read_pairs.argtypes = [ctypes.c_char_p, ctypes.c_char_p, P(c_vp)]
     L.tsu_file_batch.argtypes = [c_vp, P(Batch)]
     L.tsu_file_header.argtypes = [c_vp, P(c_i64), P(c_i32), P(c_i32)]
     L.tsu_file_free.argtypes = [c_vp]
@@ -416,6 +417,21 @@ def read_sequences(path: str):
     rc = L.tsu_file_read(path.encode(), ctypes.byref(h))
     if rc != TSU_OK:
         raise AlignError(rc, f"cannot read {path}")
+    return _file_contents(L, h)
+
+
+def read_pairs(pattern_path: str, text_path: str):
+    """Pairs from two FASTA/FASTQ files (record i of each file is pair i).
+    Returns (header, patterns, texts) like read_sequences."""
+    L = lib()
+    h = c_vp()
+    rc = L.tsu_file_read_pairs(pattern_path.encode(), text_path.encode(), ctypes.byref(h))
+    if rc != TSU_OK:
+        raise AlignError(rc, f"cannot read {pattern_path} / {text_path}")
+    return _file_contents(L, h)
+
+
+def _file_contents(L, h):
     try:
         b = Batch()
         L.tsu_file_batch(h, ctypes.byref(b))

@@ -1,7 +1,17 @@
 // tsu_host.cpp -- host-side formats of the WFA engine: the sequences.txt
 // reader (reference wfa_gpu.cu:71-81, format generate_dataset.cpp:39-41,
-// 68-69) and the seeded synthetic pair generator that replaces
-// generate_dataset.cpp:11-75.
+// 68-69), a FASTA/FASTQ pair reader, and the seeded synthetic pair
+// generator that replaces generate_dataset.cpp:11-75.
+//
+// The reference reads its input with a single-threaded fscanf into pageable
+// memory.  Here a file is read with parallel pread calls straight into
+// page-locked memory (when a CUDA device is present: the engine's copies to
+// the GPU then run at full link speed) and tokenized in parallel chunks.
+#include <cuda_runtime.h>
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -12,10 +22,99 @@
 
 #include "../../include/tsunami_b200.h"
 
+namespace {
+
+// Host bytes: page-locked when a CUDA device is present, else malloc'ed.
+struct HostBytes {
+  char* p = nullptr;
+  size_t n = 0;
+  bool pinned = false;
+  HostBytes() = default;
+  HostBytes(const HostBytes&) = delete;
+  HostBytes& operator=(const HostBytes&) = delete;
+  ~HostBytes() { reset(); }
+  void reset() {
+    if (p) {
+      if (pinned)
+        cudaFreeHost(p);
+      else
+        free(p);
+    }
+    p = nullptr;
+    n = 0;
+    pinned = false;
+  }
+  bool alloc(size_t bytes) {
+    reset();
+    const size_t b = std::max<size_t>(bytes, 1);
+    int dev = 0;
+    if (cudaGetDeviceCount(&dev) == cudaSuccess && dev > 0 &&
+        cudaHostAlloc(reinterpret_cast<void**>(&p), b, cudaHostAllocPortable) == cudaSuccess) {
+      pinned = true;
+    } else {
+      cudaGetLastError();
+      p = static_cast<char*>(malloc(b));
+      if (!p) return false;
+    }
+    n = bytes;
+    return true;
+  }
+};
+
+int reader_threads() {
+  const unsigned h = std::thread::hardware_concurrency();
+  return (int)std::min<unsigned>(std::max<unsigned>(h, 1), 32);
+}
+
+// Run fn(t) for t in [0, T) on T threads (the caller's thread runs t = 0).
+template <class F>
+void parallel(int T, F&& fn) {
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back([&, t] { fn(t); });
+  fn(0);
+  for (auto& x : th) x.join();
+}
+
+// Whole file into b (parallel preads).
+bool read_file(const char* path, HostBytes* b) {
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) return false;
+  struct stat stt {};
+  if (fstat(fd, &stt) != 0 || stt.st_size < 0) {
+    close(fd);
+    return false;
+  }
+  const size_t size = (size_t)stt.st_size;
+  if (!b->alloc(size)) {
+    close(fd);
+    return false;
+  }
+  const int T = size < (8u << 20) ? 1 : reader_threads();
+  std::vector<char> ok((size_t)T, 1);
+  parallel(T, [&](int t) {
+    size_t off = size * (size_t)t / (size_t)T;
+    const size_t end = size * (size_t)(t + 1) / (size_t)T;
+    while (off < end) {
+      const ssize_t r = pread(fd, b->p + off, end - off, (off_t)off);
+      if (r <= 0) {
+        ok[(size_t)t] = 0;
+        return;
+      }
+      off += (size_t)r;
+    }
+  });
+  close(fd);
+  for (char v : ok)
+    if (!v) return false;
+  return true;
+}
+
+}  // namespace
+
 struct tsu_file {
   int64_t num = 0;
   int32_t seq_len = 0, err = 0;
-  std::vector<char> buf;  // file contents, tokens NUL-separated in place
+  HostBytes buf;  // file contents (sequences.txt) or the sequences themselves (FASTA/FASTQ)
   std::vector<int64_t> poff, toff;
   std::vector<int32_t> plen, tlen;
 };
@@ -25,25 +124,25 @@ namespace {
 inline bool is_space(unsigned char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t' || c == '\v' || c == '\f'; }
 
 // Next whitespace-delimited token starting at *pos (like fscanf "%s").
-bool next_token(const std::vector<char>& b, size_t* pos, size_t* start, size_t* len) {
+bool next_token(const HostBytes& b, size_t* pos, size_t* start, size_t* len) {
   size_t i = *pos;
-  const size_t n = b.size();
-  while (i < n && is_space((unsigned char)b[i])) ++i;
+  const size_t n = b.n;
+  while (i < n && is_space((unsigned char)b.p[i])) ++i;
   if (i >= n) return false;
   size_t j = i;
-  while (j < n && !is_space((unsigned char)b[j])) ++j;
+  while (j < n && !is_space((unsigned char)b.p[j])) ++j;
   *start = i;
   *len = j - i;
   *pos = j;
   return true;
 }
 
-bool parse_int(const std::vector<char>& b, size_t* pos, int64_t* out) {
+bool parse_int(const HostBytes& b, size_t* pos, int64_t* out) {
   size_t s, l;
   if (!next_token(b, pos, &s, &l)) return false;
   char tmp[32];
   if (l >= sizeof tmp) return false;
-  memcpy(tmp, &b[s], l);
+  memcpy(tmp, b.p + s, l);
   tmp[l] = 0;
   char* end = nullptr;
   long long v = strtoll(tmp, &end, 10);
@@ -181,22 +280,11 @@ int tsu_gen_batch(uint64_t seed, int64_t first, int64_t count, const int32_t* le
 int tsu_file_read(const char* path, tsu_file** out) {
   if (!path || !out) return TSU_EINVAL;
   *out = nullptr;
-  FILE* fp = fopen(path, "rb");
-  if (!fp) return TSU_EIO;
   auto* f = new tsu_file();
-  if (fseek(fp, 0, SEEK_END) == 0) {
-    long sz = ftell(fp);
-    if (sz > 0) {
-      f->buf.resize((size_t)sz);
-      fseek(fp, 0, SEEK_SET);
-      if (fread(f->buf.data(), 1, (size_t)sz, fp) != (size_t)sz) {
-        fclose(fp);
-        delete f;
-        return TSU_EIO;
-      }
-    }
+  if (!read_file(path, &f->buf)) {
+    delete f;
+    return TSU_EIO;
   }
-  fclose(fp);
   size_t pos = 0;
   int64_t num = 0, len = 0, err = 0;
   if (!parse_int(f->buf, &pos, &num) || !parse_int(f->buf, &pos, &len) || !parse_int(f->buf, &pos, &err) || num < 0 ||
@@ -207,25 +295,182 @@ int tsu_file_read(const char* path, tsu_file** out) {
   f->num = num;
   f->seq_len = (int32_t)len;
   f->err = (int32_t)err;
+  // Tokens after the header, found in parallel: chunk t lists the tokens
+  // that start in its byte range; the chunks' lists in order are the file's.
+  const char* p = f->buf.p;
+  const size_t size = f->buf.n;
+  const int T = size - pos < (8u << 20) ? 1 : reader_threads();
+  std::vector<std::vector<std::pair<int64_t, int64_t>>> toks((size_t)T);
+  parallel(T, [&](int t) {
+    size_t i = pos + (size - pos) * (size_t)t / (size_t)T;
+    const size_t end = pos + (size - pos) * (size_t)(t + 1) / (size_t)T;
+    // a token starts at i when i follows whitespace: skip the tail of a token
+    // begun in the previous chunk
+    if (t > 0)
+      while (i < end && !is_space((unsigned char)p[i - 1])) ++i;
+    auto& v = toks[(size_t)t];
+    while (i < end) {
+      while (i < end && is_space((unsigned char)p[i])) ++i;
+      if (i >= end) break;
+      size_t j = i;
+      while (j < size && !is_space((unsigned char)p[j])) ++j;  // a token may run past the chunk
+      v.emplace_back((int64_t)i, (int64_t)(j - i));
+      i = j;
+    }
+  });
+  size_t have = 0;
+  for (auto& v : toks) have += v.size();
+  if (have < 2 * (size_t)num) {
+    delete f;
+    return TSU_EIO;
+  }
   f->poff.resize((size_t)num);
   f->toff.resize((size_t)num);
   f->plen.resize((size_t)num);
   f->tlen.resize((size_t)num);
-  for (int64_t i = 0; i < num; ++i) {
-    size_t s, l;
-    if (!next_token(f->buf, &pos, &s, &l) || l > (1u << 26)) {
-      delete f;
-      return TSU_EIO;
+  size_t k = 0;  // token index: pair i is tokens 2i, 2i + 1 (exactly N pairs are read, as the reference does)
+  for (auto& v : toks)
+    for (auto& tk : v) {
+      if (k >= 2 * (size_t)num) break;
+      if (tk.second > (1 << 26)) {
+        delete f;
+        return TSU_EIO;
+      }
+      const size_t i = k >> 1;
+      if (k & 1) {
+        f->toff[i] = tk.first;
+        f->tlen[i] = (int32_t)tk.second;
+      } else {
+        f->poff[i] = tk.first;
+        f->plen[i] = (int32_t)tk.second;
+      }
+      ++k;
     }
-    f->poff[(size_t)i] = (int64_t)s;
-    f->plen[(size_t)i] = (int32_t)l;
-    if (!next_token(f->buf, &pos, &s, &l) || l > (1u << 26)) {
-      delete f;
-      return TSU_EIO;
+  *out = f;
+  return TSU_OK;
+}
+
+namespace {
+
+// Records of a FASTA or FASTQ file: [start, end) of each record's sequence
+// lines (line breaks included), in file order.  FASTA: a '>' header line,
+// then sequence lines up to the next '>' at the start of a line.  FASTQ: an
+// '@' header line, one sequence line, a '+' line, a quality line.  False on
+// a malformed file.
+bool index_records(const HostBytes& b, std::vector<std::pair<int64_t, int64_t>>* recs) {
+  const char* p = b.p;
+  const size_t n = b.n;
+  size_t i = 0;
+  while (i < n && is_space((unsigned char)p[i])) ++i;
+  if (i >= n) return true;  // empty file: no records
+  const char kind = p[i];
+  if (kind != '>' && kind != '@') return false;
+  auto line_end = [&](size_t a) {
+    if (a >= n) return n;
+    return (size_t)(std::find(p + a, p + n, '\n') - p);
+  };
+  if (kind == '@') {
+    while (i < n) {
+      if (p[i] != '@') return false;
+      const size_t s0 = std::min(line_end(i) + 1, n), s1 = line_end(s0);
+      const size_t plus = std::min(s1 + 1, n);
+      if (plus >= n || p[plus] != '+') return false;
+      const size_t q0 = std::min(line_end(plus) + 1, n), q1 = line_end(q0);
+      recs->emplace_back((int64_t)s0, (int64_t)s1);
+      i = std::min(q1 + 1, n);
+      while (i < n && is_space((unsigned char)p[i])) ++i;
     }
-    f->toff[(size_t)i] = (int64_t)s;
-    f->tlen[(size_t)i] = (int32_t)l;
+    return true;
   }
+  // FASTA records start at a '>' that begins a line; found in parallel
+  const int T = n - i < (8u << 20) ? 1 : reader_threads();
+  std::vector<std::vector<int64_t>> starts((size_t)T);
+  parallel(T, [&](int t) {
+    const size_t a = i + (n - i) * (size_t)t / (size_t)T, e = i + (n - i) * (size_t)(t + 1) / (size_t)T;
+    for (size_t k = a; k < e; ++k)
+      if (p[k] == '>' && (k == i || p[k - 1] == '\n')) starts[(size_t)t].push_back((int64_t)k);
+  });
+  std::vector<int64_t> all;
+  for (auto& v : starts) all.insert(all.end(), v.begin(), v.end());
+  for (size_t r = 0; r < all.size(); ++r) {
+    const size_t s0 = std::min(line_end((size_t)all[r]) + 1, n);
+    const size_t s1 = r + 1 < all.size() ? (size_t)all[r + 1] : n;
+    recs->emplace_back((int64_t)s0, (int64_t)std::max(s0, s1));
+  }
+  return true;
+}
+
+// Each record's sequence without whitespace: lengths and offsets (from
+// base) into len/off; with out, the bytes too (in parallel).
+bool pack_records(const HostBytes& src, const std::vector<std::pair<int64_t, int64_t>>& recs, char* out,
+                  int64_t base, std::vector<int64_t>* off, std::vector<int32_t>* len) {
+  const size_t R = recs.size();
+  off->resize(R);
+  len->resize(R);
+  std::vector<int64_t> l(R);
+  const int T = R < 1024 ? 1 : reader_threads();
+  parallel(T, [&](int t) {
+    for (size_t r = R * (size_t)t / (size_t)T; r < R * (size_t)(t + 1) / (size_t)T; ++r) {
+      int64_t c = 0;
+      for (int64_t k = recs[r].first; k < recs[r].second; ++k) c += !is_space((unsigned char)src.p[k]);
+      l[r] = c;
+    }
+  });
+  int64_t acc = base;
+  for (size_t r = 0; r < R; ++r) {
+    if (l[r] > (1 << 26)) return false;
+    (*off)[r] = acc;
+    (*len)[r] = (int32_t)l[r];
+    acc += l[r];
+  }
+  if (!out) return true;
+  parallel(T, [&](int t) {
+    for (size_t r = R * (size_t)t / (size_t)T; r < R * (size_t)(t + 1) / (size_t)T; ++r) {
+      char* d = out + (*off)[r];
+      for (int64_t k = recs[r].first; k < recs[r].second; ++k)
+        if (!is_space((unsigned char)src.p[k])) *d++ = src.p[k];
+    }
+  });
+  return true;
+}
+
+}  // namespace
+
+int tsu_file_read_pairs(const char* pattern_path, const char* text_path, tsu_file** out) {
+  if (!pattern_path || !text_path || !out) return TSU_EINVAL;
+  *out = nullptr;
+  HostBytes pf, tf;
+  if (!read_file(pattern_path, &pf) || !read_file(text_path, &tf)) return TSU_EIO;
+  std::vector<std::pair<int64_t, int64_t>> pr, tr;
+  if (!index_records(pf, &pr) || !index_records(tf, &tr) || pr.size() != tr.size()) return TSU_EIO;
+  auto* f = new tsu_file();
+  std::vector<int64_t> po, to;
+  std::vector<int32_t> pl, tl;
+  // sizes first, then one buffer holding the patterns, then the texts
+  if (!pack_records(pf, pr, nullptr, 0, &po, &pl)) {
+    delete f;
+    return TSU_EIO;
+  }
+  const int64_t pbytes = pr.empty() ? 0 : po.back() + pl.back();
+  if (!pack_records(tf, tr, nullptr, pbytes, &to, &tl)) {
+    delete f;
+    return TSU_EIO;
+  }
+  const int64_t total = tr.empty() ? pbytes : to.back() + tl.back();
+  if (!f->buf.alloc((size_t)total) || !pack_records(pf, pr, f->buf.p, 0, &po, &pl) ||
+      !pack_records(tf, tr, f->buf.p, pbytes, &to, &tl)) {
+    delete f;
+    return TSU_EIO;
+  }
+  f->num = (int64_t)pr.size();
+  int32_t longest = 0;
+  for (size_t i = 0; i < pl.size(); ++i) longest = std::max({longest, pl[i], tl[i]});
+  f->seq_len = longest;
+  f->err = 0;
+  f->poff = std::move(po);
+  f->toff = std::move(to);
+  f->plen = std::move(pl);
+  f->tlen = std::move(tl);
   *out = f;
   return TSU_OK;
 }
@@ -233,10 +478,10 @@ int tsu_file_read(const char* path, tsu_file** out) {
 int tsu_file_batch(const tsu_file* f, tsu_batch* out) {
   if (!f || !out) return TSU_EINVAL;
   out->num_pairs = f->num;
-  out->pattern = f->buf.data();
+  out->pattern = f->buf.p;
   out->pattern_off = f->poff.data();
   out->pattern_len = f->plen.data();
-  out->text = f->buf.data();
+  out->text = f->buf.p;
   out->text_off = f->toff.data();
   out->text_len = f->tlen.data();
   return TSU_OK;
