@@ -89,6 +89,18 @@ int ora_ops_to_rle(const char* ops, int len, uint32_t* runs, int cap);
 
 int ora_max_threads(void);
 
+/* Dual gap-affine (two-piece) mode, wfa_oracle2.c: a gap of length L costs
+ * min(o1 + e1*L, o2 + e2*L).  Same return conventions as the one-piece
+ * functions above. */
+int ora_align2(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2, char* ops,
+               int ops_cap, int* ops_len, ora_stats_t* st);
+int ora_gotoh2_score(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2);
+int64_t ora_cigar_cost2(const char* ops, int len, const char* pattern, int m, const char* text, int n, int x, int o1,
+                        int e1, int o2, int e2);
+int ora_align_batch2(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                     const int64_t* toff, const int32_t* tlen, int x, int o1, int e1, int o2, int e2, int32_t* scores,
+                     char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads);
+
 /* CPU-check plugin for the wfa_gpu command line (TSU_CHECK_LIB). */
 int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                            const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,

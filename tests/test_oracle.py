@@ -67,3 +67,62 @@ def test_checker_plugin_symbol(oracle):
             ctypes.c_void_p(tl.ctypes.data), 4, 6, 2, ctypes.c_void_p(out.ctypes.data), 2)
     assert rc == 0
     assert list(out) == [4, 8, 10]
+
+
+# --- dual gap-affine (two-piece) oracle --------------------------------------
+
+DUAL_PENS = [(4, 6, 2, 24, 1), (4, 4, 2, 12, 1), (3, 5, 3, 20, 1), (6, 2, 3, 10, 1), (2, 0, 2, 5, 1),
+             (1, 1, 1, 1, 1), (5, 3, 3, 3, 1)]
+
+
+def test_dual_known_answers(oracle):
+    """Hand-derived: a lone gap of length L costs min(o1 + e1*L, o2 + e2*L)."""
+    pen = (4, 6, 2, 24, 1)
+    assert oracle.align2("", "AAAAA", *pen) == (16, "IIIII")      # 6+2*5 < 24+5
+    assert oracle.align2("A" * 20, "", *pen) == (44, "D" * 20)    # 24+20 < 6+2*20
+    assert oracle.align2("ACGT", "ACGT", *pen) == (0, "MMMM")
+    assert oracle.align2("ACGT", "AGGT", *pen) == (4, "MXMM")
+    # an 18-base insertion is where the pieces cross (6+36 == 24+18)
+    p = "ACGTTGCA" * 4
+    t = p[:16] + "G" * 18 + p[16:]
+    s, ops = oracle.align2(p, t, *pen)
+    assert s == 42 and oracle.cigar_cost2(ops, p, t, *pen) == 42
+
+
+@pytest.mark.parametrize("pen", DUAL_PENS)
+def test_dual_random_vs_dp(oracle, pen):
+    """The dual oracle's score is the five-matrix DP optimum and its
+    operation string costs exactly that score."""
+    rng = random.Random(hash(pen) & 0xFFFF)
+    for it in range(250):
+        alpha = "ACGT" if it % 3 else "AC"
+        m = rng.randint(0, 60)
+        p = "".join(rng.choice(alpha) for _ in range(m))
+        if it % 2:
+            t = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 60)))
+        else:  # a long indel, where the second piece is the cheaper one
+            i = rng.randint(0, m)
+            L = rng.randint(1, 40)
+            t = p[:i] + "".join(rng.choice(alpha) for _ in range(L)) + p[i:] if it % 4 else p[:i] + p[i + L:]
+        s, ops = oracle.align2(p, t, *pen)
+        assert s == oracle.gotoh2(p, t, *pen)
+        assert oracle.cigar_cost2(ops, p, t, *pen) == s
+
+
+def test_dual_reduces_to_one_piece(oracle):
+    """With a second piece that never wins, the two-piece result (score and
+    operation string) is the one-piece result."""
+    rng = random.Random(11)
+    for _ in range(200):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 80)))
+        t = "".join(c for c in p if rng.random() > 0.1) + "".join(rng.choice("ACGT") for _ in range(3))
+        assert oracle.align2(p, t, 4, 6, 2, 1000, 5) == oracle.align(p, t, 4, 6, 2)
+
+
+def test_dual_batch_matches_single(oracle):
+    rng = random.Random(5)
+    pats = ["".join(rng.choice("ACGT") for _ in range(rng.randint(0, 150))) for _ in range(48)]
+    txts = [p[: len(p) // 2] + "T" * rng.randint(0, 40) + p[len(p) // 2:] for p in pats]
+    sc, cg = oracle.align_batch2(pats, txts, threads=4)
+    for i in range(48):
+        assert (sc[i], cg[i]) == oracle.align2(pats[i], txts[i])
