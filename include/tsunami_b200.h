@@ -66,6 +66,21 @@ typedef struct {
   int32_t gap_extension; /* > 0  (wfa_gpu.cu:61)  */
 } tsu_penalties;
 
+/* Dual gap-affine ("affine 2-pieces") penalties: a gap of length L costs
+ * min(gap_opening + gap_extension*L, gap_opening2 + gap_extension2*L).  The
+ * reference declares the second piece (penalties_t gap_open2 / gap_ext2,
+ * common.h:80-87; matrices I2 / D2, common.h:52-58; backtrace codes
+ * bt_I2_* / bt_D2_*, common.h:67-77) but aligns with one piece only.  In a
+ * context made by tsu_create_dual every align call uses both pieces; pattern
+ * and text lengths are then limited to 2^24 - 2. */
+typedef struct {
+  int32_t mismatch;       /* > 0  */
+  int32_t gap_opening;    /* >= 0 */
+  int32_t gap_extension;  /* > 0  */
+  int32_t gap_opening2;   /* >= 0 */
+  int32_t gap_extension2; /* > 0  */
+} tsu_penalties2;
+
 typedef struct {
   int32_t device;        /* CUDA device ordinal                                */
   int32_t reserved0;
@@ -122,6 +137,9 @@ typedef struct {
  * (wfa_gpu.cu:96-108).  One context = one device, one stream, one memory
  * budget.  A context is used by one host thread at a time. */
 int tsu_create(const tsu_penalties* pen, const tsu_config* cfg /* nullable */, tsu_ctx** out);
+/* A context whose align calls use dual gap-affine penalties (tsu_penalties2).
+ * Not available through tsu_align_scores_noalloc (one piece only). */
+int tsu_create_dual(const tsu_penalties2* pen, const tsu_config* cfg /* nullable */, tsu_ctx** out);
 int tsu_destroy(tsu_ctx* ctx);
 const char* tsu_status_str(int status);
 const char* tsu_last_error(const tsu_ctx* ctx);
@@ -308,6 +326,9 @@ typedef struct {
 } tsu_server_stats;
 
 int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg /* nullable */, tsu_server** out);
+/* A server whose workers align with dual gap-affine penalties. */
+int tsu_server_create_dual(const tsu_penalties2* pen, const tsu_server_config* cfg /* nullable */,
+                           tsu_server** out);
 /* Queued requests are dropped; running jobs finish first. */
 int tsu_server_destroy(tsu_server* srv);
 /* flags: TSU_SCORE_ONLY or 0.  TSU_EINVAL for bad pairs, TSU_ENOMEM when the

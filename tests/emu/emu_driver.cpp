@@ -3,8 +3,9 @@
 // emulator.  Test infrastructure: compiled by tests/test_kernel_emu.py with
 // AddressSanitizer, it checks the kernels' indexing and outputs on the CPU.
 //
-// Input (stdin):  x o e cigar hint first_mode first_gw N
+// Input (stdin):  x o e o2 e2 cigar hint first_mode first_gw N
 //                 then N records "m n\n<pattern>\n<text>\n"
+//   o2 < 0: one gap piece; else dual gap-affine (the kDual kernels)
 //   first_mode 1 = shared ring, 0 = global ring; first_gw = warps per pair
 //   of the first pass (1, 2, 4, 8, 16).  Retry passes follow the engine's
 //   ladder (tsu_plan.h next_pass).
@@ -37,33 +38,39 @@ struct Buf {  // exact-size heap block
   Buf& operator=(const Buf&) = delete;
 };
 
-static int gcd(int a, int b) {
-  while (b) {
-    int t = a % b;
-    a = b;
-    b = t;
-  }
-  return a;
-}
-
-template <bool kCigar, int kMode>
+template <bool kCigar, int kMode, bool kDual>
 static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
   switch (gw) {
-    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1>(a); }); break;
-    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2>(a); }); break;
-    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4>(a); }); break;
-    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8>(a); }); break;
-    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16>(a); }); break;
-    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32>(a); }); break;
+    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, kDual>(a); }); break;
+    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, kDual>(a); }); break;
+    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, kDual>(a); }); break;
+    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, kDual>(a); }); break;
+    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, kDual>(a); }); break;
+    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, kDual>(a); }); break;
     default: std::abort();
   }
 }
 
+template <bool kDual>
+static void run_pass(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
+  if (cigar) {
+    if (mode == tsu::kModeShared)
+      run_gw<true, tsu::kModeShared, kDual>(gw, threads, smem, a);
+    else
+      run_gw<true, tsu::kModeGlobal, kDual>(gw, threads, smem, a);
+  } else {
+    if (mode == tsu::kModeShared)
+      run_gw<false, tsu::kModeShared, kDual>(gw, threads, smem, a);
+    else
+      run_gw<false, tsu::kModeGlobal, kDual>(gw, threads, smem, a);
+  }
+}
+
 int main() {
-  int X, O, E, cigar, first_mode, first_gw;
+  int X, O, E, O2, E2, cigar, first_mode, first_gw;
   double hint;
   int64_t N;
-  if (!(std::cin >> X >> O >> E >> cigar >> hint >> first_mode >> first_gw >> N)) return 2;
+  if (!(std::cin >> X >> O >> E >> O2 >> E2 >> cigar >> hint >> first_mode >> first_gw >> N)) return 2;
   std::vector<std::string> pats(N), txts(N);
   for (int64_t i = 0; i < N; ++i) {
     int m, n;
@@ -76,9 +83,8 @@ int main() {
     std::cin.read(&txts[i][0], n);
     std::cin.get();
   }
-  const int g = gcd(gcd(X, O), E);
-  const int x = X / g, go = (O + E) / g, ge = E / g;
-  const int rm = std::max(x, go) + 1, re = ge + 1;
+  int g = 1;
+  const tsu::Pen rp = tsu::reduce_penalties(X, O, E, O2, E2, &g);
   const int smem_optin = 232448;
   // sequences: exact-size buffers (pattern i, text i concatenated)
   int64_t ptot = 0, ttot = 0;
@@ -121,7 +127,7 @@ int main() {
   Buf<int64_t> cpos(std::max<int64_t>(N, 1));
   Buf<int32_t> clen(std::max<int64_t>(N, 1)), retry(std::max<int64_t>(N, 1)), order(std::max<int64_t>(N, 1));
   Buf<unsigned long long> counters(8);  // [0]: queue (u32) + retry count (u32), [2]: cursor, [3..4]: work
-  int64_t arena_cap = tsu::arena_runs(x, go, N, max_m, max_n, hint);
+  int64_t arena_cap = tsu::arena_runs(rp, N, max_m, max_n, hint);
   Buf<uint32_t> arena(arena_cap);
   const bool want_cigar = cigar != 0;
   int64_t n_order = N;
@@ -136,7 +142,7 @@ int main() {
   int32_t pm = max_m, pn = max_n;
   std::string gws;
   for (;;) {
-    const tsu::PassGeom geo = tsu::plan_geometry(x, go, ge, rm, re, pm, pn, pc.mode, pc.gw, h, want_cigar, smem_optin);
+    const tsu::PassGeom geo = tsu::plan_geometry(rp, pm, pn, pc.mode, pc.gw, h, want_cigar, smem_optin);
     const int groups = geo.groups_per_cta;  // one block
     Buf<int32_t> ring(geo.mode == tsu::kModeGlobal ? (size_t)groups * geo.ring_ints : 0);
     Buf<uint32_t> hist(want_cigar ? (size_t)groups * geo.hist_cap : 0);
@@ -146,12 +152,8 @@ int main() {
     a.pk = pk;
     a.order = ord;
     a.n_order = n_order;
-    a.x = x;
-    a.go = go;
-    a.ge = ge;
+    a.pen = rp;
     a.g = g;
-    a.rm = rm;
-    a.re = re;
     a.ring_w = geo.ring_w;
     a.seq_cap = geo.seq_cap;
     a.ring_global = ring.p;
@@ -174,17 +176,10 @@ int main() {
     const size_t smem = (size_t)groups * geo.group_smem;
     const int threads = geo.cta_threads;
     gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);
-    if (want_cigar) {
-      if (geo.mode == tsu::kModeShared)
-        run_gw<true, tsu::kModeShared>(geo.gw, threads, smem, a);
-      else
-        run_gw<true, tsu::kModeGlobal>(geo.gw, threads, smem, a);
-    } else {
-      if (geo.mode == tsu::kModeShared)
-        run_gw<false, tsu::kModeShared>(geo.gw, threads, smem, a);
-      else
-        run_gw<false, tsu::kModeGlobal>(geo.gw, threads, smem, a);
-    }
+    if (rp.dual())
+      run_pass<true>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+    else
+      run_pass<false>(want_cigar, geo.mode, geo.gw, threads, smem, a);
     ++passes;
     const unsigned nretry = *retry_cnt;
     if (nretry == 0) break;
@@ -211,12 +206,12 @@ int main() {
     // the ladder's global step at 8 warps: emulating 16-warp groups (one
     // host thread per lane) is slow; the 16-warp global kernel has its own
     // test (test_warp_groups)
-    pc = tsu::next_pass(pc, rm, re, pm, pn, smem_optin, 8);
+    pc = tsu::next_pass(pc, rp, pm, pn, smem_optin, 8);
     if (want_cigar) {
       const unsigned long long used = *cursor;
       const int64_t maxlen = std::max(pm, pn);
       const int64_t need =
-          (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(x, go, maxlen, h) / std::min(x, go) + 1);
+          (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(rp, maxlen, h) / rp.min_pen() + 1);
       if (need > arena_cap) {
         Buf<uint32_t> nb(need);
         std::memcpy(nb.p, arena.p, sizeof(uint32_t) * (size_t)std::min<int64_t>((int64_t)used, arena_cap));

@@ -148,3 +148,19 @@ def test_no_gpu_fails_loudly():
 
     with pytest.raises(T.AlignError):
         T.Aligner(4, 6, 2)
+
+
+def test_dual_create_rejects_bad_penalties():
+    """tsu_create_dual / tsu_server_create_dual check the second gap piece
+    before touching a device."""
+    import ctypes
+
+    import tsunami_pact_b200 as T
+    from tsunami_pact_b200._lib import Penalties2
+
+    L = T.lib()
+    h = ctypes.c_void_p()
+    for pen in [(4, 6, 2, -1, 1), (4, 6, 2, 24, 0), (0, 6, 2, 24, 1), (4, 6, 2, 24, 1 << 21)]:
+        p2 = Penalties2(*pen)
+        assert L.tsu_create_dual(ctypes.byref(p2), None, ctypes.byref(h)) == 1, pen  # TSU_EINVAL
+        assert L.tsu_server_create_dual(ctypes.byref(p2), None, ctypes.byref(h)) == 1, pen

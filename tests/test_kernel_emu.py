@@ -32,7 +32,8 @@ def emu():
 
 
 def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1):
-    hdr = f"{pen[0]} {pen[1]} {pen[2]} {int(cigar)} {hint} {int(shared_first)} {gw} {len(pairs)}\n"
+    o2, e2 = (pen[3], pen[4]) if len(pen) == 5 else (-1, 0)
+    hdr = f"{pen[0]} {pen[1]} {pen[2]} {o2} {e2} {int(cigar)} {hint} {int(shared_first)} {gw} {len(pairs)}\n"
     body = b"".join(f"{len(p)} {len(t)}\n".encode() + p + b"\n" + t + b"\n" for p, t in pairs)
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1")
     r = subprocess.run([exe], input=hdr.encode() + body, capture_output=True, env=env, timeout=600)
@@ -187,3 +188,68 @@ def test_ladder_to_groups(emu, oracle):
     passes, retried, gws = check(emu, oracle, pairs)
     steps = gws.split(",")
     assert steps[0] == "s1" and steps[1].startswith("s") and int(steps[1][1:]) > 1, gws
+
+
+# --- dual gap-affine kernels (align_kernel<..., kDual = true>) ---------------
+
+def check_dual(exe, oracle, pairs, pen, **kw):
+    pairs = [(_b(p), _b(t)) for p, t in pairs]
+    got, passes, retried, gws = run_emu(exe, pairs, pen, **kw)
+    for (p, t), (s, ops) in zip(pairs, got):
+        es, eops = oracle.align2(p, t, *pen)
+        if kw.get("cigar", True):
+            assert (s, ops) == (es, eops), (p, t, pen, s, es, ops, eops)
+        else:
+            assert s == es and ops == "", (p, t, pen, s, es)
+    return passes, retried, gws
+
+
+def _long_indels(rng, n, lo=0, hi=160):
+    """Pairs with substitutions and long insertions / deletions (where the
+    second gap piece is the cheaper one)."""
+    pairs = []
+    for _ in range(n):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(lo, hi)))
+        t = list(p)
+        for _ in range(rng.randint(0, 4)):
+            pos = rng.randint(0, len(t))
+            L = rng.randint(1, 30)
+            if rng.random() < 0.5:
+                t[pos:pos] = [rng.choice("ACGT") for _ in range(L)]
+            else:
+                del t[pos:pos + L]
+        for _ in range(rng.randint(0, 6)):
+            if t:
+                t[rng.randrange(len(t))] = rng.choice("ACGT")
+        pairs.append((p, "".join(t)))
+    return pairs
+
+
+@pytest.mark.parametrize("pen", [(4, 6, 2, 24, 1), (3, 5, 3, 20, 1), (6, 2, 3, 10, 1), (1, 1, 1, 1, 1),
+                                 (8, 4, 4, 12, 2)])
+def test_dual_random(emu, oracle, pen):
+    """One warp per pair, shared ring first, ladder as the engine."""
+    rng = random.Random(sum(pen))
+    pairs = _long_indels(rng, 24) + [("", ""), ("", "ACGTACGT"), ("ACGTAC", ""), ("ACGTNNACGT", "ACGTACGT")]
+    check_dual(emu, oracle, pairs, pen)
+
+
+def test_dual_score_only(emu, oracle):
+    rng = random.Random(3)
+    check_dual(emu, oracle, _long_indels(rng, 20), (4, 6, 2, 24, 1), cigar=False)
+
+
+@pytest.mark.parametrize("gw,shared", [(4, True), (16, True), (2, False), (8, False), (32, False)])
+def test_dual_warp_groups(emu, oracle, gw, shared):
+    """Several warps per pair: the 11 partials combined across warps."""
+    rng = random.Random(gw * 5 + shared)
+    pairs = _long_indels(rng, 3, 150, 360)
+    check_dual(emu, oracle, pairs, (4, 6, 2, 24, 1), shared_first=shared, gw=gw)
+
+
+def test_dual_ladder(emu, oracle):
+    """Wide dual wavefronts leave one warp's shared ring and climb the ladder."""
+    rng = random.Random(9)
+    pairs = [_edited(rng, 400, 0.22)] + _long_indels(rng, 2, 200, 300)
+    passes, retried, gws = check_dual(emu, oracle, pairs, (4, 6, 2, 24, 1))
+    assert passes > 1, gws

@@ -30,6 +30,13 @@ class Penalties(ctypes.Structure):
     _fields_ = [("mismatch", c_i32), ("gap_opening", c_i32), ("gap_extension", c_i32)]
 
 
+class Penalties2(ctypes.Structure):
+    """Dual gap-affine penalties: a gap of length L costs
+    min(gap_opening + gap_extension*L, gap_opening2 + gap_extension2*L)."""
+    _fields_ = [("mismatch", c_i32), ("gap_opening", c_i32), ("gap_extension", c_i32), ("gap_opening2", c_i32),
+                ("gap_extension2", c_i32)]
+
+
 class Config(ctypes.Structure):
     _fields_ = [("device", c_i32), ("reserved0", c_i32), ("mem_budget", ctypes.c_size_t),
                 ("max_error_hint", ctypes.c_double)]
@@ -100,6 +107,7 @@ def lib():
         raise RuntimeError(f"{_LIB} is missing: build the CUDA engine first (tsunami_pact_b200.build())")
     L = ctypes.CDLL(_LIB)
     L.tsu_create.argtypes = [P(Penalties), P(Config), P(c_vp)]
+    L.tsu_create_dual.argtypes = [P(Penalties2), P(Config), P(c_vp)]
     L.tsu_destroy.argtypes = [c_vp]
     L.tsu_status_str.restype = ctypes.c_char_p
     L.tsu_status_str.argtypes = [ctypes.c_int]
@@ -125,6 +133,7 @@ def lib():
                                 ctypes.c_int]
     L.tsu_predict_bytes.argtypes = [c_vp, P(Batch), c_u32, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.tsu_server_create.argtypes = [P(Penalties), P(ServerConfig), P(c_vp)]
+    L.tsu_server_create_dual.argtypes = [P(Penalties2), P(ServerConfig), P(c_vp)]
     L.tsu_server_destroy.argtypes = [c_vp]
     L.tsu_submit.argtypes = [c_vp, P(Batch), c_u32, P(ctypes.c_uint64)]
     L.tsu_poll.argtypes = [c_vp, ctypes.c_uint64, P(Result), P(RequestInfo)]
@@ -171,16 +180,24 @@ def runs_to_string(runs: np.ndarray) -> str:
 
 class Aligner:
     """One device context with fixed penalties (reference argv 1-3,
-    wfa_gpu.cu:59-61)."""
+    wfa_gpu.cu:59-61).  With ``gap_opening2`` and ``gap_extension2`` the
+    context aligns under dual gap-affine penalties (tsu_create_dual)."""
 
     def __init__(self, mismatch: int = 4, gap_opening: int = 6, gap_extension: int = 2, device: int = 0,
-                 mem_budget: int = 0, max_error_hint: float = 0.0):
-        self.penalties = (mismatch, gap_opening, gap_extension)
+                 mem_budget: int = 0, max_error_hint: float = 0.0, gap_opening2: Optional[int] = None,
+                 gap_extension2: Optional[int] = None):
         L = lib()
-        pen = Penalties(mismatch, gap_opening, gap_extension)
         cfg = Config(device, 0, mem_budget, max_error_hint)
         h = c_vp()
-        rc = L.tsu_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
+        if gap_opening2 is None and gap_extension2 is None:
+            self.penalties = (mismatch, gap_opening, gap_extension)
+            pen = Penalties(mismatch, gap_opening, gap_extension)
+            rc = L.tsu_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
+        else:
+            self.penalties = (mismatch, gap_opening, gap_extension, gap_opening2, gap_extension2)
+            pen2 = Penalties2(mismatch, gap_opening, gap_extension, -1 if gap_opening2 is None else gap_opening2,
+                              0 if gap_extension2 is None else gap_extension2)
+            rc = L.tsu_create_dual(ctypes.byref(pen2), ctypes.byref(cfg), ctypes.byref(h))
         if rc != TSU_OK:
             raise AlignError(rc, L.tsu_status_str(rc).decode())
         self._h = h
@@ -309,14 +326,20 @@ class Server:
     def __init__(self, mismatch: int = 4, gap_opening: int = 6, gap_extension: int = 2, device: int = 0,
                  workers: int = 0, mem_budget: int = 0, max_error_hint: float = 0.0, max_queue: int = 0,
                  max_job_pairs: int = 0, max_job_requests: int = 0, heavy_len: int = 0, heavy_workers: int = 0,
-                 estimate_hint: bool = True, watchdog_ms: float = 0.0, resident_bytes: int = 0):
+                 estimate_hint: bool = True, watchdog_ms: float = 0.0, resident_bytes: int = 0,
+                 gap_opening2: Optional[int] = None, gap_extension2: Optional[int] = None):
         L = lib()
-        pen = Penalties(mismatch, gap_opening, gap_extension)
         cfg = ServerConfig(device, workers, mem_budget, max_error_hint, max_queue, max_job_pairs,
                            max_job_requests, heavy_len, heavy_workers, 0 if estimate_hint else -1, watchdog_ms,
                            resident_bytes)
         h = c_vp()
-        rc = L.tsu_server_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
+        if gap_opening2 is None and gap_extension2 is None:
+            pen = Penalties(mismatch, gap_opening, gap_extension)
+            rc = L.tsu_server_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
+        else:
+            pen2 = Penalties2(mismatch, gap_opening, gap_extension, -1 if gap_opening2 is None else gap_opening2,
+                              0 if gap_extension2 is None else gap_extension2)
+            rc = L.tsu_server_create_dual(ctypes.byref(pen2), ctypes.byref(cfg), ctypes.byref(h))
         if rc != TSU_OK:
             raise AlignError(rc, L.tsu_status_str(rc).decode())
         self._h = h

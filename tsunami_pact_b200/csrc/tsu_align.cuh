@@ -29,6 +29,11 @@
 // and then overwrite one, take a barrier in between.
 // Thread 0 of the group walks the backtrace once the end is reached
 // (tsu_backtrace.cuh).
+// kDual: dual gap-affine (a gap of length L costs min(o1 + e1 L, o2 + e2 L)),
+// the I2 / D2 components the reference declares (common.h:52-58,67-77,80-87):
+// two more gap components with their own ring slots (s - o2 - e2, s - e2),
+// M = max(mismatch, D2, D1, I2, I1) with ties in that (piggyback) order, and
+// a backtrace word with a 3-bit M source and four extension bits.
 #pragma once
 
 #include <type_traits>
@@ -61,7 +66,7 @@ constexpr int cta_min_blocks() {
   return kMode == kModeShared ? (GW <= 4 ? 6 : (GW == 8 ? 3 : 1)) : (GW <= 4 ? 4 : (GW == 8 ? 2 : 1));
 }
 
-template <bool kCigar, int kMode, int GW>
+template <bool kCigar, int kMode, int GW, bool kDual = false>
 __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>())) align_kernel(AlignArgs a) {
   static_assert(GW == 1 || GW == 2 || GW == 4 || GW == 8 || GW == 16 || GW == 32, "warps per pair");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
@@ -80,14 +85,16 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
   const int wig = gt >> 5;  // warp within the group
   const int gpb = blockDim.x / GT;
   const int64_t ggroup = (int64_t)blockIdx.x * gpb + gid;
-  const int ns = ring_slots(a.rm, a.re);
+  constexpr int PW = kDual ? 16 : 8;  // partial words per warp and step parity
+  const int ns = a.pen.slots();
   const int W = a.ring_w;
-  unsigned char* gsm = smem_raw + (size_t)gid * group_smem_bytes(a.rm, a.re, W, kMode, a.seq_cap, GW);
+  const int rm = a.pen.rm, re = a.pen.re;
+  unsigned char* gsm = smem_raw + (size_t)gid * group_smem_bytes(a.pen, W, kMode, a.seq_cap, GW);
   int* s_lo = reinterpret_cast<int*>(gsm);
   int* s_hi = s_lo + ns;
   int* s_alo = s_hi + ns;
-  int* part = s_alo + ns;                  // [2][GW][8] warp partials (GW > 1)
-  int* bc = part + (GW > 1 ? 16 * GW : 0);  // broadcast words
+  int* part = s_alo + ns;                      // [2][GW][PW] warp partials (GW > 1)
+  int* bc = part + (GW > 1 ? 2 * PW * GW : 0);  // broadcast words
   unsigned char* tail = reinterpret_cast<unsigned char*>(bc + 4);
   RT* ring;
   uint32_t* sseq = nullptr;
@@ -121,7 +128,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
     const uint8_t* pb = a.seq.pat + a.seq.pat_off[pair];
     const uint8_t* tb = a.seq.txt + a.seq.txt_off[pair];
     const int k_end = n - m;
-    const int64_t s_max = score_bound(m, n, a.x, a.go, a.ge);
+    const int64_t s_max = score_bound(m, n, a.pen);
     const int pwn = 2 * ((m + 31) / 32 + 1);
     const int twn = 2 * ((n + 31) / 32 + 1);
 
@@ -130,6 +137,9 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       // bytes outside ACGT, lengths beyond int16 or sequences beyond the
       // staging area: handled by the global variant
       if (bytemode || m > 32000 || n > 32000 || pwn + twn > a.seq_cap) st = kPairScratch;
+    }
+    if constexpr (kDual) {
+      if (m > kDualMaxLen || n > kDualMaxLen) st = kPairInternal;  // beyond the backtrace word
     }
     int s_end = -1;
     int64_t hbase = 0;
@@ -184,26 +194,29 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       }
 
       int s = 0;
-      int slm = 0, sli = 0;  // s mod rm, s mod re
+      int slm = 0, sli = 0, sli2 = 0;  // s mod rm, s mod re, s mod re2
       while (s_end < 0) {
         ++s;
-        if (++slm == a.rm) slm = 0;
-        if (++sli == a.re) sli = 0;
+        if (++slm == rm) slm = 0;
+        if (++sli == re) sli = 0;
+        if constexpr (kDual) {
+          if (++sli2 == a.pen.re2) sli2 = 0;
+        }
         if (s > s_max) {  // the end is reachable by s_max: inconsistency
           st = kPairInternal;
           break;
         }
         int q;
-        q = slm - a.x;
-        if (q < 0) q += a.rm;
+        q = slm - a.pen.x;
+        if (q < 0) q += rm;
         const int slot_mm = q;
-        q = slm - a.go;
-        if (q < 0) q += a.rm;
+        q = slm - a.pen.go;
+        if (q < 0) q += rm;
         const int slot_mo = q;
-        q = sli - a.ge;
-        if (q < 0) q += a.re;
-        const int slot_ie = a.rm + q;
-        const int slot_de = a.rm + a.re + q;
+        q = sli - a.pen.ge;
+        if (q < 0) q += re;
+        const int slot_ie = rm + q;
+        const int slot_de = rm + re + q;
         // sources: first diagonal, cell count (0 = null), ring index of lo.
         // Slot limits are either a trimmed range inside the slot's compute
         // range or the empty range (1, 0); the count is taken by comparison.
@@ -217,18 +230,39 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             b_x = slot * W + l - s_alo[slot];
           }
         };
-        if (s - a.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
-        if (s - a.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
-        if (s - a.ge >= 0) {
+        if (s - a.pen.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
+        if (s - a.pen.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
+        if (s - a.pen.ge >= 0) {
           src(slot_ie, lo_ie, c_ie, b_ie);
           src(slot_de, lo_de, c_de, b_de);
         }
-        const int out_m = slm, out_i = a.rm + sli, out_d = a.rm + a.re + sli;
-        if ((c_mm | c_mo | c_ie | c_de) == 0) {  // null step (wfa_gpu.cu:417-422)
+        // second gap piece (kDual): M at s - o2 - e2, I2 / D2 at s - e2
+        int lo_mo2 = 0, c_mo2 = 0, b_mo2 = 0, lo_ie2 = 0, c_ie2 = 0, b_ie2 = 0, lo_de2 = 0, c_de2 = 0, b_de2 = 0;
+        int out_i2 = 0, out_d2 = 0;
+        if constexpr (kDual) {
+          const int re2 = a.pen.re2;
+          q = slm - a.pen.go2;
+          if (q < 0) q += rm;
+          if (s - a.pen.go2 >= 0) src(q, lo_mo2, c_mo2, b_mo2);
+          q = sli2 - a.pen.ge2;
+          if (q < 0) q += re2;
+          if (s - a.pen.ge2 >= 0) {
+            src(rm + 2 * re + q, lo_ie2, c_ie2, b_ie2);
+            src(rm + 2 * re + re2 + q, lo_de2, c_de2, b_de2);
+          }
+          out_i2 = rm + 2 * re + sli2;
+          out_d2 = rm + 2 * re + re2 + sli2;
+        }
+        const int out_m = slm, out_i = rm + sli, out_d = rm + re + sli;
+        if ((c_mm | c_mo | c_ie | c_de | c_mo2 | c_ie2 | c_de2) == 0) {  // null step (wfa_gpu.cu:417-422)
           group_sync<GW>(gid);  // everyone has read the slot limits
           s_lo[out_m] = 1; s_hi[out_m] = 0;
           s_lo[out_i] = 1; s_hi[out_i] = 0;
           s_lo[out_d] = 1; s_hi[out_d] = 0;
+          if constexpr (kDual) {
+            s_lo[out_i2] = 1; s_hi[out_i2] = 0;
+            s_lo[out_d2] = 1; s_hi[out_d2] = 0;
+          }
           if constexpr (GW == 1) __syncwarp();
           continue;
         }
@@ -237,16 +271,25 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         if (c_mo) { lo = min(lo, lo_mo - 1); hi = max(hi, lo_mo + c_mo); }
         if (c_ie) { lo = min(lo, lo_ie + 1); hi = max(hi, lo_ie + c_ie); }
         if (c_de) { lo = min(lo, lo_de - 1); hi = max(hi, lo_de + c_de - 2); }
+        if constexpr (kDual) {
+          if (c_mo2) { lo = min(lo, lo_mo2 - 1); hi = max(hi, lo_mo2 + c_mo2); }
+          if (c_ie2) { lo = min(lo, lo_ie2 + 1); hi = max(hi, lo_ie2 + c_ie2); }
+          if (c_de2) { lo = min(lo, lo_de2 - 1); hi = max(hi, lo_de2 + c_de2 - 2); }
+        }
         const int width = hi - lo + 1;
         const bool i_present = c_mo || c_ie;
         const bool d_present = c_mo || c_de;
+        const bool i2_present = kDual && (c_mo2 || c_ie2);
+        const bool d2_present = kDual && (c_mo2 || c_de2);
         if (width > W || (kCigar && (s >= a.table_cap || hbase + width > a.hist_cap))) {
           st = kPairScratch;
           break;
         }
         const int w_m = out_m * W - lo, w_i = out_i * W - lo, w_d = out_d * W - lo;
+        const int w_i2 = out_i2 * W - lo, w_d2 = out_d2 * W - lo;
         uint32_t* hrow = kCigar ? hist + hbase - lo : nullptr;
         int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
+        int fi2 = INT_MAX, li2 = INT_MIN, fd2 = INT_MAX, ld2 = INT_MIN;
         bool found = false;
         for (int k = lo + gt; k <= hi; k += GT) {
           int j;
@@ -262,13 +305,41 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
           const int32_t ins = max(ins_o, ins_e) + 1;
           const int32_t del = max(del_o, del_e);
-          // M = max(D, mismatch, I); ties: mismatch > D > I (piggyback order)
-          int32_t p = ins;
-          uint32_t bits = kSrcIns;
-          if (del >= p) { p = del; bits = kSrcDel; }
-          if (mis >= p) { p = mis; bits = kSrcMis; }
-          if (ins_e >= ins_o) bits |= kIExt;
-          if (del_e >= del_o) bits |= kDExt;
+          int32_t ins2 = kNull, del2 = kNull;
+          uint32_t bits;
+          int32_t p;
+          if constexpr (kDual) {
+            j = k - 1 - lo_mo2;
+            const int32_t ins2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+            j = k - 1 - lo_ie2;
+            const int32_t ins2_e = ((unsigned)j < (unsigned)c_ie2) ? (int32_t)ring[b_ie2 + j] : kNull;
+            j = k + 1 - lo_mo2;
+            const int32_t del2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+            j = k + 1 - lo_de2;
+            const int32_t del2_e = ((unsigned)j < (unsigned)c_de2) ? (int32_t)ring[b_de2 + j] : kNull;
+            ins2 = max(ins2_o, ins2_e) + 1;
+            del2 = max(del2_o, del2_e);
+            // M = max(mismatch, D2, D1, I2, I1), ties in that order
+            // (piggyback codes 9 > 8,7 > 6,5 > 4,3 > 2,1)
+            p = ins;
+            bits = kSrcIns;
+            if (ins2 >= p) { p = ins2; bits = kSrcIns2; }
+            if (del >= p) { p = del; bits = kSrcDel; }
+            if (del2 >= p) { p = del2; bits = kSrcDel2; }
+            if (mis >= p) { p = mis; bits = kSrcMis; }
+            if (ins_e >= ins_o) bits |= kI1Ext2;
+            if (del_e >= del_o) bits |= kD1Ext2;
+            if (ins2_e >= ins2_o) bits |= kI2Ext2;
+            if (del2_e >= del2_o) bits |= kD2Ext2;
+          } else {
+            // M = max(D, mismatch, I); ties: mismatch > D > I (piggyback order)
+            p = ins;
+            bits = kSrcIns;
+            if (del >= p) { p = del; bits = kSrcDel; }
+            if (mis >= p) { p = mis; bits = kSrcMis; }
+            if (ins_e >= ins_o) bits |= kIExt;
+            if (del_e >= del_o) bits |= kDExt;
+          }
           int32_t om = kNull;
           if (in_bounds(p, k, m, n)) {
             const int vv = p - k;
@@ -287,7 +358,17 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             store(w_d + k, del);
             if (in_bounds(del, k, m, n)) { fd = min(fd, k); ld = k; }
           }
-          if (kCigar) hrow[k] = ((uint32_t)p << 4) | bits;
+          if constexpr (kDual) {
+            if (i2_present) {
+              store(w_i2 + k, ins2);
+              if (in_bounds(ins2, k, m, n)) { fi2 = min(fi2, k); li2 = k; }
+            }
+            if (d2_present) {
+              store(w_d2 + k, del2);
+              if (in_bounds(del2, k, m, n)) { fd2 = min(fd2, k); ld2 = k; }
+            }
+          }
+          if (kCigar) hrow[k] = ((uint32_t)p << (kDual ? 8 : 4)) | bits;
         }
         fm = __reduce_min_sync(FULL, fm);
         lm = __reduce_max_sync(FULL, lm);
@@ -296,18 +377,31 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         fd = __reduce_min_sync(FULL, fd);
         ld = __reduce_max_sync(FULL, ld);
         bool any_found = __any_sync(FULL, found);
+        if constexpr (kDual) {
+          fi2 = __reduce_min_sync(FULL, fi2);
+          li2 = __reduce_max_sync(FULL, li2);
+          fd2 = __reduce_min_sync(FULL, fd2);
+          ld2 = __reduce_max_sync(FULL, ld2);
+        }
         if constexpr (GW > 1) {
-          int* pp = part + ((s & 1) * GW + wig) * 8;
+          int* pp = part + ((s & 1) * GW + wig) * PW;
           if (lane == 0) {
             pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = any_found;
+            if constexpr (kDual) {
+              pp[7] = fi2; pp[8] = li2; pp[9] = fd2; pp[10] = ld2;
+            }
           }
           group_sync<GW>(gid);  // the step's ring writes and partials are complete
           // lane w takes warp w's partials; warp reductions combine them
           // (7 loads and 7 reductions per thread instead of 7 * GW)
           int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = 0;
+          int p7 = INT_MAX, p8 = INT_MIN, p9 = INT_MAX, p10 = INT_MIN;
           if (lane < GW) {
-            const int* qw = part + ((s & 1) * GW + lane) * 8;
+            const int* qw = part + ((s & 1) * GW + lane) * PW;
             p0 = qw[0]; p1 = qw[1]; p2 = qw[2]; p3 = qw[3]; p4 = qw[4]; p5 = qw[5]; p6 = qw[6];
+            if constexpr (kDual) {
+              p7 = qw[7]; p8 = qw[8]; p9 = qw[9]; p10 = qw[10];
+            }
           }
           fm = __reduce_min_sync(FULL, p0);
           lm = __reduce_max_sync(FULL, p1);
@@ -316,6 +410,12 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           fd = __reduce_min_sync(FULL, p4);
           ld = __reduce_max_sync(FULL, p5);
           any_found = __any_sync(FULL, p6 != 0);
+          if constexpr (kDual) {
+            fi2 = __reduce_min_sync(FULL, p7);
+            li2 = __reduce_max_sync(FULL, p8);
+            fd2 = __reduce_min_sync(FULL, p9);
+            ld2 = __reduce_max_sync(FULL, p10);
+          }
         }
         {
           // trimmed limits (wfa_gpu.cu:636-719), written by every thread
@@ -325,6 +425,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
           s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
           s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
+          if constexpr (kDual) {
+            const bool ei2 = !i2_present || fi2 > li2, ed2 = !d2_present || fd2 > ld2;
+            s_lo[out_i2] = ei2 ? 1 : fi2; s_hi[out_i2] = ei2 ? 0 : li2; s_alo[out_i2] = lo;
+            s_lo[out_d2] = ed2 ? 1 : fd2; s_hi[out_d2] = ed2 ? 0 : ld2; s_alo[out_d2] = lo;
+          }
           if (kCigar && gt == 0) table[s] = make_int2(lo, (int)hbase);
         }
         hbase += width;
@@ -339,7 +444,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       if (gt == 0) a.score[pair] = s_end * a.g;
       if (kCigar) {
         // reserve the run bound 2*s/min_pen + 1 in the arena, then walk
-        const int min_pen = min(a.x, a.go);
+        const int min_pen = a.pen.min_pen();
         const int64_t bound = 2 * (int64_t)s_end / min_pen + 1;
         if (gt == 0) {
           int32_t len = 0;
@@ -348,8 +453,12 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           if ((int64_t)(at + bound) > a.arena_cap) {
             st = kPairArena;
           } else {
-            const int r =
-                backtrace_walk(hist, hbase, table, s_end, m, n, a.x, a.go, a.ge, a.arena + at + bound, (int)bound);
+            int r;
+            if constexpr (kDual)
+              r = backtrace_walk_dual(hist, hbase, table, s_end, m, n, a.pen, a.arena + at + bound, (int)bound);
+            else
+              r = backtrace_walk(hist, hbase, table, s_end, m, n, a.pen.x, a.pen.go, a.pen.ge, a.arena + at + bound,
+                                 (int)bound);
             if (r < 0) {
               st = kPairInternal;
             } else {

@@ -123,4 +123,84 @@ static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t 
   return w.cnt <= cap ? w.cnt : -1;
 }
 
+// Dual gap-affine walk over words of the kDual kernel: five states (M, I1,
+// D1, I2, D2); in M the 3-bit source picks the component, whose extension
+// bit (kI1Ext2 ... kD2Ext2) then says open (back to M, s - o_j - e_j) or
+// extend (stay, s - e_j).  Same return convention as backtrace_walk.
+static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int64_t hist_used,
+                                          const int2* __restrict__ table, int s_end, int m, int n, const Pen& pen,
+                                          uint32_t* out_end, int cap) {
+  RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
+  // state = M source code of the component being walked (kSrcMis for M)
+  uint32_t state = kSrcMis;
+  int s = s_end, k = n - m;
+  int32_t off = n;
+  int v = off - k, h = off;
+  int guard = 4 * (m + n) + 8;
+  while (v > 0 && h > 0 && s > 0) {
+    if (--guard < 0) return -1;
+    const int2 te = table[s];
+    const int64_t hidx = (int64_t)te.y + (k - te.x);
+    if (k < te.x || hidx >= hist_used) return -1;  // never on a valid path
+    const uint32_t word = hist[hidx];
+    uint32_t comp = state;
+    if (state == kSrcMis) {
+      const int32_t p = (int32_t)(word >> 8);
+      if (p > off) return -1;
+      w.put(kOpM, off - p);
+      off = p;
+      v = off - k;
+      h = off;
+      if (v <= 0 || h <= 0) break;
+      comp = word & 7u;
+      if (comp == kSrcMis) {
+        w.put(kOpX, 1);
+        s -= pen.x;
+        --off;
+        v = off - k;
+        h = off;
+        if (s < 0) return -1;
+        continue;
+      }
+    }
+    bool ext, ins;
+    int go, ge;
+    switch (comp) {
+      case kSrcIns: ext = word & kI1Ext2; ins = true; go = pen.go; ge = pen.ge; break;
+      case kSrcDel: ext = word & kD1Ext2; ins = false; go = pen.go; ge = pen.ge; break;
+      case kSrcIns2: ext = word & kI2Ext2; ins = true; go = pen.go2; ge = pen.ge2; break;
+      case kSrcDel2: ext = word & kD2Ext2; ins = false; go = pen.go2; ge = pen.ge2; break;
+      default: return -1;
+    }
+    if (ins) {
+      w.put(kOpI, 1);
+      --k;
+      --off;
+    } else {
+      w.put(kOpD, 1);
+      ++k;
+    }
+    if (ext) {
+      s -= ge;
+      state = comp;
+    } else {
+      s -= go;
+      state = kSrcMis;
+    }
+    v = off - k;
+    h = off;
+    if (s < 0) return -1;
+  }
+  if (v > 0 && h > 0) {
+    const int nm = v < h ? v : h;
+    w.put(kOpM, nm);
+    v -= nm;
+    h -= nm;
+  }
+  w.put(kOpD, v);
+  w.put(kOpI, h);
+  w.flush();
+  return w.cnt <= cap ? w.cnt : -1;
+}
+
 }  // namespace tsu

@@ -18,6 +18,11 @@ constexpr int16_t kNull16 = -16384;       // int16 ring null (any negative value
 enum : int32_t { kPairOk = 0, kPairScratch = 1, kPairArena = 2, kPairInternal = 3 };
 // backtrace word: bits 31..4 pre-extension M offset, 1..0 M source, 2 I ext, 3 D ext
 enum : uint32_t { kSrcMis = 0, kSrcIns = 1, kSrcDel = 2, kIExt = 4, kDExt = 8 };
+// dual gap-affine backtrace word: bits 31..8 pre-extension M offset, 2..0 M
+// source (kSrcMis, kSrcIns, kSrcDel, kSrcIns2, kSrcDel2), then one extension
+// bit per gap component
+enum : uint32_t { kSrcIns2 = 3, kSrcDel2 = 4, kI1Ext2 = 8, kD1Ext2 = 16, kI2Ext2 = 32, kD2Ext2 = 64 };
+constexpr int kDualMaxLen = (1 << 24) - 2;  // offsets of the dual backtrace word
 enum : uint32_t { kOpM = 0, kOpI = 1, kOpD = 2, kOpX = 8 };
 // align kernel variants
 enum : int { kModeShared = 0, kModeGlobal = 1 };
@@ -38,13 +43,72 @@ struct PackView {
   uint8_t* nonacgt;     // [2n]: 1 if the sequence holds a byte outside ACGT
 };
 
+// Penalties in score units g = gcd of all penalties, and the depths of the
+// wavefront ring: rm M slots (the scores s - x, s - o - e, s - o2 - e2 back),
+// re slots of I1 and of D1 (s - e back) and, for dual gap-affine, re2 slots
+// of I2 and of D2.  go = o + e (a gap of length L costs go + ge (L - 1)).
+// One piece: go2 = ge2 = re2 = 0.
+struct Pen {
+  int x = 0, go = 0, ge = 0, go2 = 0, ge2 = 0;
+  int rm = 0, re = 0, re2 = 0;
+  __host__ __device__ bool dual() const { return re2 > 0; }
+  __host__ __device__ int slots() const { return rm + 2 * re + 2 * re2; }
+  // cheapest and dearest single edit, smallest extension
+  __host__ __device__ int min_pen() const {
+    const int a = x < go ? x : go;
+    return dual() && go2 < a ? go2 : a;
+  }
+  __host__ __device__ int max_pen() const {
+    const int a = x > go ? x : go;
+    return dual() && go2 > a ? go2 : a;
+  }
+  __host__ __device__ int min_ge() const { return dual() && ge2 < ge ? ge2 : ge; }
+  // cost of one gap of length L >= 1
+  __host__ __device__ int64_t gap(int64_t L) const {
+    const int64_t a = (int64_t)go + (int64_t)ge * (L - 1);
+    if (!dual()) return a;
+    const int64_t b = (int64_t)go2 + (int64_t)ge2 * (L - 1);
+    return a < b ? a : b;
+  }
+};
+
+inline int gcd_int(int a, int b) {
+  while (b) {
+    const int t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Reduce raw penalties (mismatch, open, extend; open2 / ext2 < 0: one piece)
+// to score units; *g receives the unit.
+inline Pen reduce_penalties(int mismatch, int open, int ext, int open2, int ext2, int* g) {
+  const bool dual = open2 >= 0 && ext2 > 0;
+  int u = gcd_int(gcd_int(mismatch, open), ext);
+  if (dual) u = gcd_int(gcd_int(u, open2), ext2);
+  Pen p;
+  p.x = mismatch / u;
+  p.go = (open + ext) / u;
+  p.ge = ext / u;
+  if (dual) {
+    p.go2 = (open2 + ext2) / u;
+    p.ge2 = ext2 / u;
+  }
+  p.re = p.ge + 1;
+  p.re2 = dual ? p.ge2 + 1 : 0;
+  p.rm = p.max_pen() + 1;
+  if (g) *g = u;
+  return p;
+}
+
 struct AlignArgs {
   SeqView seq;
   PackView pk;
   const int32_t* order;  // pairs of this launch (nullptr: 0..n_order-1)
   int64_t n_order;
-  int x, go, ge, g;      // reduced mismatch, open+extend, extend; gcd
-  int rm, re;            // ring depths: rm = max(x, go) + 1, re = ge + 1
+  Pen pen;               // reduced penalties and ring depths
+  int g;                 // score unit
   int ring_w;            // diagonals per ring slot
   int seq_cap;           // shared-memory sequence words (uint32) per warp
   int32_t* ring_global;  // per-warp rings (global mode)
@@ -66,15 +130,16 @@ struct AlignArgs {
   unsigned long long* work;  // [2]: wavefront cells computed, score steps
 };
 
-__host__ __device__ inline int ring_slots(int rm, int re) { return rm + 2 * re; }
+// Warp partials per warp and step parity: 7 (one piece) or 11 values.
+__host__ __device__ inline int partial_words(const Pen& p) { return p.dual() ? 16 : 8; }
 
 // Shared memory per group of gw warps, in bytes: slot limits (lo, hi, alo
-// per slot), warp partials [2][gw][8] (gw > 1), 4 broadcast words, then in
-// shared mode an int16 ring of ring_slots * ring_w and seq_cap sequence
-// words.
-__host__ __device__ inline int group_smem_bytes(int rm, int re, int ring_w, int mode, int seq_cap, int gw) {
-  const int ns = ring_slots(rm, re);
-  int b = 3 * ns * 4 + (gw > 1 ? 16 * gw * 4 : 0) + 16;
+// per slot), warp partials [2][gw][partial_words] (gw > 1), 4 broadcast
+// words, then in shared mode an int16 ring of slots * ring_w and seq_cap
+// sequence words.
+__host__ __device__ inline int group_smem_bytes(const Pen& p, int ring_w, int mode, int seq_cap, int gw) {
+  const int ns = p.slots();
+  int b = 3 * ns * 4 + (gw > 1 ? 2 * partial_words(p) * gw * 4 : 0) + 16;
   if (mode == kModeShared) {
     b += ((ns * ring_w * 2 + 15) & ~15) + seq_cap * 4;
   }
@@ -87,11 +152,11 @@ __device__ __forceinline__ bool in_bounds(int32_t off, int k, int m, int n) {
 
 // Reduced-unit upper bound of the optimal score: all mismatches plus the
 // length difference as one gap, or one gap per sequence.
-__device__ __forceinline__ int64_t score_bound(int m, int n, int x, int go, int ge) {
+__host__ __device__ __forceinline__ int64_t score_bound(int m, int n, const Pen& p) {
   const int mn = m < n ? m : n;
   const int d = m > n ? m - n : n - m;
-  const int64_t a = (int64_t)x * mn + (d ? (int64_t)(go - ge) + (int64_t)ge * d : 0);
-  const int64_t b = (m ? (int64_t)(go - ge) + (int64_t)ge * m : 0) + (n ? (int64_t)(go - ge) + (int64_t)ge * n : 0);
+  const int64_t a = (int64_t)p.x * mn + (d ? p.gap(d) : 0);
+  const int64_t b = (m ? p.gap(m) : 0) + (n ? p.gap(n) : 0);
   return a < b ? a : b;
 }
 

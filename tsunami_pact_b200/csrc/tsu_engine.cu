@@ -26,6 +26,7 @@
 #include "../../include/tsunami_b200.h"
 #include "tsu_engine_internal.h"
 #include "tsu_kernels.cuh"
+#include "tsu_launch.cuh"
 #include "tsu_plan.h"
 
 namespace {
@@ -55,8 +56,9 @@ struct tsu_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
-  tsu_penalties pen{};
-  int x = 0, go = 0, ge = 0, g = 1, rm = 0, re = 0;
+  tsu_penalties2 pen{};  // raw penalties (gap_opening2 < 0: one piece)
+  tsu::Pen rp;  // reduced penalties, ring depths
+  int g = 1;    // score unit
   size_t budget = 0;
   double err_hint = 0.2;
   int sms = 0;
@@ -134,13 +136,17 @@ int set_err(tsu_ctx* c, int code, const char* fmt, ...) {
       return set_err(ctx, TSU_EDEVICE, "%s at %s:%d: %s", #call, __FILE__, __LINE__, cudaGetErrorString(e_)); \
   } while (0)
 
-int gcd(int a, int b) {
-  while (b) {
-    int t = a % b;
-    a = b;
-    b = t;
-  }
-  return a;
+// Longest pattern or text of a pair: 2^26, or the dual backtrace word's
+// offset range.
+int32_t max_len(const tsu_ctx* ctx) { return ctx->rp.dual() ? tsu::kDualMaxLen : (1 << 26); }
+
+// Raw penalties within the supported ranges: mismatch > 0, opening >= 0,
+// extension > 0, each at most 2^20; the second gap piece is off
+// (gap_opening2 < 0) or obeys the same ranges.
+bool valid_penalties(const tsu_penalties2* p) {
+  auto ok = [](int32_t o, int32_t e) { return o >= 0 && e > 0 && o <= (1 << 20) && e <= (1 << 20); };
+  if (p->mismatch <= 0 || p->mismatch > (1 << 20) || !ok(p->gap_opening, p->gap_extension)) return false;
+  return p->gap_opening2 < 0 || ok(p->gap_opening2, p->gap_extension2);
 }
 
 // Device memory of every context comes from one stream-ordered pool per
@@ -271,72 +277,20 @@ struct BatchInfo {
   int64_t total_words = 0;
 };
 
-// The align_kernel instantiations: CIGAR or score only, shared or global
-// wavefront ring, 1/2/4/8/16/32 warps per pair.  Each kernel's dynamic shared
-// memory limit is set to the device maximum once per device (always the same
-// value, so contexts planning on several host threads cannot lower it under
-// another's launch).
-template <bool kCigar, int kMode, int GW>
-cudaError_t occ_one(int threads, size_t smem, int optin, int* occ) {
-  static std::atomic<uint64_t> limit_set{0};  // bit d: set on device d
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  const uint64_t bit = dev < 64 ? (1ull << dev) : 0;
-  if (!bit || !(limit_set.load() & bit)) {
-    e = cudaFuncSetAttribute(tsu::align_kernel<kCigar, kMode, GW>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    if (e != cudaSuccess) return e;
-    limit_set.fetch_or(bit);
-  }
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, tsu::align_kernel<kCigar, kMode, GW>, threads, smem);
+// The align_kernel instantiations (tsu_launch.cuh): one-piece kernels here,
+// dual gap-affine ones in tsu_dual.cu.
+cudaError_t align_occupancy(const tsu_ctx* ctx, bool cigar, int mode, int gw, int threads, size_t smem, int optin,
+                            int* occ) {
+  if (ctx->rp.dual()) return tsu::align_occupancy_dual(cigar, mode, gw, threads, smem, optin, occ);
+  return tsu::launch_detail::occupancy<false>(cigar, mode, gw, threads, smem, optin, occ);
 }
 
-template <bool kCigar, int kMode>
-cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
-  switch (gw) {
-    case 1: return occ_one<kCigar, kMode, 1>(threads, smem, optin, occ);
-    case 2: return occ_one<kCigar, kMode, 2>(threads, smem, optin, occ);
-    case 4: return occ_one<kCigar, kMode, 4>(threads, smem, optin, occ);
-    case 8: return occ_one<kCigar, kMode, 8>(threads, smem, optin, occ);
-    case 16: return occ_one<kCigar, kMode, 16>(threads, smem, optin, occ);
-    case 32: return occ_one<kCigar, kMode, 32>(threads, smem, optin, occ);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-cudaError_t align_occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ) {
-  if (cigar) return mode == tsu::kModeShared ? occ_gw<true, tsu::kModeShared>(gw, threads, smem, optin, occ)
-                                             : occ_gw<true, tsu::kModeGlobal>(gw, threads, smem, optin, occ);
-  return mode == tsu::kModeShared ? occ_gw<false, tsu::kModeShared>(gw, threads, smem, optin, occ)
-                                  : occ_gw<false, tsu::kModeGlobal>(gw, threads, smem, optin, occ);
-}
-
-template <bool kCigar, int kMode>
-void launch_gw(int gw, int blocks, int threads, size_t smem, cudaStream_t st, const tsu::AlignArgs& a) {
-  switch (gw) {
-    case 1: tsu::align_kernel<kCigar, kMode, 1><<<blocks, threads, smem, st>>>(a); break;
-    case 2: tsu::align_kernel<kCigar, kMode, 2><<<blocks, threads, smem, st>>>(a); break;
-    case 4: tsu::align_kernel<kCigar, kMode, 4><<<blocks, threads, smem, st>>>(a); break;
-    case 8: tsu::align_kernel<kCigar, kMode, 8><<<blocks, threads, smem, st>>>(a); break;
-    case 16: tsu::align_kernel<kCigar, kMode, 16><<<blocks, threads, smem, st>>>(a); break;
-    case 32: tsu::align_kernel<kCigar, kMode, 32><<<blocks, threads, smem, st>>>(a); break;
-    default: break;
-  }
-}
-
-void launch_align(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
-                  const tsu::AlignArgs& a) {
-  if (cigar) {
-    if (mode == tsu::kModeShared)
-      launch_gw<true, tsu::kModeShared>(gw, blocks, threads, smem, st, a);
-    else
-      launch_gw<true, tsu::kModeGlobal>(gw, blocks, threads, smem, st, a);
-  } else {
-    if (mode == tsu::kModeShared)
-      launch_gw<false, tsu::kModeShared>(gw, blocks, threads, smem, st, a);
-    else
-      launch_gw<false, tsu::kModeGlobal>(gw, blocks, threads, smem, st, a);
-  }
+void launch_align(const tsu_ctx* ctx, bool cigar, int mode, int gw, int blocks, int threads, size_t smem,
+                  cudaStream_t st, const tsu::AlignArgs& a) {
+  if (ctx->rp.dual())
+    tsu::launch_align_dual(cigar, mode, gw, blocks, threads, smem, st, a);
+  else
+    tsu::launch_detail::launch<false>(cigar, mode, gw, blocks, threads, smem, st, a);
 }
 
 // Scratch bytes of one group of a pass (ring, history, step table).
@@ -350,13 +304,13 @@ size_t group_scratch_bytes(const tsu::PassGeom& g) {
 int plan_pass_within(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint,
                      bool want_cigar, size_t avail, Pass* out) {
   Pass p;
-  const tsu::PassGeom g = tsu::plan_geometry(ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, bi.max_m, bi.max_n, pc.mode,
+  const tsu::PassGeom g = tsu::plan_geometry(ctx->rp, bi.max_m, bi.max_n, pc.mode,
                                              pc.gw, hint, want_cigar, ctx->smem_optin);
   p.g = g;
   const int gpc = g.groups_per_cta;
   int occ = 0;
   cudaError_t e =
-      align_occupancy(want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, ctx->smem_optin, &occ);
+      align_occupancy(ctx, want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, ctx->smem_optin, &occ);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
   int64_t warps = (int64_t)ctx->sms * occ * gpc;  // groups
   const size_t per_warp = group_scratch_bytes(g);
@@ -557,10 +511,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   // and retry count of band slot b
   constexpr size_t kCounterBytes = 64 + 8 * tsu::kBands;
   if ((rc = grow(ctx, ctx->b_counters, kCounterBytes))) return rc;
-  const int min_pen = std::min(ctx->x, ctx->go);
+  const int min_pen = ctx->rp.min_pen();
   int64_t arena_cap = 0;
   if (want_cigar) {
-    arena_cap = tsu::arena_runs(ctx->x, ctx->go, n, bi.max_m, bi.max_n, ctx->err_hint);
+    arena_cap = tsu::arena_runs(ctx->rp, n, bi.max_m, bi.max_n, ctx->err_hint);
     // the wavefront scratch of an earlier call is regrown for this call's
     // passes anyway: drop it rather than let it shrink the arena
     if (ctx->held() + sizeof(uint32_t) * (size_t)arena_cap > ctx->budget) release(ctx, ctx->b_scratch);
@@ -637,8 +591,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       r.slot = (int)k;
       r.hint = ctx->err_hint;
       if (ctx->fit_start && !ctx->one_warp)
-        r.pc = tsu::fit_start(r.pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, r.bi.max_m, r.bi.max_n, r.hint,
-                              ctx->smem_optin);
+        r.pc = tsu::fit_start(r.pc, ctx->rp, r.bi.max_m, r.bi.max_n, r.hint, ctx->smem_optin);
       if ((rc = plan_pass_within(ctx, r.bi, r.n, r.pc, r.hint, want_cigar, avail, &r.ps))) return rc;
       need = std::max(need, scratch_bytes(r.ps, want_cigar));
     }
@@ -657,12 +610,8 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.pk = pk;
     a.order = order;
     a.n_order = n_order;
-    a.x = ctx->x;
-    a.go = ctx->go;
-    a.ge = ctx->ge;
+    a.pen = ctx->rp;
     a.g = ctx->g;
-    a.rm = ctx->rm;
-    a.re = ctx->re;
     a.ring_w = ps.g.ring_w;
     a.seq_cap = ps.g.seq_cap;
     carve_scratch(ctx, ps, want_cigar, &a);
@@ -709,7 +658,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       const tsu::AlignArgs a = align_args(r.ps, all_pairs ? nullptr : P<int32_t>(ctx->b_order) + r.off, r.n, r.slot,
                                           P<int32_t>(ctx->b_retry) + r.off);
       CU(record(ctx, ctx->bev[2 * r.slot], st));
-      launch_align(want_cigar, r.ps.g.mode, r.ps.g.gw, r.ps.blocks, r.ps.threads, r.ps.smem_bytes, st, a);
+      launch_align(ctx, want_cigar, r.ps.g.mode, r.ps.g.gw, r.ps.blocks, r.ps.threads, r.ps.smem_bytes, st, a);
       CU(cudaGetLastError());
       CU(record(ctx, ctx->bev[2 * r.slot + 1], st));
     }
@@ -770,7 +719,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       CU(cudaMemcpyAsync(d_order, ctx->h_list.p, sizeof(int32_t) * nretry, cudaMemcpyHostToDevice, st));
       hint = tsu::next_hint(hint, last_mode == tsu::kModeGlobal);
       pc = ctx->one_warp ? tsu::PassChoice{tsu::kModeGlobal, 1}
-                         : tsu::next_pass(pc, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, ctx->smem_optin);
+                         : tsu::next_pass(pc, ctx->rp, pbi.max_m, pbi.max_n, ctx->smem_optin);
       if (want_cigar) {
         unsigned long long* h_used = reinterpret_cast<unsigned long long*>(h_cnt + 16);
         CU(cudaMemcpyAsync(h_used, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
@@ -778,7 +727,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
         const unsigned long long used = *h_used;
         const int64_t maxlen = std::max(pbi.max_m, pbi.max_n);
         const int64_t need =
-            (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->x, ctx->go, maxlen, hint) / min_pen + 1);
+            (int64_t)used + (int64_t)nretry * (2 * tsu::hint_score(ctx->rp, maxlen, hint) / min_pen + 1);
         if (need > arena_cap) {
           // keep the runs written so far: grow by copy
           DevBuf nb;
@@ -810,7 +759,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       CU(cudaMemsetAsync(d_slot, 0, 8, st));  // queue head + retry count
       const tsu::AlignArgs a = align_args(ps, d_order, nretry, r.slot, d_retry);
       CU(cudaEventRecord(ctx->pev[0], st));
-      launch_align(want_cigar, ps.g.mode, ps.g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
+      launch_align(ctx, want_cigar, ps.g.mode, ps.g.gw, ps.blocks, ps.threads, ps.smem_bytes, st, a);
       ctx->timing.kernel_launches++;
       CU(cudaGetLastError());
       CU(cudaEventRecord(ctx->pev[1], st));
@@ -883,7 +832,7 @@ int check_batch_host(tsu_ctx* ctx, const tsu_batch* b, BatchInfo* bi, int64_t* p
   int32_t mm = 0, mn = 0;
   for (int64_t i = 0; i < b->num_pairs; ++i) {
     const int32_t m = b->pattern_len[i], n = b->text_len[i];
-    if (m < 0 || n < 0 || m > (1 << 26) || n > (1 << 26) || b->pattern_off[i] < 0 || b->text_off[i] < 0)
+    if (m < 0 || n < 0 || m > max_len(ctx) || n > max_len(ctx) || b->pattern_off[i] < 0 || b->text_off[i] < 0)
       return set_err(ctx, TSU_EINVAL, "pair %lld: bad length/offset", (long long)i);
     pe = std::max(pe, b->pattern_off[i] + m);
     te = std::max(te, b->text_off[i] + n);
@@ -954,7 +903,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
                3 * r(4 * (size_t)nc) + r(64);
     size_t tmp = scan_tmp(2 * nc);
     if (want_cigar) {
-      const int64_t arena = std::max<int64_t>(tsu::arena_runs(ctx->x, ctx->go, nc, ci.max_m, ci.max_n, hint), 1024);
+      const int64_t arena = std::max<int64_t>(tsu::arena_runs(ctx->rp, nc, ci.max_m, ci.max_n, hint), 1024);
       const int64_t out_runs = std::min<int64_t>(arena, len_sum + 1);
       f += r(4 * (size_t)arena) + r(8 * (size_t)(nc + 1)) + (K > 1 ? 2 : 1) * r(4 * (size_t)out_runs);
       tmp = std::max(tmp, scan_tmp(nc + 1));
@@ -982,7 +931,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
         pc = tsu::band_start_in(ctx->band_start, band, std::max(pbi.max_m, pbi.max_n));
       }
       if (ctx->fit_start && !one_warp)
-        pc = tsu::fit_start(pc, ctx->x, ctx->go, ctx->ge, ctx->rm, ctx->re, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
+        pc = tsu::fit_start(pc, ctx->rp, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
       Pass ps;
       const int rc = plan_pass_within(ctx, pbi, np, pc, hint, want_cigar, SIZE_MAX / 4, &ps);
       if (rc) return rc;
@@ -997,22 +946,17 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
   return TSU_OK;
 }
 
-int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out) {
+int create(const tsu_penalties2* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out) {
   tsu_ctx* ctx = nullptr;
   if (!pen || !out) return TSU_EINVAL;
   *out = nullptr;
-  if (pen->mismatch <= 0 || pen->gap_opening < 0 || pen->gap_extension <= 0 || pen->mismatch > 1 << 20 ||
-      pen->gap_opening > 1 << 20 || pen->gap_extension > 1 << 20)
-    return TSU_EINVAL;
+  if (!valid_penalties(pen)) return TSU_EINVAL;
+  const bool dual = pen->gap_opening2 >= 0 && pen->gap_extension2 > 0;
   ctx = new tsu_ctx();
   ctx->pen = *pen;
-  ctx->g = gcd(gcd(pen->mismatch, pen->gap_opening), pen->gap_extension);
-  ctx->x = pen->mismatch / ctx->g;
-  ctx->go = (pen->gap_opening + pen->gap_extension) / ctx->g;
-  ctx->ge = pen->gap_extension / ctx->g;
-  ctx->rm = std::max(ctx->x, ctx->go) + 1;
-  ctx->re = ctx->ge + 1;
-  if (tsu::ring_slots(ctx->rm, ctx->re) > 4096) {
+  ctx->rp = tsu::reduce_penalties(pen->mismatch, pen->gap_opening, pen->gap_extension, dual ? pen->gap_opening2 : -1,
+                                  dual ? pen->gap_extension2 : 0, &ctx->g);
+  if (ctx->rp.slots() > 4096) {
     delete ctx;
     return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
   }
@@ -1144,6 +1088,13 @@ const char* tsu_last_error(const tsu_ctx* ctx) { return ctx ? ctx->err.c_str() :
 const char* tsu_pass_log(const tsu_ctx* ctx) { return ctx ? ctx->passlog.c_str() : ""; }
 
 int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
+  if (!pen || !out) return TSU_EINVAL;
+  const tsu_penalties2 p2 = tsu::engine::one_piece(*pen);
+  return tsu::engine::create(&p2, cfg, false, out);
+}
+
+int tsu_create_dual(const tsu_penalties2* pen, const tsu_config* cfg, tsu_ctx** out) {
+  if (!pen || !out || pen->gap_opening2 < 0 || pen->gap_extension2 <= 0) return TSU_EINVAL;
   return tsu::engine::create(pen, cfg, false, out);
 }
 
@@ -1376,7 +1327,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
       CU(wait_stream(ctx, st));
     }
     for (int64_t i = 0; i < n; ++i) {
-      if (pl[(size_t)i] < 0 || tl[(size_t)i] < 0 || pl[(size_t)i] > (1 << 26) || tl[(size_t)i] > (1 << 26))
+      if (pl[(size_t)i] < 0 || tl[(size_t)i] < 0 || pl[(size_t)i] > max_len(ctx) || tl[(size_t)i] > max_len(ctx))
         return set_err(ctx, TSU_EINVAL, "pair %lld: bad length", (long long)i);
       bi.max_m = std::max(bi.max_m, pl[(size_t)i]);
       bi.max_n = std::max(bi.max_n, tl[(size_t)i]);

@@ -15,7 +15,11 @@ namespace engine {
 // limited number of hardware queues (CUDA_DEVICE_MAX_CONNECTIONS) that
 // streams share in turn; work queued behind a long kernel on a shared queue
 // waits for it, so contexts of many host threads use one stream each.
-int create(const tsu_penalties* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out);
+// pen->gap_opening2 < 0: one gap piece.
+int create(const tsu_penalties2* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out);
+inline tsu_penalties2 one_piece(const tsu_penalties& p) {
+  return tsu_penalties2{p.mismatch, p.gap_opening, p.gap_extension, -1, 0};
+}
 
 // Lengths of the pairs of a planned batch (host memory).
 struct BatchShape {

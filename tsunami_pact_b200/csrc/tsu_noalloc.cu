@@ -98,15 +98,6 @@ __global__ void noalloc_count_bad_kernel(int64_t n, const int32_t* __restrict__ 
 
 size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-int gcd(int a, int b) {
-  while (b) {
-    const int t = a % b;
-    a = b;
-    b = t;
-  }
-  return a;
-}
-
 // The kernel's dynamic shared memory limit is set to the device maximum, the
 // value the engine's contexts set too, so concurrent callers never lower it
 // under each other's launches.
@@ -198,18 +189,16 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
 
   // align passes: shared-memory ring first, then a global ring for the pairs
   // it hands back (score only: no history, no step table, no arena)
-  const int g = gcd(gcd(pen->mismatch, pen->gap_opening), pen->gap_extension);
-  const int x = pen->mismatch / g, go = (pen->gap_opening + pen->gap_extension) / g, ge = pen->gap_extension / g;
-  const int rm = std::max(x, go) + 1, re = ge + 1;
-  if (tsu::ring_slots(rm, re) > 4096) return TSU_EINVAL;
+  int g = 1;
+  const tsu::Pen rp = tsu::reduce_penalties(pen->mismatch, pen->gap_opening, pen->gap_extension, -1, 0, &g);
+  if (rp.slots() > 4096) return TSU_EINVAL;
   unsigned int* queue = reinterpret_cast<unsigned int*>(hdr + kHdrQueue);
   const int32_t* ord = nullptr;
   int64_t n_order = n;
   for (int pass = 0; pass < 2; ++pass) {
     const int wpb = 4;
-    const tsu::PassGeom geo = tsu::plan_geometry(x, go, ge, rm, re, max_m, max_n,
-                                                 pass == 0 ? tsu::kModeShared : tsu::kModeGlobal, 1, 0.2, false,
-                                                 smem_optin);
+    const tsu::PassGeom geo = tsu::plan_geometry(rp, max_m, max_n, pass == 0 ? tsu::kModeShared : tsu::kModeGlobal,
+                                                 1, 0.2, false, smem_optin);
     int occ = 0;
     NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ)
                                        : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ));
@@ -225,12 +214,8 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
     a.pk = pk;
     a.order = ord;
     a.n_order = n_order;
-    a.x = x;
-    a.go = go;
-    a.ge = ge;
+    a.pen = rp;
     a.g = g;
-    a.rm = rm;
-    a.re = re;
     a.ring_w = geo.ring_w;
     a.seq_cap = geo.seq_cap;
     a.ring_global = geo.mode == tsu::kModeGlobal ? reinterpret_cast<int32_t*>(ring_base) : nullptr;

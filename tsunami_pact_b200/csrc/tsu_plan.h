@@ -40,8 +40,8 @@ constexpr int kSharedMaxLen = 32000;   // int16 ring limit
 constexpr int kSmemPerSM = 228 * 1024; // B200 shared memory per SM (bytes)
 
 // Reduced-unit score expected at edit rate `hint` for a pair of length L.
-inline int64_t hint_score(int x, int go, int64_t L, double hint) {
-  return (int64_t)(hint * (double)L * (double)std::max(x, go)) + 16;
+inline int64_t hint_score(const Pen& pen, int64_t L, double hint) {
+  return (int64_t)(hint * (double)L * (double)pen.max_pen()) + 16;
 }
 
 inline int cta_threads_for(int gw) { return gw <= 4 ? 128 : 32 * gw; }
@@ -51,25 +51,26 @@ inline int min_blocks_for(int mode, int gw) {
 
 // Ring width a shared-mode group of gw warps can hold with seq_cap staged
 // words, at the block count the kernel is compiled for.
-inline int shared_ring_width(int rm, int re, int gw, int seq_cap, int smem_optin) {
-  const int ns = ring_slots(rm, re);
+inline int shared_ring_width(const Pen& pen, int gw, int seq_cap, int smem_optin) {
+  const int ns = pen.slots();
   const int blocks = min_blocks_for(kModeShared, gw);
   const int per_cta = std::min(smem_optin, kSmemPerSM / blocks - 1024);
   const int gpc = cta_threads_for(gw) / (32 * gw);
   const int per_group = per_cta / gpc;
-  const int fixed = group_smem_bytes(rm, re, 0, kModeShared, seq_cap, gw) + 16;
+  const int fixed = group_smem_bytes(pen, 0, kModeShared, seq_cap, gw) + 16;
   const int w = (per_group - fixed) / (2 * ns);
   return std::max(0, w & ~15);
 }
 
 // mode/gw: the configuration of this pass.  Shared mode needs lengths within
 // the int16 ring; otherwise the pass falls back to the global ring.
-inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max_m, int32_t max_n, int mode, int gw,
-                              double hint, bool want_cigar, int smem_optin) {
+inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int mode, int gw, double hint,
+                              bool want_cigar, int smem_optin) {
   PassGeom p;
-  const int ns = ring_slots(rm, re);
+  const int ns = pen.slots();
+  const int ge = pen.min_ge();
   const int64_t maxlen = std::max(max_m, max_n);
-  const int64_t s_hint = hint_score(x, go, maxlen, hint);
+  const int64_t s_hint = hint_score(pen, maxlen, hint);
   const int64_t full_w = (int64_t)max_m + max_n + 3;
   const int64_t width_hint = std::min<int64_t>(full_w, 2 * s_hint / ge + 3);
   p.gw = gw;
@@ -79,7 +80,7 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
   if (p.mode == kModeShared) {
     const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
     p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
-    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(rm, re, gw, p.seq_cap, smem_optin);
+    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(pen, gw, p.seq_cap, smem_optin);
     p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, cap) + 15) & ~15);
     if (cap < 64) p.mode = kModeGlobal;
   }
@@ -88,7 +89,7 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
     p.seq_cap = 0;
   }
   p.min_blocks = min_blocks_for(p.mode, gw);
-  p.group_smem = group_smem_bytes(rm, re, p.ring_w, p.mode, p.seq_cap, gw);
+  p.group_smem = group_smem_bytes(pen, p.ring_w, p.mode, p.seq_cap, gw);
   // Backtrace words up to score s: sum_j (2j/ge + 1) ~= s^2/ge + 2s.
   p.table_cap = want_cigar ? (int)std::min<int64_t>(s_hint + 1, INT32_MAX / 2) : 0;
   if (want_cigar) {
@@ -106,7 +107,7 @@ inline PassGeom plan_geometry(int x, int go, int ge, int rm, int re, int32_t max
 // global_gw (16) warps per pair (the pairs that reach it are the longest and
 // most divergent ones; their count in flight is bounded by memory, not by
 // warps).
-inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int32_t max_n, int smem_optin,
+inline PassChoice next_pass(PassChoice prev, const Pen& pen, int32_t max_m, int32_t max_n, int smem_optin,
                             int global_gw = 16) {
   const int64_t need_w = (int64_t)max_m + max_n + 3;
   if (prev.mode == kModeShared && std::max(max_m, max_n) <= kSharedMaxLen) {
@@ -115,7 +116,7 @@ inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int3
     static const int kGW[] = {2, 4, 8, 16};
     for (int gw : kGW) {
       if (gw <= prev.gw) continue;
-      if (shared_ring_width(rm, re, gw, (int)seqw, smem_optin) >= need_w) return {kModeShared, gw};
+      if (shared_ring_width(pen, gw, (int)seqw, smem_optin) >= need_w) return {kModeShared, gw};
     }
     if (prev.gw < 16) return {kModeShared, 16};
   }
@@ -128,10 +129,11 @@ inline PassChoice next_pass(PassChoice prev, int rm, int re, int32_t max_m, int3
 // global ring with 8 or more warps.  Used when the hint is a per-pair
 // estimate, so a pair that is bound to outgrow the shared ring does not
 // start there; a wavefront wider than 16,384 diagonals gets 32 warps.
-inline PassChoice fit_start(PassChoice pc, int x, int go, int ge, int rm, int re, int32_t max_m, int32_t max_n,
-                            double hint, int smem_optin) {
+inline PassChoice fit_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_t max_n, double hint,
+                            int smem_optin) {
   const int64_t maxlen = std::max(max_m, max_n);
-  const int64_t w = std::min<int64_t>((int64_t)max_m + max_n + 3, 2 * hint_score(x, go, maxlen, hint) / ge + 3);
+  const int64_t w =
+      std::min<int64_t>((int64_t)max_m + max_n + 3, 2 * hint_score(pen, maxlen, hint) / pen.min_ge() + 3);
   if (pc.mode != kModeShared) return {kModeGlobal, w > 16384 ? 32 : pc.gw};
   if (maxlen > kSharedMaxLen) return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
   const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
@@ -139,7 +141,7 @@ inline PassChoice fit_start(PassChoice pc, int x, int go, int ge, int rm, int re
   for (int gw : kGW) {
     if (gw < pc.gw) continue;
     if (seqw > (gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN)) continue;
-    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(rm, re, gw, (int)seqw, smem_optin);
+    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(pen, gw, (int)seqw, smem_optin);
     if (cap >= w) return {kModeShared, gw};
   }
   // wavefronts wider than 16,384 diagonals: 32 warps (one 1024-thread block)
@@ -179,10 +181,10 @@ inline PassChoice band_start(int band, int32_t maxlen) { return band_start_in(ba
 constexpr double kHintCeiling = 2.0;
 inline double next_hint(double hint, bool grow) { return grow ? std::min(hint * 4.0, kHintCeiling) : hint; }
 
-// CIGAR arena runs for a batch: 2*s/min(x, go) + 1 per pair at the hint.
-inline int64_t arena_runs(int x, int go, int64_t n, int32_t max_m, int32_t max_n, double hint) {
+// CIGAR arena runs for a batch: 2*s/(cheapest edit) + 1 per pair at the hint.
+inline int64_t arena_runs(const Pen& pen, int64_t n, int32_t max_m, int32_t max_n, double hint) {
   const int64_t maxlen = std::max(max_m, max_n);
-  const int64_t per_pair = 2 * hint_score(x, go, maxlen, hint) / std::min(x, go) + 1;
+  const int64_t per_pair = 2 * hint_score(pen, maxlen, hint) / pen.min_pen() + 1;
   return std::max<int64_t>(n * std::min<int64_t>(per_pair, (int64_t)max_m + max_n + 1), 1024);
 }
 

@@ -145,7 +145,7 @@ class EngineExecutor final : public tsu::serve::Executor {
   HostStage in_, out_;
 };
 
-int make_ctx(const tsu_penalties* pen, int device, double hint, size_t budget, tsu_ctx** out) {
+int make_ctx(const tsu_penalties2* pen, int device, double hint, size_t budget, tsu_ctx** out) {
   tsu_config c{};
   c.device = device;
   c.mem_budget = budget;
@@ -160,10 +160,9 @@ struct tsu_server {
   std::string err;
 };
 
-extern "C" {
+namespace {
 
-int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, tsu_server** out) {
-  if (!pen || !out) return TSU_EINVAL;
+int server_create(const tsu_penalties2* pen, const tsu_server_config* cfg, tsu_server** out) {
   *out = nullptr;
   tsu_server_config c{};
   if (cfg) c = *cfg;
@@ -203,6 +202,21 @@ int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, ts
   srv->s = std::make_unique<tsu::serve::Server>(sc, std::move(ws), std::move(plan));
   *out = srv;
   return TSU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, tsu_server** out) {
+  if (!pen || !out) return TSU_EINVAL;
+  const tsu_penalties2 p2 = tsu::engine::one_piece(*pen);
+  return server_create(&p2, cfg, out);
+}
+
+int tsu_server_create_dual(const tsu_penalties2* pen, const tsu_server_config* cfg, tsu_server** out) {
+  if (!pen || !out || pen->gap_opening2 < 0 || pen->gap_extension2 <= 0) return TSU_EINVAL;
+  return server_create(pen, cfg, out);
 }
 
 int tsu_server_destroy(tsu_server* srv) {
