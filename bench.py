@@ -40,7 +40,18 @@ WORKLOADS = {
     "c3": [20_000, "10,000 bp, 15% edits"],
     "c4": [200_000, "lengths log-uniform 100-20,000 bp, edits uniform 1-15% per pair"],
 }
-PEN = (4, 6, 2)
+PEN = (4, 6, 2)  # --penalties; five values (open2, extend2 last): dual gap-affine
+
+
+def pen_str() -> str:
+    return "/".join(str(v) for v in PEN) + (" (dual gap-affine)" if len(PEN) == 5 else "")
+
+
+def oracle_batch(O, pbuf, poff, plen, tbuf, toff, tlen, threads):
+    """The oracle over the bench's penalties (one or two gap pieces)."""
+    if len(PEN) == 5:
+        return O.align_batch2_arrays(pbuf, poff, plen, tbuf, toff, tlen, *PEN, cigar=True, threads=threads)
+    return O.align_batch_arrays(pbuf, poff, plen, tbuf, toff, tlen, *PEN, cigar=True, threads=threads)
 
 
 def dist_env():
@@ -142,14 +153,12 @@ def cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen, target_s=15.0):
     n = len(plen)
     probe = min(n, max(256, cores * 64))
     t0 = time.perf_counter()
-    O.align_batch_arrays(pbuf, poff[:probe], plen[:probe], tbuf, toff[:probe], tlen[:probe], *PEN, cigar=True,
-                         threads=cores)
+    oracle_batch(O, pbuf, poff[:probe], plen[:probe], tbuf, toff[:probe], tlen[:probe], cores)
     dt = time.perf_counter() - t0
     rate = probe / max(dt, 1e-6)
     sample = int(min(n, max(probe, rate * target_s)))
     t0 = time.perf_counter()
-    O.align_batch_arrays(pbuf, poff[:sample], plen[:sample], tbuf, toff[:sample], tlen[:sample], *PEN, cigar=True,
-                         threads=cores)
+    oracle_batch(O, pbuf, poff[:sample], plen[:sample], tbuf, toff[:sample], tlen[:sample], cores)
     dt = time.perf_counter() - t0
     cells = float(np.sum(plen[:sample].astype(np.float64) * tlen[:sample]))
     return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": "port",
@@ -172,8 +181,9 @@ def run_serving(args):
 
     rates = [float(x) for x in args.rates.split(",") if x]
     budget = int(args.budget_gb * (1 << 30))
-    srv = T.Server(*PEN, workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2,
-                   estimate_hint=not args.no_estimate)
+    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
+    srv = T.Server(*PEN[:3], workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2,
+                   estimate_hint=not args.no_estimate, **dual_kw)
 
     def stream(index, n_req, rate):
         arrivals, sizes = D.c5_stream(n_req, rate if rate > 0 else 1.0, index=index)
@@ -231,7 +241,7 @@ def run_serving(args):
             "metric": "pairs/s (serving)", "value": st["pairs_completed"] / wall, "unit": "pairs/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "int32", "data": "synthetic",
             "config": {"workload": "c5 serving: Poisson arrivals, requests of U{1..256} pairs, mixture 70% 150 bp "
-                                   "@1-3%, 25% 1-5 kbp @5-10%, 5% 10-50 kbp @10-20%, penalties 4/6/2",
+                                   "@1-3%, 25% 1-5 kbp @5-10%, 5% 10-50 kbp @10-20%, penalties " + pen_str(),
                        "offered_rate_rps": rate, "requests": len(reqs), "pairs": int(sizes.sum()),
                        "workers": args.workers, "budget_gb": st["budget_bytes"] / 2**30,
                        "long_pair_memory": "max_error_hint" if args.no_estimate else "k-mer estimate"},
@@ -265,18 +275,18 @@ def run_reference(args, workload):
     probe = max(256, cores * 64)
     pb, po, pl, tb, to, tl = datasets.generate(workload, probe)
     t0 = time.perf_counter()
-    O.align_batch_arrays(pb, po, pl, tb, to, tl, *PEN, cigar=True, threads=cores)
+    oracle_batch(O, pb, po, pl, tb, to, tl, cores)
     r = probe / max(time.perf_counter() - t0, 1e-6)
     sample = int(min(n_all, max(probe, r * 6.0)))
     pb, po, pl, tb, to, tl = datasets.generate(workload, sample)
     cells = float(np.sum(pl.astype(np.float64) * tl))
     for _ in range(args.warmup):
-        O.align_batch_arrays(pb, po[: min(sample, probe)], pl[: min(sample, probe)], tb, to[: min(sample, probe)],
-                             tl[: min(sample, probe)], *PEN, cigar=True, threads=cores)
+        k = min(sample, probe)
+        oracle_batch(O, pb, po[:k], pl[:k], tb, to[:k], tl[:k], cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.align_batch_arrays(pb, po, pl, tb, to, tl, *PEN, cigar=True, threads=cores)
+        oracle_batch(O, pb, po, pl, tb, to, tl, cores)
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
     gcups = cells / t / 1e9
@@ -285,7 +295,7 @@ def run_reference(args, workload):
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
         "impl": "reference",
-        "config": {"workload": f"{workload}: {n_all} pairs, {desc}, penalties 4/6/2", "sample_pairs": sample},
+        "config": {"workload": f"{workload}: {n_all} pairs, {desc}, penalties {pen_str()}", "sample_pairs": sample},
         "pairs_per_s": sample / t,
         "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": cores, "kind": "port",
                          "sample": f"first {sample} pairs of the workload per step, scores + CIGARs, "
@@ -314,7 +324,13 @@ def main():
     ap.add_argument("--workers", type=int, default=32, help="c5: server workers")
     ap.add_argument("--no-estimate", action="store_true", help="c5: size long pairs by --hint, not by estimate")
     ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
+    ap.add_argument("--penalties", default="4,6,2",
+                    help="mismatch,open,extend[,open2,extend2]: five values align with dual gap-affine penalties")
     args = ap.parse_args()
+    global PEN
+    PEN = tuple(int(v) for v in args.penalties.split(","))
+    if len(PEN) not in (3, 5):
+        raise SystemExit("--penalties takes 3 or 5 values")
     if args.workload == "c5":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "no serving path in the reference"}))
@@ -355,7 +371,8 @@ def main():
     pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank, world)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
-    al = T.Aligner(*PEN, device=local, max_error_hint=args.hint)
+    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
+    al = T.Aligner(*PEN[:3], device=local, max_error_hint=args.hint, **dual_kw)
 
     # ---- value: batch resident in HBM ----------------------------------
     dev = torch.device("cuda", local)
@@ -488,7 +505,7 @@ def main():
     hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
     algo = packed_in + out_bytes + hist_bytes
     achieved = algo / (a_ms / 1e3) / 1e9
-    prof = load_traffic(f"align_{workload}") if want_cigar else None
+    prof = load_traffic(f"align_{workload}" + ("_dual" if len(PEN) == 5 else "")) if want_cigar else None
     traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
@@ -510,7 +527,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded, uniform ACGT, equal sub/ins/del edits)",
-            "config": {"workload": f"{workload}: {n_pairs} pairs per GPU, {desc}, penalties 4/6/2",
+            "config": {"workload": f"{workload}: {n_pairs} pairs per GPU, {desc}, penalties {pen_str()}",
                        "output": "scores + CIGARs" if want_cigar else "scores only",
                        "l2": f"inputs larger than L2 ({(pbuf.nbytes + tbuf.nbytes) / 1e9:.1f} GB ASCII per GPU)",
                        "parallelism": f"data-parallel over pairs, {world} GPU(s)"},

@@ -53,12 +53,18 @@ struct Pen {
   int rm = 0, re = 0, re2 = 0;
   __host__ __device__ bool dual() const { return re2 > 0; }
   __host__ __device__ int slots() const { return rm + 2 * re + 2 * re2; }
-  // cheapest and dearest single edit, smallest extension
+  // cheapest and dearest single-base edit (a one-base gap costs
+  // min(go, go2)), smallest extension
   __host__ __device__ int min_pen() const {
     const int a = x < go ? x : go;
     return dual() && go2 < a ? go2 : a;
   }
   __host__ __device__ int max_pen() const {
+    const int g1 = dual() && go2 < go ? go2 : go;
+    return x > g1 ? x : g1;
+  }
+  // deepest M source: max(x, go, go2) scores back
+  __host__ __device__ int ring_depth() const {
     const int a = x > go ? x : go;
     return dual() && go2 > a ? go2 : a;
   }
@@ -97,7 +103,7 @@ inline Pen reduce_penalties(int mismatch, int open, int ext, int open2, int ext2
   }
   p.re = p.ge + 1;
   p.re2 = dual ? p.ge2 + 1 : 0;
-  p.rm = p.max_pen() + 1;
+  p.rm = p.ring_depth() + 1;
   if (g) *g = u;
   return p;
 }

@@ -961,7 +961,7 @@ int create(const tsu_penalties2* pen, const tsu_config* cfg, bool single_stream,
     return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
   }
   ctx->device = cfg ? cfg->device : 0;
-  for (int b = 0; b < tsu::kBands; ++b) ctx->band_start[b] = tsu::band_start_table()[b];
+  for (int b = 0; b < tsu::kBands; ++b) ctx->band_start[b] = tsu::band_start_table(ctx->rp.dual())[b];
   ctx->err_hint = (cfg && cfg->max_error_hint > 0) ? cfg->max_error_hint : 0.2;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) {

@@ -11,6 +11,7 @@
 
 #include "tsu_common.cuh"
 #include "tsu_tuning.h"
+#include "tsu_tuning_dual.h"
 
 namespace tsu {
 
@@ -150,7 +151,8 @@ inline PassChoice fit_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_
 
 // Length bands of the batched scheduler: max(m, n) < 1024, < 2048, < 4096,
 // < 8192, < 16384, >= 16384.  Each band starts its ladder at the rung the
-// autotuner measured fastest for it (tsu_tuning.h).
+// autotuner measured fastest for it (tsu_tuning.h; the dual gap-affine
+// kernels, with their deeper and wider rings: tsu_tuning_dual.h).
 constexpr int kBands = 6;
 inline int length_band(int32_t L) {
   if (L < 1024) return 0;
@@ -167,17 +169,18 @@ inline PassChoice band_start_in(const PassChoice* table, int band, int32_t maxle
   if (r.mode == kModeShared && maxlen > kSharedMaxLen) r = {kModeGlobal, r.gw >= 8 ? r.gw : 8};
   return r;
 }
-inline const PassChoice* band_start_table() {
+inline const PassChoice* band_start_table(bool dual = false) {
   static const PassChoice kStart[kBands] = TSU_BAND_START;
-  return kStart;
+  static const PassChoice kStartDual[kBands] = TSU_BAND_START_DUAL;
+  return dual ? kStartDual : kStart;
 }
-inline PassChoice band_start(int band, int32_t maxlen) { return band_start_in(band_start_table(), band, maxlen); }
 
 // Edit-rate hint of the next retry pass.  Shared-ring passes keep the hint
 // (they fail on ring width, staging or history); from the second global pass
 // on it grows 4x up to kHintCeiling, at which the step table and the history
-// cover the score bound of every pair (s_max <= max(x, o+e) * maxlen + o+e <
-// s_hint), so a pass there can fail only on memory.
+// cover the score bound of every pair (s_max <= max_pen * maxlen < s_hint,
+// max_pen the dearest single-base edit), so a pass there can fail only on
+// memory.
 constexpr double kHintCeiling = 2.0;
 inline double next_hint(double hint, bool grow) { return grow ? std::min(hint * 4.0, kHintCeiling) : hint; }
 

@@ -17,10 +17,14 @@ it, whose weight depends on how many pairs share the band.
 
 It writes the table as a C header (tsunami_pact_b200/csrc/tsu_tuning.h by
 default; rebuild the library afterwards) and every measurement as JSON.
+With five --penalties (mismatch, open, extend, open2, extend2) it tunes the
+dual gap-affine kernels instead and writes their table, TSU_BAND_START_DUAL,
+to tsu_tuning_dual.h: their wavefront ring is deeper (M back to s - o2 - e2)
+and, with a small e2, wider, so they start at other rungs.
 
 usage: python -m tsunami_pact_b200.tune [--out-header PATH] [--out-json PATH]
                                          [--workloads c2:200000,c4:100000,c3:5000]
-                                         [--reps N] [--device D]
+                                         [--reps N] [--device D] [--penalties 4,6,2]
 """
 from __future__ import annotations
 
@@ -69,11 +73,16 @@ def band_batches(workloads: str):
     return out
 
 
-def render_header(table, source: str, times=None) -> str:
-    """tsu_tuning.h for a table [(mode, warps)] * 6; times[band][rung] in ms
-    become a comment."""
+def header_macro(dual: bool) -> str:
+    return "TSU_BAND_START_DUAL" if dual else "TSU_BAND_START"
+
+
+def render_header(table, source: str, times=None, dual: bool = False) -> str:
+    """tsu_tuning.h (tsu_tuning_dual.h) for a table [(mode, warps)] * 6;
+    times[band][rung] in ms become a comment."""
     lines = [
-        "// tsu_tuning.h -- starting rung of the pass ladder per length band.",
+        "// %s -- starting rung of the pass ladder per length band%s." % (
+            "tsu_tuning_dual.h" if dual else "tsu_tuning.h", " (dual gap-affine kernels)" if dual else ""),
         "// Written by tsunami_pact_b200/tune.py (the autotuner); rebuild the library after changing it.",
         "// band: max(m, n) < 1024, < 2048, < 4096, < 8192, < 16384, >= 16384",
         "// rung: {ring mode (0 shared, 1 global), warps per pair}",
@@ -85,20 +94,20 @@ def render_header(table, source: str, times=None) -> str:
             lines.append("//   band %d (%s): %s" % (b, BAND_NAMES[b], cells))
     lines += [
         "#pragma once",
-        '#define TSU_TUNING_SOURCE "%s"' % source,
-        "#define TSU_BAND_START {" + ", ".join("{%d, %d}" % (m, w) for m, w in table) + "}",
+        '#define %s "%s"' % ("TSU_TUNING_DUAL_SOURCE" if dual else "TSU_TUNING_SOURCE", source),
+        "#define %s {" % header_macro(dual) + ", ".join("{%d, %d}" % (m, w) for m, w in table) + "}",
         "",
     ]
     return "\n".join(lines)
 
 
-def parse_header(text: str):
-    """The table of a tsu_tuning.h: [(mode, warps)] * 6."""
+def parse_header(text: str, dual: bool = False):
+    """The table of a tsu_tuning.h (tsu_tuning_dual.h): [(mode, warps)] * 6."""
     import re
 
-    m = re.search(r"#define TSU_BAND_START \{(.*)\}", text)
+    m = re.search(r"#define %s \{(.*)\}" % header_macro(dual), text)
     if not m:
-        raise ValueError("no TSU_BAND_START")
+        raise ValueError("no " + header_macro(dual))
     pairs = re.findall(r"\{\s*(\d+)\s*,\s*(\d+)\s*\}", m.group(1))
     return [(int(a), int(b)) for a, b in pairs]
 
@@ -112,7 +121,7 @@ def gpu_name(device: int) -> str:
         return "unknown GPU"
 
 
-def tune(workloads: str = DEFAULT_WORKLOADS, reps: int = 2, device: int = 0, log=print):
+def tune(workloads: str = DEFAULT_WORKLOADS, reps: int = 2, device: int = 0, log=print, penalties=(4, 6, 2)):
     """Returns (table, times per band {rung: ms}, one record per measurement)."""
     import ctypes
 
@@ -124,7 +133,8 @@ def tune(workloads: str = DEFAULT_WORKLOADS, reps: int = 2, device: int = 0, log
                                      ctypes.POINTER(ctypes.c_int)]
     per_band = band_batches(workloads)
     table, times, record = [], [], []
-    with Aligner(4, 6, 2, device=device) as al:
+    dual_kw = {"gap_opening2": penalties[3], "gap_extension2": penalties[4]} if len(penalties) == 5 else {}
+    with Aligner(*penalties[:3], device=device, **dual_kw) as al:
         for band in range(N_BANDS):
             if not per_band[band]:  # no pairs of this band: keep the compiled rung
                 m, w = ctypes.c_int(), ctypes.c_int()
@@ -171,17 +181,24 @@ def tune(workloads: str = DEFAULT_WORKLOADS, reps: int = 2, device: int = 0, log
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--out-header", default=os.path.join(HERE, "csrc", "tsu_tuning.h"))
+    ap.add_argument("--out-header", default="", help="default: csrc/tsu_tuning.h (csrc/tsu_tuning_dual.h)")
     ap.add_argument("--out-json", default="")
     ap.add_argument("--workloads", default=DEFAULT_WORKLOADS, help="name:pairs,... (tsunami_pact_b200/datasets.py)")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--penalties", default="4,6,2", help="mismatch,open,extend[,open2,extend2]")
     args = ap.parse_args(argv)
-    table, times, record = tune(args.workloads, args.reps, args.device)
+    pen = tuple(int(v) for v in args.penalties.split(","))
+    if len(pen) not in (3, 5):
+        raise SystemExit("--penalties takes 3 or 5 values")
+    dual = len(pen) == 5
+    out_header = args.out_header or os.path.join(HERE, "csrc", "tsu_tuning_dual.h" if dual else "tsu_tuning.h")
+    table, times, record = tune(args.workloads, args.reps, args.device, penalties=pen)
     stamp = datetime.datetime.now(datetime.timezone.utc).strftime("%Y-%m-%d")
-    source = "tune.py on %s, %s, workloads %s" % (gpu_name(args.device), stamp, args.workloads)
-    with open(args.out_header, "w") as f:
-        f.write(render_header(table, source, times))
+    source = "tune.py on %s, %s, workloads %s, penalties %s" % (gpu_name(args.device), stamp, args.workloads,
+                                                               "/".join(map(str, pen)))
+    with open(out_header, "w") as f:
+        f.write(render_header(table, source, times, dual))
     if args.out_json:
         with open(args.out_json, "w") as f:
             json.dump({"source": source, "workloads": args.workloads, "table": table, "times_ms": times,
