@@ -41,14 +41,38 @@ WORKLOADS = {
     "c4": [200_000, "lengths log-uniform 100-20,000 bp, edits uniform 1-15% per pair"],
 }
 PEN = (4, 6, 2)  # --penalties; five values (open2, extend2 last): dual gap-affine
+METRIC_NAME = None  # --metric edit | indel | gap_linear (PEN then (mismatch, gap_extension))
+LINEAR_XE = {"edit": (1, 1), "indel": (3, 1)}  # the gap-linear penalties of these metrics
+
+
+def linear_xe():
+    return LINEAR_XE.get(METRIC_NAME, PEN[:2])
 
 
 def pen_str() -> str:
+    if METRIC_NAME in LINEAR_XE:
+        return METRIC_NAME + " distance"
+    if METRIC_NAME == "gap_linear":
+        return "gap-linear %d/%d" % PEN[:2]
     return "/".join(str(v) for v in PEN) + (" (dual gap-affine)" if len(PEN) == 5 else "")
 
 
+def make_aligner(T, **kw):
+    """An engine context over the bench's penalties or metric."""
+    if METRIC_NAME in LINEAR_XE:
+        return T.Aligner(metric=METRIC_NAME, **kw)
+    if METRIC_NAME == "gap_linear":
+        return T.Aligner(PEN[0], 0, PEN[1], metric="gap_linear", **kw)
+    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
+    return T.Aligner(*PEN[:3], **dual_kw, **kw)
+
+
 def oracle_batch(O, pbuf, poff, plen, tbuf, toff, tlen, threads):
-    """The oracle over the bench's penalties (one or two gap pieces)."""
+    """The oracle over the bench's penalties (one or two gap pieces, or a
+    gap-linear metric)."""
+    if METRIC_NAME is not None:
+        return O.align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, *linear_xe(), cigar=True,
+                                           threads=threads)
     if len(PEN) == 5:
         return O.align_batch2_arrays(pbuf, poff, plen, tbuf, toff, tlen, *PEN, cigar=True, threads=threads)
     return O.align_batch_arrays(pbuf, poff, plen, tbuf, toff, tlen, *PEN, cigar=True, threads=threads)
@@ -181,9 +205,13 @@ def run_serving(args):
 
     rates = [float(x) for x in args.rates.split(",") if x]
     budget = int(args.budget_gb * (1 << 30))
-    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
-    srv = T.Server(*PEN[:3], workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2,
-                   estimate_hint=not args.no_estimate, **dual_kw)
+    if METRIC_NAME:
+        pen_args, pen_kw = ((PEN[0], 0, PEN[1]) if METRIC_NAME == "gap_linear" else ()), {"metric": METRIC_NAME}
+    else:
+        pen_args = PEN[:3]
+        pen_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
+    srv = T.Server(*pen_args, workers=args.workers, mem_budget=budget, max_error_hint=args.hint or 0.2,
+                   estimate_hint=not args.no_estimate, **pen_kw)
 
     def stream(index, n_req, rate):
         arrivals, sizes = D.c5_stream(n_req, rate if rate > 0 else 1.0, index=index)
@@ -326,10 +354,17 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
     ap.add_argument("--penalties", default="4,6,2",
                     help="mismatch,open,extend[,open2,extend2]: five values align with dual gap-affine penalties")
+    ap.add_argument("--metric", default=None, choices=["edit", "indel", "gap_linear"],
+                    help="a gap-linear metric instead of gap-affine (gap_linear: --penalties mismatch,extend)")
     args = ap.parse_args()
-    global PEN
+    global PEN, METRIC_NAME
     PEN = tuple(int(v) for v in args.penalties.split(","))
-    if len(PEN) not in (3, 5):
+    METRIC_NAME = args.metric
+    if METRIC_NAME == "gap_linear" and args.penalties == "4,6,2":
+        PEN = (4, 2)
+    if METRIC_NAME == "gap_linear" and len(PEN) != 2:
+        raise SystemExit("--metric gap_linear takes --penalties mismatch,extend")
+    if METRIC_NAME is None and len(PEN) not in (3, 5):
         raise SystemExit("--penalties takes 3 or 5 values")
     if args.workload == "c5":
         if args.impl == "reference":
@@ -371,8 +406,7 @@ def main():
     pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank, world)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
-    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
-    al = T.Aligner(*PEN[:3], device=local, max_error_hint=args.hint, **dual_kw)
+    al = make_aligner(T, device=local, max_error_hint=args.hint)
 
     # ---- value: batch resident in HBM ----------------------------------
     dev = torch.device("cuda", local)
@@ -505,7 +539,8 @@ def main():
     hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
     algo = packed_in + out_bytes + hist_bytes
     achieved = algo / (a_ms / 1e3) / 1e9
-    prof = load_traffic(f"align_{workload}" + ("_dual" if len(PEN) == 5 else "")) if want_cigar else None
+    model = "_" + METRIC_NAME if METRIC_NAME else ("_dual" if len(PEN) == 5 else "")
+    prof = load_traffic(f"align_{workload}{model}") if want_cigar else None
     traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else

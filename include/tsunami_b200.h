@@ -140,6 +140,27 @@ int tsu_create(const tsu_penalties* pen, const tsu_config* cfg /* nullable */, t
 /* A context whose align calls use dual gap-affine penalties (tsu_penalties2).
  * Not available through tsu_align_scores_noalloc (one piece only). */
 int tsu_create_dual(const tsu_penalties2* pen, const tsu_config* cfg /* nullable */, tsu_ctx** out);
+
+/* Distance metrics -- WFA2-lib's distance_metric_t, which the reference sets
+ * to gap_affine for its check (wfa_gpu.cu:157).  penalties[] holds, in order:
+ *   TSU_METRIC_INDEL          none (gaps cost 1 per base; a mismatch is never
+ *                             cheaper than a deletion plus an insertion, so the
+ *                             CIGAR has no X)
+ *   TSU_METRIC_EDIT           none (Levenshtein: mismatch and gap base cost 1)
+ *   TSU_METRIC_GAP_LINEAR     mismatch, gap_extension (a gap of L costs e*L)
+ *   TSU_METRIC_GAP_AFFINE     mismatch, gap_opening, gap_extension (tsu_create)
+ *   TSU_METRIC_GAP_AFFINE_2P  mismatch, gap_opening, gap_extension,
+ *                             gap_opening2, gap_extension2 (tsu_create_dual)
+ * Indel, edit and gap-linear contexts run kernels with the M wavefront only
+ * (no I/D components); their CIGARs resolve ties mismatch > deletion >
+ * insertion. */
+#define TSU_METRIC_INDEL 0
+#define TSU_METRIC_EDIT 1
+#define TSU_METRIC_GAP_LINEAR 2
+#define TSU_METRIC_GAP_AFFINE 3
+#define TSU_METRIC_GAP_AFFINE_2P 4
+int tsu_create_metric(int metric, const int32_t* penalties /* nullable when none */, int num_penalties,
+                      const tsu_config* cfg /* nullable */, tsu_ctx** out);
 int tsu_destroy(tsu_ctx* ctx);
 const char* tsu_status_str(int status);
 const char* tsu_last_error(const tsu_ctx* ctx);
@@ -326,9 +347,12 @@ typedef struct {
 } tsu_server_stats;
 
 int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg /* nullable */, tsu_server** out);
-/* A server whose workers align with dual gap-affine penalties. */
+/* A server whose workers align with dual gap-affine penalties, or with any
+ * metric of tsu_create_metric. */
 int tsu_server_create_dual(const tsu_penalties2* pen, const tsu_server_config* cfg /* nullable */,
                            tsu_server** out);
+int tsu_server_create_metric(int metric, const int32_t* penalties, int num_penalties,
+                             const tsu_server_config* cfg /* nullable */, tsu_server** out);
 /* Queued requests are dropped; running jobs finish first. */
 int tsu_server_destroy(tsu_server* srv);
 /* flags: TSU_SCORE_ONLY or 0.  TSU_EINVAL for bad pairs, TSU_ENOMEM when the

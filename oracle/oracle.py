@@ -72,6 +72,14 @@ def lib():
         L.ora_cigar_cost2.restype = i64
         L.ora_cigar_cost2.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, c_char_p,
                                       ctypes.c_int] + [ctypes.c_int] * 5
+        L.ora_align_linear.restype = ctypes.c_int
+        L.ora_align_linear.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(OraStats)]
+        L.ora_linear_dp_score.restype = ctypes.c_int
+        L.ora_linear_dp_score.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.ora_align_batch_linear.restype = ctypes.c_int
+        L.ora_align_batch_linear.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 2 + [
+            ctypes.c_void_p] * 4 + [ctypes.c_int]
         L.ora_align_batch2.restype = ctypes.c_int
         L.ora_align_batch2.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
@@ -215,6 +223,65 @@ def align_batch2_arrays(pbuf, poff, plen, tbuf, toff, tlen, x=4, o1=6, e1=2, o2=
     r = lib().ora_align_batch2(
         n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
         tlen.ctypes.data, x, o1, e1, o2, e2, scores.ctypes.data,
+        ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
+        ops_len.ctypes.data if cigar else None, threads)
+    if r < 0:
+        raise RuntimeError(f"oracle batch error {r}")
+    cig: Optional[List[str]] = None
+    if cigar:
+        raw = ops.tobytes()
+        cig = [raw[ops_off[i]: ops_off[i] + ops_len[i]].decode() for i in range(n)]
+    return scores, cig
+
+
+# --- gap-linear mode (edit distance: x = e = 1; indel: x = 3, e = 1) ---------
+
+def align_linear(pattern, text, x=1, e=1, cigar=True) -> Tuple[int, Optional[str]]:
+    """Align one pair with gap cost e*L; returns (score, ops or None)."""
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap) if cigar else None
+    n_ops = ctypes.c_int(0)
+    r = lib().ora_align_linear(p, len(p), t, len(t), x, e, buf, cap, ctypes.byref(n_ops), None)
+    if r < 0:
+        raise RuntimeError(f"oracle error {r}")
+    return r, (buf.raw[: n_ops.value].decode() if cigar else None)
+
+
+def linear_dp(pattern, text, x=1, e=1) -> int:
+    p, t = _b(pattern), _b(text)
+    return lib().ora_linear_dp_score(p, len(p), t, len(t), x, e)
+
+
+def align_batch_linear(patterns: Sequence, texts: Sequence, x=1, e=1, cigar=True, threads=0):
+    """OpenMP batch with gap cost e*L.  Returns (scores int32[N], op strings or None)."""
+    pats = [_b(p) for p in patterns]
+    txts = [_b(t) for t in texts]
+    n = len(pats)
+    plen = np.array([len(p) for p in pats], dtype=np.int32)
+    tlen = np.array([len(t) for t in txts], dtype=np.int32)
+    poff = np.zeros(n + 1, dtype=np.int64)
+    toff = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(plen, out=poff[1:])
+    np.cumsum(tlen, out=toff[1:])
+    pbuf = np.frombuffer(b"".join(pats) + b"\0", dtype=np.uint8)
+    tbuf = np.frombuffer(b"".join(txts) + b"\0", dtype=np.uint8)
+    return align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, x, e, cigar, threads)
+
+
+def align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, x=1, e=1, cigar=True, threads=0):
+    n = len(plen)
+    scores = np.zeros(n, dtype=np.int32)
+    ops = ops_off = ops_len = None
+    if cigar:
+        caps = plen.astype(np.int64) + tlen.astype(np.int64) + 1
+        ops_off = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(caps, out=ops_off[1:])
+        ops = np.zeros(int(ops_off[-1]) + 1, dtype=np.uint8)
+        ops_len = np.zeros(n, dtype=np.int32)
+    r = lib().ora_align_batch_linear(
+        n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+        tlen.ctypes.data, x, e, scores.ctypes.data,
         ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
         ops_len.ctypes.data if cigar else None, threads)
     if r < 0:

@@ -101,6 +101,15 @@ int ora_align_batch2(int npairs, const char* pat, const int64_t* poff, const int
                      const int64_t* toff, const int32_t* tlen, int x, int o1, int e1, int o2, int e2, int32_t* scores,
                      char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads);
 
+/* Gap-linear mode, wfa_oracle_linear.c: a gap of length L costs e*L (edit
+ * distance: x = e = 1; indel distance: x = 3, e = 1). */
+int ora_align_linear(const char* pattern, int m, const char* text, int n, int x, int e, char* ops, int ops_cap,
+                     int* ops_len, ora_stats_t* st);
+int ora_linear_dp_score(const char* pattern, int m, const char* text, int n, int x, int e);
+int ora_align_batch_linear(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                           const int64_t* toff, const int32_t* tlen, int x, int e, int32_t* scores, char* ops,
+                           const int64_t* ops_off, int32_t* ops_len, int nthreads);
+
 /* CPU-check plugin for the wfa_gpu command line (TSU_CHECK_LIB). */
 int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                            const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,

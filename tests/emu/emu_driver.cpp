@@ -5,7 +5,8 @@
 //
 // Input (stdin):  x o e o2 e2 cigar hint first_mode first_gw N
 //                 then N records "m n\n<pattern>\n<text>\n"
-//   o2 < 0: one gap piece; else dual gap-affine (the kDual kernels)
+//   o2 < 0: one gap piece; else dual gap-affine (the kModelDual kernels);
+//   o < 0: gap-linear with mismatch x and gap e per base (kModelLinear)
 //   first_mode 1 = shared ring, 0 = global ring; first_gw = warps per pair
 //   of the first pass (1, 2, 4, 8, 16).  Retry passes follow the engine's
 //   ladder (tsu_plan.h next_pass).
@@ -38,31 +39,31 @@ struct Buf {  // exact-size heap block
   Buf& operator=(const Buf&) = delete;
 };
 
-template <bool kCigar, int kMode, bool kDual>
+template <bool kCigar, int kMode, int kModel>
 static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
   switch (gw) {
-    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, kDual>(a); }); break;
-    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, kDual>(a); }); break;
-    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, kDual>(a); }); break;
-    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, kDual>(a); }); break;
-    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, kDual>(a); }); break;
-    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, kDual>(a); }); break;
+    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, kModel>(a); }); break;
+    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, kModel>(a); }); break;
+    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, kModel>(a); }); break;
+    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, kModel>(a); }); break;
+    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, kModel>(a); }); break;
+    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, kModel>(a); }); break;
     default: std::abort();
   }
 }
 
-template <bool kDual>
+template <int kModel>
 static void run_pass(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
   if (cigar) {
     if (mode == tsu::kModeShared)
-      run_gw<true, tsu::kModeShared, kDual>(gw, threads, smem, a);
+      run_gw<true, tsu::kModeShared, kModel>(gw, threads, smem, a);
     else
-      run_gw<true, tsu::kModeGlobal, kDual>(gw, threads, smem, a);
+      run_gw<true, tsu::kModeGlobal, kModel>(gw, threads, smem, a);
   } else {
     if (mode == tsu::kModeShared)
-      run_gw<false, tsu::kModeShared, kDual>(gw, threads, smem, a);
+      run_gw<false, tsu::kModeShared, kModel>(gw, threads, smem, a);
     else
-      run_gw<false, tsu::kModeGlobal, kDual>(gw, threads, smem, a);
+      run_gw<false, tsu::kModeGlobal, kModel>(gw, threads, smem, a);
   }
 }
 
@@ -84,7 +85,7 @@ int main() {
     std::cin.get();
   }
   int g = 1;
-  const tsu::Pen rp = tsu::reduce_penalties(X, O, E, O2, E2, &g);
+  const tsu::Pen rp = O < 0 ? tsu::reduce_linear(X, E, &g) : tsu::reduce_penalties(X, O, E, O2, E2, &g);
   const int smem_optin = 232448;
   // sequences: exact-size buffers (pattern i, text i concatenated)
   int64_t ptot = 0, ttot = 0;
@@ -176,10 +177,12 @@ int main() {
     const size_t smem = (size_t)groups * geo.group_smem;
     const int threads = geo.cta_threads;
     gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);
-    if (rp.dual())
-      run_pass<true>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+    if (rp.linear())
+      run_pass<tsu::kModelLinear>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+    else if (rp.dual())
+      run_pass<tsu::kModelDual>(want_cigar, geo.mode, geo.gw, threads, smem, a);
     else
-      run_pass<false>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass<tsu::kModelAffine>(want_cigar, geo.mode, geo.gw, threads, smem, a);
     ++passes;
     const unsigned nretry = *retry_cnt;
     if (nretry == 0) break;

@@ -164,3 +164,23 @@ def test_dual_create_rejects_bad_penalties():
         p2 = Penalties2(*pen)
         assert L.tsu_create_dual(ctypes.byref(p2), None, ctypes.byref(h)) == 1, pen  # TSU_EINVAL
         assert L.tsu_server_create_dual(ctypes.byref(p2), None, ctypes.byref(h)) == 1, pen
+
+
+def test_metric_create_rejects_bad_arguments():
+    """tsu_create_metric / tsu_server_create_metric check the metric and its
+    penalties before touching a device."""
+    import ctypes
+
+    import tsunami_pact_b200 as T
+
+    L = T.lib()
+    h = ctypes.c_void_p()
+    bad = [(7, []), (-1, []), (1, [1]), (0, [1, 1]), (2, [0, 1]), (2, [1, 0]), (2, [1]), (3, [4, 6]),
+           (3, [4, -1, 2]), (4, [4, 6, 2, 24]), (4, [4, 6, 2, -1, 1]), (3, [1 << 21, 6, 2])]
+    for metric, pens in bad:
+        arr = (ctypes.c_int32 * max(1, len(pens)))(*pens)
+        ptr = ctypes.cast(arr, ctypes.c_void_p) if pens else None
+        assert L.tsu_create_metric(metric, ptr, len(pens), None, ctypes.byref(h)) == 1, (metric, pens)
+        assert L.tsu_server_create_metric(metric, ptr, len(pens), None, ctypes.byref(h)) == 1, (metric, pens)
+    with pytest.raises(ValueError):
+        T.Aligner(metric="levenshtein")

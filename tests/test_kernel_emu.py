@@ -253,3 +253,40 @@ def test_dual_ladder(emu, oracle):
     pairs = [_edited(rng, 400, 0.22)] + _long_indels(rng, 2, 200, 300)
     passes, retried, gws = check_dual(emu, oracle, pairs, (4, 6, 2, 24, 1))
     assert passes > 1, gws
+
+
+# --- gap-linear kernels (align_kernel<..., kModelLinear>; edit, indel) -------
+
+def check_linear(exe, oracle, pairs, x, e, **kw):
+    pairs = [(_b(p), _b(t)) for p, t in pairs]
+    got, passes, retried, gws = run_emu(exe, pairs, (x, -1, e), **kw)
+    for (p, t), (s, ops) in zip(pairs, got):
+        es, eops = oracle.align_linear(p, t, x, e)
+        if kw.get("cigar", True):
+            assert (s, ops) == (es, eops), (p, t, x, e, s, es, ops, eops)
+        else:
+            assert s == es and ops == "", (p, t, x, e, s, es)
+    return passes, retried, gws
+
+
+@pytest.mark.parametrize("xe", [(1, 1), (3, 1), (2, 3), (4, 2)])
+def test_linear_random(emu, oracle, xe):
+    rng = random.Random(xe[0] * 10 + xe[1])
+    pairs = [_edited(rng, rng.randint(0, 160), 0.1) for _ in range(24)]
+    pairs += [("", ""), ("", "ACGT"), ("ACG", ""), ("ACGTNNACGT", "ACGTACGT"), ("kitten", "sitting")]
+    check_linear(emu, oracle, pairs, *xe)
+
+
+def test_linear_score_only_and_groups(emu, oracle):
+    rng = random.Random(4)
+    pairs = [_edited(rng, rng.randint(100, 400), 0.12) for _ in range(4)]
+    check_linear(emu, oracle, pairs, 1, 1, cigar=False)
+    for gw, shared in [(4, True), (8, False)]:
+        check_linear(emu, oracle, pairs, 1, 1, shared_first=shared, gw=gw)
+
+
+def test_linear_ladder(emu, oracle):
+    rng = random.Random(12)
+    pairs = [_edited(rng, 800, 0.5)]  # edit distance 244: 489 diagonals > one warp's 384
+    passes, retried, gws = check_linear(emu, oracle, pairs, 1, 1)
+    assert passes > 1, gws

@@ -126,3 +126,64 @@ def test_dual_batch_matches_single(oracle):
     sc, cg = oracle.align_batch2(pats, txts, threads=4)
     for i in range(48):
         assert (sc[i], cg[i]) == oracle.align2(pats[i], txts[i])
+
+
+# --- gap-linear oracle (edit, indel) ----------------------------------------
+
+def _levenshtein(a, b):
+    prev = list(range(len(b) + 1))
+    for i, ca in enumerate(a, 1):
+        cur = [i]
+        for j, cb in enumerate(b, 1):
+            cur.append(min(prev[j] + 1, cur[j - 1] + 1, prev[j - 1] + (ca != cb)))
+        prev = cur
+    return prev[-1]
+
+
+def _lcs(a, b):
+    prev = [0] * (len(b) + 1)
+    for ca in a:
+        cur = [0]
+        for j, cb in enumerate(b, 1):
+            cur.append(prev[j - 1] + 1 if ca == cb else max(prev[j], cur[j - 1]))
+        prev = cur
+    return prev[-1]
+
+
+def test_linear_known_answers(oracle):
+    assert oracle.align_linear("kitten", "sitting") == (3, "XMMMXMI")
+    assert oracle.align_linear("", "ACG") == (3, "III")
+    assert oracle.align_linear("ACG", "", 2, 3) == (9, "DDD")
+    assert oracle.align_linear("ACGT", "ACGT", 3, 1) == (0, "MMMM")
+    # indel distance: a substitution becomes a deletion and an insertion
+    s, ops = oracle.align_linear("ACGT", "AGGT", 3, 1)
+    assert s == 2 and "X" not in ops
+
+
+@pytest.mark.parametrize("pen", [(1, 1), (3, 1), (2, 3), (4, 2), (5, 1), (1, 4)])
+def test_linear_random_vs_dp(oracle, pen):
+    """Scores equal the Needleman-Wunsch optimum (edit distance: also a plain
+    Levenshtein; indel distance: m + n - 2 LCS), and the operation string
+    costs exactly the score."""
+    rng = random.Random(hash(pen) & 0xFFFF)
+    for it in range(250):
+        alpha = "ACGT" if it % 3 else "AC"
+        p = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 50)))
+        t = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 50)))
+        s, ops = oracle.align_linear(p, t, *pen)
+        assert s == oracle.linear_dp(p, t, *pen)
+        if pen == (1, 1):
+            assert s == _levenshtein(p, t)
+        if pen == (3, 1):
+            assert s == len(p) + len(t) - 2 * _lcs(p, t)
+        # cost of the string under linear gaps = affine with open 0
+        assert oracle.cigar_cost(ops, p, t, pen[0], 0, pen[1]) == s
+
+
+def test_linear_batch_matches_single(oracle):
+    rng = random.Random(13)
+    pats = ["".join(rng.choice("ACGT") for _ in range(rng.randint(0, 150))) for _ in range(40)]
+    txts = ["".join(rng.choice("ACGT") for _ in range(rng.randint(0, 150))) for _ in range(40)]
+    sc, cg = oracle.align_batch_linear(pats, txts, 2, 1, threads=4)
+    for i in range(40):
+        assert (sc[i], cg[i]) == oracle.align_linear(pats[i], txts[i], 2, 1)

@@ -108,6 +108,8 @@ def lib():
     L = ctypes.CDLL(_LIB)
     L.tsu_create.argtypes = [P(Penalties), P(Config), P(c_vp)]
     L.tsu_create_dual.argtypes = [P(Penalties2), P(Config), P(c_vp)]
+    L.tsu_create_metric.argtypes = [ctypes.c_int, c_vp, ctypes.c_int, P(Config), P(c_vp)]
+    L.tsu_server_create_metric.argtypes = [ctypes.c_int, c_vp, ctypes.c_int, c_vp, P(c_vp)]
     L.tsu_destroy.argtypes = [c_vp]
     L.tsu_status_str.restype = ctypes.c_char_p
     L.tsu_status_str.argtypes = [ctypes.c_int]
@@ -178,26 +180,45 @@ def runs_to_string(runs: np.ndarray) -> str:
     return out.raw[:w].decode()
 
 
+# TSU_METRIC_* (include/tsunami_b200.h): WFA2-lib's distance metrics
+METRICS = {"indel": 0, "edit": 1, "gap_linear": 2, "gap_affine": 3, "gap_affine_2p": 4}
+
+
+def metric_penalties(metric: Optional[str], mismatch, gap_opening, gap_extension, gap_opening2, gap_extension2):
+    """(TSU_METRIC_* code, penalties tuple) of the constructor arguments:
+    metric None means gap_affine, or gap_affine_2p when a second gap piece is
+    given."""
+    if metric is None:
+        metric = "gap_affine" if gap_opening2 is None and gap_extension2 is None else "gap_affine_2p"
+    if metric not in METRICS:
+        raise ValueError(f"unknown metric {metric!r} (one of {', '.join(METRICS)})")
+    pens = {"indel": (), "edit": (), "gap_linear": (mismatch, gap_extension),
+            "gap_affine": (mismatch, gap_opening, gap_extension),
+            "gap_affine_2p": (mismatch, gap_opening, gap_extension,
+                              -1 if gap_opening2 is None else gap_opening2,
+                              0 if gap_extension2 is None else gap_extension2)}[metric]
+    return METRICS[metric], tuple(int(v) for v in pens)
+
+
 class Aligner:
     """One device context with fixed penalties (reference argv 1-3,
     wfa_gpu.cu:59-61).  With ``gap_opening2`` and ``gap_extension2`` the
-    context aligns under dual gap-affine penalties (tsu_create_dual)."""
+    context aligns under dual gap-affine penalties; ``metric`` selects any of
+    WFA2-lib's distance metrics ("indel", "edit", "gap_linear" with mismatch
+    and gap_extension, "gap_affine", "gap_affine_2p"), tsu_create_metric."""
 
     def __init__(self, mismatch: int = 4, gap_opening: int = 6, gap_extension: int = 2, device: int = 0,
                  mem_budget: int = 0, max_error_hint: float = 0.0, gap_opening2: Optional[int] = None,
-                 gap_extension2: Optional[int] = None):
+                 gap_extension2: Optional[int] = None, metric: Optional[str] = None):
         L = lib()
         cfg = Config(device, 0, mem_budget, max_error_hint)
         h = c_vp()
-        if gap_opening2 is None and gap_extension2 is None:
-            self.penalties = (mismatch, gap_opening, gap_extension)
-            pen = Penalties(mismatch, gap_opening, gap_extension)
-            rc = L.tsu_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
-        else:
-            self.penalties = (mismatch, gap_opening, gap_extension, gap_opening2, gap_extension2)
-            pen2 = Penalties2(mismatch, gap_opening, gap_extension, -1 if gap_opening2 is None else gap_opening2,
-                              0 if gap_extension2 is None else gap_extension2)
-            rc = L.tsu_create_dual(ctypes.byref(pen2), ctypes.byref(cfg), ctypes.byref(h))
+        code, pens = metric_penalties(metric, mismatch, gap_opening, gap_extension, gap_opening2, gap_extension2)
+        self.metric = [k for k, v in METRICS.items() if v == code][0]
+        self.penalties = pens
+        arr = (ctypes.c_int32 * max(1, len(pens)))(*pens)
+        rc = L.tsu_create_metric(code, ctypes.cast(arr, c_vp) if pens else None, len(pens), ctypes.byref(cfg),
+                                 ctypes.byref(h))
         if rc != TSU_OK:
             raise AlignError(rc, L.tsu_status_str(rc).decode())
         self._h = h
@@ -327,19 +348,17 @@ class Server:
                  workers: int = 0, mem_budget: int = 0, max_error_hint: float = 0.0, max_queue: int = 0,
                  max_job_pairs: int = 0, max_job_requests: int = 0, heavy_len: int = 0, heavy_workers: int = 0,
                  estimate_hint: bool = True, watchdog_ms: float = 0.0, resident_bytes: int = 0,
-                 gap_opening2: Optional[int] = None, gap_extension2: Optional[int] = None):
+                 gap_opening2: Optional[int] = None, gap_extension2: Optional[int] = None,
+                 metric: Optional[str] = None):
         L = lib()
         cfg = ServerConfig(device, workers, mem_budget, max_error_hint, max_queue, max_job_pairs,
                            max_job_requests, heavy_len, heavy_workers, 0 if estimate_hint else -1, watchdog_ms,
                            resident_bytes)
         h = c_vp()
-        if gap_opening2 is None and gap_extension2 is None:
-            pen = Penalties(mismatch, gap_opening, gap_extension)
-            rc = L.tsu_server_create(ctypes.byref(pen), ctypes.byref(cfg), ctypes.byref(h))
-        else:
-            pen2 = Penalties2(mismatch, gap_opening, gap_extension, -1 if gap_opening2 is None else gap_opening2,
-                              0 if gap_extension2 is None else gap_extension2)
-            rc = L.tsu_server_create_dual(ctypes.byref(pen2), ctypes.byref(cfg), ctypes.byref(h))
+        code, pens = metric_penalties(metric, mismatch, gap_opening, gap_extension, gap_opening2, gap_extension2)
+        arr = (ctypes.c_int32 * max(1, len(pens)))(*pens)
+        rc = L.tsu_server_create_metric(code, ctypes.cast(arr, c_vp) if pens else None, len(pens),
+                                        ctypes.byref(cfg), ctypes.byref(h))
         if rc != TSU_OK:
             raise AlignError(rc, L.tsu_status_str(rc).decode())
         self._h = h

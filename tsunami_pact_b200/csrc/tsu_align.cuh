@@ -29,11 +29,15 @@
 // and then overwrite one, take a barrier in between.
 // Thread 0 of the group walks the backtrace once the end is reached
 // (tsu_backtrace.cuh).
-// kDual: dual gap-affine (a gap of length L costs min(o1 + e1 L, o2 + e2 L)),
-// the I2 / D2 components the reference declares (common.h:52-58,67-77,80-87):
-// two more gap components with their own ring slots (s - o2 - e2, s - e2),
-// M = max(mismatch, D2, D1, I2, I1) with ties in that (piggyback) order, and
-// a backtrace word with a 3-bit M source and four extension bits.
+// kModel = kModelDual: dual gap-affine (a gap of length L costs
+// min(o1 + e1 L, o2 + e2 L)), the I2 / D2 components the reference declares
+// (common.h:52-58,67-77,80-87): two more gap components with their own ring
+// slots (s - o2 - e2, s - e2), M = max(mismatch, D2, D1, I2, I1) with ties in
+// that (piggyback) order, and a backtrace word with a 3-bit M source and four
+// extension bits.
+// kModel = kModelLinear: gap-linear (a gap costs e per base; edit and indel
+// distance): the M component alone, M = max(M[s-x][k] + 1, M[s-e][k-1] + 1,
+// M[s-e][k+1]), ties mismatch > deletion > insertion; no I/D ring slots.
 #pragma once
 
 #include <type_traits>
@@ -66,9 +70,11 @@ constexpr int cta_min_blocks() {
   return kMode == kModeShared ? (GW <= 4 ? 6 : (GW == 8 ? 3 : 1)) : (GW <= 4 ? 4 : (GW == 8 ? 2 : 1));
 }
 
-template <bool kCigar, int kMode, int GW, bool kDual = false>
+template <bool kCigar, int kMode, int GW, int kModel = kModelAffine>
 __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>())) align_kernel(AlignArgs a) {
   static_assert(GW == 1 || GW == 2 || GW == 4 || GW == 8 || GW == 16 || GW == 32, "warps per pair");
+  constexpr bool kDual = kModel == kModelDual;
+  constexpr bool kLin = kModel == kModelLinear;
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
 #ifdef TSU_WARP_EMU
@@ -198,7 +204,9 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       while (s_end < 0) {
         ++s;
         if (++slm == rm) slm = 0;
-        if (++sli == re) sli = 0;
+        if constexpr (!kLin) {
+          if (++sli == re) sli = 0;
+        }
         if constexpr (kDual) {
           if (++sli2 == a.pen.re2) sli2 = 0;
         }
@@ -215,7 +223,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         const int slot_mo = q;
         q = sli - a.pen.ge;
         if (q < 0) q += re;
-        const int slot_ie = rm + q;
+        const int slot_ie = rm + q;  // (unused by kLin)
         const int slot_de = rm + re + q;
         // sources: first diagonal, cell count (0 = null), ring index of lo.
         // Slot limits are either a trimmed range inside the slot's compute
@@ -232,7 +240,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         };
         if (s - a.pen.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
         if (s - a.pen.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
-        if (s - a.pen.ge >= 0) {
+        if (!kLin && s - a.pen.ge >= 0) {
           src(slot_ie, lo_ie, c_ie, b_ie);
           src(slot_de, lo_de, c_de, b_de);
         }
@@ -257,8 +265,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         if ((c_mm | c_mo | c_ie | c_de | c_mo2 | c_ie2 | c_de2) == 0) {  // null step (wfa_gpu.cu:417-422)
           group_sync<GW>(gid);  // everyone has read the slot limits
           s_lo[out_m] = 1; s_hi[out_m] = 0;
-          s_lo[out_i] = 1; s_hi[out_i] = 0;
-          s_lo[out_d] = 1; s_hi[out_d] = 0;
+          if constexpr (!kLin) {
+            s_lo[out_i] = 1; s_hi[out_i] = 0;
+            s_lo[out_d] = 1; s_hi[out_d] = 0;
+          }
           if constexpr (kDual) {
             s_lo[out_i2] = 1; s_hi[out_i2] = 0;
             s_lo[out_d2] = 1; s_hi[out_d2] = 0;
@@ -277,8 +287,8 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           if (c_de2) { lo = min(lo, lo_de2 - 1); hi = max(hi, lo_de2 + c_de2 - 2); }
         }
         const int width = hi - lo + 1;
-        const bool i_present = c_mo || c_ie;
-        const bool d_present = c_mo || c_de;
+        const bool i_present = !kLin && (c_mo || c_ie);
+        const bool d_present = !kLin && (c_mo || c_de);
         const bool i2_present = kDual && (c_mo2 || c_ie2);
         const bool d2_present = kDual && (c_mo2 || c_de2);
         if (width > W || (kCigar && (s >= a.table_cap || hbase + width > a.hist_cap))) {
@@ -296,11 +306,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           j = k - 1 - lo_mo;
           const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
           j = k - 1 - lo_ie;
-          const int32_t ins_e = ((unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
+          const int32_t ins_e = (!kLin && (unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
           j = k + 1 - lo_mo;
           const int32_t del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
           j = k + 1 - lo_de;
-          const int32_t del_e = ((unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
+          const int32_t del_e = (!kLin && (unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
           j = k - lo_mm;
           const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
           const int32_t ins = max(ins_o, ins_e) + 1;
@@ -337,8 +347,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             bits = kSrcIns;
             if (del >= p) { p = del; bits = kSrcDel; }
             if (mis >= p) { p = mis; bits = kSrcMis; }
-            if (ins_e >= ins_o) bits |= kIExt;
-            if (del_e >= del_o) bits |= kDExt;
+            if constexpr (!kLin) {
+              if (ins_e >= ins_o) bits |= kIExt;
+              if (del_e >= del_o) bits |= kDExt;
+            }
           }
           int32_t om = kNull;
           if (in_bounds(p, k, m, n)) {
@@ -423,8 +435,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           // empty range (1, 0)
           const bool em = fm > lm, ei = !i_present || fi > li, ed = !d_present || fd > ld;
           s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
-          s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
-          s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
+          if constexpr (!kLin) {
+            s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
+            s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
+          }
           if constexpr (kDual) {
             const bool ei2 = !i2_present || fi2 > li2, ed2 = !d2_present || fd2 > ld2;
             s_lo[out_i2] = ei2 ? 1 : fi2; s_hi[out_i2] = ei2 ? 0 : li2; s_alo[out_i2] = lo;

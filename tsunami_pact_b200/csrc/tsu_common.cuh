@@ -24,8 +24,10 @@ enum : uint32_t { kSrcMis = 0, kSrcIns = 1, kSrcDel = 2, kIExt = 4, kDExt = 8 };
 enum : uint32_t { kSrcIns2 = 3, kSrcDel2 = 4, kI1Ext2 = 8, kD1Ext2 = 16, kI2Ext2 = 32, kD2Ext2 = 64 };
 constexpr int kDualMaxLen = (1 << 24) - 2;  // offsets of the dual backtrace word
 enum : uint32_t { kOpM = 0, kOpI = 1, kOpD = 2, kOpX = 8 };
-// align kernel variants
+// align kernel variants: ring mode; penalty model (gap-affine; dual
+// gap-affine; gap-linear, which edit and indel distance are cases of)
 enum : int { kModeShared = 0, kModeGlobal = 1 };
+enum : int { kModelAffine = 0, kModelDual = 1, kModelLinear = 2 };
 
 struct SeqView {
   int64_t n;  // pairs
@@ -47,11 +49,14 @@ struct PackView {
 // wavefront ring: rm M slots (the scores s - x, s - o - e, s - o2 - e2 back),
 // re slots of I1 and of D1 (s - e back) and, for dual gap-affine, re2 slots
 // of I2 and of D2.  go = o + e (a gap of length L costs go + ge (L - 1)).
-// One piece: go2 = ge2 = re2 = 0.
+// One piece: go2 = ge2 = re2 = 0.  Gap-linear (a gap costs ge per base): go =
+// ge and no I/D components (re = re2 = 0).
 struct Pen {
   int x = 0, go = 0, ge = 0, go2 = 0, ge2 = 0;
   int rm = 0, re = 0, re2 = 0;
   __host__ __device__ bool dual() const { return re2 > 0; }
+  __host__ __device__ bool linear() const { return re == 0; }
+  __host__ __device__ int model() const { return linear() ? kModelLinear : (dual() ? kModelDual : kModelAffine); }
   __host__ __device__ int slots() const { return rm + 2 * re + 2 * re2; }
   // cheapest and dearest single-base edit (a one-base gap costs
   // min(go, go2)), smallest extension
@@ -103,6 +108,18 @@ inline Pen reduce_penalties(int mismatch, int open, int ext, int open2, int ext2
   }
   p.re = p.ge + 1;
   p.re2 = dual ? p.ge2 + 1 : 0;
+  p.rm = p.ring_depth() + 1;
+  if (g) *g = u;
+  return p;
+}
+
+// Gap-linear penalties (mismatch, per-base gap) in score units.
+inline Pen reduce_linear(int mismatch, int ext, int* g) {
+  const int u = gcd_int(mismatch, ext);
+  Pen p;
+  p.x = mismatch / u;
+  p.go = p.ge = ext / u;
+  p.re = p.re2 = 0;
   p.rm = p.ring_depth() + 1;
   if (g) *g = u;
   return p;

@@ -56,7 +56,7 @@ struct tsu_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
-  tsu_penalties2 pen{};  // raw penalties (gap_opening2 < 0: one piece)
+  tsu::engine::Spec spec;  // metric and raw penalties
   tsu::Pen rp;  // reduced penalties, ring depths
   int g = 1;    // score unit
   size_t budget = 0;
@@ -140,14 +140,6 @@ int set_err(tsu_ctx* c, int code, const char* fmt, ...) {
 // offset range.
 int32_t max_len(const tsu_ctx* ctx) { return ctx->rp.dual() ? tsu::kDualMaxLen : (1 << 26); }
 
-// Raw penalties within the supported ranges: mismatch > 0, opening >= 0,
-// extension > 0, each at most 2^20; the second gap piece is off
-// (gap_opening2 < 0) or obeys the same ranges.
-bool valid_penalties(const tsu_penalties2* p) {
-  auto ok = [](int32_t o, int32_t e) { return o >= 0 && e > 0 && o <= (1 << 20) && e <= (1 << 20); };
-  if (p->mismatch <= 0 || p->mismatch > (1 << 20) || !ok(p->gap_opening, p->gap_extension)) return false;
-  return p->gap_opening2 < 0 || ok(p->gap_opening2, p->gap_extension2);
-}
 
 // Device memory of every context comes from one stream-ordered pool per
 // device: a buffer is regrown with cudaFreeAsync + cudaMallocFromPoolAsync on
@@ -277,20 +269,24 @@ struct BatchInfo {
   int64_t total_words = 0;
 };
 
-// The align_kernel instantiations (tsu_launch.cuh): one-piece kernels here,
-// dual gap-affine ones in tsu_dual.cu.
+// The align_kernel instantiations (tsu_launch.cuh): gap-affine kernels here,
+// dual gap-affine ones in tsu_dual.cu, gap-linear ones in tsu_linear.cu.
 cudaError_t align_occupancy(const tsu_ctx* ctx, bool cigar, int mode, int gw, int threads, size_t smem, int optin,
                             int* occ) {
-  if (ctx->rp.dual()) return tsu::align_occupancy_dual(cigar, mode, gw, threads, smem, optin, occ);
-  return tsu::launch_detail::occupancy<false>(cigar, mode, gw, threads, smem, optin, occ);
+  switch (ctx->rp.model()) {
+    case tsu::kModelDual: return tsu::align_occupancy_dual(cigar, mode, gw, threads, smem, optin, occ);
+    case tsu::kModelLinear: return tsu::align_occupancy_linear(cigar, mode, gw, threads, smem, optin, occ);
+    default: return tsu::launch_detail::occupancy<tsu::kModelAffine>(cigar, mode, gw, threads, smem, optin, occ);
+  }
 }
 
 void launch_align(const tsu_ctx* ctx, bool cigar, int mode, int gw, int blocks, int threads, size_t smem,
                   cudaStream_t st, const tsu::AlignArgs& a) {
-  if (ctx->rp.dual())
-    tsu::launch_align_dual(cigar, mode, gw, blocks, threads, smem, st, a);
-  else
-    tsu::launch_detail::launch<false>(cigar, mode, gw, blocks, threads, smem, st, a);
+  switch (ctx->rp.model()) {
+    case tsu::kModelDual: tsu::launch_align_dual(cigar, mode, gw, blocks, threads, smem, st, a); break;
+    case tsu::kModelLinear: tsu::launch_align_linear(cigar, mode, gw, blocks, threads, smem, st, a); break;
+    default: tsu::launch_detail::launch<tsu::kModelAffine>(cigar, mode, gw, blocks, threads, smem, st, a); break;
+  }
 }
 
 // Scratch bytes of one group of a pass (ring, history, step table).
@@ -946,16 +942,54 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
   return TSU_OK;
 }
 
-int create(const tsu_penalties2* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out) {
+int make_spec(int metric, const int32_t* pen, int count, Spec* out) {
+  static const int kCount[5] = {0, 0, 2, 3, 5};  // penalties per TSU_METRIC_*
+  if (!out || metric < TSU_METRIC_INDEL || metric > TSU_METRIC_GAP_AFFINE_2P) return TSU_EINVAL;
+  if (count != kCount[metric] || (count && !pen)) return TSU_EINVAL;
+  auto in = [](int32_t v, int32_t lo) { return v >= lo && v <= (1 << 20); };
+  Spec s;
+  s.metric = metric;
+  switch (metric) {
+    case TSU_METRIC_INDEL: s.x = 3; s.e = 1; break;  // a mismatch (3) never beats D + I (2)
+    case TSU_METRIC_EDIT: s.x = 1; s.e = 1; break;
+    case TSU_METRIC_GAP_LINEAR:
+      if (!in(pen[0], 1) || !in(pen[1], 1)) return TSU_EINVAL;
+      s.x = pen[0];
+      s.e = pen[1];
+      break;
+    case TSU_METRIC_GAP_AFFINE_2P:
+      if (!in(pen[3], 0) || !in(pen[4], 1)) return TSU_EINVAL;
+      s.o2 = pen[3];
+      s.e2 = pen[4];
+      [[fallthrough]];
+    default:
+      if (!in(pen[0], 1) || !in(pen[1], 0) || !in(pen[2], 1)) return TSU_EINVAL;
+      s.x = pen[0];
+      s.o = pen[1];
+      s.e = pen[2];
+      break;
+  }
+  *out = s;
+  return TSU_OK;
+}
+
+int create(const Spec& spec, const tsu_config* cfg, bool single_stream, tsu_ctx** out) {
   tsu_ctx* ctx = nullptr;
-  if (!pen || !out) return TSU_EINVAL;
+  if (!out) return TSU_EINVAL;
   *out = nullptr;
-  if (!valid_penalties(pen)) return TSU_EINVAL;
-  const bool dual = pen->gap_opening2 >= 0 && pen->gap_extension2 > 0;
   ctx = new tsu_ctx();
-  ctx->pen = *pen;
-  ctx->rp = tsu::reduce_penalties(pen->mismatch, pen->gap_opening, pen->gap_extension, dual ? pen->gap_opening2 : -1,
-                                  dual ? pen->gap_extension2 : 0, &ctx->g);
+  ctx->spec = spec;
+  switch (spec.metric) {
+    case TSU_METRIC_GAP_AFFINE:
+      ctx->rp = tsu::reduce_penalties(spec.x, spec.o, spec.e, -1, 0, &ctx->g);
+      break;
+    case TSU_METRIC_GAP_AFFINE_2P:
+      ctx->rp = tsu::reduce_penalties(spec.x, spec.o, spec.e, spec.o2, spec.e2, &ctx->g);
+      break;
+    default:  // indel, edit, gap-linear
+      ctx->rp = tsu::reduce_linear(spec.x, spec.e, &ctx->g);
+      break;
+  }
   if (ctx->rp.slots() > 4096) {
     delete ctx;
     return TSU_EINVAL;  // reduced penalties too large for the wavefront ring
@@ -1087,15 +1121,25 @@ const char* tsu_last_error(const tsu_ctx* ctx) { return ctx ? ctx->err.c_str() :
 
 const char* tsu_pass_log(const tsu_ctx* ctx) { return ctx ? ctx->passlog.c_str() : ""; }
 
+int tsu_create_metric(int metric, const int32_t* penalties, int num_penalties, const tsu_config* cfg,
+                      tsu_ctx** out) {
+  if (!out) return TSU_EINVAL;
+  *out = nullptr;
+  tsu::engine::Spec spec;
+  const int rc = tsu::engine::make_spec(metric, penalties, num_penalties, &spec);
+  return rc ? rc : tsu::engine::create(spec, cfg, false, out);
+}
+
 int tsu_create(const tsu_penalties* pen, const tsu_config* cfg, tsu_ctx** out) {
-  if (!pen || !out) return TSU_EINVAL;
-  const tsu_penalties2 p2 = tsu::engine::one_piece(*pen);
-  return tsu::engine::create(&p2, cfg, false, out);
+  if (!pen) return TSU_EINVAL;
+  const int32_t p[3] = {pen->mismatch, pen->gap_opening, pen->gap_extension};
+  return tsu_create_metric(TSU_METRIC_GAP_AFFINE, p, 3, cfg, out);
 }
 
 int tsu_create_dual(const tsu_penalties2* pen, const tsu_config* cfg, tsu_ctx** out) {
-  if (!pen || !out || pen->gap_opening2 < 0 || pen->gap_extension2 <= 0) return TSU_EINVAL;
-  return tsu::engine::create(pen, cfg, false, out);
+  if (!pen) return TSU_EINVAL;
+  const int32_t p[5] = {pen->mismatch, pen->gap_opening, pen->gap_extension, pen->gap_opening2, pen->gap_extension2};
+  return tsu_create_metric(TSU_METRIC_GAP_AFFINE_2P, p, 5, cfg, out);
 }
 
 int tsu_destroy(tsu_ctx* ctx) {

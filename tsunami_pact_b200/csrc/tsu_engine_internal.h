@@ -15,11 +15,16 @@ namespace engine {
 // limited number of hardware queues (CUDA_DEVICE_MAX_CONNECTIONS) that
 // streams share in turn; work queued behind a long kernel on a shared queue
 // waits for it, so contexts of many host threads use one stream each.
-// pen->gap_opening2 < 0: one gap piece.
-int create(const tsu_penalties2* pen, const tsu_config* cfg, bool single_stream, tsu_ctx** out);
-inline tsu_penalties2 one_piece(const tsu_penalties& p) {
-  return tsu_penalties2{p.mismatch, p.gap_opening, p.gap_extension, -1, 0};
-}
+// The penalties of a context: a distance metric (TSU_METRIC_*) and its raw
+// penalties (those the metric does not use are 0).
+struct Spec {
+  int metric = TSU_METRIC_GAP_AFFINE;
+  int32_t x = 0, o = 0, e = 0, o2 = 0, e2 = 0;
+};
+int create(const Spec& spec, const tsu_config* cfg, bool single_stream, tsu_ctx** out);
+// The spec of tsu_create_metric's arguments; TSU_EINVAL for an unknown
+// metric, a wrong penalty count or a penalty out of range.
+int make_spec(int metric, const int32_t* pen, int count, Spec* out);
 
 // Lengths of the pairs of a planned batch (host memory).
 struct BatchShape {

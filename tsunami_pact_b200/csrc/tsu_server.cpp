@@ -145,7 +145,7 @@ class EngineExecutor final : public tsu::serve::Executor {
   HostStage in_, out_;
 };
 
-int make_ctx(const tsu_penalties2* pen, int device, double hint, size_t budget, tsu_ctx** out) {
+int make_ctx(const tsu::engine::Spec& pen, int device, double hint, size_t budget, tsu_ctx** out) {
   tsu_config c{};
   c.device = device;
   c.mem_budget = budget;
@@ -162,7 +162,7 @@ struct tsu_server {
 
 namespace {
 
-int server_create(const tsu_penalties2* pen, const tsu_server_config* cfg, tsu_server** out) {
+int server_create(const tsu::engine::Spec& pen, const tsu_server_config* cfg, tsu_server** out) {
   *out = nullptr;
   tsu_server_config c{};
   if (cfg) c = *cfg;
@@ -208,15 +208,25 @@ int server_create(const tsu_penalties2* pen, const tsu_server_config* cfg, tsu_s
 
 extern "C" {
 
+int tsu_server_create_metric(int metric, const int32_t* penalties, int num_penalties, const tsu_server_config* cfg,
+                             tsu_server** out) {
+  if (!out) return TSU_EINVAL;
+  *out = nullptr;
+  tsu::engine::Spec spec;
+  const int rc = tsu::engine::make_spec(metric, penalties, num_penalties, &spec);
+  return rc ? rc : server_create(spec, cfg, out);
+}
+
 int tsu_server_create(const tsu_penalties* pen, const tsu_server_config* cfg, tsu_server** out) {
-  if (!pen || !out) return TSU_EINVAL;
-  const tsu_penalties2 p2 = tsu::engine::one_piece(*pen);
-  return server_create(&p2, cfg, out);
+  if (!pen) return TSU_EINVAL;
+  const int32_t p[3] = {pen->mismatch, pen->gap_opening, pen->gap_extension};
+  return tsu_server_create_metric(TSU_METRIC_GAP_AFFINE, p, 3, cfg, out);
 }
 
 int tsu_server_create_dual(const tsu_penalties2* pen, const tsu_server_config* cfg, tsu_server** out) {
-  if (!pen || !out || pen->gap_opening2 < 0 || pen->gap_extension2 <= 0) return TSU_EINVAL;
-  return server_create(pen, cfg, out);
+  if (!pen) return TSU_EINVAL;
+  const int32_t p[5] = {pen->mismatch, pen->gap_opening, pen->gap_extension, pen->gap_opening2, pen->gap_extension2};
+  return tsu_server_create_metric(TSU_METRIC_GAP_AFFINE_2P, p, 5, cfg, out);
 }
 
 int tsu_server_destroy(tsu_server* srv) {
