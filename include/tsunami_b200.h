@@ -181,6 +181,19 @@ const char* tsu_pass_log(const tsu_ctx* ctx);
  * retried at the next one, so a rung never changes a result.  No
  * counterpart in the reference (one fixed launch shape, wfa_gpu.cu:113-114). */
 int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair);
+
+/* Ends-free alignment: WFA2-lib's alignment_span = ends_free
+ * (wavefront_aligner_set_alignment_free_ends), which the reference leaves at
+ * its end-to-end default (wfa_gpu.cu:156-160).  The alignment may start at
+ * (v, 0) with v <= pattern_begin_free or at (0, h) with h <= text_begin_free
+ * at no cost, and end at (m, h) with h >= n - text_end_free or at (v, n) with
+ * v >= m - pattern_end_free.  The free end gaps stay in the CIGAR as I / D
+ * runs (costing 0); of several ends at the optimal score the lowest diagonal
+ * h - v wins.  All 0 (the default): end-to-end.  Gap-affine contexts only
+ * (TSU_EINVAL otherwise); applies to the context's later align calls. */
+int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_end_free, int32_t text_begin_free,
+                      int32_t text_end_free);
+int tsu_get_ends_free(const tsu_ctx* ctx, int32_t* out4);
 int tsu_get_band_start(const tsu_ctx* ctx, int band, int* mode, int* warps_per_pair);
 
 /* ---- batch alignment, host buffers -------------------------------------

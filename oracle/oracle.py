@@ -32,6 +32,12 @@ class OraStats(ctypes.Structure):
     ]
 
 
+class OraEnds(ctypes.Structure):
+    """Free ends: pattern_begin_free, pattern_end_free, text_begin_free, text_end_free."""
+    _fields_ = [("pattern_begin_free", ctypes.c_int32), ("pattern_end_free", ctypes.c_int32),
+                ("text_begin_free", ctypes.c_int32), ("text_end_free", ctypes.c_int32)]
+
+
 def build() -> str:
     """Compile liboracle.so with the Makefile beside this file."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -80,6 +86,19 @@ def lib():
         L.ora_align_batch_linear.restype = ctypes.c_int
         L.ora_align_batch_linear.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 2 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.ora_align_ends_free.restype = ctypes.c_int
+        L.ora_align_ends_free.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, P(OraEnds), ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int),
+                                          P(OraStats)]
+        L.ora_align_batch_ends_free.restype = ctypes.c_int
+        L.ora_align_batch_ends_free.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3 + [
+            P(OraEnds)] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.ora_gotoh_ends_free_score.restype = ctypes.c_int
+        L.ora_gotoh_ends_free_score.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, P(OraEnds)]
+        L.ora_cigar_cost_ends_free.restype = i64
+        L.ora_cigar_cost_ends_free.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, c_char_p,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(OraEnds)]
         L.ora_align_batch2.restype = ctypes.c_int
         L.ora_align_batch2.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
@@ -282,6 +301,65 @@ def align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, x=1, e=1, ciga
     r = lib().ora_align_batch_linear(
         n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
         tlen.ctypes.data, x, e, scores.ctypes.data,
+        ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
+        ops_len.ctypes.data if cigar else None, threads)
+    if r < 0:
+        raise RuntimeError(f"oracle batch error {r}")
+    cig: Optional[List[str]] = None
+    if cigar:
+        raw = ops.tobytes()
+        cig = [raw[ops_off[i]: ops_off[i] + ops_len[i]].decode() for i in range(n)]
+    return scores, cig
+
+
+# --- ends-free gap-affine (free = (pattern_begin, pattern_end, text_begin, text_end)) --
+
+def align_ends_free(pattern, text, free, x=4, o=6, e=2, cigar=True) -> Tuple[int, Optional[str]]:
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap) if cigar else None
+    n_ops = ctypes.c_int(0)
+    r = lib().ora_align_ends_free(p, len(p), t, len(t), x, o, e, ctypes.byref(OraEnds(*free)), buf, cap,
+                                  ctypes.byref(n_ops), None)
+    if r < 0:
+        raise RuntimeError(f"oracle error {r}")
+    return r, (buf.raw[: n_ops.value].decode() if cigar else None)
+
+
+def gotoh_ends_free(pattern, text, free, x=4, o=6, e=2) -> int:
+    p, t = _b(pattern), _b(text)
+    return lib().ora_gotoh_ends_free_score(p, len(p), t, len(t), x, o, e, ctypes.byref(OraEnds(*free)))
+
+
+def cigar_cost_ends_free(ops: str, pattern, text, free, x=4, o=6, e=2) -> int:
+    p, t, c = _b(pattern), _b(text), _b(ops)
+    return lib().ora_cigar_cost_ends_free(c, len(c), p, len(p), t, len(t), x, o, e, ctypes.byref(OraEnds(*free)))
+
+
+def align_batch_ends_free(patterns: Sequence, texts: Sequence, free, x=4, o=6, e=2, cigar=True, threads=0):
+    """OpenMP batch with free ends.  Returns (scores int32[N], op strings or None)."""
+    pats = [_b(p) for p in patterns]
+    txts = [_b(t) for t in texts]
+    n = len(pats)
+    plen = np.array([len(p) for p in pats], dtype=np.int32)
+    tlen = np.array([len(t) for t in txts], dtype=np.int32)
+    poff = np.zeros(n + 1, dtype=np.int64)
+    toff = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(plen, out=poff[1:])
+    np.cumsum(tlen, out=toff[1:])
+    pbuf = np.frombuffer(b"".join(pats) + b"\0", dtype=np.uint8)
+    tbuf = np.frombuffer(b"".join(txts) + b"\0", dtype=np.uint8)
+    scores = np.zeros(n, dtype=np.int32)
+    ops = ops_off = ops_len = None
+    if cigar:
+        caps = plen.astype(np.int64) + tlen.astype(np.int64) + 1
+        ops_off = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(caps, out=ops_off[1:])
+        ops = np.zeros(int(ops_off[-1]) + 1, dtype=np.uint8)
+        ops_len = np.zeros(n, dtype=np.int32)
+    r = lib().ora_align_batch_ends_free(
+        n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+        tlen.ctypes.data, x, o, e, ctypes.byref(OraEnds(*free)), scores.ctypes.data,
         ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
         ops_len.ctypes.data if cigar else None, threads)
     if r < 0:

@@ -227,9 +227,11 @@ static inline int64_t bt_src(const ws_t* ws, const wf_t* w, int k, int delta, in
 
 enum { ST_M = 0, ST_I = 1, ST_D = 2 };
 
-/* Wavefront backtrace from M[s_end][n - m] (the end2end end point).  Writes
- * operations backwards into ws->opbuf and returns the start index, or < 0. */
-static int wf_backtrace(ws_t* ws, int s_end, int x, int o, int e, int m, int n, int* start) {
+/* Wavefront backtrace from M[s_end][k_end] (n - m for end-to-end; with free
+ * ends the end diagonal found by align_ws, whose trailing pattern or text
+ * gap is emitted first).  Writes operations backwards into ws->opbuf and
+ * returns the start index, or < 0. */
+static int wf_backtrace(ws_t* ws, int s_end, int k_end, int x, int o, int e, int m, int n, int* start) {
   const int cap = m + n + 1;
   if (ws->opbuf_cap < cap) {
     char* nb = (char*)realloc(ws->opbuf, (size_t)cap);
@@ -244,9 +246,12 @@ static int wf_backtrace(ws_t* ws, int s_end, int x, int o, int e, int m, int n, 
     if (pos < 0) return ORA_ECIGCAP;   \
     ops[pos--] = (c);                  \
   } while (0)
-  int state = ST_M, s = s_end, k = n - m;
-  int32_t off = n;
+  int state = ST_M, s = s_end, k = k_end;
+  int32_t off = wf_get(ws, &ws->M[s_end], k_end);
   int v = off - k, h = off;
+  /* free end gap: the rest of the pattern (text consumed) or of the text */
+  for (int i = v; i < m; ++i) EMIT('D');
+  for (int i = h; i < n; ++i) EMIT('I');
   while (v > 0 && h > 0 && s > 0) {
     const int smis = s - x, sgo = s - o - e, sge = s - e;
     const wf_t* wm_mis = smis >= 0 ? &ws->M[smis] : NULL;
@@ -299,30 +304,50 @@ static int wf_backtrace(ws_t* ws, int s_end, int x, int o, int e, int m, int n, 
   return 0;
 }
 
+/* The end diagonal of M[s] (the lowest k that ends an alignment), or
+ * INT_MIN.  End-to-end: k = n - m at offset n.  With free ends: the text is
+ * consumed with at most pef pattern characters left, or the pattern with at
+ * most tef text characters left (WFA2-lib's ends-free termination). */
+static int wf_end_diagonal(const ws_t* ws, const wf_t* M, int m, int n, const ora_ends_t* ef) {
+  if (wf_null(M)) return INT_MIN;
+  for (int k = M->lo; k <= M->hi; ++k) {
+    const int32_t off = wf_get(ws, M, k);
+    if (off == ONULL) continue;
+    const int v = off - k;
+    if ((off >= n && v >= m - ef->pattern_end_free) || (v >= m && off >= n - ef->text_end_free)) return k;
+  }
+  return INT_MIN;
+}
+
 static int align_ws(ws_t* ws, const char* pattern, int m, const char* text, int n, int x, int o, int e,
-                    char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
+                    const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
   if (m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;
+  if (ef->pattern_begin_free < 0 || ef->pattern_end_free < 0 || ef->text_begin_free < 0 || ef->text_end_free < 0)
+    return ORA_EINVAL;
   const unsigned char* p = (const unsigned char*)pattern;
   const unsigned char* t = (const unsigned char*)text;
   ws->arena_used = 0;
   if (ws_reserve_scores(ws, 1)) return ORA_ENOMEM;
-  /* Score 0: M[0] = {k=0: offset 0} (wfa_gpu.cu:239-242). */
+  /* Score 0: M[0] = {k=0: offset 0} (wfa_gpu.cu:239-242); with free
+   * beginnings every start (v, 0), v <= pattern_begin_free, and (0, h),
+   * h <= text_begin_free: diagonals -pbf..tbf at offset max(k, 0). */
+  const int lo0 = -(ef->pattern_begin_free < m ? ef->pattern_begin_free : m);
+  const int hi0 = ef->text_begin_free < n ? ef->text_begin_free : n;
   wf_t* M0 = &ws->M[0];
   memset(M0, 0, sizeof(*M0));
   memset(&ws->I[0], 0, sizeof(wf_t));
   memset(&ws->D[0], 0, sizeof(wf_t));
   ws->I[0].lo = ws->D[0].lo = 1;
-  int64_t b0 = ws_alloc(ws, 1);
+  int64_t b0 = ws_alloc(ws, hi0 - lo0 + 1);
   if (b0 < 0) return ORA_ENOMEM;
-  M0->present = 1; M0->lo = M0->hi = M0->alo = M0->ahi = 0; M0->base = b0;
-  ws->arena[b0] = 0;
-  if (st) { st->steps++; st->cells += 1; }
-  const int k_end = n - m;
-  int s = 0;
+  M0->present = 1; M0->lo = M0->alo = lo0; M0->hi = M0->ahi = hi0; M0->base = b0;
+  for (int k = lo0; k <= hi0; ++k) ws->arena[b0 + (k - lo0)] = k > 0 ? k : 0;
+  if (st) { st->steps++; st->cells += hi0 - lo0 + 1; }
+  int s = 0, k_end;
   for (;;) {
     wf_extend(ws, s, p, m, t, n, st);
-    const wf_t* M = &ws->M[s];
-    if (!wf_null(M) && k_end >= M->lo && k_end <= M->hi && wf_get(ws, M, k_end) >= n) break;
+    k_end = wf_end_diagonal(ws, &ws->M[s], m, n, ef);
+    if (k_end != INT_MIN) break;
     ++s;
     if (ws_reserve_scores(ws, s + 1)) return ORA_ENOMEM;
     int rc = wf_compute(ws, s, x, o, e, m, n, st);
@@ -331,7 +356,7 @@ static int align_ws(ws_t* ws, const char* pattern, int m, const char* text, int 
   if (st) st->final_score = s;
   if (ops) {
     int start = 0;
-    int rc = wf_backtrace(ws, s, x, o, e, m, n, &start);
+    int rc = wf_backtrace(ws, s, k_end, x, o, e, m, n, &start);
     if (rc) return rc;
     const int len = (m + n + 1) - start;
     if (len > ops_cap) return ORA_ECIGCAP;
@@ -341,11 +366,22 @@ static int align_ws(ws_t* ws, const char* pattern, int m, const char* text, int 
   return s;
 }
 
+static const ora_ends_t kEndToEnd = {0, 0, 0, 0};
+
 int ora_align(const char* pattern, int m, const char* text, int n, int x, int o, int e, char* ops, int ops_cap,
               int* ops_len, ora_stats_t* st) {
   ws_t ws;
   memset(&ws, 0, sizeof(ws));
-  int r = align_ws(&ws, pattern, m, text, n, x, o, e, ops, ops_cap, ops_len, st);
+  int r = align_ws(&ws, pattern, m, text, n, x, o, e, &kEndToEnd, ops, ops_cap, ops_len, st);
+  ws_free(&ws);
+  return r;
+}
+
+int ora_align_ends_free(const char* pattern, int m, const char* text, int n, int x, int o, int e,
+                        const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
+  ws_t ws;
+  memset(&ws, 0, sizeof(ws));
+  int r = align_ws(&ws, pattern, m, text, n, x, o, e, ef ? ef : &kEndToEnd, ops, ops_cap, ops_len, st);
   ws_free(&ws);
   return r;
 }
@@ -440,9 +476,10 @@ int ora_max_threads(void) {
 #endif
 }
 
-int ora_align_batch(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
-                    const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores, char* ops,
-                    const int64_t* ops_off, int32_t* ops_len, int nthreads, ora_stats_t* st) {
+static int batch_impl(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                      const int64_t* toff, const int32_t* tlen, int x, int o, int e, const ora_ends_t* ef,
+                      int32_t* scores, char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads,
+                      ora_stats_t* st) {
   int err = 0;
   int64_t steps = 0, cells = 0, extc = 0, extn = 0;
 #ifdef _OPENMP
@@ -461,7 +498,7 @@ int ora_align_batch(int npairs, const char* pat, const int64_t* poff, const int3
       char* po = ops ? ops + ops_off[i] : NULL;
       const int cap = ops ? (int)(ops_off[i + 1] - ops_off[i]) : 0;
       int len = 0;
-      int r = align_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o, e, po, cap, &len,
+      int r = align_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o, e, ef, po, cap, &len,
                        st ? &ls : NULL);
       scores[i] = r;
       if (ops_len) ops_len[i] = ops ? len : 0;
@@ -491,6 +528,109 @@ int ora_align_batch(int npairs, const char* pat, const int64_t* poff, const int3
  * looks up in the library named by TSU_CHECK_LIB when check=1.  Computes the
  * full alignment of every pair (as the reference's WFA2-lib check does,
  * wfa_gpu.cu:154-166) and returns the scores. */
+int ora_align_batch(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                    const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores, char* ops,
+                    const int64_t* ops_off, int32_t* ops_len, int nthreads, ora_stats_t* st) {
+  return batch_impl(npairs, pat, poff, plen, txt, toff, tlen, x, o, e, &kEndToEnd, scores, ops, ops_off, ops_len,
+                    nthreads, st);
+}
+
+int ora_align_batch_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                              const int64_t* toff, const int32_t* tlen, int x, int o, int e, const ora_ends_t* ef,
+                              int32_t* scores, char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads) {
+  return batch_impl(npairs, pat, poff, plen, txt, toff, tlen, x, o, e, ef ? ef : &kEndToEnd, scores, ops, ops_off,
+                    ops_len, nthreads, NULL);
+}
+
+/* Gotoh DP with free ends: a start (v, 0) with v <= pattern_begin_free or
+ * (0, h) with h <= text_begin_free costs nothing, and the best of the last
+ * row at h >= n - text_end_free and of the last column at v >= m -
+ * pattern_end_free is the score. */
+int ora_gotoh_ends_free_score(const char* pattern, int m, const char* text, int n, int x, int o, int e,
+                              const ora_ends_t* ef) {
+  const int64_t INF = (int64_t)1 << 40;
+  int64_t* H = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  int64_t* F = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  if (!H || !F) { free(H); free(F); return ORA_ENOMEM; }
+  /* row 0: free up to text_begin_free, then an insertion run from there */
+  int64_t E0 = INF;
+  H[0] = 0;
+  F[0] = INF;
+  for (int j = 1; j <= n; ++j) {
+    E0 = (E0 + e < H[j - 1] + o + e) ? E0 + e : H[j - 1] + o + e;
+    H[j] = j <= ef->text_begin_free ? 0 : E0;
+    F[j] = INF;
+  }
+  int64_t best_end = INF;
+  if (m <= ef->pattern_end_free || m == 0)  /* last column of row 0 */
+    best_end = H[n];
+  for (int j = (n - ef->text_end_free > 0 ? n - ef->text_end_free : 0); j <= n && m == 0; ++j)
+    if (H[j] < best_end) best_end = H[j];
+  for (int i = 1; i <= m; ++i) {
+    int64_t diag = H[0];
+    /* column 0: free up to pattern_begin_free, then a deletion run */
+    F[0] = (F[0] + e < H[0] + o + e) ? F[0] + e : H[0] + o + e;
+    H[0] = i <= ef->pattern_begin_free ? 0 : F[0];
+    int64_t E = INF;
+    for (int j = 1; j <= n; ++j) {
+      const int64_t up_h = H[j];
+      E = (E + e < H[j - 1] + o + e) ? E + e : H[j - 1] + o + e;
+      F[j] = (F[j] + e < up_h + o + e) ? F[j] + e : up_h + o + e;
+      int64_t best = diag + (pattern[i - 1] == text[j - 1] ? 0 : x);
+      if (E < best) best = E;
+      if (F[j] < best) best = F[j];
+      diag = up_h;
+      H[j] = best;
+    }
+    if (i >= m - ef->pattern_end_free && H[n] < best_end) best_end = H[n];
+    if (i == m)
+      for (int j = (n - ef->text_end_free > 0 ? n - ef->text_end_free : 0); j <= n; ++j)
+        if (H[j] < best_end) best_end = H[j];
+  }
+  free(H);
+  free(F);
+  return (int)best_end;
+}
+
+/* Cost of an operation string with free ends: a leading insertion run costs
+ * gap(L - text_begin_free) beyond the free part (a leading deletion run
+ * likewise with pattern_begin_free), trailing runs with the end allowances;
+ * -1 if the string is not an alignment of pattern to text. */
+int64_t ora_cigar_cost_ends_free(const char* ops, int len, const char* pattern, int m, const char* text, int n,
+                                 int x, int o, int e, const ora_ends_t* ef) {
+  int v = 0, h = 0;
+  int64_t cost = 0;
+  for (int i = 0; i < len;) {
+    const char c = ops[i];
+    if (c == 'M' || c == 'X') {
+      if (v >= m || h >= n || (c == 'M') != (pattern[v] == text[h])) return -1;
+      if (c == 'X') cost += x;
+      ++v;
+      ++h;
+      ++i;
+      continue;
+    }
+    if (c != 'I' && c != 'D') return -1;
+    int j = i;
+    while (j < len && ops[j] == c) ++j;
+    int64_t L = j - i;
+    if (c == 'I') {
+      if (h + L > n) return -1;
+      h += (int)L;
+    } else {
+      if (v + L > m) return -1;
+      v += (int)L;
+    }
+    int64_t free_len = 0;  /* a run that is both first and last has both allowances */
+    if (i == 0) free_len += c == 'I' ? ef->text_begin_free : ef->pattern_begin_free;
+    if (j == len) free_len += c == 'I' ? ef->text_end_free : ef->pattern_end_free;
+    if (L > free_len) cost += (int64_t)o + (int64_t)e * (L - free_len);
+    i = j;
+  }
+  if (v != m || h != n) return -1;
+  return cost;
+}
+
 int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                            const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,
                            int threads) {
@@ -515,7 +655,8 @@ int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, cons
         ops_cap = ops ? need : 0;
       }
       int len = 0;
-      int r = ops ? align_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o, e, ops, ops_cap, &len, NULL)
+      int r = ops ? align_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o, e, &kEndToEnd, ops, ops_cap,
+                             &len, NULL)
                   : ORA_ENOMEM;
       scores[i] = r;
       if (r < 0) {

@@ -89,6 +89,28 @@ int ora_ops_to_rle(const char* ops, int len, uint32_t* runs, int cap);
 
 int ora_max_threads(void);
 
+/* Ends-free alignment (WFA2-lib's alignment_span = ends_free, set by
+ * wavefront_aligner_set_alignment_free_ends): the alignment may start at
+ * (v, 0) with v <= pattern_begin_free or (0, h) with h <= text_begin_free at
+ * no cost, and end at (m, h) with h >= n - text_end_free or (v, n) with v >=
+ * m - pattern_end_free.  All zero: end-to-end (ora_align).  The free end
+ * gaps are part of the operation string ('I' / 'D' runs) at no cost; of
+ * several ends at the optimal score the lowest diagonal k = h - v wins. */
+typedef struct {
+  int32_t pattern_begin_free, pattern_end_free, text_begin_free, text_end_free;
+} ora_ends_t;
+int ora_align_ends_free(const char* pattern, int m, const char* text, int n, int x, int o, int e,
+                        const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st);
+int ora_align_batch_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                              const int64_t* toff, const int32_t* tlen, int x, int o, int e, const ora_ends_t* ef,
+                              int32_t* scores, char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads);
+/* Independent Gotoh DP with the same free ends, and the cost of an
+ * operation string under them. */
+int ora_gotoh_ends_free_score(const char* pattern, int m, const char* text, int n, int x, int o, int e,
+                              const ora_ends_t* ef);
+int64_t ora_cigar_cost_ends_free(const char* ops, int len, const char* pattern, int m, const char* text, int n,
+                                 int x, int o, int e, const ora_ends_t* ef);
+
 /* Dual gap-affine (two-piece) mode, wfa_oracle2.c: a gap of length L costs
  * min(o1 + e1*L, o2 + e2*L).  Same return conventions as the one-piece
  * functions above. */

@@ -3,10 +3,11 @@
 // emulator.  Test infrastructure: compiled by tests/test_kernel_emu.py with
 // AddressSanitizer, it checks the kernels' indexing and outputs on the CPU.
 //
-// Input (stdin):  x o e o2 e2 cigar hint first_mode first_gw N
+// Input (stdin):  x o e o2 e2 pbf pef tbf tef cigar hint first_mode first_gw N
 //                 then N records "m n\n<pattern>\n<text>\n"
 //   o2 < 0: one gap piece; else dual gap-affine (the kModelDual kernels);
-//   o < 0: gap-linear with mismatch x and gap e per base (kModelLinear)
+//   o < 0: gap-linear with mismatch x and gap e per base (kModelLinear);
+//   pbf pef tbf tef: free ends (all 0: end-to-end)
 //   first_mode 1 = shared ring, 0 = global ring; first_gw = warps per pair
 //   of the first pass (1, 2, 4, 8, 16).  Retry passes follow the engine's
 //   ladder (tsu_plan.h next_pass).
@@ -68,10 +69,12 @@ static void run_pass(bool cigar, int mode, int gw, int threads, size_t smem, con
 }
 
 int main() {
-  int X, O, E, O2, E2, cigar, first_mode, first_gw;
+  int X, O, E, O2, E2, PBF, PEF, TBF, TEF, cigar, first_mode, first_gw;
   double hint;
   int64_t N;
-  if (!(std::cin >> X >> O >> E >> O2 >> E2 >> cigar >> hint >> first_mode >> first_gw >> N)) return 2;
+  if (!(std::cin >> X >> O >> E >> O2 >> E2 >> PBF >> PEF >> TBF >> TEF >> cigar >> hint >> first_mode >> first_gw >>
+        N))
+    return 2;
   std::vector<std::string> pats(N), txts(N);
   for (int64_t i = 0; i < N; ++i) {
     int m, n;
@@ -174,6 +177,10 @@ int main() {
     a.retry = retry.p;
     a.retry_count = retry_cnt;
     a.work = counters.p + 3;
+    a.ef_pb = PBF;
+    a.ef_pe = PEF;
+    a.ef_tb = TBF;
+    a.ef_te = TEF;
     const size_t smem = (size_t)groups * geo.group_smem;
     const int threads = geo.cta_threads;
     gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);

@@ -31,9 +31,10 @@ def emu():
     return EXE
 
 
-def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1):
+def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1, free=(0, 0, 0, 0)):
     o2, e2 = (pen[3], pen[4]) if len(pen) == 5 else (-1, 0)
-    hdr = f"{pen[0]} {pen[1]} {pen[2]} {o2} {e2} {int(cigar)} {hint} {int(shared_first)} {gw} {len(pairs)}\n"
+    hdr = (f"{pen[0]} {pen[1]} {pen[2]} {o2} {e2} {free[0]} {free[1]} {free[2]} {free[3]} {int(cigar)} {hint} "
+           f"{int(shared_first)} {gw} {len(pairs)}\n")
     body = b"".join(f"{len(p)} {len(t)}\n".encode() + p + b"\n" + t + b"\n" for p, t in pairs)
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1")
     r = subprocess.run([exe], input=hdr.encode() + body, capture_output=True, env=env, timeout=600)
@@ -125,9 +126,9 @@ def test_global_mode_and_retries(emu, oracle):
     """A tiny hint forces scratch overflow and several global-mode passes."""
     rng = random.Random(3)
     pairs = []
-    for _ in range(5):
-        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 160)))
-        t = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 160)))
+    for _ in range(3):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 120)))
+        t = "".join(rng.choice("ACGT") for _ in range(rng.randint(40, 120)))
         pairs.append((p, t))
     passes, retried, gws = check(emu, oracle, pairs, hint=0.0001)
     assert passes > 1 and retried > 0
@@ -250,7 +251,7 @@ def test_dual_warp_groups(emu, oracle, gw, shared):
 def test_dual_ladder(emu, oracle):
     """Wide dual wavefronts leave one warp's shared ring and climb the ladder."""
     rng = random.Random(9)
-    pairs = [_edited(rng, 400, 0.22)] + _long_indels(rng, 2, 200, 300)
+    pairs = [_edited(rng, 400, 0.22)] + _long_indels(rng, 1, 200, 300)
     passes, retried, gws = check_dual(emu, oracle, pairs, (4, 6, 2, 24, 1))
     assert passes > 1, gws
 
@@ -287,6 +288,51 @@ def test_linear_score_only_and_groups(emu, oracle):
 
 def test_linear_ladder(emu, oracle):
     rng = random.Random(12)
-    pairs = [_edited(rng, 800, 0.5)]  # edit distance 244: 489 diagonals > one warp's 384
+    # two unrelated 420 bp sequences: edit distance > 192, so more than one
+    # warp's 384 diagonals
+    pairs = [("".join(rng.choice("ACGT") for _ in range(420)), "".join(rng.choice("ACGT") for _ in range(420)))]
     passes, retried, gws = check_linear(emu, oracle, pairs, 1, 1)
     assert passes > 1, gws
+
+
+# --- free ends (gap-affine) --------------------------------------------------
+
+def check_ends_free(exe, oracle, pairs, free, pen=(4, 6, 2), **kw):
+    pairs = [(_b(p), _b(t)) for p, t in pairs]
+    got, passes, retried, gws = run_emu(exe, pairs, pen, free=free, **kw)
+    for (p, t), (s, ops) in zip(pairs, got):
+        es, eops = oracle.align_ends_free(p, t, free, *pen)
+        if kw.get("cigar", True):
+            assert (s, ops) == (es, eops), (p, t, free, s, es, ops, eops)
+        else:
+            assert s == es and ops == "", (p, t, free, s, es)
+    return passes, retried, gws
+
+
+def _flanked(rng, n, lo, hi):
+    """A core sequence with random flanks on the pattern and on the text."""
+    out = []
+    for _ in range(n):
+        core = "".join(rng.choice("ACGT") for _ in range(rng.randint(lo, hi)))
+        t = list(core)
+        for _ in range(len(core) // 20):
+            t[rng.randrange(len(t))] = rng.choice("ACGT")
+        fl = lambda: "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 30)))
+        out.append((fl() + core + fl(), fl() + "".join(t) + fl()))
+    return out
+
+
+@pytest.mark.parametrize("free", [(0, 0, 0, 0), (30, 30, 30, 30), (0, 0, 40, 40), (40, 40, 0, 0), (5, 0, 0, 12),
+                                  (1000, 1000, 1000, 1000)])
+def test_ends_free_random(emu, oracle, free):
+    rng = random.Random(sum(free) + 1)
+    pairs = _flanked(rng, 16, 0, 150) + [("", ""), ("", "ACGT"), ("ACG", ""), ("ACGTNNACGT", "ACGTACGT")]
+    check_ends_free(emu, oracle, pairs, free)
+
+
+def test_ends_free_groups_and_score_only(emu, oracle):
+    rng = random.Random(31)
+    pairs = _flanked(rng, 4, 200, 400)
+    check_ends_free(emu, oracle, pairs, (50, 50, 50, 50), cigar=False)
+    for gw, shared in [(4, True), (8, False)]:
+        check_ends_free(emu, oracle, pairs, (50, 50, 50, 50), shared_first=shared, gw=gw)

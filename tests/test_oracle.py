@@ -187,3 +187,54 @@ def test_linear_batch_matches_single(oracle):
     sc, cg = oracle.align_batch_linear(pats, txts, 2, 1, threads=4)
     for i in range(40):
         assert (sc[i], cg[i]) == oracle.align_linear(pats[i], txts[i], 2, 1)
+
+
+# --- ends-free gap-affine ----------------------------------------------------
+
+FREES = [(0, 0, 0, 0), (5, 5, 5, 5), (100, 100, 0, 0), (0, 0, 100, 100), (3, 0, 0, 7), (0, 9, 2, 0),
+         (1000, 1000, 1000, 1000)]
+
+
+def test_ends_free_known_answers(oracle):
+    pen = (4, 6, 2)
+    # the pattern inside the text: the text's flanks are free insertions
+    assert oracle.align_ends_free("ACGTTGCA", "GGGACGTTGCATT", (0, 0, 3, 2), *pen) == (0, "IIIMMMMMMMMII")
+    # flanks longer than allowed cost the excess as one gap: 2 free + gap(1)
+    s, ops = oracle.align_ends_free("ACGTTGCA", "GGGACGTTGCA", (0, 0, 2, 0), *pen)
+    assert s == 8 and ops == "IIIMMMMMMMM"
+    # the text inside the pattern: free deletions
+    assert oracle.align_ends_free("TTACGTAA", "ACGT", (2, 2, 0, 0), *pen) == (0, "DDMMMMDD")
+    # overlap (suffix of the pattern = prefix of the text)
+    assert oracle.align_ends_free("GGGGACGT", "ACGTCCCC", (4, 0, 0, 4), *pen) == (0, "DDDDMMMMIIII")
+    # all zero: end-to-end
+    assert oracle.align_ends_free("ACGT", "AGGT", (0, 0, 0, 0), *pen) == oracle.align("ACGT", "AGGT", *pen)
+
+
+@pytest.mark.parametrize("free", FREES)
+def test_ends_free_random_vs_dp(oracle, free):
+    rng = random.Random(hash(free) & 0xFFFF)
+    pen = (4, 6, 2)
+    for it in range(200):
+        alpha = "ACGT" if it % 3 else "AC"
+        core = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 40)))
+        p = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 8))) + core + \
+            "".join(rng.choice(alpha) for _ in range(rng.randint(0, 8)))
+        t = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 8))) + core + \
+            "".join(rng.choice(alpha) for _ in range(rng.randint(0, 8)))
+        if it % 4 == 0:
+            t = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 40)))
+        s, ops = oracle.align_ends_free(p, t, free, *pen)
+        assert s == oracle.gotoh_ends_free(p, t, free, *pen), (p, t, free)
+        assert oracle.cigar_cost_ends_free(ops, p, t, free, *pen) == s, (p, t, free, ops)
+        if free == (0, 0, 0, 0):
+            assert (s, ops) == oracle.align(p, t, *pen)
+
+
+def test_ends_free_batch_matches_single(oracle):
+    rng = random.Random(17)
+    pats = ["".join(rng.choice("ACGT") for _ in range(rng.randint(0, 120))) for _ in range(40)]
+    txts = [p[rng.randint(0, 10):] + "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 10))) for p in pats]
+    free = (10, 10, 10, 10)
+    sc, cg = oracle.align_batch_ends_free(pats, txts, free, threads=4)
+    for i in range(40):
+        assert (sc[i], cg[i]) == oracle.align_ends_free(pats[i], txts[i], free)

@@ -250,6 +250,15 @@ class Aligner:
         lib().tsu_get_timing(self._h, ctypes.byref(t))
         return {f: getattr(t, f) for f, _ in Timing._fields_}
 
+    def set_ends_free(self, pattern_begin_free: int = 0, pattern_end_free: int = 0, text_begin_free: int = 0,
+                      text_end_free: int = 0) -> None:
+        """Ends-free alignment for the later calls (tsu_set_ends_free; WFA2-lib's
+        wavefront_aligner_set_alignment_free_ends).  All 0: end-to-end."""
+        L = lib()
+        L.tsu_set_ends_free.argtypes = [c_vp, c_i32, c_i32, c_i32, c_i32]
+        self._check(L.tsu_set_ends_free(self._h, pattern_begin_free, pattern_end_free, text_begin_free,
+                                        text_end_free))
+
     def pass_log(self) -> str:
         """Align passes of the last call: mode+warps per pair x groups : pairs @ time."""
         L = lib()

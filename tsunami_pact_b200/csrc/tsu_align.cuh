@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       if (m > kDualMaxLen || n > kDualMaxLen) st = kPairInternal;  // beyond the backtrace word
     }
     int s_end = -1;
+    int k_fin = k_end;  // end diagonal (free ends: the lowest that ends)
     int64_t hbase = 0;
     unsigned long long n_cells = 0, n_steps = 0;
 
@@ -177,7 +178,8 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           ring[idx] = v;
       };
       // ---- score 0: M[0] = {k = 0: offset 0}, extended (wfa_gpu.cu:239-242)
-      {
+      const int lo0 = -min(a.ef_pb, m), hi0 = min(a.ef_tb, n);
+      if (lo0 == hi0) {
         if (gt == 0) {
           const int rem = m < n ? m : n;
           const int32_t o0 =
@@ -196,12 +198,59 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         const int32_t o0 = bc[1];
         hbase = 1;
         n_cells = n_steps = 1;
-        if (k_end == 0 && o0 >= n) s_end = 0;
+        if (o0 >= n && (k_end == 0 || (a.ef_pe >= m - o0))) {
+          s_end = 0;
+          k_fin = 0;
+        } else if (a.ef_te > 0 && o0 >= m && o0 >= n - a.ef_te) {
+          s_end = 0;
+          k_fin = 0;
+        }
+      } else if (hi0 - lo0 + 1 > W || (kCigar && hi0 - lo0 + 1 > a.hist_cap)) {
+        st = kPairScratch;
+      } else {
+        // free beginnings: diagonals -pattern_begin_free..text_begin_free at
+        // offset max(k, 0), each extended; the lowest ending diagonal wins
+        int fk = INT_MAX;
+        for (int k = lo0 + gt; k <= hi0; k += GT) {
+          const int32_t p0 = k > 0 ? k : 0;
+          const int vv = p0 - k;
+          const int rem = min(m - vv, n - p0);
+          const int32_t om =
+              p0 + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p0, rem) : lcp16(P, vv, T, p0, rem));
+          store(k - lo0, om);
+          if (kCigar) hist[k - lo0] = (uint32_t)p0 << (kDual ? 8 : 4);
+          const int ov = om - k;
+          if (fk == INT_MAX && ((om >= n && ov >= m - a.ef_pe) || (ov >= m && om >= n - a.ef_te))) fk = k;
+        }
+        fk = __reduce_min_sync(FULL, fk);
+        if constexpr (GW > 1) {
+          if (lane == 0) part[wig * PW + 6] = fk;
+          group_sync<GW>(gid);
+          fk = __reduce_min_sync(FULL, lane < GW ? part[lane * PW + 6] : INT_MAX);
+        }
+        s_lo[0] = lo0;
+        s_hi[0] = hi0;
+        s_alo[0] = lo0;
+        if (kCigar && gt == 0) table[0] = make_int2(lo0, 0);
+        hbase = hi0 - lo0 + 1;
+        n_cells = (unsigned long long)(hi0 - lo0 + 1);
+        n_steps = 1;
+        if (fk != INT_MAX) {
+          s_end = 0;
+          k_fin = fk;
+        }
+        if constexpr (GW == 1) __syncwarp();
       }
 
       int s = 0;
       int slm = 0, sli = 0, sli2 = 0;  // s mod rm, s mod re, s mod re2
-      while (s_end < 0) {
+      // ends of free-ended alignments: text consumed with at most ef_pe
+      // pattern characters left (k <= k_end + ef_pe), or the pattern with at
+      // most ef_te text characters left; end-to-end: k_end at offset n
+      const int k_hi = k_end + a.ef_pe;
+      const bool free_te = a.ef_te > 0;
+      const int n_te = n - a.ef_te;
+      while (s_end < 0 && st == kPairOk) {
         ++s;
         if (++slm == rm) slm = 0;
         if constexpr (!kLin) {
@@ -300,7 +349,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         uint32_t* hrow = kCigar ? hist + hbase - lo : nullptr;
         int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
         int fi2 = INT_MAX, li2 = INT_MIN, fd2 = INT_MAX, ld2 = INT_MIN;
-        bool found = false;
+        int fk = INT_MAX;  // lowest ending diagonal of this thread
         for (int k = lo + gt; k <= hi; k += GT) {
           int j;
           j = k - 1 - lo_mo;
@@ -359,7 +408,9 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             om = p + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem));
             fm = min(fm, k);
             lm = k;
-            found |= (k == k_end) & (om >= n);
+            bool ends = (om >= n) & (k <= k_hi);
+            if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
+            if (ends) fk = min(fk, k);
           }
           store(w_m + k, om);
           if (i_present) {
@@ -388,7 +439,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         li = __reduce_max_sync(FULL, li);
         fd = __reduce_min_sync(FULL, fd);
         ld = __reduce_max_sync(FULL, ld);
-        bool any_found = __any_sync(FULL, found);
+        fk = __reduce_min_sync(FULL, fk);
         if constexpr (kDual) {
           fi2 = __reduce_min_sync(FULL, fi2);
           li2 = __reduce_max_sync(FULL, li2);
@@ -398,7 +449,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         if constexpr (GW > 1) {
           int* pp = part + ((s & 1) * GW + wig) * PW;
           if (lane == 0) {
-            pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = any_found;
+            pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = fk;
             if constexpr (kDual) {
               pp[7] = fi2; pp[8] = li2; pp[9] = fd2; pp[10] = ld2;
             }
@@ -406,7 +457,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           group_sync<GW>(gid);  // the step's ring writes and partials are complete
           // lane w takes warp w's partials; warp reductions combine them
           // (7 loads and 7 reductions per thread instead of 7 * GW)
-          int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = 0;
+          int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = INT_MAX;
           int p7 = INT_MAX, p8 = INT_MIN, p9 = INT_MAX, p10 = INT_MIN;
           if (lane < GW) {
             const int* qw = part + ((s & 1) * GW + lane) * PW;
@@ -421,7 +472,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           li = __reduce_max_sync(FULL, p3);
           fd = __reduce_min_sync(FULL, p4);
           ld = __reduce_max_sync(FULL, p5);
-          any_found = __any_sync(FULL, p6 != 0);
+          fk = __reduce_min_sync(FULL, p6);
           if constexpr (kDual) {
             fi2 = __reduce_min_sync(FULL, p7);
             li2 = __reduce_max_sync(FULL, p8);
@@ -450,7 +501,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         n_cells += (unsigned long long)width;
         ++n_steps;
         if constexpr (GW == 1) __syncwarp();
-        if (any_found) s_end = s;
+        if (fk != INT_MAX) {
+          s_end = s;
+          k_fin = fk;
+        }
       }
     }
 
@@ -459,7 +513,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       if (kCigar) {
         // reserve the run bound 2*s/min_pen + 1 in the arena, then walk
         const int min_pen = a.pen.min_pen();
-        const int64_t bound = 2 * (int64_t)s_end / min_pen + 1;
+        const int64_t bound = 2 * (int64_t)s_end / min_pen + 3;  // + a free gap at each end
         if (gt == 0) {
           int32_t len = 0;
           int64_t pos = 0;
@@ -469,10 +523,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           } else {
             int r;
             if constexpr (kDual)
-              r = backtrace_walk_dual(hist, hbase, table, s_end, m, n, a.pen, a.arena + at + bound, (int)bound);
+              r = backtrace_walk_dual(hist, hbase, table, s_end, k_fin, m, n, a.pen, a.arena + at + bound,
+                                      (int)bound);
             else
-              r = backtrace_walk(hist, hbase, table, s_end, m, n, a.pen.x, a.pen.go, a.pen.ge, a.arena + at + bound,
-                                 (int)bound);
+              r = backtrace_walk(hist, hbase, table, s_end, k_fin, m, n, a.pen.x, a.pen.go, a.pen.ge,
+                                 a.arena + at + bound, (int)bound);
             if (r < 0) {
               st = kPairInternal;
             } else {

@@ -38,15 +38,21 @@ struct RunWriter {
   }
 };
 
+// The walk starts on the end diagonal k_end (n - m end-to-end; with free
+// ends the diagonal the kernel found), at offset min(n, m + k_end): the text
+// or the pattern is consumed there, and the rest of the other is the free
+// trailing gap, written first.
 // Returns the number of runs, or -1 on an inconsistency (a word outside the
 // history, a predecessor beyond the current offset, more runs than cap).
 static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
-                              int s_end, int m, int n, int x, int go, int ge, uint32_t* out_end, int cap) {
+                              int s_end, int k_end, int m, int n, int x, int go, int ge, uint32_t* out_end, int cap) {
   RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
   enum { M = 0, I = 1, D = 2 };
-  int state = M, s = s_end, k = n - m;
-  int32_t off = n;
+  int state = M, s = s_end, k = k_end;
+  int32_t off = min(n, m + k_end);
   int v = off - k, h = off;
+  w.put(kOpD, m - v);
+  w.put(kOpI, n - h);
   int guard = 4 * (m + n) + 8;
   while (v > 0 && h > 0 && s > 0) {
     if (--guard < 0) return -1;
@@ -128,14 +134,16 @@ static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t 
 // bit (kI1Ext2 ... kD2Ext2) then says open (back to M, s - o_j - e_j) or
 // extend (stay, s - e_j).  Same return convention as backtrace_walk.
 static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int64_t hist_used,
-                                          const int2* __restrict__ table, int s_end, int m, int n, const Pen& pen,
-                                          uint32_t* out_end, int cap) {
+                                          const int2* __restrict__ table, int s_end, int k_end, int m, int n,
+                                          const Pen& pen, uint32_t* out_end, int cap) {
   RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
   // state = M source code of the component being walked (kSrcMis for M)
   uint32_t state = kSrcMis;
-  int s = s_end, k = n - m;
-  int32_t off = n;
+  int s = s_end, k = k_end;
+  int32_t off = min(n, m + k_end);
   int v = off - k, h = off;
+  w.put(kOpD, m - v);
+  w.put(kOpI, n - h);
   int guard = 4 * (m + n) + 8;
   while (v > 0 && h > 0 && s > 0) {
     if (--guard < 0) return -1;

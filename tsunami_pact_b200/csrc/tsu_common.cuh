@@ -151,6 +151,10 @@ struct AlignArgs {
   int32_t* retry;        // [n] pairs to re-run with more scratch / arena
   unsigned int* retry_count;
   unsigned long long* work;  // [2]: wavefront cells computed, score steps
+  // free ends (all 0: end-to-end): starts (v, 0), v <= ef_pb, and (0, h),
+  // h <= ef_tb, cost nothing, and so do ends (m, h), h >= n - ef_te, and
+  // (v, n), v >= m - ef_pe
+  int32_t ef_pb, ef_pe, ef_tb, ef_te;
 };
 
 // Warp partials per warp and step parity: 7 (one piece) or 11 values.

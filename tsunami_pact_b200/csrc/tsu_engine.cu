@@ -105,6 +105,9 @@ struct tsu_ctx {
   cudaEvent_t bev[2 * tsu::kBands] = {};  // first pass of each band: start, end
   cudaEvent_t wait_ev = nullptr;  // blocking-sync event of those waits
   size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
+  // free ends (tsu_set_ends_free): pattern begin, pattern end, text begin,
+  // text end; all 0: end-to-end
+  int32_t ends_free[4] = {0, 0, 0, 0};
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
             &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
@@ -625,6 +628,10 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     a.retry = retry;
     a.retry_count = a.queue + 1;
     a.work = d_work;
+    a.ef_pb = ctx->ends_free[0];
+    a.ef_pe = ctx->ends_free[1];
+    a.ef_tb = ctx->ends_free[2];
+    a.ef_te = ctx->ends_free[3];
     return a;
   };
   std::string passlog;  // mode, warps per pair x groups : pairs @ time, per pass (for error messages)
@@ -1405,6 +1412,27 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
     CU(cudaMemcpy(hs.data(), d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
   }
   return collect_status(ctx, hs.data(), n);
+}
+
+int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_end_free, int32_t text_begin_free,
+                      int32_t text_end_free) {
+  if (!ctx) return TSU_EINVAL;
+  if (pattern_begin_free < 0 || pattern_end_free < 0 || text_begin_free < 0 || text_end_free < 0)
+    return set_err(ctx, TSU_EINVAL, "negative free end");
+  if (ctx->spec.metric != TSU_METRIC_GAP_AFFINE &&
+      (pattern_begin_free | pattern_end_free | text_begin_free | text_end_free))
+    return set_err(ctx, TSU_EINVAL, "free ends need a gap-affine context");
+  ctx->ends_free[0] = pattern_begin_free;
+  ctx->ends_free[1] = pattern_end_free;
+  ctx->ends_free[2] = text_begin_free;
+  ctx->ends_free[3] = text_end_free;
+  return TSU_OK;
+}
+
+int tsu_get_ends_free(const tsu_ctx* ctx, int32_t* out4) {
+  if (!ctx || !out4) return TSU_EINVAL;
+  for (int i = 0; i < 4; ++i) out4[i] = ctx->ends_free[i];
+  return TSU_OK;
 }
 
 int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair) {
