@@ -42,6 +42,7 @@ WORKLOADS = {
 }
 PEN = (4, 6, 2)  # --penalties; five values (open2, extend2 last): dual gap-affine
 METRIC_NAME = None  # --metric edit | indel | gap_linear (PEN then (mismatch, gap_extension))
+ENDS_FREE = (0, 0, 0, 0)  # --ends-free pattern_begin,pattern_end,text_begin,text_end (gap-affine)
 LINEAR_XE = {"edit": (1, 1), "indel": (3, 1)}  # the gap-linear penalties of these metrics
 
 
@@ -54,7 +55,8 @@ def pen_str() -> str:
         return METRIC_NAME + " distance"
     if METRIC_NAME == "gap_linear":
         return "gap-linear %d/%d" % PEN[:2]
-    return "/".join(str(v) for v in PEN) + (" (dual gap-affine)" if len(PEN) == 5 else "")
+    ef = ", free ends %d/%d/%d/%d" % ENDS_FREE if any(ENDS_FREE) else ""
+    return "/".join(str(v) for v in PEN) + (" (dual gap-affine)" if len(PEN) == 5 else "") + ef
 
 
 def make_aligner(T, **kw):
@@ -64,12 +66,18 @@ def make_aligner(T, **kw):
     if METRIC_NAME == "gap_linear":
         return T.Aligner(PEN[0], 0, PEN[1], metric="gap_linear", **kw)
     dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
-    return T.Aligner(*PEN[:3], **dual_kw, **kw)
+    al = T.Aligner(*PEN[:3], **dual_kw, **kw)
+    if any(ENDS_FREE):
+        al.set_ends_free(*ENDS_FREE)
+    return al
 
 
 def oracle_batch(O, pbuf, poff, plen, tbuf, toff, tlen, threads):
     """The oracle over the bench's penalties (one or two gap pieces, or a
     gap-linear metric)."""
+    if any(ENDS_FREE):
+        return O.align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, ENDS_FREE, *PEN, cigar=True,
+                                              threads=threads)
     if METRIC_NAME is not None:
         return O.align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, *linear_xe(), cigar=True,
                                            threads=threads)
@@ -356,8 +364,13 @@ def main():
                     help="mismatch,open,extend[,open2,extend2]: five values align with dual gap-affine penalties")
     ap.add_argument("--metric", default=None, choices=["edit", "indel", "gap_linear"],
                     help="a gap-linear metric instead of gap-affine (gap_linear: --penalties mismatch,extend)")
+    ap.add_argument("--ends-free", default="0,0,0,0",
+                    help="pattern_begin,pattern_end,text_begin,text_end free lengths (gap-affine)")
     args = ap.parse_args()
-    global PEN, METRIC_NAME
+    global PEN, METRIC_NAME, ENDS_FREE
+    ENDS_FREE = tuple(int(v) for v in args.ends_free.split(","))
+    if len(ENDS_FREE) != 4:
+        raise SystemExit("--ends-free takes 4 values")
     PEN = tuple(int(v) for v in args.penalties.split(","))
     METRIC_NAME = args.metric
     if METRIC_NAME == "gap_linear" and args.penalties == "4,6,2":

@@ -349,6 +349,11 @@ def align_batch_ends_free(patterns: Sequence, texts: Sequence, free, x=4, o=6, e
     np.cumsum(tlen, out=toff[1:])
     pbuf = np.frombuffer(b"".join(pats) + b"\0", dtype=np.uint8)
     tbuf = np.frombuffer(b"".join(txts) + b"\0", dtype=np.uint8)
+    return align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, free, x, o, e, cigar, threads)
+
+
+def align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, free, x=4, o=6, e=2, cigar=True, threads=0):
+    n = len(plen)
     scores = np.zeros(n, dtype=np.int32)
     ops = ops_off = ops_len = None
     if cigar:
