@@ -51,22 +51,23 @@ def linear_xe():
 
 
 def pen_str() -> str:
-    if METRIC_NAME in LINEAR_XE:
-        return METRIC_NAME + " distance"
-    if METRIC_NAME == "gap_linear":
-        return "gap-linear %d/%d" % PEN[:2]
     ef = ", free ends %d/%d/%d/%d" % ENDS_FREE if any(ENDS_FREE) else ""
+    if METRIC_NAME in LINEAR_XE:
+        return METRIC_NAME + " distance" + ef
+    if METRIC_NAME == "gap_linear":
+        return "gap-linear %d/%d" % PEN[:2] + ef
     return "/".join(str(v) for v in PEN) + (" (dual gap-affine)" if len(PEN) == 5 else "") + ef
 
 
 def make_aligner(T, **kw):
-    """An engine context over the bench's penalties or metric."""
+    """An engine context over the bench's penalties or metric (and free ends)."""
     if METRIC_NAME in LINEAR_XE:
-        return T.Aligner(metric=METRIC_NAME, **kw)
-    if METRIC_NAME == "gap_linear":
-        return T.Aligner(PEN[0], 0, PEN[1], metric="gap_linear", **kw)
-    dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
-    al = T.Aligner(*PEN[:3], **dual_kw, **kw)
+        al = T.Aligner(metric=METRIC_NAME, **kw)
+    elif METRIC_NAME == "gap_linear":
+        al = T.Aligner(PEN[0], 0, PEN[1], metric="gap_linear", **kw)
+    else:
+        dual_kw = {"gap_opening2": PEN[3], "gap_extension2": PEN[4]} if len(PEN) == 5 else {}
+        al = T.Aligner(*PEN[:3], **dual_kw, **kw)
     if any(ENDS_FREE):
         al.set_ends_free(*ENDS_FREE)
     return al
@@ -74,10 +75,16 @@ def make_aligner(T, **kw):
 
 def oracle_batch(O, pbuf, poff, plen, tbuf, toff, tlen, threads):
     """The oracle over the bench's penalties (one or two gap pieces, or a
-    gap-linear metric)."""
+    gap-linear metric; free ends when set)."""
     if any(ENDS_FREE):
-        return O.align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, ENDS_FREE, *PEN, cigar=True,
-                                              threads=threads)
+        if METRIC_NAME is None and len(PEN) == 3:
+            return O.align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, ENDS_FREE, *PEN, cigar=True,
+                                                  threads=threads)
+        pats = [bytes(pbuf[poff[i]:poff[i] + plen[i]]) for i in range(len(plen))]
+        txts = [bytes(tbuf[toff[i]:toff[i] + tlen[i]]) for i in range(len(tlen))]
+        if METRIC_NAME is not None:
+            return O.align_batch_linear_ends_free(pats, txts, ENDS_FREE, *linear_xe(), threads=threads)
+        return O.align_batch2_ends_free(pats, txts, ENDS_FREE, *PEN, threads=threads)
     if METRIC_NAME is not None:
         return O.align_batch_linear_arrays(pbuf, poff, plen, tbuf, toff, tlen, *linear_xe(), cigar=True,
                                            threads=threads)

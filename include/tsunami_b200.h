@@ -189,8 +189,10 @@ int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair);
  * at no cost, and end at (m, h) with h >= n - text_end_free or at (v, n) with
  * v >= m - pattern_end_free.  The free end gaps stay in the CIGAR as I / D
  * runs (costing 0); of several ends at the optimal score the lowest diagonal
- * h - v wins.  All 0 (the default): end-to-end.  Gap-affine contexts only
- * (TSU_EINVAL otherwise); applies to the context's later align calls. */
+ * h - v wins.  All 0 (the default): end-to-end.  Every metric (gap-affine,
+ * dual gap-affine, gap-linear, edit, indel -- e.g. semi-global edit distance
+ * of a read against a longer region); applies to the context's later align
+ * calls. */
 int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_end_free, int32_t text_begin_free,
                       int32_t text_end_free);
 int tsu_get_ends_free(const tsu_ctx* ctx, int32_t* out4);

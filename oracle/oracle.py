@@ -99,6 +99,22 @@ def lib():
         L.ora_cigar_cost_ends_free.restype = i64
         L.ora_cigar_cost_ends_free.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, c_char_p,
                                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(OraEnds)]
+        L.ora_align_linear_ends_free.restype = ctypes.c_int
+        L.ora_align_linear_ends_free.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, P(OraEnds), ctypes.c_void_p, ctypes.c_int,
+                                                 P(ctypes.c_int), P(OraStats)]
+        L.ora_align_batch_linear_ends_free.restype = ctypes.c_int
+        L.ora_align_batch_linear_ends_free.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 2 + [
+            P(OraEnds)] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.ora_align2_ends_free.restype = ctypes.c_int
+        L.ora_align2_ends_free.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 5 + [
+            P(OraEnds), ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(OraStats)]
+        L.ora_align_batch2_ends_free.restype = ctypes.c_int
+        L.ora_align_batch2_ends_free.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
+            P(OraEnds)] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.ora_gotoh2_ends_free_score.restype = ctypes.c_int
+        L.ora_gotoh2_ends_free_score.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [
+            ctypes.c_int] * 5 + [P(OraEnds)]
         L.ora_align_batch2.restype = ctypes.c_int
         L.ora_align_batch2.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
@@ -374,3 +390,75 @@ def align_batch_ends_free_arrays(pbuf, poff, plen, tbuf, toff, tlen, free, x=4, 
         raw = ops.tobytes()
         cig = [raw[ops_off[i]: ops_off[i] + ops_len[i]].decode() for i in range(n)]
     return scores, cig
+
+
+# --- free ends for the gap-linear and dual gap-affine oracles ------------------
+
+def align_linear_ends_free(pattern, text, free, x=1, e=1, cigar=True):
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap) if cigar else None
+    n_ops = ctypes.c_int(0)
+    r = lib().ora_align_linear_ends_free(p, len(p), t, len(t), x, e, ctypes.byref(OraEnds(*free)), buf, cap,
+                                         ctypes.byref(n_ops), None)
+    if r < 0:
+        raise RuntimeError(f"oracle error {r}")
+    return r, (buf.raw[: n_ops.value].decode() if cigar else None)
+
+
+def align2_ends_free(pattern, text, free, x=4, o1=6, e1=2, o2=24, e2=1, cigar=True):
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap) if cigar else None
+    n_ops = ctypes.c_int(0)
+    r = lib().ora_align2_ends_free(p, len(p), t, len(t), x, o1, e1, o2, e2, ctypes.byref(OraEnds(*free)), buf, cap,
+                                   ctypes.byref(n_ops), None)
+    if r < 0:
+        raise RuntimeError(f"oracle error {r}")
+    return r, (buf.raw[: n_ops.value].decode() if cigar else None)
+
+
+def gotoh2_ends_free(pattern, text, free, x=4, o1=6, e1=2, o2=24, e2=1) -> int:
+    p, t = _b(pattern), _b(text)
+    return lib().ora_gotoh2_ends_free_score(p, len(p), t, len(t), x, o1, e1, o2, e2, ctypes.byref(OraEnds(*free)))
+
+
+def _batch_free(fn, patterns, texts, pen, free, cigar, threads):
+    pats = [_b(p) for p in patterns]
+    txts = [_b(t) for t in texts]
+    n = len(pats)
+    plen = np.array([len(p) for p in pats], dtype=np.int32)
+    tlen = np.array([len(t) for t in txts], dtype=np.int32)
+    poff = np.zeros(n + 1, dtype=np.int64)
+    toff = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(plen, out=poff[1:])
+    np.cumsum(tlen, out=toff[1:])
+    pbuf = np.frombuffer(b"".join(pats) + b"\0", dtype=np.uint8)
+    tbuf = np.frombuffer(b"".join(txts) + b"\0", dtype=np.uint8)
+    scores = np.zeros(n, dtype=np.int32)
+    ops = ops_off = ops_len = None
+    if cigar:
+        caps = plen.astype(np.int64) + tlen.astype(np.int64) + 1
+        ops_off = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(caps, out=ops_off[1:])
+        ops = np.zeros(int(ops_off[-1]) + 1, dtype=np.uint8)
+        ops_len = np.zeros(n, dtype=np.int32)
+    r = fn(n, pbuf.ctypes.data, poff.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, toff.ctypes.data,
+           tlen.ctypes.data, *pen, ctypes.byref(OraEnds(*free)), scores.ctypes.data,
+           ops.ctypes.data if cigar else None, ops_off.ctypes.data if cigar else None,
+           ops_len.ctypes.data if cigar else None, threads)
+    if r < 0:
+        raise RuntimeError(f"oracle batch error {r}")
+    cig: Optional[List[str]] = None
+    if cigar:
+        raw = ops.tobytes()
+        cig = [raw[ops_off[i]: ops_off[i] + ops_len[i]].decode() for i in range(n)]
+    return scores, cig
+
+
+def align_batch_linear_ends_free(patterns, texts, free, x=1, e=1, cigar=True, threads=0):
+    return _batch_free(lib().ora_align_batch_linear_ends_free, patterns, texts, (x, e), free, cigar, threads)
+
+
+def align_batch2_ends_free(patterns, texts, free, x=4, o1=6, e1=2, o2=24, e2=1, cigar=True, threads=0):
+    return _batch_free(lib().ora_align_batch2_ends_free, patterns, texts, (x, o1, e1, o2, e2), free, cigar, threads)

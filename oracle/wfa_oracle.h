@@ -132,6 +132,24 @@ int ora_align_batch_linear(int npairs, const char* pat, const int64_t* poff, con
                            const int64_t* toff, const int32_t* tlen, int x, int e, int32_t* scores, char* ops,
                            const int64_t* ops_off, int32_t* ops_len, int nthreads);
 
+/* Free ends for the gap-linear and dual gap-affine oracles (same semantics
+ * as ora_align_ends_free; the gap-linear scores are the gap-affine ones with
+ * opening 0, so ora_gotoh_ends_free_score pins them). */
+int ora_align_linear_ends_free(const char* pattern, int m, const char* text, int n, int x, int e,
+                               const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st);
+int ora_align_batch_linear_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen,
+                                     const char* txt, const int64_t* toff, const int32_t* tlen, int x, int e,
+                                     const ora_ends_t* ef, int32_t* scores, char* ops, const int64_t* ops_off,
+                                     int32_t* ops_len, int nthreads);
+int ora_align2_ends_free(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2,
+                         const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st);
+int ora_align_batch2_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                               const int64_t* toff, const int32_t* tlen, int x, int o1, int e1, int o2, int e2,
+                               const ora_ends_t* ef, int32_t* scores, char* ops, const int64_t* ops_off,
+                               int32_t* ops_len, int nthreads);
+int ora_gotoh2_ends_free_score(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2,
+                               int e2, const ora_ends_t* ef);
+
 /* CPU-check plugin for the wfa_gpu command line (TSU_CHECK_LIB). */
 int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                            const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,

@@ -208,7 +208,8 @@ static inline int64_t bsrc(const ws2_t* ws, const wf2_t* w, int k, int delta, in
   return pb2(ws->arena[w->base + (k - w->alo)] + delta, type);
 }
 
-static int w2_backtrace(ws2_t* ws, int s_end, int x, int o1, int e1, int o2, int e2, int m, int n, int* start) {
+static int w2_backtrace(ws2_t* ws, int s_end, int k_end, int x, int o1, int e1, int o2, int e2, int m, int n,
+                        int* start) {
   const int cap = m + n + 1;
   if (ws->opbuf_cap < cap) {
     char* nb = (char*)realloc(ws->opbuf, (size_t)cap);
@@ -223,9 +224,11 @@ static int w2_backtrace(ws2_t* ws, int s_end, int x, int o1, int e1, int o2, int
     if (pos < 0) return ORA_ECIGCAP; \
     ops[pos--] = (c);                \
   } while (0)
-  int state = C_M, s = s_end, k = n - m;
-  int32_t off = n;
+  int state = C_M, s = s_end, k = k_end;
+  int32_t off = w2_get(ws, &ws->w[C_M][s_end], k_end);
   int v = off - k, h = off;
+  for (int i = v; i < m; ++i) EMIT('D');  /* free trailing gap */
+  for (int i = h; i < n; ++i) EMIT('I');
   while (v > 0 && h > 0 && s > 0) {
     const wf2_t* wmm = src(ws, C_M, s - x);
     const wf2_t* wo1 = src(ws, C_M, s - o1 - e1);
@@ -290,7 +293,7 @@ static int w2_backtrace(ws2_t* ws, int s_end, int x, int o1, int e1, int o2, int
 }
 
 static int align2_ws(ws2_t* ws, const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2,
-                     int e2, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
+                     int e2, const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
   if (m < 0 || n < 0 || x <= 0 || o1 < 0 || e1 <= 0 || o2 < 0 || e2 <= 0) return ORA_EINVAL;
   const unsigned char* p = (const unsigned char*)pattern;
   const unsigned char* t = (const unsigned char*)text;
@@ -300,23 +303,37 @@ static int align2_ws(ws2_t* ws, const char* pattern, int m, const char* text, in
     memset(&ws->w[c][0], 0, sizeof(wf2_t));
     ws->w[c][0].lo = 1;
   }
+  /* score 0: diagonal 0, or every free start (as in the gap-affine oracle) */
+  const int lo0 = -(ef->pattern_begin_free < m ? ef->pattern_begin_free : m);
+  const int hi0 = ef->text_begin_free < n ? ef->text_begin_free : n;
   wf2_t* M0 = &ws->w[C_M][0];
-  const int64_t b0 = ws2_alloc(ws, 1);
+  const int64_t b0 = ws2_alloc(ws, hi0 - lo0 + 1);
   if (b0 < 0) return ORA_ENOMEM;
   M0->present = 1;
-  M0->lo = M0->hi = M0->alo = M0->ahi = 0;
+  M0->lo = M0->alo = lo0;
+  M0->hi = M0->ahi = hi0;
   M0->base = b0;
-  ws->arena[b0] = 0;
+  for (int k = lo0; k <= hi0; ++k) ws->arena[b0 + (k - lo0)] = k > 0 ? k : 0;
   if (st) {
     st->steps++;
-    st->cells += 1;
+    st->cells += hi0 - lo0 + 1;
   }
-  const int k_end = n - m;
-  int s = 0;
+  int s = 0, k_end = INT_MIN;
   for (;;) {
     w2_extend(ws, s, p, m, t, n, st);
     const wf2_t* M = &ws->w[C_M][s];
-    if (!w2_null(M) && k_end >= M->lo && k_end <= M->hi && w2_get(ws, M, k_end) >= n) break;
+    k_end = INT_MIN;
+    if (!w2_null(M))
+      for (int k = M->lo; k <= M->hi; ++k) {  /* lowest ending diagonal */
+        const int32_t off = w2_get(ws, M, k);
+        if (off == ONULL2) continue;
+        const int v = off - k;
+        if ((off >= n && v >= m - ef->pattern_end_free) || (v >= m && off >= n - ef->text_end_free)) {
+          k_end = k;
+          break;
+        }
+      }
+    if (k_end != INT_MIN) break;
     ++s;
     if (ws2_reserve(ws, s + 1)) return ORA_ENOMEM;
     const int rc = w2_compute(ws, s, x, o1, e1, o2, e2, m, n, st);
@@ -325,7 +342,7 @@ static int align2_ws(ws2_t* ws, const char* pattern, int m, const char* text, in
   if (st) st->final_score = s;
   if (ops) {
     int start = 0;
-    const int rc = w2_backtrace(ws, s, x, o1, e1, o2, e2, m, n, &start);
+    const int rc = w2_backtrace(ws, s, k_end, x, o1, e1, o2, e2, m, n, &start);
     if (rc) return rc;
     const int len = (m + n + 1) - start;
     if (len > ops_cap) return ORA_ECIGCAP;
@@ -335,17 +352,82 @@ static int align2_ws(ws2_t* ws, const char* pattern, int m, const char* text, in
   return s;
 }
 
+static const ora_ends_t kEndToEnd2 = {0, 0, 0, 0};
+
 int ora_align2(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2, char* ops,
                int ops_cap, int* ops_len, ora_stats_t* st) {
+  return ora_align2_ends_free(pattern, m, text, n, x, o1, e1, o2, e2, &kEndToEnd2, ops, ops_cap, ops_len, st);
+}
+
+int ora_align2_ends_free(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2,
+                         const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
   ws2_t ws;
   memset(&ws, 0, sizeof(ws));
-  const int r = align2_ws(&ws, pattern, m, text, n, x, o1, e1, o2, e2, ops, ops_cap, ops_len, st);
+  const int r = align2_ws(&ws, pattern, m, text, n, x, o1, e1, o2, e2, ef ? ef : &kEndToEnd2, ops, ops_cap, ops_len,
+                          st);
   ws2_free(&ws);
   return r;
 }
 
 /* Five-matrix DP: H best, E1/E2 ending in an insertion run of piece 1/2,
- * F1/F2 ending in a deletion run of piece 1/2.  O(n) memory. */
+ * F1/F2 ending in a deletion run of piece 1/2.  O(n) memory.  With free
+ * ends: a start (v, 0), v <= pattern_begin_free, or (0, h), h <= text_begin_free,
+ * costs nothing, and the best of the last row (h >= n - text_end_free) and
+ * column (v >= m - pattern_end_free) is the score. */
+int ora_gotoh2_ends_free_score(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2,
+                               int e2, const ora_ends_t* ef) {
+  const int64_t INF = (int64_t)1 << 40;
+  int64_t* H = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  int64_t* F1 = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  int64_t* F2 = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  if (!H || !F1 || !F2) {
+    free(H);
+    free(F1);
+    free(F2);
+    return ORA_ENOMEM;
+  }
+#define MIN2(a, b) ((a) < (b) ? (a) : (b))
+  int64_t E1 = INF, E2 = INF;
+  H[0] = 0;
+  F1[0] = F2[0] = INF;
+  for (int j = 1; j <= n; ++j) {
+    E1 = MIN2(E1 + e1, H[j - 1] + o1 + e1);
+    E2 = MIN2(E2 + e2, H[j - 1] + o2 + e2);
+    H[j] = j <= ef->text_begin_free ? 0 : MIN2(E1, E2);
+    F1[j] = F2[j] = INF;
+  }
+  int64_t best = INF;
+  if (m <= ef->pattern_end_free) best = H[n];
+  if (m == 0)
+    for (int j = n - ef->text_end_free > 0 ? n - ef->text_end_free : 0; j <= n; ++j) best = MIN2(best, H[j]);
+  for (int i = 1; i <= m; ++i) {
+    int64_t diag = H[0];
+    F1[0] = MIN2(F1[0] + e1, H[0] + o1 + e1);
+    F2[0] = MIN2(F2[0] + e2, H[0] + o2 + e2);
+    H[0] = i <= ef->pattern_begin_free ? 0 : MIN2(F1[0], F2[0]);
+    E1 = E2 = INF;
+    for (int j = 1; j <= n; ++j) {
+      const int64_t up = H[j];
+      E1 = MIN2(E1 + e1, H[j - 1] + o1 + e1);
+      E2 = MIN2(E2 + e2, H[j - 1] + o2 + e2);
+      F1[j] = MIN2(F1[j] + e1, up + o1 + e1);
+      F2[j] = MIN2(F2[j] + e2, up + o2 + e2);
+      int64_t b = diag + (pattern[i - 1] == text[j - 1] ? 0 : x);
+      b = MIN2(b, MIN2(MIN2(E1, E2), MIN2(F1[j], F2[j])));
+      diag = up;
+      H[j] = b;
+    }
+    if (i >= m - ef->pattern_end_free) best = MIN2(best, H[n]);
+    if (i == m)
+      for (int j = n - ef->text_end_free > 0 ? n - ef->text_end_free : 0; j <= n; ++j) best = MIN2(best, H[j]);
+  }
+#undef MIN2
+  free(H);
+  free(F1);
+  free(F2);
+  return (int)best;
+}
+
 int ora_gotoh2_score(const char* pattern, int m, const char* text, int n, int x, int o1, int e1, int o2, int e2) {
   const int64_t INF = (int64_t)1 << 40;
   int64_t* H = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n + 1));
@@ -437,6 +519,14 @@ int64_t ora_cigar_cost2(const char* ops, int len, const char* pattern, int m, co
 int ora_align_batch2(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                      const int64_t* toff, const int32_t* tlen, int x, int o1, int e1, int o2, int e2, int32_t* scores,
                      char* ops, const int64_t* ops_off, int32_t* ops_len, int nthreads) {
+  return ora_align_batch2_ends_free(npairs, pat, poff, plen, txt, toff, tlen, x, o1, e1, o2, e2, &kEndToEnd2, scores,
+                                    ops, ops_off, ops_len, nthreads);
+}
+
+int ora_align_batch2_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                               const int64_t* toff, const int32_t* tlen, int x, int o1, int e1, int o2, int e2,
+                               const ora_ends_t* ef, int32_t* scores, char* ops, const int64_t* ops_off,
+                               int32_t* ops_len, int nthreads) {
   int err = 0;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -451,7 +541,7 @@ int ora_align_batch2(int npairs, const char* pat, const int64_t* poff, const int
     for (int i = 0; i < npairs; ++i) {
       int ol = 0;
       const int r = align2_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o1, e1, o2, e2,
-                              ops ? ops + ops_off[i] : NULL, ops ? (int)(ops_off[i + 1] - ops_off[i]) : 0, &ol, NULL);
+                              ef ? ef : &kEndToEnd2, ops ? ops + ops_off[i] : NULL, ops ? (int)(ops_off[i + 1] - ops_off[i]) : 0, &ol, NULL);
       if (r < 0) {
 #ifdef _OPENMP
 #pragma omp critical

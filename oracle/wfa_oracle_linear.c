@@ -146,7 +146,7 @@ static inline int64_t pbl(const wsl_t* ws, const wfl_t* w, int k, int delta, int
   return (int64_t)(o + delta) * 16 + code;
 }
 
-static int wl_backtrace(wsl_t* ws, int s_end, int x, int e, int m, int n, int* start) {
+static int wl_backtrace(wsl_t* ws, int s_end, int k_end, int x, int e, int m, int n, int* start) {
   const int cap = m + n + 1;
   if (ws->opbuf_cap < cap) {
     char* nb = (char*)realloc(ws->opbuf, (size_t)cap);
@@ -161,9 +161,11 @@ static int wl_backtrace(wsl_t* ws, int s_end, int x, int e, int m, int n, int* s
     if (pos < 0) return ORA_ECIGCAP; \
     ops[pos--] = (c);                \
   } while (0)
-  int s = s_end, k = n - m;
-  int32_t off = n;
+  int s = s_end, k = k_end;
+  int32_t off = wl_get(ws, &ws->w[s_end], k_end);
   int v = off - k, h = off;
+  for (int i = v; i < m; ++i) EMITL('D');  /* free trailing gap */
+  for (int i = h; i < n; ++i) EMITL('I');
   while (v > 0 && h > 0 && s > 0) {
     const int64_t mis = pbl(ws, srcl(ws, s - x), k, 1, 9);
     const int64_t del = pbl(ws, srcl(ws, s - e), k + 1, 0, 5);
@@ -204,30 +206,45 @@ static int wl_backtrace(wsl_t* ws, int s_end, int x, int e, int m, int n, int* s
   return 0;
 }
 
-static int alignl_ws(wsl_t* ws, const char* pattern, int m, const char* text, int n, int x, int e, char* ops,
-                     int ops_cap, int* ops_len, ora_stats_t* st) {
+static int alignl_ws(wsl_t* ws, const char* pattern, int m, const char* text, int n, int x, int e,
+                     const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
   if (m < 0 || n < 0 || x <= 0 || e <= 0) return ORA_EINVAL;
   const unsigned char* p = (const unsigned char*)pattern;
   const unsigned char* t = (const unsigned char*)text;
   ws->arena_used = 0;
   if (wsl_reserve(ws, 1)) return ORA_ENOMEM;
+  /* score 0: diagonal 0, or every free start (as in the gap-affine oracle) */
+  const int lo0 = -(ef->pattern_begin_free < m ? ef->pattern_begin_free : m);
+  const int hi0 = ef->text_begin_free < n ? ef->text_begin_free : n;
   wfl_t* M0 = &ws->w[0];
   memset(M0, 0, sizeof(*M0));
-  const int64_t b0 = wsl_alloc(ws, 1);
+  const int64_t b0 = wsl_alloc(ws, hi0 - lo0 + 1);
   if (b0 < 0) return ORA_ENOMEM;
   M0->present = 1;
+  M0->lo = M0->alo = lo0;
+  M0->hi = M0->ahi = hi0;
   M0->base = b0;
-  ws->arena[b0] = 0;
+  for (int k = lo0; k <= hi0; ++k) ws->arena[b0 + (k - lo0)] = k > 0 ? k : 0;
   if (st) {
     st->steps++;
-    st->cells++;
+    st->cells += hi0 - lo0 + 1;
   }
-  const int k_end = n - m;
-  int s = 0;
+  int s = 0, k_end = INT_MIN;
   for (;;) {
     wl_extend(ws, s, p, m, t, n);
     const wfl_t* M = &ws->w[s];
-    if (!wl_null(M) && k_end >= M->lo && k_end <= M->hi && wl_get(ws, M, k_end) >= n) break;
+    k_end = INT_MIN;
+    if (!wl_null(M))
+      for (int k = M->lo; k <= M->hi; ++k) {  /* lowest ending diagonal */
+        const int32_t off = wl_get(ws, M, k);
+        if (off == LNULL) continue;
+        const int v = off - k;
+        if ((off >= n && v >= m - ef->pattern_end_free) || (v >= m && off >= n - ef->text_end_free)) {
+          k_end = k;
+          break;
+        }
+      }
+    if (k_end != INT_MIN) break;
     ++s;
     if (wsl_reserve(ws, s + 1)) return ORA_ENOMEM;
     const int rc = wl_compute(ws, s, x, e, m, n, st);
@@ -236,7 +253,7 @@ static int alignl_ws(wsl_t* ws, const char* pattern, int m, const char* text, in
   if (st) st->final_score = s;
   if (ops) {
     int start = 0;
-    const int rc = wl_backtrace(ws, s, x, e, m, n, &start);
+    const int rc = wl_backtrace(ws, s, k_end, x, e, m, n, &start);
     if (rc) return rc;
     const int len = (m + n + 1) - start;
     if (len > ops_cap) return ORA_ECIGCAP;
@@ -252,11 +269,18 @@ static void wsl_free(wsl_t* ws) {
   free(ws->opbuf);
 }
 
+static const ora_ends_t kLinEndToEnd = {0, 0, 0, 0};
+
 int ora_align_linear(const char* pattern, int m, const char* text, int n, int x, int e, char* ops, int ops_cap,
                      int* ops_len, ora_stats_t* st) {
+  return ora_align_linear_ends_free(pattern, m, text, n, x, e, &kLinEndToEnd, ops, ops_cap, ops_len, st);
+}
+
+int ora_align_linear_ends_free(const char* pattern, int m, const char* text, int n, int x, int e,
+                               const ora_ends_t* ef, char* ops, int ops_cap, int* ops_len, ora_stats_t* st) {
   wsl_t ws;
   memset(&ws, 0, sizeof(ws));
-  const int r = alignl_ws(&ws, pattern, m, text, n, x, e, ops, ops_cap, ops_len, st);
+  const int r = alignl_ws(&ws, pattern, m, text, n, x, e, ef ? ef : &kLinEndToEnd, ops, ops_cap, ops_len, st);
   wsl_free(&ws);
   return r;
 }
@@ -286,6 +310,14 @@ int ora_linear_dp_score(const char* pattern, int m, const char* text, int n, int
 int ora_align_batch_linear(int npairs, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
                            const int64_t* toff, const int32_t* tlen, int x, int e, int32_t* scores, char* ops,
                            const int64_t* ops_off, int32_t* ops_len, int nthreads) {
+  return ora_align_batch_linear_ends_free(npairs, pat, poff, plen, txt, toff, tlen, x, e, &kLinEndToEnd, scores, ops,
+                                          ops_off, ops_len, nthreads);
+}
+
+int ora_align_batch_linear_ends_free(int npairs, const char* pat, const int64_t* poff, const int32_t* plen,
+                                     const char* txt, const int64_t* toff, const int32_t* tlen, int x, int e,
+                                     const ora_ends_t* ef, int32_t* scores, char* ops, const int64_t* ops_off,
+                                     int32_t* ops_len, int nthreads) {
   int err = 0;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -299,7 +331,7 @@ int ora_align_batch_linear(int npairs, const char* pat, const int64_t* poff, con
 #endif
     for (int i = 0; i < npairs; ++i) {
       int ol = 0;
-      const int r = alignl_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, e,
+      const int r = alignl_ws(&ws, pat + poff[i], plen[i], txt + toff[i], tlen[i], x, e, ef ? ef : &kLinEndToEnd,
                               ops ? ops + ops_off[i] : NULL, ops ? (int)(ops_off[i + 1] - ops_off[i]) : 0, &ol, NULL);
       if (r < 0) {
 #ifdef _OPENMP

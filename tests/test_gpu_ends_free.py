@@ -97,7 +97,22 @@ def test_ends_free_score_only_and_checks(oracle):
         assert list(scores) == list(oracle.align_batch_ends_free(pats, txts, free, cigar=False)[0])
         with pytest.raises(T.AlignError):
             al.set_ends_free(-1, 0, 0, 0)
+
+
+
+@pytest.mark.parametrize("free", [(30, 30, 30, 30), (0, 0, 300, 300)])
+def test_ends_free_edit_and_dual(oracle, free):
+    """Semi-global edit distance and dual gap-affine with free ends."""
+    import tsunami_pact_b200 as T
+
+    pats, txts = _flanked(50 + free[2], 400, 0, 1200, flank=200)
     with T.Aligner(metric="edit") as al:
-        with pytest.raises(T.AlignError):
-            al.set_ends_free(1, 1, 1, 1)
-        al.set_ends_free(0, 0, 0, 0)
+        al.set_ends_free(*free)
+        s, ops = al.align(pats, txts)
+        osc, oops = oracle.align_batch_linear_ends_free(pats, txts, free, 1, 1)
+        assert list(s) == list(osc) and ops == oops
+    with T.Aligner(4, 6, 2, gap_opening2=24, gap_extension2=1) as al:
+        al.set_ends_free(*free)
+        s, ops = al.align(pats, txts)
+        osc, oops = oracle.align_batch2_ends_free(pats, txts, free)
+        assert list(s) == list(osc) and ops == oops

@@ -336,3 +336,18 @@ def test_ends_free_groups_and_score_only(emu, oracle):
     check_ends_free(emu, oracle, pairs, (50, 50, 50, 50), cigar=False)
     for gw, shared in [(4, True), (8, False)]:
         check_ends_free(emu, oracle, pairs, (50, 50, 50, 50), shared_first=shared, gw=gw)
+
+
+
+def test_ends_free_linear_and_dual(emu, oracle):
+    """Free ends with the gap-linear and the dual gap-affine kernels."""
+    rng = random.Random(41)
+    pairs = _flanked(rng, 10, 0, 120) + [("", "ACGT"), ("ACG", "")]
+    bpairs = [(_b(p), _b(t)) for p, t in pairs]
+    for free in [(20, 20, 20, 20), (0, 0, 30, 30)]:
+        got, _, _, _ = run_emu(emu, bpairs, (1, -1, 1), free=free)
+        for (p, t), (s, ops) in zip(bpairs, got):
+            assert (s, ops) == oracle.align_linear_ends_free(p, t, free, 1, 1), (p, t, free)
+        got, _, _, _ = run_emu(emu, bpairs, (4, 6, 2, 24, 1), free=free)
+        for (p, t), (s, ops) in zip(bpairs, got):
+            assert (s, ops) == oracle.align2_ends_free(p, t, free), (p, t, free)

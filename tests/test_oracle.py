@@ -238,3 +238,76 @@ def test_ends_free_batch_matches_single(oracle):
     sc, cg = oracle.align_batch_ends_free(pats, txts, free, threads=4)
     for i in range(40):
         assert (sc[i], cg[i]) == oracle.align_ends_free(pats[i], txts[i], free)
+
+
+def _cost_free(ops, p, t, free, x, gap):
+    """Cost of an operation string with free ends under a gap cost function
+    (test-side restatement, independent of the oracle's C code)."""
+    v = h = 0
+    cost = 0
+    runs = []
+    i = 0
+    while i < len(ops):
+        j = i
+        while j < len(ops) and ops[j] == ops[i]:
+            j += 1
+        runs.append((ops[i], j - i))
+        i = j
+    for r, (c, L) in enumerate(runs):
+        if c in "MX":
+            for _ in range(L):
+                assert (c == "M") == (p[v] == t[h])
+                cost += x if c == "X" else 0
+                v += 1
+                h += 1
+            continue
+        free_len = 0
+        if r == 0:
+            free_len += free[2] if c == "I" else free[0]
+        if r == len(runs) - 1:
+            free_len += free[3] if c == "I" else free[1]
+        if c == "I":
+            h += L
+        else:
+            v += L
+        if L > free_len:
+            cost += gap(L - free_len)
+    assert v == len(p) and h == len(t)
+    return cost
+
+
+@pytest.mark.parametrize("free", FREES)
+def test_linear_and_dual_ends_free_vs_dp(oracle, free):
+    """Gap-linear (scores = gap-affine with opening 0) and dual gap-affine
+    with free ends, against the ends-free DPs; operation strings cost the
+    score; all-zero free ends reproduce the end-to-end oracles."""
+    rng = random.Random(hash(free) & 0xFFF)
+    for it in range(120):
+        alpha = "ACGT" if it % 3 else "AC"
+        core = "".join(rng.choice(alpha) for _ in range(rng.randint(0, 40)))
+        fl = lambda: "".join(rng.choice(alpha) for _ in range(rng.randint(0, 10)))
+        p, t = fl() + core + fl(), fl() + core + fl()
+        for x, e in [(1, 1), (3, 1), (2, 3)]:
+            s, ops = oracle.align_linear_ends_free(p, t, free, x, e)
+            assert s == oracle.gotoh_ends_free(p, t, free, x, 0, e), (p, t, free, x, e)
+            assert _cost_free(ops, p, t, free, x, lambda L: e * L) == s
+            if free == (0, 0, 0, 0):
+                assert (s, ops) == oracle.align_linear(p, t, x, e)
+        pen = (4, 6, 2, 24, 1)
+        s, ops = oracle.align2_ends_free(p, t, free, *pen)
+        assert s == oracle.gotoh2_ends_free(p, t, free, *pen), (p, t, free)
+        assert _cost_free(ops, p, t, free, 4, lambda L: min(6 + 2 * L, 24 + L)) == s
+        if free == (0, 0, 0, 0):
+            assert (s, ops) == oracle.align2(p, t, *pen)
+
+
+def test_linear_dual_ends_free_batches(oracle):
+    rng = random.Random(23)
+    pats = ["".join(rng.choice("ACGT") for _ in range(rng.randint(0, 100))) for _ in range(30)]
+    txts = [p[rng.randint(0, 8):] + "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 8))) for p in pats]
+    free = (8, 8, 8, 8)
+    sc, cg = oracle.align_batch_linear_ends_free(pats, txts, free, 1, 1, threads=4)
+    sc2, cg2 = oracle.align_batch2_ends_free(pats, txts, free, threads=4)
+    for i in range(30):
+        assert (sc[i], cg[i]) == oracle.align_linear_ends_free(pats[i], txts[i], free, 1, 1)
+        assert (sc2[i], cg2[i]) == oracle.align2_ends_free(pats[i], txts[i], free)

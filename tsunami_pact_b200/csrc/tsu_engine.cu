@@ -1419,9 +1419,6 @@ int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_
   if (!ctx) return TSU_EINVAL;
   if (pattern_begin_free < 0 || pattern_end_free < 0 || text_begin_free < 0 || text_end_free < 0)
     return set_err(ctx, TSU_EINVAL, "negative free end");
-  if (ctx->spec.metric != TSU_METRIC_GAP_AFFINE &&
-      (pattern_begin_free | pattern_end_free | text_begin_free | text_end_free))
-    return set_err(ctx, TSU_EINVAL, "free ends need a gap-affine context");
   ctx->ends_free[0] = pattern_begin_free;
   ctx->ends_free[1] = pattern_end_free;
   ctx->ends_free[2] = text_begin_free;
