@@ -297,12 +297,6 @@ size_t group_scratch_bytes(const tsu::PassGeom& g) {
   return (size_t)(g.ring_ints * 4 + g.hist_cap * 4 + (int64_t)g.table_cap * 8 + 64);
 }
 
-// Diagonals beyond the first of the score-0 wavefront with free beginnings
-// (0 end-to-end).
-int free_start_width(const tsu_ctx* ctx, const BatchInfo& bi) {
-  return std::min(ctx->ends_free[0], bi.max_m) + std::min(ctx->ends_free[2], bi.max_n);
-}
-
 // Configure a pass of configuration pc over pairs of at most bi's lengths:
 // geometry, then as many groups as fit the SMs, the pairs and `avail` bytes
 // of scratch.
@@ -597,9 +591,6 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       r.hint = ctx->err_hint;
       if (ctx->fit_start && !ctx->one_warp)
         r.pc = tsu::fit_start(r.pc, ctx->rp, r.bi.max_m, r.bi.max_n, r.hint, ctx->smem_optin);
-      if (!ctx->one_warp)
-        r.pc = tsu::widen_for_free_start(r.pc, ctx->rp, r.bi.max_m, r.bi.max_n, free_start_width(ctx, r.bi),
-                                         ctx->smem_optin);
       if ((rc = plan_pass_within(ctx, r.bi, r.n, r.pc, r.hint, want_cigar, avail, &r.ps))) return rc;
       need = std::max(need, scratch_bytes(r.ps, want_cigar));
     }
@@ -944,9 +935,6 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
       }
       if (ctx->fit_start && !one_warp)
         pc = tsu::fit_start(pc, ctx->rp, pbi.max_m, pbi.max_n, hint, ctx->smem_optin);
-      if (!one_warp)
-        pc = tsu::widen_for_free_start(pc, ctx->rp, pbi.max_m, pbi.max_n, free_start_width(ctx, pbi),
-                                       ctx->smem_optin);
       Pass ps;
       const int rc = plan_pass_within(ctx, pbi, np, pc, hint, want_cigar, SIZE_MAX / 4, &ps);
       if (rc) return rc;

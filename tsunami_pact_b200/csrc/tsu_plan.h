@@ -149,26 +149,6 @@ inline PassChoice fit_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_
   return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
 }
 
-// With free beginnings the score-0 wavefront already spans w_free + 1
-// diagonals (every free start); the tuned starting rungs assume one.  A
-// shared-ring start is widened to the smallest shared group whose ring
-// holds the starting rung's ring plus w_free, so pairs do not overflow the
-// first pass by the free range alone.
-inline PassChoice widen_for_free_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_t max_n, int w_free,
-                                       int smem_optin) {
-  if (w_free <= 0 || pc.mode != kModeShared) return pc;
-  const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
-  auto ring = [&](int gw) {
-    return gw == 1 ? (seqw > kSharedSeqWords1 ? 0 : kSharedW1)
-                   : (seqw > kSharedSeqWordsN ? 0 : shared_ring_width(pen, gw, (int)seqw, smem_optin));
-  };
-  const int64_t need = (int64_t)ring(pc.gw) + w_free;
-  static const int kGW[] = {1, 2, 4, 8, 16};
-  for (int gw : kGW)
-    if (gw >= pc.gw && ring(gw) >= need) return {kModeShared, gw};
-  return pc;  // no shared group holds it: the ladder takes over
-}
-
 // Length bands of the batched scheduler: max(m, n) < 1024, < 2048, < 4096,
 // < 8192, < 16384, >= 16384.  Each band starts its ladder at the rung the
 // autotuner measured fastest for it (tsu_tuning.h; the dual gap-affine
