@@ -40,33 +40,11 @@ struct Buf {  // exact-size heap block
   Buf& operator=(const Buf&) = delete;
 };
 
-template <bool kCigar, int kMode, int kModel>
-static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
-  switch (gw) {
-    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, kModel>(a); }); break;
-    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, kModel>(a); }); break;
-    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, kModel>(a); }); break;
-    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, kModel>(a); }); break;
-    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, kModel>(a); }); break;
-    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, kModel>(a); }); break;
-    default: std::abort();
-  }
-}
-
-template <int kModel>
-static void run_pass(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
-  if (cigar) {
-    if (mode == tsu::kModeShared)
-      run_gw<true, tsu::kModeShared, kModel>(gw, threads, smem, a);
-    else
-      run_gw<true, tsu::kModeGlobal, kModel>(gw, threads, smem, a);
-  } else {
-    if (mode == tsu::kModeShared)
-      run_gw<false, tsu::kModeShared, kModel>(gw, threads, smem, a);
-    else
-      run_gw<false, tsu::kModeGlobal, kModel>(gw, threads, smem, a);
-  }
-}
+// The align passes of each penalty model (emu_model.cpp, compiled once per
+// model).
+void run_pass_affine(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
+void run_pass_dual(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
+void run_pass_linear(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
 
 int main() {
   int X, O, E, O2, E2, PBF, PEF, TBF, TEF, cigar, first_mode, first_gw;
@@ -185,11 +163,11 @@ int main() {
     const int threads = geo.cta_threads;
     gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);
     if (rp.linear())
-      run_pass<tsu::kModelLinear>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_linear(want_cigar, geo.mode, geo.gw, threads, smem, a);
     else if (rp.dual())
-      run_pass<tsu::kModelDual>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_dual(want_cigar, geo.mode, geo.gw, threads, smem, a);
     else
-      run_pass<tsu::kModelAffine>(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_affine(want_cigar, geo.mode, geo.gw, threads, smem, a);
     ++passes;
     const unsigned nretry = *retry_cnt;
     if (nretry == 0) break;

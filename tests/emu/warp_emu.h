@@ -37,34 +37,47 @@ inline thread_local emu_dim3 tid, bid;
 inline emu_dim3 bdim, gdim;
 inline unsigned char* smem_block = nullptr;
 
+// Lane exchange slots, double-buffered by collective parity: a collective
+// writes its lane's slot of the current parity, waits once, and reads.  A
+// lane writes that parity again only two collectives later, after the
+// barrier of the next collective, which no lane reaches before it has read
+// this one -- so one barrier per collective suffices.  Every lane of a warp
+// runs the same sequence of collectives (converged code), so the lanes'
+// parities agree.
 struct Warp {
   std::barrier<> bar{32};
-  uint64_t slot[32];
+  uint64_t slot[2][32];
 };
 inline std::vector<std::unique_ptr<Warp>> warps;
+inline thread_local unsigned coll_parity = 0;
 
 inline Warp& W() { return *warps[tid.x >> 5]; }
 inline int lane() { return (int)(tid.x & 31); }
 inline void syncwarp() { W().bar.arrive_and_wait(); }
+// Publish this lane's value and wait for the warp; returns the slots of this
+// collective.
+inline const uint64_t* exchange(uint64_t v) {
+  Warp& w = W();
+  const unsigned p = coll_parity;
+  coll_parity ^= 1u;
+  w.slot[p][lane()] = v;
+  w.bar.arrive_and_wait();
+  return w.slot[p];
+}
 template <class T>
 inline T shfl(T v, int src) {
   uint64_t b = 0;
   std::memcpy(&b, &v, sizeof(T));
-  W().slot[lane()] = b;
-  syncwarp();
-  uint64_t r = W().slot[src & 31];
-  syncwarp();
+  const uint64_t r = exchange(b)[src & 31];
   T out;
   std::memcpy(&out, &r, sizeof(T));
   return out;
 }
 template <class F>
 inline uint64_t all_reduce(uint64_t v, F f) {
-  W().slot[lane()] = v;
-  syncwarp();
-  uint64_t acc = W().slot[0];
-  for (int i = 1; i < 32; ++i) acc = f(acc, W().slot[i]);
-  syncwarp();
+  const uint64_t* s = exchange(v);
+  uint64_t acc = s[0];
+  for (int i = 1; i < 32; ++i) acc = f(acc, s[i]);
   return acc;
 }
 inline int reduce_min(int v) {
@@ -78,11 +91,9 @@ inline int reduce_max(int v) {
   });
 }
 inline unsigned ballot(bool p) {
-  W().slot[lane()] = p ? 1u : 0u;
-  syncwarp();
+  const uint64_t* s = exchange(p ? 1u : 0u);
   unsigned r = 0;
-  for (int i = 0; i < 32; ++i) r |= (W().slot[i] ? 1u : 0u) << i;
-  syncwarp();
+  for (int i = 0; i < 32; ++i) r |= (s[i] ? 1u : 0u) << i;
   return r;
 }
 inline unsigned char* dyn_smem() { return smem_block; }

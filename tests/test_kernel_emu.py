@@ -13,7 +13,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EMU_DIR = os.path.join(ROOT, "tests", "emu")
 EXE = os.path.join(EMU_DIR, "_build", "emu_driver")
-SRCS = [os.path.join(EMU_DIR, "emu_driver.cpp"), os.path.join(EMU_DIR, "warp_emu.h")] + [
+SRCS = [os.path.join(EMU_DIR, f) for f in ("emu_driver.cpp", "emu_model.cpp", "warp_emu.h")] + [
     os.path.join(ROOT, "tsunami_pact_b200", "csrc", f)
     for f in os.listdir(os.path.join(ROOT, "tsunami_pact_b200", "csrc"))
     if f.endswith((".cuh", ".h"))
@@ -25,9 +25,17 @@ def emu():
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     newest = max(os.path.getmtime(s) for s in SRCS)
     if not os.path.exists(EXE) or os.path.getmtime(EXE) < newest:
-        subprocess.run(["g++", "-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
-                        "-fno-sanitize-recover=undefined", "-o", EXE, os.path.join(EMU_DIR, "emu_driver.cpp"),
-                        "-lpthread"], check=True)
+        # the driver and one object per penalty model, compiled in parallel
+        flags = ["-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+                 "-fno-sanitize-recover=undefined"]
+        build = os.path.dirname(EXE)
+        jobs = [(os.path.join(build, "driver.o"), [os.path.join(EMU_DIR, "emu_driver.cpp")])]
+        for model, fn in ((0, "run_pass_affine"), (1, "run_pass_dual"), (2, "run_pass_linear")):
+            jobs.append((os.path.join(build, f"model{model}.o"),
+                         [f"-DEMU_MODEL={model}", f"-DEMU_RUN_FN={fn}", os.path.join(EMU_DIR, "emu_model.cpp")]))
+        procs = [subprocess.Popen(["g++", *flags, "-c", "-o", obj, *args]) for obj, args in jobs]
+        assert all(p.wait() == 0 for p in procs), "emulator build failed"
+        subprocess.run(["g++", *flags, "-o", EXE, *(obj for obj, _ in jobs), "-lpthread"], check=True)
     return EXE
 
 
