@@ -43,6 +43,7 @@ WORKLOADS = {
 PEN = (4, 6, 2)  # --penalties; five values (open2, extend2 last): dual gap-affine
 METRIC_NAME = None  # --metric edit | indel | gap_linear (PEN then (mismatch, gap_extension))
 ENDS_FREE = (0, 0, 0, 0)  # --ends-free pattern_begin,pattern_end,text_begin,text_end (gap-affine)
+LOW_MEM = 0  # --low-memory checkpoint interval (0 off, < 0 chosen per pass)
 LINEAR_XE = {"edit": (1, 1), "indel": (3, 1)}  # the gap-linear penalties of these metrics
 
 
@@ -52,6 +53,8 @@ def linear_xe():
 
 def pen_str() -> str:
     ef = ", free ends %d/%d/%d/%d" % ENDS_FREE if any(ENDS_FREE) else ""
+    if LOW_MEM:
+        ef += ", low-memory (checkpoint interval %s)" % ("auto" if LOW_MEM < 0 else LOW_MEM)
     if METRIC_NAME in LINEAR_XE:
         return METRIC_NAME + " distance" + ef
     if METRIC_NAME == "gap_linear":
@@ -70,6 +73,8 @@ def make_aligner(T, **kw):
         al = T.Aligner(*PEN[:3], **dual_kw, **kw)
     if any(ENDS_FREE):
         al.set_ends_free(*ENDS_FREE)
+    if LOW_MEM:
+        al.set_low_memory(LOW_MEM)
     return al
 
 
@@ -373,8 +378,11 @@ def main():
                     help="a gap-linear metric instead of gap-affine (gap_linear: --penalties mismatch,extend)")
     ap.add_argument("--ends-free", default="0,0,0,0",
                     help="pattern_begin,pattern_end,text_begin,text_end free lengths (gap-affine)")
+    ap.add_argument("--low-memory", type=int, default=0,
+                    help="checkpointed-history CIGARs: checkpoint interval (-1: chosen per pass)")
     args = ap.parse_args()
-    global PEN, METRIC_NAME, ENDS_FREE
+    global PEN, METRIC_NAME, ENDS_FREE, LOW_MEM
+    LOW_MEM = args.low_memory
     ENDS_FREE = tuple(int(v) for v in args.ends_free.split(","))
     if len(ENDS_FREE) != 4:
         raise SystemExit("--ends-free takes 4 values")
@@ -595,6 +603,11 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        try:  # device memory the engine plans for this batch (tsu_predict_bytes)
+            full_b, min_b = al.predict_bytes(plen, tlen, cigar=want_cigar)
+            out["predicted_device_bytes"] = {"full": int(full_b), "min": int(min_b)}
+        except T.AlignError:
+            pass
         print(json.dumps(out), flush=True)
     al.close()
     if dist is not None:

@@ -196,6 +196,21 @@ int tsu_set_band_start(tsu_ctx* ctx, int band, int mode, int warps_per_pair);
 int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_end_free, int32_t text_begin_free,
                       int32_t text_end_free);
 int tsu_get_ends_free(const tsu_ctx* ctx, int32_t* out4);
+
+/* Low-memory mode for the CIGAR of long or divergent pairs (the role of
+ * WFA2-lib's memory modes, wavefront_memory_*; the reference keeps its
+ * default, wfa_gpu.cu:156-160).  The backtrace history normally holds one
+ * 4-byte word per wavefront cell of every score (about s^2 / e words for a
+ * pair of score s).  With a checkpoint interval K the score pass keeps no
+ * history but saves the wavefront ring every K scores; the backtrace then
+ * recomputes the history K scores at a time, from the last segment to the
+ * first, and walks each.  The CIGAR is the same; device memory per pair
+ * falls to about (s / K) checkpoints plus K rows, for about twice the
+ * compute.  checkpoint_interval: 0 off (default), > 0 K in score steps
+ * (units of gcd of the penalties), < 0 chosen per pass (K near
+ * sqrt(s * checkpoint size / row size)).  Low-memory passes run with the
+ * wavefront ring in device memory. */
+int tsu_set_low_memory(tsu_ctx* ctx, int32_t checkpoint_interval);
 int tsu_get_band_start(const tsu_ctx* ctx, int band, int* mode, int* warps_per_pair);
 
 /* ---- batch alignment, host buffers -------------------------------------

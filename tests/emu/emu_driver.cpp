@@ -3,11 +3,12 @@
 // emulator.  Test infrastructure: compiled by tests/test_kernel_emu.py with
 // AddressSanitizer, it checks the kernels' indexing and outputs on the CPU.
 //
-// Input (stdin):  x o e o2 e2 pbf pef tbf tef cigar hint first_mode first_gw N
+// Input (stdin):  x o e o2 e2 pbf pef tbf tef lowmem cigar hint first_mode first_gw N
 //                 then N records "m n\n<pattern>\n<text>\n"
 //   o2 < 0: one gap piece; else dual gap-affine (the kModelDual kernels);
 //   o < 0: gap-linear with mismatch x and gap e per base (kModelLinear);
-//   pbf pef tbf tef: free ends (all 0: end-to-end)
+//   pbf pef tbf tef: free ends (all 0: end-to-end); lowmem: checkpoint
+//   interval of the low-memory mode (0 off, < 0 chosen by the planner)
 //   first_mode 1 = shared ring, 0 = global ring; first_gw = warps per pair
 //   of the first pass (1, 2, 4, 8, 16).  Retry passes follow the engine's
 //   ladder (tsu_plan.h next_pass).
@@ -42,16 +43,16 @@ struct Buf {  // exact-size heap block
 
 // The align passes of each penalty model (emu_model.cpp, compiled once per
 // model).
-void run_pass_affine(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
-void run_pass_dual(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
-void run_pass_linear(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a);
+void run_pass_affine(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a, bool lowmem);
+void run_pass_dual(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a, bool lowmem);
+void run_pass_linear(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a, bool lowmem);
 
 int main() {
-  int X, O, E, O2, E2, PBF, PEF, TBF, TEF, cigar, first_mode, first_gw;
+  int X, O, E, O2, E2, PBF, PEF, TBF, TEF, LOWMEM, cigar, first_mode, first_gw;
   double hint;
   int64_t N;
-  if (!(std::cin >> X >> O >> E >> O2 >> E2 >> PBF >> PEF >> TBF >> TEF >> cigar >> hint >> first_mode >> first_gw >>
-        N))
+  if (!(std::cin >> X >> O >> E >> O2 >> E2 >> PBF >> PEF >> TBF >> TEF >> LOWMEM >> cigar >> hint >> first_mode >>
+        first_gw >> N))
     return 2;
   std::vector<std::string> pats(N), txts(N);
   for (int64_t i = 0; i < N; ++i) {
@@ -124,11 +125,12 @@ int main() {
   int32_t pm = max_m, pn = max_n;
   std::string gws;
   for (;;) {
-    const tsu::PassGeom geo = tsu::plan_geometry(rp, pm, pn, pc.mode, pc.gw, h, want_cigar, smem_optin);
+    const tsu::PassGeom geo = tsu::plan_geometry(rp, pm, pn, pc.mode, pc.gw, h, want_cigar, smem_optin, LOWMEM);
     const int groups = geo.groups_per_cta;  // one block
     Buf<int32_t> ring(geo.mode == tsu::kModeGlobal ? (size_t)groups * geo.ring_ints : 0);
     Buf<uint32_t> hist(want_cigar ? (size_t)groups * geo.hist_cap : 0);
     Buf<int2> table(want_cigar ? (size_t)groups * geo.table_cap : 0);
+    Buf<uint8_t> ckpt(geo.ckpt_k > 0 ? (size_t)groups * geo.ckpt_cap * geo.ckpt_bytes : 0);
     tsu::AlignArgs a{};
     a.seq = sv;
     a.pk = pk;
@@ -159,15 +161,21 @@ int main() {
     a.ef_pe = PEF;
     a.ef_tb = TBF;
     a.ef_te = TEF;
+    a.ckpt = ckpt.p;
+    a.ckpt_k = geo.ckpt_k;
+    a.ckpt_cap = geo.ckpt_cap;
+    a.ckpt_bytes = (int32_t)geo.ckpt_bytes;
+    a.ckpt_stride = (int64_t)geo.ckpt_cap * geo.ckpt_bytes;
     const size_t smem = (size_t)groups * geo.group_smem;
     const int threads = geo.cta_threads;
     gws += (gws.empty() ? "" : ",") + std::string(geo.mode == tsu::kModeShared ? "s" : "g") + std::to_string(geo.gw);
+    const bool lowmem = geo.ckpt_k > 0;
     if (rp.linear())
-      run_pass_linear(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_linear(want_cigar, geo.mode, geo.gw, threads, smem, a, lowmem);
     else if (rp.dual())
-      run_pass_dual(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_dual(want_cigar, geo.mode, geo.gw, threads, smem, a, lowmem);
     else
-      run_pass_affine(want_cigar, geo.mode, geo.gw, threads, smem, a);
+      run_pass_affine(want_cigar, geo.mode, geo.gw, threads, smem, a, lowmem);
     ++passes;
     const unsigned nretry = *retry_cnt;
     if (nretry == 0) break;

@@ -1,0 +1,81 @@
+"""GPU parity of the low-memory mode (tsu_set_low_memory: checkpointed
+wavefront rings, history recomputed segment by segment): the same scores and
+CIGARs as the oracle, and less predicted device memory for long pairs."""
+import random
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _pairs(seed, n, lo, hi, rate):
+    rng = random.Random(seed)
+    pats, txts = [], []
+    for _ in range(n):
+        p = "".join(rng.choice("ACGT") for _ in range(rng.randint(lo, hi)))
+        t = list(p)
+        for _ in range(int(len(p) * rate)):
+            pos = rng.randint(0, max(0, len(t) - 1))
+            r = rng.random()
+            if r < 0.33 and t:
+                t[pos] = rng.choice("ACGT")
+            elif r < 0.66:
+                t.insert(pos, rng.choice("ACGT"))
+            elif t:
+                del t[pos]
+        pats.append(p)
+        txts.append("".join(t))
+    return pats, txts
+
+
+@pytest.mark.parametrize("K", [1, 7, 64, -1])
+def test_low_memory_affine(oracle, K):
+    import tsunami_pact_b200 as T
+
+    pats, txts = _pairs(80 + K, 400, 0, 1500, 0.1)
+    pats += ["", "ACGT", "ACGTNNNNACGT"]
+    txts += ["ACGTAC", "", "ACGTACGT"]
+    with T.Aligner(4, 6, 2) as al:
+        al.set_low_memory(K)
+        s, ops = al.align(pats, txts)
+        assert al.pass_log().startswith("g"), al.pass_log()
+    osc, oops = oracle.align_batch(pats, txts, 4, 6, 2)
+    assert list(s) == list(osc) and ops == oops
+
+
+def test_low_memory_long_reads_and_models(oracle):
+    import tsunami_pact_b200 as T
+
+    pats, txts = _pairs(90, 10, 8000, 25000, 0.15)
+    with T.Aligner(4, 6, 2) as al:
+        al.set_low_memory(-1)
+        s, ops = al.align(pats, txts)
+    osc, oops = oracle.align_batch(pats, txts, 4, 6, 2)
+    assert list(s) == list(osc) and ops == oops
+    pats, txts = _pairs(91, 200, 100, 3000, 0.1)
+    with T.Aligner(4, 6, 2, gap_opening2=24, gap_extension2=1) as al:
+        al.set_low_memory(-1)
+        s, ops = al.align(pats, txts)
+    osc, oops = oracle.align_batch2(pats, txts)
+    assert list(s) == list(osc) and ops == oops
+    with T.Aligner(metric="edit") as al:
+        al.set_low_memory(-1)
+        al.set_ends_free(50, 50, 50, 50)
+        s, ops = al.align(pats, txts)
+    osc, oops = oracle.align_batch_linear_ends_free(pats, txts, (50, 50, 50, 50), 1, 1)
+    assert list(s) == list(osc) and ops == oops
+
+
+def test_low_memory_needs_less_memory():
+    """The predicted device memory of a batch of long divergent pairs is much
+    smaller with checkpoints."""
+    import tsunami_pact_b200 as T
+
+    plen = np.full(64, 50000, np.int32)
+    with T.Aligner(4, 6, 2, max_error_hint=0.2) as al:
+        full_hi, min_hi = al.predict_bytes(plen, plen)
+        al.set_low_memory(-1)
+        full_lo, min_lo = al.predict_bytes(plen, plen)
+    assert min_lo * 4 < min_hi, (min_lo, min_hi)
+    assert full_lo < full_hi

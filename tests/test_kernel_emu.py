@@ -39,10 +39,10 @@ def emu():
     return EXE
 
 
-def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1, free=(0, 0, 0, 0)):
+def run_emu(exe, pairs, pen=(4, 6, 2), cigar=True, hint=0.2, shared_first=True, gw=1, free=(0, 0, 0, 0), lowmem=0):
     o2, e2 = (pen[3], pen[4]) if len(pen) == 5 else (-1, 0)
-    hdr = (f"{pen[0]} {pen[1]} {pen[2]} {o2} {e2} {free[0]} {free[1]} {free[2]} {free[3]} {int(cigar)} {hint} "
-           f"{int(shared_first)} {gw} {len(pairs)}\n")
+    hdr = (f"{pen[0]} {pen[1]} {pen[2]} {o2} {e2} {free[0]} {free[1]} {free[2]} {free[3]} {lowmem} {int(cigar)} "
+           f"{hint} {int(shared_first)} {gw} {len(pairs)}\n")
     body = b"".join(f"{len(p)} {len(t)}\n".encode() + p + b"\n" + t + b"\n" for p, t in pairs)
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1")
     r = subprocess.run([exe], input=hdr.encode() + body, capture_output=True, env=env, timeout=600)
@@ -359,3 +359,39 @@ def test_ends_free_linear_and_dual(emu, oracle):
         got, _, _, _ = run_emu(emu, bpairs, (4, 6, 2, 24, 1), free=free)
         for (p, t), (s, ops) in zip(bpairs, got):
             assert (s, ops) == oracle.align2_ends_free(p, t, free), (p, t, free)
+
+
+
+# --- low-memory mode (checkpointed history) ----------------------------------
+
+@pytest.mark.parametrize("K", [1, 3, 10, -1])
+def test_low_memory_same_cigars(emu, oracle, K):
+    """Checkpoint every K scores and recompute the history segment by
+    segment: the same scores and CIGARs as the oracle (gap-affine; K = 1
+    makes every segment one score, -1 lets the planner choose)."""
+    rng = random.Random(60 + K)
+    pairs = [_edited(rng, rng.randint(0, 250), 0.15) for _ in range(10)]
+    pairs += [("", ""), ("", "ACGT"), ("ACG", ""), ("ACGTNNACGT", "ACGTACGT"), ("A" * 64, "A" * 64)]
+    bp = [(_b(p), _b(t)) for p, t in pairs]
+    got, passes, retried, gws = run_emu(emu, bp, lowmem=K)
+    assert gws.startswith("g"), gws  # low-memory passes use the global ring
+    for (p, t), (s, ops) in zip(bp, got):
+        assert (s, ops) == oracle.align(p, t), (p, t, K)
+
+
+def test_low_memory_models_groups_free_ends(emu, oracle):
+    """Low-memory mode with the dual and gap-linear kernels, warp groups and
+    free ends."""
+    rng = random.Random(70)
+    pairs = [_edited(rng, rng.randint(50, 300), 0.12) for _ in range(5)]
+    bp = [(_b(p), _b(t)) for p, t in pairs]
+    got, _, _, _ = run_emu(emu, bp, (4, 6, 2, 24, 1), lowmem=4)
+    for (p, t), (s, ops) in zip(bp, got):
+        assert (s, ops) == oracle.align2(p, t), (p, t)
+    got, _, _, _ = run_emu(emu, bp, (1, -1, 1), lowmem=5, gw=4, shared_first=False)
+    for (p, t), (s, ops) in zip(bp, got):
+        assert (s, ops) == oracle.align_linear(p, t, 1, 1), (p, t)
+    free = (20, 20, 20, 20)
+    got, _, _, _ = run_emu(emu, bp, lowmem=7, gw=2, shared_first=False, free=free)
+    for (p, t), (s, ops) in zip(bp, got):
+        assert (s, ops) == oracle.align_ends_free(p, t, free), (p, t)

@@ -259,6 +259,34 @@ class Aligner:
         self._check(L.tsu_set_ends_free(self._h, pattern_begin_free, pattern_end_free, text_begin_free,
                                         text_end_free))
 
+    def set_low_memory(self, checkpoint_interval: int = -1) -> None:
+        """Low-memory CIGARs (tsu_set_low_memory): checkpoint the wavefront
+        ring every checkpoint_interval scores (< 0: chosen per pass; 0: off)
+        and recompute the history segment by segment for the backtrace."""
+        L = lib()
+        L.tsu_set_low_memory.argtypes = [c_vp, c_i32]
+        self._check(L.tsu_set_low_memory(self._h, checkpoint_interval))
+
+    def predict_bytes(self, plen, tlen, cigar: bool = True):
+        """(full, min) device bytes tsu_align_batch would hold for pairs of
+        these lengths (tsu_predict_bytes)."""
+        L = lib()
+        plen = np.ascontiguousarray(plen, dtype=np.int32)
+        tlen = np.ascontiguousarray(tlen, dtype=np.int32)
+        n = len(plen)
+        poff = np.zeros(n, dtype=np.int64)
+        toff = np.zeros(n, dtype=np.int64)
+        if n:
+            np.cumsum(plen[:-1], out=poff[1:])
+            np.cumsum(tlen[:-1], out=toff[1:])
+        dummy = np.zeros(1, dtype=np.uint8)  # sequences are not read, only lengths and offsets
+        b = Batch(n, dummy.ctypes.data, poff.ctypes.data, plen.ctypes.data, dummy.ctypes.data, toff.ctypes.data,
+                  tlen.ctypes.data)
+        full, mn = ctypes.c_size_t(), ctypes.c_size_t()
+        self._check(L.tsu_predict_bytes(self._h, ctypes.byref(b), 0 if cigar else TSU_SCORE_ONLY, ctypes.byref(full),
+                                        ctypes.byref(mn)))
+        return full.value, mn.value
+
     def pass_log(self) -> str:
         """Align passes of the last call: mode+warps per pair x groups : pairs @ time."""
         L = lib()

@@ -73,8 +73,10 @@ constexpr int cta_min_blocks() {
 template <bool kCigar, int kMode, int GW, int kModel = kModelAffine>
 __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>())) align_kernel(AlignArgs a) {
   static_assert(GW == 1 || GW == 2 || GW == 4 || GW == 8 || GW == 16 || GW == 32, "warps per pair");
-  constexpr bool kDual = kModel == kModelDual;
-  constexpr bool kLin = kModel == kModelLinear;
+  constexpr bool kDual = (kModel & 7) == kModelDual;
+  constexpr bool kLin = (kModel & 7) == kModelLinear;
+  constexpr bool kLowMem = kCigar && (kModel & kLowMemFlag) != 0;
+  static_assert(!(kModel & kLowMemFlag) || (kCigar && kMode == kModeGlobal), "low-memory: CIGAR, global ring");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
 #ifdef TSU_WARP_EMU
@@ -149,6 +151,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
     }
     int s_end = -1;
     int k_fin = k_end;  // end diagonal (free ends: the lowest that ends)
+    constexpr bool lowmem = kLowMem;  // checkpointed history (low-memory mode)
+    const int K = a.ckpt_k;
+    int32_t lm_len = 0;  // the low-memory walk's CIGAR (thread 0 of the group)
+    int64_t lm_pos = 0;
     int64_t hbase = 0;
     unsigned long long n_cells = 0, n_steps = 0;
 
@@ -250,267 +256,383 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       const int k_hi = k_end + a.ef_pe;
       const bool free_te = a.ef_te > 0;
       const int n_te = n - a.ef_te;
-      while (s_end < 0 && st == kPairOk) {
-        ++s;
-        if (++slm == rm) slm = 0;
-        if constexpr (!kLin) {
-          if (++sli == re) sli = 0;
-        }
-        if constexpr (kDual) {
-          if (++sli2 == a.pen.re2) sli2 = 0;
-        }
-        if (s > s_max) {  // the end is reachable by s_max: inconsistency
-          st = kPairInternal;
-          break;
-        }
-        int q;
-        q = slm - a.pen.x;
-        if (q < 0) q += rm;
-        const int slot_mm = q;
-        q = slm - a.pen.go;
-        if (q < 0) q += rm;
-        const int slot_mo = q;
-        q = sli - a.pen.ge;
-        if (q < 0) q += re;
-        const int slot_ie = rm + q;  // (unused by kLin)
-        const int slot_de = rm + re + q;
-        // sources: first diagonal, cell count (0 = null), ring index of lo.
-        // Slot limits are either a trimmed range inside the slot's compute
-        // range or the empty range (1, 0); the count is taken by comparison.
-        int lo_mm = 0, c_mm = 0, b_mm = 0, lo_mo = 0, c_mo = 0, b_mo = 0;
-        int lo_ie = 0, c_ie = 0, b_ie = 0, lo_de = 0, c_de = 0, b_de = 0;
-        auto src = [&](int slot, int& lo_x, int& c_x, int& b_x) {
-          const int l = s_lo[slot], h = s_hi[slot];
-          if (h >= l) {
-            lo_x = l;
-            c_x = h - l + 1;
-            b_x = slot * W + l - s_alo[slot];
+      // One score step: the wavefronts of score s + 1 from the ring.  kH (a
+      // compile-time tag): write the step's backtrace words and step-table
+      // entry; detect: test for the end (not while recomputing history).
+      auto step = [&](auto hist_tag, bool detect) {
+        constexpr bool kH = kCigar && decltype(hist_tag)::value;
+          ++s;
+          if (++slm == rm) slm = 0;
+          if constexpr (!kLin) {
+            if (++sli == re) sli = 0;
           }
-        };
-        if (s - a.pen.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
-        if (s - a.pen.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
-        if (!kLin && s - a.pen.ge >= 0) {
-          src(slot_ie, lo_ie, c_ie, b_ie);
-          src(slot_de, lo_de, c_de, b_de);
-        }
-        // second gap piece (kDual): M at s - o2 - e2, I2 / D2 at s - e2
-        int lo_mo2 = 0, c_mo2 = 0, b_mo2 = 0, lo_ie2 = 0, c_ie2 = 0, b_ie2 = 0, lo_de2 = 0, c_de2 = 0, b_de2 = 0;
-        int out_i2 = 0, out_d2 = 0;
-        if constexpr (kDual) {
-          const int re2 = a.pen.re2;
-          q = slm - a.pen.go2;
+          if constexpr (kDual) {
+            if (++sli2 == a.pen.re2) sli2 = 0;
+          }
+          if (s > s_max) {  // the end is reachable by s_max: inconsistency
+            st = kPairInternal;
+            return;
+          }
+          int q;
+          q = slm - a.pen.x;
           if (q < 0) q += rm;
-          if (s - a.pen.go2 >= 0) src(q, lo_mo2, c_mo2, b_mo2);
-          q = sli2 - a.pen.ge2;
-          if (q < 0) q += re2;
-          if (s - a.pen.ge2 >= 0) {
-            src(rm + 2 * re + q, lo_ie2, c_ie2, b_ie2);
-            src(rm + 2 * re + re2 + q, lo_de2, c_de2, b_de2);
+          const int slot_mm = q;
+          q = slm - a.pen.go;
+          if (q < 0) q += rm;
+          const int slot_mo = q;
+          q = sli - a.pen.ge;
+          if (q < 0) q += re;
+          const int slot_ie = rm + q;  // (unused by kLin)
+          const int slot_de = rm + re + q;
+          // sources: first diagonal, cell count (0 = null), ring index of lo.
+          // Slot limits are either a trimmed range inside the slot's compute
+          // range or the empty range (1, 0); the count is taken by comparison.
+          int lo_mm = 0, c_mm = 0, b_mm = 0, lo_mo = 0, c_mo = 0, b_mo = 0;
+          int lo_ie = 0, c_ie = 0, b_ie = 0, lo_de = 0, c_de = 0, b_de = 0;
+          auto src = [&](int slot, int& lo_x, int& c_x, int& b_x) {
+            const int l = s_lo[slot], h = s_hi[slot];
+            if (h >= l) {
+              lo_x = l;
+              c_x = h - l + 1;
+              b_x = slot * W + l - s_alo[slot];
+            }
+          };
+          if (s - a.pen.x >= 0) src(slot_mm, lo_mm, c_mm, b_mm);
+          if (s - a.pen.go >= 0) src(slot_mo, lo_mo, c_mo, b_mo);
+          if (!kLin && s - a.pen.ge >= 0) {
+            src(slot_ie, lo_ie, c_ie, b_ie);
+            src(slot_de, lo_de, c_de, b_de);
           }
-          out_i2 = rm + 2 * re + sli2;
-          out_d2 = rm + 2 * re + re2 + sli2;
-        }
-        const int out_m = slm, out_i = rm + sli, out_d = rm + re + sli;
-        if ((c_mm | c_mo | c_ie | c_de | c_mo2 | c_ie2 | c_de2) == 0) {  // null step (wfa_gpu.cu:417-422)
-          group_sync<GW>(gid);  // everyone has read the slot limits
-          s_lo[out_m] = 1; s_hi[out_m] = 0;
-          if constexpr (!kLin) {
-            s_lo[out_i] = 1; s_hi[out_i] = 0;
-            s_lo[out_d] = 1; s_hi[out_d] = 0;
-          }
+          // second gap piece (kDual): M at s - o2 - e2, I2 / D2 at s - e2
+          int lo_mo2 = 0, c_mo2 = 0, b_mo2 = 0, lo_ie2 = 0, c_ie2 = 0, b_ie2 = 0, lo_de2 = 0, c_de2 = 0, b_de2 = 0;
+          int out_i2 = 0, out_d2 = 0;
           if constexpr (kDual) {
-            s_lo[out_i2] = 1; s_hi[out_i2] = 0;
-            s_lo[out_d2] = 1; s_hi[out_d2] = 0;
+            const int re2 = a.pen.re2;
+            q = slm - a.pen.go2;
+            if (q < 0) q += rm;
+            if (s - a.pen.go2 >= 0) src(q, lo_mo2, c_mo2, b_mo2);
+            q = sli2 - a.pen.ge2;
+            if (q < 0) q += re2;
+            if (s - a.pen.ge2 >= 0) {
+              src(rm + 2 * re + q, lo_ie2, c_ie2, b_ie2);
+              src(rm + 2 * re + re2 + q, lo_de2, c_de2, b_de2);
+            }
+            out_i2 = rm + 2 * re + sli2;
+            out_d2 = rm + 2 * re + re2 + sli2;
           }
-          if constexpr (GW == 1) __syncwarp();
-          continue;
-        }
-        int lo = INT_MAX, hi = INT_MIN;  // envelope of the sources (wfa_gpu.cu:429-439)
-        if (c_mm) { lo = lo_mm; hi = lo_mm + c_mm - 1; }
-        if (c_mo) { lo = min(lo, lo_mo - 1); hi = max(hi, lo_mo + c_mo); }
-        if (c_ie) { lo = min(lo, lo_ie + 1); hi = max(hi, lo_ie + c_ie); }
-        if (c_de) { lo = min(lo, lo_de - 1); hi = max(hi, lo_de + c_de - 2); }
-        if constexpr (kDual) {
-          if (c_mo2) { lo = min(lo, lo_mo2 - 1); hi = max(hi, lo_mo2 + c_mo2); }
-          if (c_ie2) { lo = min(lo, lo_ie2 + 1); hi = max(hi, lo_ie2 + c_ie2); }
-          if (c_de2) { lo = min(lo, lo_de2 - 1); hi = max(hi, lo_de2 + c_de2 - 2); }
-        }
-        const int width = hi - lo + 1;
-        const bool i_present = !kLin && (c_mo || c_ie);
-        const bool d_present = !kLin && (c_mo || c_de);
-        const bool i2_present = kDual && (c_mo2 || c_ie2);
-        const bool d2_present = kDual && (c_mo2 || c_de2);
-        if (width > W || (kCigar && (s >= a.table_cap || hbase + width > a.hist_cap))) {
-          st = kPairScratch;
-          break;
-        }
-        const int w_m = out_m * W - lo, w_i = out_i * W - lo, w_d = out_d * W - lo;
-        const int w_i2 = out_i2 * W - lo, w_d2 = out_d2 * W - lo;
-        uint32_t* hrow = kCigar ? hist + hbase - lo : nullptr;
-        int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
-        int fi2 = INT_MAX, li2 = INT_MIN, fd2 = INT_MAX, ld2 = INT_MIN;
-        int fk = INT_MAX;  // lowest ending diagonal of this thread
-        for (int k = lo + gt; k <= hi; k += GT) {
-          int j;
-          j = k - 1 - lo_mo;
-          const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
-          j = k - 1 - lo_ie;
-          const int32_t ins_e = (!kLin && (unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
-          j = k + 1 - lo_mo;
-          const int32_t del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
-          j = k + 1 - lo_de;
-          const int32_t del_e = (!kLin && (unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
-          j = k - lo_mm;
-          const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
-          const int32_t ins = max(ins_o, ins_e) + 1;
-          const int32_t del = max(del_o, del_e);
-          int32_t ins2 = kNull, del2 = kNull;
-          uint32_t bits;
-          int32_t p;
-          if constexpr (kDual) {
-            j = k - 1 - lo_mo2;
-            const int32_t ins2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
-            j = k - 1 - lo_ie2;
-            const int32_t ins2_e = ((unsigned)j < (unsigned)c_ie2) ? (int32_t)ring[b_ie2 + j] : kNull;
-            j = k + 1 - lo_mo2;
-            const int32_t del2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
-            j = k + 1 - lo_de2;
-            const int32_t del2_e = ((unsigned)j < (unsigned)c_de2) ? (int32_t)ring[b_de2 + j] : kNull;
-            ins2 = max(ins2_o, ins2_e) + 1;
-            del2 = max(del2_o, del2_e);
-            // M = max(mismatch, D2, D1, I2, I1), ties in that order
-            // (piggyback codes 9 > 8,7 > 6,5 > 4,3 > 2,1)
-            p = ins;
-            bits = kSrcIns;
-            if (ins2 >= p) { p = ins2; bits = kSrcIns2; }
-            if (del >= p) { p = del; bits = kSrcDel; }
-            if (del2 >= p) { p = del2; bits = kSrcDel2; }
-            if (mis >= p) { p = mis; bits = kSrcMis; }
-            if (ins_e >= ins_o) bits |= kI1Ext2;
-            if (del_e >= del_o) bits |= kD1Ext2;
-            if (ins2_e >= ins2_o) bits |= kI2Ext2;
-            if (del2_e >= del2_o) bits |= kD2Ext2;
-          } else {
-            // M = max(D, mismatch, I); ties: mismatch > D > I (piggyback order)
-            p = ins;
-            bits = kSrcIns;
-            if (del >= p) { p = del; bits = kSrcDel; }
-            if (mis >= p) { p = mis; bits = kSrcMis; }
+          const int out_m = slm, out_i = rm + sli, out_d = rm + re + sli;
+          if ((c_mm | c_mo | c_ie | c_de | c_mo2 | c_ie2 | c_de2) == 0) {  // null step (wfa_gpu.cu:417-422)
+            group_sync<GW>(gid);  // everyone has read the slot limits
+            s_lo[out_m] = 1; s_hi[out_m] = 0;
             if constexpr (!kLin) {
-              if (ins_e >= ins_o) bits |= kIExt;
-              if (del_e >= del_o) bits |= kDExt;
+              s_lo[out_i] = 1; s_hi[out_i] = 0;
+              s_lo[out_d] = 1; s_hi[out_d] = 0;
             }
-          }
-          int32_t om = kNull;
-          if (in_bounds(p, k, m, n)) {
-            const int vv = p - k;
-            const int rem = min(m - vv, n - p);
-            om = p + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem));
-            fm = min(fm, k);
-            lm = k;
-            bool ends = (om >= n) & (k <= k_hi);
-            if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
-            if (ends) fk = min(fk, k);
-          }
-          store(w_m + k, om);
-          if (i_present) {
-            store(w_i + k, ins);
-            if (in_bounds(ins, k, m, n)) { fi = min(fi, k); li = k; }
-          }
-          if (d_present) {
-            store(w_d + k, del);
-            if (in_bounds(del, k, m, n)) { fd = min(fd, k); ld = k; }
-          }
-          if constexpr (kDual) {
-            if (i2_present) {
-              store(w_i2 + k, ins2);
-              if (in_bounds(ins2, k, m, n)) { fi2 = min(fi2, k); li2 = k; }
-            }
-            if (d2_present) {
-              store(w_d2 + k, del2);
-              if (in_bounds(del2, k, m, n)) { fd2 = min(fd2, k); ld2 = k; }
-            }
-          }
-          if (kCigar) hrow[k] = ((uint32_t)p << (kDual ? 8 : 4)) | bits;
-        }
-        fm = __reduce_min_sync(FULL, fm);
-        lm = __reduce_max_sync(FULL, lm);
-        fi = __reduce_min_sync(FULL, fi);
-        li = __reduce_max_sync(FULL, li);
-        fd = __reduce_min_sync(FULL, fd);
-        ld = __reduce_max_sync(FULL, ld);
-        fk = __reduce_min_sync(FULL, fk);
-        if constexpr (kDual) {
-          fi2 = __reduce_min_sync(FULL, fi2);
-          li2 = __reduce_max_sync(FULL, li2);
-          fd2 = __reduce_min_sync(FULL, fd2);
-          ld2 = __reduce_max_sync(FULL, ld2);
-        }
-        if constexpr (GW > 1) {
-          int* pp = part + ((s & 1) * GW + wig) * PW;
-          if (lane == 0) {
-            pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = fk;
             if constexpr (kDual) {
-              pp[7] = fi2; pp[8] = li2; pp[9] = fd2; pp[10] = ld2;
+              s_lo[out_i2] = 1; s_hi[out_i2] = 0;
+              s_lo[out_d2] = 1; s_hi[out_d2] = 0;
             }
+            if constexpr (GW == 1) __syncwarp();
+            return;
           }
-          group_sync<GW>(gid);  // the step's ring writes and partials are complete
-          // lane w takes warp w's partials; warp reductions combine them
-          // (7 loads and 7 reductions per thread instead of 7 * GW)
-          int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = INT_MAX;
-          int p7 = INT_MAX, p8 = INT_MIN, p9 = INT_MAX, p10 = INT_MIN;
-          if (lane < GW) {
-            const int* qw = part + ((s & 1) * GW + lane) * PW;
-            p0 = qw[0]; p1 = qw[1]; p2 = qw[2]; p3 = qw[3]; p4 = qw[4]; p5 = qw[5]; p6 = qw[6];
+          int lo = INT_MAX, hi = INT_MIN;  // envelope of the sources (wfa_gpu.cu:429-439)
+          if (c_mm) { lo = lo_mm; hi = lo_mm + c_mm - 1; }
+          if (c_mo) { lo = min(lo, lo_mo - 1); hi = max(hi, lo_mo + c_mo); }
+          if (c_ie) { lo = min(lo, lo_ie + 1); hi = max(hi, lo_ie + c_ie); }
+          if (c_de) { lo = min(lo, lo_de - 1); hi = max(hi, lo_de + c_de - 2); }
+          if constexpr (kDual) {
+            if (c_mo2) { lo = min(lo, lo_mo2 - 1); hi = max(hi, lo_mo2 + c_mo2); }
+            if (c_ie2) { lo = min(lo, lo_ie2 + 1); hi = max(hi, lo_ie2 + c_ie2); }
+            if (c_de2) { lo = min(lo, lo_de2 - 1); hi = max(hi, lo_de2 + c_de2 - 2); }
+          }
+          const int width = hi - lo + 1;
+          const bool i_present = !kLin && (c_mo || c_ie);
+          const bool d_present = !kLin && (c_mo || c_de);
+          const bool i2_present = kDual && (c_mo2 || c_ie2);
+          const bool d2_present = kDual && (c_mo2 || c_de2);
+          if (width > W || (kH && (s >= a.table_cap || hbase + width > a.hist_cap))) {
+            st = kPairScratch;
+            return;
+          }
+          const int w_m = out_m * W - lo, w_i = out_i * W - lo, w_d = out_d * W - lo;
+          const int w_i2 = out_i2 * W - lo, w_d2 = out_d2 * W - lo;
+          uint32_t* hrow = kH ? hist + hbase - lo : nullptr;
+          int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
+          int fi2 = INT_MAX, li2 = INT_MIN, fd2 = INT_MAX, ld2 = INT_MIN;
+          int fk = INT_MAX;  // lowest ending diagonal of this thread
+          for (int k = lo + gt; k <= hi; k += GT) {
+            int j;
+            j = k - 1 - lo_mo;
+            const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+            j = k - 1 - lo_ie;
+            const int32_t ins_e = (!kLin && (unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
+            j = k + 1 - lo_mo;
+            const int32_t del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+            j = k + 1 - lo_de;
+            const int32_t del_e = (!kLin && (unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
+            j = k - lo_mm;
+            const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
+            const int32_t ins = max(ins_o, ins_e) + 1;
+            const int32_t del = max(del_o, del_e);
+            int32_t ins2 = kNull, del2 = kNull;
+            uint32_t bits;
+            int32_t p;
             if constexpr (kDual) {
-              p7 = qw[7]; p8 = qw[8]; p9 = qw[9]; p10 = qw[10];
+              j = k - 1 - lo_mo2;
+              const int32_t ins2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+              j = k - 1 - lo_ie2;
+              const int32_t ins2_e = ((unsigned)j < (unsigned)c_ie2) ? (int32_t)ring[b_ie2 + j] : kNull;
+              j = k + 1 - lo_mo2;
+              const int32_t del2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+              j = k + 1 - lo_de2;
+              const int32_t del2_e = ((unsigned)j < (unsigned)c_de2) ? (int32_t)ring[b_de2 + j] : kNull;
+              ins2 = max(ins2_o, ins2_e) + 1;
+              del2 = max(del2_o, del2_e);
+              // M = max(mismatch, D2, D1, I2, I1), ties in that order
+              // (piggyback codes 9 > 8,7 > 6,5 > 4,3 > 2,1)
+              p = ins;
+              bits = kSrcIns;
+              if (ins2 >= p) { p = ins2; bits = kSrcIns2; }
+              if (del >= p) { p = del; bits = kSrcDel; }
+              if (del2 >= p) { p = del2; bits = kSrcDel2; }
+              if (mis >= p) { p = mis; bits = kSrcMis; }
+              if (ins_e >= ins_o) bits |= kI1Ext2;
+              if (del_e >= del_o) bits |= kD1Ext2;
+              if (ins2_e >= ins2_o) bits |= kI2Ext2;
+              if (del2_e >= del2_o) bits |= kD2Ext2;
+            } else {
+              // M = max(D, mismatch, I); ties: mismatch > D > I (piggyback order)
+              p = ins;
+              bits = kSrcIns;
+              if (del >= p) { p = del; bits = kSrcDel; }
+              if (mis >= p) { p = mis; bits = kSrcMis; }
+              if constexpr (!kLin) {
+                if (ins_e >= ins_o) bits |= kIExt;
+                if (del_e >= del_o) bits |= kDExt;
+              }
+            }
+            int32_t om = kNull;
+            if (in_bounds(p, k, m, n)) {
+              const int vv = p - k;
+              const int rem = min(m - vv, n - p);
+              om = p + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem));
+              fm = min(fm, k);
+              lm = k;
+              bool ends = (om >= n) & (k <= k_hi);
+              if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
+              if (ends) fk = min(fk, k);
+            }
+            store(w_m + k, om);
+            if (i_present) {
+              store(w_i + k, ins);
+              if (in_bounds(ins, k, m, n)) { fi = min(fi, k); li = k; }
+            }
+            if (d_present) {
+              store(w_d + k, del);
+              if (in_bounds(del, k, m, n)) { fd = min(fd, k); ld = k; }
+            }
+            if constexpr (kDual) {
+              if (i2_present) {
+                store(w_i2 + k, ins2);
+                if (in_bounds(ins2, k, m, n)) { fi2 = min(fi2, k); li2 = k; }
+              }
+              if (d2_present) {
+                store(w_d2 + k, del2);
+                if (in_bounds(del2, k, m, n)) { fd2 = min(fd2, k); ld2 = k; }
+              }
+            }
+            if constexpr (kH) hrow[k] = ((uint32_t)p << (kDual ? 8 : 4)) | bits;
+          }
+          fm = __reduce_min_sync(FULL, fm);
+          lm = __reduce_max_sync(FULL, lm);
+          fi = __reduce_min_sync(FULL, fi);
+          li = __reduce_max_sync(FULL, li);
+          fd = __reduce_min_sync(FULL, fd);
+          ld = __reduce_max_sync(FULL, ld);
+          fk = __reduce_min_sync(FULL, fk);
+          if constexpr (kDual) {
+            fi2 = __reduce_min_sync(FULL, fi2);
+            li2 = __reduce_max_sync(FULL, li2);
+            fd2 = __reduce_min_sync(FULL, fd2);
+            ld2 = __reduce_max_sync(FULL, ld2);
+          }
+          if constexpr (GW > 1) {
+            int* pp = part + ((s & 1) * GW + wig) * PW;
+            if (lane == 0) {
+              pp[0] = fm; pp[1] = lm; pp[2] = fi; pp[3] = li; pp[4] = fd; pp[5] = ld; pp[6] = fk;
+              if constexpr (kDual) {
+                pp[7] = fi2; pp[8] = li2; pp[9] = fd2; pp[10] = ld2;
+              }
+            }
+            group_sync<GW>(gid);  // the step's ring writes and partials are complete
+            // lane w takes warp w's partials; warp reductions combine them
+            // (7 loads and 7 reductions per thread instead of 7 * GW)
+            int p0 = INT_MAX, p1 = INT_MIN, p2 = INT_MAX, p3 = INT_MIN, p4 = INT_MAX, p5 = INT_MIN, p6 = INT_MAX;
+            int p7 = INT_MAX, p8 = INT_MIN, p9 = INT_MAX, p10 = INT_MIN;
+            if (lane < GW) {
+              const int* qw = part + ((s & 1) * GW + lane) * PW;
+              p0 = qw[0]; p1 = qw[1]; p2 = qw[2]; p3 = qw[3]; p4 = qw[4]; p5 = qw[5]; p6 = qw[6];
+              if constexpr (kDual) {
+                p7 = qw[7]; p8 = qw[8]; p9 = qw[9]; p10 = qw[10];
+              }
+            }
+            fm = __reduce_min_sync(FULL, p0);
+            lm = __reduce_max_sync(FULL, p1);
+            fi = __reduce_min_sync(FULL, p2);
+            li = __reduce_max_sync(FULL, p3);
+            fd = __reduce_min_sync(FULL, p4);
+            ld = __reduce_max_sync(FULL, p5);
+            fk = __reduce_min_sync(FULL, p6);
+            if constexpr (kDual) {
+              fi2 = __reduce_min_sync(FULL, p7);
+              li2 = __reduce_max_sync(FULL, p8);
+              fd2 = __reduce_min_sync(FULL, p9);
+              ld2 = __reduce_max_sync(FULL, p10);
             }
           }
-          fm = __reduce_min_sync(FULL, p0);
-          lm = __reduce_max_sync(FULL, p1);
-          fi = __reduce_min_sync(FULL, p2);
-          li = __reduce_max_sync(FULL, p3);
-          fd = __reduce_min_sync(FULL, p4);
-          ld = __reduce_max_sync(FULL, p5);
-          fk = __reduce_min_sync(FULL, p6);
-          if constexpr (kDual) {
-            fi2 = __reduce_min_sync(FULL, p7);
-            li2 = __reduce_max_sync(FULL, p8);
-            fd2 = __reduce_min_sync(FULL, p9);
-            ld2 = __reduce_max_sync(FULL, p10);
+          {
+            // trimmed limits (wfa_gpu.cu:636-719), written by every thread
+            // (identical values); no in-bounds cell (first > last) stores the
+            // empty range (1, 0)
+            const bool em = fm > lm, ei = !i_present || fi > li, ed = !d_present || fd > ld;
+            s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
+            if constexpr (!kLin) {
+              s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
+              s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
+            }
+            if constexpr (kDual) {
+              const bool ei2 = !i2_present || fi2 > li2, ed2 = !d2_present || fd2 > ld2;
+              s_lo[out_i2] = ei2 ? 1 : fi2; s_hi[out_i2] = ei2 ? 0 : li2; s_alo[out_i2] = lo;
+              s_lo[out_d2] = ed2 ? 1 : fd2; s_hi[out_d2] = ed2 ? 0 : ld2; s_alo[out_d2] = lo;
+            }
+            if (kH && gt == 0) table[s] = make_int2(lo, (int)hbase);
+          }
+          if constexpr (kH) hbase += width;
+          n_cells += (unsigned long long)width;
+          ++n_steps;
+          if constexpr (GW == 1) __syncwarp();
+          if (detect && fk != INT_MAX) {
+            s_end = s;
+            k_fin = fk;
+          }
+      };
+
+      // Low-memory mode (a.ckpt_k = K > 0, CIGAR kernels): the score pass
+      // keeps no history; it saves the ring every K scores (each slot's
+      // limits and trimmed values) in the group's checkpoint area.  The
+      // backtrace then takes the segments (jK, (j+1)K] from the last to the
+      // first: restore checkpoint j, recompute the segment with history, walk
+      // down to score jK.  The recomputed words are the ones the full pass
+      // writes, so the CIGAR is the same.
+      uint8_t* const ck = lowmem ? a.ckpt + ggroup * a.ckpt_stride : nullptr;
+      (void)ck;
+      auto save_ckpt = [&](int jc) {
+        if (jc >= a.ckpt_cap) {
+          st = kPairScratch;
+          return;
+        }
+        uint8_t* base = ck + (int64_t)jc * a.ckpt_bytes;
+        int* lim = reinterpret_cast<int*>(base);
+        RT* val = reinterpret_cast<RT*>(base + 12 * ns);
+        for (int i = gt; i < ns; i += GT) {
+          lim[i] = s_lo[i];
+          lim[ns + i] = s_hi[i];
+          lim[2 * ns + i] = s_alo[i];
+        }
+        for (int sl = 0; sl < ns; ++sl) {
+          const int l = s_lo[sl], h = s_hi[sl];
+          const int b = sl * W - s_alo[sl];
+          for (int k = l + gt; k <= h; k += GT) val[b + k] = ring[b + k];
+        }
+        group_sync<GW>(gid);  // copied before the next step overwrites the ring
+      };
+      auto restore_ckpt = [&](int jc) {
+        const uint8_t* base = ck + (int64_t)jc * a.ckpt_bytes;
+        const int* lim = reinterpret_cast<const int*>(base);
+        const RT* val = reinterpret_cast<const RT*>(base + 12 * ns);
+        group_sync<GW>(gid);  // the previous segment is done with the ring and limits
+        for (int i = gt; i < ns; i += GT) {
+          s_lo[i] = lim[i];
+          s_hi[i] = lim[ns + i];
+          s_alo[i] = lim[2 * ns + i];
+        }
+        for (int sl = 0; sl < ns; ++sl) {
+          const int l = lim[sl], h = lim[ns + sl];
+          const int b = sl * W - lim[2 * ns + sl];
+          for (int k = l + gt; k <= h; k += GT) ring[b + k] = val[b + k];
+        }
+        group_sync<GW>(gid);
+      };
+
+      if constexpr (lowmem) {
+        if (st == kPairOk && s_end < 0) save_ckpt(0);
+        while (s_end < 0 && st == kPairOk) {
+          step(std::false_type{}, true);
+          if (st == kPairOk && s % K == 0) save_ckpt(s / K);
+        }
+        if (st == kPairOk && s_end >= a.table_cap) st = kPairScratch;
+      } else {
+        while (s_end < 0 && st == kPairOk) step(std::true_type{}, true);
+      }
+
+      if constexpr (lowmem) {
+       if (st == kPairOk) {
+        // reserve the run bound in the arena, then walk segment by segment
+        const int64_t bound = 2 * (int64_t)s_end / a.pen.min_pen() + 3;  // + a free gap at each end
+        unsigned long long at = 0;
+        if (gt == 0) {
+          at = atomicAdd(a.arena_cursor, (unsigned long long)bound);
+          bc[2] = ((int64_t)(at + bound) > a.arena_cap) ? kPairArena : kPairOk;
+        }
+        group_sync<GW>(gid);
+        st = bc[2];
+        Walk wk;
+        if (gt == 0 && st == kPairOk) walk_begin(wk, s_end, k_fin, m, n, a.arena + at + bound, (int)bound);
+        for (int jc = s_end > 0 ? (s_end - 1) / K : -1; jc >= 0 && st == kPairOk; --jc) {
+          restore_ckpt(jc);
+          s = jc * K;
+          slm = s % rm;
+          if constexpr (!kLin) sli = s % re;
+          if constexpr (kDual) sli2 = s % a.pen.re2;
+          hbase = 0;
+          const int s_stop = min(s + K, s_end);
+          while (s < s_stop && st == kPairOk) step(std::true_type{}, false);
+          if (st != kPairOk) break;
+          group_sync<GW>(gid);  // the segment's backtrace words and step table are written
+          if (gt == 0) {
+            int r;
+            if constexpr (kDual)
+              r = walk_run_dual(wk, hist, hbase, table, jc * K, a.pen);
+            else
+              r = walk_run(wk, hist, hbase, table, jc * K, a.pen.x, a.pen.go, a.pen.ge);
+            bc[2] = r ? kPairInternal : kPairOk;
+            bc[3] = walk_done(wk) ? 1 : 0;
+          }
+          group_sync<GW>(gid);
+          st = bc[2];
+          if (bc[3]) break;
+        }
+        if (gt == 0 && st == kPairOk) {
+          const int r = walk_finish(wk);
+          if (r < 0) {
+            st = kPairInternal;
+          } else {
+            lm_len = r;
+            lm_pos = (int64_t)(at + bound) - r;
           }
         }
-        {
-          // trimmed limits (wfa_gpu.cu:636-719), written by every thread
-          // (identical values); no in-bounds cell (first > last) stores the
-          // empty range (1, 0)
-          const bool em = fm > lm, ei = !i_present || fi > li, ed = !d_present || fd > ld;
-          s_lo[out_m] = em ? 1 : fm; s_hi[out_m] = em ? 0 : lm; s_alo[out_m] = lo;
-          if constexpr (!kLin) {
-            s_lo[out_i] = ei ? 1 : fi; s_hi[out_i] = ei ? 0 : li; s_alo[out_i] = lo;
-            s_lo[out_d] = ed ? 1 : fd; s_hi[out_d] = ed ? 0 : ld; s_alo[out_d] = lo;
-          }
-          if constexpr (kDual) {
-            const bool ei2 = !i2_present || fi2 > li2, ed2 = !d2_present || fd2 > ld2;
-            s_lo[out_i2] = ei2 ? 1 : fi2; s_hi[out_i2] = ei2 ? 0 : li2; s_alo[out_i2] = lo;
-            s_lo[out_d2] = ed2 ? 1 : fd2; s_hi[out_d2] = ed2 ? 0 : ld2; s_alo[out_d2] = lo;
-          }
-          if (kCigar && gt == 0) table[s] = make_int2(lo, (int)hbase);
-        }
-        hbase += width;
-        n_cells += (unsigned long long)width;
-        ++n_steps;
-        if constexpr (GW == 1) __syncwarp();
-        if (fk != INT_MAX) {
-          s_end = s;
-          k_fin = fk;
-        }
+       }
       }
     }
 
     if (st == kPairOk) {
       if (gt == 0) a.score[pair] = s_end * a.g;
-      if (kCigar) {
+      if (kCigar && lowmem) {
+        if (gt == 0) {
+          a.cig_pos[pair] = lm_pos;
+          a.cig_len[pair] = lm_len;
+        }
+      } else if (kCigar) {
         // reserve the run bound 2*s/min_pen + 1 in the arena, then walk
         const int min_pen = a.pen.min_pen();
         const int64_t bound = 2 * (int64_t)s_end / min_pen + 3;  // + a free gap at each end

@@ -38,31 +38,76 @@ struct RunWriter {
   }
 };
 
+// A walk in progress: the position (s, k, offset), the component being
+// walked (0 = M; the one-piece walk uses 1 = I, 2 = D, the dual walk the
+// M-source codes of its word), and the runs written so far.  The walk runs
+// in pieces when the history is recomputed segment by segment (low-memory
+// mode): walk_*_run stops once the score falls to s_min or below.
+struct Walk {
+  RunWriter w;
+  uint32_t state;
+  int s, k;
+  int32_t off;
+  int v, h;
+  int guard;
+};
+
 // The walk starts on the end diagonal k_end (n - m end-to-end; with free
 // ends the diagonal the kernel found), at offset min(n, m + k_end): the text
 // or the pattern is consumed there, and the rest of the other is the free
 // trailing gap, written first.
-// Returns the number of runs, or -1 on an inconsistency (a word outside the
-// history, a predecessor beyond the current offset, more runs than cap).
-static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
-                              int s_end, int k_end, int m, int n, int x, int go, int ge, uint32_t* out_end, int cap) {
-  RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
+static __device__ __forceinline__ void walk_begin(Walk& wk, int s_end, int k_end, int m, int n, uint32_t* out_end,
+                                                  int cap) {
+  wk.w = RunWriter{out_end, 0, cap, 0xffffffffu, 0};
+  wk.state = 0;
+  wk.s = s_end;
+  wk.k = k_end;
+  wk.off = min(n, m + k_end);
+  wk.v = wk.off - wk.k;
+  wk.h = wk.off;
+  wk.guard = 4 * (m + n) + 8;
+  wk.w.put(kOpD, m - wk.v);
+  wk.w.put(kOpI, n - wk.h);
+}
+
+// Whether the walk reached the start (nothing left but matches and the free
+// leading gap).
+static __device__ __forceinline__ bool walk_done(const Walk& wk) { return !(wk.v > 0 && wk.h > 0 && wk.s > 0); }
+
+// The leading matches and free leading gap; the number of runs, or -1.
+static __device__ __forceinline__ int walk_finish(Walk& wk) {
+  if (wk.v > 0 && wk.h > 0) {
+    const int nm = wk.v < wk.h ? wk.v : wk.h;
+    wk.w.put(kOpM, nm);
+    wk.v -= nm;
+    wk.h -= nm;
+  }
+  wk.w.put(kOpD, wk.v);
+  wk.w.put(kOpI, wk.h);
+  wk.w.flush();
+  return wk.w.cnt <= wk.w.cap ? wk.w.cnt : -1;
+}
+
+// One-piece (and gap-linear) walk down to score s_min.  0, or -1 on an
+// inconsistency (a word outside the history, a predecessor beyond the
+// current offset, a negative score).
+static __device__ int walk_run(Walk& wk, const uint32_t* __restrict__ hist, int64_t hist_used,
+                               const int2* __restrict__ table, int s_min, int x, int go, int ge) {
   enum { M = 0, I = 1, D = 2 };
-  int state = M, s = s_end, k = k_end;
-  int32_t off = min(n, m + k_end);
-  int v = off - k, h = off;
-  w.put(kOpD, m - v);
-  w.put(kOpI, n - h);
-  int guard = 4 * (m + n) + 8;
-  while (v > 0 && h > 0 && s > 0) {
-    if (--guard < 0) return -1;
+  uint32_t state = wk.state;
+  int s = wk.s, k = wk.k, v = wk.v, h = wk.h, guard = wk.guard;
+  int32_t off = wk.off;
+  RunWriter& w = wk.w;
+  int rc = 0;
+  while (v > 0 && h > 0 && s > s_min) {
+    if (--guard < 0) { rc = -1; break; }
     const int2 te = table[s];
     const int64_t hidx = (int64_t)te.y + (k - te.x);
-    if (k < te.x || hidx >= hist_used) return -1;  // never on a valid path
+    if (k < te.x || hidx >= hist_used) { rc = -1; break; }  // never on a valid path
     const uint32_t word = hist[hidx];
     if (state == M) {
       const int32_t p = (int32_t)(word >> 4);
-      if (p > off) return -1;
+      if (p > off) { rc = -1; break; }
       w.put(kOpM, off - p);
       off = p;
       v = off - k;
@@ -115,46 +160,39 @@ static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t 
     }
     v = off - k;
     h = off;
-    if (s < 0) return -1;
+    if (s < 0) { rc = -1; break; }
   }
-  if (v > 0 && h > 0) {
-    const int nm = v < h ? v : h;
-    w.put(kOpM, nm);
-    v -= nm;
-    h -= nm;
-  }
-  w.put(kOpD, v);
-  w.put(kOpI, h);
-  w.flush();
-  return w.cnt <= cap ? w.cnt : -1;
+  wk.state = state;
+  wk.s = s;
+  wk.k = k;
+  wk.off = off;
+  wk.v = v;
+  wk.h = h;
+  wk.guard = guard;
+  return rc;
 }
 
-// Dual gap-affine walk over words of the kDual kernel: five states (M, I1,
-// D1, I2, D2); in M the 3-bit source picks the component, whose extension
-// bit (kI1Ext2 ... kD2Ext2) then says open (back to M, s - o_j - e_j) or
-// extend (stay, s - e_j).  Same return convention as backtrace_walk.
-static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int64_t hist_used,
-                                          const int2* __restrict__ table, int s_end, int k_end, int m, int n,
-                                          const Pen& pen, uint32_t* out_end, int cap) {
-  RunWriter w{out_end, 0, cap, 0xffffffffu, 0};
-  // state = M source code of the component being walked (kSrcMis for M)
-  uint32_t state = kSrcMis;
-  int s = s_end, k = k_end;
-  int32_t off = min(n, m + k_end);
-  int v = off - k, h = off;
-  w.put(kOpD, m - v);
-  w.put(kOpI, n - h);
-  int guard = 4 * (m + n) + 8;
-  while (v > 0 && h > 0 && s > 0) {
-    if (--guard < 0) return -1;
+// Dual gap-affine walk over words of the kModelDual kernel: five states (M,
+// I1, D1, I2, D2); in M the 3-bit source picks the component, whose
+// extension bit (kI1Ext2 ... kD2Ext2) then says open (back to M,
+// s - o_j - e_j) or extend (stay, s - e_j).  Same conventions as walk_run.
+static __device__ int walk_run_dual(Walk& wk, const uint32_t* __restrict__ hist, int64_t hist_used,
+                                    const int2* __restrict__ table, int s_min, const Pen& pen) {
+  uint32_t state = wk.state;  // M-source code of the component being walked (kSrcMis for M)
+  int s = wk.s, k = wk.k, v = wk.v, h = wk.h, guard = wk.guard;
+  int32_t off = wk.off;
+  RunWriter& w = wk.w;
+  int rc = 0;
+  while (v > 0 && h > 0 && s > s_min) {
+    if (--guard < 0) { rc = -1; break; }
     const int2 te = table[s];
     const int64_t hidx = (int64_t)te.y + (k - te.x);
-    if (k < te.x || hidx >= hist_used) return -1;  // never on a valid path
+    if (k < te.x || hidx >= hist_used) { rc = -1; break; }  // never on a valid path
     const uint32_t word = hist[hidx];
     uint32_t comp = state;
     if (state == kSrcMis) {
       const int32_t p = (int32_t)(word >> 8);
-      if (p > off) return -1;
+      if (p > off) { rc = -1; break; }
       w.put(kOpM, off - p);
       off = p;
       v = off - k;
@@ -167,7 +205,7 @@ static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int
         --off;
         v = off - k;
         h = off;
-        if (s < 0) return -1;
+        if (s < 0) { rc = -1; break; }
         continue;
       }
     }
@@ -178,8 +216,9 @@ static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int
       case kSrcDel: ext = word & kD1Ext2; ins = false; go = pen.go; ge = pen.ge; break;
       case kSrcIns2: ext = word & kI2Ext2; ins = true; go = pen.go2; ge = pen.ge2; break;
       case kSrcDel2: ext = word & kD2Ext2; ins = false; go = pen.go2; ge = pen.ge2; break;
-      default: return -1;
+      default: ext = ins = false; go = ge = 0; rc = -1; break;
     }
+    if (rc) break;
     if (ins) {
       w.put(kOpI, 1);
       --k;
@@ -197,18 +236,36 @@ static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int
     }
     v = off - k;
     h = off;
-    if (s < 0) return -1;
+    if (s < 0) { rc = -1; break; }
   }
-  if (v > 0 && h > 0) {
-    const int nm = v < h ? v : h;
-    w.put(kOpM, nm);
-    v -= nm;
-    h -= nm;
-  }
-  w.put(kOpD, v);
-  w.put(kOpI, h);
-  w.flush();
-  return w.cnt <= cap ? w.cnt : -1;
+  wk.state = state;
+  wk.s = s;
+  wk.k = k;
+  wk.off = off;
+  wk.v = v;
+  wk.h = h;
+  wk.guard = guard;
+  return rc;
+}
+
+// The whole walk at once (history of every score in memory).  Returns the
+// number of runs (written backwards, ending at out_end), or -1.
+static __device__ int backtrace_walk(const uint32_t* __restrict__ hist, int64_t hist_used, const int2* __restrict__ table,
+                                     int s_end, int k_end, int m, int n, int x, int go, int ge, uint32_t* out_end,
+                                     int cap) {
+  Walk wk;
+  walk_begin(wk, s_end, k_end, m, n, out_end, cap);
+  if (walk_run(wk, hist, hist_used, table, 0, x, go, ge)) return -1;
+  return walk_finish(wk);
+}
+
+static __device__ int backtrace_walk_dual(const uint32_t* __restrict__ hist, int64_t hist_used,
+                                          const int2* __restrict__ table, int s_end, int k_end, int m, int n,
+                                          const Pen& pen, uint32_t* out_end, int cap) {
+  Walk wk;
+  walk_begin(wk, s_end, k_end, m, n, out_end, cap);
+  if (walk_run_dual(wk, hist, hist_used, table, 0, pen)) return -1;
+  return walk_finish(wk);
 }
 
 }  // namespace tsu

@@ -28,6 +28,9 @@ enum : uint32_t { kOpM = 0, kOpI = 1, kOpD = 2, kOpX = 8 };
 // gap-affine; gap-linear, which edit and indel distance are cases of)
 enum : int { kModeShared = 0, kModeGlobal = 1 };
 enum : int { kModelAffine = 0, kModelDual = 1, kModelLinear = 2 };
+// added to a model: the low-memory (checkpointed history) variant of its
+// CIGAR kernel with the global ring
+enum : int { kLowMemFlag = 8 };
 
 struct SeqView {
   int64_t n;  // pairs
@@ -155,7 +158,20 @@ struct AlignArgs {
   // h <= ef_tb, cost nothing, and so do ends (m, h), h >= n - ef_te, and
   // (v, n), v >= m - ef_pe
   int32_t ef_pb, ef_pe, ef_tb, ef_te;
+  // low-memory mode (ckpt_k > 0): checkpoints every ckpt_k scores, ckpt_cap
+  // of ckpt_bytes each per group (ckpt_stride bytes apart); the history then
+  // holds one segment of ckpt_k scores
+  uint8_t* ckpt;
+  int64_t ckpt_stride;
+  int32_t ckpt_bytes, ckpt_cap, ckpt_k;
 };
+
+// Bytes of one low-memory checkpoint: limits (3 ints per slot), then the
+// ring's values (ring_w per slot) in the ring's element type.
+__host__ __device__ inline int64_t ckpt_bytes_for(const Pen& p, int ring_w, int mode) {
+  const int64_t b = 12 * (int64_t)p.slots() + (int64_t)p.slots() * ring_w * (mode == kModeShared ? 2 : 4);
+  return (b + 15) & ~(int64_t)15;
+}
 
 // Warp partials per warp and step parity: 7 (one piece) or 11 values.
 __host__ __device__ inline int partial_words(const Pen& p) { return p.dual() ? 16 : 8; }

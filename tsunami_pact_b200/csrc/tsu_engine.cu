@@ -108,6 +108,9 @@ struct tsu_ctx {
   // free ends (tsu_set_ends_free): pattern begin, pattern end, text begin,
   // text end; all 0: end-to-end
   int32_t ends_free[4] = {0, 0, 0, 0};
+  // low-memory mode (tsu_set_low_memory): 0 off, > 0 checkpoint interval in
+  // score steps, < 0 chosen per pass
+  int32_t low_mem = 0;
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
             &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
@@ -274,27 +277,34 @@ struct BatchInfo {
 
 // The align_kernel instantiations (tsu_launch.cuh): gap-affine kernels here,
 // dual gap-affine ones in tsu_dual.cu, gap-linear ones in tsu_linear.cu.
+// lowmem: the checkpointed-history variant (CIGAR passes of a low-memory
+// context; global ring).
 cudaError_t align_occupancy(const tsu_ctx* ctx, bool cigar, int mode, int gw, int threads, size_t smem, int optin,
-                            int* occ) {
+                            int* occ, bool lowmem) {
   switch (ctx->rp.model()) {
-    case tsu::kModelDual: return tsu::align_occupancy_dual(cigar, mode, gw, threads, smem, optin, occ);
-    case tsu::kModelLinear: return tsu::align_occupancy_linear(cigar, mode, gw, threads, smem, optin, occ);
-    default: return tsu::launch_detail::occupancy<tsu::kModelAffine>(cigar, mode, gw, threads, smem, optin, occ);
+    case tsu::kModelDual: return tsu::align_occupancy_dual(cigar, mode, gw, threads, smem, optin, occ, lowmem);
+    case tsu::kModelLinear: return tsu::align_occupancy_linear(cigar, mode, gw, threads, smem, optin, occ, lowmem);
+    default:
+      return tsu::launch_detail::occupancy<tsu::kModelAffine>(cigar, mode, gw, threads, smem, optin, occ, lowmem);
   }
 }
 
 void launch_align(const tsu_ctx* ctx, bool cigar, int mode, int gw, int blocks, int threads, size_t smem,
                   cudaStream_t st, const tsu::AlignArgs& a) {
+  const bool lowmem = cigar && a.ckpt_k > 0;
   switch (ctx->rp.model()) {
-    case tsu::kModelDual: tsu::launch_align_dual(cigar, mode, gw, blocks, threads, smem, st, a); break;
-    case tsu::kModelLinear: tsu::launch_align_linear(cigar, mode, gw, blocks, threads, smem, st, a); break;
-    default: tsu::launch_detail::launch<tsu::kModelAffine>(cigar, mode, gw, blocks, threads, smem, st, a); break;
+    case tsu::kModelDual: tsu::launch_align_dual(cigar, mode, gw, blocks, threads, smem, st, a, lowmem); break;
+    case tsu::kModelLinear: tsu::launch_align_linear(cigar, mode, gw, blocks, threads, smem, st, a, lowmem); break;
+    default:
+      tsu::launch_detail::launch<tsu::kModelAffine>(cigar, mode, gw, blocks, threads, smem, st, a, lowmem);
+      break;
   }
 }
 
 // Scratch bytes of one group of a pass (ring, history, step table).
 size_t group_scratch_bytes(const tsu::PassGeom& g) {
-  return (size_t)(g.ring_ints * 4 + g.hist_cap * 4 + (int64_t)g.table_cap * 8 + 64);
+  return (size_t)(g.ring_ints * 4 + g.hist_cap * 4 + (int64_t)g.table_cap * 8 + (int64_t)g.ckpt_cap * g.ckpt_bytes +
+                  64);
 }
 
 // Configure a pass of configuration pc over pairs of at most bi's lengths:
@@ -303,13 +313,14 @@ size_t group_scratch_bytes(const tsu::PassGeom& g) {
 int plan_pass_within(tsu_ctx* ctx, const BatchInfo& bi, int64_t n_pairs, tsu::PassChoice pc, double hint,
                      bool want_cigar, size_t avail, Pass* out) {
   Pass p;
-  const tsu::PassGeom g = tsu::plan_geometry(ctx->rp, bi.max_m, bi.max_n, pc.mode,
-                                             pc.gw, hint, want_cigar, ctx->smem_optin);
+  const tsu::PassGeom g = tsu::plan_geometry(ctx->rp, bi.max_m, bi.max_n, pc.mode, pc.gw, hint, want_cigar,
+                                             ctx->smem_optin, want_cigar ? ctx->low_mem : 0);
   p.g = g;
   const int gpc = g.groups_per_cta;
   int occ = 0;
   cudaError_t e =
-      align_occupancy(ctx, want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, ctx->smem_optin, &occ);
+      align_occupancy(ctx, want_cigar, g.mode, g.gw, g.cta_threads, (size_t)gpc * g.group_smem, ctx->smem_optin, &occ,
+                      g.ckpt_k > 0);
   if (e != cudaSuccess || occ < 1) return set_err(ctx, TSU_EDEVICE, "occupancy query failed (%d)", (int)e);
   int64_t warps = (int64_t)ctx->sms * occ * gpc;  // groups
   const size_t per_warp = group_scratch_bytes(g);
@@ -445,6 +456,7 @@ size_t scratch_bytes(const Pass& ps, bool cigar) {
   size_t b = 0;
   if (cigar) b += up(4 * groups * (size_t)ps.g.hist_cap) + up(8 * groups * (size_t)ps.g.table_cap);
   if (ps.g.mode == tsu::kModeGlobal) b += up(4 * groups * (size_t)ps.g.ring_ints);
+  if (cigar && ps.g.ckpt_k > 0) b += up(groups * (size_t)ps.g.ckpt_cap * (size_t)ps.g.ckpt_bytes);
   return std::max<size_t>(b, 256);
 }
 
@@ -461,7 +473,20 @@ void carve_scratch(tsu_ctx* ctx, const Pass& ps, bool cigar, tsu::AlignArgs* a) 
     a->table = reinterpret_cast<int2*>(p);
     p += up(8 * groups * (size_t)ps.g.table_cap);
   }
-  if (ps.g.mode == tsu::kModeGlobal) a->ring_global = reinterpret_cast<int32_t*>(p);
+  a->ckpt = nullptr;
+  a->ckpt_k = a->ckpt_cap = a->ckpt_bytes = 0;
+  a->ckpt_stride = 0;
+  if (ps.g.mode == tsu::kModeGlobal) {
+    a->ring_global = reinterpret_cast<int32_t*>(p);
+    p += up(4 * groups * (size_t)ps.g.ring_ints);
+  }
+  if (cigar && ps.g.ckpt_k > 0) {
+    a->ckpt = reinterpret_cast<uint8_t*>(p);
+    a->ckpt_k = ps.g.ckpt_k;
+    a->ckpt_cap = ps.g.ckpt_cap;
+    a->ckpt_bytes = (int32_t)ps.g.ckpt_bytes;
+    a->ckpt_stride = (int64_t)ps.g.ckpt_cap * ps.g.ckpt_bytes;
+  }
 }
 
 // Core: inputs resident on the device (sv).  Writes score/status (device)
@@ -1423,6 +1448,12 @@ int tsu_set_ends_free(tsu_ctx* ctx, int32_t pattern_begin_free, int32_t pattern_
   ctx->ends_free[1] = pattern_end_free;
   ctx->ends_free[2] = text_begin_free;
   ctx->ends_free[3] = text_end_free;
+  return TSU_OK;
+}
+
+int tsu_set_low_memory(tsu_ctx* ctx, int32_t checkpoint_interval) {
+  if (!ctx) return TSU_EINVAL;
+  ctx->low_mem = checkpoint_interval;
   return TSU_OK;
 }
 

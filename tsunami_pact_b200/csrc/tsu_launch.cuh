@@ -19,12 +19,16 @@ namespace tsu {
 
 // The dual gap-affine kernels (tsu_dual.cu) and the gap-linear ones
 // (tsu_linear.cu).
-cudaError_t align_occupancy_dual(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ);
+// lowmem: the low-memory variant (CIGAR, global ring; cigar and mode are
+// then ignored).
+cudaError_t align_occupancy_dual(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ,
+                                 bool lowmem);
 void launch_align_dual(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
-                       const AlignArgs& a);
-cudaError_t align_occupancy_linear(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ);
+                       const AlignArgs& a, bool lowmem);
+cudaError_t align_occupancy_linear(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ,
+                                   bool lowmem);
 void launch_align_linear(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
-                         const AlignArgs& a);
+                         const AlignArgs& a, bool lowmem);
 
 namespace launch_detail {
 
@@ -58,7 +62,8 @@ cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
 }
 
 template <int kModel>
-cudaError_t occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ) {
+cudaError_t occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ, bool lowmem) {
+  if (lowmem) return occ_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, threads, smem, optin, occ);
   if (cigar)
     return mode == kModeShared ? occ_gw<true, kModeShared, kModel>(gw, threads, smem, optin, occ)
                                : occ_gw<true, kModeGlobal, kModel>(gw, threads, smem, optin, occ);
@@ -80,9 +85,11 @@ void launch_gw(int gw, int blocks, int threads, size_t smem, cudaStream_t st, co
 }
 
 template <int kModel>
-void launch(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
-            const AlignArgs& a) {
-  if (cigar) {
+void launch(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st, const AlignArgs& a,
+            bool lowmem) {
+  if (lowmem) {
+    launch_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, blocks, threads, smem, st, a);
+  } else if (cigar) {
     if (mode == kModeShared)
       launch_gw<true, kModeShared, kModel>(gw, blocks, threads, smem, st, a);
     else

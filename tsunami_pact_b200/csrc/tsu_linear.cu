@@ -6,13 +6,14 @@
 
 namespace tsu {
 
-cudaError_t align_occupancy_linear(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ) {
-  return launch_detail::occupancy<kModelLinear>(cigar, mode, gw, threads, smem, optin, occ);
+cudaError_t align_occupancy_linear(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ,
+                                   bool lowmem) {
+  return launch_detail::occupancy<kModelLinear>(cigar, mode, gw, threads, smem, optin, occ, lowmem);
 }
 
 void launch_align_linear(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
-                         const AlignArgs& a) {
-  launch_detail::launch<kModelLinear>(cigar, mode, gw, blocks, threads, smem, st, a);
+                         const AlignArgs& a, bool lowmem) {
+  launch_detail::launch<kModelLinear>(cigar, mode, gw, blocks, threads, smem, st, a, lowmem);
 }
 
 }  // namespace tsu

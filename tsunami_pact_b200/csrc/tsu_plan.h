@@ -7,6 +7,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 
 #include "tsu_common.cuh"
@@ -32,6 +33,9 @@ struct PassGeom {
   int table_cap = 0;       // step-table entries per group
   int group_smem = 0;      // dynamic shared memory per group (bytes)
   int64_t ring_ints = 0;   // global ring int32 per group (global mode)
+  int ckpt_k = 0;          // low-memory mode: checkpoint interval (0: off)
+  int ckpt_cap = 0;        // checkpoints per group
+  int64_t ckpt_bytes = 0;  // bytes per checkpoint
 };
 
 constexpr int kSharedW1 = 384;         // shared-mode ring width for one warp per pair (diagonals)
@@ -65,9 +69,12 @@ inline int shared_ring_width(const Pen& pen, int gw, int seq_cap, int smem_optin
 
 // mode/gw: the configuration of this pass.  Shared mode needs lengths within
 // the int16 ring; otherwise the pass falls back to the global ring.
+// low_mem (CIGAR passes): 0 off; > 0 checkpoint every low_mem scores; < 0
+// an interval chosen here.  Low-memory passes use the global ring.
 inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int mode, int gw, double hint,
-                              bool want_cigar, int smem_optin) {
+                              bool want_cigar, int smem_optin, int low_mem = 0) {
   PassGeom p;
+  const bool lowmem = want_cigar && low_mem != 0;
   const int ns = pen.slots();
   const int ge = pen.min_ge();
   const int64_t maxlen = std::max(max_m, max_n);
@@ -77,7 +84,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   p.gw = gw;
   p.cta_threads = cta_threads_for(gw);
   p.groups_per_cta = p.cta_threads / (32 * gw);
-  p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen) ? kModeShared : kModeGlobal;
+  p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen && !lowmem) ? kModeShared : kModeGlobal;
   if (p.mode == kModeShared) {
     const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
     p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
@@ -98,6 +105,22 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
     p.hist_cap = std::min<int64_t>(std::min<int64_t>(sq, (s_hint + 1) * width_hint), INT32_MAX - 64);
   }
   p.ring_ints = p.mode == kModeShared ? 0 : (int64_t)ns * p.ring_w;
+  if (lowmem) {
+    // The checkpoints of a pair (s_hint / K + 2 of ckpt_bytes) plus one
+    // segment of history (K + 1 rows of at most width_hint words): K near
+    // sqrt(s_hint * ckpt_bytes / (4 width_hint)) balances the two.  K is at
+    // least the ring depth, so a backtrace step crosses one segment at most.
+    p.ckpt_bytes = ckpt_bytes_for(pen, p.ring_w, kModeGlobal);
+    int64_t K = low_mem;
+    if (K < 0) {
+      const double k = std::sqrt((double)s_hint * (double)p.ckpt_bytes / (4.0 * (double)std::max<int64_t>(width_hint, 1)));
+      K = (int64_t)k;
+    }
+    K = std::max<int64_t>(std::min<int64_t>(K, std::max<int64_t>(s_hint, 1)), pen.rm);
+    p.ckpt_k = (int)K;
+    p.ckpt_cap = (int)std::min<int64_t>(s_hint / K + 2, INT32_MAX / 2);
+    p.hist_cap = std::min<int64_t>(p.hist_cap, (K + 1) * width_hint + 64);
+  }
   return p;
 }
 
