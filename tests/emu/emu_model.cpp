@@ -7,35 +7,26 @@
 #include "../../tsunami_pact_b200/csrc/tsu_kernels.cuh"
 // clang-format on
 
-template <bool kCigar, int kMode>
+template <bool kCigar, int kMode, int kM = EMU_MODEL>
 static void run_gw(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
   switch (gw) {
-    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, EMU_MODEL>(a); }); break;
-    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, EMU_MODEL>(a); }); break;
-    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, EMU_MODEL>(a); }); break;
-    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, EMU_MODEL>(a); }); break;
-    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, EMU_MODEL>(a); }); break;
-    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, EMU_MODEL>(a); }); break;
-    default: std::abort();
-  }
-}
-
-static void run_gw_lowmem(int gw, int threads, size_t smem, const tsu::AlignArgs& a) {
-  constexpr int kM = EMU_MODEL | tsu::kLowMemFlag;
-  switch (gw) {
-    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 1, kM>(a); }); break;
-    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 2, kM>(a); }); break;
-    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 4, kM>(a); }); break;
-    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 8, kM>(a); }); break;
-    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 16, kM>(a); }); break;
-    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<true, tsu::kModeGlobal, 32, kM>(a); }); break;
+    case 1: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 1, kM>(a); }); break;
+    case 2: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 2, kM>(a); }); break;
+    case 4: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 4, kM>(a); }); break;
+    case 8: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 8, kM>(a); }); break;
+    case 16: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 16, kM>(a); }); break;
+    case 32: emu::launch(1, threads, smem, [&] { tsu::align_kernel<kCigar, kMode, 32, kM>(a); }); break;
     default: std::abort();
   }
 }
 
 void EMU_RUN_FN(bool cigar, int mode, int gw, int threads, size_t smem, const tsu::AlignArgs& a, bool lowmem) {
+  constexpr int kM = EMU_MODEL | tsu::kLowMemFlag;
   if (lowmem) {
-    run_gw_lowmem(gw, threads, smem, a);
+    if (mode == tsu::kModeShared)
+      run_gw<true, tsu::kModeShared, kM>(gw, threads, smem, a);
+    else
+      run_gw<true, tsu::kModeGlobal, kM>(gw, threads, smem, a);
   } else if (cigar) {
     if (mode == tsu::kModeShared)
       run_gw<true, tsu::kModeShared>(gw, threads, smem, a);

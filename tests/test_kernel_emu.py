@@ -373,10 +373,10 @@ def test_low_memory_same_cigars(emu, oracle, K):
     pairs = [_edited(rng, rng.randint(0, 250), 0.15) for _ in range(10)]
     pairs += [("", ""), ("", "ACGT"), ("ACG", ""), ("ACGTNNACGT", "ACGTACGT"), ("A" * 64, "A" * 64)]
     bp = [(_b(p), _b(t)) for p, t in pairs]
-    got, passes, retried, gws = run_emu(emu, bp, lowmem=K)
-    assert gws.startswith("g"), gws  # low-memory passes use the global ring
-    for (p, t), (s, ops) in zip(bp, got):
-        assert (s, ops) == oracle.align(p, t), (p, t, K)
+    for shared in (True, False):
+        got, passes, retried, gws = run_emu(emu, bp, lowmem=K, shared_first=shared)
+        for (p, t), (s, ops) in zip(bp, got):
+            assert (s, ops) == oracle.align(p, t), (p, t, K, shared)
 
 
 def test_low_memory_models_groups_free_ends(emu, oracle):

@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
   constexpr bool kDual = (kModel & 7) == kModelDual;
   constexpr bool kLin = (kModel & 7) == kModelLinear;
   constexpr bool kLowMem = kCigar && (kModel & kLowMemFlag) != 0;
-  static_assert(!(kModel & kLowMemFlag) || (kCigar && kMode == kModeGlobal), "low-memory: CIGAR, global ring");
+  static_assert(!(kModel & kLowMemFlag) || kCigar, "low-memory: CIGAR kernels");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
 #ifdef TSU_WARP_EMU

@@ -29,7 +29,7 @@ enum : uint32_t { kOpM = 0, kOpI = 1, kOpD = 2, kOpX = 8 };
 enum : int { kModeShared = 0, kModeGlobal = 1 };
 enum : int { kModelAffine = 0, kModelDual = 1, kModelLinear = 2 };
 // added to a model: the low-memory (checkpointed history) variant of its
-// CIGAR kernel with the global ring
+// CIGAR kernels
 enum : int { kLowMemFlag = 8 };
 
 struct SeqView {

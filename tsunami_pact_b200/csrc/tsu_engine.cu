@@ -278,7 +278,7 @@ struct BatchInfo {
 // The align_kernel instantiations (tsu_launch.cuh): gap-affine kernels here,
 // dual gap-affine ones in tsu_dual.cu, gap-linear ones in tsu_linear.cu.
 // lowmem: the checkpointed-history variant (CIGAR passes of a low-memory
-// context; global ring).
+// context).
 cudaError_t align_occupancy(const tsu_ctx* ctx, bool cigar, int mode, int gw, int threads, size_t smem, int optin,
                             int* occ, bool lowmem) {
   switch (ctx->rp.model()) {

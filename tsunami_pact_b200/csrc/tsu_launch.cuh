@@ -19,8 +19,8 @@ namespace tsu {
 
 // The dual gap-affine kernels (tsu_dual.cu) and the gap-linear ones
 // (tsu_linear.cu).
-// lowmem: the low-memory variant (CIGAR, global ring; cigar and mode are
-// then ignored).
+// lowmem: the low-memory variant of the CIGAR kernel (cigar is then
+// ignored).
 cudaError_t align_occupancy_dual(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ,
                                  bool lowmem);
 void launch_align_dual(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st,
@@ -63,7 +63,9 @@ cudaError_t occ_gw(int gw, int threads, size_t smem, int optin, int* occ) {
 
 template <int kModel>
 cudaError_t occupancy(bool cigar, int mode, int gw, int threads, size_t smem, int optin, int* occ, bool lowmem) {
-  if (lowmem) return occ_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, threads, smem, optin, occ);
+  if (lowmem)
+    return mode == kModeShared ? occ_gw<true, kModeShared, kModel | kLowMemFlag>(gw, threads, smem, optin, occ)
+                               : occ_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, threads, smem, optin, occ);
   if (cigar)
     return mode == kModeShared ? occ_gw<true, kModeShared, kModel>(gw, threads, smem, optin, occ)
                                : occ_gw<true, kModeGlobal, kModel>(gw, threads, smem, optin, occ);
@@ -88,7 +90,10 @@ template <int kModel>
 void launch(bool cigar, int mode, int gw, int blocks, int threads, size_t smem, cudaStream_t st, const AlignArgs& a,
             bool lowmem) {
   if (lowmem) {
-    launch_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, blocks, threads, smem, st, a);
+    if (mode == kModeShared)
+      launch_gw<true, kModeShared, kModel | kLowMemFlag>(gw, blocks, threads, smem, st, a);
+    else
+      launch_gw<true, kModeGlobal, kModel | kLowMemFlag>(gw, blocks, threads, smem, st, a);
   } else if (cigar) {
     if (mode == kModeShared)
       launch_gw<true, kModeShared, kModel>(gw, blocks, threads, smem, st, a);

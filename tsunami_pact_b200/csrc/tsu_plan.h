@@ -70,7 +70,7 @@ inline int shared_ring_width(const Pen& pen, int gw, int seq_cap, int smem_optin
 // mode/gw: the configuration of this pass.  Shared mode needs lengths within
 // the int16 ring; otherwise the pass falls back to the global ring.
 // low_mem (CIGAR passes): 0 off; > 0 checkpoint every low_mem scores; < 0
-// an interval chosen here.  Low-memory passes use the global ring.
+// an interval chosen here.
 inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int mode, int gw, double hint,
                               bool want_cigar, int smem_optin, int low_mem = 0) {
   PassGeom p;
@@ -84,7 +84,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   p.gw = gw;
   p.cta_threads = cta_threads_for(gw);
   p.groups_per_cta = p.cta_threads / (32 * gw);
-  p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen && !lowmem) ? kModeShared : kModeGlobal;
+  p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen) ? kModeShared : kModeGlobal;
   if (p.mode == kModeShared) {
     const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
     p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
@@ -110,7 +110,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
     // segment of history (K + 1 rows of at most width_hint words): K near
     // sqrt(s_hint * ckpt_bytes / (4 width_hint)) balances the two.  K is at
     // least the ring depth, so a backtrace step crosses one segment at most.
-    p.ckpt_bytes = ckpt_bytes_for(pen, p.ring_w, kModeGlobal);
+    p.ckpt_bytes = ckpt_bytes_for(pen, p.ring_w, p.mode);
     int64_t K = low_mem;
     if (K < 0) {
       const double k = std::sqrt((double)s_hint * (double)p.ckpt_bytes / (4.0 * (double)std::max<int64_t>(width_hint, 1)));
