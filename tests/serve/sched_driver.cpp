@@ -67,15 +67,17 @@ struct FakeOpts {
   int32_t heavy_len = 1 << 30;  // runs with a pair this long count as heavy
 };
 FakeOpts g_opts;
+std::atomic<int> g_lowmem_runs{0};
 
 class Fake final : public Executor {
  public:
-  int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t, double,
+  int predict(int64_t n, const int32_t* plen, const int32_t* tlen, int64_t pb, int64_t tb, uint32_t flags, double,
               size_t* full, size_t* min) override {
     (void)n;
     (void)plen;
     (void)tlen;
     *full = g_opts.fixed + (size_t)(g_opts.bytes_per_base * (double)(pb + tb));
+    if (flags & kLowMem) *full /= 8;  // checkpointed history: an eighth
     *min = (size_t)((double)*full * g_opts.min_frac);
     return TSU_OK;
   }
@@ -119,6 +121,7 @@ class Fake final : public Executor {
       }
     }
     ++g_runs;
+    if (flags & kLowMem) ++g_lowmem_runs;
     {
       std::lock_guard<std::mutex> lk(g_log_mu);
       for (int64_t i = 0; i < n; ++i)
@@ -410,6 +413,25 @@ void degraded() {
   uint64_t id = 0;
   CHECK(s->submit(r.bp(), 0, &id) == TSU_OK);
   CHECK(check_result(*s, id, r, true) == TSU_OK);
+  CHECK(g_held_peak.load() <= (int64_t)c.budget);
+}
+
+void lowmem() {
+  // a CIGAR request whose smallest footprint exceeds the budget runs in
+  // low-memory mode (its footprint an eighth) instead of failing; the same
+  // request score-only has no such mode and is rejected
+  std::mt19937 rng(19);
+  Config c;
+  c.workers = 2;
+  Req r = make_req(rng, 0, 4, 'B', 100);
+  const size_t full = g_opts.fixed + (size_t)(g_opts.bytes_per_base * (double)(r.ps.size() + r.ts.size()));
+  c.budget = (size_t)((double)full * g_opts.min_frac / 2);
+  auto s = make_server(c);
+  uint64_t id = 0;
+  CHECK(s->submit(r.bp(), TSU_SCORE_ONLY, &id) == TSU_ENOMEM);
+  CHECK(s->submit(r.bp(), 0, &id) == TSU_OK);
+  CHECK(check_result(*s, id, r, true) == TSU_OK);
+  CHECK(g_lowmem_runs.load() >= 1);
   CHECK(g_held_peak.load() <= (int64_t)c.budget);
 }
 
@@ -770,7 +792,8 @@ int main(int argc, char** argv) {
                {"fifo", fifo},             {"cancel", cancel},         {"pending", pending},
                {"watchdog", watchdog},     {"nomem_retry", nomem_retry}, {"failure_isolation", failure_isolation},
                {"queue_full", queue_full}, {"stress", stress},         {"shutdown", shutdown_busy},
-               {"heavy_split", heavy_split}, {"heavy_fail", heavy_fail}, {"estimate", estimate}};
+               {"heavy_split", heavy_split}, {"heavy_fail", heavy_fail}, {"estimate", estimate},
+               {"lowmem", lowmem}};
   for (auto& e : table)
     if (sc == e.name) {
       e.fn();

@@ -99,3 +99,31 @@ def test_low_memory_every_starting_rung(oracle):
             scores, ops = al.align(pats, txts)
             assert list(scores) == list(osc), (mode, gw)
             assert ops == oops, (mode, gw)
+
+
+def test_server_runs_oversized_cigar_in_low_memory(oracle):
+    """A request whose smallest CIGAR footprint exceeds the server's budget
+    runs in low-memory mode instead of failing; its score-only form has no
+    such mode and is rejected."""
+    import tsunami_pact_b200 as T
+
+    pats, txts = _pairs(97, 1, 30000, 30000, 0.2)
+    plen = np.array([len(pats[0])], np.int32)
+    tlen = np.array([len(txts[0])], np.int32)
+    with T.Aligner(4, 6, 2) as al:
+        _, min_hi = al.predict_bytes(plen, tlen)
+        al.set_low_memory(-1)
+        _, min_lo = al.predict_bytes(plen, tlen)
+        _, min_score = al.predict_bytes(plen, tlen, cigar=False)
+    assert min_lo < min_hi
+    budget = (min_lo + min_hi) // 2
+    # the server sizes the pair by the same hint as the predictions above
+    with T.Server(4, 6, 2, workers=2, mem_budget=budget, estimate_hint=False) as srv:
+        rid = srv.submit(pats, txts)
+        s, co, runs, _info = srv.wait(rid, 300000)
+        ops = T.runs_to_ops(runs[co[0]:co[1]])
+        if min_score > budget:
+            with pytest.raises(T.AlignError):
+                srv.submit(pats, txts, cigar=False)
+    osc, oops = oracle.align_batch(pats, txts, 4, 6, 2)
+    assert int(s[0]) == int(osc[0]) and ops == oops[0]

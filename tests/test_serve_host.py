@@ -20,7 +20,7 @@ EXE = os.path.join(ROOT, "tests", "serve", "_build", "sched_driver")
 
 SCENARIOS = ["basic", "score_only", "admission", "concurrency", "reject", "degraded", "fifo", "cancel", "pending",
              "watchdog", "nomem_retry", "failure_isolation", "queue_full", "stress", "shutdown", "heavy_split",
-             "heavy_fail", "estimate"]
+             "heavy_fail", "estimate", "lowmem"]
 
 
 @pytest.fixture(scope="module")

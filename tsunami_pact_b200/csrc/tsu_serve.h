@@ -26,7 +26,8 @@
 //     resident_cap and until the memory is needed elsewhere.  A job of
 //     several parts that does not fit is halved down to one part; a part
 //     that fits only with fewer pairs in flight runs when nothing else does;
-//     a part that cannot fit even then fails with TSU_ENOMEM.  Each queue
+//     a CIGAR part that cannot fit even then runs in low-memory mode
+//     (checkpointed history) if that fits, else fails with TSU_ENOMEM.  Each queue
 //     starts its parts in order (no overtaking within a queue);
 //   * a request is done when all its parts are: its results are assembled
 //     in its own pair order and made visible to poll/wait; latency is
@@ -65,6 +66,10 @@ namespace serve {
 // Executor flag beside TSU_SCORE_ONLY: the hint is a per-pair estimate, so
 // choose the first rung by the width it predicts (tsu::fit_start).
 constexpr uint32_t kFitStart = 0x100;
+// Executor flag: align with checkpointed history (low-memory mode).  Set by
+// admission on a CIGAR part whose smallest footprint exceeds the budget, when
+// the low-memory footprint fits: such a request runs instead of failing.
+constexpr uint32_t kLowMem = 0x200;
 
 using Clock = std::chrono::steady_clock;
 
@@ -290,6 +295,14 @@ class Server {
       }
       const int rc = predict_parts({p}, p->flags, p->hint, &p->full, &p->min);
       if (rc) return rc;
+      if (p->min > cfg_.budget && !(p->flags & TSU_SCORE_ONLY)) {
+        size_t full2 = 0, min2 = 0;
+        if (predict_parts({p}, p->flags | kLowMem, p->hint, &full2, &min2) == TSU_OK && min2 <= cfg_.budget) {
+          p->flags |= kLowMem;
+          p->full = full2;
+          p->min = min2;
+        }
+      }
     }
     std::lock_guard<std::mutex> lk(mu_);
     if (stopping_) return TSU_EBUSY;

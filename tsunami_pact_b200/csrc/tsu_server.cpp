@@ -82,6 +82,7 @@ class EngineExecutor final : public tsu::serve::Executor {
     sh.pattern_bytes = pb;
     sh.text_bytes = tb;
     tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
+    tsu_set_low_memory(ctx_, (flags & tsu::serve::kLowMem) ? -1 : 0);
     return tsu::engine::predict_bytes(ctx_, sh, flags & TSU_SCORE_ONLY, hint, full, min);
   }
   size_t held() override { return tsu::engine::held_bytes(ctx_); }
@@ -93,6 +94,7 @@ class EngineExecutor final : public tsu::serve::Executor {
   int run(const Pairs& in, uint32_t flags, double hint, Output* out) override {
     tsu::engine::set_hint(ctx_, hint > 0 ? hint : default_hint_);
     tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
+    tsu_set_low_memory(ctx_, (flags & tsu::serve::kLowMem) ? -1 : 0);
     const size_t n = (size_t)in.n();
     const bool cig = !(flags & TSU_SCORE_ONLY);
     int64_t cap = 1;  // a pair has at most m + n runs
