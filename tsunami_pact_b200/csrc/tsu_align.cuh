@@ -67,7 +67,7 @@ constexpr int cta_threads() {
 }
 template <int kMode, int GW>
 constexpr int cta_min_blocks() {
-  return kMode == kModeShared ? (GW <= 4 ? 6 : (GW == 8 ? 3 : 1)) : (GW <= 4 ? 4 : (GW == 8 ? 2 : 1));
+  return kMode == kModeShared ? (GW == 1 ? 7 : (GW <= 4 ? 6 : (GW == 8 ? 3 : 1))) : (GW <= 4 ? 4 : (GW == 8 ? 2 : 1));
 }
 
 template <bool kCigar, int kMode, int GW, int kModel = kModelAffine>

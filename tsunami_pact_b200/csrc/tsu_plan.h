@@ -51,7 +51,7 @@ inline int64_t hint_score(const Pen& pen, int64_t L, double hint) {
 
 inline int cta_threads_for(int gw) { return gw <= 4 ? 128 : 32 * gw; }
 inline int min_blocks_for(int mode, int gw) {
-  return mode == kModeShared ? (gw <= 4 ? 6 : (gw == 8 ? 3 : 1)) : (gw <= 4 ? 4 : (gw == 8 ? 2 : 1));
+  return mode == kModeShared ? (gw == 1 ? 7 : (gw <= 4 ? 6 : (gw == 8 ? 3 : 1))) : (gw <= 4 ? 4 : (gw == 8 ? 2 : 1));
 }
 
 // Ring width a shared-mode group of gw warps can hold with seq_cap staged
