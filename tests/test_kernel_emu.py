@@ -6,6 +6,7 @@ shared- or global-memory access outside its buffer aborts the run, and every
 score and operation string must equal the oracle's."""
 import os
 import random
+import shutil
 import subprocess
 
 import pytest
@@ -28,14 +29,21 @@ def emu():
         # the driver and one object per penalty model, compiled in parallel
         flags = ["-std=c++20", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
                  "-fno-sanitize-recover=undefined"]
-        build = os.path.dirname(EXE)
+        # objects and the executable are built under a per-process name and
+        # renamed into place, so parallel pytest workers never run a
+        # half-written binary
+        build = os.path.join(os.path.dirname(EXE), f"tmp{os.getpid()}")
+        os.makedirs(build, exist_ok=True)
         jobs = [(os.path.join(build, "driver.o"), [os.path.join(EMU_DIR, "emu_driver.cpp")])]
         for model, fn in ((0, "run_pass_affine"), (1, "run_pass_dual"), (2, "run_pass_linear")):
             jobs.append((os.path.join(build, f"model{model}.o"),
                          [f"-DEMU_MODEL={model}", f"-DEMU_RUN_FN={fn}", os.path.join(EMU_DIR, "emu_model.cpp")]))
         procs = [subprocess.Popen(["g++", *flags, "-c", "-o", obj, *args]) for obj, args in jobs]
         assert all(p.wait() == 0 for p in procs), "emulator build failed"
-        subprocess.run(["g++", *flags, "-o", EXE, *(obj for obj, _ in jobs), "-lpthread"], check=True)
+        tmp_exe = os.path.join(build, "emu_driver")
+        subprocess.run(["g++", *flags, "-o", tmp_exe, *(obj for obj, _ in jobs), "-lpthread"], check=True)
+        os.replace(tmp_exe, EXE)
+        shutil.rmtree(build, ignore_errors=True)
     return EXE
 
 

@@ -28,8 +28,12 @@ def driver():
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     newest = max(os.path.getmtime(s) for s in [SRC] + HDRS)
     if not os.path.exists(EXE) or os.path.getmtime(EXE) < newest:
-        subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-fsanitize=thread", "-o", EXE, SRC, "-lpthread"],
+        # built under a per-process name and renamed into place, so parallel
+        # pytest workers never run a half-written binary
+        tmp_exe = f"{EXE}.tmp{os.getpid()}"
+        subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-fsanitize=thread", "-o", tmp_exe, SRC, "-lpthread"],
                        check=True)
+        os.replace(tmp_exe, EXE)
     return EXE
 
 
