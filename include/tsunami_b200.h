@@ -303,6 +303,20 @@ int tsu_gen_batch(uint64_t seed, int64_t first, int64_t count, const int32_t* le
  * 68-69): header num / seq_len / error_rate, then pattern and text lines. */
 int tsu_file_write(const char* path, int64_t num, int32_t seq_len, int32_t error_rate, const tsu_batch* batch);
 
+/* Multi-GPU plan for one batch (host only, no device call).  The reference
+ * aligns a file on one GPU in one launch (wfa_gpu.cu:113-123); pairs are
+ * independent, so a batch splits into num_shards shards that separate GPUs
+ * align with no communication, the results being put back in pair order on
+ * the host.  Each pair's work is predicted from its lengths and edit rate
+ * (max_error_hint > 0: that rate for every pair; 0: estimated per pair from
+ * shared k-mers, which needs the sequence bytes) as the square of its
+ * predicted score in extension steps plus its length; pairs are placed
+ * largest first on the least-loaded shard.  Writes shard_of_pair[num_pairs]
+ * and, when not NULL, shard_work[num_shards] (predicted work per shard).
+ * Deterministic: every rank computes the same plan from the same batch. */
+int tsu_shard_plan(const tsu_penalties* pen, const tsu_batch* batch, int32_t num_shards, double max_error_hint,
+                   int32_t* shard_of_pair, double* shard_work);
+
 /* ---- request server -------------------------------------------------------
  * No counterpart in the reference (one file per process, wfa_gpu.cu:43-188).
  * Continuous batching on one device: tsu_submit copies a request (a batch of

@@ -134,6 +134,7 @@ def lib():
     L.tsu_gen_batch.argtypes = [ctypes.c_uint64, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                                 ctypes.c_int]
     L.tsu_predict_bytes.argtypes = [c_vp, P(Batch), c_u32, P(ctypes.c_size_t), P(ctypes.c_size_t)]
+    L.tsu_shard_plan.argtypes = [P(Penalties), P(Batch), c_i32, ctypes.c_double, c_vp, c_vp]
     L.tsu_server_create.argtypes = [P(Penalties), P(ServerConfig), P(c_vp)]
     L.tsu_server_create_dual.argtypes = [P(Penalties2), P(ServerConfig), P(c_vp)]
     L.tsu_server_destroy.argtypes = [c_vp]

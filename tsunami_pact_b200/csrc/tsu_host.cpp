@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/tsunami_b200.h"
+#include "tsu_estimate.h"
 
 namespace {
 
@@ -513,6 +514,80 @@ int tsu_file_write(const char* path, int64_t num, int32_t seq_len, int32_t error
   int bad = ferror(fp);
   fclose(fp);
   return bad ? TSU_EIO : TSU_OK;
+}
+
+// Predicted work of every pair, then longest-processing-time-first
+// placement: pairs in decreasing work (ties by index) each go to the shard
+// with the least work so far (ties to the lowest shard).  The result depends
+// only on the inputs, so every rank that calls this gets the same plan.
+int tsu_shard_plan(const tsu_penalties* pen, const tsu_batch* b, int32_t num_shards, double max_error_hint,
+                   int32_t* shard_of_pair, double* shard_work) {
+  if (!pen || !b || num_shards < 1 || b->num_pairs < 0 || !(max_error_hint >= 0.0) || max_error_hint > 2.0)
+    return TSU_EINVAL;
+  if (pen->mismatch <= 0 || pen->gap_opening < 0 || pen->gap_extension <= 0) return TSU_EINVAL;
+  const int64_t n = b->num_pairs;
+  if (n && (!shard_of_pair || !b->pattern_len || !b->text_len)) return TSU_EINVAL;
+  const bool estimate = max_error_hint == 0.0;
+  if (n && estimate && (!b->pattern || !b->pattern_off || !b->text || !b->text_off)) return TSU_EINVAL;
+  for (int64_t i = 0; i < n; ++i)
+    if (b->pattern_len[i] < 0 || b->text_len[i] < 0) return TSU_EINVAL;
+
+  const double x = pen->mismatch, o = pen->gap_opening, e = pen->gap_extension;
+  const double dear = std::max(x, o + e);  // dearest one-base edit
+  std::vector<double> work((size_t)n);
+  auto predict = [&](int64_t i) {
+    const double m = b->pattern_len[i], t = b->text_len[i];
+    // upper bound of the optimal score: mismatches plus one gap for the
+    // length difference, or delete everything and insert everything
+    const double ub = std::min(x * std::min(m, t) + (m != t ? o + e * std::fabs(m - t) : 0.0),
+                               (m > 0 ? o + e * m : 0.0) + (t > 0 ? o + e * t : 0.0));
+    double rate = max_error_hint;
+    if (estimate) {
+      rate = tsu::estimate_edit_rate(b->pattern + b->pattern_off[i], b->pattern_len[i], b->text + b->text_off[i],
+                                     b->text_len[i]);
+      if (rate < 0.0) rate = 0.1;  // too short to estimate: small either way
+    }
+    const double s = std::min(ub, rate * std::max(m, t) * dear);
+    // wavefront cells grow with the square of the score (the envelope widens
+    // by one diagonal per extension step); the packed sequences are read once
+    const double steps = s / e + 1.0;
+    work[(size_t)i] = steps * steps + (m + t) / 16.0;
+  };
+  int threads = estimate ? (int)std::max(1u, std::thread::hardware_concurrency()) : 1;
+  threads = (int)std::min<int64_t>(threads, std::max<int64_t>(n / 256, 1));
+  {
+    std::vector<std::thread> th;
+    auto run = [&](int tid) {
+      for (int64_t i = tid; i < n; i += threads) predict(i);
+    };
+    for (int t = 1; t < threads; ++t) th.emplace_back(run, t);
+    run(0);
+    for (auto& t : th) t.join();
+  }
+
+  std::vector<int64_t> order((size_t)n);
+  for (int64_t i = 0; i < n; ++i) order[(size_t)i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int64_t a, int64_t c) { return work[(size_t)a] > work[(size_t)c]; });
+  // min-heap of (load, shard)
+  std::vector<std::pair<double, int32_t>> heap;
+  for (int32_t s = 0; s < num_shards; ++s) heap.emplace_back(0.0, s);
+  auto later = [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& c) {
+    return a.first != c.first ? a.first > c.first : a.second > c.second;
+  };
+  std::make_heap(heap.begin(), heap.end(), later);
+  std::vector<double> load((size_t)num_shards, 0.0);
+  for (int64_t i : order) {
+    std::pop_heap(heap.begin(), heap.end(), later);
+    auto& top = heap.back();
+    shard_of_pair[i] = top.second;
+    top.first += work[(size_t)i];
+    load[(size_t)top.second] = top.first;
+    std::push_heap(heap.begin(), heap.end(), later);
+  }
+  if (shard_work)
+    for (int32_t s = 0; s < num_shards; ++s) shard_work[s] = load[(size_t)s];
+  return TSU_OK;
 }
 
 }  // extern "C"
