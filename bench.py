@@ -367,6 +367,7 @@ def main():
     ap.add_argument("--hint", type=float, default=0.0, help="max_error_hint of the engine context")
     ap.add_argument("--plain", action="store_true", help="also time the plain one-warp-per-pair bucketed form")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain form (c4)")
+    ap.add_argument("--plain-steps", type=int, default=1, help="timed repetitions of the plain form")
     ap.add_argument("--rates", default="5,10,20,0", help="c5: offered request rates (requests/s; 0: all at once)")
     ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
     ap.add_argument("--workers", type=int, default=32, help="c5: server workers")
@@ -493,7 +494,10 @@ def main():
             idx = np.nonzero(buckets == b)[0]
             sub.append((int(b), len(idx), [torch.from_numpy(x[idx]).to(dev) for x in (poff, plen, toff, tlen)]))
         p_ms, p_launch = [], 0
-        for rep in range(max(args.steps, 1) + 1):  # the first repetition warms up
+        # the first repetition warms up; each timed one is a whole uneven
+        # batch in one-warp launches (about a minute on c4), so the plain
+        # form has its own repetition count
+        for rep in range(max(args.plain_steps, 1) + 1):
             tot = 0.0
             for b, nb, (bo, bl, to_, tl_) in sub:
                 sc = torch.zeros(nb, dtype=torch.int32, device=dev)
@@ -520,7 +524,8 @@ def main():
         plain = {"form": "one call per floor(log2 L) bucket, one warp per pair (TSU_ONE_WARP), in turn",
                  "buckets": len(sub), "ms_per_step": pm, "value": throughput(cells_all, pm) / 1e9,
                  "unit": "GCUPS", "pairs_per_s": throughput(pairs_all, pm),
-                 "batched_over_plain_pairs_per_s": pm / ms, "gpu_launches": p_launch}
+                 "batched_over_plain_pairs_per_s": pm / ms, "gpu_launches": p_launch,
+                 "steps": max(args.plain_steps, 1), "warmup": 1}
 
     # ---- e2e: host buffers (pinned) through tsu_align_batch ---------------
     e2e = None
