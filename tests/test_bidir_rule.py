@@ -26,3 +26,68 @@ def test_first_breakpoint_is_the_optimal_score(oracle):
         best = oracle.gotoh(p, t, *pen)
         total, where = bidir_rule.first_breakpoint(p, t, *pen, best + 2)
         assert total == best, (p, t, pen, best, total, where)
+
+
+def _case(rng, it, maxlen=14, maxedits=5):
+    p = "".join(rng.choice("AC" if it % 2 else "ACGT") for _ in range(rng.randint(0, maxlen)))
+    t = list(p)
+    for _ in range(rng.randint(0, maxedits)):
+        pos = rng.randint(0, max(0, len(t) - 1))
+        r = rng.random()
+        if r < 0.33 and t:
+            t[pos] = rng.choice("ACGT")
+        elif r < 0.66:
+            t.insert(pos, rng.choice("ACGT"))
+        elif t:
+            del t[pos]
+    return p, "".join(t), rng.choice([(4, 6, 2), (2, 3, 1), (3, 5, 2), (1, 1, 1), (5, 2, 3)])
+
+
+def test_segments_with_gap_components():
+    """Segments that continue a gap from the left (begin I/D) or must end in
+    one (end I/D), as a recursion on breakpoints produces them: the first
+    overlap total equals the component-constrained Gotoh DP, for all nine
+    begin/end pairs."""
+    rng = random.Random(5)
+    checked = 0
+    for it in range(500):
+        p, t, pen = _case(rng, it)
+        if not p and not t:
+            continue
+        for a in "MID":
+            for b in "MID":
+                best = bidir_rule.gotoh_components(p, t, *pen, a, b)
+                if best >= bidir_rule.INF:
+                    continue
+                total, where = bidir_rule.first_breakpoint(p, t, *pen, best + pen[1] + pen[2] + 2, a, b)
+                assert total == best, (p, t, pen, a, b, best, total, where)
+                checked += 1
+    assert checked > 3000
+
+
+def test_split_halves_are_optimal():
+    """Cutting a segment at its breakpoint: the halves' optimal costs add up
+    to the segment's, and where the score is positive both halves are
+    usually cheaper (the cut sits near the middle in score)."""
+    rng = random.Random(9)
+    positive = cheaper = 0
+    for it in range(300):
+        p, t, pen = _case(rng, it)
+        if not p and not t:
+            continue
+        for a in "MID":
+            for b in "MID":
+                best = bidir_rule.gotoh_components(p, t, *pen, a, b)
+                if best >= bidir_rule.INF:
+                    continue
+                total, left, right = bidir_rule.split(p, t, *pen, a, b)
+                assert total == best
+                assert left[0] + right[0] == p and left[1] + right[1] == t
+                assert left[2] == a and right[3] == b and left[3] == right[2]
+                cl = bidir_rule.gotoh_components(left[0], left[1], *pen, left[2], left[3])
+                cr = bidir_rule.gotoh_components(right[0], right[1], *pen, right[2], right[3])
+                assert cl + cr == best, (p, t, pen, a, b, left, right, cl, cr)
+                if best > 0:
+                    positive += 1
+                    cheaper += max(cl, cr) < best
+    assert cheaper > positive // 2
