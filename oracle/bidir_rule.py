@@ -24,6 +24,16 @@ I/D: the reverse pass is forced to begin with it).  gotoh_components is
 the O(mn) DP of exactly those costs, which pins the rule for all nine
 begin/end pairs, and split() cuts a segment into two halves whose optimal
 costs add up to the segment's.
+
+bialign() is the whole bidirectional alignment: split until a segment's
+score is small, then wfa_segment(), the plain WFA of the segment with its
+components and the C oracle's backtrace (byte-identical to it for free
+ends).  A segment that must end in a gap is aligned on the reversed
+sequences, because greedy extension towards a constrained end can pass the
+cell the closing gap has to leave from.  Its CIGARs are optimal; where the
+optimum is tied they may differ from the one-direction backtrace, so a GPU
+bidirectional mode is checked against this recursion, not against the
+plain oracle.
 """
 from __future__ import annotations
 
@@ -167,3 +177,160 @@ def split(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "
     comp, _, _, k, h = where
     v = h - k
     return T, (p[:v], t[:h], begin, comp), (p[v:], t[h:], comp, end)
+
+
+# piggyback codes of the backtrace's tie order (oracle/wfa_oracle.c, after
+# the reference's bt_type_t, common.h:67-77): M > D_ext > D_open > I_ext > I_open
+_BT_M, _BT_DX, _BT_DO, _BT_IX, _BT_IO = 9, 6, 5, 2, 1
+
+
+def _wfa_forward(p: str, t: str, x: int, o: int, e: int, start: str, forced: str, free_end: str):
+    """(score, operations) by the plain WFA with greedy extension: wavefronts
+    from `start` / `forced` (as in wavefronts()), ended in M at (m, n), or
+    -- free_end "I"/"D" -- in that gap at a discount of o (a trailing run
+    that continues a gap opened after the segment), the lower cost winning
+    (M on ties); then the backtrace of oracle/wfa_oracle.c (wf_backtrace:
+    the highest piggyback value among the sources, M runs emitted from the
+    pre-extension offset, the border reached with v or h at 0 finished by
+    D and I runs)."""
+    m, n = len(p), len(t)
+    k_end = n - m
+    smax = (m + n) * max(x, o + e) + 2 * (o + e)
+    M, Mp, I, D = wavefronts(p, t, x, o, e, smax, start=start, forced=forced)
+    best = None  # (cost, score, component)
+    for s in range(smax + 1):
+        if best is not None and s - (o if free_end != "M" else 0) > best[0]:
+            break
+        if M.get(s, {}).get(k_end, NULL) >= n and (best is None or s < best[0]):
+            best = (s, s, "M")
+        if free_end in ("I", "D"):
+            g = (I if free_end == "I" else D).get(s, {})
+            if g.get(k_end, NULL) == n and (best is None or s - o < best[0]):
+                best = (s - o, s, free_end)
+    if best is None:
+        return None, None
+    cost, s_end, state = best
+    comp = {"M": M, "I": I, "D": D}[state]
+
+    def src(w, s, k, delta, code):
+        if s < 0 or k not in w.get(s, {}):
+            return NULL
+        return (w[s][k] + delta) * 16 + code
+
+    ops = []
+    s, k = s_end, k_end
+    off = comp[s_end][k_end]
+    v, h = off - k, off
+    while v > 0 and h > 0 and s > 0:
+        io = src(M, s - o - e, k - 1, 1, _BT_IO)
+        ix = src(I, s - e, k - 1, 1, _BT_IX)
+        dop = src(M, s - o - e, k + 1, 0, _BT_DO)
+        dx = src(D, s - e, k + 1, 0, _BT_DX)
+        # a forced first gap opens from the empty origin
+        if forced == "I" and s == o + e and k == 1:
+            io = max(io, 1 * 16 + _BT_IO)
+        if forced == "D" and s == o + e and k == -1:
+            dop = max(dop, 0 * 16 + _BT_DO)
+        if state == "M":
+            best_src = max(src(M, s - x, k, 1, _BT_M), io, ix, dop, dx)
+        elif state == "I":
+            best_src = max(io, ix)
+        else:
+            best_src = max(dop, dx)
+        if best_src < 0:
+            raise AssertionError("backtrace found no source")
+        if state == "M":
+            moff = best_src // 16
+            ops.extend("M" * (off - moff))
+            off = moff
+            v, h = off - k, off
+            if v <= 0 or h <= 0:
+                break
+        code = best_src % 16
+        if code == _BT_M:
+            s, state = s - x, "M"
+            ops.append("X")
+            off -= 1
+        elif code in (_BT_IO, _BT_IX):
+            s, state = (s - o - e, "M") if code == _BT_IO else (s - e, "I")
+            ops.append("I")
+            k -= 1
+            off -= 1
+        else:
+            s, state = (s - o - e, "M") if code == _BT_DO else (s - e, "D")
+            ops.append("D")
+            k += 1
+        v, h = off - k, off
+    if v > 0 and h > 0:
+        nm = min(v, h)
+        ops.extend("M" * nm)
+        v, h = v - nm, h - nm
+    ops.extend("D" * max(v, 0))
+    ops.extend("I" * max(h, 0))
+    return cost, "".join(reversed(ops))
+
+
+def wfa_segment(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
+    """(score, operations) of one segment with components by the plain WFA.
+    A segment free at its end runs forward from `begin`.  One that must end
+    in a gap runs on the reversed sequences instead, forced to begin with
+    that gap (greedy extension forward could run an M run past the cell the
+    closing gap has to leave from; a constraint at the start of the greedy
+    direction costs nothing), a gap it continues becoming a free trailing
+    run; its operations are then read backwards."""
+    if not p and not t:
+        return 0, ""
+    if end == "M":
+        return _wfa_forward(p, t, x, o, e, begin, "M", "M")
+    cost, ops = _wfa_forward(p[::-1], t[::-1], x, o, e, "M", end, begin)
+    return cost, None if ops is None else ops[::-1]
+
+
+def bialign(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M", base_score: int = 0) -> str:
+    """Operations of a bidirectional alignment: split at the breakpoint
+    until a segment's score is at most base_score (default two of the
+    dearest single edits) or a cut makes no progress, then the plain WFA of
+    the segment (wfa_segment), the pieces concatenated in order."""
+    if not p and not t:
+        return ""
+    base = base_score or 2 * max(x, o + e)
+    total, left, right = split(p, t, x, o, e, begin, end)
+    if total is None:
+        raise AssertionError("no breakpoint")
+    whole = len(p) + len(t)
+    if total <= base or len(left[0]) + len(left[1]) in (0, whole) or len(right[0]) + len(right[1]) in (0, whole):
+        return wfa_segment(p, t, x, o, e, begin, end)[1]
+    return (bialign(left[0], left[1], x, o, e, left[2], left[3], base)
+            + bialign(right[0], right[1], x, o, e, right[2], right[3], base))
+
+
+def ops_cost(ops: str, p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
+    """Cost of an operation string for a segment with components, or None
+    if it does not turn p into t or breaks the end component."""
+    i = j = 0
+    cost = 0
+    prev = begin  # a leading run of the begin gap continues it
+    for c in ops:
+        if c in "MX":
+            if i >= len(p) or j >= len(t) or (p[i] == t[j]) != (c == "M"):
+                return None
+            cost += 0 if c == "M" else x
+            i, j = i + 1, j + 1
+        elif c == "I":
+            if j >= len(t):
+                return None
+            cost += e if prev == "I" else o + e
+            j += 1
+        elif c == "D":
+            if i >= len(p):
+                return None
+            cost += e if prev == "D" else o + e
+            i += 1
+        else:
+            return None
+        prev = c if c in "ID" else "M"
+    if i != len(p) or j != len(t):
+        return None
+    if end in "ID" and (not ops or ops[-1] != end) and not (not ops and begin == end):
+        return None
+    return cost

@@ -91,3 +91,51 @@ def test_split_halves_are_optimal():
                     positive += 1
                     cheaper += max(cl, cr) < best
     assert cheaper > positive // 2
+
+
+def test_segment_wfa_with_components(oracle):
+    """The base case of the recursion: the plain WFA of a segment with
+    components reaches the component-constrained optimum with operations
+    that cost exactly that, and for free ends (M, M) it is the C oracle
+    byte for byte (same backtrace, same ties)."""
+    rng = random.Random(4)
+    for it in range(120):
+        p, t, pen = _case(rng, it)
+        if not p and not t:
+            continue
+        for a in "MID":
+            for b in "MID":
+                best = bidir_rule.gotoh_components(p, t, *pen, a, b)
+                if best >= bidir_rule.INF:
+                    continue
+                score, ops = bidir_rule.wfa_segment(p, t, *pen, a, b)
+                assert score == best and bidir_rule.ops_cost(ops, p, t, *pen, a, b) == best, (p, t, pen, a, b)
+        assert bidir_rule.wfa_segment(p, t, *pen) == oracle.align(p, t, *pen)
+
+
+def test_bidirectional_alignment_is_optimal(oracle):
+    """Recursion on breakpoints down to segment WFAs: every operation string
+    turns the pattern into the text at the Gotoh optimum (ties at a cut may
+    resolve differently from the plain backtrace)."""
+    rng = random.Random(12)
+    identical = 0
+    for it in range(40):
+        L = rng.randint(0, 80)
+        p = "".join(rng.choice("ACGT") for _ in range(L))
+        t = list(p)
+        for _ in range(int(L * rng.uniform(0, 0.2))):
+            pos = rng.randint(0, max(0, len(t) - 1))
+            r = rng.random()
+            if r < 0.33 and t:
+                t[pos] = rng.choice("ACGT")
+            elif r < 0.66:
+                t.insert(pos, rng.choice("ACGT"))
+            elif t:
+                del t[pos]
+        t = "".join(t)
+        pen = rng.choice([(4, 6, 2), (2, 3, 1), (3, 5, 2), (1, 1, 1), (5, 2, 3)])
+        ops = bidir_rule.bialign(p, t, *pen)
+        assert bidir_rule.ops_cost(ops, p, t, *pen) == oracle.gotoh(p, t, *pen), (p, t, pen, ops)
+        assert oracle.cigar_cost(ops, p, t, *pen) == oracle.gotoh(p, t, *pen)
+        identical += ops == oracle.align(p, t, *pen)[1]
+    assert identical >= 20
