@@ -116,7 +116,7 @@ def first_breakpoint(p: str, t: str, x: int, o: int, e: int, smax: int, begin: s
             sr = T - sf
             if sr > smax:
                 continue
-            for k, hf in FM[sf].items():
+            for k, hf in sorted(FM[sf].items()):  # diagonals in ascending order
                 kr = (n - m) - k
                 if kr in RM[sr]:
                     lo = max(FMp[sf][k], n - RM[sr][kr])
@@ -128,7 +128,7 @@ def first_breakpoint(p: str, t: str, x: int, o: int, e: int, smax: int, begin: s
             if sr > smax or sr < 0:
                 continue
             for comp, Fw, Rw in (("I", FI, RI), ("D", FD, RD)):
-                for k, hf in Fw[sf].items():
+                for k, hf in sorted(Fw[sf].items()):
                     kr = (n - m) - k
                     if kr in Rw[sr] and hf + Rw[sr][kr] == n:
                         return T, (comp, sf, sr, k, hf)

@@ -155,6 +155,15 @@ int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, cons
                            const int64_t* toff, const int32_t* tlen, int x, int o, int e, int32_t* scores,
                            int threads);
 
+/* Bidirectional (BiWFA-style) alignment, wfa_oracle_bidir.c: breakpoints
+ * of forward and reverse wavefronts, recursion down to segments whose score
+ * is at most base_score (<= 0: two of the dearest single edits), each
+ * aligned by the plain WFA with its gap components.  Writes the operation
+ * string to ops (no terminator), its length to *ops_len; returns 0 or a
+ * negative error.  ops_cap >= m + n suffices. */
+int ora_bialign(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
+                char* ops, int ops_cap, int* ops_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -139,3 +139,39 @@ def test_bidirectional_alignment_is_optimal(oracle):
         assert oracle.cigar_cost(ops, p, t, *pen) == oracle.gotoh(p, t, *pen)
         identical += ops == oracle.align(p, t, *pen)[1]
     assert identical >= 20
+
+
+def test_c_bialign_equals_the_model(oracle):
+    """ora_bialign (oracle/wfa_oracle_bidir.c) is the Python recursion byte
+    for byte, zero gap-open penalties included."""
+    rng = random.Random(21)
+    for it in range(60):
+        L = rng.randint(0, 70)
+        p = "".join(rng.choice("AC" if it % 4 == 0 else "ACGT") for _ in range(L))
+        t = list(p)
+        for _ in range(int(L * rng.uniform(0, 0.25))):
+            pos = rng.randint(0, max(0, len(t) - 1))
+            r = rng.random()
+            if r < 0.33 and t:
+                t[pos] = rng.choice("ACGT")
+            elif r < 0.66:
+                t.insert(pos, rng.choice("ACGT"))
+            elif t:
+                del t[pos]
+        t = "".join(t)
+        pen = rng.choice([(4, 6, 2), (2, 3, 1), (3, 5, 2), (1, 1, 1), (5, 2, 3), (4, 0, 2)])
+        assert oracle.bialign(p, t, *pen) == bidir_rule.bialign(p, t, *pen), (p, t, pen)
+
+
+def test_c_bialign_optimal_at_1kbp(oracle):
+    """At the 1 kbp, 5 % shape every bidirectional CIGAR costs the optimum
+    (about half of them differ from the one-direction backtrace)."""
+    import numpy as np
+
+    from tsunami_pact_b200 import gen_batch
+
+    pb, po, pl, tb, to, tl = gen_batch(77, np.full(16, 1000, np.int32), np.full(16, 0.05))
+    for i in range(16):
+        p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
+        ops = oracle.bialign(p, t, 4, 6, 2)
+        assert oracle.cigar_cost(ops, p, t, 4, 6, 2) == oracle.align(p, t, 4, 6, 2)[0]
