@@ -68,7 +68,10 @@ def test_segments_with_gap_components():
 def test_split_halves_are_optimal():
     """Cutting a segment at its breakpoint: the halves' optimal costs add up
     to the segment's, and where the score is positive both halves are
-    usually cheaper (the cut sits near the middle in score)."""
+    usually cheaper (the cut sits near the middle in score).  The search
+    must still try every split of a total: forward and reverse greedy
+    passes can follow different optimal paths (a gap placed in different
+    rows) that meet only at an outer split."""
     rng = random.Random(9)
     positive = cheaper = 0
     for it in range(300):
@@ -159,7 +162,7 @@ def test_c_bialign_equals_the_model(oracle):
             elif t:
                 del t[pos]
         t = "".join(t)
-        pen = rng.choice([(4, 6, 2), (2, 3, 1), (3, 5, 2), (1, 1, 1), (5, 2, 3), (4, 0, 2)])
+        pen = rng.choice([(4, 6, 2), (2, 3, 1), (3, 5, 2), (1, 1, 1), (5, 2, 3), (4, 0, 2), (1, 10, 1), (9, 1, 1)])
         assert oracle.bialign(p, t, *pen) == bidir_rule.bialign(p, t, *pen), (p, t, pen)
 
 
@@ -175,3 +178,12 @@ def test_c_bialign_optimal_at_1kbp(oracle):
         p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
         ops = oracle.bialign(p, t, 4, 6, 2)
         assert oracle.cigar_cost(ops, p, t, 4, 6, 2) == oracle.align(p, t, 4, 6, 2)[0]
+
+
+def test_outer_split_needed():
+    """'GC' against 'GTGAGC' at 5/2/3: the forward pass puts the gap after
+    the first base, the reverse pass before it, so the first overlap is at
+    an outer split (one side at score 0), not near the middle."""
+    total, where = bidir_rule.first_breakpoint("GC", "GTGAGC", 5, 2, 3, 30)
+    assert total == 14 == bidir_rule.gotoh_components("GC", "GTGAGC", 5, 2, 3)
+    assert 0 in (where[1], where[2])
