@@ -334,3 +334,47 @@ def ops_cost(ops: str, p: str, t: str, x: int, o: int, e: int, begin: str = "M",
     if end in "ID" and (not ops or ops[-1] != end) and not (not ops and begin == end):
         return None
     return cost
+
+
+def crossing_total(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
+    """Lowest total found the way a two-ring kernel could search: forward and
+    reverse advance in turns (the lower score first, forward on ties), and
+    each new wavefront is checked only against the other direction's last
+    max(x, o + e) + 1 scores.  Overlap is offsets crossing on a diagonal
+    (forward + reverse >= n; in I or D the total counts one opening).  The
+    search stops once no unchecked pair can beat the best total.  It finds
+    the optimum of segments free at their end (pinned by the tests).  For a
+    segment that must end in a gap it can miss it: the forward greedy run
+    passes the cell the closing gap leaves from, and only an outer split,
+    outside the window, meets."""
+    m, n = len(p), len(t)
+    mx = max(x, o + e)
+    smax = (m + n) * mx + 2 * (o + e) + 2
+    FM, _, FI, FD = wavefronts(p, t, x, o, e, smax, start=begin)
+    RM, _, RI, RD = wavefronts(p[::-1], t[::-1], x, o, e, smax, forced=end)
+
+    def check(sf, sr):
+        found = None
+        for Fw, Rw, cut in ((FM, RM, 0), (FI, RI, o), (FD, RD, o)):
+            for k, hf in Fw.get(sf, {}).items():
+                hr = Rw.get(sr, {}).get((n - m) - k)
+                if hr is not None and hf + hr >= n:
+                    found = sf + sr - cut if found is None else min(found, sf + sr - cut)
+        return found
+
+    sf = sr = 0
+    best = check(0, 0)
+    while sf <= smax:
+        if best is not None and sf + sr - 2 * mx - o > best:
+            break
+        if sf <= sr:
+            sf += 1
+            pairs = [(sf, s2) for s2 in range(max(0, sr - mx), sr + 1)]
+        else:
+            sr += 1
+            pairs = [(s1, sr) for s1 in range(max(0, sf - mx), sf + 1)]
+        for a, b in pairs:
+            c = check(a, b)
+            if c is not None and (best is None or c < best):
+                best = c
+    return best

@@ -187,3 +187,24 @@ def test_outer_split_needed():
     total, where = bidir_rule.first_breakpoint("GC", "GTGAGC", 5, 2, 3, 30)
     assert total == 14 == bidir_rule.gotoh_components("GC", "GTGAGC", 5, 2, 3)
     assert 0 in (where[1], where[2])
+
+
+def test_ring_window_crossing_finds_free_end_optimum():
+    """The overlap search a two-ring kernel could run (turns, a window of the
+    last max(x, o+e) + 1 scores, offsets crossing) reaches the optimum of
+    segments free at their end; for 'AG' against 'AG' forced to end in an
+    insertion it does not (the outer split it needs lies outside the
+    window)."""
+    rng = random.Random(1)
+    checked = 0
+    for it in range(600):
+        p, t, pen = _case(rng, it)
+        if not p and not t:
+            continue
+        for a in "MID":
+            best = bidir_rule.gotoh_components(p, t, *pen, a, "M")
+            assert bidir_rule.crossing_total(p, t, *pen, a, "M") == best, (p, t, pen, a)
+            checked += 1
+    assert checked > 1500
+    assert bidir_rule.crossing_total("AG", "AG", 1, 1, 1, "M", "I") != bidir_rule.gotoh_components(
+        "AG", "AG", 1, 1, 1, "M", "I")
