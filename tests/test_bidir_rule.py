@@ -208,3 +208,30 @@ def test_ring_window_crossing_finds_free_end_optimum():
     assert checked > 1500
     assert bidir_rule.crossing_total("AG", "AG", 1, 1, 1, "M", "I") != bidir_rule.gotoh_components(
         "AG", "AG", 1, 1, 1, "M", "I")
+
+
+def test_ring_window_crossing_on_recursion_segments():
+    """The segments a recursion on breakpoints actually produces -- a
+    gap-ended left half comes from a gap meet, where the forward pass itself
+    reached the corner in that gap -- all get their optimum from the
+    ring-window crossing search."""
+    rng = random.Random(7)
+    count = 0
+
+    def walk(p, t, pen, a, b):
+        nonlocal count
+        if not p and not t:
+            return
+        assert bidir_rule.crossing_total(p, t, *pen, a, b) == bidir_rule.gotoh_components(p, t, *pen, a, b)
+        count += 1
+        total, left, right = bidir_rule.split(p, t, *pen, a, b)
+        whole = len(p) + len(t)
+        if total <= 0 or len(left[0]) + len(left[1]) in (0, whole) or len(right[0]) + len(right[1]) in (0, whole):
+            return
+        walk(*left[:2], pen, *left[2:])
+        walk(*right[:2], pen, *right[2:])
+
+    for it in range(100):
+        p, t, pen = _case(rng, it, maxlen=40, maxedits=10)
+        walk(p, t, pen, "M", "M")
+    assert count > 250
