@@ -336,36 +336,31 @@ def ops_cost(ops: str, p: str, t: str, x: int, o: int, e: int, begin: str = "M",
     return cost
 
 
-def crossing_total(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
-    """Lowest total found the way a two-ring kernel could search: forward and
-    reverse advance in turns (the lower score first, forward on ties), and
-    each new wavefront is checked only against the other direction's last
-    max(x, o + e) + 1 scores.  Overlap is offsets crossing on a diagonal
-    (forward + reverse >= n; in I or D the total counts one opening).  The
-    search stops once no unchecked pair can beat the best total.  It finds
-    the optimum of segments free at their end (pinned by the tests).  For a
-    segment that must end in a gap it can miss it: the forward greedy run
-    passes the cell the closing gap leaves from, and only an outer split,
-    outside the window, meets."""
+def _crossing_search(p: str, t: str, x: int, o: int, e: int, begin: str, end: str):
+    """(total, component, k, h) of the ring-window crossing search (see
+    crossing_total), or None."""
     m, n = len(p), len(t)
     mx = max(x, o + e)
     smax = (m + n) * mx + 2 * (o + e) + 2
-    FM, _, FI, FD = wavefronts(p, t, x, o, e, smax, start=begin)
+    FM, FMp, FI, FD = wavefronts(p, t, x, o, e, smax, start=begin)
     RM, _, RI, RD = wavefronts(p[::-1], t[::-1], x, o, e, smax, forced=end)
 
     def check(sf, sr):
         found = None
-        for Fw, Rw, cut in ((FM, RM, 0), (FI, RI, o), (FD, RD, o)):
-            for k, hf in Fw.get(sf, {}).items():
+        for comp, Fw, Rw, cut in (("M", FM, RM, 0), ("I", FI, RI, o), ("D", FD, RD, o)):
+            for k in sorted(Fw.get(sf, {})):
+                hf = Fw[sf][k]
                 hr = Rw.get(sr, {}).get((n - m) - k)
                 if hr is not None and hf + hr >= n:
-                    found = sf + sr - cut if found is None else min(found, sf + sr - cut)
+                    h = max(FMp[sf][k], n - hr) if comp == "M" else hf
+                    if found is None or sf + sr - cut < found[0]:
+                        found = (sf + sr - cut, comp, k, h)
         return found
 
     sf = sr = 0
     best = check(0, 0)
     while sf <= smax:
-        if best is not None and sf + sr - 2 * mx - o > best:
+        if best is not None and sf + sr - 2 * mx - o > best[0]:
             break
         if sf <= sr:
             sf += 1
@@ -375,6 +370,36 @@ def crossing_total(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end
             pairs = [(s1, sr) for s1 in range(max(0, sf - mx), sf + 1)]
         for a, b in pairs:
             c = check(a, b)
-            if c is not None and (best is None or c < best):
+            if c is not None and (best is None or c[0] < best[0]):
                 best = c
     return best
+
+
+def crossing_total(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
+    """Lowest total found the way a two-ring kernel could search: forward and
+    reverse advance in turns (the lower score first, forward on ties), and
+    each new wavefront is checked only against the other direction's last
+    max(x, o + e) + 1 scores.  Overlap is offsets crossing on a diagonal
+    (forward + reverse >= n; in I or D the total counts one opening); the
+    lowest total wins (the first found on ties: M before I before D,
+    diagonals ascending).  The search stops once no unchecked pair can beat
+    the best total.  It finds the optimum of segments free at their end and
+    of every segment the recursion produces (pinned by the tests).  For an
+    arbitrary segment forced to end in a gap it can miss it: the forward
+    greedy run passes the cell the closing gap leaves from, and only an
+    outer split, outside the window, meets."""
+    found = _crossing_search(p, t, x, o, e, begin, end)
+    return None if found is None else found[0]
+
+
+def crossing_split(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):
+    """split() driven by the ring-window crossing search: (T, left, right).
+    An M crossing is cut at max(forward pre-extension offset, n - reverse
+    offset) -- inside the forward run, where the reverse side has already
+    reached -- and a gap crossing where the forward gap cell is."""
+    found = _crossing_search(p, t, x, o, e, begin, end)
+    if found is None:
+        return None, None, None
+    T, comp, k, h = found
+    v = h - k
+    return T, (p[:v], t[:h], begin, comp), (p[v:], t[h:], comp, end)

@@ -235,3 +235,33 @@ def test_ring_window_crossing_on_recursion_segments():
         p, t, pen = _case(rng, it, maxlen=40, maxedits=10)
         walk(p, t, pen, "M", "M")
     assert count > 250
+
+
+def test_crossing_split_recursion_is_optimal():
+    """A recursion driven only by the ring-window crossing search: every cut
+    yields halves whose optimal costs add up to the segment's optimum."""
+    rng = random.Random(3)
+    count = 0
+
+    def walk(p, t, pen, a, b):
+        nonlocal count
+        if not p and not t:
+            return
+        best = bidir_rule.gotoh_components(p, t, *pen, a, b)
+        total, left, right = bidir_rule.crossing_split(p, t, *pen, a, b)
+        assert total == best
+        assert left[0] + right[0] == p and left[1] + right[1] == t
+        cl = bidir_rule.gotoh_components(left[0], left[1], *pen, left[2], left[3])
+        cr = bidir_rule.gotoh_components(right[0], right[1], *pen, right[2], right[3])
+        assert cl + cr == best, (p, t, pen, a, b, left, right, cl, cr)
+        count += 1
+        whole = len(p) + len(t)
+        if total <= 0 or len(left[0]) + len(left[1]) in (0, whole) or len(right[0]) + len(right[1]) in (0, whole):
+            return
+        walk(*left[:2], pen, *left[2:])
+        walk(*right[:2], pen, *right[2:])
+
+    for it in range(120):
+        p, t, pen = _case(rng, it, maxlen=40, maxedits=10)
+        walk(p, t, pen, "M", "M")
+    assert count > 300
