@@ -286,22 +286,25 @@ def wfa_segment(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: s
     return cost, None if ops is None else ops[::-1]
 
 
-def bialign(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M", base_score: int = 0) -> str:
+def bialign(p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M", base_score: int = 0,
+            ring: bool = False) -> str:
     """Operations of a bidirectional alignment: split at the breakpoint
     until a segment's score is at most base_score (default two of the
     dearest single edits) or a cut makes no progress, then the plain WFA of
-    the segment (wfa_segment), the pieces concatenated in order."""
+    the segment (wfa_segment), the pieces concatenated in order.  ring:
+    cut by the two-ring crossing search (crossing_split) instead of the
+    full intersection search (split)."""
     if not p and not t:
         return ""
     base = base_score or 2 * max(x, o + e)
-    total, left, right = split(p, t, x, o, e, begin, end)
+    total, left, right = (crossing_split if ring else split)(p, t, x, o, e, begin, end)
     if total is None:
         raise AssertionError("no breakpoint")
     whole = len(p) + len(t)
     if total <= base or len(left[0]) + len(left[1]) in (0, whole) or len(right[0]) + len(right[1]) in (0, whole):
         return wfa_segment(p, t, x, o, e, begin, end)[1]
-    return (bialign(left[0], left[1], x, o, e, left[2], left[3], base)
-            + bialign(right[0], right[1], x, o, e, right[2], right[3], base))
+    return (bialign(left[0], left[1], x, o, e, left[2], left[3], base, ring)
+            + bialign(right[0], right[1], x, o, e, right[2], right[3], base, ring))
 
 
 def ops_cost(ops: str, p: str, t: str, x: int, o: int, e: int, begin: str = "M", end: str = "M"):

@@ -57,6 +57,9 @@ def lib():
         L.ora_align.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(OraStats)]
         L.ora_bialign.restype = ctypes.c_int
+        L.ora_bialign_ring.restype = ctypes.c_int
+        L.ora_bialign_ring.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 4 + [
+            ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.ora_bialign.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 4 + [
             ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.ora_gotoh_score.restype = ctypes.c_int
@@ -467,14 +470,16 @@ def align_batch2_ends_free(patterns, texts, free, x=4, o1=6, e1=2, o2=24, e2=1, 
     return _batch_free(lib().ora_align_batch2_ends_free, patterns, texts, (x, o1, e1, o2, e2), free, cigar, threads)
 
 
-def bialign(pattern, text, x=4, o=6, e=2, base_score=0) -> str:
+def bialign(pattern, text, x=4, o=6, e=2, base_score=0, ring=False) -> str:
     """Operations of the bidirectional alignment (ora_bialign: breakpoint
-    recursion, the C form of bidir_rule.bialign)."""
+    recursion, the C form of bidir_rule.bialign; ring=True: cut by the
+    two-ring crossing search, ora_bialign_ring)."""
     p, t = _b(pattern), _b(text)
     cap = len(p) + len(t) + 1
     buf = ctypes.create_string_buffer(cap)
     n = ctypes.c_int(0)
-    rc = lib().ora_bialign(p, len(p), t, len(t), x, o, e, base_score, buf, cap, ctypes.byref(n))
+    fn = lib().ora_bialign_ring if ring else lib().ora_bialign
+    rc = fn(p, len(p), t, len(t), x, o, e, base_score, buf, cap, ctypes.byref(n))
     if rc != 0:
         raise RuntimeError(f"ora_bialign failed: {rc}")
     return buf.raw[: n.value].decode()

@@ -163,6 +163,12 @@ int tsu_check_align_scores(int64_t n, const char* pat, const int64_t* poff, cons
  * negative error.  ops_cap >= m + n suffices. */
 int ora_bialign(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
                 char* ops, int ops_cap, int* ops_len);
+/* The same recursion cut by the two-ring search (forward and reverse in
+ * turns, each new wavefront checked against the other side's last
+ * max(x, o+e) + 1 scores for crossing offsets): what a GPU kernel with two
+ * rings per pair computes. */
+int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
+                     char* ops, int ops_cap, int* ops_len);
 
 #ifdef __cplusplus
 }

@@ -429,15 +429,103 @@ out:
   return rc ? rc : found;
 }
 
+/* The two-ring search: forward and reverse advance in turns (the lower
+ * score first, forward on ties); each new wavefront is checked against the
+ * other side's last max(x, o+e) + 1 scores for offsets crossing on a
+ * diagonal (forward + reverse >= n; gaps count one opening), components M,
+ * I, D in turn, diagonals ascending, the strictly lowest total kept.  An M
+ * crossing is cut at max(forward pre-extension offset, n - reverse
+ * offset), a gap crossing at the forward gap cell (bidir_rule.py
+ * _crossing_search). */
+typedef struct {
+  int have, T, k, h;
+  char comp;
+} bcut_t;
+
+static void cross_check(const bpass_t* F, const bpass_t* R, int sf, int sr, int n, int m, int o, bcut_t* best) {
+  const bwf_t* fw = &F->w[sf];
+  static const int comps[3] = {CM, CI, CD};
+  for (int ci = 0; ci < 3; ++ci) {
+    const int c = comps[ci];
+    if (fw->plo[c] > fw->phi[c]) continue;
+    for (int k = fw->plo[c]; k <= fw->phi[c]; ++k) {
+      const int32_t hf = bw_get(fw, c, k);
+      if (hf == BNULL) continue;
+      const int32_t hr = bget(R, sr, c, (n - m) - k);
+      if (hr == BNULL || hf + hr < n) continue;
+      const int total = sf + sr - (c == CM ? 0 : o);
+      if (best->have && total >= best->T) continue;
+      best->have = 1;
+      best->T = total;
+      best->k = k;
+      best->comp = c == CM ? 'M' : (c == CI ? 'I' : 'D');
+      if (c == CM) {
+        const int32_t pre = bw_get(fw, CMP, k);
+        best->h = pre > n - hr ? pre : n - hr;
+      } else {
+        best->h = hf;
+      }
+    }
+  }
+}
+
+static int crossing_breakpoint(const char* p, int m, const char* t, int n, int x, int o, int e, char begin,
+                               char end, int* T_out, char* comp, int* k_out, int* h_out) {
+  const int mx = x > o + e ? x : o + e;
+  const int smax = (m + n) * mx + 2 * (o + e) + 2;
+  char* rp = (char*)malloc((size_t)m + 1);
+  char* rt = (char*)malloc((size_t)n + 1);
+  bpass_t F = {p, t, m, n, x, o, e, begin, 'M', NULL, 0, 0};
+  bpass_t R = {NULL, NULL, m, n, x, o, e, 'M', end, NULL, 0, 0};
+  bcut_t best = {0, 0, 0, 0, 'M'};
+  int rc = 0;
+  if (!rp || !rt) {
+    rc = ORA_ENOMEM;
+    goto out;
+  }
+  rev_copy(p, m, rp);
+  rev_copy(t, n, rt);
+  R.p = rp;
+  R.t = rt;
+  if ((rc = bp_upto(&F, 0)) || (rc = bp_upto(&R, 0))) goto out;
+  cross_check(&F, &R, 0, 0, n, m, o, &best);
+  int sf = 0, sr = 0;
+  while (sf <= smax) {
+    if (best.have && sf + sr - 2 * mx - o > best.T) break;
+    if (sf <= sr) {
+      ++sf;
+      if ((rc = bp_upto(&F, sf))) goto out;
+      for (int s2 = sr - mx > 0 ? sr - mx : 0; s2 <= sr; ++s2) cross_check(&F, &R, sf, s2, n, m, o, &best);
+    } else {
+      ++sr;
+      if ((rc = bp_upto(&R, sr))) goto out;
+      for (int s1 = sf - mx > 0 ? sf - mx : 0; s1 <= sf; ++s1) cross_check(&F, &R, s1, sr, n, m, o, &best);
+    }
+  }
+  if (best.have) {
+    *T_out = best.T;
+    *comp = best.comp;
+    *k_out = best.k;
+    *h_out = best.h;
+  }
+out:
+  bp_free(&F);
+  bp_free(&R);
+  free(rp);
+  free(rt);
+  return rc ? rc : best.have;
+}
+
 static int bialign_rec(const char* p, int m, const char* t, int n, int x, int o, int e, char begin, char end,
-                       int base, char* ops, int* len) {
+                       int base, int ring, char* ops, int* len) {
   if (m == 0 && n == 0) {
     *len = 0;
     return 0;
   }
   int T = 0, k = 0, h = 0;
   char comp = 'M';
-  const int f = first_breakpoint(p, m, t, n, x, o, e, begin, end, &T, &comp, &k, &h);
+  const int f = ring ? crossing_breakpoint(p, m, t, n, x, o, e, begin, end, &T, &comp, &k, &h)
+                    : first_breakpoint(p, m, t, n, x, o, e, begin, end, &T, &comp, &k, &h);
   if (f < 0) return f;
   if (f == 0) return ORA_EINVAL;
   const int v = h - k;
@@ -445,9 +533,9 @@ static int bialign_rec(const char* p, int m, const char* t, int n, int x, int o,
   if (T <= base || left == 0 || left == whole || right == 0 || right == whole)
     return wfa_segment(p, m, t, n, x, o, e, begin, end, ops, len);
   int l1 = 0, l2 = 0;
-  int rc = bialign_rec(p, v, t, h, x, o, e, begin, comp, base, ops, &l1);
+  int rc = bialign_rec(p, v, t, h, x, o, e, begin, comp, base, ring, ops, &l1);
   if (rc) return rc;
-  rc = bialign_rec(p + v, m - v, t + h, n - h, x, o, e, comp, end, base, ops + l1, &l2);
+  rc = bialign_rec(p + v, m - v, t + h, n - h, x, o, e, comp, end, base, ring, ops + l1, &l2);
   if (rc) return rc;
   *len = l1 + l2;
   return 0;
@@ -458,5 +546,15 @@ int ora_bialign(const char* pattern, int m, const char* text, int n, int x, int 
   if (!pattern || !text || !ops || !ops_len || m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;
   if (ops_cap < m + n) return ORA_ECIGCAP;
   const int mx = x > o + e ? x : o + e;
-  return bialign_rec(pattern, m, text, n, x, o, e, 'M', 'M', base_score > 0 ? base_score : 2 * mx, ops, ops_len);
+  return bialign_rec(pattern, m, text, n, x, o, e, 'M', 'M', base_score > 0 ? base_score : 2 * mx, 0, ops,
+                     ops_len);
+}
+
+int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
+                     char* ops, int ops_cap, int* ops_len) {
+  if (!pattern || !text || !ops || !ops_len || m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;
+  if (ops_cap < m + n) return ORA_ECIGCAP;
+  const int mx = x > o + e ? x : o + e;
+  return bialign_rec(pattern, m, text, n, x, o, e, 'M', 'M', base_score > 0 ? base_score : 2 * mx, 1, ops,
+                     ops_len);
 }

@@ -265,3 +265,23 @@ def test_crossing_split_recursion_is_optimal():
         p, t, pen = _case(rng, it, maxlen=40, maxedits=10)
         walk(p, t, pen, "M", "M")
     assert count > 300
+
+
+def test_c_ring_bialign_equals_the_model_and_is_optimal(oracle):
+    """ora_bialign_ring (the recursion a two-ring GPU kernel computes) is
+    bidir_rule.bialign(ring=True) byte for byte, and optimal at the 1 kbp,
+    5 % shape and on a 5 kbp, 15 % pair."""
+    import numpy as np
+
+    from tsunami_pact_b200 import gen_batch
+
+    rng = random.Random(22)
+    for it in range(50):
+        p, t, pen = _case(rng, it, maxlen=60, maxedits=12)
+        assert oracle.bialign(p, t, *pen, ring=True) == bidir_rule.bialign(p, t, *pen, ring=True), (p, t, pen)
+    lengths = np.array([1000] * 12 + [5000], np.int32)
+    pb, po, pl, tb, to, tl = gen_batch(79, lengths, np.array([0.05] * 12 + [0.15]))
+    for i in range(len(lengths)):
+        p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
+        ops = oracle.bialign(p, t, 4, 6, 2, ring=True)
+        assert oracle.cigar_cost(ops, p, t, 4, 6, 2) == oracle.gotoh(p, t, 4, 6, 2)
