@@ -57,6 +57,9 @@ def lib():
         L.ora_align.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(OraStats)]
         L.ora_bialign.restype = ctypes.c_int
+        L.ora_align_segment.restype = ctypes.c_int
+        L.ora_align_segment.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 3 + [
+            ctypes.c_char, ctypes.c_char, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.ora_bialign_ring.restype = ctypes.c_int
         L.ora_bialign_ring.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 4 + [
             ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -483,3 +486,17 @@ def bialign(pattern, text, x=4, o=6, e=2, base_score=0, ring=False) -> str:
     if rc != 0:
         raise RuntimeError(f"ora_bialign failed: {rc}")
     return buf.raw[: n.value].decode()
+
+
+def align_segment(pattern, text, x=4, o=6, e=2, begin="M", end="M"):
+    """(cost, operations) of one segment with gap components
+    (ora_align_segment, the C form of bidir_rule.wfa_segment)."""
+    p, t = _b(pattern), _b(text)
+    cap = len(p) + len(t) + 1
+    buf = ctypes.create_string_buffer(cap)
+    n = ctypes.c_int(0)
+    rc = lib().ora_align_segment(p, len(p), t, len(t), x, o, e, begin.encode(), end.encode(), buf, cap,
+                                 ctypes.byref(n))
+    if rc < 0:
+        raise RuntimeError(f"ora_align_segment failed: {rc}")
+    return rc, buf.raw[: n.value].decode()

@@ -169,6 +169,13 @@ int ora_bialign(const char* pattern, int m, const char* text, int n, int x, int 
  * rings per pair computes. */
 int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
                      char* ops, int ops_cap, int* ops_len);
+/* One segment of a bidirectional alignment by the plain WFA with gap
+ * components (the recursion's base case): begin 'I'/'D' continues a gap
+ * from the left (a leading run costs e per base), end 'I'/'D' requires the
+ * last operation to be that gap ('M': free).  Returns the cost (>= 0) or a
+ * negative error; operations as ora_align. */
+int ora_align_segment(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
+                      char end, char* ops, int ops_cap, int* ops_len);
 
 #ifdef __cplusplus
 }

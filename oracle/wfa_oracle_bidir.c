@@ -193,7 +193,7 @@ static int64_t max64(int64_t a, int64_t b) { return a > b ? a : b; }
 /* Operations of (p, t) forward from start/forced, ended in M or (free_end
  * I/D) in that gap at a discount of o; written in order to ops[0..len). */
 static int wfa_forward(const char* p, int m, const char* t, int n, int x, int o, int e, char start, char forced,
-                       char free_end, char* ops, int* len) {
+                       char free_end, char* ops, int* len, int* cost) {
   bpass_t bp = {p, t, m, n, x, o, e, start, forced, NULL, 0, 0};
   const int k_end = n - m;
   const int mx = x > o + e ? x : o + e;
@@ -224,6 +224,7 @@ static int wfa_forward(const char* p, int m, const char* t, int n, int x, int o,
     rc = ORA_EINVAL;
     goto out;
   }
+  if (cost) *cost = best_cost;
   {
     /* operations backwards into ops[cap-1 ...] */
     const int cap = m + n + 1;
@@ -302,12 +303,13 @@ out:
 }
 
 static int wfa_segment(const char* p, int m, const char* t, int n, int x, int o, int e, char begin, char end,
-                       char* ops, int* len) {
+                       char* ops, int* len, int* cost) {
   if (m == 0 && n == 0) {
     *len = 0;
+    if (cost) *cost = 0;
     return 0;
   }
-  if (end == 'M') return wfa_forward(p, m, t, n, x, o, e, begin, 'M', 'M', ops, len);
+  if (end == 'M') return wfa_forward(p, m, t, n, x, o, e, begin, 'M', 'M', ops, len, cost);
   char* rp = (char*)malloc((size_t)m + 1);
   char* rt = (char*)malloc((size_t)n + 1);
   if (!rp || !rt) {
@@ -317,7 +319,7 @@ static int wfa_segment(const char* p, int m, const char* t, int n, int x, int o,
   }
   rev_copy(p, m, rp);
   rev_copy(t, n, rt);
-  int rc = wfa_forward(rp, m, rt, n, x, o, e, 'M', end, begin, ops, len);
+  int rc = wfa_forward(rp, m, rt, n, x, o, e, 'M', end, begin, ops, len, cost);
   free(rp);
   free(rt);
   if (rc) return rc;
@@ -531,7 +533,7 @@ static int bialign_rec(const char* p, int m, const char* t, int n, int x, int o,
   const int v = h - k;
   const int whole = m + n, left = v + h, right = whole - left;
   if (T <= base || left == 0 || left == whole || right == 0 || right == whole)
-    return wfa_segment(p, m, t, n, x, o, e, begin, end, ops, len);
+    return wfa_segment(p, m, t, n, x, o, e, begin, end, ops, len, NULL);
   int l1 = 0, l2 = 0;
   int rc = bialign_rec(p, v, t, h, x, o, e, begin, comp, base, ring, ops, &l1);
   if (rc) return rc;
@@ -557,4 +559,14 @@ int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x,
   const int mx = x > o + e ? x : o + e;
   return bialign_rec(pattern, m, text, n, x, o, e, 'M', 'M', base_score > 0 ? base_score : 2 * mx, 1, ops,
                      ops_len);
+}
+
+int ora_align_segment(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
+                      char end, char* ops, int ops_cap, int* ops_len) {
+  if (!pattern || !text || !ops || !ops_len || m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;
+  if (!strchr("MID", begin) || !strchr("MID", end) || !begin || !end) return ORA_EINVAL;
+  if (ops_cap < m + n) return ORA_ECIGCAP;
+  int cost = 0;
+  const int rc = wfa_segment(pattern, m, text, n, x, o, e, begin, end, ops, ops_len, &cost);
+  return rc ? rc : cost;
 }

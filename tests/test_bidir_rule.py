@@ -285,3 +285,20 @@ def test_c_ring_bialign_equals_the_model_and_is_optimal(oracle):
         p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
         ops = oracle.bialign(p, t, 4, 6, 2, ring=True)
         assert oracle.cigar_cost(ops, p, t, 4, 6, 2) == oracle.gotoh(p, t, 4, 6, 2)
+
+
+def test_c_segment_equals_the_model(oracle):
+    """ora_align_segment, the checker for segment components in a GPU CIGAR
+    kernel, is bidir_rule.wfa_segment (cost and operations) for all nine
+    begin/end pairs."""
+    rng = random.Random(8)
+    checked = 0
+    for it in range(120):
+        p, t, pen = _case(rng, it, maxlen=16, maxedits=6)
+        for a in "MID":
+            for b in "MID":
+                if (p or t) and bidir_rule.gotoh_components(p, t, *pen, a, b) >= bidir_rule.INF:
+                    continue
+                assert oracle.align_segment(p, t, *pen, a, b) == bidir_rule.wfa_segment(p, t, *pen, a, b)
+                checked += 1
+    assert checked > 800
