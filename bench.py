@@ -9,12 +9,19 @@ WFA2-style CIGARs) -> CIGAR compaction, for the whole batch.
   e2e    the same through tsu_align_batch with pinned HOST buffers: H2D of
          the sequences, the device work and D2H of scores + CIGARs per step
 
-Default workload: 1,000,000 pairs of 1,000 bp, 5% edits (equal sub/ins/del),
-penalties 4/6/2, seeded synthetic data.  `--impl reference` times the CPU
-path (the oracle's WFA, the stand-in for the reference's WFA2-lib check,
-wfa_gpu.cu:150-166) on all host cores over a bounded sample of the same
-workload.  Under torchrun each rank aligns its own batch (weak scaling, no
-collective on the data path); the step time is the max over ranks.
+Default workload (c4): 200,000 pairs of uneven length (log-uniform
+100-20,000 bp) and edit rate (uniform 1-15 % per pair, equal
+sub/ins/del), penalties 4/6/2, seeded synthetic data, aligned by the batched
+form (length bands, persistent launches over a device work queue, one CUDA
+graph per call) and, beside it, by the plain form (one launch per
+floor(log2 L) bucket, one warp per pair).  A full c2 record (1,000,000 x
+1 kbp at 5 %, the plain one-launch shape) is nested under "secondary".
+`--impl reference` times the CPU path (the oracle's WFA, the stand-in for
+the reference's WFA2-lib check, wfa_gpu.cu:150-166) on all host cores over
+a bounded sample of the same workload, with pairs from the oracle's copy of
+the generator.  Under torchrun each rank aligns its own batch (weak
+scaling, no collective on the data path); the step time is the max over
+ranks.
 """
 from __future__ import annotations
 
@@ -309,24 +316,31 @@ def run_serving(args):
 
 
 def run_reference(args, workload):
-    """CPU path on the host cores, rank 0 only (other ranks exit 0)."""
+    """CPU path on the host cores, rank 0 only (other ranks exit 0).  The
+    pairs come from the oracle's copy of the seeded generator, so this arm
+    never loads the engine library (checked at the end)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
 
-    from tsunami_pact_b200 import datasets
+    from tsunami_pact_b200.datasets import shape
 
     n_all, desc = WORKLOADS[workload]
     cores = os.cpu_count() or 1
+
+    def generate(n):
+        lengths, rates, seed = shape(workload, n)
+        return O.gen_batch(seed, lengths, rates)
+
     # a bounded sample of the same workload: sized so each step is ~5-10 s
     probe = max(256, cores * 64)
-    pb, po, pl, tb, to, tl = datasets.generate(workload, probe)
+    pb, po, pl, tb, to, tl = generate(probe)
     t0 = time.perf_counter()
     oracle_batch(O, pb, po, pl, tb, to, tl, cores)
     r = probe / max(time.perf_counter() - t0, 1e-6)
     sample = int(min(n_all, max(probe, r * 6.0)))
-    pb, po, pl, tb, to, tl = datasets.generate(workload, sample)
+    pb, po, pl, tb, to, tl = generate(sample)
     cells = float(np.sum(pl.astype(np.float64) * tl))
     for _ in range(args.warmup):
         k = min(sample, probe)
@@ -338,6 +352,12 @@ def run_reference(args, workload):
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
     gcups = cells / t / 1e9
+    try:
+        with open("/proc/self/maps") as f:
+            if "libtsunami_b200" in f.read():
+                raise SystemExit("reference arm: the engine library was loaded")
+    except OSError:
+        pass
     out = {
         "metric": METRIC, "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -359,7 +379,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tsunami", choices=["tsunami", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c5"])
+    ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS) + ["c5"])
+    ap.add_argument("--no-secondary", action="store_true", help="c4: skip the nested c2 record")
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="timed steps of the host-buffer leg (0: --steps; c4: at most 3)")
     ap.add_argument("--score-only", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -407,10 +430,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, workload)
         return
+    if workload == "c4" and args.e2e_steps <= 0:
+        args.e2e_steps = min(args.steps, 3)  # one c4 step is seconds long
 
     import torch
-
-    import tsunami_pact_b200 as T
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -422,6 +445,31 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    head = measure(args, workload, rank, world, local, dist,
+                   with_plain=(workload == "c4" or args.plain) and not args.no_plain,
+                   with_cpu=world == 1 and not args.no_cpu_baseline, e2e_steps=args.e2e_steps)
+    # the default run (c4) nests a full c2 record: the plain one-launch GPU
+    # shape at scale (1,000,000 x 1 kbp), measured the same way
+    if workload == "c4" and not args.no_secondary and not args.pairs:
+        sec = measure(args, "c2", rank, world, local, dist, with_plain=False, with_cpu=False, e2e_steps=args.steps)
+        if head is not None:
+            head["secondary"] = {"c2": {k: sec[k] for k in ("value", "unit", "ms_per_step", "pairs_per_s", "steps",
+                                                           "warmup", "gpu_launches", "e2e", "roofline", "clocks",
+                                                           "config")}}
+    if rank == 0 and head is not None:
+        print(json.dumps(head), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_steps):
+    """One workload on this rank's GPU: the device-resident leg (value), the
+    plain form (with_plain), the host-buffer leg (e2e) and the roofline of the
+    align passes; the JSON record on rank 0 (None elsewhere)."""
+    import torch
+
+    import tsunami_pact_b200 as T
     from tsunami_pact_b200.shard import barrier as shard_barrier
     from tsunami_pact_b200.shard import combine, throughput
 
@@ -463,7 +511,7 @@ def main():
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    step_ms, align_ms, launches, work_cells = [], [], 0, 0
+    step_ms, align_ms, launches, work_cells, work_steps = [], [], 0, 0, 0
     t_wall = time.perf_counter()
     for _ in range(args.steps):
         nruns = dev_step()
@@ -471,7 +519,7 @@ def main():
         step_ms.append(tm["total_ms"])
         align_ms.append(tm["align_ms"])
         launches += int(tm["kernel_launches"])
-        work_cells = tm["cells"]
+        work_cells, work_steps = tm["cells"], tm["steps"]
         pass_log = al.pass_log()
     barrier()
     wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
@@ -481,10 +529,11 @@ def main():
                                        f"cuda:{local}")
     value = throughput(cells_all, ms) / 1e9
     pairs_s = throughput(pairs_all, ms)
+    cigar_ops = int(torch.sum(d_runs[:nruns].view(torch.int32) >> 4).item()) if want_cigar and nruns else 0
 
-    # ---- plain form (c4): one call per log2-length bucket, one warp per pair
+    # ---- plain form: one call per log2-length bucket, one warp per pair
     plain = None
-    if (workload == "c4" or args.plain) and not args.no_plain:
+    if with_plain:
         from tsunami_pact_b200 import datasets
 
         buckets = datasets.length_buckets(plen)
@@ -495,8 +544,8 @@ def main():
             sub.append((int(b), len(idx), [torch.from_numpy(x[idx]).to(dev) for x in (poff, plen, toff, tlen)]))
         p_ms, p_launch = [], 0
         # the first repetition warms up; each timed one is a whole uneven
-        # batch in one-warp launches (about a minute on c4), so the plain
-        # form has its own repetition count
+        # batch in one-warp launches, so the plain form has its own
+        # repetition count
         for rep in range(max(args.plain_steps, 1) + 1):
             tot = 0.0
             for b, nb, (bo, bl, to_, tl_) in sub:
@@ -530,6 +579,8 @@ def main():
     # ---- e2e: host buffers (pinned) through tsu_align_batch ---------------
     e2e = None
     if not args.no_e2e:
+        e_steps = max(1, e2e_steps if e2e_steps > 0 else args.steps)
+
         def pinned(a):
             t = torch.empty(a.shape, dtype={np.uint8: torch.uint8, np.int64: torch.int64,
                                             np.int32: torch.int32}[a.dtype.type], pin_memory=True)
@@ -549,47 +600,28 @@ def main():
             e2e_step()
         barrier()
         e_ms, hb, db = [], 0, 0
-        for _ in range(args.steps):
+        for _ in range(e_steps):
             e2e_step()
             tm = al.timing()
             e_ms.append(tm["total_ms"])
             hb, db = tm["h2d_bytes"], tm["d2h_bytes"]
-            launches_e2e = int(tm["kernel_launches"])
         barrier()
         ems = max_over_ranks(float(np.mean(e_ms)))
         e2e = {"value": throughput(cells_all, ems) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": int(hb),
-               "d2h_bytes_per_step": int(db), "ms_per_step": ems, "pairs_per_s": throughput(pairs_all, ems)}
+               "d2h_bytes_per_step": int(db), "ms_per_step": ems, "pairs_per_s": throughput(pairs_all, ems),
+               "steps": e_steps}
         # correctness of the e2e output against the device leg
         if want_cigar and not np.array_equal(outs[0], d_sc.cpu().numpy()):
             raise SystemExit("e2e scores differ from the device-resident leg")
 
-    # ---- roofline of the align kernel ------------------------------------
-    peak, peak_kind = measured_peaks()
+    # ---- roofline of the align passes ---------------------------------------
     a_ms = float(np.mean(align_ms))
-    words = float(np.sum((plen.astype(np.int64) + 31) // 32 + 1) + np.sum((tlen.astype(np.int64) + 31) // 32 + 1))
-    packed_in = words * 8
-    out_bytes = n_pairs * 4 + (4 * nruns if want_cigar else 0)
-    hist_bytes = 4 * work_cells if want_cigar else 0  # one backtrace word per (score, diagonal) cell
-    algo = packed_in + out_bytes + hist_bytes
-    achieved = algo / (a_ms / 1e3) / 1e9
-    model = "_" + METRIC_NAME if METRIC_NAME else ("_dual" if len(PEN) == 5 else "")
-    prof = load_traffic(f"align_{workload}{model}") if want_cigar else None
-    traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
-            "align_kernel<score>", "kernel_ms": a_ms,
-            "algorithmic_bytes_per_launch": algo,
-            "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log}
-    if prof:
-        # the binding resource of this integer kernel is instruction issue, not DRAM
-        roof["issue_active_frac"] = prof.get("issue_active_frac")
-        roof["alu_pipe_frac"] = prof.get("alu_pipe_frac")
-        roof["traffic_source"] = prof.get("source")
+    roof = roofline(workload, n_pairs, plen, tlen, nruns if want_cigar else 0, work_cells, work_steps, cigar_ops,
+                    a_ms, clk, want_cigar, pass_log)
 
+    cpu = cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen) if (with_cpu and rank == 0) else None
+    out = None
     if rank == 0:
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen)
         out = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -613,11 +645,39 @@ def main():
             out["predicted_device_bytes"] = {"full": int(full_b), "min": int(min_b)}
         except T.AlignError:
             pass
-        print(json.dumps(out), flush=True)
     al.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    del d_p, d_t, d_po, d_pl, d_to, d_tl, d_sc, d_off, d_runs
+    torch.cuda.empty_cache()
+    return out
+
+
+def roofline(workload, n_pairs, plen, tlen, nruns, work_cells, work_steps, cigar_ops, a_ms, clk, want_cigar,
+             pass_log):
+    """Roofline of the align passes (the dominant kernels: 95-99.9 % of
+    device time).  HBM: algorithmic bytes (packed input, scores, CIGAR runs,
+    one 4-byte backtrace word per wavefront cell) per second against the
+    measured copy bandwidth, with the DRAM traffic of an ncu capture of the
+    same kernel scaled by pairs."""
+    peak, peak_kind = measured_peaks()
+    words = float(np.sum((plen.astype(np.int64) + 31) // 32 + 1) + np.sum((tlen.astype(np.int64) + 31) // 32 + 1))
+    packed_in = words * 8
+    out_bytes = n_pairs * 4 + 4 * nruns
+    hist_bytes = 4 * work_cells if want_cigar else 0
+    algo = packed_in + out_bytes + hist_bytes
+    achieved = algo / (a_ms / 1e3) / 1e9
+    model = "_" + METRIC_NAME if METRIC_NAME else ("_dual" if len(PEN) == 5 else "")
+    prof = load_traffic(f"align_{workload}{model}") if want_cigar else None
+    traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
+            "align_kernel<score>", "kernel_ms": a_ms,
+            "algorithmic_bytes_per_launch": algo, "cells": work_cells, "score_steps": work_steps,
+            "cigar_ops": cigar_ops, "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log}
+    if prof:
+        roof["issue_active_frac"] = prof.get("issue_active_frac")
+        roof["alu_pipe_frac"] = prof.get("alu_pipe_frac")
+        roof["traffic_source"] = prof.get("source")
+    return roof
 
 
 if __name__ == "__main__":

@@ -127,6 +127,7 @@ def lib():
         L.ora_align_batch2.restype = ctypes.c_int
         L.ora_align_batch2.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.ora_gen_batch.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64] + [ctypes.c_void_p] * 8
         _lib = L
     return _lib
 
@@ -500,3 +501,25 @@ def align_segment(pattern, text, x=4, o=6, e=2, begin="M", end="M"):
     if rc < 0:
         raise RuntimeError(f"ora_align_segment failed: {rc}")
     return rc, buf.raw[: n.value].decode()
+
+
+def gen_batch(seed: int, lengths: np.ndarray, rates: np.ndarray, first: int = 0):
+    """Seeded synthetic pairs (ora_gen_batch, wfa_gen.c): the same bytes as
+    the engine's tsu_gen_batch for the same arguments, without loading the
+    engine library.  Returns (pbuf, poff, plen, tbuf, toff, tlen)."""
+    lengths = np.ascontiguousarray(lengths, dtype=np.int32)
+    rates = np.ascontiguousarray(rates, dtype=np.float64)
+    n = lengths.size
+    off = np.zeros(n, dtype=np.int64)
+    if n > 1:
+        np.cumsum(lengths[:-1], out=off[1:])
+    total = int(lengths.sum())
+    pbuf = np.zeros(total + 16, dtype=np.uint8)
+    tbuf = np.zeros(total + 16, dtype=np.uint8)
+    plen = np.zeros(n, dtype=np.int32)
+    tlen = np.zeros(n, dtype=np.int32)
+    rc = lib().ora_gen_batch(seed, first, n, lengths.ctypes.data, rates.ctypes.data, pbuf.ctypes.data,
+                             off.ctypes.data, plen.ctypes.data, tbuf.ctypes.data, off.ctypes.data, tlen.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ora_gen_batch error {rc}")
+    return pbuf, off, plen, tbuf, off.copy(), tlen

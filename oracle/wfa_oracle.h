@@ -177,6 +177,26 @@ int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x,
 int ora_align_segment(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
                       char end, char* ops, int ops_cap, int* ops_len);
 
+/* The seeded pair generator (wfa_gen.c): the same pairs as the engine's
+ * tsu_gen_batch for the same seed, first index and lengths/rates, without
+ * the engine library.  Returns 0 or a negative error. */
+int ora_gen_batch(uint64_t seed, int64_t first, int64_t count, const int32_t* lengths, const double* rates, char* pat,
+                  const int64_t* pat_off, int32_t* pat_len, char* txt, const int64_t* txt_off, int32_t* txt_len);
+
+/* CPU model of the reference's GPU kernel wfa_dispatcher, its defects
+ * included (ref_kernel_model.c).  Pairs of seq_len bytes each at
+ * pat0 + i * seq_len and txt0 + i * seq_len; `front` / `back` bytes are
+ * readable before the first and after the last pair.  scores[i] receives the
+ * kernel's int16 score, codes[i] 0 or the first violation: a wavefront index
+ * outside the pair's ring, a byte read outside the buffers, or no end within
+ * step_cap score steps (steps[i], nullable, receives the steps taken;
+ * maxk[i], nullable, the largest |diagonal| addressed in the ring). */
+#define ORA_REFK_RING  (-10)
+#define ORA_REFK_SEQ   (-11)
+#define ORA_REFK_STEPS (-12)
+int ora_refk_batch(const char* pat0, const char* txt0, int64_t front, int64_t back, int64_t num, int seq_len, int x,
+                   int o, int e, int wf_length, int step_cap, int16_t* scores, int32_t* codes, int32_t* steps,
+                   int32_t* maxk);
 #ifdef __cplusplus
 }
 #endif

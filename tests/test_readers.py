@@ -117,3 +117,17 @@ def test_pair_files_rejected(tmp_path):
         T.read_pairs(str(a), str(b))
     with pytest.raises(T.AlignError):
         T.read_pairs(str(a), str(tmp_path / "missing.fa"))
+
+
+@pytest.mark.parametrize("workload,seed_first", [("c1", 0), ("c2", 5), ("c3", 0), ("c4", 123), ("c5", 40)])
+def test_oracle_generator_matches_engine(oracle, workload, seed_first):
+    """bench.py's CPU reference arm generates its pairs with the oracle's
+    ora_gen_batch so that it never loads the engine library: the bytes must
+    equal tsu_gen_batch's for the same seed, first index and shapes."""
+    from tsunami_pact_b200 import datasets
+
+    lengths, rates, seed = datasets.shape(workload, 300 if workload != "c3" else 20)
+    a = T.gen_batch(seed, lengths, rates, first=seed_first)
+    b = oracle.gen_batch(seed, lengths, rates, first=seed_first)
+    for x, y in zip(a, b):
+        assert x.dtype == y.dtype and np.array_equal(x, y)

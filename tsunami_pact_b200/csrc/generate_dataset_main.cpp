@@ -8,7 +8,7 @@
 // reproducible: pair i depends only on (seed, i).  mode "mixed" (default)
 // splits the round(L*err/100) edits into equal insertion and deletion counts
 // plus substitutions, so every text keeps length L; mode "sub" makes
-// floor(L*err/100) substitutions only, like generate_dataset.cpp:112.
+// floor(L*err/100) substitutions only, like generate_dataset.cpp:23,56-66.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>

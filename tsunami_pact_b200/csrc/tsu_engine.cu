@@ -197,6 +197,11 @@ int grow(tsu_ctx* ctx, DevBuf& b, size_t bytes) {
   nb = (nb + 255) & ~(size_t)255;
   if (ctx->held() - b.cap + nb > ctx->budget) {
     nb = (bytes + 255) & ~(size_t)255;
+    // The wavefront scratch is sized per pass and regrown by the next pass
+    // that needs it (a released buffer has capacity 0): give back the one an
+    // earlier call or pass left behind before refusing.
+    if (ctx->held() - b.cap + nb > ctx->budget && &b != &ctx->b_scratch && ctx->b_scratch.p)
+      release(ctx, ctx->b_scratch);
     if (ctx->held() - b.cap + nb > ctx->budget) {
       ctx->need_bytes = ctx->held() - b.cap + nb;
       return set_err(ctx, TSU_ENOMEM, "device budget %zu B exceeded (need %zu more)", ctx->budget, bytes);

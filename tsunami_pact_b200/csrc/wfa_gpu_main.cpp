@@ -11,8 +11,10 @@
 //     lengths, any byte values are compared exactly;
 //   * check=1 compares against a CPU aligner loaded at run time from the
 //     shared library named by TSU_CHECK_LIB, which must export
-//     tsu_check_align_scores (see INTEGRATION.md for a WFA2-lib adapter);
-//     the reference linked WFA2-lib directly (wfa_gpu.cu:9-11,150-166).
+//     tsu_check_align_scores (a WFA2-lib adapter, or this project's CPU
+//     oracle, oracle/liboracle.so); the reference linked WFA2-lib directly
+//     (wfa_gpu.cu:9-11,150-166).  Without TSU_CHECK_LIB, check=1 prints the
+//     GPU lines, a message on stderr and exits with status 2.
 //   * TSU_CIGAR_OUT=<path> additionally writes "score<TAB>cigar" per pair.
 #include <dlfcn.h>
 
@@ -30,6 +32,8 @@ typedef int (*check_fn)(int64_t n, const char* pat, const int64_t* poff, const i
 int main(int argc, char const* argv[]) {
   if (argc != 7) {  // wfa_gpu.cu:45-48
     printf("ERROR! Please specify in order: mismatch, gap_opening, gap_extension, file name, wf_length, check\n");
+    fprintf(stderr, "check=1 compares the GPU scores with the CPU aligner of the library named by TSU_CHECK_LIB "
+                    "(exporting tsu_check_align_scores)\n");
     return 0;
   }
   const int mismatch = atoi(argv[1]);
