@@ -236,20 +236,22 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* dev_batch, tsu_result*
 
 /* ---- scores without allocating -----------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
- * code recording a CUDA graph (allocation is illegal during capture),
- * plug-ins whose host framework owns every device allocation, services that
- * must not block on or fail in the driver's allocator mid-request.
+ * plug-ins whose host framework owns every device allocation through its own
+ * pool, and services that must not block on, or fail in, the driver's
+ * allocator in the middle of a request.
  * Same inputs as tsu_align_batch_device (device pointers), scores only, work
- * queued on `stream` (a cudaStream_t; NULL = default stream) and finished
- * before the call returns.  It allocates no device memory: its scratch is a
- * fixed 32 MiB array compiled into this library, held by every GPU that
- * loads the library until the process exits.  The first call on a device
- * looks up that array's device address (driver work: make it before any
+ * queued on `stream` (a cudaStream_t; NULL = default stream); the call reads
+ * small counters back from the device on that stream and waits for its work
+ * before it returns.  It allocates no device memory: its scratch is a fixed
+ * 32 MiB array compiled into this library, held by every GPU that loads the
+ * library until the process exits.  The first call on a device looks up that
+ * array's device address (driver work: make that first call before any
  * stream capture).  All calls share the one array: calls whose GPU work
  * overlaps race on it, so serialize them per device.  Batches needing more
- * than the array holds (about 55,000 pairs of 1 kbp, fewer for longer
- * pairs) return TSU_EOVERFLOW without touching the outputs; bad lengths or
- * penalties return TSU_EINVAL. */
+ * than the array holds (about 55,000 pairs of 1 kbp, fewer for longer pairs;
+ * also any batch whose longest pair's HBM wavefront ring would not fit beside
+ * its packed input) return TSU_EOVERFLOW before any score is written; bad
+ * lengths or penalties return TSU_EINVAL. */
 int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batch* dev_batch, int32_t* dev_score, void* stream);
 
 /* ---- render ------------------------------------------------------------

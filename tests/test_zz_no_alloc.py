@@ -1,12 +1,13 @@
 """tsu_align_scores_noalloc: scores without any device allocation.
 
-Callers that cannot call cudaMalloc (CUDA graph capture in progress, host
-frameworks that own all device memory, latency-critical services) use this
-entry point; its scratch is a fixed array compiled into the library.  The test
-calls it through the C ABI twice in a row and checks each result against the
-context-based entry point (tsu_align_batch_device); scores are integers, so
-the tolerance is exact equality.  It also checks that an oversized batch is
-refused and that the second call takes no device memory.
+Callers that cannot call cudaMalloc (plug-ins under a host framework that
+owns all device memory, services that must not block in the allocator
+mid-request) use this entry point; its scratch is a fixed array compiled into
+the library.  The test calls it through the C ABI twice in a row and checks
+each result against the context-based entry point (tsu_align_batch_device)
+and against the CPU oracle; scores are integers, so the tolerance is exact
+equality.  It also checks that oversized batches are refused before any score
+is written and that the second call takes no device memory.
 
 This file is named to be collected last, so a run that stops at the first
 failure has already run every other test."""
@@ -90,6 +91,13 @@ def test_noalloc_matches_context_path_twice():
         got = out.cpu().numpy()
         ref = _reference_scores(t)
         assert np.array_equal(got, ref), np.nonzero(got != ref)[0][:10]
+        # and against the oracle directly: the long pairs (2500, 4000 bp)
+        # take the score-only global-ring pass, which keeps no history
+        from oracle import oracle as O
+
+        h = [x.cpu().numpy() for x in t]
+        osc, _ = O.align_batch_arrays(h[0], h[1], h[2], h[3], h[4], h[5], 4, 6, 2, cigar=False)
+        assert np.array_equal(got, osc), np.nonzero(got != osc)[0][:10]
 
 
 def test_noalloc_takes_no_device_memory_and_refuses_oversized():
@@ -112,3 +120,20 @@ def test_noalloc_takes_no_device_memory_and_refuses_oversized():
     # invalid penalties are refused
     rc, _ = _call_noalloc(fn, Batch, Penalties, t, pen=(0, 6, 2))
     assert rc == TSU_EINVAL
+
+
+def test_noalloc_refuses_a_ring_beyond_the_array_before_any_pass():
+    """Long pairs with a deep ring (mismatch 1000, opening 0, extension 1:
+    1,005 ring slots) need an HBM ring of about 32 MB per pair, more than the
+    array has left beside the packed input: refused up front, no score
+    written."""
+    torch = pytest.importorskip("torch")
+    fn, Batch, Penalties = _noalloc_fn()
+    t = _device_batch(torch, 505, np.full(4, 4000), np.full(4, 0.05))
+    rc, out = _call_noalloc(fn, Batch, Penalties, t, pen=(1000, 0, 1))
+    assert rc == TSU_EOVERFLOW
+    assert int((out == -7).sum()) == 4
+    # the same pairs with the usual penalties fit
+    rc, out = _call_noalloc(fn, Batch, Penalties, t)
+    assert rc == TSU_OK
+    assert np.array_equal(out.cpu().numpy(), _reference_scores(t))

@@ -1,13 +1,12 @@
 // tsu_noalloc.cu -- tsu_align_scores_noalloc: scores for a batch that is
 // already on the device, computed without allocating any device memory.
 //
-// Why it exists: some callers cannot call cudaMalloc at all -- code running
-// inside a CUDA graph that is being captured (allocation calls are illegal
-// during capture), plug-ins that live under a host framework which owns every
-// device allocation through its own pool, and real-time services that must not
-// stall on the driver's allocator or fail on memory pressure in mid-request.
-// The context-based entry points (tsu_create / tsu_align_batch_device) grow a
-// workspace with cudaMalloc and so cannot serve them.
+// Why it exists: some callers cannot call cudaMalloc -- plug-ins that live
+// under a host framework which owns every device allocation through its own
+// pool, and services that must not stall on the driver's allocator or fail on
+// memory pressure in the middle of a request.  The context-based entry points
+// (tsu_create / tsu_align_batch_device) grow a workspace with cudaMalloc and
+// so cannot serve them.
 //
 // How: all scratch of the call lives in one fixed array compiled into this
 // library, g_noalloc_scratch (kNoAllocScratchBytes = 32 MiB).  Every GPU that
@@ -24,7 +23,8 @@
 // two calls whose work overlaps on the GPU (on different streams, or from
 // different host threads) race on it and corrupt each other's results; calls
 // on one device must be serialized.  Batches that need more scratch than the
-// array holds are refused with TSU_EOVERFLOW; nothing is truncated.
+// array holds are refused with TSU_EOVERFLOW before the first align pass;
+// nothing is truncated.
 #include <cuda_runtime.h>
 #include <cub/device/device_scan.cuh>
 
@@ -171,6 +171,15 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
   if (at > kNoAllocScratchBytes) return TSU_EOVERFLOW;  // batch beyond the fixed scratch
   unsigned char* ring_base = base + at;
   const size_t ring_room = kNoAllocScratchBytes - at;
+  int g = 1;
+  const tsu::Pen rp = tsu::reduce_penalties(pen->mismatch, pen->gap_opening, pen->gap_extension, -1, 0, &g);
+  if (rp.slots() > 4096) return TSU_EINVAL;
+  // Pairs the shared-memory ring hands back take a second pass on an HBM
+  // ring of the longest pair's width; refuse the batch now, before any score
+  // is written, if not even one such ring fits beside the packed input.
+  const tsu::PassGeom geo_global =
+      tsu::plan_geometry(rp, max_m, max_n, tsu::kModeGlobal, 1, 0.2, false, smem_optin);
+  if ((size_t)geo_global.ring_ints * sizeof(int32_t) > ring_room) return TSU_EOVERFLOW;
 
   // pack (same kernels as the context path)
   tsu::word_count_kernel<<<(int)std::min<int64_t>((2 * n + 255) / 256, 4096), 256, 0, st>>>(n, b->pattern_len,
@@ -189,9 +198,6 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
 
   // align passes: shared-memory ring first, then a global ring for the pairs
   // it hands back (score only: no history, no step table, no arena)
-  int g = 1;
-  const tsu::Pen rp = tsu::reduce_penalties(pen->mismatch, pen->gap_opening, pen->gap_extension, -1, 0, &g);
-  if (rp.slots() > 4096) return TSU_EINVAL;
   unsigned int* queue = reinterpret_cast<unsigned int*>(hdr + kHdrQueue);
   const int32_t* ord = nullptr;
   int64_t n_order = n;
@@ -206,7 +212,7 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
     int64_t warps = std::min<int64_t>((int64_t)sms * occ * wpb, n_order);
     if (geo.mode == tsu::kModeGlobal)
       warps = std::min<int64_t>(warps, (int64_t)(ring_room / ((size_t)geo.ring_ints * sizeof(int32_t))));
-    if (warps < 1) return TSU_EOVERFLOW;  // not even one global ring fits
+    if (warps < 1) return TSU_EINTERNAL;  // one global ring fits: checked before the first pass
     const int bw = warps >= wpb ? wpb : (int)warps;
     warps = warps / bw * bw;
     tsu::AlignArgs a{};
