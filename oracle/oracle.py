@@ -128,6 +128,8 @@ def lib():
         L.ora_align_batch2.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int] * 5 + [
             ctypes.c_void_p] * 4 + [ctypes.c_int]
         L.ora_gen_batch.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64] + [ctypes.c_void_p] * 8
+        L.ora_refk_batch.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int64] * 3 + [ctypes.c_int] * 6 + [
+            ctypes.c_void_p] * 4
         _lib = L
     return _lib
 
@@ -523,3 +525,33 @@ def gen_batch(seed: int, lengths: np.ndarray, rates: np.ndarray, first: int = 0)
     if rc != 0:
         raise RuntimeError(f"ora_gen_batch error {rc}")
     return pbuf, off, plen, tbuf, off.copy(), tlen
+
+
+def refk_batch(seed: int, first: int, num: int, length: int, rate: float, x=4, o=6, e=2, wf_length: int = 0,
+               step_cap: int = 32000):
+    """The CPU model of the reference's GPU kernel (ref_kernel_model.c) on the
+    pairs oracle/_ref/ref_harness generates for the same arguments, laid out
+    as the harness lays them out (pairs of `length` bytes back to back,
+    2 * length + 256 pad bytes before and after, 0x01 in the pattern buffer
+    and 0x02 in the text buffer).  Returns (scores int16, codes, steps,
+    max |k|) per pair; codes are 0 or ORA_REFK_* (-10 ring, -11 sequence
+    read, -12 step cap)."""
+    lengths = np.full(num, length, np.int32)
+    pb, po, pl, tb, to, tl = gen_batch(seed, lengths, np.full(num, rate), first=first)
+    if not (np.all(pl == length) and np.all(tl == length)):
+        raise ValueError("the reference kernel needs pairs of equal length")
+    pad = 2 * length + 256
+    P = np.full(pad + num * length + pad, 1, np.uint8)
+    T = np.full(pad + num * length + pad, 2, np.uint8)
+    P[pad:pad + num * length] = pb[:num * length]
+    T[pad:pad + num * length] = tb[:num * length]
+    wf = wf_length or 2 * (length + 3) + 2
+    sc = np.zeros(num, np.int16)
+    codes = np.zeros(num, np.int32)
+    steps = np.zeros(num, np.int32)
+    maxk = np.zeros(num, np.int32)
+    rc = lib().ora_refk_batch(P.ctypes.data + pad, T.ctypes.data + pad, pad, pad, num, length, x, o, e, wf, step_cap,
+                              sc.ctypes.data, codes.ctypes.data, steps.ctypes.data, maxk.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ora_refk_batch error {rc}")
+    return sc, codes, steps, maxk
