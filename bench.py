@@ -511,7 +511,7 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    step_ms, align_ms, launches, work_cells, work_steps = [], [], 0, 0, 0
+    step_ms, align_ms, launches, work_cells, work_steps, ext_bases = [], [], 0, 0, 0, 0
     t_wall = time.perf_counter()
     for _ in range(args.steps):
         nruns = dev_step()
@@ -519,7 +519,7 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
         step_ms.append(tm["total_ms"])
         align_ms.append(tm["align_ms"])
         launches += int(tm["kernel_launches"])
-        work_cells, work_steps = tm["cells"], tm["steps"]
+        work_cells, work_steps, ext_bases = tm["cells"], tm["steps"], tm["ext_bases"]
         pass_log = al.pass_log()
     barrier()
     wall_ms = (time.perf_counter() - t_wall) * 1e3 / args.steps
@@ -529,7 +529,6 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
                                        f"cuda:{local}")
     value = throughput(cells_all, ms) / 1e9
     pairs_s = throughput(pairs_all, ms)
-    cigar_ops = int(torch.sum(d_runs[:nruns].view(torch.int32) >> 4).item()) if want_cigar and nruns else 0
 
     # ---- plain form: one call per log2-length bucket, one warp per pair
     plain = None
@@ -616,7 +615,7 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
 
     # ---- roofline of the align passes ---------------------------------------
     a_ms = float(np.mean(align_ms))
-    roof = roofline(workload, n_pairs, plen, tlen, nruns if want_cigar else 0, work_cells, work_steps, cigar_ops,
+    roof = roofline(workload, n_pairs, plen, tlen, nruns if want_cigar else 0, work_cells, work_steps, ext_bases,
                     a_ms, clk, want_cigar, pass_log)
 
     cpu = cpu_baseline(pbuf, poff, plen, tbuf, toff, tlen) if (with_cpu and rank == 0) else None
@@ -651,13 +650,30 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
     return out
 
 
-def roofline(workload, n_pairs, plen, tlen, nruns, work_cells, work_steps, cigar_ops, a_ms, clk, want_cigar,
+# Integer-issue model of the align kernel (see the kernel roofline section of
+# the design notes): the fewest thread instructions the algorithm as written
+# needs per (score, diagonal) cell (five ring loads, the I/D/M maxima and
+# source bits, the bounds test, one 16-base extend window, the end test, the
+# trimming bounds, three ring stores with their int16 clamps, the history
+# word, the loop), per further 16-base extend window, and the warp
+# instructions of one score step of a pair (source limits, envelope, seven
+# warp reductions, limit stores, step table) and of one CIGAR run of the
+# backtrace walk (one lane).
+C_CELL, C_EXT, C_STEP, C_RUN = 76, 16, 70, 24
+
+
+def roofline(workload, n_pairs, plen, tlen, nruns, work_cells, work_steps, ext_bases, a_ms, clk, want_cigar,
              pass_log):
     """Roofline of the align passes (the dominant kernels: 95-99.9 % of
-    device time).  HBM: algorithmic bytes (packed input, scores, CIGAR runs,
-    one 4-byte backtrace word per wavefront cell) per second against the
-    measured copy bandwidth, with the DRAM traffic of an ncu capture of the
-    same kernel scaled by pairs."""
+    device time).  Binding resource: integer instruction issue --
+    algorithmic warp instructions (the model above times the counted cells,
+    extension bases, steps and runs) per second against 148 SMs x 4
+    schedulers x the sampled SM clock.  Secondary: HBM, algorithmic bytes
+    (packed input, scores, CIGAR runs, one 4-byte backtrace word per
+    wavefront cell) per second against the measured copy bandwidth, with the
+    DRAM traffic of an ncu capture of the same kernel scaled by pairs."""
+    import torch
+
     peak, peak_kind = measured_peaks()
     words = float(np.sum((plen.astype(np.int64) + 31) // 32 + 1) + np.sum((tlen.astype(np.int64) + 31) // 32 + 1))
     packed_in = words * 8
@@ -668,14 +684,23 @@ def roofline(workload, n_pairs, plen, tlen, nruns, work_cells, work_steps, cigar
     model = "_" + METRIC_NAME if METRIC_NAME else ("_dual" if len(PEN) == 5 else "")
     prof = load_traffic(f"align_{workload}{model}") if want_cigar else None
     traffic = prof["dram_bytes"] * n_pairs / prof["pairs"] if prof else None
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_kind": peak_kind, "kernel": "align_kernel<cigar>" if want_cigar else
-            "align_kernel<score>", "kernel_ms": a_ms,
-            "algorithmic_bytes_per_launch": algo, "cells": work_cells, "score_steps": work_steps,
-            "cigar_ops": cigar_ops, "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log}
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    warp_inst = (C_CELL * work_cells + C_EXT * ext_bases / 16.0) / 32.0 + C_STEP * work_steps + C_RUN * nruns
+    issue_peak = sms * 4 * mhz * 1e6  # warp instructions per second
+    inst_rate = warp_inst / (a_ms / 1e3)
+    roof = {"bound": "int_issue", "achieved": inst_rate / 1e9, "peak": issue_peak / 1e9, "unit": "Gwarp-inst/s",
+            "frac": inst_rate / issue_peak, "traffic": traffic, "peak_kind": f"{sms} SMs x 4 schedulers x {mhz:.0f} MHz "
+            "(sampled SM clock under load)", "kernel": "align_kernel<cigar>" if want_cigar else "align_kernel<score>",
+            "kernel_ms": a_ms, "algorithmic_warp_instructions": warp_inst,
+            "model": {"c_cell": C_CELL, "c_ext_per_16_bases": C_EXT, "c_step": C_STEP, "c_run": C_RUN},
+            "cells": work_cells, "score_steps": work_steps, "extension_bases": ext_bases, "cigar_runs": nruns,
+            "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log,
+            "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_kind": peak_kind, "algorithmic_bytes_per_launch": algo, "traffic": traffic}}
     if prof:
-        roof["issue_active_frac"] = prof.get("issue_active_frac")
-        roof["alu_pipe_frac"] = prof.get("alu_pipe_frac")
+        roof["ncu_issue_active_frac"] = prof.get("issue_active_frac")
+        roof["ncu_alu_pipe_frac"] = prof.get("alu_pipe_frac")
         roof["traffic_source"] = prof.get("source")
     return roof
 

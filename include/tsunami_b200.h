@@ -130,6 +130,7 @@ typedef struct {
   int64_t h2d_bytes, d2h_bytes;
   int64_t cells; /* wavefront (score, diagonal) cells computed, all passes */
   int64_t steps; /* non-null score steps computed, all passes              */
+  int64_t ext_bases; /* bases matched by extend steps, all passes         */
 } tsu_timing;
 
 /* ---- context ------------------------------------------------------------

@@ -90,6 +90,9 @@ inline int reduce_max(int v) {
     return (uint64_t)std::max((int64_t)a, (int64_t)b);
   });
 }
+inline unsigned reduce_add(unsigned v) {
+  return (unsigned)all_reduce((uint64_t)v, [](uint64_t a, uint64_t b) { return (uint64_t)(uint32_t)(a + b); });
+}
 inline unsigned ballot(bool p) {
   const uint64_t* s = exchange(p ? 1u : 0u);
   unsigned r = 0;
@@ -151,6 +154,7 @@ void launch(int blocks, int threads, size_t smem_bytes, F body) {
 #define __shfl_sync(mask, v, src) emu::shfl((v), (src))
 #define __reduce_min_sync(mask, v) emu::reduce_min(v)
 #define __reduce_max_sync(mask, v) emu::reduce_max(v)
+#define __reduce_add_sync(mask, v) emu::reduce_add(v)
 #define __any_sync(mask, p) (emu::ballot(p) != 0u)
 #define __ballot_sync(mask, p) emu::ballot(p)
 

@@ -122,18 +122,27 @@ def test_noalloc_takes_no_device_memory_and_refuses_oversized():
     assert rc == TSU_EINVAL
 
 
-def test_noalloc_refuses_a_ring_beyond_the_array_before_any_pass():
-    """Long pairs with a deep ring (mismatch 1000, opening 0, extension 1:
-    1,005 ring slots) need an HBM ring of about 32 MB per pair, more than the
-    array has left beside the packed input: refused up front, no score
-    written."""
+def test_noalloc_deep_rings_refused_up_front_or_aligned_in_hbm():
+    """A deep ring (mismatch 1000, opening 0, extension 1: 1,005 ring slots)
+    does not fit one warp's shared memory, so every pair takes the HBM ring.
+    For 5 kbp pairs that ring is 1,005 x 10,003 x 4 B = 40 MB, more than the
+    32 MiB array: refused up front, no score written.  For 4 kbp pairs it is
+    32.2 MB, which fits: the scores equal the context path's and the
+    oracle's."""
     torch = pytest.importorskip("torch")
     fn, Batch, Penalties = _noalloc_fn()
-    t = _device_batch(torch, 505, np.full(4, 4000), np.full(4, 0.05))
-    rc, out = _call_noalloc(fn, Batch, Penalties, t, pen=(1000, 0, 1))
+    pen = (1000, 0, 1)
+    t = _device_batch(torch, 505, np.full(4, 5000), np.full(4, 0.05))
+    rc, out = _call_noalloc(fn, Batch, Penalties, t, pen=pen)
     assert rc == TSU_EOVERFLOW
     assert int((out == -7).sum()) == 4
-    # the same pairs with the usual penalties fit
-    rc, out = _call_noalloc(fn, Batch, Penalties, t)
+    t = _device_batch(torch, 506, np.full(4, 4000), np.full(4, 0.05))
+    rc, out = _call_noalloc(fn, Batch, Penalties, t, pen=pen)
     assert rc == TSU_OK
-    assert np.array_equal(out.cpu().numpy(), _reference_scores(t))
+    got = out.cpu().numpy()
+    assert np.array_equal(got, _reference_scores(t, pen))
+    from oracle import oracle as O
+
+    h = [x.cpu().numpy() for x in t]
+    osc, _ = O.align_batch_arrays(h[0], h[1], h[2], h[3], h[4], h[5], *pen, cigar=False)
+    assert np.array_equal(got, osc)

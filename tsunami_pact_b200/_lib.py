@@ -56,7 +56,7 @@ class Timing(ctypes.Structure):
     _fields_ = [("h2d_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("align_ms", ctypes.c_double),
                 ("compact_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("kernel_launches", c_i64), ("retried_pairs", c_i64), ("h2d_bytes", c_i64),
-                ("d2h_bytes", c_i64), ("cells", c_i64), ("steps", c_i64)]
+                ("d2h_bytes", c_i64), ("cells", c_i64), ("steps", c_i64), ("ext_bases", c_i64)]
 
 
 class ServerConfig(ctypes.Structure):

@@ -76,6 +76,15 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
   constexpr bool kDual = (kModel & 7) == kModelDual;
   constexpr bool kLin = (kModel & 7) == kModelLinear;
   constexpr bool kLowMem = kCigar && (kModel & kLowMemFlag) != 0;
+  // Groups of 2 to 16 warps (wide wavefronts) read the sources of a warp's
+  // block of diagonals without range tests where all of them lie inside
+  // their trimmed ranges, and extend and track the trimmed ends with selects
+  // instead of divergent branches (measured: 10 kbp at 15 %, 16 warps, -5 %).
+  // The one-warp kernel runs at 72 registers with its ALU pipe the busiest,
+  // and the 32-warp kernels at 64 registers: there the selects and the extra
+  // registers cost more than the branches (+8 % at 1 kbp), so they keep the
+  // branches.
+  constexpr bool kWide = GW > 1 && GW < 32;
   static_assert(!(kModel & kLowMemFlag) || kCigar, "low-memory: CIGAR kernels");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
   using S = typename std::conditional<kMode == kModeShared, SharedSeq, GlobalSeq>::type;
@@ -157,6 +166,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
     int64_t lm_pos = 0;
     int64_t hbase = 0;
     unsigned long long n_cells = 0, n_steps = 0;
+    uint32_t n_ext = 0;  // bases matched by this thread's extend steps
 
     if (st == kPairOk) {
       const uint32_t* pws;
@@ -177,9 +187,15 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
         s_alo[i] = 0;
       }
       group_sync<GW>(gid);
+      // int16 ring: values above n + 1 are stored as n + 1 and values below
+      // kNull16 as kNull16.  A stored value in (kNull16, 0) can only come from
+      // an I chain of +1 per step that moves one diagonal per step inside the
+      // component's trimmed range, at most ring_w (< 16,384) diagonals wide,
+      // so it stays negative: every clamped value keeps its validity and its
+      // order against any valid offset.
       auto store = [&](int idx, int32_t v) {
         if constexpr (kMode == kModeShared)
-          ring[idx] = (RT)(v < 0 ? (int32_t)kNull16 : (v > n + 1 ? n + 1 : v));
+          ring[idx] = (RT)max(min(v, n + 1), (int32_t)kNull16);
         else
           ring[idx] = v;
       };
@@ -360,18 +376,47 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           int fm = INT_MAX, lm = INT_MIN, fi = INT_MAX, li = INT_MIN, fd = INT_MAX, ld = INT_MIN;
           int fi2 = INT_MAX, li2 = INT_MIN, fd2 = INT_MAX, ld2 = INT_MIN;
           int fk = INT_MAX;  // lowest ending diagonal of this thread
+          // Where every one-piece source is present, the diagonals kA..kB
+          // read all of them inside their trimmed ranges; a warp whose block
+          // of 32 diagonals (k - lane .. + 31, the same for all its lanes)
+          // lies there reads without range tests.
+          int kA = INT_MAX, kB = INT_MIN;
+          if (kWide && !kDual && c_mm && c_mo && (kLin || (c_ie && c_de))) {
+            kA = max(lo_mm, lo_mo + 1);
+            kB = min(lo_mm + c_mm - 1, lo_mo + c_mo - 2);
+            if constexpr (!kLin) {
+              kA = max(kA, max(lo_ie + 1, lo_de - 1));
+              kB = min(kB, min(lo_ie + c_ie, lo_de + c_de - 2));
+            }
+            kB -= 31;  // block start bound
+          }
           for (int k = lo + gt; k <= hi; k += GT) {
+            int32_t ins_o, ins_e = kNull, del_o, del_e = kNull, mis;
+            const int kb = k - lane;
+            if (kWide && kb >= kA && kb <= kB) {
+              ins_o = ring[b_mo - 1 - lo_mo + k];
+              del_o = ring[b_mo + 1 - lo_mo + k];
+              mis = (int32_t)ring[b_mm - lo_mm + k] + 1;
+              if constexpr (!kLin) {
+                ins_e = ring[b_ie - 1 - lo_ie + k];
+                del_e = ring[b_de + 1 - lo_de + k];
+              }
+            } else {
+              int j;
+              j = k - 1 - lo_mo;
+              ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+              j = k + 1 - lo_mo;
+              del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+              j = k - lo_mm;
+              mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
+              if constexpr (!kLin) {
+                j = k - 1 - lo_ie;
+                ins_e = ((unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
+                j = k + 1 - lo_de;
+                del_e = ((unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
+              }
+            }
             int j;
-            j = k - 1 - lo_mo;
-            const int32_t ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
-            j = k - 1 - lo_ie;
-            const int32_t ins_e = (!kLin && (unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
-            j = k + 1 - lo_mo;
-            const int32_t del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
-            j = k + 1 - lo_de;
-            const int32_t del_e = (!kLin && (unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
-            j = k - lo_mm;
-            const int32_t mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
             const int32_t ins = max(ins_o, ins_e) + 1;
             const int32_t del = max(del_o, del_e);
             int32_t ins2 = kNull, del2 = kNull;
@@ -412,10 +457,37 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
               }
             }
             int32_t om = kNull;
-            if (in_bounds(p, k, m, n)) {
+            if constexpr (kWide) {
+              // Extend M (wfa_gpu.cu:257-287) without a divergent region
+              // around it: every lane compares its first 16-base window (an
+              // invalid cell at position 0, a valid one at v <= m and h <= n:
+              // both inside the staged words and their padding word), and
+              // only lanes whose window matches entirely continue in a loop.
+              const bool vm = in_bounds_sel(p, k, m, n);
+              const int vv = vm ? p - k : 0, hh = vm ? p : 0;
+              const int rem = vm ? min(m - vv, n - p) : 0;
+              int lx;
+              if (kMode == kModeGlobal && bytemode) {
+                lx = lcp8(pb, m, vv, tb, n, hh, rem);
+              } else {
+                const uint32_t d0 = win16(P, vv) ^ win16(T, hh);
+                lx = d0 ? (__ffs(d0) - 1) >> 1 : 16;
+                if (!d0 && rem > 16) lx = 16 + lcp16(P, vv + 16, T, hh + 16, rem - 16);
+                lx = min(lx, rem);
+              }
+              om = vm ? p + lx : kNull;
+              n_ext += (uint32_t)lx;
+              fm = vm ? min(fm, k) : fm;
+              lm = vm ? k : lm;
+              bool ends = vm & (om >= n) & (k <= k_hi);
+              if (free_te) ends |= vm & ((om - k) >= m) & (om >= n_te);
+              fk = ends ? min(fk, k) : fk;
+            } else if (in_bounds(p, k, m, n)) {
               const int vv = p - k;
               const int rem = min(m - vv, n - p);
-              om = p + ((kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem));
+              const int lx = (kMode == kModeGlobal && bytemode) ? lcp8(pb, m, vv, tb, n, p, rem) : lcp16(P, vv, T, p, rem);
+              om = p + lx;
+              n_ext += (uint32_t)lx;
               fm = min(fm, k);
               lm = k;
               bool ends = (om >= n) & (k <= k_hi);
@@ -425,20 +497,38 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             store(w_m + k, om);
             if (i_present) {
               store(w_i + k, ins);
-              if (in_bounds(ins, k, m, n)) { fi = min(fi, k); li = k; }
+              if constexpr (kWide) {
+                const bool vi = in_bounds_sel(ins, k, m, n);
+                fi = vi ? min(fi, k) : fi;
+                li = vi ? k : li;
+              } else if (in_bounds(ins, k, m, n)) {
+                fi = min(fi, k);
+                li = k;
+              }
             }
             if (d_present) {
               store(w_d + k, del);
-              if (in_bounds(del, k, m, n)) { fd = min(fd, k); ld = k; }
+              if constexpr (kWide) {
+                const bool vd = in_bounds_sel(del, k, m, n);
+                fd = vd ? min(fd, k) : fd;
+                ld = vd ? k : ld;
+              } else if (in_bounds(del, k, m, n)) {
+                fd = min(fd, k);
+                ld = k;
+              }
             }
             if constexpr (kDual) {
               if (i2_present) {
                 store(w_i2 + k, ins2);
-                if (in_bounds(ins2, k, m, n)) { fi2 = min(fi2, k); li2 = k; }
+                const bool vi2 = in_bounds_sel(ins2, k, m, n);
+                fi2 = vi2 ? min(fi2, k) : fi2;
+                li2 = vi2 ? k : li2;
               }
               if (d2_present) {
                 store(w_d2 + k, del2);
-                if (in_bounds(del2, k, m, n)) { fd2 = min(fd2, k); ld2 = k; }
+                const bool vd2 = in_bounds_sel(del2, k, m, n);
+                fd2 = vd2 ? min(fd2, k) : fd2;
+                ld2 = vd2 ? k : ld2;
               }
             }
             if constexpr (kH) hrow[k] = ((uint32_t)p << (kDual ? 8 : 4)) | bits;
@@ -661,6 +751,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
           a.cig_len[pair] = len;
         }
       }
+    }
+    if (a.work) {
+      const unsigned we = __reduce_add_sync(FULL, n_ext);
+      if (lane == 0 && we) atomicAdd(a.work + 2, (unsigned long long)we);
     }
     if (gt == 0) {
       a.status[pair] = st;

@@ -153,7 +153,7 @@ struct AlignArgs {
   unsigned int* queue;   // work-queue head
   int32_t* retry;        // [n] pairs to re-run with more scratch / arena
   unsigned int* retry_count;
-  unsigned long long* work;  // [2]: wavefront cells computed, score steps
+  unsigned long long* work;  // [3]: wavefront cells computed, score steps, bases matched by extend steps
   // free ends (all 0: end-to-end): starts (v, 0), v <= ef_pb, and (0, h),
   // h <= ef_tb, cost nothing, and so do ends (m, h), h >= n - ef_te, and
   // (v, n), v >= m - ef_pe
@@ -191,6 +191,10 @@ __host__ __device__ inline int group_smem_bytes(const Pen& p, int ring_w, int mo
 
 __device__ __forceinline__ bool in_bounds(int32_t off, int k, int m, int n) {
   return (uint32_t)off <= (uint32_t)n && (uint32_t)(off - k) <= (uint32_t)m;
+}
+// The same test without a short-circuit, for select-based code.
+__device__ __forceinline__ bool in_bounds_sel(int32_t off, int k, int m, int n) {
+  return ((uint32_t)off <= (uint32_t)n) & ((uint32_t)(off - k) <= (uint32_t)m);
 }
 
 // Reduced-unit upper bound of the optimal score: all mismatches plus the

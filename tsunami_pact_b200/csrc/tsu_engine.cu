@@ -536,7 +536,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   if ((rc = grow(ctx, ctx->b_clen, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_retry, sizeof(int32_t) * n))) return rc;
   if ((rc = grow(ctx, ctx->b_order, sizeof(int32_t) * n))) return rc;
-  // counters: +16 arena cursor, +24 work (cells, steps), +64 + 8b queue head
+  // counters: +16 arena cursor, +24 work (cells, steps, extension bases), +64 + 8b queue head
   // and retry count of band slot b
   constexpr size_t kCounterBytes = 64 + 8 * tsu::kBands;
   if ((rc = grow(ctx, ctx->b_counters, kCounterBytes))) return rc;
@@ -811,11 +811,12 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
   }
   CU(cudaEventRecord(ctx->ev[5], st));
   if (laddered) {
-    CU(cudaMemcpyAsync(h_cnt + 24, d_work, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h_cnt + 24, d_work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CU(wait_stream(ctx, st));
   }
   ctx->timing.cells = (int64_t)reinterpret_cast<const unsigned long long*>(h_cnt + 24)[0];
   ctx->timing.steps = (int64_t)reinterpret_cast<const unsigned long long*>(h_cnt + 24)[1];
+  ctx->timing.ext_bases = (int64_t)reinterpret_cast<const unsigned long long*>(h_cnt + 24)[2];
 
   // ---- CIGAR compaction
   if (want_cigar) {
@@ -1288,7 +1289,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   ctx->timing.h2d_bytes = h2d;
   int64_t needed = 0, d2h = 0;
   double pack_ms = 0, align_ms = 0, compact_ms = 0;
-  int64_t launches = 0, retried = 0, cells = 0, steps = 0;
+  int64_t launches = 0, retried = 0, cells = 0, steps = 0, ext_bases = 0;
   std::vector<int64_t> run_base((size_t)K + 1, 0);
   for (int c = 0; c < K; ++c) {
     const int64_t c0 = cs[(size_t)c], nc = cbi[(size_t)c].n;
@@ -1321,6 +1322,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
     retried += ctx->timing.retried_pairs;
     cells += ctx->timing.cells;
     steps += ctx->timing.steps;
+    ext_bases += ctx->timing.ext_bases;
     CU(cudaEventRecord(ev_done[(size_t)c], st));
     CU(cudaStreamWaitEvent(ctx->d2h_stream, ev_done[(size_t)c], 0));
     if (nc) {
@@ -1355,6 +1357,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   ctx->timing.retried_pairs = retried;
   ctx->timing.cells = cells;
   ctx->timing.steps = steps;
+  ctx->timing.ext_bases = ext_bases;
   ctx->timing.total_ms = ev_ms(t_begin, t_end);
   ctx->timing.h2d_ms = 0;  // overlapped with the alignment
   ctx->timing.d2h_ms = 0;

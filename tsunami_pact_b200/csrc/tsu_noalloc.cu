@@ -205,10 +205,16 @@ extern "C" int tsu_align_scores_noalloc(const tsu_penalties* pen, const tsu_batc
     const int wpb = 4;
     const tsu::PassGeom geo = tsu::plan_geometry(rp, max_m, max_n, pass == 0 ? tsu::kModeShared : tsu::kModeGlobal,
                                                  1, 0.2, false, smem_optin);
+    // penalties with very deep rings: the shared-memory ring of one warp
+    // does not fit a block, and every pair takes the global pass
+    if (pass == 0 && geo.mode == tsu::kModeShared && (size_t)wpb * geo.group_smem > (size_t)smem_optin) continue;
     int occ = 0;
     NA_CU(geo.mode == tsu::kModeShared ? occupancy<tsu::kModeShared>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ)
                                        : occupancy<tsu::kModeGlobal>(32 * wpb, (size_t)wpb * geo.group_smem, smem_optin, &occ));
-    if (occ < 1) return TSU_EDEVICE;
+    if (occ < 1) {
+      if (pass == 0) continue;
+      return TSU_EDEVICE;
+    }
     int64_t warps = std::min<int64_t>((int64_t)sms * occ * wpb, n_order);
     if (geo.mode == tsu::kModeGlobal)
       warps = std::min<int64_t>(warps, (int64_t)(ring_room / ((size_t)geo.ring_ints * sizeof(int32_t))));

@@ -42,6 +42,9 @@ constexpr int kSharedW1 = 384;         // shared-mode ring width for one warp pe
 constexpr int kSharedSeqWords1 = 544;  // staging area for one warp per pair (uint32 words)
 constexpr int kSharedSeqWordsN = 4096; // staging area for a group of warps
 constexpr int kSharedMaxLen = 32000;   // int16 ring limit
+// widest int16 ring: a negative (invalid) I value grows by one per diagonal
+// of the ring's width and must stay negative (the kernel's store clamp)
+constexpr int kSharedMaxW = 16368;
 constexpr int kSmemPerSM = 228 * 1024; // B200 shared memory per SM (bytes)
 
 // Reduced-unit score expected at edit rate `hint` for a pair of length L.
@@ -63,7 +66,19 @@ inline int shared_ring_width(const Pen& pen, int gw, int seq_cap, int smem_optin
   const int gpc = cta_threads_for(gw) / (32 * gw);
   const int per_group = per_cta / gpc;
   const int fixed = group_smem_bytes(pen, 0, kModeShared, seq_cap, gw) + 16;
-  const int w = (per_group - fixed) / (2 * ns);
+  const int w = std::min((per_group - fixed) / (2 * ns), kSharedMaxW);
+  return std::max(0, w & ~15);
+}
+
+// Shared ring width of a group of gw warps.  One warp per pair has a fixed
+// width (kSharedW1), unless penalties with a very deep ring leave four such
+// groups unable to fit one block; then the width one block can hold (below
+// 64 diagonals the pass takes the global ring).
+inline int shared_cap(const Pen& pen, int gw, int seq_cap, int smem_optin) {
+  if (gw != 1) return shared_ring_width(pen, gw, seq_cap, smem_optin);
+  const int gpc = cta_threads_for(1) / 32;
+  if (gpc * group_smem_bytes(pen, kSharedW1, kModeShared, seq_cap, 1) <= smem_optin) return kSharedW1;
+  const int w = (smem_optin / gpc - group_smem_bytes(pen, 0, kModeShared, seq_cap, 1) - 16) / (2 * pen.slots());
   return std::max(0, w & ~15);
 }
 
@@ -88,7 +103,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   if (p.mode == kModeShared) {
     const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
     p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
-    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(pen, gw, p.seq_cap, smem_optin);
+    const int cap = shared_cap(pen, gw, p.seq_cap, smem_optin);
     p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, cap) + 15) & ~15);
     if (cap < 64) p.mode = kModeGlobal;
   }
@@ -165,8 +180,8 @@ inline PassChoice fit_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_
   for (int gw : kGW) {
     if (gw < pc.gw) continue;
     if (seqw > (gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN)) continue;
-    const int cap = gw == 1 ? kSharedW1 : shared_ring_width(pen, gw, (int)seqw, smem_optin);
-    if (cap >= w) return {kModeShared, gw};
+    const int cap = shared_cap(pen, gw, (int)seqw, smem_optin);
+    if (cap >= w && cap >= 64) return {kModeShared, gw};
   }
   // wavefronts wider than 16,384 diagonals: 32 warps (one 1024-thread block)
   return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
