@@ -136,7 +136,7 @@ struct AlignArgs {
   Pen pen;               // reduced penalties and ring depths
   int g;                 // score unit
   int ring_w;            // diagonals per ring slot
-  int seq_cap;           // shared-memory sequence words (uint32) per warp
+  int seq_cap;           // shared-memory sequence words (uint32) per group (global mode: 0 = not staged)
   int32_t* ring_global;  // per-warp rings (global mode)
   int64_t ring_stride;   // int32 per warp in ring_global
   uint32_t* hist;        // per-warp backtrace words
@@ -179,15 +179,24 @@ __host__ __device__ inline int partial_words(const Pen& p) { return p.dual() ? 1
 // Shared memory per group of gw warps, in bytes: slot limits (lo, hi, alo
 // per slot), warp partials [2][gw][partial_words] (gw > 1), 4 broadcast
 // words, then in shared mode an int16 ring of slots * ring_w and seq_cap
-// sequence words.
+// sequence words; in global mode with seq_cap > 0, at the next 16-byte
+// boundary, the staging mbarrier (16 bytes) and seq_cap sequence words.
 __host__ __device__ inline int group_smem_bytes(const Pen& p, int ring_w, int mode, int seq_cap, int gw) {
   const int ns = p.slots();
   int b = 3 * ns * 4 + (gw > 1 ? 2 * partial_words(p) * gw * 4 : 0) + 16;
   if (mode == kModeShared) {
     b += ((ns * ring_w * 2 + 15) & ~15) + seq_cap * 4;
+  } else if (seq_cap > 0) {
+    b = ((b + 15) & ~15) + 16 + seq_cap * 4;
   }
   return (b + 15) & ~15;
 }
+
+// Packed 64-bit words allocated per sequence of len bases: ceil(len / 32)
+// data words and a zero padding word (read by the unaligned window loads),
+// rounded up to an even count so that every sequence starts on a 16-byte
+// boundary (what a bulk copy needs).
+__host__ __device__ __forceinline__ int64_t packed_words(int64_t len) { return ((len + 31) / 32 + 2) & ~(int64_t)1; }
 
 __device__ __forceinline__ bool in_bounds(int32_t off, int k, int m, int n) {
   return (uint32_t)off <= (uint32_t)n && (uint32_t)(off - k) <= (uint32_t)m;

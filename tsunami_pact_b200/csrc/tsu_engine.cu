@@ -872,7 +872,7 @@ int check_batch_host(tsu_ctx* ctx, const tsu_batch* b, BatchInfo* bi, int64_t* p
     te = std::max(te, b->text_off[i] + n);
     mm = std::max(mm, m);
     mn = std::max(mn, n);
-    words += (m + 31) / 32 + 1 + (n + 31) / 32 + 1;
+    words += tsu::packed_words(m) + tsu::packed_words(n);
   }
   bi->n = b->num_pairs;
   bi->max_m = mm;
@@ -930,7 +930,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
     for (int64_t i = 0; i < nc; ++i) {
       ci.max_m = std::max(ci.max_m, pl[i]);
       ci.max_n = std::max(ci.max_n, tl[i]);
-      ci.total_words += (pl[i] + 31) / 32 + 1 + (tl[i] + 31) / 32 + 1;
+      ci.total_words += tsu::packed_words(pl[i]) + tsu::packed_words(tl[i]);
       len_sum += (int64_t)pl[i] + tl[i];
     }
     size_t f = 2 * r(16 * (size_t)nc) + r(8 * (size_t)ci.total_words) + r(2 * (size_t)nc) + r(8 * (size_t)nc) +
@@ -1272,7 +1272,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
       t1 = std::max(t1, b->text_off[i] + t);
       ci.max_m = std::max(ci.max_m, m);
       ci.max_n = std::max(ci.max_n, t);
-      ci.total_words += (m + 31) / 32 + 1 + (t + 31) / 32 + 1;
+      ci.total_words += tsu::packed_words(m) + tsu::packed_words(t);
     }
     if (p1 > p0) {
       CU(cudaMemcpyAsync(P<char>(ctx->b_pat) + p0, b->pattern + p0, (size_t)(p1 - p0), cudaMemcpyHostToDevice,
@@ -1415,7 +1415,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
         return set_err(ctx, TSU_EINVAL, "pair %lld: bad length", (long long)i);
       bi.max_m = std::max(bi.max_m, pl[(size_t)i]);
       bi.max_n = std::max(bi.max_n, tl[(size_t)i]);
-      bi.total_words += (pl[(size_t)i] + 31) / 32 + 1 + (tl[(size_t)i] + 31) / 32 + 1;
+      bi.total_words += tsu::packed_words(pl[(size_t)i]) + tsu::packed_words(tl[(size_t)i]);
     }
   }
   CU(cudaEventRecord(ctx->ev[0], st));

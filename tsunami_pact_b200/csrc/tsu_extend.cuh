@@ -22,6 +22,13 @@ struct GlobalSeq {
   const uint32_t* __restrict__ p;
   __device__ __forceinline__ uint32_t operator[](int i) const { return __ldg(p + i); }
 };
+// Global-ring groups: the pair's words staged in shared memory, or (pairs
+// too long to stage) the packed words in global memory, through one generic
+// pointer.
+struct AnySeq {
+  const uint32_t* p;
+  __device__ __forceinline__ uint32_t operator[](int i) const { return p[i]; }
+};
 
 template <class S>
 __device__ __forceinline__ uint32_t win16(const S& w, int pos) {

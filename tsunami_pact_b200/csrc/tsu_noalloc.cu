@@ -81,7 +81,7 @@ __global__ void noalloc_stats_kernel(int64_t n, const int32_t* __restrict__ plen
     }
     mm = max(mm, (unsigned long long)m);
     mn = max(mn, (unsigned long long)t);
-    words += (unsigned long long)((m + 31) / 32 + 1) + (unsigned long long)((t + 31) / 32 + 1);
+    words += (unsigned long long)(tsu::packed_words(m) + tsu::packed_words(t));
   }
   atomicMax(hdr + kHdrMaxM, mm);
   atomicMax(hdr + kHdrMaxN, mn);

@@ -46,17 +46,18 @@ static __global__ void pack_kernel(SeqView sv, PackView pk) {
     }
     if (lane == 0) {
       dst[nw] = 0;  // padding word read by the unaligned window loads
+      if (!(nw & 1)) dst[nw + 1] = 0;  // the word that makes the count even
       pk.nonacgt[j] = bad ? 1 : 0;
     }
   }
 }
 
-// words per sequence: ceil(len/32) data words + 1 padding word
+// words per sequence: packed_words (data words, padding, even count)
 static __global__ void word_count_kernel(int64_t n, const int32_t* __restrict__ pat_len, const int32_t* __restrict__ txt_len,
                                   int64_t* __restrict__ words) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += (int64_t)gridDim.x * blockDim.x) {
     const int len = j < n ? pat_len[j] : txt_len[j - n];
-    words[j] = ((int64_t)len + 31) / 32 + 1;
+    words[j] = packed_words(len);
   }
 }
 

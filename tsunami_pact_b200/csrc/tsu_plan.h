@@ -101,7 +101,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   p.groups_per_cta = p.cta_threads / (32 * gw);
   p.mode = (mode == kModeShared && maxlen <= kSharedMaxLen) ? kModeShared : kModeGlobal;
   if (p.mode == kModeShared) {
-    const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
+    const int64_t seqw = 2 * packed_words(max_m) + 2 * packed_words(max_n);
     p.seq_cap = (int)std::min<int64_t>(seqw, gw == 1 ? kSharedSeqWords1 : kSharedSeqWordsN);
     const int cap = shared_cap(pen, gw, p.seq_cap, smem_optin);
     p.ring_w = (int)std::max<int64_t>(16, (std::min<int64_t>(full_w, cap) + 15) & ~15);
@@ -109,7 +109,14 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   }
   if (p.mode == kModeGlobal) {
     p.ring_w = (int)full_w;
-    p.seq_cap = 0;
+    // the pair's packed words staged in shared memory by bulk copies when
+    // they fit beside the group's limits at the block count the kernel is
+    // compiled for (0: read from global memory; always for 32-warp groups)
+    const int64_t seqw = 2 * packed_words(max_m) + 2 * packed_words(max_n);
+    const int per_cta = std::min(smem_optin, kSmemPerSM / min_blocks_for(kModeGlobal, gw) - 1024);
+    const int gpc = cta_threads_for(gw) / (32 * gw);
+    const int64_t room = per_cta / gpc - group_smem_bytes(pen, 0, kModeGlobal, 0, gw) - 48;
+    p.seq_cap = (gw < 32 && seqw * 4 <= room) ? (int)seqw : 0;
   }
   p.min_blocks = min_blocks_for(p.mode, gw);
   p.group_smem = group_smem_bytes(pen, p.ring_w, p.mode, p.seq_cap, gw);
@@ -151,7 +158,7 @@ inline PassChoice next_pass(PassChoice prev, const Pen& pen, int32_t max_m, int3
   const int64_t need_w = (int64_t)max_m + max_n + 3;
   if (prev.mode == kModeShared && std::max(max_m, max_n) <= kSharedMaxLen) {
     const int64_t seqw =
-        std::min<int64_t>(2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1), kSharedSeqWordsN);
+        std::min<int64_t>(2 * packed_words(max_m) + 2 * packed_words(max_n), kSharedSeqWordsN);
     static const int kGW[] = {2, 4, 8, 16};
     for (int gw : kGW) {
       if (gw <= prev.gw) continue;
@@ -175,7 +182,7 @@ inline PassChoice fit_start(PassChoice pc, const Pen& pen, int32_t max_m, int32_
       std::min<int64_t>((int64_t)max_m + max_n + 3, 2 * hint_score(pen, maxlen, hint) / pen.min_ge() + 3);
   if (pc.mode != kModeShared) return {kModeGlobal, w > 16384 ? 32 : pc.gw};
   if (maxlen > kSharedMaxLen) return {kModeGlobal, w > 16384 ? 32 : std::max(8, pc.gw)};
-  const int64_t seqw = 2 * ((max_m + 31) / 32 + 1) + 2 * ((max_n + 31) / 32 + 1);
+  const int64_t seqw = 2 * packed_words(max_m) + 2 * packed_words(max_n);
   static const int kGW[] = {1, 2, 4, 8, 16};
   for (int gw : kGW) {
     if (gw < pc.gw) continue;
