@@ -180,7 +180,7 @@ __host__ __device__ inline int partial_words(const Pen& p) { return p.dual() ? 1
 // per slot), warp partials [2][gw][partial_words] (gw > 1), 4 broadcast
 // words, then in shared mode an int16 ring of slots * ring_w and seq_cap
 // sequence words; in global mode with seq_cap > 0, at the next 16-byte
-// boundary, the staging mbarrier (16 bytes) and seq_cap sequence words.
+// boundary, 16 reserved bytes and seq_cap sequence words.
 __host__ __device__ inline int group_smem_bytes(const Pen& p, int ring_w, int mode, int seq_cap, int gw) {
   const int ns = p.slots();
   int b = 3 * ns * 4 + (gw > 1 ? 2 * partial_words(p) * gw * 4 : 0) + 16;

@@ -109,7 +109,7 @@ inline PassGeom plan_geometry(const Pen& pen, int32_t max_m, int32_t max_n, int 
   }
   if (p.mode == kModeGlobal) {
     p.ring_w = (int)full_w;
-    // the pair's packed words staged in shared memory by bulk copies when
+    // the pair's packed words staged in shared memory when
     // they fit beside the group's limits at the block count the kernel is
     // compiled for (0: read from global memory; always for 32-warp groups)
     const int64_t seqw = 2 * packed_words(max_m) + 2 * packed_words(max_n);
