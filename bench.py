@@ -51,6 +51,7 @@ PEN = (4, 6, 2)  # --penalties; five values (open2, extend2 last): dual gap-affi
 METRIC_NAME = None  # --metric edit | indel | gap_linear (PEN then (mismatch, gap_extension))
 ENDS_FREE = (0, 0, 0, 0)  # --ends-free pattern_begin,pattern_end,text_begin,text_end (gap-affine)
 LOW_MEM = 0  # --low-memory checkpoint interval (0 off, < 0 chosen per pass)
+BIDIR = False  # --bidirectional: TSU_BIDIRECTIONAL (breakpoint search; CIGARs by its recursion)
 LINEAR_XE = {"edit": (1, 1), "indel": (3, 1)}  # the gap-linear penalties of these metrics
 
 
@@ -62,6 +63,8 @@ def pen_str() -> str:
     ef = ", free ends %d/%d/%d/%d" % ENDS_FREE if any(ENDS_FREE) else ""
     if LOW_MEM:
         ef += ", low-memory (checkpoint interval %s)" % ("auto" if LOW_MEM < 0 else LOW_MEM)
+    if BIDIR:
+        ef += ", bidirectional"
     if METRIC_NAME in LINEAR_XE:
         return METRIC_NAME + " distance" + ef
     if METRIC_NAME == "gap_linear":
@@ -395,7 +398,8 @@ def main():
     ap.add_argument("--requests", type=int, default=200, help="c5: requests per rate")
     ap.add_argument("--workers", type=int, default=32, help="c5: server workers")
     ap.add_argument("--no-estimate", action="store_true", help="c5: size long pairs by --hint, not by estimate")
-    ap.add_argument("--budget-gb", type=float, default=0.0, help="c5: device budget (0: 80%% of free)")
+    ap.add_argument("--budget-gb", type=float, default=0.0,
+                    help="device memory budget of the engine context (0: 80%% of free)")
     ap.add_argument("--penalties", default="4,6,2",
                     help="mismatch,open,extend[,open2,extend2]: five values align with dual gap-affine penalties")
     ap.add_argument("--metric", default=None, choices=["edit", "indel", "gap_linear"],
@@ -404,9 +408,12 @@ def main():
                     help="pattern_begin,pattern_end,text_begin,text_end free lengths (gap-affine)")
     ap.add_argument("--low-memory", type=int, default=0,
                     help="checkpointed-history CIGARs: checkpoint interval (-1: chosen per pass)")
+    ap.add_argument("--bidirectional", action="store_true",
+                    help="bidirectional WFA (TSU_BIDIRECTIONAL): breakpoint search, CIGARs by its recursion")
     args = ap.parse_args()
-    global PEN, METRIC_NAME, ENDS_FREE, LOW_MEM
+    global PEN, METRIC_NAME, ENDS_FREE, LOW_MEM, BIDIR
     LOW_MEM = args.low_memory
+    BIDIR = args.bidirectional
     ENDS_FREE = tuple(int(v) for v in args.ends_free.split(","))
     if len(ENDS_FREE) != 4:
         raise SystemExit("--ends-free takes 4 values")
@@ -446,7 +453,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     head = measure(args, workload, rank, world, local, dist,
-                   with_plain=(workload == "c4" or args.plain) and not args.no_plain,
+                   with_plain=(workload == "c4" or args.plain) and not args.no_plain and not BIDIR,
                    with_cpu=world == 1 and not args.no_cpu_baseline, e2e_steps=args.e2e_steps)
     # the default run (c4) nests a full c2 record: the plain one-launch GPU
     # shape at scale (1,000,000 x 1 kbp), measured the same way
@@ -483,7 +490,7 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
     pbuf, poff, plen, tbuf, toff, tlen = make_batch(workload, rank, world)
     cells = float(np.sum(plen.astype(np.float64) * tlen))
     want_cigar = not args.score_only
-    al = make_aligner(T, device=local, max_error_hint=args.hint)
+    al = make_aligner(T, device=local, max_error_hint=args.hint, mem_budget=int(args.budget_gb * (1 << 30)))
 
     # ---- value: batch resident in HBM ----------------------------------
     dev = torch.device("cuda", local)
@@ -498,13 +505,14 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
     def dev_step():
         nonlocal d_runs, cap
         try:
-            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off if want_cigar else None)
+            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off if want_cigar else None,
+                                   bidirectional=BIDIR)
         except T.AlignError as e:
             if e.code != 5:
                 raise
             cap = int(e.needed) + 1024
             d_runs = torch.zeros(cap, dtype=torch.int32, device=dev)
-            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off)
+            return al.align_device(d_p, d_po, d_pl, d_t, d_to, d_tl, d_sc, d_runs, d_off, bidirectional=BIDIR)
 
     for _ in range(max(args.warmup, 1)):
         nruns = dev_step()
@@ -593,7 +601,7 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
         outs = (h_sc.numpy(), h_off.numpy(), h_runs.numpy().view(np.uint32)) if want_cigar else None
 
         def e2e_step():
-            return al.align_arrays(*(t.numpy() for t in hp), cigar=want_cigar, out=outs)
+            return al.align_arrays(*(t.numpy() for t in hp), cigar=want_cigar, out=outs, bidirectional=BIDIR)
 
         for _ in range(max(1, min(args.warmup, 2))):
             e2e_step()
@@ -639,9 +647,10 @@ def measure(args, workload, rank, world, local, dist, with_plain, with_cpu, e2e_
             "cpu_baseline": cpu,
             "clocks": clk,
         }
-        try:  # device memory the engine plans for this batch (tsu_predict_bytes)
-            full_b, min_b = al.predict_bytes(plen, tlen, cigar=want_cigar)
-            out["predicted_device_bytes"] = {"full": int(full_b), "min": int(min_b)}
+        try:  # device memory the engine plans for this batch (tsu_predict_bytes, forward passes)
+            if not BIDIR:
+                full_b, min_b = al.predict_bytes(plen, tlen, cigar=want_cigar)
+                out["predicted_device_bytes"] = {"full": int(full_b), "min": int(min_b)}
         except T.AlignError:
             pass
     al.close()
@@ -674,6 +683,14 @@ def roofline(workload, n_pairs, plen, tlen, nruns, work_cells, work_steps, ext_b
     DRAM traffic of an ncu capture of the same kernel scaled by pairs."""
     import torch
 
+    if BIDIR:
+        # the issue model above is the forward kernel's; the bidirectional
+        # kernels report their wavefront cells and steps only
+        return {"bound": "int_issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
+                "traffic": None, "kernel": "bidir_kernel" + (" + segment_kernel" if want_cigar else ""),
+                "kernel_ms": a_ms, "cells": work_cells, "score_steps": work_steps,
+                "cells_per_s": work_cells / (a_ms / 1e3), "passes": pass_log,
+                "note": "no calibrated issue model for the bidirectional kernels"}
     peak, peak_kind = measured_peaks()
     words = float(np.sum((plen.astype(np.int64) + 31) // 32 + 1) + np.sum((tlen.astype(np.int64) + 31) // 32 + 1))
     packed_in = words * 8

@@ -57,6 +57,18 @@ extern "C" {
                                 no longest-first order: the reference's scheduling
                                 (one 32-thread block per pair, wfa_gpu.cu:113-114),
                                 kept as the "plain" baseline of the benchmarks */
+#define TSU_BIDIRECTIONAL 0x4u /* one-piece gap-affine, end to end: bidirectional
+                                  WFA.  Each score is the lowest total at which a
+                                  forward and a reverse wavefront pass cross (the
+                                  breakpoint search, two rings per pair), about
+                                  half the wavefront cells of the forward pass; the
+                                  same scores.  CIGARs come from the recursion on
+                                  crossings down to segments of at most
+                                  max(2 max(x, o+e), 32 g) (g = gcd(x, o, e)),
+                                  each aligned with its full history: memory
+                                  linear in the score per pair.  WFA2-lib's
+                                  ultralow memory mode; the reference keeps the
+                                  default mode (wfa_gpu.cu:156-160) */
 
 typedef struct tsu_ctx tsu_ctx;
 
@@ -131,6 +143,9 @@ typedef struct {
   int64_t cells; /* wavefront (score, diagonal) cells computed, all passes */
   int64_t steps; /* non-null score steps computed, all passes              */
   int64_t ext_bases; /* bases matched by extend steps, all passes         */
+  int64_t device_bytes; /* most device memory the context's buffers held
+                           during the call (the workspace carried over from
+                           earlier calls included)                        */
 } tsu_timing;
 
 /* ---- context ------------------------------------------------------------

@@ -60,6 +60,9 @@ def lib():
         L.ora_align_segment.restype = ctypes.c_int
         L.ora_align_segment.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 3 + [
             ctypes.c_char, ctypes.c_char, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.ora_crossing_split.restype = ctypes.c_int
+        L.ora_crossing_split.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 3 + [
+            ctypes.c_char, ctypes.c_char, P(ctypes.c_int), ctypes.c_char_p, P(ctypes.c_int), P(ctypes.c_int)]
         L.ora_bialign_ring.restype = ctypes.c_int
         L.ora_bialign_ring.argtypes = [c_char_p, ctypes.c_int, c_char_p, ctypes.c_int] + [ctypes.c_int] * 4 + [
             ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -555,3 +558,19 @@ def refk_batch(seed: int, first: int, num: int, length: int, rate: float, x=4, o
     if rc != 0:
         raise RuntimeError(f"ora_refk_batch error {rc}")
     return sc, codes, steps, maxk
+
+
+def crossing_split(pattern, text, x=4, o=6, e=2, begin="M", end="M"):
+    """The two-ring breakpoint search on one segment (ora_crossing_split):
+    (total, component, forward diagonal, cut offset), or None when nothing
+    crosses."""
+    p, t = _b(pattern), _b(text)
+    T, k, h = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    comp = ctypes.create_string_buffer(1)
+    rc = lib().ora_crossing_split(p, len(p), t, len(t), x, o, e, begin.encode(), end.encode(), ctypes.byref(T),
+                                  comp, ctypes.byref(k), ctypes.byref(h))
+    if rc < 0:
+        raise RuntimeError(f"ora_crossing_split failed: {rc}")
+    if rc == 0:
+        return None
+    return T.value, comp.raw[:1].decode(), k.value, h.value

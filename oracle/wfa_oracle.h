@@ -169,6 +169,16 @@ int ora_bialign(const char* pattern, int m, const char* text, int n, int x, int 
  * rings per pair computes. */
 int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x, int o, int e, int base_score,
                      char* ops, int ops_cap, int* ops_len);
+/* The two-ring breakpoint search on one segment with gap components (begin
+ * and end 'M', 'I' or 'D'): the lowest crossing total *T, its component
+ * *comp, forward diagonal *k and cut offset *h (text position).  Returns 1
+ * when a crossing was found, 0 when none, or a negative error. */
+int ora_crossing_split(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
+                       char end, int* T, char* comp, int* k, int* h);
+/* The same over a batch (OpenMP over segments): T[i] = -1 where none. */
+int ora_crossing_split_batch(int64_t num, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                             const int64_t* toff, const int32_t* tlen, const char* begin, const char* end, int x,
+                             int o, int e, int32_t* T, char* comp, int32_t* k, int32_t* h);
 /* One segment of a bidirectional alignment by the plain WFA with gap
  * components (the recursion's base case): begin 'I'/'D' continues a gap
  * from the left (a leading run costs e per base), end 'I'/'D' requires the

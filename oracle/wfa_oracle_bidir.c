@@ -561,6 +561,37 @@ int ora_bialign_ring(const char* pattern, int m, const char* text, int n, int x,
                      ops_len);
 }
 
+int ora_crossing_split(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
+                       char end, int* T, char* comp, int* k, int* h) {
+  if (!pattern || !text || !T || !comp || !k || !h || m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;
+  if (!strchr("MID", begin) || !strchr("MID", end) || !begin || !end) return ORA_EINVAL;
+  return crossing_breakpoint(pattern, m, text, n, x, o, e, begin, end, T, comp, k, h);
+}
+
+int ora_crossing_split_batch(int64_t num, const char* pat, const int64_t* poff, const int32_t* plen, const char* txt,
+                             const int64_t* toff, const int32_t* tlen, const char* begin, const char* end, int x,
+                             int o, int e, int32_t* T, char* comp, int32_t* k, int32_t* h) {
+  if (num < 0 || !pat || !poff || !plen || !txt || !toff || !tlen || !begin || !end || !T || !comp || !k || !h)
+    return ORA_EINVAL;
+  int rc = 0;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t i = 0; i < num; ++i) {
+    int t_ = 0, k_ = 0, h_ = 0;
+    char c_ = 'M';
+    const int r = ora_crossing_split(pat + poff[i], plen[i], txt + toff[i], tlen[i], x, o, e, begin[i], end[i], &t_,
+                                     &c_, &k_, &h_);
+    if (r < 0) {
+#pragma omp atomic write
+      rc = r;
+    }
+    T[i] = r == 1 ? t_ : -1;
+    comp[i] = c_;
+    k[i] = k_;
+    h[i] = h_;
+  }
+  return rc;
+}
+
 int ora_align_segment(const char* pattern, int m, const char* text, int n, int x, int o, int e, char begin,
                       char end, char* ops, int ops_cap, int* ops_len) {
   if (!pattern || !text || !ops || !ops_len || m < 0 || n < 0 || x <= 0 || o < 0 || e <= 0) return ORA_EINVAL;

@@ -1,7 +1,7 @@
 // warp_emu.h -- runs the engine's CUDA kernel source on the CPU (test
 // infrastructure).  Each lane is a std::thread; every warp collective
-// (__syncwarp, __shfl_sync, __reduce_*_sync, __any_sync, __ballot_sync) is a
-// barrier over the lanes of that warp.  Dynamic shared memory and all
+// (__syncwarp, __shfl_sync, __shfl_xor_sync, __reduce_*_sync, __any_sync,
+// __ballot_sync) is a barrier over the lanes of that warp.  Dynamic shared memory and all
 // buffers are exact-size heap blocks, so AddressSanitizer reports any access
 // outside them.  Used to check the kernels' index arithmetic without a GPU.
 #pragma once
@@ -93,6 +93,16 @@ inline int reduce_max(int v) {
 inline unsigned reduce_add(unsigned v) {
   return (unsigned)all_reduce((uint64_t)v, [](uint64_t a, uint64_t b) { return (uint64_t)(uint32_t)(a + b); });
 }
+// the value of lane (this lane ^ m)
+template <class T>
+inline T shfl_xor(T v, int m) {
+  uint64_t b = 0;
+  std::memcpy(&b, &v, sizeof(T));
+  const uint64_t r = exchange(b)[(lane() ^ m) & 31];
+  T out;
+  std::memcpy(&out, &r, sizeof(T));
+  return out;
+}
 inline unsigned ballot(bool p) {
   const uint64_t* s = exchange(p ? 1u : 0u);
   unsigned r = 0;
@@ -152,6 +162,7 @@ void launch(int blocks, int threads, size_t smem_bytes, F body) {
 #define gridDim (emu::gdim)
 #define __syncwarp(...) emu::syncwarp()
 #define __shfl_sync(mask, v, src) emu::shfl((v), (src))
+#define __shfl_xor_sync(mask, v, m) emu::shfl_xor((v), (m))
 #define __reduce_min_sync(mask, v) emu::reduce_min(v)
 #define __reduce_max_sync(mask, v) emu::reduce_max(v)
 #define __reduce_add_sync(mask, v) emu::reduce_add(v)

@@ -14,6 +14,7 @@ from ._lib import (  # noqa: F401
     Aligner,
     AlignError,
     Server,
+    TSU_BIDIRECTIONAL,
     TSU_SCORE_ONLY,
     build,
     gen_batch,
@@ -30,6 +31,7 @@ __all__ = [
     "Aligner",
     "AlignError",
     "Server",
+    "TSU_BIDIRECTIONAL",
     "TSU_SCORE_ONLY",
     "build",
     "gen_batch",

@@ -21,6 +21,7 @@ TSU_ENOTFOUND = 7
 TSU_EPENDING = 10
 TSU_SCORE_ONLY = 0x1
 TSU_ONE_WARP = 0x2
+TSU_BIDIRECTIONAL = 0x4
 
 P = ctypes.POINTER
 c_i32, c_i64, c_u32, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p
@@ -56,7 +57,8 @@ class Timing(ctypes.Structure):
     _fields_ = [("h2d_ms", ctypes.c_double), ("pack_ms", ctypes.c_double), ("align_ms", ctypes.c_double),
                 ("compact_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("kernel_launches", c_i64), ("retried_pairs", c_i64), ("h2d_bytes", c_i64),
-                ("d2h_bytes", c_i64), ("cells", c_i64), ("steps", c_i64), ("ext_bases", c_i64)]
+                ("d2h_bytes", c_i64), ("cells", c_i64), ("steps", c_i64), ("ext_bases", c_i64),
+                ("device_bytes", c_i64)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -298,13 +300,16 @@ class Aligner:
     # -- host buffers ------------------------------------------------------
     def align_arrays(self, pbuf: np.ndarray, poff: np.ndarray, plen: np.ndarray, tbuf: np.ndarray,
                      toff: np.ndarray, tlen: np.ndarray, cigar: bool = True, status: bool = False,
-                     cigar_capacity: Optional[int] = None, out=None):
+                     cigar_capacity: Optional[int] = None, out=None, bidirectional: bool = False):
         """Align pairs given as concatenated byte buffers + offsets/lengths.
 
         Returns ``(scores, cigar_offsets, runs)``; the CIGAR parts are None
         with ``cigar=False``.  ``status=True`` appends per-pair statuses.
         ``out=(scores, offsets, runs)`` supplies preallocated (e.g. pinned)
-        output arrays; ``runs.size`` is then the CIGAR capacity."""
+        output arrays; ``runs.size`` is then the CIGAR capacity.
+        ``bidirectional=True``: TSU_BIDIRECTIONAL -- scores by the
+        bidirectional breakpoint search and CIGARs by its recursion, in
+        memory linear in the score per pair."""
         n = len(plen)
         poff = np.ascontiguousarray(poff, dtype=np.int64)
         toff = np.ascontiguousarray(toff, dtype=np.int64)
@@ -316,7 +321,8 @@ class Aligner:
         L = lib()
         if not cigar:
             r = Result(_ptr(scores), None, 0, None, 0, _ptr(st))
-            self._check(L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), TSU_SCORE_ONLY))
+            flags = TSU_SCORE_ONLY | (TSU_BIDIRECTIONAL if bidirectional else 0)
+            self._check(L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), flags))
             return (scores, None, None, st) if status else (scores, None, None)
         if out is not None:
             coff, runs = out[1], out[2]
@@ -327,12 +333,13 @@ class Aligner:
         if out is None:
             runs = np.zeros(max(cap, 1), dtype=np.uint32)
         r = Result(_ptr(scores), _ptr(runs), cap, _ptr(coff), 0, _ptr(st))
-        rc = L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), 0)
+        flags = TSU_BIDIRECTIONAL if bidirectional else 0
+        rc = L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), flags)
         if rc == TSU_EOVERFLOW and cigar_capacity is None:
             need = int(r.cigar_needed)
             runs = np.zeros(max(need, 1), dtype=np.uint32)
             r = Result(_ptr(scores), _ptr(runs), need, _ptr(coff), 0, _ptr(st))
-            rc = L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), 0)
+            rc = L.tsu_align_batch(self._h, ctypes.byref(b), ctypes.byref(r), flags)
         self._check(rc)
         runs = runs[: int(coff[-1])]
         return (scores, coff, runs, st) if status else (scores, coff, runs)
@@ -359,13 +366,15 @@ class Aligner:
 
     # -- device buffers (torch CUDA tensors) --------------------------------
     def align_device(self, pat, poff, plen, txt, toff, tlen, scores, cigar_runs=None, cigar_off=None,
-                     pair_status=None, one_warp: bool = False) -> int:
+                     pair_status=None, one_warp: bool = False, bidirectional: bool = False) -> int:
         """All arguments are CUDA tensors (uint8 / int64 / int32).  Returns the
-        number of CIGAR runs written (0 with cigar_runs=None)."""
+        number of CIGAR runs written (0 with cigar_runs=None).
+        ``bidirectional=True``: TSU_BIDIRECTIONAL."""
         n = int(plen.numel())
         b = Batch(n, pat.data_ptr(), poff.data_ptr(), plen.data_ptr(), txt.data_ptr(), toff.data_ptr(),
                   tlen.data_ptr())
-        flags = (0 if cigar_runs is not None else TSU_SCORE_ONLY) | (TSU_ONE_WARP if one_warp else 0)
+        flags = ((0 if cigar_runs is not None else TSU_SCORE_ONLY) | (TSU_ONE_WARP if one_warp else 0) |
+                 (TSU_BIDIRECTIONAL if bidirectional else 0))
         r = Result(scores.data_ptr(), cigar_runs.data_ptr() if cigar_runs is not None else None,
                    int(cigar_runs.numel()) if cigar_runs is not None else 0,
                    cigar_off.data_ptr() if cigar_off is not None else None, 0,

@@ -25,6 +25,7 @@
 
 #include "../../include/tsunami_b200.h"
 #include "tsu_engine_internal.h"
+#include "tsu_bidir.cuh"
 #include "tsu_kernels.cuh"
 #include "tsu_launch.cuh"
 #include "tsu_plan.h"
@@ -72,7 +73,10 @@ struct tsu_ctx {
   DevBuf b_order, b_retry, b_counters;                    // queue, retry list, counters
   DevBuf b_scratch, b_arena, b_scan_tmp;                  // wavefront scratch of a pass (carve_scratch), CIGAR arena
   DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
+  DevBuf b_rwords, b_rnonacgt, b_segs, b_bout;            // bidirectional mode: reversed words, segments, cuts
+  DevBuf b_bsegs, b_boff, b_blen, b_bruns, b_bfirst;      // bidirectional CIGARs: base cases, their runs
   bool one_warp = false;  // TSU_ONE_WARP of the current call
+  bool bidir = false;     // TSU_BIDIRECTIONAL of the current call
   cudaEvent_t pev[2] = {};  // per-pass timing
   std::string passlog;      // passes of the last align call (tsu_pass_log)
   cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;  // chunk pipeline copy streams
@@ -88,6 +92,7 @@ struct tsu_ctx {
   HostBuf h_scalars;  // 64 bytes: retry count, arena cursor, work counters, run total
   HostBuf h_list;     // int32 pass order / retry list
   HostBuf h_status;   // int32 pair statuses (tsu_align_batch)
+  HostBuf h_bidir;    // bidirectional mode: segments down, cuts and run counts up
   std::vector<void*> h_retired;  // outgrown page-locked buffers, freed at destroy
   // events of the host-buffer pipeline (tsu_align_batch): 8 chunks at most
   cudaEvent_t cev_up[8] = {}, cev_done[8] = {}, cev_down[8] = {}, cev_t[2] = {};
@@ -105,6 +110,7 @@ struct tsu_ctx {
   cudaEvent_t bev[2 * tsu::kBands] = {};  // first pass of each band: start, end
   cudaEvent_t wait_ev = nullptr;  // blocking-sync event of those waits
   size_t need_bytes = 0;         // budget the last TSU_ENOMEM step needed
+  size_t peak_held = 0;          // most bytes held during the current call (tsu_timing.device_bytes)
   // free ends (tsu_set_ends_free): pattern begin, pattern end, text begin,
   // text end; all 0: end-to-end
   int32_t ends_free[4] = {0, 0, 0, 0};
@@ -114,7 +120,8 @@ struct tsu_ctx {
   std::vector<DevBuf*> bufs() {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
             &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
-            &b_retry, &b_counters, &b_scratch, &b_arena, &b_scan_tmp, &b_out2};
+            &b_retry, &b_counters, &b_scratch, &b_arena, &b_scan_tmp, &b_out2, &b_rwords, &b_rnonacgt,
+            &b_segs,  &b_bout, &b_bsegs, &b_boff, &b_blen, &b_bruns, &b_bfirst};
   }
   size_t held() const {
     size_t s = 0;
@@ -216,6 +223,7 @@ int grow(tsu_ctx* ctx, DevBuf& b, size_t bytes) {
     return set_err(ctx, TSU_ENOMEM, "device allocation of %zu B failed: %s", nb, cudaGetErrorString(e));
   }
   b.cap = nb;
+  ctx->peak_held = std::max(ctx->peak_held, ctx->held());
   return TSU_OK;
 }
 
@@ -494,6 +502,463 @@ void carve_scratch(tsu_ctx* ctx, const Pass& ps, bool cigar, tsu::AlignArgs* a) 
   }
 }
 
+// ---- bidirectional mode (TSU_BIDIRECTIONAL) --------------------------------
+
+// Segments of the score-only mode: every pair whole, free at both ends.
+__global__ void bidir_seg_kernel(int64_t n, const int32_t* __restrict__ plen, const int32_t* __restrict__ tlen,
+                                 tsu::BidirSeg* __restrict__ segs) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    segs[i] = tsu::BidirSeg{(int32_t)i, 0, 0, plen[i], tlen[i], 'M', 'M'};
+}
+
+// Scores from the crossing totals (score units).
+__global__ void bidir_score_kernel(int64_t n, const int32_t* __restrict__ T, int g, int32_t* __restrict__ score) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    score[i] = T[i] >= 0 ? T[i] * g : 0;
+}
+
+// Checks of the bidirectional mode's settings.
+int bidir_check(tsu_ctx* ctx) {
+  const tsu::Pen& rp = ctx->rp;
+  if (rp.model() != tsu::kModelAffine)
+    return set_err(ctx, TSU_EINVAL, "bidirectional mode: one-piece gap-affine penalties only");
+  if (ctx->ends_free[0] | ctx->ends_free[1] | ctx->ends_free[2] | ctx->ends_free[3])
+    return set_err(ctx, TSU_EINVAL, "bidirectional mode: end-to-end alignment only");
+  if (ctx->low_mem) return set_err(ctx, TSU_EINVAL, "bidirectional mode: no low-memory mode");
+  if (rp.rm > 64) return set_err(ctx, TSU_EINVAL, "bidirectional mode: rings deeper than 64 score units");
+  return TSU_OK;
+}
+
+// Packs the pairs forward and reversed (between events ev[2] and ev[3]).
+int bidir_pack(tsu_ctx* ctx, const tsu::SeqView& sv, const BatchInfo& bi, tsu::PackView* pk, tsu::PackView* pkr) {
+  const int64_t n = sv.n;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if ((rc = grow(ctx, ctx->b_words_cnt, sizeof(int64_t) * 2 * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_woff, sizeof(int64_t) * 2 * n))) return rc;
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff), (int)(2 * n),
+                                st);
+  if ((rc = grow(ctx, ctx->b_scan_tmp, tmp_bytes))) return rc;
+  if ((rc = grow(ctx, ctx->b_words, sizeof(uint64_t) * (size_t)bi.total_words))) return rc;
+  if ((rc = grow(ctx, ctx->b_rwords, sizeof(uint64_t) * (size_t)bi.total_words))) return rc;
+  if ((rc = grow(ctx, ctx->b_nonacgt, (size_t)(2 * n)))) return rc;
+  if ((rc = grow(ctx, ctx->b_rnonacgt, (size_t)(2 * n)))) return rc;
+  *pk = tsu::PackView{P<uint64_t>(ctx->b_words), P<int64_t>(ctx->b_woff), P<uint8_t>(ctx->b_nonacgt)};
+  *pkr = tsu::PackView{P<uint64_t>(ctx->b_rwords), P<int64_t>(ctx->b_woff), P<uint8_t>(ctx->b_rnonacgt)};
+  CU(cudaEventRecord(ctx->ev[2], st));
+  tsu::word_count_kernel<<<std::min<int64_t>((2 * n + 255) / 256, 4096), 256, 0, st>>>(n, sv.pat_len, sv.txt_len,
+                                                                                       P<int64_t>(ctx->b_words_cnt));
+  size_t tb = tmp_bytes;
+  CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tb, P<int64_t>(ctx->b_words_cnt), P<int64_t>(ctx->b_woff),
+                                   (int)(2 * n), st));
+  const int64_t pblocks = std::min<int64_t>((2 * n + 7) / 8, (int64_t)ctx->sms * 16);
+  tsu::pack_kernel<<<(int)pblocks, 256, 0, st>>>(sv, *pk);
+  tsu::pack_kernel<true><<<(int)pblocks, 256, 0, st>>>(sv, *pkr);
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(ctx->ev[3], st));
+  return TSU_OK;
+}
+
+// One persistent launch of the breakpoint kernel (tsu_bidir.cuh) over c
+// segments (device), one group per segment at a time (1, 4 or 16 warps by
+// the longest side max_side), both rings of a group in device memory (2
+// directions x ring depth x 4 components x (max_bases + 3) int32, from the
+// scratch buffer).  Writes T, comp, k, h at out, out + c, out + 2c, out + 3c
+// and the statuses; adds cells and steps to d_work[0..1].
+int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, const tsu::PackView& pkr,
+                const tsu::BidirSeg* segs, int64_t c, int32_t max_side, int32_t max_bases, int32_t* out,
+                int32_t* status, unsigned int* d_queue, unsigned long long* d_work, std::string* log) {
+  cudaStream_t st = ctx->stream;
+  int rc;
+  const tsu::Pen& rp = ctx->rp;
+  const int gw = max_side < 2048 ? 1 : (max_side < 16384 ? 4 : 16);
+  const int threads = gw <= 4 ? 128 : 32 * gw;
+  const int gpb = threads / (32 * gw);
+  const size_t smem = (size_t)gpb * tsu::bidir_group_smem(rp, gw);
+  int occ = 0;
+  CU(tsu::bidir_occupancy(gw, threads, smem, &occ));
+  if (occ < 1) return set_err(ctx, TSU_EDEVICE, "bidirectional kernel: no occupancy");
+  const int ring_w = max_bases + 3;
+  const int64_t ring_stride = (int64_t)2 * rp.rm * 4 * ring_w;
+  int64_t groups = std::min<int64_t>((int64_t)ctx->sms * occ * gpb, c);
+  const size_t fixed = ctx->held() - ctx->b_scratch.cap;
+  const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+  groups = std::min<int64_t>(groups, (int64_t)(avail / (sizeof(int32_t) * (size_t)ring_stride)));
+  if (groups < 1) return set_err(ctx, TSU_ENOMEM, "bidirectional mode: rings of one pair exceed the budget");
+  int bpg = gpb;  // groups per block
+  if (groups >= gpb)
+    groups = groups / gpb * gpb;
+  else
+    bpg = (int)groups;
+  const size_t need = sizeof(int32_t) * (size_t)(groups * ring_stride);
+  if (need > ctx->b_scratch.cap) {
+    release(ctx, ctx->b_scratch);
+    if ((rc = grow(ctx, ctx->b_scratch, need))) return rc;
+  }
+  CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+  tsu::BidirArgs a{};
+  a.seq = sv;
+  a.pk = pk;
+  a.pkr = pkr;
+  a.segs = segs;
+  a.n_segs = c;
+  a.pen = rp;
+  a.ring_w = ring_w;
+  a.ring = P<int32_t>(ctx->b_scratch);
+  a.ring_stride = ring_stride;
+  a.out_T = out;
+  a.out_comp = out + c;
+  a.out_k = out + 2 * c;
+  a.out_h = out + 3 * c;
+  a.status = status;
+  a.queue = d_queue;
+  a.work = d_work;
+  tsu::launch_bidir(gw, (int)(groups / bpg), 32 * gw * bpg, (size_t)bpg * tsu::bidir_group_smem(rp, gw), st, a);
+  CU(cudaGetLastError());
+  ctx->timing.kernel_launches++;
+  if (log) *log += (log->empty() ? "b" : " b") + std::to_string(gw) + "x" + std::to_string(groups) + ":" + std::to_string(c);
+  return TSU_OK;
+}
+
+// TSU_BIDIRECTIONAL score-only calls: pack the pairs forward and reversed,
+// then one breakpoint launch over all pairs, each pair whole and free at
+// both ends.  A pair's score is its lowest crossing total; for an
+// end-to-end pair that is the optimal score.
+int run_bidir(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d_status, const BatchInfo& bi) {
+  const int64_t n = sv.n;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if ((rc = bidir_check(ctx))) return rc;
+  if ((rc = grow(ctx, ctx->b_segs, sizeof(tsu::BidirSeg) * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_bout, sizeof(int32_t) * 4 * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
+  tsu::PackView pk, pkr;
+  if ((rc = bidir_pack(ctx, sv, bi, &pk, &pkr))) return rc;
+  tsu::BidirSeg* segs = P<tsu::BidirSeg>(ctx->b_segs);
+  const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
+  bidir_seg_kernel<<<eblocks, 256, 0, st>>>(n, sv.pat_len, sv.txt_len, segs);
+  unsigned long long* d_cnt = P<unsigned long long>(ctx->b_counters);
+  CU(cudaMemsetAsync(d_cnt, 0, 64, st));
+  int32_t* bo = P<int32_t>(ctx->b_bout);
+  ctx->timing.kernel_launches = 4;
+  std::string log;
+  CU(cudaEventRecord(ctx->ev[4], st));
+  if ((rc = bidir_split(ctx, sv, pk, pkr, segs, n, std::max(bi.max_m, bi.max_n), bi.max_m + bi.max_n, bo, d_status,
+                        reinterpret_cast<unsigned int*>(d_cnt), d_cnt + 1, &log)))
+    return rc;
+  bidir_score_kernel<<<eblocks, 256, 0, st>>>(n, bo, ctx->g, d_score);
+  CU(cudaGetLastError());
+  ctx->timing.kernel_launches++;
+  CU(cudaEventRecord(ctx->ev[5], st));
+  CU(cudaEventRecord(ctx->ev[6], st));
+  char* h = static_cast<char*>(ctx->h_scalars.p);
+  CU(cudaMemcpyAsync(h, d_cnt + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(wait_stream(ctx, st));
+  ctx->timing.cells = (int64_t)reinterpret_cast<const unsigned long long*>(h)[0];
+  ctx->timing.steps = (int64_t)reinterpret_cast<const unsigned long long*>(h)[1];
+  ctx->passlog = log;
+  return TSU_OK;
+}
+
+// TSU_BIDIRECTIONAL calls with CIGARs: the BiWFA recursion, level by level.
+// Level 0 is every pair whole; each level's segments go through one
+// breakpoint launch, and the host cuts each segment at its crossing (k, h)
+// into a left part (begin component, crossing component) and a right part
+// (crossing component, end component) for the next level -- unless the
+// crossing total is at most the base score max(2 max(x, o + e), 32) (score
+// units) or the cut leaves one side empty, when the segment is a leaf.
+// Leaves, ordered by pair and position, then run through the segment kernel
+// (tsu_segment.cuh) in launches of growing step caps (a leaf that outgrows
+// its launch's history goes to the next), and one thread per pair joins its
+// leaves' runs.  Scores come from level 0.
+int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d_status, uint32_t* d_out_runs,
+                    int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, const BatchInfo& bi,
+                    const int32_t* h_plen, const int32_t* h_tlen, uint32_t** out_used, DevBuf* out_buf) {
+  const int64_t n = sv.n;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if ((rc = bidir_check(ctx))) return rc;
+  const tsu::Pen& rp = ctx->rp;
+  if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
+  if ((rc = grow(ctx, ctx->b_clen64, sizeof(int64_t) * (n + 1)))) return rc;
+  if ((rc = grow(ctx, ctx->b_bfirst, sizeof(int64_t) * (n + 1)))) return rc;
+  tsu::PackView pk, pkr;
+  if ((rc = bidir_pack(ctx, sv, bi, &pk, &pkr))) return rc;
+  unsigned long long* d_cnt = P<unsigned long long>(ctx->b_counters);
+  unsigned int* d_queue = reinterpret_cast<unsigned int*>(d_cnt);
+  CU(cudaMemsetAsync(d_cnt, 0, 64, st));
+  ctx->timing.kernel_launches = 3;
+  std::string log;
+  CU(cudaEventRecord(ctx->ev[4], st));
+  const int base = std::max(2 * (rp.rm - 1), 32);
+  std::vector<int32_t> pst((size_t)n, tsu::kPairOk);  // pair statuses
+  std::vector<tsu::BidirSeg> cur((size_t)n), next, leaves;
+  std::vector<int32_t> leaf_T;
+  for (int64_t i = 0; i < n; ++i) cur[(size_t)i] = tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'};
+  for (int level = 0; !cur.empty(); ++level) {
+    const int64_t c = (int64_t)cur.size();
+    int32_t max_side = 0, max_bases = 0;
+    for (const tsu::BidirSeg& s : cur) {
+      max_side = std::max(max_side, std::max(s.m, s.n));
+      max_bases = std::max(max_bases, s.m + s.n);
+    }
+    if ((rc = grow(ctx, ctx->b_segs, sizeof(tsu::BidirSeg) * c))) return rc;
+    if ((rc = grow(ctx, ctx->b_bout, sizeof(int32_t) * 5 * c))) return rc;
+    const size_t seg_bytes = sizeof(tsu::BidirSeg) * (size_t)c, res_bytes = sizeof(int32_t) * 5 * (size_t)c;
+    if ((rc = host_grow(ctx, ctx->h_bidir, std::max(seg_bytes, res_bytes)))) return rc;
+    std::memcpy(ctx->h_bidir.p, cur.data(), seg_bytes);
+    CU(cudaMemcpyAsync(ctx->b_segs.p, ctx->h_bidir.p, seg_bytes, cudaMemcpyHostToDevice, st));
+    int32_t* bo = P<int32_t>(ctx->b_bout);
+    int32_t* bst = level == 0 ? d_status : bo + 4 * c;
+    if ((rc = bidir_split(ctx, sv, pk, pkr, P<tsu::BidirSeg>(ctx->b_segs), c, max_side, max_bases, bo, bst, d_queue,
+                          d_cnt + 1, &log)))
+      return rc;
+    if (level == 0) {
+      const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
+      bidir_score_kernel<<<eblocks, 256, 0, st>>>(n, bo, ctx->g, d_score);
+      CU(cudaGetLastError());
+      ctx->timing.kernel_launches++;
+      CU(cudaMemcpyAsync(bo + 4 * c, d_status, sizeof(int32_t) * c, cudaMemcpyDeviceToDevice, st));
+    }
+    CU(cudaMemcpyAsync(ctx->h_bidir.p, bo, res_bytes, cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    const int32_t* hr = static_cast<const int32_t*>(ctx->h_bidir.p);
+    next.clear();
+    for (int64_t j = 0; j < c; ++j) {
+      const tsu::BidirSeg& s = cur[(size_t)j];
+      int32_t& ps = pst[(size_t)s.pair];
+      if (ps != tsu::kPairOk) continue;
+      const int32_t T = hr[j], comp = hr[c + j], k = hr[2 * c + j], h = hr[3 * c + j], sst = hr[4 * c + j];
+      if (sst != tsu::kPairOk || T < 0) {
+        ps = sst != tsu::kPairOk ? sst : tsu::kPairInternal;
+        continue;
+      }
+      if (s.m == 0 && s.n == 0) continue;
+      const int32_t v = h - k, left = v + h, whole = s.m + s.n;
+      if (T <= base || left <= 0 || left >= whole) {
+        leaves.push_back(s);
+        leaf_T.push_back(T);
+        continue;
+      }
+      next.push_back(tsu::BidirSeg{s.pair, s.v0, s.h0, v, h, s.begin, comp});
+      next.push_back(tsu::BidirSeg{s.pair, s.v0 + v, s.h0 + h, s.m - v, s.n - h, comp, s.end});
+    }
+    cur.swap(next);
+  }
+  // leaves in pair and position order: a counting sort by pair, then each
+  // pair's few leaves by position
+  const int64_t L = (int64_t)leaves.size();
+  std::vector<int64_t> first((size_t)n + 1, 0);
+  for (const tsu::BidirSeg& s : leaves) first[(size_t)s.pair + 1]++;
+  for (int64_t i = 0; i < n; ++i) first[(size_t)i + 1] += first[(size_t)i];
+  std::vector<int64_t> idx((size_t)L);
+  {
+    std::vector<int64_t> fill(first.begin(), first.end() - 1);
+    for (int64_t i = 0; i < L; ++i) idx[(size_t)fill[(size_t)leaves[(size_t)i].pair]++] = i;
+  }
+  for (int64_t p = 0; p < n; ++p)
+    if (first[(size_t)p + 1] - first[(size_t)p] > 1)
+      std::sort(idx.begin() + first[(size_t)p], idx.begin() + first[(size_t)p + 1], [&](int64_t a, int64_t b) {
+        return leaves[(size_t)a].v0 + leaves[(size_t)a].h0 < leaves[(size_t)b].v0 + leaves[(size_t)b].h0;
+      });
+  std::vector<tsu::BidirSeg> segs((size_t)L);
+  std::vector<int32_t> lT((size_t)L);
+  for (int64_t i = 0; i < L; ++i) {
+    segs[(size_t)i] = leaves[(size_t)idx[(size_t)i]];
+    lT[(size_t)i] = leaf_T[(size_t)idx[(size_t)i]];
+  }
+  // launches of growing step caps: a leaf starts in the first launch whose
+  // cap exceeds its crossing total + 2 (o + e) + 4, then moves up while it
+  // runs out of history
+  const int step0 = base + 2 * rp.go + 4;
+  auto cap_of = [&](int32_t T) {
+    int s = step0;
+    while (s < T + 2 * rp.go + 4) s *= 2;
+    return s;
+  };
+  std::vector<int32_t> lstat((size_t)L, tsu::kPairScratch), lcap((size_t)L);
+  std::vector<int64_t> roff((size_t)L, 0);
+  for (int64_t i = 0; i < L; ++i) lcap[(size_t)i] = cap_of(lT[(size_t)i]);
+  int64_t run_total = 0;  // run slots handed out so far
+  if ((rc = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(L, 1)))) return rc;
+  if ((rc = grow(ctx, ctx->b_boff, sizeof(int64_t) * std::max<int64_t>(L, 1)))) return rc;
+  if ((rc = grow(ctx, ctx->b_blen, 2 * sizeof(int32_t) * std::max<int64_t>(L, 1)))) return rc;
+  int32_t* d_rlen = P<int32_t>(ctx->b_blen);
+  int32_t* d_lst = d_rlen + L;
+  int segs_occ = 0;
+  CU(tsu::segment_occupancy(&segs_occ));
+  if (segs_occ < 1) return set_err(ctx, TSU_EDEVICE, "segment kernel: no occupancy");
+  const int64_t max_smax = (int64_t)(std::max(bi.max_m, 0) + std::max(bi.max_n, 0)) * (rp.rm - 1) + 2 * rp.go + 1;
+  for (;;) {
+    // the pending leaves of the lowest cap
+    int scap = INT32_MAX;
+    for (int64_t i = 0; i < L; ++i)
+      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)segs[(size_t)i].pair] == tsu::kPairOk)
+        scap = std::min(scap, lcap[(size_t)i]);
+    if (scap == INT32_MAX) break;
+    if (scap > 2 * max_smax + 2 * step0) return set_err(ctx, TSU_EINTERNAL, "segment kernel: step cap runaway");
+    std::vector<int64_t> pick;
+    int32_t bases = 0;
+    for (int64_t i = 0; i < L; ++i)
+      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)segs[(size_t)i].pair] == tsu::kPairOk &&
+          lcap[(size_t)i] == scap) {
+        pick.push_back(i);
+        bases = std::max(bases, segs[(size_t)i].m + segs[(size_t)i].n);
+      }
+    const int64_t c = (int64_t)pick.size();
+    // run regions of this launch, after those handed out before
+    std::vector<tsu::BidirSeg> ls((size_t)c);
+    std::vector<int64_t> lo((size_t)c);
+    int64_t add = 0;
+    for (int64_t j = 0; j < c; ++j) {
+      const tsu::BidirSeg& s = segs[(size_t)pick[(size_t)j]];
+      ls[(size_t)j] = s;
+      lo[(size_t)j] = run_total + add;
+      add += tsu::seg_run_cap(rp, (int64_t)s.m + s.n, scap);
+    }
+    const size_t run_bytes = sizeof(uint32_t) * (size_t)(run_total + add);
+    if (run_bytes > ctx->b_bruns.cap) {
+      // keep the runs written so far: grow by copy
+      DevBuf nb;
+      const size_t bytes = (std::max(run_bytes, ctx->b_bruns.cap + ctx->b_bruns.cap / 2) + 255) & ~(size_t)255;
+      if (ctx->held() + bytes > ctx->budget) release(ctx, ctx->b_scratch);
+      if (ctx->held() + bytes > ctx->budget) {
+        ctx->need_bytes = ctx->held() + bytes;
+        return set_err(ctx, TSU_ENOMEM, "bidirectional mode: CIGAR runs exceed the budget");
+      }
+      CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
+      nb.cap = bytes;
+      if (run_total)
+        CU(cudaMemcpyAsync(nb.p, ctx->b_bruns.p, sizeof(uint32_t) * (size_t)run_total, cudaMemcpyDeviceToDevice, st));
+      ctx->peak_held = std::max(ctx->peak_held, ctx->held() + nb.cap);
+      release(ctx, ctx->b_bruns);
+      ctx->b_bruns = nb;
+    }
+    // per-warp history and step table
+    const int64_t hcap = tsu::seg_hist_cap(scap, bases);
+    const size_t per_warp = sizeof(int32_t) * (size_t)(4 * hcap + 9 * (int64_t)scap);
+    const int wpb = tsu::kSegThreads / 32;
+    int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
+    const size_t fixed = ctx->held() - ctx->b_scratch.cap;
+    const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+    warps = std::min<int64_t>(warps, (int64_t)(avail / per_warp));
+    if (warps < 1) {
+      ctx->need_bytes = fixed + per_warp;
+      return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
+    }
+    const int64_t blocks = (warps + wpb - 1) / wpb;
+    const size_t need = per_warp * (size_t)(blocks * wpb);
+    if (need > ctx->b_scratch.cap) {
+      release(ctx, ctx->b_scratch);
+      if ((rc = grow(ctx, ctx->b_scratch, need))) return rc;
+    }
+    const size_t sb = sizeof(tsu::BidirSeg) * (size_t)c, ob = sizeof(int64_t) * (size_t)c;
+    if ((rc = host_grow(ctx, ctx->h_bidir, sb + ob + 2 * sizeof(int32_t) * (size_t)c))) return rc;
+    char* hb = static_cast<char*>(ctx->h_bidir.p);
+    std::memcpy(hb, ls.data(), sb);
+    std::memcpy(hb + sb, lo.data(), ob);
+    CU(cudaMemcpyAsync(ctx->b_bsegs.p, hb, sb, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->b_boff.p, hb + sb, ob, cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+    tsu::SegArgs a{};
+    a.seq = sv;
+    a.pk = pk;
+    a.pkr = pkr;
+    a.segs = P<tsu::BidirSeg>(ctx->b_bsegs);
+    a.n_segs = c;
+    a.pen = rp;
+    a.hist = P<int32_t>(ctx->b_scratch);
+    a.hist_cap = hcap;
+    a.table = P<int32_t>(ctx->b_scratch) + (size_t)(blocks * wpb) * 4 * (size_t)hcap;
+    a.step_cap = scap;
+    a.runs = P<uint32_t>(ctx->b_bruns);
+    a.run_off = P<int64_t>(ctx->b_boff);
+    a.run_len = d_rlen;
+    a.status = d_lst;
+    a.queue = d_queue;
+    tsu::launch_segment((int)blocks, st, a);
+    CU(cudaGetLastError());
+    ctx->timing.kernel_launches++;
+    log += " s" + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" + std::to_string(c);
+    int32_t* h_len = reinterpret_cast<int32_t*>(hb + sb + ob);
+    CU(cudaMemcpyAsync(h_len, d_rlen, 2 * sizeof(int32_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    for (int64_t j = 0; j < c; ++j) {
+      const int64_t i = pick[(size_t)j];
+      const int32_t s = h_len[c + j];
+      lstat[(size_t)i] = s;
+      if (s == tsu::kPairOk) {
+        roff[(size_t)i] = lo[(size_t)j];
+        lcap[(size_t)i] = h_len[j];  // runs written
+      } else if (s == tsu::kPairScratch) {
+        lcap[(size_t)i] = 2 * scap;
+      } else {
+        pst[(size_t)segs[(size_t)i].pair] = s;
+      }
+    }
+    run_total += add;
+  }
+  // join the runs of each pair's leaves
+  if ((rc = host_grow(ctx, ctx->h_bidir,
+                      sizeof(int64_t) * (size_t)(L + n + 1) + sizeof(int32_t) * (size_t)(L + n) + 64)))
+    return rc;
+  {
+    char* hb = static_cast<char*>(ctx->h_bidir.p);
+    int64_t* h_off = reinterpret_cast<int64_t*>(hb);
+    int64_t* h_first = h_off + L;
+    int32_t* h_rl = reinterpret_cast<int32_t*>(h_first + n + 1);
+    int32_t* h_ps = h_rl + L;
+    for (int64_t i = 0; i < L; ++i) {
+      h_off[i] = roff[(size_t)i];
+      h_rl[i] = lstat[(size_t)i] == tsu::kPairOk ? lcap[(size_t)i] : 0;
+    }
+    for (int64_t i = 0; i <= n; ++i) h_first[i] = first[(size_t)i];
+    for (int64_t i = 0; i < n; ++i) h_ps[i] = pst[(size_t)i];
+    if (L) {
+      CU(cudaMemcpyAsync(ctx->b_boff.p, h_off, sizeof(int64_t) * L, cudaMemcpyHostToDevice, st));
+      CU(cudaMemcpyAsync(d_rlen, h_rl, sizeof(int32_t) * L, cudaMemcpyHostToDevice, st));
+    }
+    CU(cudaMemcpyAsync(ctx->b_bfirst.p, h_first, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(d_status, h_ps, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  }
+  if (!ctx->b_bruns.p && (rc = grow(ctx, ctx->b_bruns, 256))) return rc;
+  CU(cudaEventRecord(ctx->ev[5], st));
+  const int rblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
+  int64_t* d_len = P<int64_t>(ctx->b_clen64);
+  tsu::launch_seg_runs(false, rblocks, st, n, P<int64_t>(ctx->b_bfirst), P<int64_t>(ctx->b_boff), d_rlen,
+                       P<uint32_t>(ctx->b_bruns), d_status, d_len, nullptr, nullptr);
+  CU(cudaMemsetAsync(d_len + n, 0, sizeof(int64_t), st));
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, d_len, d_out_off, (int)(n + 1), st);
+  if ((rc = grow(ctx, ctx->b_scan_tmp, tb))) return rc;
+  CU(cub::DeviceScan::ExclusiveSum(ctx->b_scan_tmp.p, tb, d_len, d_out_off, (int)(n + 1), st));
+  int64_t* h_total = reinterpret_cast<int64_t*>(static_cast<char*>(ctx->h_scalars.p) + 32);
+  CU(cudaMemcpyAsync(h_total, d_out_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  char* hc = static_cast<char*>(ctx->h_scalars.p);
+  CU(cudaMemcpyAsync(hc, d_cnt + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(wait_stream(ctx, st));
+  ctx->timing.cells = (int64_t)reinterpret_cast<const unsigned long long*>(hc)[0];
+  ctx->timing.steps = (int64_t)reinterpret_cast<const unsigned long long*>(hc)[1];
+  const int64_t total = *h_total;
+  if (runs_needed) *runs_needed = total;
+  if (!d_out_runs) {
+    DevBuf& ob = out_buf ? *out_buf : ctx->b_out;
+    if ((rc = grow(ctx, ob, sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)))) return rc;
+    d_out_runs = P<uint32_t>(ob);
+    out_cap = total;
+    if (out_used) *out_used = d_out_runs;
+  }
+  if (total > out_cap) return TSU_EOVERFLOW;
+  tsu::launch_seg_runs(true, rblocks, st, n, P<int64_t>(ctx->b_bfirst), P<int64_t>(ctx->b_boff), d_rlen,
+                       P<uint32_t>(ctx->b_bruns), d_status, nullptr, d_out_off, d_out_runs);
+  CU(cudaGetLastError());
+  ctx->timing.kernel_launches += 3;
+  CU(cudaEventRecord(ctx->ev[6], st));
+  ctx->passlog = log;
+  return TSU_OK;
+}
+
 // Core: inputs resident on the device (sv).  Writes score/status (device)
 // and, for CIGARs, compacts runs into out_runs with offsets out_off
 // (device, n+1 entries).  *runs_needed receives the total.
@@ -522,6 +987,13 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
     if (runs_needed) *runs_needed = 0;
     if (want_cigar && d_out_off) CU(cudaMemsetAsync(d_out_off, 0, sizeof(int64_t), st));
     return TSU_OK;
+  }
+  if (ctx->bidir) {
+    if (want_cigar)
+      return run_bidir_cigar(ctx, sv, d_score, d_status, d_out_runs, out_cap, d_out_off, runs_needed, bi, h_plen,
+                             h_tlen, out_used, out_buf);
+    if (runs_needed) *runs_needed = 0;
+    return run_bidir(ctx, sv, d_score, d_status, bi);
   }
   // ---- buffers (all grown before the launch sequence is captured)
   if ((rc = grow(ctx, ctx->b_words_cnt, sizeof(int64_t) * 2 * n))) return rc;
@@ -775,6 +1247,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
           nb.cap = bytes;
           const int64_t keep = std::min<int64_t>((int64_t)used, arena_cap);
           CU(cudaMemcpyAsync(nb.p, ctx->b_arena.p, sizeof(uint32_t) * (size_t)keep, cudaMemcpyDeviceToDevice, st));
+          ctx->peak_held = std::max(ctx->peak_held, ctx->held() + nb.cap);
           release(ctx, ctx->b_arena);
           ctx->b_arena = nb;
           arena_cap = need;
@@ -1196,7 +1669,7 @@ int tsu_destroy(tsu_ctx* ctx) {
   if (ctx->wait_ev) cudaEventDestroy(ctx->wait_ev);
   for (auto& ev : ctx->bev) cudaEventDestroy(ev);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
-  for (HostBuf* hb : {&ctx->h_scalars, &ctx->h_list, &ctx->h_status})
+  for (HostBuf* hb : {&ctx->h_scalars, &ctx->h_list, &ctx->h_status, &ctx->h_bidir})
     if (hb->p) cudaFreeHost(hb->p);
   for (void* p : ctx->h_retired) cudaFreeHost(p);
   if (ctx->h2d_stream && ctx->h2d_stream != ctx->stream) cudaStreamDestroy(ctx->h2d_stream);
@@ -1216,6 +1689,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   if (!ctx || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null result") : TSU_EINVAL;
   const bool want_cigar = !(flags & TSU_SCORE_ONLY);
   ctx->one_warp = (flags & TSU_ONE_WARP) != 0;
+  ctx->bidir = (flags & TSU_BIDIRECTIONAL) != 0;
   if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
   BatchInfo bi;
   int64_t pb = 0, tb = 0;
@@ -1223,6 +1697,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   if (rc) return rc;
   CU(cudaSetDevice(ctx->device));
   ctx->timing = tsu_timing{};
+  ctx->peak_held = ctx->held();
   const int64_t n = bi.n;
   cudaStream_t st = ctx->stream;
   // Pipeline of K chunks of consecutive pairs on three streams: chunk c's
@@ -1358,6 +1833,7 @@ int tsu_align_batch(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, uint32_t 
   ctx->timing.cells = cells;
   ctx->timing.steps = steps;
   ctx->timing.ext_bases = ext_bases;
+  ctx->timing.device_bytes = (int64_t)ctx->peak_held;
   ctx->timing.total_ms = ev_ms(t_begin, t_end);
   ctx->timing.h2d_ms = 0;  // overlapped with the alignment
   ctx->timing.d2h_ms = 0;
@@ -1394,9 +1870,11 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
   if (!ctx || !b || !res || !res->score) return ctx ? set_err(ctx, TSU_EINVAL, "null argument") : TSU_EINVAL;
   const bool want_cigar = !(flags & TSU_SCORE_ONLY);
   ctx->one_warp = (flags & TSU_ONE_WARP) != 0;
+  ctx->bidir = (flags & TSU_BIDIRECTIONAL) != 0;
   if (want_cigar && !res->cigar_offset) return set_err(ctx, TSU_EINVAL, "cigar_offset required");
   CU(cudaSetDevice(ctx->device));
   ctx->timing = tsu_timing{};
+  ctx->peak_held = ctx->held();
   const int64_t n = b->num_pairs;
   if (n < 0 || n > INT32_MAX) return set_err(ctx, TSU_EINVAL, "bad num_pairs");
   cudaStream_t st = ctx->stream;
@@ -1439,6 +1917,7 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* b, tsu_result* res, ui
   ctx->timing.align_ms = n ? ev_ms(ctx->ev[4], ctx->ev[5]) : 0;
   ctx->timing.compact_ms = (n && want_cigar) ? ev_ms(ctx->ev[5], ctx->ev[6]) : 0;
   ctx->timing.total_ms = ev_ms(ctx->ev[0], ctx->ev[7]);
+  ctx->timing.device_bytes = (int64_t)ctx->peak_held;
   // statuses
   std::vector<int32_t> hs((size_t)n);
   if (n) {

@@ -20,7 +20,10 @@ __device__ __forceinline__ uint64_t spread32(uint32_t v) {
 // One warp per sequence; lane l of iteration w looks at byte 32*w + l, so each
 // load instruction of the warp touches 32 consecutive bytes.  The 2-bit code
 // of a base is (c >> 1) & 3 (A=0, C=1, T=2, G=3), a bijection on "ACGT"; any
-// other byte marks the sequence for the byte-compare path.
+// other byte marks the sequence for the byte-compare path.  kRev packs each
+// sequence reversed (base p of the packed form is byte len - 1 - p), for the
+// reverse passes of the bidirectional mode.
+template <bool kRev = false>
 static __global__ void pack_kernel(SeqView sv, PackView pk) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -36,7 +39,7 @@ static __global__ void pack_kernel(SeqView sv, PackView pk) {
     for (int w = 0; w < nw; ++w) {
       const int p = (w << 5) + lane;
       uint32_t c = 0x41;  // 'A' beyond the end (masked by the lengths)
-      if (p < len) c = src[p];
+      if (p < len) c = src[kRev ? len - 1 - p : p];
       const uint32_t code = (c >> 1) & 3u;
       const bool ok = (c == 0x41u) | (c == 0x43u) | (c == 0x47u) | (c == 0x54u);
       bad |= __ballot_sync(0xffffffffu, !ok);
