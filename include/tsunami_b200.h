@@ -64,7 +64,7 @@ extern "C" {
                                   half the wavefront cells of the forward pass; the
                                   same scores.  CIGARs come from the recursion on
                                   crossings down to segments of at most
-                                  max(2 max(x, o+e), 32 g) (g = gcd(x, o, e)),
+                                  max(2 max(x, o+e), 256 g) (g = gcd(x, o, e)),
                                   each aligned with its full history: memory
                                   linear in the score per pair.  WFA2-lib's
                                   ultralow memory mode; the reference keeps the

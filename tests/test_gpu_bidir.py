@@ -83,11 +83,11 @@ def test_bidirectional_argument_checks(oracle):
 
 def base_score(pen):
     """The base score of the recursion in penalty units: segments whose
-    crossing total is at most max(2 max(x, o + e), 32) score units are
+    crossing total is at most max(2 max(x, o + e), 256) score units are
     aligned whole."""
     g = math.gcd(*pen)
     x, go = pen[0] // g, (pen[1] + pen[2]) // g
-    return max(2 * max(x, go), 32) * g
+    return max(2 * max(x, go), 256) * g
 
 
 def _check_cigars(T, oracle, al, pen, pb, po, pl, tb, to, tl):

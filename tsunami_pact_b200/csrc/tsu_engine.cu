@@ -666,8 +666,9 @@ int run_bidir(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d
 // breakpoint launch, and the host cuts each segment at its crossing (k, h)
 // into a left part (begin component, crossing component) and a right part
 // (crossing component, end component) for the next level -- unless the
-// crossing total is at most the base score max(2 max(x, o + e), 32) (score
-// units) or the cut leaves one side empty, when the segment is a leaf.
+// crossing total is at most the base score (tsu::bidir_base: max(2 max(x,
+// o + e), 256) score units) or the cut leaves one side empty, when the
+// segment is a leaf.
 // Leaves, ordered by pair and position, then run through the segment kernel
 // (tsu_segment.cuh) in launches of growing step caps (a leaf that outgrows
 // its launch's history goes to the next), and one thread per pair joins its
@@ -691,7 +692,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   ctx->timing.kernel_launches = 3;
   std::string log;
   CU(cudaEventRecord(ctx->ev[4], st));
-  const int base = std::max(2 * (rp.rm - 1), 32);
+  const int base = tsu::bidir_base(rp);
   std::vector<int32_t> pst((size_t)n, tsu::kPairOk);  // pair statuses
   std::vector<tsu::BidirSeg> cur((size_t)n), next, leaves;
   std::vector<int32_t> leaf_T;
