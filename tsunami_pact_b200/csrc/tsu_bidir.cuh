@@ -122,8 +122,10 @@ __device__ __forceinline__ int bidir_lcp(bool bytes, bool fwd, const uint32_t* p
   return l;
 }
 
+// 128-thread blocks (1- and 4-warp groups): at least 5 per SM (96 registers,
+// no spills; 20 warps per SM).
 template <int GW>
-__global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArgs a) {
+__global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidir_kernel(BidirArgs a) {
 #ifdef TSU_WARP_EMU
   unsigned char* smem_raw = emu::dyn_smem();
 #else
@@ -175,6 +177,11 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
     unsigned long long n_cells = 0, n_steps = 0;
 
     auto L = [&](int d, int s) -> int* { return lim + (d * rm + s % rm) * kBLim; };
+    // slots by index (0..rm-1): the callers keep each direction's current
+    // slot and step back from it, so the hot paths divide by rm nowhere
+    auto LS = [&](int d, int sl) -> int* { return lim + (d * rm + sl) * kBLim; };
+    auto CS = [&](int d, int sl, int c) -> int32_t* { return ring + ((int64_t)(d * rm + sl) * 4 + c) * W + koff; };
+    auto back = [&](int sl, int b) -> int { return sl - b + (sl < b ? rm : 0); };  // slot of b scores before (b < rm)
     auto cells = [&](int d, int s, int c) -> int32_t* {
       return ring + ((int64_t)(d * rm + s % rm) * 4 + c) * W + koff;
     };
@@ -188,15 +195,16 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
       return ((uint32_t)off <= (uint32_t)n) & ((uint32_t)(off - k) <= (uint32_t)m);
     };
 
-    // One wavefront of direction d (0 forward, 1 reverse) at score s.
-    auto compute = [&](int d, int s) {
+    // One wavefront of direction d (0 forward, 1 reverse) at score s, in
+    // ring slot sl (= s mod rm).
+    auto compute = [&](int d, int s, int sl) {
       const int start = d == 0 ? sg.begin : 'M';
       const int forced = d == 0 ? 'M' : sg.end;
-      int* out = L(d, s);
-      int32_t* cM = cells(d, s, kCM);
-      int32_t* cMP = cells(d, s, kCMP);
-      int32_t* cI = cells(d, s, kCI);
-      int32_t* cD = cells(d, s, kCD);
+      int* out = LS(d, sl);
+      int32_t* cM = CS(d, sl, kCM);
+      int32_t* cMP = CS(d, sl, kCMP);
+      int32_t* cI = CS(d, sl, kCI);
+      int32_t* cD = CS(d, sl, kCD);
       if (s == 0) {
         if (gt == 0) {
           if (forced == 'M') {
@@ -228,7 +236,7 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
       int lo = INT_MAX, hi = INT_MIN;
       auto widen = [&](int ss, int c) {
         if (ss < 0) return;
-        const int* l = L(d, ss);
+        const int* l = LS(d, back(sl, s - ss));
         const int plo = l[2 + 2 * c], phi = l[3 + 2 * c];
         if (plo > phi) return;
         lo = min(lo, plo - 1);
@@ -254,13 +262,22 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
       };
       auto src = [&](int ss) -> Src {
         if (ss < 0) return Src{ring, 1, 0};
-        const int* l = L(d, ss);
-        return Src{ring + (int64_t)(d * rm + ss % rm) * 4 * W + koff, l[0], l[1]};
+        const int b = back(sl, s - ss);
+        const int* l = LS(d, b);
+        return Src{CS(d, b, 0), l[0], l[1]};
       };
       const Src SX = src(s - x), SG = src(s - go), SE = src(s - ge);
       auto rd = [&](const Src& S, int c, int k) -> int32_t {
         return (k < S.lo || k > S.hi) ? kBNull : S.base[(int64_t)c * W + k];
       };
+      // this direction's words and the position of its base 0 (packed:
+      // forward (v0, h0), reversed (rv0, rh0); bytes: read forwards from
+      // (v0, h0) or backwards from (v0 + m - 1, h0 + n - 1))
+      const uint32_t* dpw = d == 0 ? fpw : rpw;
+      const uint32_t* dtw = d == 0 ? ftw : rtw;
+      const int dv0 = d == 0 ? sg.v0 : (bytes ? sg.v0 + m - 1 : rv0);
+      const int dh0 = d == 0 ? sg.h0 : (bytes ? sg.h0 + n - 1 : rh0);
+      const int dir = d == 0 || !bytes ? 1 : -1;
       for (int k = lo + gt; k <= hi; k += GT) {
         int32_t ins = max(rd(SG, kCM, k - 1), rd(SE, kCI, k - 1)) + 1;
         if (seed_i && k == 1) ins = max(ins, 1);
@@ -276,9 +293,7 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
         if (inb(pv, k)) {
           const int vv = pv - k;
           const int rem = min(m - vv, n - pv);
-          const int lx = d == 0 ? bidir_lcp(bytes, true, fpw, ftw, pb, tb, sg.v0 + vv, sg.h0 + pv, rem)
-                                : bidir_lcp(bytes, false, rpw, rtw, pb, tb, bytes ? sg.v0 + m - 1 - vv : rv0 + vv,
-                                            bytes ? sg.h0 + n - 1 - pv : rh0 + pv, rem);
+          const int lx = bidir_lcp(bytes, dir > 0, dpw, dtw, pb, tb, dv0 + dir * vv, dh0 + dir * pv, rem);
           cMP[k] = pv;
           cM[k] = pv + lx;
           pm0 = min(pm0, k), pm1 = k;
@@ -358,19 +373,22 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
       }
     };
 
-    auto check = [&](int d_new, int s_new, int s_lo, int s_hi) {
+    // sl_new: slot of s_new; sl_hi: the other side's slot of s_hi.
+    auto check = [&](int d_new, int s_new, int sl_new, int s_lo, int s_hi, int sl_hi) {
       unsigned long long key = ~0ull;
       for (int s2 = s_lo; s2 <= s_hi; ++s2) {
         const int sf = d_new == 0 ? s_new : s2, sr = d_new == 0 ? s2 : s_new;
-        const int* lf = L(0, sf);
-        const int* lr = L(1, sr);
+        const int sl2 = back(sl_hi, s_hi - s2);
+        const int slf = d_new == 0 ? sl_new : sl2, slr = d_new == 0 ? sl2 : sl_new;
+        const int* lf = LS(0, slf);
+        const int* lr = LS(1, slr);
         for (int ci = 0; ci < 3; ++ci) {
           // nothing crosses below an anti-diagonal sum of m + n
           if (lf[8 + ci] + lr[8 + ci] < m + n) continue;
           const int plo = lf[2 + 2 * ci], phi = lf[3 + 2 * ci];
           const int c = ci == 0 ? kCM : (ci == 1 ? kCI : kCD);
-          const int32_t* fc = cells(0, sf, c);
-          const int32_t* rc = cells(1, sr, c);
+          const int32_t* fc = CS(0, slf, c);
+          const int32_t* rc = CS(1, slr, c);
           const int rlo = lr[0], rhi = lr[1];
           for (int k = plo + gt; k <= phi; k += GT) {
             const int32_t hf = fc[k];
@@ -386,11 +404,13 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
           }
         }
       }
-      // group minimum of the 64-bit keys (butterflies: every lane ends with it)
-      for (int sh = 16; sh > 0; sh >>= 1) {
-        const unsigned long long o2 = __shfl_xor_sync(FULL, key, sh);
-        key = o2 < key ? o2 : key;
-      }
+      // group minimum of the 64-bit keys (butterflies: every lane ends with
+      // it; a warp whose lanes found nothing keeps ~0 without them)
+      if (__any_sync(FULL, key != ~0ull))
+        for (int sh = 16; sh > 0; sh >>= 1) {
+          const unsigned long long o2 = __shfl_xor_sync(FULL, key, sh);
+          key = o2 < key ? o2 : key;
+        }
       if constexpr (GW > 1) {
         unsigned long long* kp = reinterpret_cast<unsigned long long*>(part);  // GW words (part holds kBLim GW ints)
         bidir_sync<GW>(gid);
@@ -409,20 +429,22 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>()) bidir_kernel(BidirArg
       bidir_sync<GW>(gid);
     };
     int st = kPairOk;
-    compute(0, 0);
-    compute(1, 0);
-    check(0, 0, 0, 0);
-    int sf = 0, sr = 0;
+    compute(0, 0, 0);
+    compute(1, 0, 0);
+    check(0, 0, 0, 0, 0, 0);
+    int sf = 0, sr = 0, slf = 0, slr = 0;  // scores and their ring slots
     while (sf <= smax) {
       if (have && sf + sr - 2 * mx - oo > bT) break;
       if (sf <= sr) {
         ++sf;
-        compute(0, sf);
-        check(0, sf, max(0, sr - mx), sr);
+        slf = slf + 1 == rm ? 0 : slf + 1;
+        compute(0, sf, slf);
+        check(0, sf, slf, max(0, sr - mx), sr, slr);
       } else {
         ++sr;
-        compute(1, sr);
-        check(1, sr, max(0, sf - mx), sf);
+        slr = slr + 1 == rm ? 0 : slr + 1;
+        compute(1, sr, slr);
+        check(1, sr, slr, max(0, sf - mx), sf, slf);
       }
     }
     if (!have) st = kPairInternal;

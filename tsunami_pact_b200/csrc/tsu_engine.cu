@@ -504,19 +504,6 @@ void carve_scratch(tsu_ctx* ctx, const Pass& ps, bool cigar, tsu::AlignArgs* a) 
 
 // ---- bidirectional mode (TSU_BIDIRECTIONAL) --------------------------------
 
-// Segments of the score-only mode: every pair whole, free at both ends.
-__global__ void bidir_seg_kernel(int64_t n, const int32_t* __restrict__ plen, const int32_t* __restrict__ tlen,
-                                 tsu::BidirSeg* __restrict__ segs) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    segs[i] = tsu::BidirSeg{(int32_t)i, 0, 0, plen[i], tlen[i], 'M', 'M'};
-}
-
-// Scores from the crossing totals (score units).
-__global__ void bidir_score_kernel(int64_t n, const int32_t* __restrict__ T, int g, int32_t* __restrict__ score) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    score[i] = T[i] >= 0 ? T[i] * g : 0;
-}
-
 // Checks of the bidirectional mode's settings.
 int bidir_check(tsu_ctx* ctx) {
   const tsu::Pen& rp = ctx->rp;
@@ -560,19 +547,21 @@ int bidir_pack(tsu_ctx* ctx, const tsu::SeqView& sv, const BatchInfo& bi, tsu::P
   return TSU_OK;
 }
 
+// Warps per segment of the breakpoint kernel by the segment's longest side.
+int bidir_gw(int32_t side) { return side < 2048 ? 1 : (side < 16384 ? 4 : 16); }
+
 // One persistent launch of the breakpoint kernel (tsu_bidir.cuh) over c
-// segments (device), one group per segment at a time (1, 4 or 16 warps by
-// the longest side max_side), both rings of a group in device memory (2
-// directions x ring depth x 4 components x (max_bases + 3) int32, from the
-// scratch buffer).  Writes T, comp, k, h at out, out + c, out + 2c, out + 3c
-// and the statuses; adds cells and steps to d_work[0..1].
+// segments (device) of one size class, one group per segment at a time (gw
+// = 1, 4 or 16 warps), both rings of a group in device memory (2 directions
+// x ring depth x 4 components x (max_bases + 3) int32, from the scratch
+// buffer).  Writes T, comp, k, h at out + 0, out + stride, out + 2 stride,
+// out + 3 stride and the statuses; adds cells and steps to d_work[0..1].
 int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, const tsu::PackView& pkr,
-                const tsu::BidirSeg* segs, int64_t c, int32_t max_side, int32_t max_bases, int32_t* out,
+                const tsu::BidirSeg* segs, int64_t c, int gw, int32_t max_bases, int32_t* out, int64_t stride,
                 int32_t* status, unsigned int* d_queue, unsigned long long* d_work, std::string* log) {
   cudaStream_t st = ctx->stream;
   int rc;
   const tsu::Pen& rp = ctx->rp;
-  const int gw = max_side < 2048 ? 1 : (max_side < 16384 ? 4 : 16);
   const int threads = gw <= 4 ? 128 : 32 * gw;
   const int gpb = threads / (32 * gw);
   const size_t smem = (size_t)gpb * tsu::bidir_group_smem(rp, gw);
@@ -608,9 +597,9 @@ int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, c
   a.ring = P<int32_t>(ctx->b_scratch);
   a.ring_stride = ring_stride;
   a.out_T = out;
-  a.out_comp = out + c;
-  a.out_k = out + 2 * c;
-  a.out_h = out + 3 * c;
+  a.out_comp = out + stride;
+  a.out_k = out + 2 * stride;
+  a.out_h = out + 3 * stride;
   a.status = status;
   a.queue = d_queue;
   a.work = d_work;
@@ -621,33 +610,91 @@ int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, c
   return TSU_OK;
 }
 
+// One breakpoint level over the host segments cur: ordered by size class
+// (16-warp segments first, then 4, then 1; stable, so a class keeps the
+// input order), copied to the device, one launch per class.  Results per
+// segment of the reordered cur: T, comp, k, h at bo + 0, c, 2c, 3c, status
+// at bo + 4c (bo: 5 c int32).
+int bidir_level(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, const tsu::PackView& pkr,
+                std::vector<tsu::BidirSeg>* cur, int32_t* bo, unsigned int* d_queue, unsigned long long* d_work,
+                std::string* log) {
+  cudaStream_t st = ctx->stream;
+  int rc;
+  const int64_t c = (int64_t)cur->size();
+  {
+    // stable partition into the classes 16, 4, 1 warps (three buckets)
+    int64_t cnt[3] = {0, 0, 0};
+    auto cls = [](const tsu::BidirSeg& q) {
+      const int gw = bidir_gw(std::max(q.m, q.n));
+      return gw == 16 ? 0 : (gw == 4 ? 1 : 2);
+    };
+    for (const tsu::BidirSeg& q : *cur) cnt[cls(q)]++;
+    if (cnt[0] + cnt[1] && cnt[1] + cnt[2] && cnt[0] + cnt[2]) {  // more than one class
+      int64_t pos[3] = {0, cnt[0], cnt[0] + cnt[1]};
+      std::vector<tsu::BidirSeg> sorted((size_t)c);
+      for (const tsu::BidirSeg& q : *cur) sorted[(size_t)pos[cls(q)]++] = q;
+      cur->swap(sorted);
+    }
+  }
+  if ((rc = grow(ctx, ctx->b_segs, sizeof(tsu::BidirSeg) * c))) return rc;
+  const size_t seg_bytes = sizeof(tsu::BidirSeg) * (size_t)c;
+  if ((rc = host_grow(ctx, ctx->h_bidir, std::max(seg_bytes, sizeof(int32_t) * 5 * (size_t)c)))) return rc;
+  std::memcpy(ctx->h_bidir.p, cur->data(), seg_bytes);
+  CU(cudaMemcpyAsync(ctx->b_segs.p, ctx->h_bidir.p, seg_bytes, cudaMemcpyHostToDevice, st));
+  const tsu::BidirSeg* d_segs = P<tsu::BidirSeg>(ctx->b_segs);
+  for (int64_t c0 = 0; c0 < c;) {
+    const int gw = bidir_gw(std::max((*cur)[(size_t)c0].m, (*cur)[(size_t)c0].n));
+    int64_t c1 = c0;
+    int32_t max_bases = 0;
+    while (c1 < c && bidir_gw(std::max((*cur)[(size_t)c1].m, (*cur)[(size_t)c1].n)) == gw) {
+      max_bases = std::max(max_bases, (*cur)[(size_t)c1].m + (*cur)[(size_t)c1].n);
+      ++c1;
+    }
+    if ((rc = bidir_split(ctx, sv, pk, pkr, d_segs + c0, c1 - c0, gw, max_bases, bo + c0, c, bo + 4 * c + c0, d_queue,
+                          d_work, log)))
+      return rc;
+    c0 = c1;
+  }
+  return TSU_OK;
+}
+
+// Level 0's results to the pairs: score[pair] = T g (0 when none),
+// status[pair].
+__global__ void bidir_level0_kernel(int64_t c, const tsu::BidirSeg* __restrict__ segs, const int32_t* __restrict__ bo,
+                                    int g, int32_t* __restrict__ score, int32_t* __restrict__ status) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < c; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t p = segs[j].pair;
+    score[p] = bo[j] >= 0 ? bo[j] * g : 0;
+    status[p] = bo[4 * c + j];
+  }
+}
+
 // TSU_BIDIRECTIONAL score-only calls: pack the pairs forward and reversed,
 // then one breakpoint launch over all pairs, each pair whole and free at
 // both ends.  A pair's score is its lowest crossing total; for an
 // end-to-end pair that is the optimal score.
-int run_bidir(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d_status, const BatchInfo& bi) {
+int run_bidir(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d_status, const BatchInfo& bi,
+              const int32_t* h_plen, const int32_t* h_tlen) {
   const int64_t n = sv.n;
   cudaStream_t st = ctx->stream;
   int rc;
   if ((rc = bidir_check(ctx))) return rc;
-  if ((rc = grow(ctx, ctx->b_segs, sizeof(tsu::BidirSeg) * n))) return rc;
-  if ((rc = grow(ctx, ctx->b_bout, sizeof(int32_t) * 4 * n))) return rc;
+  if ((rc = grow(ctx, ctx->b_bout, sizeof(int32_t) * 5 * n))) return rc;
   if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
   tsu::PackView pk, pkr;
   if ((rc = bidir_pack(ctx, sv, bi, &pk, &pkr))) return rc;
-  tsu::BidirSeg* segs = P<tsu::BidirSeg>(ctx->b_segs);
-  const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
-  bidir_seg_kernel<<<eblocks, 256, 0, st>>>(n, sv.pat_len, sv.txt_len, segs);
   unsigned long long* d_cnt = P<unsigned long long>(ctx->b_counters);
   CU(cudaMemsetAsync(d_cnt, 0, 64, st));
   int32_t* bo = P<int32_t>(ctx->b_bout);
-  ctx->timing.kernel_launches = 4;
+  ctx->timing.kernel_launches = 3;
   std::string log;
+  std::vector<tsu::BidirSeg> cur((size_t)n);
+  for (int64_t i = 0; i < n; ++i) cur[(size_t)i] = tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'};
   CU(cudaEventRecord(ctx->ev[4], st));
-  if ((rc = bidir_split(ctx, sv, pk, pkr, segs, n, std::max(bi.max_m, bi.max_n), bi.max_m + bi.max_n, bo, d_status,
-                        reinterpret_cast<unsigned int*>(d_cnt), d_cnt + 1, &log)))
+  if ((rc = bidir_level(ctx, sv, pk, pkr, &cur, bo, reinterpret_cast<unsigned int*>(d_cnt), d_cnt + 1, &log)))
     return rc;
-  bidir_score_kernel<<<eblocks, 256, 0, st>>>(n, bo, ctx->g, d_score);
+  const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
+  bidir_level0_kernel<<<eblocks, 256, 0, st>>>(n, P<tsu::BidirSeg>(ctx->b_segs), bo, ctx->g, d_score, d_status);
   CU(cudaGetLastError());
   ctx->timing.kernel_launches++;
   CU(cudaEventRecord(ctx->ev[5], st));
@@ -699,28 +746,15 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   for (int64_t i = 0; i < n; ++i) cur[(size_t)i] = tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'};
   for (int level = 0; !cur.empty(); ++level) {
     const int64_t c = (int64_t)cur.size();
-    int32_t max_side = 0, max_bases = 0;
-    for (const tsu::BidirSeg& s : cur) {
-      max_side = std::max(max_side, std::max(s.m, s.n));
-      max_bases = std::max(max_bases, s.m + s.n);
-    }
-    if ((rc = grow(ctx, ctx->b_segs, sizeof(tsu::BidirSeg) * c))) return rc;
-    if ((rc = grow(ctx, ctx->b_bout, sizeof(int32_t) * 5 * c))) return rc;
-    const size_t seg_bytes = sizeof(tsu::BidirSeg) * (size_t)c, res_bytes = sizeof(int32_t) * 5 * (size_t)c;
-    if ((rc = host_grow(ctx, ctx->h_bidir, std::max(seg_bytes, res_bytes)))) return rc;
-    std::memcpy(ctx->h_bidir.p, cur.data(), seg_bytes);
-    CU(cudaMemcpyAsync(ctx->b_segs.p, ctx->h_bidir.p, seg_bytes, cudaMemcpyHostToDevice, st));
+    const size_t res_bytes = sizeof(int32_t) * 5 * (size_t)c;
+    if ((rc = grow(ctx, ctx->b_bout, res_bytes))) return rc;
     int32_t* bo = P<int32_t>(ctx->b_bout);
-    int32_t* bst = level == 0 ? d_status : bo + 4 * c;
-    if ((rc = bidir_split(ctx, sv, pk, pkr, P<tsu::BidirSeg>(ctx->b_segs), c, max_side, max_bases, bo, bst, d_queue,
-                          d_cnt + 1, &log)))
-      return rc;
+    if ((rc = bidir_level(ctx, sv, pk, pkr, &cur, bo, d_queue, d_cnt + 1, &log))) return rc;
     if (level == 0) {
       const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
-      bidir_score_kernel<<<eblocks, 256, 0, st>>>(n, bo, ctx->g, d_score);
+      bidir_level0_kernel<<<eblocks, 256, 0, st>>>(n, P<tsu::BidirSeg>(ctx->b_segs), bo, ctx->g, d_score, d_status);
       CU(cudaGetLastError());
       ctx->timing.kernel_launches++;
-      CU(cudaMemcpyAsync(bo + 4 * c, d_status, sizeof(int32_t) * c, cudaMemcpyDeviceToDevice, st));
     }
     CU(cudaMemcpyAsync(ctx->h_bidir.p, bo, res_bytes, cudaMemcpyDeviceToHost, st));
     CU(wait_stream(ctx, st));
@@ -994,7 +1028,7 @@ int run_device(tsu_ctx* ctx, const tsu::SeqView& sv, bool want_cigar, int32_t* d
       return run_bidir_cigar(ctx, sv, d_score, d_status, d_out_runs, out_cap, d_out_off, runs_needed, bi, h_plen,
                              h_tlen, out_used, out_buf);
     if (runs_needed) *runs_needed = 0;
-    return run_bidir(ctx, sv, d_score, d_status, bi);
+    return run_bidir(ctx, sv, d_score, d_status, bi, h_plen, h_tlen);
   }
   // ---- buffers (all grown before the launch sequence is captured)
   if ((rc = grow(ctx, ctx->b_words_cnt, sizeof(int64_t) * 2 * n))) return rc;
