@@ -121,7 +121,7 @@ int main() {
     int32_t bases = 0;
     for (auto& sg : segs) bases = std::max(bases, sg.m + sg.n);
     const int64_t hcap = tsu::seg_hist_cap(step_cap, bases);
-    Buf<int32_t> hist((size_t)(warps * 4 * hcap)), table((size_t)warps * 9 * step_cap);
+    Buf<int32_t> hist((size_t)(warps * 3 * hcap)), table((size_t)warps * 9 * step_cap);
     Buf<int64_t> roff(N);
     int64_t rtot = 0;
     for (int64_t i = 0; i < N; ++i) {

@@ -484,7 +484,7 @@ struct SegArgs {
   const BidirSeg* segs;
   int64_t n_segs;
   Pen pen;
-  int32_t* hist;          // per warp: hist_cap x 4 int32
+  int32_t* hist;          // per warp: hist_cap x 3 int32 (M, I, D)
   int64_t hist_cap;
   int32_t* table;         // per warp: step_cap x 9 int32
   int32_t step_cap;
@@ -504,9 +504,9 @@ __host__ __device__ inline int64_t seg_run_cap(const Pen& p, int64_t bases, int 
   return bases < b ? (bases > 0 ? bases : 1) : b;
 }
 
-// History cells a warp needs for step_cap steps of segments whose m + n is
-// at most bases: the wavefront at score s spans at most 2 s + 1 diagonals,
-// and never more than m + n + 3.
+// History cells (3 int32 each) a warp needs for step_cap steps of segments
+// whose m + n is at most bases: the wavefront at score s spans at most
+// 2 s + 1 diagonals, and never more than m + n + 3.
 __host__ __device__ inline int64_t seg_hist_cap(int step_cap, int64_t bases) {
   int64_t c = 0;
   for (int s = 0; s < step_cap; ++s) c += (2 * (int64_t)s + 3 < bases + 3) ? 2 * (int64_t)s + 3 : bases + 3;

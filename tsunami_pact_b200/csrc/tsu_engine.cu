@@ -872,7 +872,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     }
     // per-warp history and step table
     const int64_t hcap = tsu::seg_hist_cap(scap, bases);
-    const size_t per_warp = sizeof(int32_t) * (size_t)(4 * hcap + 9 * (int64_t)scap);
+    const size_t per_warp = sizeof(int32_t) * (size_t)(3 * hcap + 9 * (int64_t)scap);
     const int wpb = tsu::kSegThreads / 32;
     int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
     const size_t fixed = ctx->held() - ctx->b_scratch.cap;
@@ -905,7 +905,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     a.pen = rp;
     a.hist = P<int32_t>(ctx->b_scratch);
     a.hist_cap = hcap;
-    a.table = P<int32_t>(ctx->b_scratch) + (size_t)(blocks * wpb) * 4 * (size_t)hcap;
+    a.table = P<int32_t>(ctx->b_scratch) + (size_t)(blocks * wpb) * 3 * (size_t)hcap;
     a.step_cap = scap;
     a.runs = P<uint32_t>(ctx->b_bruns);
     a.run_off = P<int64_t>(ctx->b_boff);

@@ -17,9 +17,10 @@
 // > I extend 2 > I open 1; the forced first gap opens from the empty origin.
 //
 // One warp per segment, persistent over a work queue.  Per warp in device
-// memory: the history (hist_cap cells of 4 int32: M, M before extension,
-// I, D) and the step table (step_cap rows: lo, hi, first history cell, and
-// the first / last present diagonal of M, I, D).  A segment that needs more
+// memory: the history (hist_cap cells of 3 int32: M, I, D; the backtrace
+// never reads M before extension, so it is not kept) and the step table
+// (step_cap rows: lo, hi, first history cell, and the first / last present
+// diagonal of M, I, D).  A segment that needs more
 // steps or cells than the launch gives gets status kPairScratch and runs
 // again in a launch with more.  Runs (length << 4 | kOp*) go to the
 // segment's region of the run buffer, at most seg_run_cap of them: a
@@ -33,11 +34,12 @@ namespace tsu {
 
 __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
   constexpr unsigned FULL = 0xffffffffu;
+  constexpr int hM = 0, hI = 1, hD = 2;  // components of a history cell
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const Pen pen = a.pen;
   const int x = pen.x, go = pen.go, ge = pen.ge, oo = pen.go - pen.ge;
-  int32_t* const hist = a.hist + gwarp * a.hist_cap * 4;
+  int32_t* const hist = a.hist + gwarp * a.hist_cap * 3;
   int32_t* const tab = a.table + gwarp * (int64_t)a.step_cap * 9;
   for (;;) {
     unsigned q = 0;
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       if (s < 0) return kBNull;
       const int32_t* t = tab + (int64_t)s * 9;
       if (k < t[0] || k > t[1]) return kBNull;
-      return hist[((int64_t)t[2] + (k - t[0])) * 4 + c];
+      return hist[((int64_t)t[2] + (k - t[0])) * 3 + c];
     };
     int st = kPairOk;
     int64_t used = 0;  // history cells in use
@@ -113,32 +115,44 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         st = kPairScratch;
         break;
       }
-      int32_t* row = hist + used * 4;
+      int32_t* row = hist + used * 3;
       int pm0 = INT_MAX, pm1 = INT_MIN, pi0 = INT_MAX, pi1 = INT_MIN, pd0 = INT_MAX, pd1 = INT_MIN;
+      // the source rows (s - x, s - o - e, s - e), resolved once per step
+      struct Row {
+        const int32_t* base;  // cell of diagonal k at base + 3 (k - lo)
+        int lo, hi;
+      };
+      auto row_of = [&](int ss) -> Row {
+        if (ss < 0 || s == 0) return Row{hist, 1, 0};
+        const int32_t* t = tab + (int64_t)ss * 9;
+        return Row{hist + (int64_t)t[2] * 3, t[0], t[1]};
+      };
+      const Row RX = row_of(s - x), RG = row_of(s - go), RE = row_of(s - ge);
+      auto rd = [&](const Row& R, int c, int k) -> int32_t {
+        return (k < R.lo || k > R.hi) ? kBNull : R.base[(int64_t)(k - R.lo) * 3 + c];
+      };
       for (int k = lo + lane; k <= hi; k += 32) {
-        int32_t cm = kBNull, cmp = kBNull, ci = kBNull, cd = kBNull;
+        int32_t cm = kBNull, ci = kBNull, cd = kBNull;
         if (s == 0) {
-          cmp = 0;
           cm = lcp(0, 0, min(m, n));
           ci = start == 'I' ? 0 : kBNull;
           cd = start == 'D' ? 0 : kBNull;
         } else {
-          int32_t ins = max(get(s - go, kCM, k - 1), get(s - ge, kCI, k - 1)) + 1;
+          int32_t ins = max(rd(RG, hM, k - 1), rd(RE, hI, k - 1)) + 1;
           if (seed_i && k == 1) ins = max(ins, 1);
-          int32_t del = max(get(s - go, kCM, k + 1), get(s - ge, kCD, k + 1));
+          int32_t del = max(rd(RG, hM, k + 1), rd(RE, hD, k + 1));
           if (seed_d && k == -1) del = max(del, 0);
-          const int32_t mis = get(s - x, kCM, k) + 1;
+          const int32_t mis = rd(RX, hM, k) + 1;
           if (inb(ins, k)) ci = ins;
           if (inb(del, k)) cd = del;
           const int32_t pv = max(mis, max(ins, del));
           if (inb(pv, k)) {
             const int vv = pv - k;
-            cmp = pv;
             cm = pv + lcp(vv, pv, min(m - vv, n - pv));
           }
         }
-        int32_t* cell = row + (int64_t)(k - lo) * 4;
-        cell[kCM] = cm, cell[kCMP] = cmp, cell[kCI] = ci, cell[kCD] = cd;
+        int32_t* cell = row + (int64_t)(k - lo) * 3;
+        cell[hM] = cm, cell[hI] = ci, cell[hD] = cd;
         if (cm != kBNull) pm0 = min(pm0, k), pm1 = k;
         if (ci != kBNull) pi0 = min(pi0, k), pi1 = k;
         if (cd != kBNull) pd0 = min(pd0, k), pd1 = k;
@@ -158,9 +172,9 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       }
       __syncwarp();
       used += width;
-      if (get(s, kCM, k_end) >= n && (!have || s < best)) have = 1, best = s, s_end = s, state = 'M';
+      if (get(s, hM, k_end) >= n && (!have || s < best)) have = 1, best = s, s_end = s, state = 'M';
       if (free_end == 'I' || free_end == 'D') {
-        const int32_t gv = get(s, free_end == 'I' ? kCI : kCD, k_end);
+        const int32_t gv = get(s, free_end == 'I' ? hI : hD, k_end);
         if (gv == n && (!have || s - oo < best)) have = 1, best = s - oo, s_end = s, state = free_end;
       }
     }
@@ -196,18 +210,18 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         return (long long)(v + delta) * 16 + code;
       };
       int s2 = s_end, k = k_end;
-      int32_t off = get(s_end, state == 'M' ? kCM : (state == 'I' ? kCI : kCD), k_end);
+      int32_t off = get(s_end, state == 'M' ? hM : (state == 'I' ? hI : hD), k_end);
       int v = off - k, h = off;
       while (v > 0 && h > 0 && s2 > 0) {
-        long long io = bsrc(s2 - go, kCM, k - 1, 1, 1);
-        const long long ix = bsrc(s2 - ge, kCI, k - 1, 1, 2);
-        long long dop = bsrc(s2 - go, kCM, k + 1, 0, 5);
-        const long long dx = bsrc(s2 - ge, kCD, k + 1, 0, 6);
+        long long io = bsrc(s2 - go, hM, k - 1, 1, 1);
+        const long long ix = bsrc(s2 - ge, hI, k - 1, 1, 2);
+        long long dop = bsrc(s2 - go, hM, k + 1, 0, 5);
+        const long long dx = bsrc(s2 - ge, hD, k + 1, 0, 6);
         if (forced == 'I' && s2 == go && k == 1) io = max(io, 1ll * 16 + 1);
         if (forced == 'D' && s2 == go && k == -1) dop = max(dop, 0ll * 16 + 5);
         long long b;
         if (state == 'M')
-          b = max(bsrc(s2 - x, kCM, k, 1, 9), max(max(io, ix), max(dop, dx)));
+          b = max(bsrc(s2 - x, hM, k, 1, 9), max(max(io, ix), max(dop, dx)));
         else if (state == 'I')
           b = max(io, ix);
         else
