@@ -157,3 +157,29 @@ def test_predict_is_enough():
                 s1 = tight.align_arrays(pbuf, poff, plen, tbuf, toff, tlen)[0]
             s0 = al.align_arrays(pbuf, poff, plen, tbuf, toff, tlen)[0]
             assert np.array_equal(s0, s1)
+
+
+def test_bidirectional_requests(aligner_factory):
+    """Requests with TSU_BIDIRECTIONAL, mixed with plain ones: every
+    bidirectional result equals the batch path's bidirectional one on the
+    same pairs, every plain result the plain one (requests of different
+    flags never share a job); an edit-distance server fails them with
+    TSU_EINVAL."""
+    import tsunami_pact_b200 as T
+
+    reqs = _requests(12, 48, index=3, cap_len=12_000)
+    al = aligner_factory((4, 6, 2))
+    with T.Server(4, 6, 2, workers=4, mem_budget=32 << 30) as srv:
+        ids = [srv.submit_arrays(*r, cigar=(k % 3 != 2), bidirectional=(k % 2 == 0)) for k, r in enumerate(reqs)]
+        got = _collect(srv, ids)
+    for k, (r, g) in enumerate(zip(reqs, got)):
+        cig, bi = k % 3 != 2, k % 2 == 0
+        s, c, runs = al.align_arrays(*r, cigar=cig, bidirectional=bi)
+        assert np.array_equal(g[0][: len(s)], s), k
+        if cig:
+            assert np.array_equal(g[1], c), k
+            assert np.array_equal(g[2][: int(c[-1])], runs), k
+    with T.Server(device=0, metric="edit", workers=1) as srv:
+        rid = srv.submit_arrays(*reqs[0], bidirectional=True)
+        with pytest.raises(T.AlignError):
+            srv.wait(rid, 600_000)

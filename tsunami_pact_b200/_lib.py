@@ -432,7 +432,10 @@ class Server:
         L = lib()
         return AlignError(rc, f"{L.tsu_status_str(rc).decode()}: {L.tsu_server_last_error(self._h).decode()}")
 
-    def submit_arrays(self, pbuf, poff, plen, tbuf, toff, tlen, cigar: bool = True) -> int:
+    def submit_arrays(self, pbuf, poff, plen, tbuf, toff, tlen, cigar: bool = True,
+                      bidirectional: bool = False) -> int:
+        """Submit one request (tsu_submit); ``bidirectional=True``:
+        TSU_BIDIRECTIONAL (one-piece gap-affine servers)."""
         n = len(plen)
         poff = np.ascontiguousarray(poff, dtype=np.int64)
         toff = np.ascontiguousarray(toff, dtype=np.int64)
@@ -440,19 +443,20 @@ class Server:
         tlen = np.ascontiguousarray(tlen, dtype=np.int32)
         b = Batch(n, _ptr(pbuf), _ptr(poff), _ptr(plen), _ptr(tbuf), _ptr(toff), _ptr(tlen))
         rid = ctypes.c_uint64()
-        rc = lib().tsu_submit(self._h, ctypes.byref(b), 0 if cigar else TSU_SCORE_ONLY, ctypes.byref(rid))
+        flags = (0 if cigar else TSU_SCORE_ONLY) | (TSU_BIDIRECTIONAL if bidirectional else 0)
+        rc = lib().tsu_submit(self._h, ctypes.byref(b), flags, ctypes.byref(rid))
         if rc != TSU_OK:
             raise self._err(rc)
         cap = int(plen.astype(np.int64).sum() + tlen.astype(np.int64).sum()) + 1
         self._cigar[rid.value] = (cigar, n, cap)
         return rid.value
 
-    def submit(self, patterns: Sequence, texts: Sequence, cigar: bool = True) -> int:
+    def submit(self, patterns: Sequence, texts: Sequence, cigar: bool = True, bidirectional: bool = False) -> int:
         if len(patterns) != len(texts):
             raise ValueError("patterns and texts differ in length")
         pb, po, pl = _concat(patterns)
         tb, to, tl = _concat(texts)
-        return self.submit_arrays(pb, po, pl, tb, to, tl, cigar=cigar)
+        return self.submit_arrays(pb, po, pl, tb, to, tl, cigar=cigar, bidirectional=bidirectional)
 
     def _take(self, rid: int, timeout_ms: Optional[float]):
         cig, n, cap = self._cigar[rid]

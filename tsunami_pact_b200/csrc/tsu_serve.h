@@ -258,7 +258,7 @@ class Server {
     }
     auto r = std::make_shared<Request>();
     r->t_submit = Clock::now();
-    r->flags = flags & TSU_SCORE_ONLY;
+    r->flags = flags & (TSU_SCORE_ONLY | TSU_BIDIRECTIONAL);
     r->in.assign(*b);
     // parts: each heavy pair alone (longest first), then the light pairs
     std::vector<PartPtr> parts;
@@ -295,7 +295,9 @@ class Server {
       }
       const int rc = predict_parts({p}, p->flags, p->hint, &p->full, &p->min);
       if (rc) return rc;
-      if (p->min > cfg_.budget && !(p->flags & TSU_SCORE_ONLY)) {
+      // too big for the budget: CIGARs with checkpointed history instead
+      // (the bidirectional mode keeps no history to checkpoint)
+      if (p->min > cfg_.budget && !(p->flags & (TSU_SCORE_ONLY | TSU_BIDIRECTIONAL))) {
         size_t full2 = 0, min2 = 0;
         if (predict_parts({p}, p->flags | kLowMem, p->hint, &full2, &min2) == TSU_OK && min2 <= cfg_.budget) {
           p->flags |= kLowMem;

@@ -131,7 +131,7 @@ class EngineExecutor final : public tsu::serve::Executor {
       r.cigar_capacity = cap;
       r.cigar_offset = reinterpret_cast<int64_t*>(ho + o_coff);
     }
-    const int rc = tsu_align_batch(ctx_, &b, &r, flags & TSU_SCORE_ONLY);
+    const int rc = tsu_align_batch(ctx_, &b, &r, flags & (TSU_SCORE_ONLY | TSU_BIDIRECTIONAL));
     out->score.assign(h_score, h_score + n);
     out->pair_status.assign(h_status, h_status + n);
     if (rc == TSU_OK && cig) {
