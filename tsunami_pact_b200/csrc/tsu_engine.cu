@@ -1424,6 +1424,61 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
   // buffers of the whole call (tsu_align_batch)
   size_t call = r((size_t)sh.pattern_bytes) + r((size_t)sh.text_bytes) + 2 * r(8 * (size_t)n) +
                 4 * r(4 * (size_t)n) + (want_cigar ? r(8 * (size_t)(n + K + 1)) : 0);
+  if (flags & TSU_BIDIRECTIONAL) {
+    // bidirectional mode, per chunk: packing forward and reversed, a level's
+    // segments and cuts, for CIGARs the leaves' bookkeeping and runs (at most
+    // m + n per pair); scratch: the breakpoint rings of the largest size
+    // class (groups x 2 directions x ring depth x 4 x (m + n + 3) int32) or
+    // the leaf warps' history at the base step cap, whichever is larger
+    const tsu::Pen& rp = ctx->rp;
+    size_t chunk_max = 0, scratch_full = 0, scratch_min = 0;
+    const int cap0 = tsu::bidir_base(rp) + 2 * rp.go + 4;
+    for (int c = 0; c < K; ++c) {
+      const int64_t c0 = n * c / K, nc = n * (c + 1) / K - c0;
+      if (nc == 0) continue;
+      int64_t words = 0, len_sum = 0;
+      int32_t cls_bases[3] = {0, 0, 0};
+      int64_t cls_n[3] = {0, 0, 0};
+      for (int64_t i = 0; i < nc; ++i) {
+        const int32_t m = sh.plen[c0 + i], t = sh.tlen[c0 + i];
+        words += tsu::packed_words(m) + tsu::packed_words(t);
+        len_sum += (int64_t)m + t;
+        const int gw = bidir_gw(std::max(m, t)), k = gw == 1 ? 0 : (gw == 4 ? 1 : 2);
+        cls_bases[k] = std::max(cls_bases[k], m + t);
+        cls_n[k]++;
+      }
+      size_t f = 2 * r(16 * (size_t)nc) + 2 * r(8 * (size_t)words) + 2 * r(2 * (size_t)nc) +
+                 r(sizeof(tsu::BidirSeg) * (size_t)nc) + r(20 * (size_t)nc) + r(64) + r(scan_tmp(2 * nc));
+      if (want_cigar) {
+        // leaves per pair: about 2 T / base for a crossing total T, here
+        // the hint's score of the longest pair
+        const int32_t maxb = std::max(cls_bases[0], std::max(cls_bases[1], cls_bases[2]));
+        const int64_t leaves =
+            nc * std::max<int64_t>(1, 2 * tsu::hint_score(rp, std::max(1, maxb / 2), hint) / tsu::bidir_base(rp));
+        f += 2 * r(8 * (size_t)(nc + 1)) + r(sizeof(tsu::BidirSeg) * (size_t)leaves) + r(16 * (size_t)leaves) +
+             2 * r(4 * (size_t)(len_sum + 1)) + r(scan_tmp(nc + 1));
+      }
+      chunk_max = std::max(chunk_max, f);
+      const int gws[3] = {1, 4, 16};
+      for (int k = 0; k < 3; ++k) {
+        if (!cls_n[k]) continue;
+        const size_t ring = sizeof(int32_t) * 2 * (size_t)rp.rm * 4 * ((size_t)cls_bases[k] + 3);
+        const int64_t groups = std::min<int64_t>(cls_n[k], (int64_t)ctx->sms * (gws[k] <= 4 ? 5 * (4 / gws[k]) : 1));
+        scratch_full = std::max(scratch_full, (size_t)groups * ring);
+        scratch_min = std::max(scratch_min, ring);
+      }
+      if (want_cigar) {
+        const int32_t bases = std::max(cls_bases[0], std::max(cls_bases[1], cls_bases[2]));
+        const size_t per_warp = sizeof(int32_t) * (size_t)(3 * tsu::seg_hist_cap(cap0, bases) + 9 * (int64_t)cap0);
+        scratch_full = std::max(scratch_full, per_warp * (size_t)std::min<int64_t>(nc, (int64_t)ctx->sms * 24));
+        scratch_min = std::max(scratch_min, per_warp * 4);
+      }
+    }
+    const size_t slack = 64 << 10;
+    *full = call + chunk_max + scratch_full + slack;
+    *min = call + chunk_max + scratch_min + slack;
+    return TSU_OK;
+  }
   // buffers of a chunk (run_device): reused chunk after chunk, so the largest
   // chunk sets them; scratch: the largest first pass of any band
   size_t chunk_max = 0, scratch_full = 0, scratch_min = 0;

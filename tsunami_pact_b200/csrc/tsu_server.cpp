@@ -83,7 +83,7 @@ class EngineExecutor final : public tsu::serve::Executor {
     sh.text_bytes = tb;
     tsu::engine::set_fit_start(ctx_, (flags & tsu::serve::kFitStart) != 0);
     tsu_set_low_memory(ctx_, (flags & tsu::serve::kLowMem) ? -1 : 0);
-    return tsu::engine::predict_bytes(ctx_, sh, flags & TSU_SCORE_ONLY, hint, full, min);
+    return tsu::engine::predict_bytes(ctx_, sh, flags & (TSU_SCORE_ONLY | TSU_BIDIRECTIONAL), hint, full, min);
   }
   size_t held() override { return tsu::engine::held_bytes(ctx_); }
   void set_budget(size_t bytes) override { tsu::engine::set_budget(ctx_, bytes); }
