@@ -98,18 +98,19 @@ def test_segments_match_oracle(emu_bidir, oracle, pen, gw):
     _check(emu_bidir, oracle, recs, pen, gw)
 
 
-def test_sub_ranges_and_non_acgt(emu_bidir, oracle):
+@pytest.mark.parametrize("gw", [1, 4])
+def test_sub_ranges_and_non_acgt(emu_bidir, oracle, gw):
     """Segments inside longer pairs (the recursion's halves), and pairs with
     bytes outside ACGT (compared byte by byte)."""
-    rng = random.Random(5)
+    rng = random.Random(5 + gw)
     recs = []
-    for i in range(40):
+    for i in range(40 if gw == 1 else 16):
         alpha = "ACGTN" if i % 4 == 0 else "ACGT"
         p, t = _edited(rng, rng.randint(20, 300), 0.08, alpha)
         v0, h0 = rng.randint(0, len(p) // 2), rng.randint(0, len(t) // 2)
         sm, sn = rng.randint(0, len(p) - v0), rng.randint(0, len(t) - h0)
         recs.append((p, t, rng.choice("MID"), rng.choice("MID"), (v0, h0, sm, sn)))
-    _check(emu_bidir, oracle, recs, (4, 6, 2), 1)
+    _check(emu_bidir, oracle, recs, (4, 6, 2), gw)
 
 
 def test_long_segments_warp_group(emu_bidir, oracle):

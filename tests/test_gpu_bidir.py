@@ -104,7 +104,7 @@ def _check_cigars(T, oracle, al, pen, pb, po, pl, tb, to, tl):
         assert oracle.cigar_cost(ops, p, t, *pen) == want[i]
 
 
-@pytest.mark.parametrize("pen", [(4, 6, 2), (3, 5, 1), (5, 11, 3)])
+@pytest.mark.parametrize("pen", [(4, 6, 2), (3, 5, 1), (5, 11, 3), (20, 1, 1)])
 def test_bidirectional_cigars_equal_the_oracle(aligner_factory, oracle, pen):
     import tsunami_pact_b200 as T
 
