@@ -12,7 +12,9 @@
 // Output (stdout): gw 1, 4, 16 (breakpoint kernel): per segment
 //                  "T comp k h" (T in penalty units, -1: none); gw 0
 //                  (segment kernel, one block of 4 warps, step_cap steps):
-//                  per segment "status ops" (ops '-' when empty)
+//                  per segment "status ops" (ops '-' when empty), then
+//                  "retries K": segments that found the (deliberately
+//                  small) run arena full and ran again
 #include "warp_emu.h"
 // clang-format off
 #include "../../tsunami_pact_b200/csrc/tsu_kernels.cuh"
@@ -121,16 +123,20 @@ int main() {
     int32_t bases = 0;
     for (auto& sg : segs) bases = std::max(bases, sg.m + sg.n);
     const int64_t hcap = tsu::seg_hist_cap(step_cap, bases);
+    const int64_t wcap = tsu::seg_run_cap(rp, bases, step_cap);
     Buf<int32_t> hist((size_t)(warps * 3 * hcap)), table((size_t)warps * 9 * step_cap);
-    Buf<int64_t> roff(N);
+    Buf<uint32_t> wruns((size_t)(warps * wcap));
+    // an arena too small for every segment's runs at once: some segments
+    // report kPairArena (2) and run again with a larger one
     int64_t rtot = 0;
-    for (int64_t i = 0; i < N; ++i) {
-      roff.p[i] = rtot;
-      rtot += tsu::seg_run_cap(rp, (int64_t)segs[i].m + segs[i].n, step_cap);
-    }
+    for (int64_t i = 0; i < N; ++i) rtot += tsu::seg_run_cap(rp, (int64_t)segs[i].m + segs[i].n, step_cap);
+    const int64_t small_cap = std::min<int64_t>(rtot, 24);
     Buf<uint32_t> runs(std::max<int64_t>(rtot, 1));
+    Buf<int64_t> roff(N);
     Buf<int32_t> rlen(N), sst(N);
     Buf<unsigned> queue(1);
+    Buf<unsigned long long> cursor(1);
+    int64_t retries = 0;
     Buf<tsu::BidirSeg> dsegs(N);
     std::memcpy(dsegs.p, segs.data(), sizeof(tsu::BidirSeg) * N);
     tsu::SegArgs a{};
@@ -140,16 +146,49 @@ int main() {
     a.segs = dsegs.p;
     a.n_segs = N;
     a.pen = rp;
+    a.g = g;
     a.hist = hist.p;
     a.hist_cap = hcap;
     a.table = table.p;
     a.step_cap = step_cap;
+    a.wruns = wruns.p;
+    a.wruns_cap = wcap;
     a.runs = runs.p;
+    a.runs_cap = small_cap;
+    a.cursor = cursor.p;
     a.run_off = roff.p;
     a.run_len = rlen.p;
     a.status = sst.p;
     a.queue = queue.p;
     emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel(a); });
+    // the segments that found the arena full, again with room for all
+    {
+      std::vector<int64_t> again;
+      for (int64_t i = 0; i < N; ++i)
+        if (sst.p[i] == tsu::kPairArena) again.push_back(i);
+      retries = (int64_t)again.size();
+      if (!again.empty()) {
+        Buf<tsu::BidirSeg> rsegs(again.size());
+        for (size_t j = 0; j < again.size(); ++j) rsegs.p[j] = segs[(size_t)again[j]];
+        Buf<int64_t> roff2(again.size());
+        Buf<int32_t> rlen2(again.size()), sst2(again.size());
+        queue.p[0] = 0;
+        cursor.p[0] = std::min<unsigned long long>(cursor.p[0], (unsigned long long)small_cap);
+        tsu::SegArgs b = a;
+        b.segs = rsegs.p;
+        b.n_segs = (int64_t)again.size();
+        b.runs_cap = rtot;
+        b.run_off = roff2.p;
+        b.run_len = rlen2.p;
+        b.status = sst2.p;
+        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel(b); });
+        for (size_t j = 0; j < again.size(); ++j) {
+          roff.p[again[j]] = roff2.p[j];
+          rlen.p[again[j]] = rlen2.p[j];
+          sst.p[again[j]] = sst2.p[j];
+        }
+      }
+    }
     for (int64_t i = 0; i < N; ++i) {
       std::string ops;
       if (sst.p[i] == tsu::kPairOk) {
@@ -161,6 +200,7 @@ int main() {
       }
       std::printf("%d %s\n", sst.p[i], ops.empty() ? "-" : ops.c_str());
     }
+    std::printf("retries %lld\n", (long long)retries);
     return 0;
   }
   const int threads = GW <= 4 ? 128 : 32 * GW;

@@ -119,12 +119,14 @@ def test_long_segments_warp_group(emu_bidir, oracle):
     _check(emu_bidir, oracle, recs, (4, 6, 2), 16)
 
 
-def _seg_ops(exe, recs, pen, step_cap):
+def _seg_ops(exe, recs, pen, step_cap, retries=None):
     out = []
     lines = _run(exe, _input(recs, f"{pen[0]} {pen[1]} {pen[2]} 0 {len(recs)} {step_cap}\n"))
     for ln in lines[: len(recs)]:
         st, ops = ln.split()
         out.append((int(st), "" if ops == "-" else ops))
+    if retries is not None:
+        retries.append(int(lines[len(recs)].split()[1]))
     return out
 
 
@@ -133,7 +135,9 @@ def test_base_case_segments_match_oracle(emu_bidir, oracle, pen):
     """The base-case kernel (tsu_segment.cuh): every segment's operations
     equal the oracle's segment alignment (ora_align_segment) for every begin
     and end component, whole pairs, sub-ranges and bytes outside ACGT; a
-    step cap below what a segment needs gives status 1 (more scratch)."""
+    step cap below what a segment needs gives status 1 (more scratch); a
+    run arena too small gives status 2 and the segment's second run, with
+    room, the same operations."""
     rng = random.Random(hash(pen) & 0xFFFF)
     recs = []
     for i in range(36):
@@ -146,7 +150,9 @@ def test_base_case_segments_match_oracle(emu_bidir, oracle, pen):
         recs.append((p, t, rng.choice("MID"), rng.choice("MID"), sub))
     g = math.gcd(*pen)
     step_cap = 400
-    got = _seg_ops(emu_bidir, recs, pen, step_cap)
+    retries = []
+    got = _seg_ops(emu_bidir, recs, pen, step_cap, retries)
+    assert retries[0] > 0  # the arena of 24 runs cannot hold them all
     compared = 0
     for (p, t, b, e, sub), (st, ops) in zip(recs, got):
         if sub:

@@ -484,23 +484,33 @@ struct SegArgs {
   const BidirSeg* segs;
   int64_t n_segs;
   Pen pen;
+  int g;                  // score unit
   int32_t* hist;          // per warp: hist_cap x 3 int32 (M, I, D)
   int64_t hist_cap;
   int32_t* table;         // per warp: step_cap x 9 int32
   int32_t step_cap;
-  uint32_t* runs;         // run buffer
-  const int64_t* run_off; // per segment: first run of its region
-  int32_t* run_len;       // per segment: runs written
-  int32_t* status;        // per segment
+  uint32_t* wruns;        // per warp: wruns_cap runs, where the backtrace writes
+  int64_t wruns_cap;
+  uint32_t* runs;         // run arena: each leaf's runs at run_off, packed
+  int64_t runs_cap;
+  unsigned long long* cursor;  // arena cursor (runs handed out)
+  int64_t* run_off;       // per segment: first run in the arena
+  int32_t* run_len;       // per segment: runs
+  int32_t* status;        // per segment: kPairOk, kPairScratch (more steps or
+                          // history), kPairArena (arena full), kPairInternal
+  int32_t* pair_score;    // nullable: per pair, the segment's score (penalty units)
   unsigned int* queue;
 };
 
 constexpr int kSegThreads = 128;
 
-// Run slots of a segment of m + n bases in a launch of step_cap steps.
+// Runs a segment of m + n bases can need when it ends below step_cap: each
+// mismatch run costs at least x and each gap run at least o + e, except a
+// gap continued from the segment's begin or left free at its end (one each),
+// and M runs lie between them.
 __host__ __device__ inline int64_t seg_run_cap(const Pen& p, int64_t bases, int step_cap) {
-  const int minstep = p.x < p.ge ? p.x : p.ge;
-  const int64_t b = 2 * (int64_t)step_cap / minstep + 2;
+  const int minrun = p.x < p.go ? p.x : p.go;
+  const int64_t b = 2 * ((int64_t)step_cap / minrun) + 5;
   return bases < b ? (bases > 0 ? bases : 1) : b;
 }
 

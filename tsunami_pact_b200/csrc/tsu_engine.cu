@@ -709,17 +709,21 @@ int run_bidir(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d
 }
 
 // TSU_BIDIRECTIONAL calls with CIGARs: the BiWFA recursion, level by level.
-// Level 0 is every pair whole; each level's segments go through one
-// breakpoint launch, and the host cuts each segment at its crossing (k, h)
-// into a left part (begin component, crossing component) and a right part
-// (crossing component, end component) for the next level -- unless the
-// crossing total is at most the base score (tsu::bidir_base: max(2 max(x,
-// o + e), 256) score units) or the cut leaves one side empty, when the
-// segment is a leaf.
-// Leaves, ordered by pair and position, then run through the segment kernel
-// (tsu_segment.cuh) in launches of growing step caps (a leaf that outgrows
-// its launch's history goes to the next), and one thread per pair joins its
-// leaves' runs.  Scores come from level 0.
+// First every pair runs whole through the segment kernel (tsu_segment.cuh)
+// with a step cap of the base score + 1: a pair whose optimal score is at
+// most the base score (tsu::bidir_base: max(2 max(x, o + e), 256) score
+// units) is done there -- its crossing total would be that score, so the
+// recursion would align it whole the same way -- and only the others enter
+// the recursion.  Its level 0 is those pairs whole; each level's segments
+// go through one breakpoint launch per size class, and the host cuts each
+// segment at its crossing (k, h) into a left part (begin component,
+// crossing component) and a right part (crossing component, end component)
+// for the next level -- unless the crossing total is at most the base score
+// or the cut leaves one side empty, when the segment is a leaf.  Leaves run
+// through the segment kernel in launches of growing step caps (a leaf that
+// outgrows its launch's history goes to the next), and one thread per pair
+// joins its leaves' runs in order.  Scores come from the first launch or
+// from level 0.
 int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int32_t* d_status, uint32_t* d_out_runs,
                     int64_t out_cap, int64_t* d_out_off, int64_t* runs_needed, const BatchInfo& bi,
                     const int32_t* h_plen, const int32_t* h_tlen, uint32_t** out_used, DevBuf* out_buf) {
@@ -741,9 +745,196 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   CU(cudaEventRecord(ctx->ev[4], st));
   const int base = tsu::bidir_base(rp);
   std::vector<int32_t> pst((size_t)n, tsu::kPairOk);  // pair statuses
-  std::vector<tsu::BidirSeg> cur((size_t)n), next, leaves;
-  std::vector<int32_t> leaf_T;
-  for (int64_t i = 0; i < n; ++i) cur[(size_t)i] = tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'};
+
+  // ---- leaves: segments aligned whole by the segment kernel; their runs
+  // packed into one arena (an atomic cursor at d_cnt[3]; grown by copy, so
+  // earlier runs stay)
+  std::vector<tsu::BidirSeg> leaves;
+  std::vector<int32_t> lcap, lstat, lruns;  // step cap to run at / status / runs
+  std::vector<int64_t> roff;                // first run in the arena
+  unsigned long long* d_cursor = d_cnt + 3;
+  int64_t arena_used = 0;  // the cursor after the last launch
+  int segs_occ = 0;
+  CU(tsu::segment_occupancy(&segs_occ));
+  if (segs_occ < 1) return set_err(ctx, TSU_EDEVICE, "segment kernel: no occupancy");
+  // Grow the arena by copy to hold at least `need` runs.
+  auto grow_arena = [&](int64_t need) -> int {
+    const size_t run_bytes = sizeof(uint32_t) * (size_t)std::max<int64_t>(need, 64);
+    if (run_bytes <= ctx->b_bruns.cap) return TSU_OK;
+    DevBuf nb;
+    const size_t bytes = (std::max(run_bytes, ctx->b_bruns.cap + ctx->b_bruns.cap / 2) + 255) & ~(size_t)255;
+    if (ctx->held() + bytes > ctx->budget) release(ctx, ctx->b_scratch);
+    if (ctx->held() + bytes > ctx->budget) {
+      ctx->need_bytes = ctx->held() + bytes;
+      return set_err(ctx, TSU_ENOMEM, "bidirectional mode: CIGAR runs exceed the budget");
+    }
+    CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
+    nb.cap = bytes;
+    if (arena_used)
+      CU(cudaMemcpyAsync(nb.p, ctx->b_bruns.p, sizeof(uint32_t) * (size_t)arena_used, cudaMemcpyDeviceToDevice, st));
+    ctx->peak_held = std::max(ctx->peak_held, ctx->held() + nb.cap);
+    release(ctx, ctx->b_bruns);
+    ctx->b_bruns = nb;
+    return TSU_OK;
+  };
+  // One segment-kernel launch over the leaves pick (indices into leaves) at
+  // step cap scap; d_pair_score: scores of whole pairs (nullable).  Leaves
+  // that find the arena full run again after it grows.
+  auto launch_leaves = [&](std::vector<int64_t> pick, int scap, int32_t* d_pair_score) -> int {
+    int rc2;
+    for (int attempt = 0; !pick.empty(); ++attempt) {
+      if (attempt > 8) return set_err(ctx, TSU_EINTERNAL, "segment kernel: run arena keeps overflowing");
+      const int64_t c = (int64_t)pick.size();
+      std::vector<tsu::BidirSeg> ls((size_t)c);
+      int32_t bases = 0;
+      int64_t expect = 0;  // runs expected: a quarter of the worst case, at least 16 per leaf
+      for (int64_t j = 0; j < c; ++j) {
+        const tsu::BidirSeg& s = leaves[(size_t)pick[(size_t)j]];
+        ls[(size_t)j] = s;
+        bases = std::max(bases, s.m + s.n);
+        expect += std::max<int64_t>(16, tsu::seg_run_cap(rp, (int64_t)s.m + s.n, scap) / (attempt ? 1 : 4));
+      }
+      if ((rc2 = grow_arena(arena_used + expect))) return rc2;
+      if ((rc2 = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(c, 1)))) return rc2;
+      if ((rc2 = grow(ctx, ctx->b_boff, sizeof(int64_t) * std::max<int64_t>(c, 1)))) return rc2;
+      if ((rc2 = grow(ctx, ctx->b_blen, 2 * sizeof(int32_t) * std::max<int64_t>(c, 1)))) return rc2;
+      // per-warp history, step table and run area
+      const int64_t hcap = tsu::seg_hist_cap(scap, bases);
+      const int64_t wcap = tsu::seg_run_cap(rp, bases, scap);
+      const size_t per_warp = sizeof(int32_t) * (size_t)(3 * hcap + 9 * (int64_t)scap + wcap);
+      const int wpb = tsu::kSegThreads / 32;
+      int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
+      const size_t fixed = ctx->held() - ctx->b_scratch.cap;
+      const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+      warps = std::min<int64_t>(warps, (int64_t)(avail / per_warp));
+      if (warps < 1) {
+        ctx->need_bytes = fixed + per_warp;
+        return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
+      }
+      const int64_t blocks = (warps + wpb - 1) / wpb;
+      const size_t nw = (size_t)(blocks * wpb);
+      if (per_warp * nw > ctx->b_scratch.cap) {
+        release(ctx, ctx->b_scratch);
+        if ((rc2 = grow(ctx, ctx->b_scratch, per_warp * nw))) return rc2;
+      }
+      const size_t sb = sizeof(tsu::BidirSeg) * (size_t)c;
+      if ((rc2 = host_grow(ctx, ctx->h_bidir, std::max(sb, (sizeof(int64_t) + 2 * sizeof(int32_t)) * (size_t)c) + 16)))
+        return rc2;
+      char* hb = static_cast<char*>(ctx->h_bidir.p);
+      std::memcpy(hb, ls.data(), sb);
+      CU(cudaMemcpyAsync(ctx->b_bsegs.p, hb, sb, cudaMemcpyHostToDevice, st));
+      CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+      int32_t* d_rlen = P<int32_t>(ctx->b_blen);
+      int32_t* const sc = P<int32_t>(ctx->b_scratch);
+      tsu::SegArgs a{};
+      a.seq = sv;
+      a.pk = pk;
+      a.pkr = pkr;
+      a.segs = P<tsu::BidirSeg>(ctx->b_bsegs);
+      a.n_segs = c;
+      a.pen = rp;
+      a.g = ctx->g;
+      a.hist = sc;
+      a.hist_cap = hcap;
+      a.table = sc + nw * 3 * (size_t)hcap;
+      a.step_cap = scap;
+      a.wruns = reinterpret_cast<uint32_t*>(sc + nw * (3 * (size_t)hcap + 9 * (size_t)scap));
+      a.wruns_cap = wcap;
+      a.runs = P<uint32_t>(ctx->b_bruns);
+      a.runs_cap = (int64_t)(ctx->b_bruns.cap / sizeof(uint32_t));
+      a.cursor = d_cursor;
+      a.run_off = P<int64_t>(ctx->b_boff);
+      a.run_len = d_rlen;
+      a.status = d_rlen + c;
+      a.pair_score = d_pair_score;
+      a.queue = d_queue;
+      tsu::launch_segment((int)blocks, st, a);
+      CU(cudaGetLastError());
+      ctx->timing.kernel_launches++;
+      log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" +
+             std::to_string(c);
+      int64_t* h_off = reinterpret_cast<int64_t*>(hb);
+      int32_t* h_len = reinterpret_cast<int32_t*>(h_off + c);
+      CU(cudaMemcpyAsync(h_off, ctx->b_boff.p, sizeof(int64_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
+      CU(cudaMemcpyAsync(h_len, d_rlen, 2 * sizeof(int32_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
+      unsigned long long* h_cur = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 48);
+      CU(cudaMemcpyAsync(h_cur, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      CU(wait_stream(ctx, st));
+      std::vector<int64_t> again;
+      for (int64_t j = 0; j < c; ++j) {
+        const size_t i = (size_t)pick[(size_t)j];
+        const int32_t s = h_len[c + j];
+        if (s == tsu::kPairArena) {
+          again.push_back((int64_t)i);
+          continue;
+        }
+        lstat[i] = s;
+        if (s == tsu::kPairOk) {
+          roff[i] = h_off[j];
+          lruns[i] = h_len[j];
+        }
+      }
+      // the cursor counts the overflowing leaves' runs too; the arena keeps
+      // everything below its capacity
+      arena_used = std::min<int64_t>((int64_t)*h_cur, a.runs_cap);
+      if (!again.empty()) {
+        // leaves past the end: continue from the arena's end
+        *h_cur = (unsigned long long)arena_used;
+        CU(cudaMemcpyAsync(d_cursor, h_cur, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+        CU(wait_stream(ctx, st));
+      }
+      pick.swap(again);
+    }
+    return TSU_OK;
+  };
+  auto add_leaf = [&](const tsu::BidirSeg& s, int cap) {
+    leaves.push_back(s);
+    lcap.push_back(cap);
+    lstat.push_back(tsu::kPairScratch);
+    lruns.push_back(0);
+    roff.push_back(0);
+  };
+
+  // ---- whole pairs at the base score
+  std::vector<tsu::BidirSeg> cur;
+  {
+    std::vector<int64_t> pick;
+    for (int64_t i = 0; i < n; ++i) {
+      if (h_plen[i] == 0 && h_tlen[i] == 0) {
+        pick.push_back((int64_t)leaves.size());
+        add_leaf(tsu::BidirSeg{(int32_t)i, 0, 0, 0, 0, 'M', 'M'}, base + 1);
+        continue;
+      }
+      pick.push_back((int64_t)leaves.size());
+      add_leaf(tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'}, base + 1);
+    }
+    rc = launch_leaves(pick, base + 1, d_score);
+    if (rc) return rc;
+    std::vector<tsu::BidirSeg> kept;
+    std::vector<int32_t> kcap, kstat, kruns;
+    std::vector<int64_t> koff;
+    for (int64_t i = 0; i < n; ++i) {
+      const int32_t s = lstat[(size_t)i];
+      if (s == tsu::kPairOk) {
+        kept.push_back(leaves[(size_t)i]);
+        kcap.push_back(lcap[(size_t)i]);
+        kstat.push_back(s);
+        kruns.push_back(lruns[(size_t)i]);
+        koff.push_back(roff[(size_t)i]);
+      } else if (s == tsu::kPairScratch) {
+        cur.push_back(leaves[(size_t)i]);  // score above the base: the recursion
+      } else {
+        pst[(size_t)i] = s;
+      }
+    }
+    leaves.swap(kept);
+    lcap.swap(kcap);
+    lstat.swap(kstat);
+    lruns.swap(kruns);
+    roff.swap(koff);
+  }
+
+  // ---- the recursion over the other pairs
   for (int level = 0; !cur.empty(); ++level) {
     const int64_t c = (int64_t)cur.size();
     const size_t res_bytes = sizeof(int32_t) * 5 * (size_t)c;
@@ -751,15 +942,15 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     int32_t* bo = P<int32_t>(ctx->b_bout);
     if ((rc = bidir_level(ctx, sv, pk, pkr, &cur, bo, d_queue, d_cnt + 1, &log))) return rc;
     if (level == 0) {
-      const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
-      bidir_level0_kernel<<<eblocks, 256, 0, st>>>(n, P<tsu::BidirSeg>(ctx->b_segs), bo, ctx->g, d_score, d_status);
+      const int eblocks = (int)std::min<int64_t>((c + 255) / 256, (int64_t)ctx->sms * 8);
+      bidir_level0_kernel<<<eblocks, 256, 0, st>>>(c, P<tsu::BidirSeg>(ctx->b_segs), bo, ctx->g, d_score, d_status);
       CU(cudaGetLastError());
       ctx->timing.kernel_launches++;
     }
     CU(cudaMemcpyAsync(ctx->h_bidir.p, bo, res_bytes, cudaMemcpyDeviceToHost, st));
     CU(wait_stream(ctx, st));
     const int32_t* hr = static_cast<const int32_t*>(ctx->h_bidir.p);
-    next.clear();
+    std::vector<tsu::BidirSeg> next;
     for (int64_t j = 0; j < c; ++j) {
       const tsu::BidirSeg& s = cur[(size_t)j];
       int32_t& ps = pst[(size_t)s.pair];
@@ -772,8 +963,11 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       if (s.m == 0 && s.n == 0) continue;
       const int32_t v = h - k, left = v + h, whole = s.m + s.n;
       if (T <= base || left <= 0 || left >= whole) {
-        leaves.push_back(s);
-        leaf_T.push_back(T);
+        // a leaf starts in the first launch whose cap exceeds its crossing
+        // total + 2 (o + e) + 4
+        int cap = base + 2 * rp.go + 4;
+        while (cap < T + 2 * rp.go + 4) cap *= 2;
+        add_leaf(s, cap);
         continue;
       }
       next.push_back(tsu::BidirSeg{s.pair, s.v0, s.h0, v, h, s.begin, comp});
@@ -781,8 +975,36 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     }
     cur.swap(next);
   }
-  // leaves in pair and position order: a counting sort by pair, then each
-  // pair's few leaves by position
+
+  // ---- the recursion's leaves, in launches of growing step caps
+  const int64_t max_smax = (int64_t)(std::max(bi.max_m, 0) + std::max(bi.max_n, 0)) * (rp.rm - 1) + 2 * rp.go + 1;
+  for (;;) {
+    int scap = INT32_MAX;
+    const int64_t L = (int64_t)leaves.size();
+    for (int64_t i = 0; i < L; ++i)
+      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)leaves[(size_t)i].pair] == tsu::kPairOk)
+        scap = std::min(scap, lcap[(size_t)i]);
+    if (scap == INT32_MAX) break;
+    if (scap > 2 * max_smax + 2 * (base + 2 * rp.go + 4))
+      return set_err(ctx, TSU_EINTERNAL, "segment kernel: step cap runaway");
+    std::vector<int64_t> pick;
+    for (int64_t i = 0; i < L; ++i)
+      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)leaves[(size_t)i].pair] == tsu::kPairOk &&
+          lcap[(size_t)i] == scap)
+        pick.push_back(i);
+    rc = launch_leaves(pick, scap, nullptr);
+    if (rc) return rc;
+    for (int64_t i : pick) {
+      const int32_t s = lstat[(size_t)i];
+      if (s == tsu::kPairScratch)
+        lcap[(size_t)i] = 2 * scap;
+      else if (s != tsu::kPairOk)
+        pst[(size_t)leaves[(size_t)i].pair] = s;
+    }
+  }
+
+  // ---- leaves in pair and position order: a counting sort by pair, then
+  // each pair's few leaves by position; join their runs
   const int64_t L = (int64_t)leaves.size();
   std::vector<int64_t> first((size_t)n + 1, 0);
   for (const tsu::BidirSeg& s : leaves) first[(size_t)s.pair + 1]++;
@@ -797,144 +1019,9 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       std::sort(idx.begin() + first[(size_t)p], idx.begin() + first[(size_t)p + 1], [&](int64_t a, int64_t b) {
         return leaves[(size_t)a].v0 + leaves[(size_t)a].h0 < leaves[(size_t)b].v0 + leaves[(size_t)b].h0;
       });
-  std::vector<tsu::BidirSeg> segs((size_t)L);
-  std::vector<int32_t> lT((size_t)L);
-  for (int64_t i = 0; i < L; ++i) {
-    segs[(size_t)i] = leaves[(size_t)idx[(size_t)i]];
-    lT[(size_t)i] = leaf_T[(size_t)idx[(size_t)i]];
-  }
-  // launches of growing step caps: a leaf starts in the first launch whose
-  // cap exceeds its crossing total + 2 (o + e) + 4, then moves up while it
-  // runs out of history
-  const int step0 = base + 2 * rp.go + 4;
-  auto cap_of = [&](int32_t T) {
-    int s = step0;
-    while (s < T + 2 * rp.go + 4) s *= 2;
-    return s;
-  };
-  std::vector<int32_t> lstat((size_t)L, tsu::kPairScratch), lcap((size_t)L);
-  std::vector<int64_t> roff((size_t)L, 0);
-  for (int64_t i = 0; i < L; ++i) lcap[(size_t)i] = cap_of(lT[(size_t)i]);
-  int64_t run_total = 0;  // run slots handed out so far
-  if ((rc = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(L, 1)))) return rc;
   if ((rc = grow(ctx, ctx->b_boff, sizeof(int64_t) * std::max<int64_t>(L, 1)))) return rc;
   if ((rc = grow(ctx, ctx->b_blen, 2 * sizeof(int32_t) * std::max<int64_t>(L, 1)))) return rc;
   int32_t* d_rlen = P<int32_t>(ctx->b_blen);
-  int32_t* d_lst = d_rlen + L;
-  int segs_occ = 0;
-  CU(tsu::segment_occupancy(&segs_occ));
-  if (segs_occ < 1) return set_err(ctx, TSU_EDEVICE, "segment kernel: no occupancy");
-  const int64_t max_smax = (int64_t)(std::max(bi.max_m, 0) + std::max(bi.max_n, 0)) * (rp.rm - 1) + 2 * rp.go + 1;
-  for (;;) {
-    // the pending leaves of the lowest cap
-    int scap = INT32_MAX;
-    for (int64_t i = 0; i < L; ++i)
-      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)segs[(size_t)i].pair] == tsu::kPairOk)
-        scap = std::min(scap, lcap[(size_t)i]);
-    if (scap == INT32_MAX) break;
-    if (scap > 2 * max_smax + 2 * step0) return set_err(ctx, TSU_EINTERNAL, "segment kernel: step cap runaway");
-    std::vector<int64_t> pick;
-    int32_t bases = 0;
-    for (int64_t i = 0; i < L; ++i)
-      if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)segs[(size_t)i].pair] == tsu::kPairOk &&
-          lcap[(size_t)i] == scap) {
-        pick.push_back(i);
-        bases = std::max(bases, segs[(size_t)i].m + segs[(size_t)i].n);
-      }
-    const int64_t c = (int64_t)pick.size();
-    // run regions of this launch, after those handed out before
-    std::vector<tsu::BidirSeg> ls((size_t)c);
-    std::vector<int64_t> lo((size_t)c);
-    int64_t add = 0;
-    for (int64_t j = 0; j < c; ++j) {
-      const tsu::BidirSeg& s = segs[(size_t)pick[(size_t)j]];
-      ls[(size_t)j] = s;
-      lo[(size_t)j] = run_total + add;
-      add += tsu::seg_run_cap(rp, (int64_t)s.m + s.n, scap);
-    }
-    const size_t run_bytes = sizeof(uint32_t) * (size_t)(run_total + add);
-    if (run_bytes > ctx->b_bruns.cap) {
-      // keep the runs written so far: grow by copy
-      DevBuf nb;
-      const size_t bytes = (std::max(run_bytes, ctx->b_bruns.cap + ctx->b_bruns.cap / 2) + 255) & ~(size_t)255;
-      if (ctx->held() + bytes > ctx->budget) release(ctx, ctx->b_scratch);
-      if (ctx->held() + bytes > ctx->budget) {
-        ctx->need_bytes = ctx->held() + bytes;
-        return set_err(ctx, TSU_ENOMEM, "bidirectional mode: CIGAR runs exceed the budget");
-      }
-      CU(cudaMallocFromPoolAsync(&nb.p, bytes, ctx->pool, st));
-      nb.cap = bytes;
-      if (run_total)
-        CU(cudaMemcpyAsync(nb.p, ctx->b_bruns.p, sizeof(uint32_t) * (size_t)run_total, cudaMemcpyDeviceToDevice, st));
-      ctx->peak_held = std::max(ctx->peak_held, ctx->held() + nb.cap);
-      release(ctx, ctx->b_bruns);
-      ctx->b_bruns = nb;
-    }
-    // per-warp history and step table
-    const int64_t hcap = tsu::seg_hist_cap(scap, bases);
-    const size_t per_warp = sizeof(int32_t) * (size_t)(3 * hcap + 9 * (int64_t)scap);
-    const int wpb = tsu::kSegThreads / 32;
-    int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
-    const size_t fixed = ctx->held() - ctx->b_scratch.cap;
-    const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
-    warps = std::min<int64_t>(warps, (int64_t)(avail / per_warp));
-    if (warps < 1) {
-      ctx->need_bytes = fixed + per_warp;
-      return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
-    }
-    const int64_t blocks = (warps + wpb - 1) / wpb;
-    const size_t need = per_warp * (size_t)(blocks * wpb);
-    if (need > ctx->b_scratch.cap) {
-      release(ctx, ctx->b_scratch);
-      if ((rc = grow(ctx, ctx->b_scratch, need))) return rc;
-    }
-    const size_t sb = sizeof(tsu::BidirSeg) * (size_t)c, ob = sizeof(int64_t) * (size_t)c;
-    if ((rc = host_grow(ctx, ctx->h_bidir, sb + ob + 2 * sizeof(int32_t) * (size_t)c))) return rc;
-    char* hb = static_cast<char*>(ctx->h_bidir.p);
-    std::memcpy(hb, ls.data(), sb);
-    std::memcpy(hb + sb, lo.data(), ob);
-    CU(cudaMemcpyAsync(ctx->b_bsegs.p, hb, sb, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ctx->b_boff.p, hb + sb, ob, cudaMemcpyHostToDevice, st));
-    CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
-    tsu::SegArgs a{};
-    a.seq = sv;
-    a.pk = pk;
-    a.pkr = pkr;
-    a.segs = P<tsu::BidirSeg>(ctx->b_bsegs);
-    a.n_segs = c;
-    a.pen = rp;
-    a.hist = P<int32_t>(ctx->b_scratch);
-    a.hist_cap = hcap;
-    a.table = P<int32_t>(ctx->b_scratch) + (size_t)(blocks * wpb) * 3 * (size_t)hcap;
-    a.step_cap = scap;
-    a.runs = P<uint32_t>(ctx->b_bruns);
-    a.run_off = P<int64_t>(ctx->b_boff);
-    a.run_len = d_rlen;
-    a.status = d_lst;
-    a.queue = d_queue;
-    tsu::launch_segment((int)blocks, st, a);
-    CU(cudaGetLastError());
-    ctx->timing.kernel_launches++;
-    log += " s" + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" + std::to_string(c);
-    int32_t* h_len = reinterpret_cast<int32_t*>(hb + sb + ob);
-    CU(cudaMemcpyAsync(h_len, d_rlen, 2 * sizeof(int32_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
-    CU(wait_stream(ctx, st));
-    for (int64_t j = 0; j < c; ++j) {
-      const int64_t i = pick[(size_t)j];
-      const int32_t s = h_len[c + j];
-      lstat[(size_t)i] = s;
-      if (s == tsu::kPairOk) {
-        roff[(size_t)i] = lo[(size_t)j];
-        lcap[(size_t)i] = h_len[j];  // runs written
-      } else if (s == tsu::kPairScratch) {
-        lcap[(size_t)i] = 2 * scap;
-      } else {
-        pst[(size_t)segs[(size_t)i].pair] = s;
-      }
-    }
-    run_total += add;
-  }
-  // join the runs of each pair's leaves
   if ((rc = host_grow(ctx, ctx->h_bidir,
                       sizeof(int64_t) * (size_t)(L + n + 1) + sizeof(int32_t) * (size_t)(L + n) + 64)))
     return rc;
@@ -944,9 +1031,10 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     int64_t* h_first = h_off + L;
     int32_t* h_rl = reinterpret_cast<int32_t*>(h_first + n + 1);
     int32_t* h_ps = h_rl + L;
-    for (int64_t i = 0; i < L; ++i) {
-      h_off[i] = roff[(size_t)i];
-      h_rl[i] = lstat[(size_t)i] == tsu::kPairOk ? lcap[(size_t)i] : 0;
+    for (int64_t j = 0; j < L; ++j) {
+      const size_t i = (size_t)idx[(size_t)j];
+      h_off[j] = roff[i];
+      h_rl[j] = lstat[i] == tsu::kPairOk ? lruns[i] : 0;
     }
     for (int64_t i = 0; i <= n; ++i) h_first[i] = first[(size_t)i];
     for (int64_t i = 0; i < n; ++i) h_ps[i] = pst[(size_t)i];

@@ -22,10 +22,10 @@
 // (step_cap rows: lo, hi, first history cell, and the first / last present
 // diagonal of M, I, D).  A segment that needs more
 // steps or cells than the launch gives gets status kPairScratch and runs
-// again in a launch with more.  Runs (length << 4 | kOp*) go to the
-// segment's region of the run buffer, at most seg_run_cap of them: a
-// segment that ends below step_cap made at most step_cap / min(x, e) edits,
-// so at most 2 step_cap / min(x, e) + 1 runs.
+// again in a launch with more.  The backtrace writes its runs (length << 4 |
+// kOp*; at most seg_run_cap of them) into the warp's own area, then the warp
+// takes their exact count from the run arena (an atomic cursor) and copies
+// them there; a segment that finds the arena full gets status kPairArena.
 #pragma once
 
 #include "tsu_bidir.cuh"
@@ -179,13 +179,13 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       }
     }
     if (st == kPairOk && !have) st = kPairInternal;
+    int64_t nr = 0;                // runs of the backtrace
+    const int64_t cap = min(seg_run_cap(pen, (int64_t)m + n, a.step_cap), a.wruns_cap);
+    uint32_t* const out = a.wruns + gwarp * a.wruns_cap;
     if (lane == 0 && st == kPairOk) {
-      // backtrace from the end; runs written backwards from the region's
+      // backtrace from the end; runs written backwards from the area's
       // end (forward pass: the segment's last operation comes first), or
       // forwards from its start (reversed pass: its first comes first)
-      uint32_t* out = a.runs + a.run_off[q];
-      const int64_t cap = seg_run_cap(pen, (int64_t)m + n, a.step_cap);
-      int64_t nr = 0;
       uint32_t cop = 0;
       int64_t clen = 0;
       bool bad = false;
@@ -257,12 +257,25 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       if (!bad) put(kOpD, v);
       if (!bad) put(kOpI, h);
       if (!bad) flush();
-      if (bad) {
-        st = kPairInternal;
+      if (bad) st = kPairInternal;
+    }
+    st = __shfl_sync(FULL, st, 0);
+    nr = __shfl_sync(FULL, nr, 0);
+    if (st == kPairOk) {
+      // the runs' place in the arena, then a warp-wide copy
+      unsigned long long pos = 0;
+      if (lane == 0) pos = atomicAdd(a.cursor, (unsigned long long)nr);
+      pos = __shfl_sync(FULL, pos, 0);
+      if ((int64_t)pos + nr > a.runs_cap) {
+        st = kPairArena;
       } else {
-        if (fwd)
-          for (int64_t i = 0; i < nr; ++i) out[i] = out[cap - nr + i];
-        a.run_len[q] = (int32_t)nr;
+        const uint32_t* src = fwd ? out + cap - nr : out;
+        for (int64_t i = lane; i < nr; i += 32) a.runs[pos + i] = src[i];
+        if (lane == 0) {
+          a.run_off[q] = (int64_t)pos;
+          a.run_len[q] = (int32_t)nr;
+          if (a.pair_score) a.pair_score[pair] = best * a.g;
+        }
       }
     }
     if (lane == 0) a.status[q] = st;
