@@ -500,6 +500,7 @@ struct SegArgs {
                           // history), kPairArena (arena full), kPairInternal
   int32_t* pair_score;    // nullable: per pair, the segment's score (penalty units)
   unsigned int* queue;
+  unsigned long long* work;  // nullable: [2] wavefront cells computed, score steps
 };
 
 constexpr int kSegThreads = 128;

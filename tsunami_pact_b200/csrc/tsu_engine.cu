@@ -848,6 +848,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       a.status = d_rlen + c;
       a.pair_score = d_pair_score;
       a.queue = d_queue;
+      a.work = d_cnt + 1;
       tsu::launch_segment((int)blocks, st, a);
       CU(cudaGetLastError());
       ctx->timing.kernel_launches++;

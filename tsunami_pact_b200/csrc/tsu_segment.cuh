@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
     int st = kPairOk;
     int64_t used = 0;  // history cells in use
     int have = 0, best = 0, s_end = 0, state = 'M';
+    int n_steps = 0;
     const int64_t smax = (int64_t)(m + n) * (pen.rm - 1) + 2 * go;
     for (int s = 0; s <= smax; ++s) {
       if (have && s - (free_end != 'M' ? oo : 0) > best) break;
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       }
       __syncwarp();
       used += width;
+      ++n_steps;
       if (get(s, hM, k_end) >= n && (!have || s < best)) have = 1, best = s, s_end = s, state = 'M';
       if (free_end == 'I' || free_end == 'D') {
         const int32_t gv = get(s, free_end == 'I' ? hI : hD, k_end);
@@ -278,7 +280,13 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         }
       }
     }
-    if (lane == 0) a.status[q] = st;
+    if (lane == 0) {
+      a.status[q] = st;
+      if (a.work) {
+        atomicAdd(a.work, (unsigned long long)used);
+        atomicAdd(a.work + 1, (unsigned long long)n_steps);
+      }
+    }
     __syncwarp();
   }
 }
