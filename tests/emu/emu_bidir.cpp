@@ -205,8 +205,8 @@ int main() {
   }
   const int threads = GW <= 4 ? 128 : 32 * GW;
   const int groups = threads / (32 * GW);
-  const int64_t ring_stride = (int64_t)2 * rp.rm * 4 * ring_w;
-  Buf<int32_t> ring((size_t)groups * ring_stride);
+  const int64_t ring_stride = (int64_t)2 * rp.rm * 4 * ring_w;  // elements (int16 below 16 warps)
+  Buf<char> ring((size_t)groups * ring_stride * tsu::bidir_ring_bytes(GW));
   Buf<int32_t> oT(N), oc(N), ok(N), oh(N), ost(N);
   Buf<unsigned> queue(2);
   Buf<unsigned long long> work(2);

@@ -35,12 +35,18 @@
 // cell.
 //
 // One group of GW warps per segment, persistent over a work queue.  The
-// rings of both directions live in global memory (int32, indexed by
-// diagonal: k + m + 1); each slot's limits and per-component present ranges
-// live in shared memory.  Scores run in units of g = gcd(x, o, e).
+// rings of both directions live in global memory (indexed by diagonal:
+// k + m + 1), of RT: int16 for groups of 1 and 4 warps (segments whose
+// longer side is below 16,384, so every offset fits; half the DRAM traffic
+// of int32, which bounds these groups on long segments), int32 for 16-warp
+// groups; negative values are absent cells.  Each slot's limits and
+// per-component present ranges live in shared memory.  The reverse pass's
+// M before extension is not stored (the cut reads only the forward one).
+// Scores run in units of g = gcd(x, o, e).
 #pragma once
 
 #include <climits>
+#include <type_traits>
 
 #include "tsu_common.cuh"
 #include "tsu_extend.cuh"
@@ -65,8 +71,8 @@ struct BidirArgs {
   int64_t n_segs;
   Pen pen;               // reduced penalties (one gap piece)
   int ring_w;            // diagonals per ring slot (>= m + n + 3 of every segment)
-  int32_t* ring;         // per group: [2][rm][4][ring_w]
-  int64_t ring_stride;   // int32 per group
+  void* ring;            // per group: [2][rm][4][ring_w] of the kernel's ring type
+  int64_t ring_stride;   // ring elements per group
   int32_t* out_T;        // per segment: lowest crossing total (score units), -1 none
   int32_t* out_comp;     // 'M', 'I', 'D'
   int32_t* out_k;        // forward diagonal of the cut
@@ -124,8 +130,15 @@ __device__ __forceinline__ int bidir_lcp(bool bytes, bool fwd, const uint32_t* p
 
 // 128-thread blocks (1- and 4-warp groups): at least 5 per SM (96 registers,
 // no spills; 20 warps per SM).
+// Ring element type of a group of GW warps (int16 below 16 warps).
+template <int GW>
+using bidir_ring_t = typename std::conditional<(GW < 16), int16_t, int32_t>::type;
+__host__ __device__ inline int bidir_ring_bytes(int gw) { return gw < 16 ? 2 : 4; }
+
 template <int GW>
 __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidir_kernel(BidirArgs a) {
+  using RT = bidir_ring_t<GW>;
+  constexpr RT kRNull = (RT)(sizeof(RT) == 2 ? -16384 : kBNull);  // stored absent cell
 #ifdef TSU_WARP_EMU
   unsigned char* smem_raw = emu::dyn_smem();
 #else
@@ -147,7 +160,7 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
   int* lim = reinterpret_cast<int*>(smem_raw + (size_t)gid * bidir_group_smem(pen, GW));
   int* part = lim + 2 * rm * kBLim;
   int* bc = part + GW * kBLim;
-  int32_t* const ring = a.ring + ggroup * a.ring_stride;
+  RT* const ring = static_cast<RT*>(a.ring) + ggroup * a.ring_stride;
   const int W = a.ring_w;
 
   for (;;) {
@@ -180,16 +193,22 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
     // slots by index (0..rm-1): the callers keep each direction's current
     // slot and step back from it, so the hot paths divide by rm nowhere
     auto LS = [&](int d, int sl) -> int* { return lim + (d * rm + sl) * kBLim; };
-    auto CS = [&](int d, int sl, int c) -> int32_t* { return ring + ((int64_t)(d * rm + sl) * 4 + c) * W + koff; };
+    auto CS = [&](int d, int sl, int c) -> RT* { return ring + ((int64_t)(d * rm + sl) * 4 + c) * W + koff; };
+    // a stored cell as an offset, kBNull when absent
+    auto ld = [&](const RT* p, int64_t i) -> int32_t {
+      const int32_t v = p[i];
+      return v < 0 ? kBNull : v;
+    };
+    auto sv = [&](int32_t v) -> RT { return v < 0 ? kRNull : (RT)v; };
     auto back = [&](int sl, int b) -> int { return sl - b + (sl < b ? rm : 0); };  // slot of b scores before (b < rm)
-    auto cells = [&](int d, int s, int c) -> int32_t* {
+    auto cells = [&](int d, int s, int c) -> RT* {
       return ring + ((int64_t)(d * rm + s % rm) * 4 + c) * W + koff;
     };
     auto get = [&](int d, int s, int c, int k) -> int32_t {
       if (s < 0) return kBNull;
       const int* l = L(d, s);
       if (k < l[0] || k > l[1]) return kBNull;
-      return cells(d, s, c)[k];
+      return ld(cells(d, s, c), k);
     };
     auto inb = [&](int32_t off, int k) -> bool {
       return ((uint32_t)off <= (uint32_t)n) & ((uint32_t)(off - k) <= (uint32_t)m);
@@ -201,10 +220,10 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
       const int start = d == 0 ? sg.begin : 'M';
       const int forced = d == 0 ? 'M' : sg.end;
       int* out = LS(d, sl);
-      int32_t* cM = CS(d, sl, kCM);
-      int32_t* cMP = CS(d, sl, kCMP);
-      int32_t* cI = CS(d, sl, kCI);
-      int32_t* cD = CS(d, sl, kCD);
+      RT* cM = CS(d, sl, kCM);
+      RT* cMP = CS(d, sl, kCMP);
+      RT* cI = CS(d, sl, kCI);
+      RT* cD = CS(d, sl, kCD);
       if (s == 0) {
         if (gt == 0) {
           if (forced == 'M') {
@@ -213,9 +232,9 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
                                   : bidir_lcp(bytes, false, rpw, rtw, pb, tb, bytes ? sg.v0 + m - 1 : rv0,
                                               bytes ? sg.h0 + n - 1 : rh0, rem);
             cMP[0] = 0;
-            cM[0] = lx;
-            cI[0] = start == 'I' ? 0 : kBNull;
-            cD[0] = start == 'D' ? 0 : kBNull;
+            cM[0] = sv(lx);
+            cI[0] = start == 'I' ? 0 : kRNull;
+            cD[0] = start == 'D' ? 0 : kRNull;
             out[0] = 0, out[1] = 0;
             out[2] = 0, out[3] = 0;
             out[4] = start == 'I' ? 0 : 1, out[5] = 0;
@@ -257,7 +276,7 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
       // step: cells of component c on diagonal k at base[c W + k] when k is
       // in [lo, hi]
       struct Src {
-        const int32_t* base;
+        const RT* base;
         int lo, hi;
       };
       auto src = [&](int ss) -> Src {
@@ -268,7 +287,7 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
       };
       const Src SX = src(s - x), SG = src(s - go), SE = src(s - ge);
       auto rd = [&](const Src& S, int c, int k) -> int32_t {
-        return (k < S.lo || k > S.hi) ? kBNull : S.base[(int64_t)c * W + k];
+        return (k < S.lo || k > S.hi) ? kBNull : ld(S.base, (int64_t)c * W + k);
       };
       // this direction's words and the position of its base 0 (packed:
       // forward (v0, h0), reversed (rv0, rh0); bytes: read forwards from
@@ -285,8 +304,8 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
         if (seed_d && k == -1) del = max(del, 0);
         const int32_t mis = rd(SX, kCM, k) + 1;
         const bool vi = inb(ins, k), vd = inb(del, k);
-        cI[k] = vi ? ins : kBNull;
-        cD[k] = vd ? del : kBNull;
+        cI[k] = vi ? (RT)ins : kRNull;
+        cD[k] = vd ? (RT)del : kRNull;
         if (vi) pi0 = min(pi0, k), pi1 = k, ai = max(ai, 2 * ins - k);
         if (vd) pd0 = min(pd0, k), pd1 = k, ad = max(ad, 2 * del - k);
         const int32_t pv = max(mis, max(ins, del));
@@ -294,13 +313,13 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
           const int vv = pv - k;
           const int rem = min(m - vv, n - pv);
           const int lx = bidir_lcp(bytes, dir > 0, dpw, dtw, pb, tb, dv0 + dir * vv, dh0 + dir * pv, rem);
-          cMP[k] = pv;
-          cM[k] = pv + lx;
+          if (d == 0) cMP[k] = (RT)pv;
+          cM[k] = (RT)(pv + lx);
           pm0 = min(pm0, k), pm1 = k;
           am = max(am, 2 * (pv + lx) - k);
         } else {
-          cMP[k] = kBNull;
-          cM[k] = kBNull;
+          if (d == 0) cMP[k] = kRNull;
+          cM[k] = kRNull;
         }
       }
       pm0 = __reduce_min_sync(FULL, pm0);
@@ -365,11 +384,11 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
       bK = k;
       if (ci == 0) {
         bC = 'M';
-        const int32_t pre = cells(0, sf, kCMP)[k], hr = get(1, sr, kCM, kd - k);
+        const int32_t pre = ld(cells(0, sf, kCMP), k), hr = get(1, sr, kCM, kd - k);
         bH = max(pre, n - hr);
       } else {
         bC = ci == 1 ? 'I' : 'D';
-        bH = cells(0, sf, ci == 1 ? kCI : kCD)[k];
+        bH = ld(cells(0, sf, ci == 1 ? kCI : kCD), k);
       }
     };
 
@@ -387,15 +406,15 @@ __global__ void __launch_bounds__(bidir_cta_threads<GW>(), GW <= 4 ? 5 : 1) bidi
           if (lf[8 + ci] + lr[8 + ci] < m + n) continue;
           const int plo = lf[2 + 2 * ci], phi = lf[3 + 2 * ci];
           const int c = ci == 0 ? kCM : (ci == 1 ? kCI : kCD);
-          const int32_t* fc = CS(0, slf, c);
-          const int32_t* rc = CS(1, slr, c);
+          const RT* fc = CS(0, slf, c);
+          const RT* rc = CS(1, slr, c);
           const int rlo = lr[0], rhi = lr[1];
           for (int k = plo + gt; k <= phi; k += GT) {
             const int32_t hf = fc[k];
-            if (hf == kBNull) continue;
+            if (hf < 0) continue;
             const int kr = kd - k;
-            const int32_t hr = (kr < rlo || kr > rhi) ? kBNull : rc[kr];
-            if (hr == kBNull || hf + hr < n) continue;
+            const int32_t hr = (kr < rlo || kr > rhi) ? -1 : (int32_t)rc[kr];
+            if (hr < 0 || hf + hr < n) continue;
             const int total = sf + sr - (ci == 0 ? 0 : oo);
             const unsigned long long kk = ((unsigned long long)(uint32_t)total << 40) |
                                           ((unsigned long long)(s2 - s_lo) << 34) | ((unsigned long long)ci << 32) |

@@ -569,18 +569,19 @@ int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, c
   CU(tsu::bidir_occupancy(gw, threads, smem, &occ));
   if (occ < 1) return set_err(ctx, TSU_EDEVICE, "bidirectional kernel: no occupancy");
   const int ring_w = max_bases + 3;
-  const int64_t ring_stride = (int64_t)2 * rp.rm * 4 * ring_w;
+  const int64_t ring_stride = (int64_t)2 * rp.rm * 4 * ring_w;  // elements per group
+  const size_t ring_bytes = (size_t)tsu::bidir_ring_bytes(gw) * (size_t)ring_stride;
   int64_t groups = std::min<int64_t>((int64_t)ctx->sms * occ * gpb, c);
   const size_t fixed = ctx->held() - ctx->b_scratch.cap;
   const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
-  groups = std::min<int64_t>(groups, (int64_t)(avail / (sizeof(int32_t) * (size_t)ring_stride)));
+  groups = std::min<int64_t>(groups, (int64_t)(avail / ring_bytes));
   if (groups < 1) return set_err(ctx, TSU_ENOMEM, "bidirectional mode: rings of one pair exceed the budget");
   int bpg = gpb;  // groups per block
   if (groups >= gpb)
     groups = groups / gpb * gpb;
   else
     bpg = (int)groups;
-  const size_t need = sizeof(int32_t) * (size_t)(groups * ring_stride);
+  const size_t need = ring_bytes * (size_t)groups;
   if (need > ctx->b_scratch.cap) {
     release(ctx, ctx->b_scratch);
     if ((rc = grow(ctx, ctx->b_scratch, need))) return rc;
@@ -594,7 +595,7 @@ int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, c
   a.n_segs = c;
   a.pen = rp;
   a.ring_w = ring_w;
-  a.ring = P<int32_t>(ctx->b_scratch);
+  a.ring = ctx->b_scratch.p;
   a.ring_stride = ring_stride;
   a.out_T = out;
   a.out_comp = out + stride;
@@ -1551,7 +1552,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
       const int gws[3] = {1, 4, 16};
       for (int k = 0; k < 3; ++k) {
         if (!cls_n[k]) continue;
-        const size_t ring = sizeof(int32_t) * 2 * (size_t)rp.rm * 4 * ((size_t)cls_bases[k] + 3);
+        const size_t ring = (size_t)tsu::bidir_ring_bytes(gws[k]) * 2 * (size_t)rp.rm * 4 * ((size_t)cls_bases[k] + 3);
         const int64_t groups = std::min<int64_t>(cls_n[k], (int64_t)ctx->sms * (gws[k] <= 4 ? 5 * (4 / gws[k]) : 1));
         scratch_full = std::max(scratch_full, (size_t)groups * ring);
         scratch_min = std::max(scratch_min, ring);
