@@ -10,8 +10,9 @@
 //                 pair; its segment is the whole pair, or with
 //                 "S v0 h0 sm sn" after begin end, a sub-range)
 // Output (stdout): gw 1, 4, 16 (breakpoint kernel): per segment
-//                  "T comp k h" (T in penalty units, -1: none); gw 0
-//                  (segment kernel, one block of 4 warps, step_cap steps):
+//                  "T comp k h" (T in penalty units, -1: none); gw 0 or -1
+//                  (segment kernel with int16 or int32 history, one block
+//                  of 4 warps, step_cap steps):
 //                  per segment "status ops" (ops '-' when empty), then
 //                  "retries K": segments that found the (deliberately
 //                  small) run arena full and ran again
@@ -42,7 +43,9 @@ int main() {
   int64_t N;
   if (!(std::cin >> X >> O >> E >> GW >> N)) return 2;
   int step_cap = 0;
-  if (GW == 0 && !(std::cin >> step_cap)) return 2;
+  if (GW <= 0 && !(std::cin >> step_cap)) return 2;
+  const bool h32 = GW < 0;  // segment kernel with int32 history (gw -1)
+  if (GW < 0) GW = 0;
   std::vector<std::string> pats(N), txts(N);
   std::vector<tsu::BidirSeg> segs(N);
   for (int64_t i = 0; i < N; ++i) {
@@ -124,7 +127,8 @@ int main() {
     for (auto& sg : segs) bases = std::max(bases, sg.m + sg.n);
     const int64_t hcap = tsu::seg_hist_cap(step_cap, bases);
     const int64_t wcap = tsu::seg_run_cap(rp, bases, step_cap);
-    Buf<int32_t> hist((size_t)(warps * 3 * hcap)), table((size_t)warps * 9 * step_cap);
+    Buf<char> hist((size_t)(warps * 3 * hcap) * (h32 ? 4 : 2));
+    Buf<int32_t> table((size_t)warps * 9 * step_cap);
     Buf<uint32_t> wruns((size_t)(warps * wcap));
     // an arena too small for every segment's runs at once: some segments
     // report kPairArena (2) and run again with a larger one
@@ -160,7 +164,13 @@ int main() {
     a.run_len = rlen.p;
     a.status = sst.p;
     a.queue = queue.p;
-    emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel(a); });
+    auto seg = [&](const tsu::SegArgs& x) {
+      if (h32)
+        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel<int32_t>(x); });
+      else
+        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel<int16_t>(x); });
+    };
+    seg(a);
     // the segments that found the arena full, again with room for all
     {
       std::vector<int64_t> again;
@@ -181,7 +191,7 @@ int main() {
         b.run_off = roff2.p;
         b.run_len = rlen2.p;
         b.status = sst2.p;
-        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel(b); });
+        seg(b);
         for (size_t j = 0; j < again.size(); ++j) {
           roff.p[again[j]] = roff2.p[j];
           rlen.p[again[j]] = rlen2.p[j];

@@ -119,9 +119,9 @@ def test_long_segments_warp_group(emu_bidir, oracle):
     _check(emu_bidir, oracle, recs, (4, 6, 2), 16)
 
 
-def _seg_ops(exe, recs, pen, step_cap, retries=None):
+def _seg_ops(exe, recs, pen, step_cap, retries=None, h32=False):
     out = []
-    lines = _run(exe, _input(recs, f"{pen[0]} {pen[1]} {pen[2]} 0 {len(recs)} {step_cap}\n"))
+    lines = _run(exe, _input(recs, f"{pen[0]} {pen[1]} {pen[2]} {-1 if h32 else 0} {len(recs)} {step_cap}\n"))
     for ln in lines[: len(recs)]:
         st, ops = ln.split()
         out.append((int(st), "" if ops == "-" else ops))
@@ -130,14 +130,15 @@ def _seg_ops(exe, recs, pen, step_cap, retries=None):
     return out
 
 
-@pytest.mark.parametrize("pen", [(4, 6, 2), (3, 5, 1), (20, 1, 1)])
-def test_base_case_segments_match_oracle(emu_bidir, oracle, pen):
+@pytest.mark.parametrize("pen,h32", [((4, 6, 2), False), ((3, 5, 1), False), ((20, 1, 1), False),
+                                     ((4, 6, 2), True)])
+def test_base_case_segments_match_oracle(emu_bidir, oracle, pen, h32):
     """The base-case kernel (tsu_segment.cuh): every segment's operations
     equal the oracle's segment alignment (ora_align_segment) for every begin
     and end component, whole pairs, sub-ranges and bytes outside ACGT; a
     step cap below what a segment needs gives status 1 (more scratch); a
     run arena too small gives status 2 and the segment's second run, with
-    room, the same operations."""
+    room, the same operations.  History as int16 and as int32."""
     rng = random.Random(hash(pen) & 0xFFFF)
     recs = []
     for i in range(36):
@@ -151,7 +152,7 @@ def test_base_case_segments_match_oracle(emu_bidir, oracle, pen):
     g = math.gcd(*pen)
     step_cap = 400
     retries = []
-    got = _seg_ops(emu_bidir, recs, pen, step_cap, retries)
+    got = _seg_ops(emu_bidir, recs, pen, step_cap, retries, h32)
     assert retries[0] > 0  # the arena of 24 runs cannot hold them all
     compared = 0
     for (p, t, b, e, sub), (st, ops) in zip(recs, got):
@@ -165,7 +166,7 @@ def test_base_case_segments_match_oracle(emu_bidir, oracle, pen):
             compared += 1
     assert compared >= 30
     # a cap too small for the longer segments
-    small = _seg_ops(emu_bidir, recs, pen, 3)
+    small = _seg_ops(emu_bidir, recs, pen, 3, None, h32)
     assert any(st == 1 for st, _ in small)
     for (st, ops), (st0, ops0) in zip(small, got):
         assert st in (0, 1)

@@ -32,10 +32,19 @@ void launch_bidir(int gw, int blocks, int threads, size_t smem, cudaStream_t st,
 }
 
 cudaError_t segment_occupancy(int* blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, segment_kernel, kSegThreads, 0);
+  int b16 = 0, b32 = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b16, segment_kernel<int16_t>, kSegThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, segment_kernel<int32_t>, kSegThreads, 0);
+  *blocks_per_sm = b16 < b32 ? b16 : b32;
+  return e;
 }
 
-void launch_segment(int blocks, cudaStream_t st, const SegArgs& a) { segment_kernel<<<blocks, kSegThreads, 0, st>>>(a); }
+void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a) {
+  if (int16_history)
+    segment_kernel<int16_t><<<blocks, kSegThreads, 0, st>>>(a);
+  else
+    segment_kernel<int32_t><<<blocks, kSegThreads, 0, st>>>(a);
+}
 
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int64_t* first, const int64_t* run_off,
                      const int32_t* run_len, const uint32_t* runs, const int32_t* status, int64_t* out_len,

@@ -504,7 +504,7 @@ struct SegArgs {
   int64_t n_segs;
   Pen pen;
   int g;                  // score unit
-  int32_t* hist;          // per warp: hist_cap x 3 int32 (M, I, D)
+  void* hist;             // per warp: hist_cap x 3 (M, I, D) of the launch's history type
   int64_t hist_cap;
   int32_t* table;         // per warp: step_cap x 9 int32
   int32_t step_cap;
@@ -548,8 +548,8 @@ __host__ __device__ inline int64_t seg_hist_cap(int step_cap, int64_t bases) {
 cudaError_t bidir_occupancy(int gw, int threads, size_t smem, int* occ);
 void launch_bidir(int gw, int blocks, int threads, size_t smem, cudaStream_t st, const BidirArgs& a);
 // The base-case kernels (tsu_segment.cuh), launched from tsu_bidir.cu.
-cudaError_t segment_occupancy(int* blocks_per_sm);
-void launch_segment(int blocks, cudaStream_t st, const SegArgs& a);
+cudaError_t segment_occupancy(int* blocks_per_sm);  // the lower of the two history types
+void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a);
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int64_t* first, const int64_t* run_off,
                      const int32_t* run_len, const uint32_t* runs, const int32_t* status, int64_t* out_len,
                      const int64_t* out_off, uint32_t* out);

@@ -787,12 +787,13 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       if (attempt > 8) return set_err(ctx, TSU_EINTERNAL, "segment kernel: run arena keeps overflowing");
       const int64_t c = (int64_t)pick.size();
       std::vector<tsu::BidirSeg> ls((size_t)c);
-      int32_t bases = 0;
+      int32_t bases = 0, side = 0;
       int64_t expect = 0;  // runs expected: a quarter of the worst case, at least 16 per leaf
       for (int64_t j = 0; j < c; ++j) {
         const tsu::BidirSeg& s = leaves[(size_t)pick[(size_t)j]];
         ls[(size_t)j] = s;
         bases = std::max(bases, s.m + s.n);
+        side = std::max(side, std::max(s.m, s.n));
         expect += std::max<int64_t>(16, tsu::seg_run_cap(rp, (int64_t)s.m + s.n, scap) / (attempt ? 1 : 4));
       }
       if ((rc2 = grow_arena(arena_used + expect))) return rc2;
@@ -800,9 +801,11 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       if ((rc2 = grow(ctx, ctx->b_boff, sizeof(int64_t) * std::max<int64_t>(c, 1)))) return rc2;
       if ((rc2 = grow(ctx, ctx->b_blen, 2 * sizeof(int32_t) * std::max<int64_t>(c, 1)))) return rc2;
       // per-warp history, step table and run area
+      const bool h16 = side < 32767;  // int16 history: every offset fits
       const int64_t hcap = tsu::seg_hist_cap(scap, bases);
       const int64_t wcap = tsu::seg_run_cap(rp, bases, scap);
-      const size_t per_warp = sizeof(int32_t) * (size_t)(3 * hcap + 9 * (int64_t)scap + wcap);
+      const size_t hist_w = ((h16 ? 2 : 4) * 3 * (size_t)hcap + 15) & ~(size_t)15;  // bytes per warp
+      const size_t per_warp = hist_w + sizeof(int32_t) * (size_t)(9 * (int64_t)scap + wcap);
       const int wpb = tsu::kSegThreads / 32;
       int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
       const size_t fixed = ctx->held() - ctx->b_scratch.cap;
@@ -826,7 +829,8 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       CU(cudaMemcpyAsync(ctx->b_bsegs.p, hb, sb, cudaMemcpyHostToDevice, st));
       CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
       int32_t* d_rlen = P<int32_t>(ctx->b_blen);
-      int32_t* const sc = P<int32_t>(ctx->b_scratch);
+      char* const sc = P<char>(ctx->b_scratch);
+      int32_t* const sc_tab = reinterpret_cast<int32_t*>(sc + nw * hist_w);
       tsu::SegArgs a{};
       a.seq = sv;
       a.pk = pk;
@@ -836,10 +840,10 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       a.pen = rp;
       a.g = ctx->g;
       a.hist = sc;
-      a.hist_cap = hcap;
-      a.table = sc + nw * 3 * (size_t)hcap;
+      a.hist_cap = hist_w / ((h16 ? 2 : 4) * 3);  // cells per warp (the area is rounded up to 16 B)
+      a.table = sc_tab;
       a.step_cap = scap;
-      a.wruns = reinterpret_cast<uint32_t*>(sc + nw * (3 * (size_t)hcap + 9 * (size_t)scap));
+      a.wruns = reinterpret_cast<uint32_t*>(sc_tab + nw * 9 * (size_t)scap);
       a.wruns_cap = wcap;
       a.runs = P<uint32_t>(ctx->b_bruns);
       a.runs_cap = (int64_t)(ctx->b_bruns.cap / sizeof(uint32_t));
@@ -850,7 +854,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       a.pair_score = d_pair_score;
       a.queue = d_queue;
       a.work = d_cnt + 1;
-      tsu::launch_segment((int)blocks, st, a);
+      tsu::launch_segment(h16, (int)blocks, st, a);
       CU(cudaGetLastError());
       ctx->timing.kernel_launches++;
       log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" +

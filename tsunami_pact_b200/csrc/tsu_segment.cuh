@@ -32,14 +32,19 @@
 
 namespace tsu {
 
+// HT: the history's element type -- int16 when every segment of the launch
+// has both sides below 32,767 (offsets fit; half the history traffic),
+// int32 otherwise.  Negative stored values are absent cells.
+template <typename HT>
 __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int hM = 0, hI = 1, hD = 2;  // components of a history cell
+  constexpr HT kHNull = (HT)(sizeof(HT) == 2 ? -16384 : kBNull);
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const Pen pen = a.pen;
   const int x = pen.x, go = pen.go, ge = pen.ge, oo = pen.go - pen.ge;
-  int32_t* const hist = a.hist + gwarp * a.hist_cap * 3;
+  HT* const hist = static_cast<HT*>(a.hist) + gwarp * a.hist_cap * 3;
   int32_t* const tab = a.table + gwarp * (int64_t)a.step_cap * 9;
   for (;;) {
     unsigned q = 0;
@@ -77,7 +82,8 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       if (s < 0) return kBNull;
       const int32_t* t = tab + (int64_t)s * 9;
       if (k < t[0] || k > t[1]) return kBNull;
-      return hist[((int64_t)t[2] + (k - t[0])) * 3 + c];
+      const int32_t v = hist[((int64_t)t[2] + (k - t[0])) * 3 + c];
+      return v < 0 ? kBNull : v;
     };
     int st = kPairOk;
     int64_t used = 0;  // history cells in use
@@ -116,11 +122,11 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         st = kPairScratch;
         break;
       }
-      int32_t* row = hist + used * 3;
+      HT* row = hist + used * 3;
       int pm0 = INT_MAX, pm1 = INT_MIN, pi0 = INT_MAX, pi1 = INT_MIN, pd0 = INT_MAX, pd1 = INT_MIN;
       // the source rows (s - x, s - o - e, s - e), resolved once per step
       struct Row {
-        const int32_t* base;  // cell of diagonal k at base + 3 (k - lo)
+        const HT* base;  // cell of diagonal k at base + 3 (k - lo)
         int lo, hi;
       };
       auto row_of = [&](int ss) -> Row {
@@ -130,7 +136,9 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       };
       const Row RX = row_of(s - x), RG = row_of(s - go), RE = row_of(s - ge);
       auto rd = [&](const Row& R, int c, int k) -> int32_t {
-        return (k < R.lo || k > R.hi) ? kBNull : R.base[(int64_t)(k - R.lo) * 3 + c];
+        if (k < R.lo || k > R.hi) return kBNull;
+        const int32_t v = R.base[(int64_t)(k - R.lo) * 3 + c];
+        return v < 0 ? kBNull : v;
       };
       for (int k = lo + lane; k <= hi; k += 32) {
         int32_t cm = kBNull, ci = kBNull, cd = kBNull;
@@ -152,8 +160,10 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
             cm = pv + lcp(vv, pv, min(m - vv, n - pv));
           }
         }
-        int32_t* cell = row + (int64_t)(k - lo) * 3;
-        cell[hM] = cm, cell[hI] = ci, cell[hD] = cd;
+        HT* cell = row + (int64_t)(k - lo) * 3;
+        cell[hM] = cm < 0 ? kHNull : (HT)cm;
+        cell[hI] = ci < 0 ? kHNull : (HT)ci;
+        cell[hD] = cd < 0 ? kHNull : (HT)cd;
         if (cm != kBNull) pm0 = min(pm0, k), pm1 = k;
         if (ci != kBNull) pi0 = min(pi0, k), pi1 = k;
         if (cd != kBNull) pd0 = min(pd0, k), pd1 = k;
