@@ -46,13 +46,21 @@ void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegAr
     segment_kernel<int32_t><<<blocks, kSegThreads, 0, st>>>(a);
 }
 
-void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int64_t* first, const int64_t* run_off,
-                     const int32_t* run_len, const uint32_t* runs, const int32_t* status, int64_t* out_len,
-                     const int64_t* out_off, uint32_t* out) {
+void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int32_t* pre_st, const int64_t* pre_off,
+                     const int32_t* pre_len, const int64_t* first, const int64_t* run_off, const int32_t* run_len,
+                     const uint32_t* runs, const int32_t* status, int64_t* out_len, const int64_t* out_off,
+                     uint32_t* out) {
   if (write)
-    seg_runs_kernel<true><<<blocks, 256, 0, st>>>(n, first, run_off, run_len, runs, status, out_len, out_off, out);
+    seg_runs_kernel<true><<<blocks, 256, 0, st>>>(n, pre_st, pre_off, pre_len, first, run_off, run_len, runs, status,
+                                                  out_len, out_off, out);
   else
-    seg_runs_kernel<false><<<blocks, 256, 0, st>>>(n, first, run_off, run_len, runs, status, out_len, out_off, out);
+    seg_runs_kernel<false><<<blocks, 256, 0, st>>>(n, pre_st, pre_off, pre_len, first, run_off, run_len, runs, status,
+                                                   out_len, out_off, out);
+}
+
+void launch_whole_pairs(int blocks, cudaStream_t st, int64_t n, const int32_t* plen, const int32_t* tlen,
+                        BidirSeg* segs) {
+  whole_pairs_kernel<<<blocks, 256, 0, st>>>(n, plen, tlen, segs);
 }
 
 }  // namespace tsu

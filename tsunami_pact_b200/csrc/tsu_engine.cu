@@ -75,6 +75,7 @@ struct tsu_ctx {
   DevBuf b_out2;                                          // second CIGAR output buffer (chunk pipeline)
   DevBuf b_rwords, b_rnonacgt, b_segs, b_bout;            // bidirectional mode: reversed words, segments, cuts
   DevBuf b_bsegs, b_boff, b_blen, b_bruns, b_bfirst;      // bidirectional CIGARs: base cases, their runs
+  DevBuf b_pre;                                           // bidirectional CIGARs: the whole-pair launch's results
   bool one_warp = false;  // TSU_ONE_WARP of the current call
   bool bidir = false;     // TSU_BIDIRECTIONAL of the current call
   cudaEvent_t pev[2] = {};  // per-pass timing
@@ -121,7 +122,7 @@ struct tsu_ctx {
     return {&b_pat,  &b_txt,    &b_poff,     &b_toff,  &b_plen,  &b_tlen,   &b_words_cnt, &b_woff, &b_words,
             &b_nonacgt, &b_score, &b_status, &b_cpos, &b_clen, &b_clen64, &b_coff,      &b_out,  &b_order,
             &b_retry, &b_counters, &b_scratch, &b_arena, &b_scan_tmp, &b_out2, &b_rwords, &b_rnonacgt,
-            &b_segs,  &b_bout, &b_bsegs, &b_boff, &b_blen, &b_bruns, &b_bfirst};
+            &b_segs,  &b_bout, &b_bsegs, &b_boff, &b_blen, &b_bruns, &b_bfirst, &b_pre};
   }
   size_t held() const {
     size_t s = 0;
@@ -778,10 +779,81 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     ctx->b_bruns = nb;
     return TSU_OK;
   };
-  // One segment-kernel launch over the leaves pick (indices into leaves) at
-  // step cap scap; d_pair_score: scores of whole pairs (nullable).  Leaves
-  // that find the arena full run again after it grows.
-  auto launch_leaves = [&](std::vector<int64_t> pick, int scap, int32_t* d_pair_score) -> int {
+  // One segment-kernel launch over c segments on the device (longest m + n
+  // `bases`, longest side `side`) at step cap scap, the arena grown to hold
+  // `expect` more runs first; results per segment at d_off, d_len, d_st.
+  // Afterwards arena_used is what the arena holds, and the cursor is put
+  // back there if segments found the arena full.
+  auto run_segments = [&](const tsu::BidirSeg* d_segs, int64_t c, int32_t bases, int32_t side, int scap,
+                          int64_t expect, int64_t* d_off, int32_t* d_len, int32_t* d_st, int32_t* d_pair_score) -> int {
+    int rc2;
+    if ((rc2 = grow_arena(arena_used + expect))) return rc2;
+    const bool h16 = side < 32767;  // int16 history: every offset fits
+    const int64_t hcap = tsu::seg_hist_cap(scap, bases);
+    const int64_t wcap = tsu::seg_run_cap(rp, bases, scap);
+    const size_t hist_w = ((h16 ? 2 : 4) * 3 * (size_t)hcap + 15) & ~(size_t)15;  // bytes per warp
+    const size_t per_warp = hist_w + sizeof(int32_t) * (size_t)(9 * (int64_t)scap + wcap);
+    const int wpb = tsu::kSegThreads / 32;
+    int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
+    const size_t fixed = ctx->held() - ctx->b_scratch.cap;
+    const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
+    warps = std::min<int64_t>(warps, (int64_t)(avail / per_warp));
+    if (warps < 1) {
+      ctx->need_bytes = fixed + per_warp;
+      return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
+    }
+    const int64_t blocks = (warps + wpb - 1) / wpb;
+    const size_t nw = (size_t)(blocks * wpb);
+    if (per_warp * nw > ctx->b_scratch.cap) {
+      release(ctx, ctx->b_scratch);
+      if ((rc2 = grow(ctx, ctx->b_scratch, per_warp * nw))) return rc2;
+    }
+    CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+    char* const sc = P<char>(ctx->b_scratch);
+    int32_t* const sc_tab = reinterpret_cast<int32_t*>(sc + nw * hist_w);
+    tsu::SegArgs a{};
+    a.seq = sv;
+    a.pk = pk;
+    a.pkr = pkr;
+    a.segs = d_segs;
+    a.n_segs = c;
+    a.pen = rp;
+    a.g = ctx->g;
+    a.hist = sc;
+    a.hist_cap = hist_w / ((h16 ? 2 : 4) * 3);  // cells per warp (the area is rounded up to 16 B)
+    a.table = sc_tab;
+    a.step_cap = scap;
+    a.wruns = reinterpret_cast<uint32_t*>(sc_tab + nw * 9 * (size_t)scap);
+    a.wruns_cap = wcap;
+    a.runs = P<uint32_t>(ctx->b_bruns);
+    a.runs_cap = (int64_t)(ctx->b_bruns.cap / sizeof(uint32_t));
+    a.cursor = d_cursor;
+    a.run_off = d_off;
+    a.run_len = d_len;
+    a.status = d_st;
+    a.pair_score = d_pair_score;
+    a.queue = d_queue;
+    a.work = d_cnt + 1;
+    tsu::launch_segment(h16, (int)blocks, st, a);
+    CU(cudaGetLastError());
+    ctx->timing.kernel_launches++;
+    log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" +
+           std::to_string(c);
+    unsigned long long* h_cur = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 48);
+    CU(cudaMemcpyAsync(h_cur, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
+    // the cursor counts the runs of segments that found the arena full too;
+    // the arena keeps everything below its capacity
+    arena_used = std::min<int64_t>((int64_t)*h_cur, a.runs_cap);
+    if ((int64_t)*h_cur > a.runs_cap) {
+      *h_cur = (unsigned long long)arena_used;
+      CU(cudaMemcpyAsync(d_cursor, h_cur, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+    }
+    return TSU_OK;
+  };
+  // One launch over the leaves pick (indices into leaves) at step cap scap;
+  // leaves that find the arena full run again after it grows.
+  auto launch_leaves = [&](std::vector<int64_t> pick, int scap) -> int {
     int rc2;
     for (int attempt = 0; !pick.empty(); ++attempt) {
       if (attempt > 8) return set_err(ctx, TSU_EINTERNAL, "segment kernel: run arena keeps overflowing");
@@ -796,75 +868,23 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
         side = std::max(side, std::max(s.m, s.n));
         expect += std::max<int64_t>(16, tsu::seg_run_cap(rp, (int64_t)s.m + s.n, scap) / (attempt ? 1 : 4));
       }
-      if ((rc2 = grow_arena(arena_used + expect))) return rc2;
       if ((rc2 = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(c, 1)))) return rc2;
       if ((rc2 = grow(ctx, ctx->b_boff, sizeof(int64_t) * std::max<int64_t>(c, 1)))) return rc2;
       if ((rc2 = grow(ctx, ctx->b_blen, 2 * sizeof(int32_t) * std::max<int64_t>(c, 1)))) return rc2;
-      // per-warp history, step table and run area
-      const bool h16 = side < 32767;  // int16 history: every offset fits
-      const int64_t hcap = tsu::seg_hist_cap(scap, bases);
-      const int64_t wcap = tsu::seg_run_cap(rp, bases, scap);
-      const size_t hist_w = ((h16 ? 2 : 4) * 3 * (size_t)hcap + 15) & ~(size_t)15;  // bytes per warp
-      const size_t per_warp = hist_w + sizeof(int32_t) * (size_t)(9 * (int64_t)scap + wcap);
-      const int wpb = tsu::kSegThreads / 32;
-      int64_t warps = std::min<int64_t>((int64_t)ctx->sms * segs_occ * wpb, c);
-      const size_t fixed = ctx->held() - ctx->b_scratch.cap;
-      const size_t avail = ctx->budget > fixed ? ctx->budget - fixed : 0;
-      warps = std::min<int64_t>(warps, (int64_t)(avail / per_warp));
-      if (warps < 1) {
-        ctx->need_bytes = fixed + per_warp;
-        return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
-      }
-      const int64_t blocks = (warps + wpb - 1) / wpb;
-      const size_t nw = (size_t)(blocks * wpb);
-      if (per_warp * nw > ctx->b_scratch.cap) {
-        release(ctx, ctx->b_scratch);
-        if ((rc2 = grow(ctx, ctx->b_scratch, per_warp * nw))) return rc2;
-      }
       const size_t sb = sizeof(tsu::BidirSeg) * (size_t)c;
       if ((rc2 = host_grow(ctx, ctx->h_bidir, std::max(sb, (sizeof(int64_t) + 2 * sizeof(int32_t)) * (size_t)c) + 16)))
         return rc2;
       char* hb = static_cast<char*>(ctx->h_bidir.p);
       std::memcpy(hb, ls.data(), sb);
       CU(cudaMemcpyAsync(ctx->b_bsegs.p, hb, sb, cudaMemcpyHostToDevice, st));
-      CU(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
       int32_t* d_rlen = P<int32_t>(ctx->b_blen);
-      char* const sc = P<char>(ctx->b_scratch);
-      int32_t* const sc_tab = reinterpret_cast<int32_t*>(sc + nw * hist_w);
-      tsu::SegArgs a{};
-      a.seq = sv;
-      a.pk = pk;
-      a.pkr = pkr;
-      a.segs = P<tsu::BidirSeg>(ctx->b_bsegs);
-      a.n_segs = c;
-      a.pen = rp;
-      a.g = ctx->g;
-      a.hist = sc;
-      a.hist_cap = hist_w / ((h16 ? 2 : 4) * 3);  // cells per warp (the area is rounded up to 16 B)
-      a.table = sc_tab;
-      a.step_cap = scap;
-      a.wruns = reinterpret_cast<uint32_t*>(sc_tab + nw * 9 * (size_t)scap);
-      a.wruns_cap = wcap;
-      a.runs = P<uint32_t>(ctx->b_bruns);
-      a.runs_cap = (int64_t)(ctx->b_bruns.cap / sizeof(uint32_t));
-      a.cursor = d_cursor;
-      a.run_off = P<int64_t>(ctx->b_boff);
-      a.run_len = d_rlen;
-      a.status = d_rlen + c;
-      a.pair_score = d_pair_score;
-      a.queue = d_queue;
-      a.work = d_cnt + 1;
-      tsu::launch_segment(h16, (int)blocks, st, a);
-      CU(cudaGetLastError());
-      ctx->timing.kernel_launches++;
-      log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" +
-             std::to_string(c);
+      if ((rc2 = run_segments(P<tsu::BidirSeg>(ctx->b_bsegs), c, bases, side, scap, expect, P<int64_t>(ctx->b_boff),
+                              d_rlen, d_rlen + c, nullptr)))
+        return rc2;
       int64_t* h_off = reinterpret_cast<int64_t*>(hb);
       int32_t* h_len = reinterpret_cast<int32_t*>(h_off + c);
       CU(cudaMemcpyAsync(h_off, ctx->b_boff.p, sizeof(int64_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
       CU(cudaMemcpyAsync(h_len, d_rlen, 2 * sizeof(int32_t) * (size_t)c, cudaMemcpyDeviceToHost, st));
-      unsigned long long* h_cur = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 48);
-      CU(cudaMemcpyAsync(h_cur, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
       CU(wait_stream(ctx, st));
       std::vector<int64_t> again;
       for (int64_t j = 0; j < c; ++j) {
@@ -880,15 +900,6 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
           lruns[i] = h_len[j];
         }
       }
-      // the cursor counts the overflowing leaves' runs too; the arena keeps
-      // everything below its capacity
-      arena_used = std::min<int64_t>((int64_t)*h_cur, a.runs_cap);
-      if (!again.empty()) {
-        // leaves past the end: continue from the arena's end
-        *h_cur = (unsigned long long)arena_used;
-        CU(cudaMemcpyAsync(d_cursor, h_cur, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
-        CU(wait_stream(ctx, st));
-      }
       pick.swap(again);
     }
     return TSU_OK;
@@ -901,43 +912,43 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     roff.push_back(0);
   };
 
-  // ---- whole pairs at the base score
+  // ---- whole pairs at the base score, bookkept on the device: segments
+  // built there, results in their own arrays (pre_off, pre_len, pre_st);
+  // only the statuses come back.  A pair that outgrew the cap, or found the
+  // arena full, enters the recursion (which aligns a pair of score at most
+  // the base whole, the same way).
+  if ((rc = grow(ctx, ctx->b_pre, (sizeof(int64_t) + 2 * sizeof(int32_t)) * (size_t)std::max<int64_t>(n, 1)))) return rc;
+  int64_t* const pre_off = P<int64_t>(ctx->b_pre);
+  int32_t* const pre_len = reinterpret_cast<int32_t*>(pre_off + n);
+  int32_t* const pre_st = pre_len + n;
   std::vector<tsu::BidirSeg> cur;
   {
-    std::vector<int64_t> pick;
+    if ((rc = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(n, 1)))) return rc;
+    int32_t bases = 0, side = 0;
+    int64_t expect = 0;
     for (int64_t i = 0; i < n; ++i) {
-      if (h_plen[i] == 0 && h_tlen[i] == 0) {
-        pick.push_back((int64_t)leaves.size());
-        add_leaf(tsu::BidirSeg{(int32_t)i, 0, 0, 0, 0, 'M', 'M'}, base + 1);
-        continue;
-      }
-      pick.push_back((int64_t)leaves.size());
-      add_leaf(tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'}, base + 1);
+      bases = std::max(bases, h_plen[i] + h_tlen[i]);
+      side = std::max(side, std::max(h_plen[i], h_tlen[i]));
+      expect += std::max<int64_t>(16, tsu::seg_run_cap(rp, (int64_t)h_plen[i] + h_tlen[i], base + 1) / 4);
     }
-    rc = launch_leaves(pick, base + 1, d_score);
-    if (rc) return rc;
-    std::vector<tsu::BidirSeg> kept;
-    std::vector<int32_t> kcap, kstat, kruns;
-    std::vector<int64_t> koff;
+    const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
+    tsu::launch_whole_pairs(eblocks, st, n, sv.pat_len, sv.txt_len, P<tsu::BidirSeg>(ctx->b_bsegs));
+    CU(cudaGetLastError());
+    ctx->timing.kernel_launches++;
+    if ((rc = run_segments(P<tsu::BidirSeg>(ctx->b_bsegs), n, bases, side, base + 1, expect, pre_off, pre_len, pre_st,
+                           d_score)))
+      return rc;
+    if ((rc = host_grow(ctx, ctx->h_bidir, sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)))) return rc;
+    int32_t* h_st = static_cast<int32_t*>(ctx->h_bidir.p);
+    CU(cudaMemcpyAsync(h_st, pre_st, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    CU(wait_stream(ctx, st));
     for (int64_t i = 0; i < n; ++i) {
-      const int32_t s = lstat[(size_t)i];
-      if (s == tsu::kPairOk) {
-        kept.push_back(leaves[(size_t)i]);
-        kcap.push_back(lcap[(size_t)i]);
-        kstat.push_back(s);
-        kruns.push_back(lruns[(size_t)i]);
-        koff.push_back(roff[(size_t)i]);
-      } else if (s == tsu::kPairScratch) {
-        cur.push_back(leaves[(size_t)i]);  // score above the base: the recursion
-      } else {
+      const int32_t s = h_st[i];
+      if (s == tsu::kPairScratch || s == tsu::kPairArena)
+        cur.push_back(tsu::BidirSeg{(int32_t)i, 0, 0, h_plen[i], h_tlen[i], 'M', 'M'});
+      else if (s != tsu::kPairOk)
         pst[(size_t)i] = s;
-      }
     }
-    leaves.swap(kept);
-    lcap.swap(kcap);
-    lstat.swap(kstat);
-    lruns.swap(kruns);
-    roff.swap(koff);
   }
 
   // ---- the recursion over the other pairs
@@ -998,7 +1009,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       if (lstat[(size_t)i] == tsu::kPairScratch && pst[(size_t)leaves[(size_t)i].pair] == tsu::kPairOk &&
           lcap[(size_t)i] == scap)
         pick.push_back(i);
-    rc = launch_leaves(pick, scap, nullptr);
+    rc = launch_leaves(pick, scap);
     if (rc) return rc;
     for (int64_t i : pick) {
       const int32_t s = lstat[(size_t)i];
@@ -1055,8 +1066,8 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   CU(cudaEventRecord(ctx->ev[5], st));
   const int rblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
   int64_t* d_len = P<int64_t>(ctx->b_clen64);
-  tsu::launch_seg_runs(false, rblocks, st, n, P<int64_t>(ctx->b_bfirst), P<int64_t>(ctx->b_boff), d_rlen,
-                       P<uint32_t>(ctx->b_bruns), d_status, d_len, nullptr, nullptr);
+  tsu::launch_seg_runs(false, rblocks, st, n, pre_st, pre_off, pre_len, P<int64_t>(ctx->b_bfirst),
+                       P<int64_t>(ctx->b_boff), d_rlen, P<uint32_t>(ctx->b_bruns), d_status, d_len, nullptr, nullptr);
   CU(cudaMemsetAsync(d_len + n, 0, sizeof(int64_t), st));
   size_t tb = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, tb, d_len, d_out_off, (int)(n + 1), st);
@@ -1079,8 +1090,9 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     if (out_used) *out_used = d_out_runs;
   }
   if (total > out_cap) return TSU_EOVERFLOW;
-  tsu::launch_seg_runs(true, rblocks, st, n, P<int64_t>(ctx->b_bfirst), P<int64_t>(ctx->b_boff), d_rlen,
-                       P<uint32_t>(ctx->b_bruns), d_status, nullptr, d_out_off, d_out_runs);
+  tsu::launch_seg_runs(true, rblocks, st, n, pre_st, pre_off, pre_len, P<int64_t>(ctx->b_bfirst),
+                       P<int64_t>(ctx->b_boff), d_rlen, P<uint32_t>(ctx->b_bruns), d_status, nullptr, d_out_off,
+                       d_out_runs);
   CU(cudaGetLastError());
   ctx->timing.kernel_launches += 3;
   CU(cudaEventRecord(ctx->ev[6], st));

@@ -301,15 +301,19 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
   }
 }
 
-// Runs of each pair from its base segments (contiguous, in alignment
-// order): runs of the same operation that meet at a segment boundary merge.
+// Runs of each pair from its leaves, in alignment order: the one leaf of the
+// whole-pair launch when pre_st[i] is OK (at pre_off[i], pre_len[i] runs),
+// else the recursion's leaves first[i] .. first[i + 1] (at run_off[j],
+// run_len[j]); runs of the same operation that meet at a cut merge.
 // count: out_len[i] = the pair's run count (0 unless status[i] is OK);
 // write: the runs at out[out_off[i]...].  One thread per pair.
 template <bool kWrite>
-__global__ void seg_runs_kernel(int64_t n, const int64_t* __restrict__ first, const int64_t* __restrict__ run_off,
-                                const int32_t* __restrict__ run_len, const uint32_t* __restrict__ runs,
-                                const int32_t* __restrict__ status, int64_t* __restrict__ out_len,
-                                const int64_t* __restrict__ out_off, uint32_t* __restrict__ out) {
+__global__ void seg_runs_kernel(int64_t n, const int32_t* __restrict__ pre_st, const int64_t* __restrict__ pre_off,
+                                const int32_t* __restrict__ pre_len, const int64_t* __restrict__ first,
+                                const int64_t* __restrict__ run_off, const int32_t* __restrict__ run_len,
+                                const uint32_t* __restrict__ runs, const int32_t* __restrict__ status,
+                                int64_t* __restrict__ out_len, const int64_t* __restrict__ out_off,
+                                uint32_t* __restrict__ out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     if (status[i] != kPairOk) {
       if (!kWrite) out_len[i] = 0;
@@ -318,9 +322,8 @@ __global__ void seg_runs_kernel(int64_t n, const int64_t* __restrict__ first, co
     int64_t cnt = 0, w = kWrite ? out_off[i] : 0;
     uint32_t cur = 0;
     bool open = false;
-    for (int64_t j = first[i]; j < first[i + 1]; ++j) {
-      const uint32_t* r = runs + run_off[j];
-      for (int t = 0; t < run_len[j]; ++t) {
+    auto leaf = [&](const uint32_t* r, int len) {
+      for (int t = 0; t < len; ++t) {
         const uint32_t u = r[t];
         if (open && (u & 15u) == (cur & 15u)) {
           cur += u & ~15u;
@@ -331,13 +334,24 @@ __global__ void seg_runs_kernel(int64_t n, const int64_t* __restrict__ first, co
           ++cnt;
         }
       }
-    }
+    };
+    if (pre_st[i] == kPairOk)
+      leaf(runs + pre_off[i], pre_len[i]);
+    else
+      for (int64_t j = first[i]; j < first[i + 1]; ++j) leaf(runs + run_off[j], run_len[j]);
     if (kWrite) {
       if (open) out[w] = cur;
     } else {
       out_len[i] = cnt;
     }
   }
+}
+
+// Whole pairs as segments, free at both ends.
+__global__ void whole_pairs_kernel(int64_t n, const int32_t* __restrict__ plen, const int32_t* __restrict__ tlen,
+                                   BidirSeg* __restrict__ segs) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    segs[i] = BidirSeg{(int32_t)i, 0, 0, plen[i], tlen[i], 'M', 'M'};
 }
 
 }  // namespace tsu
