@@ -924,13 +924,17 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   std::vector<tsu::BidirSeg> cur;
   {
     if ((rc = grow(ctx, ctx->b_bsegs, sizeof(tsu::BidirSeg) * std::max<int64_t>(n, 1)))) return rc;
+    // the arena sized for every pair's worst case at this cap (about 1 KB
+    // per pair at 4/6/2) when that takes at most a quarter of the budget: a
+    // pair that finds it full costs a breakpoint search
     int32_t bases = 0, side = 0;
-    int64_t expect = 0;
+    int64_t worst = 0;
     for (int64_t i = 0; i < n; ++i) {
       bases = std::max(bases, h_plen[i] + h_tlen[i]);
       side = std::max(side, std::max(h_plen[i], h_tlen[i]));
-      expect += std::max<int64_t>(16, tsu::seg_run_cap(rp, (int64_t)h_plen[i] + h_tlen[i], base + 1) / 4);
+      worst += tsu::seg_run_cap(rp, (int64_t)h_plen[i] + h_tlen[i], base + 1);
     }
+    const int64_t expect = sizeof(uint32_t) * (size_t)worst <= ctx->budget / 4 ? worst : std::max<int64_t>(worst / 4, 16 * n);
     const int eblocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sms * 8);
     tsu::launch_whole_pairs(eblocks, st, n, sv.pat_len, sv.txt_len, P<tsu::BidirSeg>(ctx->b_bsegs));
     CU(cudaGetLastError());
