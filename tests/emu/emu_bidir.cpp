@@ -165,10 +165,11 @@ int main() {
     a.status = sst.p;
     a.queue = queue.p;
     auto seg = [&](const tsu::SegArgs& x) {
+      const size_t sm = tsu::seg_smem_bytes(rp);
       if (h32)
-        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel<int32_t>(x); });
+        emu::launch(1, tsu::kSegThreads, sm, [&] { tsu::segment_kernel<int32_t>(x); });
       else
-        emu::launch(1, tsu::kSegThreads, 0, [&] { tsu::segment_kernel<int16_t>(x); });
+        emu::launch(1, tsu::kSegThreads, sm, [&] { tsu::segment_kernel<int16_t>(x); });
     };
     seg(a);
     // the segments that found the arena full, again with room for all

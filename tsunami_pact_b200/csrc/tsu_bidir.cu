@@ -31,19 +31,21 @@ void launch_bidir(int gw, int blocks, int threads, size_t smem, cudaStream_t st,
   }
 }
 
-cudaError_t segment_occupancy(int* blocks_per_sm) {
+cudaError_t segment_occupancy(const Pen& pen, int* blocks_per_sm) {
   int b16 = 0, b32 = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b16, segment_kernel<int16_t>, kSegThreads, 0);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, segment_kernel<int32_t>, kSegThreads, 0);
+  const size_t smem = seg_smem_bytes(pen);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b16, segment_kernel<int16_t>, kSegThreads, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, segment_kernel<int32_t>, kSegThreads, smem);
   *blocks_per_sm = b16 < b32 ? b16 : b32;
   return e;
 }
 
 void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a) {
+  const size_t smem = seg_smem_bytes(a.pen);
   if (int16_history)
-    segment_kernel<int16_t><<<blocks, kSegThreads, 0, st>>>(a);
+    segment_kernel<int16_t><<<blocks, kSegThreads, smem, st>>>(a);
   else
-    segment_kernel<int32_t><<<blocks, kSegThreads, 0, st>>>(a);
+    segment_kernel<int32_t><<<blocks, kSegThreads, smem, st>>>(a);
 }
 
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int32_t* pre_st, const int64_t* pre_off,

@@ -523,6 +523,11 @@ struct SegArgs {
 };
 
 constexpr int kSegThreads = 128;
+// Shared memory of a segment-kernel block: per warp the last rm rows of the
+// step table (9 int each).
+__host__ __device__ inline size_t seg_smem_bytes(const Pen& p) {
+  return (size_t)(kSegThreads / 32) * (size_t)p.rm * 9 * sizeof(int);
+}
 
 // Runs a segment of m + n bases can need when it ends below step_cap: each
 // mismatch run costs at least x and each gap run at least o + e, except a
@@ -548,7 +553,7 @@ __host__ __device__ inline int64_t seg_hist_cap(int step_cap, int64_t bases) {
 cudaError_t bidir_occupancy(int gw, int threads, size_t smem, int* occ);
 void launch_bidir(int gw, int blocks, int threads, size_t smem, cudaStream_t st, const BidirArgs& a);
 // The base-case kernels (tsu_segment.cuh), launched from tsu_bidir.cu.
-cudaError_t segment_occupancy(int* blocks_per_sm);  // the lower of the two history types
+cudaError_t segment_occupancy(const Pen& pen, int* blocks_per_sm);  // the lower of the two history types
 void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a);
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int32_t* pre_st, const int64_t* pre_off,
                      const int32_t* pre_len, const int64_t* first, const int64_t* run_off, const int32_t* run_len,

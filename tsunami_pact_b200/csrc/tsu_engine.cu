@@ -757,7 +757,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   unsigned long long* d_cursor = d_cnt + 3;
   int64_t arena_used = 0;  // the cursor after the last launch
   int segs_occ = 0;
-  CU(tsu::segment_occupancy(&segs_occ));
+  CU(tsu::segment_occupancy(rp, &segs_occ));
   if (segs_occ < 1) return set_err(ctx, TSU_EDEVICE, "segment kernel: no occupancy");
   // Grow the arena by copy to hold at least `need` runs.
   auto grow_arena = [&](int64_t need) -> int {

@@ -36,7 +36,7 @@ namespace tsu {
 // has both sides below 32,767 (offsets fit; half the history traffic),
 // int32 otherwise.  Negative stored values are absent cells.
 template <typename HT>
-__global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
+__global__ void __launch_bounds__(kSegThreads, 6) segment_kernel(SegArgs a) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int hM = 0, hI = 1, hD = 2;  // components of a history cell
   constexpr HT kHNull = (HT)(sizeof(HT) == 2 ? -16384 : kBNull);
@@ -46,6 +46,16 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
   const int x = pen.x, go = pen.go, ge = pen.ge, oo = pen.go - pen.ge;
   HT* const hist = static_cast<HT*>(a.hist) + gwarp * a.hist_cap * 3;
   int32_t* const tab = a.table + gwarp * (int64_t)a.step_cap * 9;
+  // the last rm rows of the step table in shared memory, slot s mod rm (the
+  // steps read them; the backtrace reads the table in device memory)
+#ifdef TSU_WARP_EMU
+  int* const rt = reinterpret_cast<int*>(emu::dyn_smem()) + (threadIdx.x >> 5) * pen.rm * 9;
+#else
+  extern __shared__ int seg_smem[];
+  int* const rt = seg_smem + (threadIdx.x >> 5) * pen.rm * 9;
+#endif
+  const int rm = pen.rm;
+  auto slot_back = [&](int sl, int b) -> int { return sl - b + (sl < b ? rm : 0); };  // slot b steps before (b < rm)
   for (;;) {
     unsigned q = 0;
     if (lane == 0) q = atomicAdd(a.queue, 1u);
@@ -90,7 +100,7 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
     int have = 0, best = 0, s_end = 0, state = 'M';
     int n_steps = 0;
     const int64_t smax = (int64_t)(m + n) * (pen.rm - 1) + 2 * go;
-    for (int s = 0; s <= smax; ++s) {
+    for (int s = 0, sl = 0; s <= smax; ++s, sl = sl + 1 == rm ? 0 : sl + 1) {
       if (have && s - (free_end != 'M' ? oo : 0) > best) break;
       if (s >= a.step_cap) {
         st = kPairScratch;
@@ -104,15 +114,17 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         hi = 0;
       } else {
         lo = INT_MAX, hi = INT_MIN;
-        const int src_s[4] = {s - x, s - go, s - ge, s - ge};
-        const int src_c[4] = {0, 0, 1, 2};  // present range of M, M, I, D
-        for (int i = 0; i < 4; ++i) {
-          if (src_s[i] < 0) continue;
-          const int32_t* u = tab + (int64_t)src_s[i] * 9 + 3 + 2 * src_c[i];
-          if (u[0] > u[1]) continue;
+        auto widen = [&](int b, int c) {  // present range of component c, b steps back
+          if (s < b) return;
+          const int* u = rt + slot_back(sl, b) * 9 + 3 + 2 * c;
+          if (u[0] > u[1]) return;
           lo = min(lo, u[0] - 1);
           hi = max(hi, u[1] + 1);
-        }
+        };
+        widen(x, 0);
+        widen(go, 0);
+        widen(ge, 1);
+        widen(ge, 2);
         if (seed_i) lo = min(lo, 1), hi = max(hi, 1);
         if (seed_d) lo = min(lo, -1), hi = max(hi, -1);
         if (lo > hi) lo = 1, hi = 0;
@@ -129,12 +141,13 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         const HT* base;  // cell of diagonal k at base + 3 (k - lo)
         int lo, hi;
       };
-      auto row_of = [&](int ss) -> Row {
-        if (ss < 0 || s == 0) return Row{hist, 1, 0};
-        const int32_t* t = tab + (int64_t)ss * 9;
+      auto row_of = [&](int b) -> Row {  // b steps back
+        if (s < b || s == 0) return Row{hist, 1, 0};
+        const int* t = rt + slot_back(sl, b) * 9;
         return Row{hist + (int64_t)t[2] * 3, t[0], t[1]};
       };
-      const Row RX = row_of(s - x), RG = row_of(s - go), RE = row_of(s - ge);
+      const Row RX = row_of(x), RG = row_of(go), RE = row_of(ge);
+      int32_t eM = kBNull, eI = kBNull, eD = kBNull;  // this step's cells on the end diagonal
       auto rd = [&](const Row& R, int c, int k) -> int32_t {
         if (k < R.lo || k > R.hi) return kBNull;
         const int32_t v = R.base[(int64_t)(k - R.lo) * 3 + c];
@@ -164,6 +177,7 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
         cell[hM] = cm < 0 ? kHNull : (HT)cm;
         cell[hI] = ci < 0 ? kHNull : (HT)ci;
         cell[hD] = cd < 0 ? kHNull : (HT)cd;
+        if (k == k_end) eM = cm, eI = ci, eD = cd;
         if (cm != kBNull) pm0 = min(pm0, k), pm1 = k;
         if (ci != kBNull) pi0 = min(pi0, k), pi1 = k;
         if (cd != kBNull) pd0 = min(pd0, k), pd1 = k;
@@ -174,19 +188,23 @@ __global__ void __launch_bounds__(kSegThreads) segment_kernel(SegArgs a) {
       pi1 = __reduce_max_sync(FULL, pi1);
       pd0 = __reduce_min_sync(FULL, pd0);
       pd1 = __reduce_max_sync(FULL, pd1);
+      eM = __reduce_max_sync(FULL, eM);
+      eI = __reduce_max_sync(FULL, eI);
+      eD = __reduce_max_sync(FULL, eD);
       if (lane == 0) {
+        const int32_t row9[9] = {lo, hi, (int32_t)used, pm0 <= pm1 ? pm0 : 1, pm0 <= pm1 ? pm1 : 0,
+                                 pi0 <= pi1 ? pi0 : 1, pi0 <= pi1 ? pi1 : 0, pd0 <= pd1 ? pd0 : 1,
+                                 pd0 <= pd1 ? pd1 : 0};
         int32_t* t = tab + (int64_t)s * 9;
-        t[0] = lo, t[1] = hi, t[2] = (int32_t)used;
-        t[3] = pm0 <= pm1 ? pm0 : 1, t[4] = pm0 <= pm1 ? pm1 : 0;
-        t[5] = pi0 <= pi1 ? pi0 : 1, t[6] = pi0 <= pi1 ? pi1 : 0;
-        t[7] = pd0 <= pd1 ? pd0 : 1, t[8] = pd0 <= pd1 ? pd1 : 0;
+        int* r = rt + sl * 9;
+        for (int i = 0; i < 9; ++i) t[i] = row9[i], r[i] = row9[i];
       }
       __syncwarp();
       used += width;
       ++n_steps;
-      if (get(s, hM, k_end) >= n && (!have || s < best)) have = 1, best = s, s_end = s, state = 'M';
+      if (eM >= n && (!have || s < best)) have = 1, best = s, s_end = s, state = 'M';
       if (free_end == 'I' || free_end == 'D') {
-        const int32_t gv = get(s, free_end == 'I' ? hI : hD, k_end);
+        const int32_t gv = free_end == 'I' ? eI : eD;
         if (gv == n && (!have || s - oo < best)) have = 1, best = s - oo, s_end = s, state = free_end;
       }
     }
