@@ -190,3 +190,29 @@ def test_bidirectional_memory_50kbp(oracle):
     print(f"50 kbp @ 20 %: score {s0[0]}, device bytes forward {fwd_bytes / 1e6:.1f} MB, "
           f"bidirectional {bi_bytes / 1e6:.1f} MB")
     assert 0 < bi_bytes < fwd_bytes / 4
+
+
+def test_bidirectional_chunked_host_pipeline(aligner_factory, oracle):
+    """300,000 pairs from host buffers run as a pipeline of chunks (one
+    recursion per chunk): the same scores and runs as the same pairs in
+    calls of 60,000 (one chunk each), and the scores of the forward pass."""
+    import tsunami_pact_b200 as T
+
+    rng = np.random.default_rng(71)
+    n = 300_000
+    pb, po, pl, tb, to, tl = _batch(T, 71, rng.integers(20, 120, n), rng.uniform(0.0, 0.3, n))
+    al = aligner_factory((4, 6, 2))
+    s, c, r = al.align_arrays(pb, po, pl, tb, to, tl, cigar=True, bidirectional=True)
+    fwd, _, _ = al.align_arrays(pb, po, pl, tb, to, tl, cigar=False)
+    assert np.array_equal(s, fwd)
+    step = 60_000
+    for a in range(0, n, step):
+        sl = slice(a, a + step)
+        s1, c1, r1 = al.align_arrays(pb, po[sl], pl[sl], tb, to[sl], tl[sl], cigar=True, bidirectional=True)
+        assert np.array_equal(s1, s[sl])
+        assert np.array_equal(c1, c[a:a + step + 1] - c[a])
+        assert np.array_equal(r1, r[c[a]:c[min(a + step, n)]])
+    for i in range(0, n, 9973):  # a sample against the oracle's recursion
+        p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
+        assert T.runs_to_ops(r[c[i]:c[i + 1]]) == oracle.bialign(p, t, 4, 6, 2, base_score=base_score((4, 6, 2)),
+                                                                 ring=True)
