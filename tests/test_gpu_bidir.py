@@ -216,3 +216,22 @@ def test_bidirectional_chunked_host_pipeline(aligner_factory, oracle):
         p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
         assert T.runs_to_ops(r[c[i]:c[i + 1]]) == oracle.bialign(p, t, 4, 6, 2, base_score=base_score((4, 6, 2)),
                                                                  ring=True)
+
+
+def test_bidirectional_tight_budget(aligner_factory):
+    """Under a 64 MB device budget the breakpoint groups, the leaf warps and
+    the run arena shrink to fit, and the results stay those of the default
+    budget."""
+    import tsunami_pact_b200 as T
+
+    rng = np.random.default_rng(81)
+    lengths = np.concatenate([rng.integers(100, 1500, 1500), [10_000, 10_000, 6_000]])
+    rates = np.concatenate([rng.uniform(0.0, 0.2, 1500), [0.15, 0.05, 0.3]])
+    pb, po, pl, tb, to, tl = _batch(T, 81, lengths, rates)
+    s0, c0, r0 = aligner_factory((4, 6, 2)).align_arrays(pb, po, pl, tb, to, tl, cigar=True, bidirectional=True)
+    with T.Aligner(4, 6, 2, mem_budget=64 << 20) as al:
+        s1, c1, r1 = al.align_arrays(pb, po, pl, tb, to, tl, cigar=True, bidirectional=True)
+        assert al.timing()["device_bytes"] <= 64 << 20
+    assert np.array_equal(s0, s1)
+    assert np.array_equal(c0, c1)
+    assert np.array_equal(r0, r1)
