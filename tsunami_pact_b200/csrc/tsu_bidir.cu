@@ -40,12 +40,12 @@ cudaError_t segment_occupancy(const Pen& pen, int* blocks_per_sm) {
   return e;
 }
 
-void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a) {
+void launch_segment(bool int16_history, int blocks, int threads, cudaStream_t st, const SegArgs& a) {
   const size_t smem = seg_smem_bytes(a.pen);
   if (int16_history)
-    segment_kernel<int16_t><<<blocks, kSegThreads, smem, st>>>(a);
+    segment_kernel<int16_t><<<blocks, threads, smem, st>>>(a);
   else
-    segment_kernel<int32_t><<<blocks, kSegThreads, smem, st>>>(a);
+    segment_kernel<int32_t><<<blocks, threads, smem, st>>>(a);
 }
 
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int32_t* pre_st, const int64_t* pre_off,

@@ -554,7 +554,7 @@ cudaError_t bidir_occupancy(int gw, int threads, size_t smem, int* occ);
 void launch_bidir(int gw, int blocks, int threads, size_t smem, cudaStream_t st, const BidirArgs& a);
 // The base-case kernels (tsu_segment.cuh), launched from tsu_bidir.cu.
 cudaError_t segment_occupancy(const Pen& pen, int* blocks_per_sm);  // the lower of the two history types
-void launch_segment(bool int16_history, int blocks, cudaStream_t st, const SegArgs& a);
+void launch_segment(bool int16_history, int blocks, int threads, cudaStream_t st, const SegArgs& a);
 void launch_seg_runs(bool write, int blocks, cudaStream_t st, int64_t n, const int32_t* pre_st, const int64_t* pre_off,
                      const int32_t* pre_len, const int64_t* first, const int64_t* run_off, const int32_t* run_len,
                      const uint32_t* runs, const int32_t* status, int64_t* out_len, const int64_t* out_off,

@@ -802,8 +802,12 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
       ctx->need_bytes = fixed + per_warp;
       return set_err(ctx, TSU_ENOMEM, "bidirectional mode: base-case history of one segment exceeds the budget");
     }
-    const int64_t blocks = (warps + wpb - 1) / wpb;
-    const size_t nw = (size_t)(blocks * wpb);
+    // whole blocks within the budget (rounded down); below one block's
+    // worth, one smaller block
+    int threads = tsu::kSegThreads;
+    int64_t blocks = warps / wpb;
+    if (blocks == 0) blocks = 1, threads = 32 * (int)warps;
+    const size_t nw = (size_t)(blocks * (threads / 32));
     if (per_warp * nw > ctx->b_scratch.cap) {
       release(ctx, ctx->b_scratch);
       if ((rc2 = grow(ctx, ctx->b_scratch, per_warp * nw))) return rc2;
@@ -834,11 +838,10 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
     a.pair_score = d_pair_score;
     a.queue = d_queue;
     a.work = d_cnt + 1;
-    tsu::launch_segment(h16, (int)blocks, st, a);
+    tsu::launch_segment(h16, (int)blocks, threads, st, a);
     CU(cudaGetLastError());
     ctx->timing.kernel_launches++;
-    log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(blocks * wpb) + ":" +
-           std::to_string(c);
+    log += (log.empty() ? "s" : " s") + std::to_string(scap) + "x" + std::to_string(nw) + ":" + std::to_string(c);
     unsigned long long* h_cur = reinterpret_cast<unsigned long long*>(static_cast<char*>(ctx->h_scalars.p) + 48);
     CU(cudaMemcpyAsync(h_cur, d_cursor, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CU(wait_stream(ctx, st));
