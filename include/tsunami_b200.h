@@ -57,8 +57,10 @@ extern "C" {
                                 no longest-first order: the reference's scheduling
                                 (one 32-thread block per pair, wfa_gpu.cu:113-114),
                                 kept as the "plain" baseline of the benchmarks */
-#define TSU_BIDIRECTIONAL 0x4u /* one-piece gap-affine, end to end: bidirectional
-                                  WFA.  Each score is the lowest total at which a
+#define TSU_BIDIRECTIONAL 0x4u /* one-piece gap-affine or a gap-linear metric
+                                  (edit, indel, gap-linear: run as gap-affine
+                                  with a zero gap opening), end to end:
+                                  bidirectional WFA.  Each score is the lowest total at which a
                                   forward and a reverse wavefront pass cross (the
                                   breakpoint search, two rings per pair), about
                                   half the wavefront cells of the forward pass; the

@@ -4,7 +4,8 @@ AddressSanitizer/UBSan, against the CPU oracle.  The breakpoint kernel
 (ora_crossing_split, the C form of oracle/bidir_rule.py crossing_split): the
 same lowest crossing total, component, forward diagonal and cut offset for
 every segment -- begin and end components M, I and D, empty and unequal
-segments, sub-ranges of longer pairs, one warp and warp groups.  The
+segments, sub-ranges of longer pairs, one warp and warp groups, and a
+zero gap opening (the gap-linear metrics run this way).  The
 base-case kernel (tsu_segment.cuh) against the oracle's segment alignment
 (ora_align_segment): the same operations."""
 import math
@@ -87,7 +88,7 @@ def _check(exe, oracle, recs, pen, gw):
 
 
 @pytest.mark.parametrize("pen,gw", [((4, 6, 2), 1), ((3, 5, 1), 1), ((5, 11, 3), 1), ((20, 1, 1), 1),
-                                    ((4, 6, 2), 4)])
+                                    ((4, 6, 2), 4), ((1, 0, 1), 1), ((3, 0, 1), 4)])
 def test_segments_match_oracle(emu_bidir, oracle, pen, gw):
     rng = random.Random(hash((pen, gw)) & 0xFFFF)
     recs = []
@@ -131,7 +132,7 @@ def _seg_ops(exe, recs, pen, step_cap, retries=None, h32=False):
 
 
 @pytest.mark.parametrize("pen,h32", [((4, 6, 2), False), ((3, 5, 1), False), ((20, 1, 1), False),
-                                     ((4, 6, 2), True)])
+                                     ((4, 6, 2), True), ((1, 0, 1), False)])
 def test_base_case_segments_match_oracle(emu_bidir, oracle, pen, h32):
     """The base-case kernel (tsu_segment.cuh): every segment's operations
     equal the oracle's segment alignment (ora_align_segment) for every begin

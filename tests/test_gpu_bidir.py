@@ -70,8 +70,8 @@ def test_bidirectional_argument_checks(oracle):
     import tsunami_pact_b200 as T
 
     pb, po, pl, tb, to, tl = _batch(T, 5, [100] * 4, [0.05] * 4)
-    with T.Aligner(device=0, metric="edit") as al:
-        with pytest.raises(T.AlignError):  # one-piece gap-affine only
+    with T.Aligner(4, 6, 2, gap_opening2=24, gap_extension2=1) as al:
+        with pytest.raises(T.AlignError):  # one gap piece only
             al.align_arrays(pb, po, pl, tb, to, tl, cigar=False, bidirectional=True)
     with T.Aligner(4, 6, 2) as al:
         al.set_ends_free(10, 10, 10, 10)
@@ -235,3 +235,32 @@ def test_bidirectional_tight_budget(aligner_factory):
     assert np.array_equal(s0, s1)
     assert np.array_equal(c0, c1)
     assert np.array_equal(r0, r1)
+
+
+@pytest.mark.parametrize("metric,xe", [("edit", (1, 1)), ("indel", (3, 1)), ("gap_linear", (2, 1))])
+def test_bidirectional_gap_linear_metrics(oracle, metric, xe):
+    """Edit, indel and gap-linear contexts run the bidirectional mode as
+    gap-affine with a zero gap opening: scores equal the linear oracle's (and
+    the forward kernels'), CIGARs equal the oracle's recursion at o = 0 and
+    cost the score."""
+    import tsunami_pact_b200 as T
+
+    x, e = xe
+    rng = np.random.default_rng(91 + x)
+    lengths = np.concatenate([rng.integers(0, 400, 250), rng.integers(400, 3000, 20), [0, 1, 6000]])
+    rates = np.concatenate([rng.uniform(0, 0.25, 270), [0.0, 1.0, 0.2]])
+    pb, po, pl, tb, to, tl = _batch(T, 91 + x, lengths, rates)
+    kw = {"metric": metric}
+    args = (x, 0, e) if metric == "gap_linear" else ()
+    with T.Aligner(*args, **kw) as al:
+        s, c, r = al.align_arrays(pb, po, pl, tb, to, tl, cigar=True, bidirectional=True)
+        fwd, _, _ = al.align_arrays(pb, po, pl, tb, to, tl, cigar=False)
+    want, _ = oracle.align_batch_linear_arrays(pb, po, pl, tb, to, tl, x, e, cigar=False)
+    assert np.array_equal(s, want)
+    assert np.array_equal(s, fwd)
+    base = base_score((x, 0, e))
+    for i in range(len(pl)):
+        p, t = bytes(pb[po[i]:po[i] + pl[i]]), bytes(tb[to[i]:to[i] + tl[i]])
+        ops = T.runs_to_ops(r[c[i]:c[i + 1]])
+        assert ops == oracle.bialign(p, t, x, 0, e, base_score=base, ring=True), i
+        assert oracle.cigar_cost(ops, p, t, x, 0, e) == want[i]

@@ -505,11 +505,22 @@ void carve_scratch(tsu_ctx* ctx, const Pass& ps, bool cigar, tsu::AlignArgs* a) 
 
 // ---- bidirectional mode (TSU_BIDIRECTIONAL) --------------------------------
 
+// Penalties of the bidirectional mode: the context's for gap-affine; for the
+// gap-linear models (edit, indel, gap-linear) gap-affine with a zero gap
+// opening -- the same M wavefronts (an I or D value never exceeds the M it
+// extends), so the same search and, with the oracle's recursion at o = 0,
+// the same optimal CIGARs.
+tsu::Pen bidir_pen(const tsu_ctx* ctx) {
+  const tsu::Pen& rp = ctx->rp;
+  if (rp.model() != tsu::kModelLinear) return rp;
+  return tsu::reduce_penalties(rp.x * ctx->g, 0, rp.ge * ctx->g, -1, 0, nullptr);
+}
+
 // Checks of the bidirectional mode's settings.
 int bidir_check(tsu_ctx* ctx) {
-  const tsu::Pen& rp = ctx->rp;
-  if (rp.model() != tsu::kModelAffine)
-    return set_err(ctx, TSU_EINVAL, "bidirectional mode: one-piece gap-affine penalties only");
+  const tsu::Pen rp = bidir_pen(ctx);
+  if (ctx->rp.model() == tsu::kModelDual)
+    return set_err(ctx, TSU_EINVAL, "bidirectional mode: one-piece gap-affine or gap-linear penalties only");
   if (ctx->ends_free[0] | ctx->ends_free[1] | ctx->ends_free[2] | ctx->ends_free[3])
     return set_err(ctx, TSU_EINVAL, "bidirectional mode: end-to-end alignment only");
   if (ctx->low_mem) return set_err(ctx, TSU_EINVAL, "bidirectional mode: no low-memory mode");
@@ -562,7 +573,7 @@ int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, c
                 int32_t* status, unsigned int* d_queue, unsigned long long* d_work, std::string* log) {
   cudaStream_t st = ctx->stream;
   int rc;
-  const tsu::Pen& rp = ctx->rp;
+  const tsu::Pen rp = bidir_pen(ctx);
   const int threads = gw <= 4 ? 128 : 32 * gw;
   const int gpb = threads / (32 * gw);
   const size_t smem = (size_t)gpb * tsu::bidir_group_smem(rp, gw);
@@ -733,7 +744,7 @@ int run_bidir_cigar(tsu_ctx* ctx, const tsu::SeqView& sv, int32_t* d_score, int3
   cudaStream_t st = ctx->stream;
   int rc;
   if ((rc = bidir_check(ctx))) return rc;
-  const tsu::Pen& rp = ctx->rp;
+  const tsu::Pen rp = bidir_pen(ctx);
   if ((rc = grow(ctx, ctx->b_counters, 64))) return rc;
   if ((rc = grow(ctx, ctx->b_clen64, sizeof(int64_t) * (n + 1)))) return rc;
   if ((rc = grow(ctx, ctx->b_bfirst, sizeof(int64_t) * (n + 1)))) return rc;
@@ -1543,7 +1554,7 @@ int predict_bytes(tsu_ctx* ctx, const BatchShape& sh, uint32_t flags, double hin
     // m + n per pair); scratch: the breakpoint rings of the largest size
     // class (groups x 2 directions x ring depth x 4 x (m + n + 3) int32) or
     // the leaf warps' history at the base step cap, whichever is larger
-    const tsu::Pen& rp = ctx->rp;
+    const tsu::Pen rp = bidir_pen(ctx);
     size_t chunk_max = 0, scratch_full = 0, scratch_min = 0;
     const int cap0 = tsu::bidir_base(rp) + 2 * rp.go + 4;
     for (int c = 0; c < K; ++c) {
