@@ -419,8 +419,9 @@ int tsu_server_create_metric(int metric, const int32_t* penalties, int num_penal
                              const tsu_server_config* cfg /* nullable */, tsu_server** out);
 /* Queued requests are dropped; running jobs finish first. */
 int tsu_server_destroy(tsu_server* srv);
-/* flags: TSU_SCORE_ONLY, TSU_BIDIRECTIONAL (one-piece gap-affine servers;
- * otherwise the request fails with TSU_EINVAL), both, or 0; only requests of
+/* flags: TSU_SCORE_ONLY, TSU_BIDIRECTIONAL (gap-affine and gap-linear
+ * servers; on a dual gap-affine one the request fails with TSU_EINVAL),
+ * both, or 0; only requests of
  * the same flags share a job.  TSU_EINVAL for bad pairs, TSU_ENOMEM when the
  * request cannot fit the budget even alone, TSU_EBUSY when the queue is
  * full.  The caller's buffers may be reused when it returns. */

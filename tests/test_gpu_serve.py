@@ -163,7 +163,7 @@ def test_bidirectional_requests(aligner_factory):
     """Requests with TSU_BIDIRECTIONAL, mixed with plain ones: every
     bidirectional result equals the batch path's bidirectional one on the
     same pairs, every plain result the plain one (requests of different
-    flags never share a job); an edit-distance server fails them with
+    flags never share a job); a dual gap-affine server fails them with
     TSU_EINVAL."""
     import tsunami_pact_b200 as T
 
@@ -179,7 +179,7 @@ def test_bidirectional_requests(aligner_factory):
         if cig:
             assert np.array_equal(g[1], c), k
             assert np.array_equal(g[2][: int(c[-1])], runs), k
-    with T.Server(device=0, metric="edit", workers=1) as srv:
+    with T.Server(4, 6, 2, gap_opening2=24, gap_extension2=1, workers=1) as srv:
         rid = srv.submit_arrays(*reqs[0], bidirectional=True)
         with pytest.raises(T.AlignError):
             srv.wait(rid, 600_000)

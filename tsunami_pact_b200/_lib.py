@@ -435,7 +435,7 @@ class Server:
     def submit_arrays(self, pbuf, poff, plen, tbuf, toff, tlen, cigar: bool = True,
                       bidirectional: bool = False) -> int:
         """Submit one request (tsu_submit); ``bidirectional=True``:
-        TSU_BIDIRECTIONAL (one-piece gap-affine servers)."""
+        TSU_BIDIRECTIONAL (gap-affine and gap-linear servers)."""
         n = len(plen)
         poff = np.ascontiguousarray(poff, dtype=np.int64)
         toff = np.ascontiguousarray(toff, dtype=np.int64)
