@@ -103,6 +103,29 @@ def test_c4_reduced_uneven(aligner_factory, oracle):
     _check_same(aligner_factory(), oracle, pats, txts)
 
 
+def test_wide_wavefronts_global_ring(aligner_factory, oracle):
+    """Pairs of 16-20 kbp whose wavefronts (up to ~40,000 diagonals) outgrow
+    every shared ring (16,368 diagonals at most): 32-warp passes on the
+    global ring, with bytes outside ACGT in one pair and one pair whose end
+    diagonal lies ~16,000 from 0; scores and CIGARs equal the oracle's, with
+    and without CIGARs."""
+    rng = np.random.default_rng(16)
+    lengths = rng.integers(16500, 20000, 4).astype(np.int32)
+    pats, txts = _gen(0x5453554E414D49 + 16, lengths, [0.25, 0.2, 0.15, 0.3])
+    p0 = bytearray(pats[0])
+    for i in range(0, len(p0), 997):
+        p0[i] = ord("N")
+    pats[0] = bytes(p0)
+    pats.append(pats[1][:3000])
+    txts.append(txts[1])  # n - m > 13,000: the end diagonal far from 0
+    al = aligner_factory()
+    _check_same(al, oracle, pats, txts)
+    assert "g32" in al.pass_log(), al.pass_log()
+    scores, _ = oracle.align_batch(pats, txts, 4, 6, 2, cigar=False)
+    got, _ = al.align(pats, txts, cigar=False)
+    assert list(got) == list(scores)
+
+
 def test_unequal_lengths_and_empty(aligner_factory, oracle):
     rng = random.Random(11)
     pats = ["", "", "A", "ACGT" * 50, "T" * 300, "ACGT" * 10]
