@@ -87,6 +87,10 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
   constexpr bool kWide = GW > 1 && GW < 32;
   static_assert(!(kModel & kLowMemFlag) || kCigar, "low-memory: CIGAR kernels");
   using RT = typename std::conditional<kMode == kModeShared, int16_t, int32_t>::type;
+  // null of a source read outside its slot's trimmed range: the int16 ring's
+  // null in shared mode, so that every value the cell loop computes stays
+  // within int16 and needs no lower clamp when stored
+  constexpr int32_t NUL = kMode == kModeShared ? (int32_t)kNull16 : kNull;
   // Global-ring groups of up to 16 warps stage the pair's packed words in
   // shared memory; the 32-warp groups run at 64 registers, where the staging
   // state costs spills, and read the words from global memory.
@@ -212,6 +216,21 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       auto store = [&](int idx, int32_t v) {
         if constexpr (kMode == kModeShared)
           ring[idx] = (RT)max(min(v, n + 1), (int32_t)kNull16);
+        else
+          ring[idx] = v;
+      };
+      // The cell loop's stores (sources read as NUL outside their ranges):
+      // an extended M is a valid offset (<= n) or NUL; a D value is the
+      // largest of its sources (M and D values one diagonal over), so at
+      // most n and at least kNull16; an I value is its largest source + 1, at
+      // least kNull16 + 1 and at most n + 2, clamped to n + 1.  A negative I
+      // value climbs one per diagonal it moves, as under store(), so every
+      // stored value keeps its validity and its order against any valid
+      // offset.
+      auto store_md = [&](int idx, int32_t v) { ring[idx] = (RT)v; };
+      auto store_i = [&](int idx, int32_t v) {
+        if constexpr (kMode == kModeShared)
+          ring[idx] = (RT)min(v, n + 1);
         else
           ring[idx] = v;
       };
@@ -407,7 +426,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             kB -= 31;  // block start bound
           }
           for (int k = lo + gt; k <= hi; k += GT) {
-            int32_t ins_o, ins_e = kNull, del_o, del_e = kNull, mis;
+            int32_t ins_o, ins_e = NUL, del_o, del_e = NUL, mis;
             const int kb = k - lane;
             if (kWide && kb >= kA && kb <= kB) {
               ins_o = ring[b_mo - 1 - lo_mo + k];
@@ -420,33 +439,33 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             } else {
               int j;
               j = k - 1 - lo_mo;
-              ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+              ins_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : NUL;
               j = k + 1 - lo_mo;
-              del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : kNull;
+              del_o = ((unsigned)j < (unsigned)c_mo) ? (int32_t)ring[b_mo + j] : NUL;
               j = k - lo_mm;
-              mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : kNull) + 1;
+              mis = (((unsigned)j < (unsigned)c_mm) ? (int32_t)ring[b_mm + j] : NUL) + 1;
               if constexpr (!kLin) {
                 j = k - 1 - lo_ie;
-                ins_e = ((unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : kNull;
+                ins_e = ((unsigned)j < (unsigned)c_ie) ? (int32_t)ring[b_ie + j] : NUL;
                 j = k + 1 - lo_de;
-                del_e = ((unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : kNull;
+                del_e = ((unsigned)j < (unsigned)c_de) ? (int32_t)ring[b_de + j] : NUL;
               }
             }
             int j;
             const int32_t ins = max(ins_o, ins_e) + 1;
             const int32_t del = max(del_o, del_e);
-            int32_t ins2 = kNull, del2 = kNull;
+            int32_t ins2 = NUL, del2 = NUL;
             uint32_t bits;
             int32_t p;
             if constexpr (kDual) {
               j = k - 1 - lo_mo2;
-              const int32_t ins2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+              const int32_t ins2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : NUL;
               j = k - 1 - lo_ie2;
-              const int32_t ins2_e = ((unsigned)j < (unsigned)c_ie2) ? (int32_t)ring[b_ie2 + j] : kNull;
+              const int32_t ins2_e = ((unsigned)j < (unsigned)c_ie2) ? (int32_t)ring[b_ie2 + j] : NUL;
               j = k + 1 - lo_mo2;
-              const int32_t del2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : kNull;
+              const int32_t del2_o = ((unsigned)j < (unsigned)c_mo2) ? (int32_t)ring[b_mo2 + j] : NUL;
               j = k + 1 - lo_de2;
-              const int32_t del2_e = ((unsigned)j < (unsigned)c_de2) ? (int32_t)ring[b_de2 + j] : kNull;
+              const int32_t del2_e = ((unsigned)j < (unsigned)c_de2) ? (int32_t)ring[b_de2 + j] : NUL;
               ins2 = max(ins2_o, ins2_e) + 1;
               del2 = max(del2_o, del2_e);
               // M = max(mismatch, D2, D1, I2, I1), ties in that order
@@ -472,7 +491,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
                 if (del_e >= del_o) bits |= kDExt;
               }
             }
-            int32_t om = kNull;
+            int32_t om = NUL;
             if constexpr (kWide) {
               // Extend M (wfa_gpu.cu:257-287) without a divergent region
               // around it: every lane compares its first 16-base window (an
@@ -491,7 +510,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
                 if (!d0 && rem > 16) lx = 16 + lcp16(P, vv + 16, T, hh + 16, rem - 16);
                 lx = min(lx, rem);
               }
-              om = vm ? p + lx : kNull;
+              om = vm ? p + lx : NUL;
               n_ext += (uint32_t)lx;
               fm = vm ? min(fm, k) : fm;
               lm = vm ? k : lm;
@@ -510,9 +529,9 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
               if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
               if (ends) fk = min(fk, k);
             }
-            store(w_m + k, om);
+            store_md(w_m + k, om);
             if (i_present) {
-              store(w_i + k, ins);
+              store_i(w_i + k, ins);
               if constexpr (kWide) {
                 const bool vi = in_bounds_sel(ins, k, m, n);
                 fi = vi ? min(fi, k) : fi;
@@ -523,7 +542,7 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
               }
             }
             if (d_present) {
-              store(w_d + k, del);
+              store_md(w_d + k, del);
               if constexpr (kWide) {
                 const bool vd = in_bounds_sel(del, k, m, n);
                 fd = vd ? min(fd, k) : fd;
@@ -535,13 +554,13 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             }
             if constexpr (kDual) {
               if (i2_present) {
-                store(w_i2 + k, ins2);
+                store_i(w_i2 + k, ins2);
                 const bool vi2 = in_bounds_sel(ins2, k, m, n);
                 fi2 = vi2 ? min(fi2, k) : fi2;
                 li2 = vi2 ? k : li2;
               }
               if (d2_present) {
-                store(w_d2 + k, del2);
+                store_md(w_d2 + k, del2);
                 const bool vd2 = in_bounds_sel(del2, k, m, n);
                 fd2 = vd2 ? min(fd2, k) : fd2;
                 ld2 = vd2 ? k : ld2;
