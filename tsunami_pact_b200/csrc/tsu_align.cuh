@@ -307,6 +307,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
       const int k_hi = k_end + a.ef_pe;
       const bool free_te = a.ef_te > 0;
       const int n_te = n - a.ef_te;
+      // End-to-end alignments end on diagonal k_end alone: the cell loop
+      // skips the end test, and after it the thread that computed k_end
+      // reads that M value back from the ring (its own store: a valid
+      // offset or the null, so >= n only at the end point).
+      const bool ends_free = a.ef_pe > 0 || free_te;
       // One score step: the wavefronts of score s + 1 from the ring.  kH (a
       // compile-time tag): write the step's backtrace words and step-table
       // entry; detect: test for the end (not while recomputing history).
@@ -514,9 +519,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
               n_ext += (uint32_t)lx;
               fm = vm ? min(fm, k) : fm;
               lm = vm ? k : lm;
-              bool ends = vm & (om >= n) & (k <= k_hi);
-              if (free_te) ends |= vm & ((om - k) >= m) & (om >= n_te);
-              fk = ends ? min(fk, k) : fk;
+              if (ends_free) {
+                bool ends = vm & (om >= n) & (k <= k_hi);
+                if (free_te) ends |= vm & ((om - k) >= m) & (om >= n_te);
+                fk = ends ? min(fk, k) : fk;
+              }
             } else if (in_bounds(p, k, m, n)) {
               const int vv = p - k;
               const int rem = min(m - vv, n - p);
@@ -525,9 +532,11 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
               n_ext += (uint32_t)lx;
               fm = min(fm, k);
               lm = k;
-              bool ends = (om >= n) & (k <= k_hi);
-              if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
-              if (ends) fk = min(fk, k);
+              if (ends_free) {
+                bool ends = (om >= n) & (k <= k_hi);
+                if (free_te) ends |= ((om - k) >= m) & (om >= n_te);
+                if (ends) fk = min(fk, k);
+              }
             }
             store_md(w_m + k, om);
             if (i_present) {
@@ -568,6 +577,9 @@ __global__ void __launch_bounds__(cta_threads<GW>(), (cta_min_blocks<kMode, GW>(
             }
             if constexpr (kH) hrow[k] = ((uint32_t)p << (kDual ? 8 : 4)) | bits;
           }
+          if (!ends_free && k_end >= lo && k_end <= hi && ((k_end - lo) & (GT - 1)) == gt &&
+              (int32_t)ring[w_m + k_end] >= n)
+            fk = k_end;
           fm = __reduce_min_sync(FULL, fm);
           lm = __reduce_max_sync(FULL, lm);
           fi = __reduce_min_sync(FULL, fi);
