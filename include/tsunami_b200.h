@@ -263,8 +263,8 @@ int tsu_align_batch_device(tsu_ctx* ctx, const tsu_batch* dev_batch, tsu_result*
  * before it returns.  It allocates no device memory: its scratch is a fixed
  * 32 MiB array compiled into this library, held by every GPU that loads the
  * library until the process exits.  The first call on a device looks up that
- * array's device address (driver work: make that first call before any
- * stream capture).  All calls share the one array: calls whose GPU work
+ * array's device address (driver work, once per device).  All calls share
+ * the one array: calls whose GPU work
  * overlaps race on it, so serialize them per device.  Batches needing more
  * than the array holds (about 55,000 pairs of 1 kbp, fewer for longer pairs;
  * also any batch whose longest pair's HBM wavefront ring would not fit beside

@@ -13,8 +13,8 @@
 // loads the library holds that array until the process exits.  The host code
 // below never uses the array's name as an address: on the first call on a
 // device, with that device current, it asks the driver for the array's device
-// address with cudaGetSymbolAddress and caches it per device.  That first
-// call therefore does driver work and should come before any stream capture.
+// address with cudaGetSymbolAddress and caches it per device, so that first
+// call does driver work.
 // Each call then carves its buffers (word counts, packed sequences, per-pair
 // status, the work-queue counters, and -- for pairs too wide for the shared-
 // memory ring -- a global wavefront ring) out of the array, clears what must
