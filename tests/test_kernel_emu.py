@@ -196,6 +196,30 @@ def test_warp_groups(emu, oracle, gw, shared):
     assert gws.split(",")[0] == ("s" if shared else "g") + str(gw) or not shared
 
 
+@pytest.mark.parametrize("gw,shared", [(1, True), (1, False), (2, True), (4, True), (4, False)])
+def test_end_diagonal_positions(emu, oracle, gw, shared):
+    """The end-to-end end test reads M on diagonal n - m back from the ring
+    in the thread that computed it: end diagonals at every offset around the
+    warp and group boundaries (n - m from -70 to 100, including 0, +-1,
+    +-31, +-32, +-33, 63-65), pairs that end at score 0 and empty sides,
+    with and without CIGARs, on both rings."""
+    rng = random.Random(90 + gw * 2 + shared)
+    pairs = []
+    for d in [-70, -65, -64, -63, -33, -32, -31, -1, 0, 1, 31, 32, 33, 63, 64, 65, 100]:
+        p, t = _edited(rng, rng.randint(80, 160), 0.04)
+        if d > 0:
+            t = t + "".join(rng.choice("ACGT") for _ in range(d))
+        elif d < 0:
+            p = p + "".join(rng.choice("ACGT") for _ in range(-d))
+        pairs.append((p, t))
+    pairs += [("ACGT" * 20, "ACGT" * 20), ("", "ACG"), ("ACG", ""), ("", "")]
+    check(emu, oracle, pairs, shared_first=shared, gw=gw)
+    bp = [(_b(p), _b(t)) for p, t in pairs]
+    got, _, _, _ = run_emu(emu, bp, cigar=False, shared_first=shared, gw=gw)
+    for (p, t), (sc, ops) in zip(bp, got):
+        assert sc == oracle.align(p, t)[0] and ops == "", (p, t)
+
+
 def test_ladder_to_groups(emu, oracle):
     """Pairs whose wavefronts outgrow one warp's shared ring (384 diagonals)
     climb the ladder to a group with a wider shared ring."""
