@@ -565,8 +565,8 @@ int bidir_gw(int32_t side) { return side < 2048 ? 1 : (side < 16384 ? 4 : 16); }
 // One persistent launch of the breakpoint kernel (tsu_bidir.cuh) over c
 // segments (device) of one size class, one group per segment at a time (gw
 // = 1, 4 or 16 warps), both rings of a group in device memory (2 directions
-// x ring depth x 4 components x (max_bases + 3) int32, from the scratch
-// buffer).  Writes T, comp, k, h at out + 0, out + stride, out + 2 stride,
+// x ring depth x 4 components x (max_bases + 3) values, int16 below 16 warps
+// and int32 at 16, from the scratch buffer).  Writes T, comp, k, h at out + 0, out + stride, out + 2 stride,
 // out + 3 stride and the statuses; adds cells and steps to d_work[0..1].
 int bidir_split(tsu_ctx* ctx, const tsu::SeqView& sv, const tsu::PackView& pk, const tsu::PackView& pkr,
                 const tsu::BidirSeg* segs, int64_t c, int gw, int32_t max_bases, int32_t* out, int64_t stride,
