@@ -202,7 +202,8 @@ def test_end_diagonal_positions(emu, oracle, gw, shared):
     in the thread that computed it: end diagonals at every offset around the
     warp and group boundaries (n - m from -70 to 100, including 0, +-1,
     +-31, +-32, +-33, 63-65), pairs that end at score 0 and empty sides,
-    with and without CIGARs, on both rings."""
+    with and without CIGARs, on both rings; gap-affine, dual gap-affine and
+    gap-linear kernels."""
     rng = random.Random(90 + gw * 2 + shared)
     pairs = []
     for d in [-70, -65, -64, -63, -33, -32, -31, -1, 0, 1, 31, 32, 33, 63, 64, 65, 100]:
@@ -218,6 +219,13 @@ def test_end_diagonal_positions(emu, oracle, gw, shared):
     got, _, _, _ = run_emu(emu, bp, cigar=False, shared_first=shared, gw=gw)
     for (p, t), (sc, ops) in zip(bp, got):
         assert sc == oracle.align(p, t)[0] and ops == "", (p, t)
+    # the dual gap-affine and gap-linear kernels take the same end test
+    got, _, _, _ = run_emu(emu, bp, (4, 6, 2, 24, 1), shared_first=shared, gw=gw)
+    for (p, t), (sc, ops) in zip(bp, got):
+        assert (sc, ops) == oracle.align2(p, t), (p, t)
+    got, _, _, _ = run_emu(emu, bp, (1, -1, 1), shared_first=shared, gw=gw)
+    for (p, t), (sc, ops) in zip(bp, got):
+        assert (sc, ops) == oracle.align_linear(p, t, 1, 1), (p, t)
 
 
 def test_ladder_to_groups(emu, oracle):
